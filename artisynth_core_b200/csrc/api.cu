@@ -1,0 +1,786 @@
+// api.cu -- C ABI of libb200fem.so (declared in include/b200fem.h) and the
+// pack builder that turns host models into device-resident arrays.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+
+#include "engine.h"
+
+namespace b200fem {
+
+cudaError_t launch_forces_only(Engine& eng);
+int pcg_max_grid(int device);
+int pcg_max_cta_pieces();
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_global_err;
+
+void set_global_error(const std::string& s) {
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  g_global_err = s;
+}
+
+int fail(Engine* e, int code, const std::string& msg) {
+  if (e) e->last_error = msg;
+  else set_global_error(msg);
+  return code;
+}
+
+int cuda_fail(Engine* e, cudaError_t err, const char* where) {
+  return fail(e, B200FEM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(err));
+}
+
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return cuda_fail(&eng, _e, #call); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(Engine& eng, T** ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)ptr, count * sizeof(T));
+  if (e == cudaSuccess) eng.allocations.push_back((void*)*ptr);
+  return e;
+}
+
+template <typename T>
+cudaError_t upload(Engine& eng, T** ptr, const std::vector<T>& v) {
+  cudaError_t e = dalloc(eng, ptr, v.size());
+  if (e != cudaSuccess) return e;
+  if (!v.empty()) e = cudaMemcpy(*ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+}  // namespace
+
+void free_pack(Engine& eng) {
+  for (void* p : eng.allocations) cudaFree(p);
+  eng.allocations.clear();
+  eng.d = DevPack();
+  eng.built = false;
+  eng.have_matrix = false;
+}
+
+int build_pack(Engine& eng) {
+  free_pack(eng);
+  const int M = (int)eng.models.size();
+  if (M == 0) return fail(&eng, B200FEM_ERR_STATE, "no model defined");
+  eng.elem_type = eng.models[0].elem_type;
+  for (auto& m : eng.models) {
+    if (m.elem_type != eng.elem_type)
+      return fail(&eng, B200FEM_ERR_UNSUPPORTED, "all models of a pack must use one element type");
+    if (!m.has_material) return fail(&eng, B200FEM_ERR_STATE, "material not set");
+    if (m.n_nodes <= 0 || m.n_elems <= 0) return fail(&eng, B200FEM_ERR_STATE, "mesh not set");
+  }
+  eng.hosts.assign(M, ModelHost());
+  for (int m = 0; m < M; m++) {
+    std::string err;
+    int st = setup_model_host(eng.models[m], eng.hosts[m], err);
+    if (st != B200FEM_OK) return fail(&eng, st, "model " + std::to_string(m) + ": " + err);
+  }
+  const int nen = eng.hosts[0].nen, nip = eng.hosts[0].nip, npair = eng.hosts[0].npair;
+  eng.nen = nen;
+  eng.nip = nip;
+  eng.npair = npair;
+  // offsets
+  eng.node_off.assign(M + 1, 0);
+  eng.elem_off.assign(M + 1, 0);
+  eng.row_off.assign(M + 1, 0);
+  eng.blk_off.assign(M + 1, 0);
+  for (int m = 0; m < M; m++) {
+    eng.node_off[m + 1] = eng.node_off[m] + eng.models[m].n_nodes;
+    eng.elem_off[m + 1] = eng.elem_off[m] + eng.models[m].n_elems;
+    eng.row_off[m + 1] = eng.row_off[m] + eng.hosts[m].n_active;
+    eng.blk_off[m + 1] = eng.blk_off[m] + (long long)eng.hosts[m].col.size();
+  }
+  const int N = eng.node_off[M], E = eng.elem_off[M], R = eng.row_off[M];
+  const long long NB = eng.blk_off[M];
+  if (NB >= (1ll << 31) || (long long)E * npair * 2 >= (1ll << 31))
+    return fail(&eng, B200FEM_ERR_UNSUPPORTED, "pack too large for 32-bit block indices");
+  DevPack& d = eng.d;
+  d.n_models = M;
+  d.n_nodes = N;
+  d.n_elems = E;
+  d.n_rows = R;
+  d.nnzb = NB;
+
+  // ---- host arrays
+  std::vector<double> x(3 * (size_t)N), mass(N), mat((size_t)M * kMatParams, 0.0), step((size_t)M * 8, 0.0);
+  std::vector<int> node_model(N), sidx(N), act_node(R), row_model(R);
+  std::vector<int> conn((size_t)E * nen), elem_model(E);
+  std::vector<double> invJ0((size_t)E * nip * 9), winvJ0((size_t)E * 9);
+  bool any_linear = false, any_nodal = false;
+  for (auto& m : eng.models) any_linear |= (m.mat_kind == B200FEM_MAT_LINEAR);
+  for (auto& h : eng.hosts) any_nodal |= (h.incomp == B200FEM_INCOMP_NODAL);
+  std::vector<double> K0, f0, node_rest_vol;
+  if (any_linear) {
+    K0.assign((size_t)E * nen * nen * 9, 0.0);
+    f0.assign((size_t)E * nen * 3, 0.0);
+  }
+  if (any_nodal) node_rest_vol.assign(N, 1.0);
+  std::vector<int> rowptr(R + 1, 0), col(NB), blk_diag(R), blk_row(NB);
+  for (int m = 0; m < M; m++) {
+    const ModelDesc& md = eng.models[m];
+    const ModelHost& h = eng.hosts[m];
+    const int no = eng.node_off[m], eo = eng.elem_off[m], ro = eng.row_off[m];
+    const long long bo = eng.blk_off[m];
+    std::copy(md.rest.begin(), md.rest.end(), x.begin() + 3 * (size_t)no);
+    std::copy(h.mass.begin(), h.mass.end(), mass.begin() + no);
+    for (int n = 0; n < md.n_nodes; n++) {
+      node_model[no + n] = m;
+      sidx[no + n] = h.sidx[n] >= 0 ? ro + h.sidx[n] : -1;
+    }
+    for (int r = 0; r < h.n_active; r++) {
+      act_node[ro + r] = no + h.act_node[r];
+      row_model[ro + r] = m;
+      rowptr[ro + r + 1] = (int)(bo + h.rowptr[r + 1]);
+      for (int p = h.rowptr[r]; p < h.rowptr[r + 1]; p++) {
+        col[bo + p] = ro + h.col[p];
+        blk_row[bo + p] = ro + r;
+        if (h.col[p] == r) blk_diag[ro + r] = (int)(bo + p);
+      }
+    }
+    for (size_t q = 0; q < (size_t)md.n_elems * nen; q++) conn[(size_t)eo * nen + q] = no + md.conn[q];
+    for (int e = 0; e < md.n_elems; e++) elem_model[eo + e] = m;
+    std::copy(h.invJ0.begin(), h.invJ0.end(), invJ0.begin() + (size_t)eo * nip * 9);
+    std::copy(h.winvJ0.begin(), h.winvJ0.end(), winvJ0.begin() + (size_t)eo * 9);
+    if (!h.K0.empty()) {
+      std::copy(h.K0.begin(), h.K0.end(), K0.begin() + (size_t)eo * nen * nen * 9);
+      std::copy(h.f0.begin(), h.f0.end(), f0.begin() + (size_t)eo * nen * 3);
+    }
+    if (!h.node_rest_vol.empty())
+      std::copy(h.node_rest_vol.begin(), h.node_rest_vol.end(), node_rest_vol.begin() + no);
+    std::copy(md.mat_params, md.mat_params + kMatParams, mat.begin() + (size_t)m * kMatParams);
+    step[(size_t)m * 8 + 0] = 0.01;
+    step[(size_t)m * 8 + 1] = 2.0;
+    step[(size_t)m * 8 + 6] = 1e-10;
+  }
+  // ---- element-to-block scatter map and per-block contribution lists
+  auto block_of = [&](int r, int c) -> int {
+    auto b = col.begin() + rowptr[r], e = col.begin() + rowptr[r + 1];
+    auto it = std::lower_bound(b, e, c);
+    return (it != e && *it == c) ? (int)(it - col.begin()) : -1;
+  };
+  eng.h_scatter.assign((size_t)E * nen * nen, -1);
+  std::vector<int> cptr(NB + 1, 0);
+  for (int e = 0; e < E; e++) {
+    const int* nodes = &conn[(size_t)e * nen];
+    for (int a = 0; a < nen; a++)
+      for (int b = 0; b < nen; b++) {
+        int ra = sidx[nodes[a]], rb = sidx[nodes[b]];
+        if (ra < 0 || rb < 0) continue;
+        int p = block_of(ra, rb);
+        if (p < 0) return fail(&eng, B200FEM_ERR_STATE, "internal: element pair outside the pattern");
+        eng.h_scatter[((size_t)e * nen + a) * nen + b] = p;
+        cptr[p + 1]++;
+      }
+  }
+  for (long long p = 0; p < NB; p++) cptr[p + 1] += cptr[p];
+  std::vector<int> cidx(cptr[NB]);
+  {
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int e = 0; e < E; e++) {
+      int w = 0;
+      for (int a = 0; a < nen; a++)
+        for (int b = a; b < nen; b++, w++) {
+          int pab = eng.h_scatter[((size_t)e * nen + a) * nen + b];
+          if (pab < 0) continue;
+          int code = (int)(((long long)e * npair + w) << 1);
+          cidx[fill[pab]++] = code;  // K_ab at (a, b)
+          if (a != b) {
+            int pba = eng.h_scatter[((size_t)e * nen + b) * nen + a];
+            cidx[fill[pba]++] = code | 1;  // K_ab^T at (b, a)
+          }
+        }
+    }
+  }
+  // node -> element incidences in element order
+  std::vector<int> iptr(N + 1, 0);
+  for (size_t q = 0; q < conn.size(); q++) iptr[conn[q] + 1]++;
+  for (int n = 0; n < N; n++) iptr[n + 1] += iptr[n];
+  std::vector<int> iidx(conn.size());
+  {
+    std::vector<int> fill(iptr.begin(), iptr.end() - 1);
+    for (int e = 0; e < E; e++)
+      for (int a = 0; a < nen; a++) iidx[fill[conn[(size_t)e * nen + a]]++] = e * nen + a;
+  }
+  // ---- element groups (runs of models with one material kind)
+  eng.groups.clear();
+  for (int m = 0; m < M; m++) {
+    ElemGroup g;
+    g.e0 = eng.elem_off[m];
+    g.e1 = eng.elem_off[m + 1];
+    g.elem_type = eng.elem_type;
+    g.mat_kind = eng.models[m].mat_kind;
+    g.corotated = (g.mat_kind == B200FEM_MAT_LINEAR) ? (eng.models[m].mat_params[2] != 0) : 0;
+    g.nodal = eng.hosts[m].incomp == B200FEM_INCOMP_NODAL;
+    if (!eng.groups.empty()) {
+      ElemGroup& last = eng.groups.back();
+      if (last.mat_kind == g.mat_kind && last.corotated == g.corotated && last.nodal == g.nodal &&
+          last.e1 == g.e0) {
+        last.e1 = g.e1;
+        continue;
+      }
+    }
+    eng.groups.push_back(g);
+  }
+  if (any_nodal) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "NODAL incompressibility is not built yet");
+  if (eng.precision != B200FEM_PREC_FP64)
+    return fail(&eng, B200FEM_ERR_UNSUPPORTED, "mixed precision is not built yet");
+
+  // ---- PCG work split: CTAs own contiguous row ranges balanced by blocks,
+  // cut into pieces at model boundaries
+  int gmax = pcg_max_grid(eng.device);
+  int G = std::max(1, std::min(gmax, (R + 31) / 32));
+  std::vector<int> piece_row, piece_model, cta_piece, model_piece(M + 1, 0);
+  for (;;) {
+    piece_row.clear();
+    piece_model.clear();
+    cta_piece.assign(G + 1, 0);
+    std::vector<int> cut(G + 1, R);
+    cut[0] = 0;
+    int r = 0;
+    for (int c = 1; c < G; c++) {
+      long long target = NB * c / G;
+      while (r < R && rowptr[r] < target) r++;
+      cut[c] = std::max(r, cut[c - 1]);
+    }
+    int maxp = 0;
+    for (int c = 0; c < G; c++) {
+      cta_piece[c] = (int)piece_model.size();
+      int a = cut[c], b = cut[c + 1];
+      while (a < b) {
+        int m = row_model[a];
+        int e = std::min(b, eng.row_off[m + 1]);
+        piece_row.push_back(a);
+        piece_model.push_back(m);
+        a = e;
+      }
+      maxp = std::max(maxp, (int)piece_model.size() - cta_piece[c]);
+    }
+    cta_piece[G] = (int)piece_model.size();
+    piece_row.push_back(R);
+    if (maxp <= pcg_max_cta_pieces()) break;
+    if (G >= gmax) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for one PCG launch");
+    G = std::min(gmax, G * 2);
+  }
+  for (size_t k = 0; k < piece_model.size(); k++) model_piece[piece_model[k] + 1] = (int)k + 1;
+  for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
+  eng.pcg_grid = G;
+  d.n_pieces = (int)piece_model.size();
+
+  // ---- device upload
+  CK(upload(eng, &d.x, x));
+  CK(dalloc(eng, &d.v, 3 * (size_t)N));
+  CK(cudaMemset(d.v, 0, 3 * sizeof(double) * (size_t)N));
+  CK(dalloc(eng, &d.fext, 3 * (size_t)N));
+  CK(cudaMemset(d.fext, 0, 3 * sizeof(double) * (size_t)N));
+  CK(upload(eng, &d.mass, mass));
+  CK(upload(eng, &d.node_model, node_model));
+  CK(upload(eng, &d.sidx, sidx));
+  CK(upload(eng, &d.act_node, act_node));
+  CK(upload(eng, &d.row_model, row_model));
+  CK(upload(eng, &d.conn, conn));
+  CK(upload(eng, &d.elem_model, elem_model));
+  CK(upload(eng, &d.invJ0, invJ0));
+  CK(upload(eng, &d.winvJ0, winvJ0));
+  if (any_linear) {
+    CK(upload(eng, &d.K0, K0));
+    CK(upload(eng, &d.f0, f0));
+  }
+  CK(upload(eng, &d.blk_rowptr, rowptr));
+  CK(upload(eng, &d.blk_col, col));
+  CK(upload(eng, &d.blk_diag, blk_diag));
+  CK(upload(eng, &d.blk_row, blk_row));
+  CK(upload(eng, &d.contrib_ptr, cptr));
+  CK(upload(eng, &d.contrib_idx, cidx));
+  CK(upload(eng, &d.inc_ptr, iptr));
+  CK(upload(eng, &d.inc_idx, iidx));
+  CK(dalloc(eng, &d.elemK, (size_t)E * npair * 9));
+  CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
+  CK(dalloc(eng, &d.K, (size_t)NB * 9));
+  CK(dalloc(eng, &d.S, (size_t)NB * 9));
+  CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
+  CK(dalloc(eng, &d.fint, 3 * (size_t)N));
+  for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w}) {
+    CK(dalloc(eng, v, 3 * (size_t)R));
+    CK(cudaMemset(*v, 0, 3 * sizeof(double) * (size_t)R));
+  }
+  CK(upload(eng, &d.mat, mat));
+  CK(upload(eng, &d.step, step));
+  if (any_nodal) {
+    CK(upload(eng, &d.node_rest_vol, node_rest_vol));
+    CK(dalloc(eng, &d.node_vol, (size_t)N));
+    CK(dalloc(eng, &d.node_p, (size_t)N));
+  }
+  CK(dalloc(eng, &d.partials, (size_t)d.n_pieces * 4));
+  CK(upload(eng, &d.piece_row, piece_row));
+  CK(upload(eng, &d.piece_model, piece_model));
+  CK(upload(eng, &d.model_piece, model_piece));
+  CK(upload(eng, &d.cta_piece, cta_piece));
+  d.unconv_cap = 200000;
+  CK(dalloc(eng, &d.unconv, (size_t)d.unconv_cap + 2));
+  {
+    // models without active rows never run PCG: report them converged
+    std::vector<double> ms((size_t)M * 4, 0.0);
+    for (int m = 0; m < M; m++) ms[(size_t)m * 4 + 2] = 1.0;
+    CK(upload(eng, &d.model_scal, ms));
+  }
+  CK(dalloc(eng, &d.barrier, 2));
+  CK(cudaMemset(d.barrier, 0, 2 * sizeof(unsigned)));
+  CK(dalloc(eng, &d.flags, 4));
+  CK(cudaMemset(d.flags, 0, 4 * sizeof(int)));
+  CK(dalloc(eng, &d.dmin, 1));
+  // host copies for queries
+  eng.h_rowptr = rowptr;
+  eng.h_col = col;
+  eng.h_sidx = sidx;
+  eng.h_mass = mass;
+  eng.built = true;
+  return B200FEM_OK;
+}
+
+}  // namespace b200fem
+
+using namespace b200fem;
+
+struct b200fem_engine {
+  Engine eng;
+};
+
+#define ENG(h)                                                    \
+  if (!(h)) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "null handle"); \
+  Engine& eng = (h)->eng;                                         \
+  {                                                               \
+    cudaError_t _se = cudaSetDevice(eng.device);                  \
+    if (_se != cudaSuccess) return cuda_fail(&eng, _se, "cudaSetDevice"); \
+  }
+
+#define NEED_BUILT()                                                       \
+  if (!eng.built) return fail(&eng, B200FEM_ERR_STATE, "b200fem_build has not been called")
+
+extern "C" {
+
+int b200fem_version(void) { return 10000; }
+
+b200fem_handle b200fem_create(const b200fem_config* cfg) {
+  int dev = cfg ? cfg->device : 0;
+  int prec = cfg ? cfg->precision : B200FEM_PREC_FP64;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    set_global_error(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (dev < 0 || dev >= count) {
+    set_global_error("invalid device ordinal");
+    return nullptr;
+  }
+  if (prec != B200FEM_PREC_FP64 && prec != B200FEM_PREC_MIXED) {
+    set_global_error("invalid precision");
+    return nullptr;
+  }
+  if ((e = cudaSetDevice(dev)) != cudaSuccess) {
+    set_global_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  cudaDeviceProp prop;
+  if ((e = cudaGetDeviceProperties(&prop, dev)) != cudaSuccess) {
+    set_global_error(std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (prop.major < 10) {
+    set_global_error("libb200fem requires an sm_100 (Blackwell) device");
+    return nullptr;
+  }
+  b200fem_engine* h = new b200fem_engine();
+  h->eng.device = dev;
+  h->eng.precision = prec;
+  h->eng.num_sms = prop.multiProcessorCount;
+  if ((e = cudaStreamCreateWithFlags(&h->eng.stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    set_global_error(std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    delete h;
+    return nullptr;
+  }
+  for (auto& ev : h->eng.ev) cudaEventCreate(&ev);
+  h->eng.models.assign(1, ModelDesc());
+  return h;
+}
+
+int b200fem_destroy(b200fem_handle h) {
+  if (!h) return B200FEM_OK;
+  cudaSetDevice(h->eng.device);
+  if (h->eng.stream) cudaStreamSynchronize(h->eng.stream);
+  free_pack(h->eng);
+  for (auto& ev : h->eng.ev)
+    if (ev) cudaEventDestroy(ev);
+  if (h->eng.stream) cudaStreamDestroy(h->eng.stream);
+  delete h;
+  return B200FEM_OK;
+}
+
+const char* b200fem_last_error(b200fem_handle h) {
+  if (!h) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    static thread_local std::string copy;
+    copy = g_global_err;
+    return copy.c_str();
+  }
+  return h->eng.last_error.c_str();
+}
+
+int b200fem_grid_dims(int elem_type, int nx, int ny, int nz, int* n_nodes, int* n_elems) {
+  if (!n_nodes || !n_elems) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "null output");
+  int st = grid_dims(elem_type, nx, ny, nz, n_nodes, n_elems);
+  if (st != B200FEM_OK) return fail(nullptr, st, "invalid grid arguments");
+  return B200FEM_OK;
+}
+
+int b200fem_create_grid(int elem_type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
+                        int* conn) {
+  int nn, ne;
+  if (grid_dims(elem_type, nx, ny, nz, &nn, &ne) != B200FEM_OK || !xyz || !conn)
+    return fail(nullptr, B200FEM_ERR_INVALID_ARG, "invalid grid arguments");
+  create_grid(elem_type, wx, wy, wz, nx, ny, nz, xyz, conn);
+  return B200FEM_OK;
+}
+
+int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
+                        unsigned long long seed, double* xyz) {
+  if (nx < 1 || ny < 1 || nz < 1 || !xyz) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "invalid grid arguments");
+  jitter_grid(nx, ny, nz, wx, wy, wz, frac, seed, xyz);
+  return B200FEM_OK;
+}
+
+int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz, int n_elems,
+                     const int* conn, const int* fixed) {
+  ENG(h);
+  if (elem_type != B200FEM_ELEM_TET && elem_type != B200FEM_ELEM_HEX)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
+  if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
+  int nen = elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  ModelDesc& m = eng.models[0];
+  m.elem_type = elem_type;
+  m.n_nodes = n_nodes;
+  m.n_elems = n_elems;
+  m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
+  m.conn.assign(conn, conn + (size_t)nen * n_elems);
+  m.fixed.assign(n_nodes, 0);
+  if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
+  free_pack(eng);
+  return B200FEM_OK;
+}
+
+int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, double density, int incomp) {
+  ENG(h);
+  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_MOONEYRIVLIN || !params)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
+  if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
+  ModelDesc& m = eng.models[0];
+  m.mat_kind = mat_kind;
+  int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_NEOHOOKEAN ? 2 : 8;
+  std::fill(m.mat_params, m.mat_params + kMatParams, 0.0);
+  std::copy(params, params + np, m.mat_params);
+  m.density = density;
+  m.incomp_request = incomp;
+  m.has_material = true;
+  free_pack(eng);
+  return B200FEM_OK;
+}
+
+int b200fem_build(b200fem_handle h) {
+  ENG(h);
+  return build_pack(eng);
+}
+
+int b200fem_get_sizes(b200fem_handle h, int* n_active, int* nnzb, int* crs_full, int* crs_upper) {
+  ENG(h);
+  NEED_BUILT();
+  if (n_active) *n_active = eng.d.n_rows;
+  if (nnzb) *nnzb = (int)eng.d.nnzb;
+  if (crs_full) *crs_full = (int)(9 * eng.d.nnzb);
+  if (crs_upper) {
+    long long up = 0;
+    for (int r = 0; r < eng.d.n_rows; r++)
+      for (int p = eng.h_rowptr[r]; p < eng.h_rowptr[r + 1]; p++) {
+        if (eng.h_col[p] > r) up += 9;
+        else if (eng.h_col[p] == r) up += 6;
+      }
+    *crs_upper = (int)up;
+  }
+  return B200FEM_OK;
+}
+
+int b200fem_get_solve_index(b200fem_handle h, int* sidx) {
+  ENG(h);
+  NEED_BUILT();
+  std::copy(eng.h_sidx.begin(), eng.h_sidx.end(), sidx);
+  return B200FEM_OK;
+}
+
+int b200fem_get_pattern(b200fem_handle h, int* rowptr, int* col) {
+  ENG(h);
+  NEED_BUILT();
+  if (rowptr) std::copy(eng.h_rowptr.begin(), eng.h_rowptr.end(), rowptr);
+  if (col) std::copy(eng.h_col.begin(), eng.h_col.end(), col);
+  return B200FEM_OK;
+}
+
+// SparseBlockMatrix.getCRSIndices (SparseBlockMatrix.java:1511-1532) and
+// SparseNumberedBlockMatrix.createCrsBlockSlotMap (:389-498), 0-based
+static int crs_walk(Engine& eng, int partition, int* row_offs, int* col_idx, int* slots) {
+  int nnz = 0;
+  for (int r = 0; r < eng.d.n_rows; r++) {
+    for (int i = 0; i < 3; i++) {
+      int row = 3 * r + i;
+      if (row_offs) row_offs[row] = nnz;
+      for (int p = eng.h_rowptr[r]; p < eng.h_rowptr[r + 1]; p++) {
+        int bj = eng.h_col[p];
+        for (int c = 0; c < 3; c++) {
+          int colg = 3 * bj + c;
+          if (partition == B200FEM_PART_UPPER && colg < row) {
+            if (slots) slots[(size_t)p * 9 + 3 * i + c] = -1;
+            continue;
+          }
+          if (col_idx) col_idx[nnz] = colg;
+          if (slots) slots[(size_t)p * 9 + 3 * i + c] = nnz;
+          nnz++;
+        }
+      }
+    }
+  }
+  if (row_offs) row_offs[3 * eng.d.n_rows] = nnz;
+  return nnz;
+}
+
+int b200fem_get_crs_indices(b200fem_handle h, int partition, int* row_offs, int* col_idx) {
+  ENG(h);
+  NEED_BUILT();
+  if (partition != B200FEM_PART_FULL && partition != B200FEM_PART_UPPER)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown partition");
+  crs_walk(eng, partition, row_offs, col_idx, nullptr);
+  return B200FEM_OK;
+}
+
+int b200fem_get_slot_map(b200fem_handle h, int partition, int* slots) {
+  ENG(h);
+  NEED_BUILT();
+  if (partition != B200FEM_PART_FULL && partition != B200FEM_PART_UPPER)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown partition");
+  crs_walk(eng, partition, nullptr, nullptr, slots);
+  return B200FEM_OK;
+}
+
+int b200fem_get_scatter_map(b200fem_handle h, int* map) {
+  ENG(h);
+  NEED_BUILT();
+  std::copy(eng.h_scatter.begin(), eng.h_scatter.end(), map);
+  return B200FEM_OK;
+}
+
+int b200fem_get_masses(b200fem_handle h, double* mass) {
+  ENG(h);
+  NEED_BUILT();
+  std::copy(eng.h_mass.begin(), eng.h_mass.end(), mass);
+  return B200FEM_OK;
+}
+
+int b200fem_get_incomp_method(b200fem_handle h, int* method) {
+  ENG(h);
+  NEED_BUILT();
+  *method = eng.hosts[0].incomp;
+  return B200FEM_OK;
+}
+
+int b200fem_set_state(b200fem_handle h, const double* x, const double* v) {
+  ENG(h);
+  NEED_BUILT();
+  size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
+  if (x) CK(cudaMemcpyAsync(eng.d.x, x, n, cudaMemcpyHostToDevice, eng.stream));
+  if (v) CK(cudaMemcpyAsync(eng.d.v, v, n, cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  return B200FEM_OK;
+}
+
+int b200fem_get_state(b200fem_handle h, double* x, double* v) {
+  ENG(h);
+  NEED_BUILT();
+  size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
+  if (x) CK(cudaMemcpyAsync(x, eng.d.x, n, cudaMemcpyDeviceToHost, eng.stream));
+  if (v) CK(cudaMemcpyAsync(v, eng.d.v, n, cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  return B200FEM_OK;
+}
+
+int b200fem_set_external_forces(b200fem_handle h, const double* fext) {
+  ENG(h);
+  NEED_BUILT();
+  size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
+  if (fext) CK(cudaMemcpyAsync(eng.d.fext, fext, n, cudaMemcpyHostToDevice, eng.stream));
+  else CK(cudaMemsetAsync(eng.d.fext, 0, n, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  return B200FEM_OK;
+}
+
+int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f_int, double* k_blocks,
+                                    double* crs_vals) {
+  ENG(h);
+  NEED_BUILT();
+  DevPack& d = eng.d;
+  if (x) CK(cudaMemcpyAsync(d.x, x, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  CK(cudaEventRecord(eng.ev[0], eng.stream));
+  CK(launch_assemble(eng, 1.0, 0.0, true));
+  CK(launch_forces_only(eng));
+  CK(cudaEventRecord(eng.ev[1], eng.stream));
+  if (f_int)
+    CK(cudaMemcpyAsync(f_int, d.fint, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyDeviceToHost, eng.stream));
+  if (k_blocks)
+    CK(cudaMemcpyAsync(k_blocks, d.K, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
+  if (crs_vals) {
+    CK(launch_crs_export(eng, d.K, d.S));
+    CK(cudaMemcpyAsync(crs_vals, d.S, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
+    eng.have_matrix = false;  // S was used as scratch
+  }
+  int flags[4];
+  long long dmin;
+  CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaMemcpyAsync(&dmin, d.dmin, sizeof(dmin), cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]);
+  eng.last_asm_ms = ms;
+  eng.last_solve_ms = 0;
+  eng.last_stats.num_inverted = flags[1];
+  long long bits = dmin >= 0 ? dmin : (dmin ^ 0x7fffffffffffffffll);
+  double md;
+  std::memcpy(&md, &bits, sizeof(md));
+  eng.last_stats.min_detJ = md;
+  return B200FEM_OK;
+}
+
+static int read_step_status(Engine& eng, b200fem_stats* stats, int max_iter) {
+  DevPack& d = eng.d;
+  std::vector<double> ms((size_t)d.n_models * 4);
+  int flags[4];
+  long long dmin;
+  CK(cudaMemcpyAsync(ms.data(), d.model_scal, ms.size() * sizeof(double), cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaMemcpyAsync(&dmin, d.dmin, sizeof(dmin), cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  b200fem_stats st{};
+  bool all_conv = true;
+  for (int m = 0; m < d.n_models; m++) {
+    st.iterations = std::max(st.iterations, (int)ms[(size_t)m * 4]);
+    st.rel_residual = std::max(st.rel_residual, ms[(size_t)m * 4 + 1]);
+    all_conv &= ms[(size_t)m * 4 + 2] != 0.0;
+  }
+  st.num_inverted = flags[1];
+  long long bits = dmin >= 0 ? dmin : (dmin ^ 0x7fffffffffffffffll);
+  std::memcpy(&st.min_detJ, &bits, sizeof(double));
+  eng.last_stats = st;
+  if (stats) *stats = st;
+  if (flags[0] == B200FEM_ERR_TIMEOUT) return fail(&eng, B200FEM_ERR_TIMEOUT, "PCG grid barrier timed out");
+  if (flags[0] != 0) return fail(&eng, flags[0], "singular diagonal block in the solve matrix");
+  if (flags[2] != 0 || !all_conv)
+    return fail(&eng, B200FEM_ERR_NO_CONVERGE,
+                "PCG did not reach the tolerance within " + std::to_string(max_iter) + " iterations");
+  return B200FEM_OK;
+}
+
+int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps, b200fem_stats* stats) {
+  ENG(h);
+  NEED_BUILT();
+  if (!p || nsteps < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid step parameters");
+  if (!(p->h > 0) || !(p->tol > 0) || p->max_iter <= 0)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "step size, tolerance and max_iter must be positive");
+  DevPack& d = eng.d;
+  int max_iter = std::min(p->max_iter, d.unconv_cap);
+  std::vector<double> step((size_t)d.n_models * 8);
+  for (int m = 0; m < d.n_models; m++) {
+    double* s = &step[(size_t)m * 8];
+    s[0] = p->h;
+    s[1] = p->alpha_m;
+    s[2] = p->beta_k;
+    s[3] = p->gravity[0];
+    s[4] = p->gravity[1];
+    s[5] = p->gravity[2];
+    s[6] = p->tol;
+    s[7] = 0;
+  }
+  CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  CK(cudaEventRecord(eng.ev[0], eng.stream));
+  for (int s = 0; s < nsteps; s++) {
+    CK(launch_assemble(eng, 0, 0, false));
+    CK(launch_rhs(eng));
+    if (p->abort_on_inverted) {
+      int flags[4];
+      CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
+      CK(cudaStreamSynchronize(eng.stream));
+      if (flags[1] > 0)
+        return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
+    }
+    CK(launch_pcg(eng, max_iter, true, 0));
+  }
+  CK(cudaEventRecord(eng.ev[1], eng.stream));
+  eng.have_matrix = true;
+  int st = read_step_status(eng, stats, max_iter);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]);
+  eng.last_solve_ms = ms;
+  return st;
+}
+
+int b200fem_spmv(b200fem_handle h, const double* x, double* y) {
+  ENG(h);
+  NEED_BUILT();
+  if (!eng.have_matrix) return fail(&eng, B200FEM_ERR_STATE, "no solve matrix assembled yet");
+  DevPack& d = eng.d;
+  size_t n = 3 * sizeof(double) * (size_t)d.n_rows;
+  CK(cudaMemcpyAsync(d.w, x, n, cudaMemcpyHostToDevice, eng.stream));
+  CK(launch_spmv(eng, d.w, d.q));
+  CK(cudaMemcpyAsync(y, d.q, n, cudaMemcpyDeviceToHost, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  return B200FEM_OK;
+}
+
+int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, int max_iter, b200fem_stats* stats) {
+  ENG(h);
+  NEED_BUILT();
+  if (!eng.have_matrix) return fail(&eng, B200FEM_ERR_STATE, "no solve matrix assembled yet");
+  if (!(tol > 0) || max_iter <= 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid tolerance");
+  DevPack& d = eng.d;
+  max_iter = std::min(max_iter, d.unconv_cap);
+  size_t n = 3 * sizeof(double) * (size_t)d.n_rows;
+  std::vector<double> step((size_t)d.n_models * 8);
+  CK(cudaMemcpy(step.data(), d.step, step.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int m = 0; m < d.n_models; m++) step[(size_t)m * 8 + 6] = tol;
+  CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemcpyAsync(d.b, b, n, cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemcpyAsync(d.sol, x, n, cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  CK(launch_pcg(eng, max_iter, false, 0));
+  CK(cudaMemcpyAsync(x, d.sol, n, cudaMemcpyDeviceToHost, eng.stream));
+  return read_step_status(eng, stats, max_iter);
+}
+
+int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms) {
+  ENG(h);
+  if (assemble_ms) *assemble_ms = eng.last_asm_ms;
+  if (solve_ms) *solve_ms = eng.last_solve_ms;
+  return B200FEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,188 @@
+// engine.h -- internal data structures of the B200 FEM engine.
+//
+// One engine ("Pack") holds one or more independent FEM models packed into
+// flat arrays: node, element, block-row and block indices are global across
+// the pack, and per-model tables give each model's ranges and parameters.  A
+// single-model handle is a pack of one; the batched and served forms use the
+// same arrays with many models, so every kernel below is written once.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/b200fem.h"
+
+namespace b200fem {
+
+constexpr int kMaxNen = 8;
+constexpr int kMaxIp = 8;
+constexpr int kMatParams = 8;
+
+// Model as given by the caller (host, FP64).
+struct ModelDesc {
+  int elem_type = B200FEM_ELEM_TET;
+  int n_nodes = 0, n_elems = 0;
+  std::vector<double> rest;  // 3N
+  std::vector<int> conn;     // nen*E
+  std::vector<int> fixed;    // N
+  int mat_kind = B200FEM_MAT_LINEAR;
+  double mat_params[kMatParams] = {0};
+  double density = 1000;
+  int incomp_request = B200FEM_INCOMP_AUTO;
+  bool has_material = false;
+};
+
+// Host-side derived data of one model (setup only).
+struct ModelHost {
+  int nen = 4, nip = 1, npair = 10;
+  int incomp = B200FEM_INCOMP_OFF;  // resolved method
+  int n_active = 0;
+  std::vector<int> sidx;      // per node, -1 when fixed
+  std::vector<int> act_node;  // per active row -> node
+  std::vector<double> invJ0;  // E*nip*9
+  std::vector<double> detJ0;  // E*nip
+  std::vector<double> winvJ0; // E*9 (warping point)
+  std::vector<double> rest_vol;
+  std::vector<double> mass;   // N
+  std::vector<double> K0, f0; // linear materials: E*nen*nen*9, E*nen*3
+  std::vector<double> node_rest_vol;  // NODAL
+  // block pattern over active nodes
+  std::vector<int> rowptr, col;
+  // direct node neighbours (sorted) for NODAL
+  std::vector<std::vector<int>> nbr;
+};
+
+// Device arrays for the whole pack.  Precision-dependent value arrays are
+// allocated in both FP64 and (for the mixed form) FP32.
+struct DevPack {
+  int n_models = 0;
+  int n_nodes = 0, n_elems = 0, n_rows = 0;
+  long long nnzb = 0;
+  // node data (FP64)
+  double* x = nullptr;       // 3N positions
+  double* v = nullptr;       // 3N velocities
+  double* fext = nullptr;    // 3N external forces
+  double* mass = nullptr;    // N
+  int* node_model = nullptr; // N
+  int* sidx = nullptr;       // N global row or -1
+  int* act_node = nullptr;   // rows -> node
+  int* row_model = nullptr;  // rows -> model
+  // elements
+  int* conn = nullptr;       // nen*E global node indices
+  int* elem_model = nullptr; // E
+  double* invJ0 = nullptr;   // E*nip*9
+  double* winvJ0 = nullptr;  // E*9
+  double* K0 = nullptr;      // linear: E*nen*nen*9
+  double* f0 = nullptr;      // linear: E*nen*3
+  float* invJ0_f = nullptr;  // mixed form copy
+  // assembly maps
+  int* blk_rowptr = nullptr; // n_rows+1 (global block index)
+  int* blk_col = nullptr;    // nnzb (global row index)
+  int* blk_diag = nullptr;   // n_rows
+  int* blk_row = nullptr;    // nnzb -> row
+  int* contrib_ptr = nullptr;  // nnzb+1
+  int* contrib_idx = nullptr;  // (elem*npair + pair) << 1 | transpose
+  int* inc_ptr = nullptr;      // N+1 node -> element incidences
+  int* inc_idx = nullptr;      // elem*nen + local
+  // element outputs
+  double* elemK = nullptr;     // E*npair*9
+  double* elemF = nullptr;     // E*nen*3
+  float* elemK_f = nullptr;
+  // assembled values
+  double* K = nullptr;         // nnzb*9 stiffness (drop-in output)
+  double* S = nullptr;         // nnzb*9 solve matrix
+  float* S_f = nullptr;        // FP32 copy (mixed form)
+  double* Dinv = nullptr;      // n_rows*9 block-Jacobi inverse
+  double* fint = nullptr;      // 3N internal force
+  // solve vectors (3*n_rows)
+  double* b = nullptr;
+  double* sol = nullptr;
+  double* r = nullptr;
+  double* z = nullptr;
+  double* p = nullptr;
+  double* q = nullptr;
+  double* w = nullptr;
+  // per model tables
+  double* mat = nullptr;       // n_models*kMatParams
+  double* step = nullptr;      // n_models*8: h, alpha, beta, gx, gy, gz, tol, -
+  // NODAL incompressibility
+  double* node_rest_vol = nullptr;
+  double* node_vol = nullptr;
+  double* node_p = nullptr;
+  // reductions / PCG control
+  double* partials = nullptr;  // n_pieces*4
+  int* piece_row = nullptr;    // n_pieces+1
+  int* piece_model = nullptr;  // n_pieces
+  int* model_piece = nullptr;  // n_models+1
+  int* cta_piece = nullptr;    // pcg_grid+1
+  int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
+  int unconv_cap = 0;
+  int n_pieces = 0;
+  double* model_scal = nullptr;  // n_models*8: rho, rr, bb, pq, conv, iters...
+  unsigned* barrier = nullptr;   // [count, generation]
+  int* flags = nullptr;          // [error, inverted count, ...]
+  double* dmin = nullptr;        // min detJ (atomically reduced as ordered bits)
+};
+
+// One element group: contiguous element range with one element type and
+// material kind (kernels are specialised on both).
+struct ElemGroup {
+  int e0 = 0, e1 = 0;
+  int elem_type = B200FEM_ELEM_TET;
+  int mat_kind = B200FEM_MAT_LINEAR;
+  int corotated = 1;
+  int nodal = 0;
+};
+
+struct Engine {
+  int device = 0;
+  int precision = B200FEM_PREC_FP64;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::string last_error;
+  std::vector<ModelDesc> models;
+  std::vector<ModelHost> hosts;
+  std::vector<ElemGroup> groups;
+  std::vector<int> node_off, elem_off, row_off;
+  std::vector<long long> blk_off;
+  DevPack d;
+  bool built = false;
+  bool have_matrix = false;
+  int elem_type = B200FEM_ELEM_TET;  // pack-wide element type
+  int nen = 4, nip = 1, npair = 10;
+  // host copies for queries
+  std::vector<int> h_rowptr, h_col;
+  std::vector<int> h_scatter;  // E*nen*nen
+  std::vector<int> h_sidx;
+  std::vector<double> h_mass;
+  // pcg launch geometry
+  int pcg_grid = 0, pcg_block = 256;
+  // last timing
+  float last_asm_ms = 0, last_solve_ms = 0;
+  b200fem_stats last_stats{};
+  std::vector<void*> allocations;
+};
+
+// setup.cpp
+int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err);
+int build_pack(Engine& eng);
+void free_pack(Engine& eng);
+int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne);
+void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
+                 int* conn);
+void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
+                 unsigned long long seed, double* xyz);
+
+// kernels.cu
+cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K);
+cudaError_t launch_rhs(Engine& eng);
+cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero);
+cudaError_t launch_spmv(Engine& eng, const double* x, double* y);
+cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs);
+int read_pcg_result(Engine& eng, b200fem_stats* st);
+
+}  // namespace b200fem

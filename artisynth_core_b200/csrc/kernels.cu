@@ -1,0 +1,1052 @@
+// kernels.cu -- sm_100a kernels of the FEM hot path:
+//
+//   elem_*_kernel     element-group kernels: node coordinates staged through
+//                     shared memory, per-integration-point kinematics and
+//                     material (F, sigma, D), then one thread per element node
+//                     pair forms the 3x3 tangent block and one per node the
+//                     stress force (FemModel3d.computeStressAndStiffness,
+//                     FemModel3d.java:3333-3666)
+//   gather_kernel     deterministic, atomic-free scatter: every 3x3 block
+//                     entry sums its precomputed contribution list (element
+//                     pair, transposed flag) in element order and applies the
+//                     BackwardEuler coefficients S = (h^2+h beta)K + (1+h alpha)M
+//   rows_kernel       nodal internal force gather and BackwardEuler RHS
+//   pcg_kernel        persistent cooperative block-Jacobi PCG with
+//                     deterministic two-level dot products and a bounded grid
+//                     barrier; writes v1 and x1 = x0 + h v1 at the end
+//
+// All reductions are in a fixed order: results are bit-reproducible run to run.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "device_math.cuh"
+#include "engine.h"
+
+namespace b200fem {
+
+// ---------------------------------------------------------------------------
+// constant shape tables
+// ---------------------------------------------------------------------------
+__constant__ double c_tet_gns[12];
+__constant__ double c_hex_gns[8 * 8 * 3];  // [ip][node][3]
+__constant__ double c_hex_wgns[8 * 3];     // warping point (centre)
+__constant__ float c_tet_gns_f[12];
+__constant__ float c_hex_gns_f[8 * 8 * 3];
+__constant__ int c_pair_a[36], c_pair_b[36];
+
+static bool g_const_ready[64] = {false};
+
+static cudaError_t ensure_constants(int device) {
+  if (device >= 0 && device < 64 && g_const_ready[device]) return cudaSuccess;
+  double tet[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+  static const double node[8][3] = {{-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1},
+                                    {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}};
+  double hex[8 * 8 * 3], hexw[24];
+  const double q = 1.0 / sqrt(3.0);
+  auto grad = [&](double* g, int i, double s0, double s1, double s2) {
+    double a = node[i][0], b = node[i][1], c = node[i][2];
+    g[0] = 0.125 * a * (1 + b * s1) * (1 + c * s2);
+    g[1] = 0.125 * (1 + a * s0) * b * (1 + c * s2);
+    g[2] = 0.125 * (1 + a * s0) * (1 + b * s1) * c;
+  };
+  for (int k = 0; k < 8; k++)
+    for (int i = 0; i < 8; i++) grad(&hex[(k * 8 + i) * 3], i, node[k][0] * q, node[k][1] * q, node[k][2] * q);
+  for (int i = 0; i < 8; i++) grad(&hexw[i * 3], i, 0, 0, 0);
+  float tetf[12], hexf[192];
+  for (int i = 0; i < 12; i++) tetf[i] = (float)tet[i];
+  for (int i = 0; i < 192; i++) hexf[i] = (float)hex[i];
+  int pa[36], pb[36], w = 0;
+  for (int a = 0; a < 8; a++)
+    for (int b = a; b < 8; b++) { pa[w] = a; pb[w] = b; w++; }
+  int pa4[10], pb4[10];
+  w = 0;
+  for (int a = 0; a < 4; a++)
+    for (int b = a; b < 4; b++) { pa4[w] = a; pb4[w] = b; w++; }
+  (void)pa4; (void)pb4;
+  cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_tet_gns, tet, sizeof(tet))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_hex_gns, hex, sizeof(hex))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_hex_wgns, hexw, sizeof(hexw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_tet_gns_f, tetf, sizeof(tetf))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_hex_gns_f, hexf, sizeof(hexf))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_pair_a, pa, sizeof(pa))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_pair_b, pb, sizeof(pb))) != cudaSuccess) return e;
+  if (device >= 0 && device < 64) g_const_ready[device] = true;
+  return cudaSuccess;
+}
+
+// pair index w of (a, b), a <= b, enumerated row-major over the upper
+// triangle of the nen x nen element matrix
+template <int NEN>
+__device__ __forceinline__ void pair_of(int w, int& a, int& b) {
+  if (NEN == 8) {
+    a = c_pair_a[w];
+    b = c_pair_b[w];
+  } else {
+    // 4-node table: (0,0)(0,1)(0,2)(0,3)(1,1)(1,2)(1,3)(2,2)(2,3)(3,3)
+    const int ta[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+    const int tb[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+    a = ta[w];
+    b = tb[w];
+  }
+}
+
+template <typename T, int TYPE>
+__device__ __forceinline__ T gns(int k, int n, int c) {
+  if (TYPE == B200FEM_ELEM_TET) {
+    if constexpr (sizeof(T) == 8) return c_tet_gns[3 * n + c];
+    else return c_tet_gns_f[3 * n + c];
+  } else {
+    if constexpr (sizeof(T) == 8) return c_hex_gns[(k * 8 + n) * 3 + c];
+    else return c_hex_gns_f[(k * 8 + n) * 3 + c];
+  }
+}
+
+// ordered-bits min for doubles (atomicMin on the int64 image of a double
+// works for non-negative and negative values with this mapping)
+__device__ __forceinline__ long long dbl_order(double v) {
+  long long i = __double_as_longlong(v);
+  return i >= 0 ? i : (i ^ 0x7fffffffffffffffll);
+}
+
+struct ElemArgs {
+  int e0, e1;
+  const int* conn;
+  const int* elem_model;
+  const double* x;
+  const double* invJ0;
+  const float* invJ0_f;
+  const double* winvJ0;
+  const double* K0;
+  const double* f0;
+  const int* sidx;
+  const double* mat;       // per model kMatParams
+  const double* node_p;    // NODAL pressures (or null)
+  void* elemK;             // T* E*npair*9
+  void* elemF;             // T* E*nen*3
+  int* flags;              // [err, inverted]
+  long long* mindet;       // ordered bits
+};
+
+// ---------------------------------------------------------------------------
+// non-linear materials (NeoHookean, MooneyRivlin), tet or hex
+// ---------------------------------------------------------------------------
+template <int TYPE, int MAT, bool NODAL, typename T>
+__global__ void __launch_bounds__(256) elem_nonlinear_kernel(ElemArgs a) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 4;
+  constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
+  __shared__ T sx[EPB][NEN][3];
+  __shared__ T sg[EPB * NIP][NEN][3];
+  __shared__ T sdv[EPB * NIP];
+  __shared__ T ssig[EPB * NIP][6];
+  __shared__ T sD[EPB * NIP][DS];
+  __shared__ int snode[EPB][NEN];
+  const int ebase = a.e0 + blockIdx.x * EPB;
+  // stage 0: coalesced connectivity + coordinate loads.  In FP32 the
+  // coordinates are taken relative to the element's first node in FP64 so
+  // the Jacobian keeps full single precision.
+  for (int t = threadIdx.x; t < EPB * NEN; t += blockDim.x) {
+    int el = t / NEN, n = t % NEN, e = ebase + el;
+    if (e < a.e1) snode[el][n] = a.conn[(size_t)e * NEN + n];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < EPB * NEN * 3; t += blockDim.x) {
+    int el = t / (NEN * 3), r = t % (NEN * 3), n = r / 3, c = r % 3, e = ebase + el;
+    if (e < a.e1) {
+      double v = a.x[3 * (size_t)snode[el][n] + c];
+      if constexpr (sizeof(T) == 4) v -= a.x[3 * (size_t)snode[el][0] + c];
+      sx[el][n][c] = (T)v;
+    }
+  }
+  __syncthreads();
+  // stage 1: one thread per (element, integration point)
+  for (int t = threadIdx.x; t < EPB * NIP; t += blockDim.x) {
+    int el = t / NIP, k = t % NIP, e = ebase + el;
+    if (e >= a.e1) continue;
+    T J[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) J[i] = T(0);
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      T g0 = gns<T, TYPE>(k, n, 0), g1 = gns<T, TYPE>(k, n, 1), g2 = gns<T, TYPE>(k, n, 2);
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        T p = sx[el][n][r];
+        J[3 * r] += p * g0;
+        J[3 * r + 1] += p * g1;
+        J[3 * r + 2] += p * g2;
+      }
+    }
+    T iJ0[9];
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0[((size_t)e * NIP + k) * 9 + i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0_f[((size_t)e * NIP + k) * 9 + i];
+    }
+    T F[9], invJ[9];
+    matmul3(F, J, iJ0);
+    T detF = det3(F);
+    T detJ = invert3(invJ, J);
+    if (!(detJ > T(0))) {
+      atomicAdd(&a.flags[1], 1);
+    }
+    atomicMin(a.mindet, dbl_order((double)detJ));
+    const T w = TYPE == B200FEM_ELEM_TET ? T(1.0 / 6.0) : T(1);
+    T dv = detJ * w;
+    sdv[t] = dv;
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      T g0 = gns<T, TYPE>(k, n, 0), g1 = gns<T, TYPE>(k, n, 1), g2 = gns<T, TYPE>(k, n, 2);
+#pragma unroll
+      for (int c = 0; c < 3; c++) sg[t][n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
+    }
+    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
+      T aa, bb;
+      neohookean_point<T>(ssig[t], &aa, &bb, (T)mp[0], (T)mp[1], F, detF);
+      sD[t][0] = aa;
+      sD[t][1] = bb;
+    } else {
+      T pr = T(0);
+      if constexpr (NODAL) {
+        if (TYPE == B200FEM_ELEM_TET) {
+          double s = 0;
+#pragma unroll
+          for (int n = 0; n < NEN; n++) s += a.node_p[snode[el][n]];
+          pr = (T)(s / NEN);
+        } else {
+          pr = (T)a.node_p[snode[el][k]];
+        }
+      }
+      T mpt[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) mpt[i] = (T)mp[i];
+      mooneyrivlin_point<T>(ssig[t], sD[t], mpt, F, detF, pr);
+    }
+  }
+  __syncthreads();
+  // stage 2: one thread per element pair block, then per node force
+  T* elemK = (T*)a.elemK;
+  T* elemF = (T*)a.elemF;
+  for (int t = threadIdx.x; t < EPB * (NPAIR + NEN); t += blockDim.x) {
+    int el = t / (NPAIR + NEN), w = t % (NPAIR + NEN), e = ebase + el;
+    if (e >= a.e1) continue;
+    if (w < NPAIR) {
+      int ia, ib;
+      pair_of<NEN>(w, ia, ib);
+      T K[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) K[i] = T(0);
+#pragma unroll
+      for (int k = 0; k < NIP; k++) {
+        int s = el * NIP + k;
+        if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN)
+          add_bdb_iso(K, sg[s][ia], sD[s][0], sD[s][1], sg[s][ib], sdv[s]);
+        else
+          add_bdb(K, sg[s][ia], sD[s], sg[s][ib], sdv[s]);
+        add_geometric(K, sg[s][ia], ssig[s], sg[s][ib], sdv[s]);
+      }
+      T* out = elemK + ((size_t)e * NPAIR + w) * 9;
+#pragma unroll
+      for (int i = 0; i < 9; i++) out[i] = K[i];
+    } else {
+      int n = w - NPAIR;
+      T f[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int k = 0; k < NIP; k++) {
+        int s = el * NIP + k;
+        add_stress_force(f, sg[s][n], ssig[s], sdv[s]);
+      }
+      T* out = elemF + ((size_t)e * NEN + n) * 3;
+      out[0] = f[0];
+      out[1] = f[1];
+      out[2] = f[2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// linear materials (corotated or not): cached rest stiffness K0, force
+// R (K0 R^T x - f0) and stiffness R K0 R^T (StiffnessWarper3d.java:154-307)
+// ---------------------------------------------------------------------------
+template <int TYPE, typename T>
+__global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corotated) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 8;
+  __shared__ double sx[EPB][NEN][3];
+  __shared__ double sR[EPB][9];
+  __shared__ int snode[EPB][NEN];
+  const int ebase = a.e0 + blockIdx.x * EPB;
+  for (int t = threadIdx.x; t < EPB * NEN; t += blockDim.x) {
+    int el = t / NEN, n = t % NEN, e = ebase + el;
+    if (e < a.e1) snode[el][n] = a.conn[(size_t)e * NEN + n];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < EPB * NEN * 3; t += blockDim.x) {
+    int el = t / (NEN * 3), r = t % (NEN * 3), n = r / 3, c = r % 3, e = ebase + el;
+    if (e < a.e1) sx[el][n][c] = a.x[3 * (size_t)snode[el][n] + c];
+  }
+  __syncthreads();
+  for (int el = threadIdx.x; el < EPB; el += blockDim.x) {
+    int e = ebase + el;
+    if (e >= a.e1) continue;
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (corotated) {
+      // F at the warping point (TetElement: integration point 0; HexElement:
+      // centre) -- StiffnessWarper3d.computeWarpingRotation (:154-159)
+      double J[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) J[i] = 0;
+#pragma unroll
+      for (int n = 0; n < NEN; n++) {
+        double g0, g1, g2;
+        if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * n]; g1 = c_tet_gns[3 * n + 1]; g2 = c_tet_gns[3 * n + 2]; }
+        else { g0 = c_hex_wgns[3 * n]; g1 = c_hex_wgns[3 * n + 1]; g2 = c_hex_wgns[3 * n + 2]; }
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          J[3 * r] += sx[el][n][r] * g0;
+          J[3 * r + 1] += sx[el][n][r] * g1;
+          J[3 * r + 2] += sx[el][n][r] * g2;
+        }
+      }
+      double W[9], F[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) W[i] = a.winvJ0[(size_t)e * 9 + i];
+      matmul3(F, J, W);
+      polar_rotation(F, R);
+    }
+#pragma unroll
+    for (int i = 0; i < 9; i++) sR[el][i] = R[i];
+  }
+  __syncthreads();
+  T* elemK = (T*)a.elemK;
+  T* elemF = (T*)a.elemF;
+  for (int t = threadIdx.x; t < EPB * (NPAIR + NEN); t += blockDim.x) {
+    int el = t / (NPAIR + NEN), w = t % (NPAIR + NEN), e = ebase + el;
+    if (e >= a.e1) continue;
+    const double* R = sR[el];
+    const double* K0 = a.K0 + (size_t)e * NEN * NEN * 9;
+    if (w < NPAIR) {
+      int ia, ib;
+      pair_of<NEN>(w, ia, ib);
+      const double* Kab = K0 + (ia * NEN + ib) * 9;
+      double out9[9];
+      if (corotated) {
+        // R K R^T (StiffnessWarper3d.rotateStiffness, :219-222)
+        double Tm[9];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++)
+            Tm[3 * i + j] = Kab[3 * i] * R[3 * j] + Kab[3 * i + 1] * R[3 * j + 1] + Kab[3 * i + 2] * R[3 * j + 2];
+        matmul3(out9, R, Tm);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; i++) out9[i] = Kab[i];
+      }
+      T* out = elemK + ((size_t)e * NPAIR + w) * 9;
+#pragma unroll
+      for (int i = 0; i < 9; i++) out[i] = (T)out9[i];
+    } else {
+      int n = w - NPAIR;
+      double acc[3] = {0, 0, 0};
+      if (a.sidx[snode[el][n]] >= 0) {
+        for (int j = 0; j < NEN; j++) {
+          double pos[3];
+          if (corotated) {
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+              pos[r] = R[r] * sx[el][j][0] + R[3 + r] * sx[el][j][1] + R[6 + r] * sx[el][j][2];
+          } else {
+            pos[0] = sx[el][j][0]; pos[1] = sx[el][j][1]; pos[2] = sx[el][j][2];
+          }
+          const double* Kij = K0 + (n * NEN + j) * 9;
+#pragma unroll
+          for (int r = 0; r < 3; r++) acc[r] += Kij[3 * r] * pos[0] + Kij[3 * r + 1] * pos[1] + Kij[3 * r + 2] * pos[2];
+        }
+        const double* f0 = a.f0 + ((size_t)e * NEN + n) * 3;
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc[r] -= f0[r];
+        if (corotated) {
+          double t2[3];
+#pragma unroll
+          for (int r = 0; r < 3; r++) t2[r] = R[3 * r] * acc[0] + R[3 * r + 1] * acc[1] + R[3 * r + 2] * acc[2];
+          acc[0] = t2[0]; acc[1] = t2[1]; acc[2] = t2[2];
+        }
+      }
+      T* out = elemF + ((size_t)e * NEN + n) * 3;
+      out[0] = (T)acc[0];
+      out[1] = (T)acc[1];
+      out[2] = (T)acc[2];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block gather: one thread per block entry
+// ---------------------------------------------------------------------------
+template <typename TK, typename TO>
+__global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, const int* __restrict__ cidx,
+                              const TK* __restrict__ elemK, const int* __restrict__ blk_row,
+                              const int* __restrict__ blk_diag, const int* __restrict__ row_model,
+                              const int* __restrict__ act_node, const double* __restrict__ mass,
+                              const double* __restrict__ step, int mode, TO* __restrict__ out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nnzb * 9) return;
+  long long p = t / 9;
+  int q = (int)(t - p * 9);
+  int qt = (q % 3) * 3 + q / 3;
+  TK s = TK(0);
+  int c1 = cptr[p + 1];
+  for (int c = cptr[p]; c < c1; c++) {
+    int code = cidx[c];
+    s += elemK[(size_t)(code >> 1) * 9 + ((code & 1) ? qt : q)];
+  }
+  double val;
+  if (mode == 0) {
+    val = (double)s;  // plain stiffness K
+  } else {
+    int row = blk_row[p];
+    const double* sp = step + (size_t)row_model[row] * 8;
+    double h = sp[0], al = sp[1], be = sp[2];
+    // addPosJacobian (h^2 K), addVelJacobian (h beta K + h alpha M),
+    // addActiveMassMatrix (M)  (MechSystemSolver.java:2277,2312,2334)
+    val = (h * h + h * be) * (double)s;
+    if (p == blk_diag[row] && (q == 0 || q == 4 || q == 8)) val += (1.0 + h * al) * mass[act_node[row]];
+  }
+  out[t] = (TO)val;
+}
+
+// ---------------------------------------------------------------------------
+// nodal forces and BackwardEuler right-hand side
+//   f_int(n) = sum of element stress forces at n
+//   b = M v0 + h (m g + f_ext - f_int)
+// (the mass- and stiffness-damping terms of updateNodeForces and the
+// b += (h alpha M + h beta K) v0 term of backwardEuler cancel exactly,
+// MechSystemSolver.java:2194-2301, FemModel3d.java:2783-2843)
+// ---------------------------------------------------------------------------
+template <typename TF>
+__global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                            const TF* __restrict__ elemF, const int* __restrict__ sidx,
+                            const int* __restrict__ node_model, const double* __restrict__ mass,
+                            const double* __restrict__ v, const double* __restrict__ fext,
+                            const double* __restrict__ step, double* __restrict__ fint,
+                            double* __restrict__ b, double* __restrict__ sol0) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double f[3] = {0, 0, 0};
+  int i1 = inc_ptr[n + 1];
+  for (int i = inc_ptr[n]; i < i1; i++) {
+    const TF* src = elemF + (size_t)inc_idx[i] * 3;
+    f[0] += (double)src[0];
+    f[1] += (double)src[1];
+    f[2] += (double)src[2];
+  }
+  if (fint) {
+    fint[3 * (size_t)n] = f[0];
+    fint[3 * (size_t)n + 1] = f[1];
+    fint[3 * (size_t)n + 2] = f[2];
+  }
+  int r = sidx[n];
+  if (b && r >= 0) {
+    const double* sp = step + (size_t)node_model[n] * 8;
+    double h = sp[0], m = mass[n];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      b[3 * (size_t)r + c] = m * v[3 * (size_t)n + c] + h * (m * sp[3 + c] + fext[3 * (size_t)n + c] - f[c]);
+    // the PCG starts from the current velocity
+    if (sol0)
+#pragma unroll
+      for (int c = 0; c < 3; c++) sol0[3 * (size_t)r + c] = v[3 * (size_t)n + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block SpMV helpers
+// ---------------------------------------------------------------------------
+template <typename MT>
+__device__ __forceinline__ void warp_row_spmv(int row, const int* __restrict__ rowptr,
+                                              const int* __restrict__ col, const MT* __restrict__ S,
+                                              const double* __restrict__ x, int lane, double* y) {
+  int p0 = rowptr[row], p1 = rowptr[row + 1];
+  int nval = (p1 - p0) * 9;
+  const MT* base = S + (size_t)p0 * 9;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int i = lane; i < nval; i += 32) {
+    int bk = i / 9, q = i - bk * 9, r = q / 3, c = q - r * 3;
+    double v = (double)base[i] * x[3 * (size_t)col[p0 + bk] + c];
+    if (r == 0) a0 += v;
+    else if (r == 1) a1 += v;
+    else a2 += v;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+  }
+  y[0] = a0;
+  y[1] = a1;
+  y[2] = a2;
+}
+
+template <typename MT>
+__global__ void spmv_kernel(int n_rows, const int* rowptr, const int* col, const MT* S, const double* x,
+                            double* y) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n_rows) return;
+  double out[3];
+  warp_row_spmv<MT>(warp, rowptr, col, S, x, lane, out);
+  if (lane == 0) {
+    y[3 * (size_t)warp] = out[0];
+    y[3 * (size_t)warp + 1] = out[1];
+    y[3 * (size_t)warp + 2] = out[2];
+  }
+}
+
+// full-partition scalar CRS export: value of block p entry (r, c) goes to
+// slot rowoff(3*row + r) + 3*k + c, k = position of p in its block row
+__global__ void crs_export_kernel(long long nnzb, const int* blk_row, const int* rowptr,
+                                  const double* vals, double* crs) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nnzb * 9) return;
+  long long p = t / 9;
+  int q = (int)(t - p * 9), r = q / 3, c = q % 3;
+  int row = blk_row[p];
+  long long p0 = rowptr[row];
+  long long nb = rowptr[row + 1] - p0;
+  long long slot = 9 * p0 + r * 3 * nb + 3 * (p - p0) + c;
+  crs[slot] = vals[t];
+}
+
+// ---------------------------------------------------------------------------
+// persistent cooperative PCG
+// ---------------------------------------------------------------------------
+constexpr int kPcgThreads = 512;
+constexpr int kRowChunk = 512;
+constexpr int kMaxCtaPieces = 48;
+constexpr unsigned long long kBarrierTimeoutNs = 5000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier for a cooperative launch (all CTAs co-resident).  The
+// spin is bounded: after kBarrierTimeoutNs the CTA records
+// B200FEM_ERR_TIMEOUT in flags[0] and returns false; every CTA then leaves
+// the kernel at its next barrier.
+__device__ bool grid_barrier(unsigned* bar, int* flags) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    volatile int* err = flags;
+    unsigned g = *gen;
+    __threadfence();
+    unsigned arrived = atomicAdd(bar, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned long long t0 = global_ns();
+      while (*gen == g) {
+        if (*err != 0) { ok = 0; break; }
+        if (global_ns() - t0 > kBarrierTimeoutNs) {
+          atomicExch(flags, B200FEM_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    if (*err != 0) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+struct PcgArgs {
+  int n_rows;
+  const int* rowptr;
+  const int* col;
+  const int* blk_diag;
+  const void* S;
+  double* Dinv;
+  const double* b;
+  double* x;
+  double* r;
+  double* z;
+  double* p;
+  double* q;
+  const int* piece_row;
+  const int* piece_model;
+  const int* model_piece;
+  const int* cta_piece;
+  double* partials;  // n_pieces * 4
+  const double* step;
+  double* model_out;  // n_models * 4: iterations, rel residual, converged
+  unsigned* barrier;
+  int* flags;
+  int* unconv;
+  int max_iter;
+  int update_state;
+  int init_dinv;
+  double* xpos;
+  double* vel;
+  const int* act_node;
+  const int* row_model;
+};
+
+// Reduce per-row values (ND of them, produced by fn(row, lane, vals) in
+// warp-uniform fashion) over this CTA's pieces, in a fixed order, and write
+// partials[piece*4 + k].  fn may also update row data.
+template <int ND, bool WARP_ROWS, typename Fn>
+__device__ void cta_row_pass(const PcgArgs& a, int pc0, int pc1, double (*rowbuf)[3],
+                             double (*pacc)[3], Fn fn) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int npc = pc1 - pc0;
+  for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
+  const int r0 = a.piece_row[pc0], r1 = a.piece_row[pc1];
+  for (int c0 = r0; c0 < r1; c0 += kRowChunk) {
+    const int c1 = min(c0 + kRowChunk, r1);
+    __syncthreads();
+    if (WARP_ROWS) {
+      for (int row = c0 + warp; row < c1; row += nwarps) {
+        double vals[3] = {0, 0, 0};
+        fn(row, lane, vals);
+        if (lane == 0) {
+#pragma unroll
+          for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
+        }
+      }
+    } else {
+      for (int row = c0 + (int)threadIdx.x; row < c1; row += blockDim.x) {
+        double vals[3] = {0, 0, 0};
+        fn(row, 0, vals);
+#pragma unroll
+        for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
+      }
+    }
+    __syncthreads();
+    // piece j's rows inside this chunk, summed by warp (j % nwarps)
+    for (int j = warp; j < npc; j += nwarps) {
+      int pr0 = max(a.piece_row[pc0 + j], c0), pr1 = min(a.piece_row[pc0 + j + 1], c1);
+      if (pr0 >= pr1) continue;
+      double s[3] = {0, 0, 0};
+      for (int row = pr0 + lane; row < pr1; row += 32)
+#pragma unroll
+        for (int k = 0; k < ND; k++) s[k] += rowbuf[row - c0][k];
+#pragma unroll
+      for (int k = 0; k < ND; k++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+      if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < ND; k++) pacc[j][k] += s[k];
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < npc; j += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < ND; k++) a.partials[(size_t)(pc0 + j) * 4 + k] = pacc[j][k];
+}
+
+// Sum slot k of the partials of each local piece's model (warp per piece,
+// fixed lane striding and butterfly order).
+template <int ND>
+__device__ void model_sums(const PcgArgs& a, int pc0, int pc1, double (*out)[3]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int j = warp; j < pc1 - pc0; j += nwarps) {
+    int m = a.piece_model[pc0 + j];
+    int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
+    double s[3] = {0, 0, 0};
+    for (int q = q0 + lane; q < q1; q += 32)
+#pragma unroll
+      for (int k = 0; k < ND; k++) s[k] += __ldcg(&a.partials[(size_t)q * 4 + k]);
+#pragma unroll
+    for (int k = 0; k < ND; k++)
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < ND; k++) out[j][k] = s[k];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int piece_of_row(const PcgArgs& a, int pc0, int pc1, int row) {
+  int j = 0;
+  while (pc0 + j + 1 < pc1 && a.piece_row[pc0 + j + 1] <= row) j++;
+  return j;
+}
+
+template <typename MT>
+__global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
+  __shared__ double rowbuf[kRowChunk][3];
+  __shared__ double pacc[kMaxCtaPieces][3];
+  __shared__ double sums[kMaxCtaPieces][3];
+  __shared__ double s_rho[kMaxCtaPieces], s_bb[kMaxCtaPieces], s_alpha[kMaxCtaPieces],
+      s_beta[kMaxCtaPieces], s_tol[kMaxCtaPieces];
+  __shared__ int s_conv[kMaxCtaPieces], s_iters[kMaxCtaPieces];
+  const MT* S = (const MT*)a.S;
+  const int pc0 = a.cta_piece[blockIdx.x], pc1 = a.cta_piece[blockIdx.x + 1];
+  const int npc = pc1 - pc0;
+
+  // ---- init: r = b - S x, Dinv, z = Dinv r; dots r.z, r.r, b.b
+  cta_row_pass<3, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+    double Ax[3];
+    warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
+    if (lane == 0) {
+      double* Di = a.Dinv + (size_t)row * 9;
+      if (a.init_dinv) {
+        const MT* Db = S + (size_t)a.blk_diag[row] * 9;
+        double d[9], inv[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) d[i] = (double)Db[i];
+        double det = invert3(inv, d);
+        if (det == 0.0) {
+          atomicExch(a.flags, B200FEM_ERR_INVALID_ARG);
+#pragma unroll
+          for (int i = 0; i < 9; i++) inv[i] = 0;
+        }
+#pragma unroll
+        for (int i = 0; i < 9; i++) Di[i] = inv[i];
+      }
+      double r[3], z[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) r[c] = a.b[3 * (size_t)row + c] - Ax[c];
+#pragma unroll
+      for (int c = 0; c < 3; c++) z[c] = Di[3 * c] * r[0] + Di[3 * c + 1] * r[1] + Di[3 * c + 2] * r[2];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        a.r[3 * (size_t)row + c] = r[c];
+        a.z[3 * (size_t)row + c] = z[c];
+      }
+      double bb = 0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) bb += a.b[3 * (size_t)row + c] * a.b[3 * (size_t)row + c];
+      vals[0] = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
+      vals[1] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      vals[2] = bb;
+    }
+  });
+  if (!grid_barrier(a.barrier, a.flags)) return;
+  model_sums<3>(a, pc0, pc1, sums);
+  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+    int m = a.piece_model[pc0 + j];
+    s_rho[j] = sums[j][0];
+    s_bb[j] = sums[j][2];
+    s_tol[j] = a.step[(size_t)m * 8 + 6];
+    s_conv[j] = (sums[j][1] == 0.0) || (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]));
+    s_iters[j] = 0;
+    s_beta[j] = 0;
+  }
+  __syncthreads();
+
+  int it = 0;
+  for (;;) {
+    // ---- phase A: p = z + beta p; q = S z + beta q; dot p.q
+    for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+      int m = a.piece_model[pc0 + j];
+      if (!s_conv[j] && pc0 + j == a.model_piece[m + 1] - 1) a.unconv[it] = 1;
+    }
+    cta_row_pass<1, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+      int j = piece_of_row(a, pc0, pc1, row);
+      if (s_conv[j]) return;
+      double beta = s_beta[j];
+      double Az[3];
+      warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.z, lane, Az);
+      if (lane == 0) {
+        double pq = 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          size_t i = 3 * (size_t)row + c;
+          double pn = a.z[i] + beta * a.p[i];
+          double qn = Az[c] + beta * a.q[i];
+          a.p[i] = pn;
+          a.q[i] = qn;
+          pq += pn * qn;
+        }
+        vals[0] = pq;
+      }
+    });
+    if (!grid_barrier(a.barrier, a.flags)) return;
+    if (__ldcg(&a.unconv[it]) == 0) break;
+    model_sums<1>(a, pc0, pc1, sums);
+    for (int j = threadIdx.x; j < npc; j += blockDim.x)
+      s_alpha[j] = s_conv[j] ? 0.0 : s_rho[j] / sums[j][0];
+    __syncthreads();
+    // ---- phase B: x += alpha p; r -= alpha q; z = Dinv r; dots r.z, r.r
+    cta_row_pass<2, false>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+      int j = piece_of_row(a, pc0, pc1, row);
+      if (s_conv[j]) return;
+      double al = s_alpha[j];
+      double r[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        size_t i = 3 * (size_t)row + c;
+        a.x[i] += al * a.p[i];
+        r[c] = a.r[i] - al * a.q[i];
+        a.r[i] = r[c];
+      }
+      const double* Di = a.Dinv + (size_t)row * 9;
+      double z[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        z[c] = Di[3 * c] * r[0] + Di[3 * c + 1] * r[1] + Di[3 * c + 2] * r[2];
+        a.z[3 * (size_t)row + c] = z[c];
+      }
+      vals[0] = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
+      vals[1] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    });
+    if (!grid_barrier(a.barrier, a.flags)) return;
+    model_sums<2>(a, pc0, pc1, sums);
+    it++;
+    for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+      if (s_conv[j]) continue;
+      double rho1 = sums[j][0];
+      s_beta[j] = rho1 / s_rho[j];
+      s_rho[j] = rho1;
+      s_iters[j] = it;
+      if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j])) s_conv[j] = 1;
+    }
+    __syncthreads();
+    if (it >= a.max_iter) break;
+  }
+
+  // ---- final: true residual b - S x, and the state update
+  cta_row_pass<1, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+    double Ax[3];
+    warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
+    if (lane == 0) {
+      double rr = 0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double d = a.b[3 * (size_t)row + c] - Ax[c];
+        rr += d * d;
+      }
+      vals[0] = rr;
+    }
+  });
+  if (!grid_barrier(a.barrier, a.flags)) return;
+  model_sums<1>(a, pc0, pc1, sums);
+  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+    int m = a.piece_model[pc0 + j];
+    if (pc0 + j == a.model_piece[m + 1] - 1) {
+      double* o = a.model_out + (size_t)m * 4;
+      o[0] = s_iters[j];
+      o[1] = s_bb[j] > 0 ? sqrt(sums[j][0] / s_bb[j]) : sqrt(sums[j][0]);
+      o[2] = s_conv[j];
+    }
+  }
+  if (a.update_state) {
+    const int r0 = a.piece_row[pc0], r1 = a.piece_row[pc1];
+    for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+      int n = a.act_node[row];
+      double h = a.step[(size_t)a.row_model[row] * 8];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double vn = a.x[3 * (size_t)row + c];
+        a.vel[3 * (size_t)n + c] = vn;
+        a.xpos[3 * (size_t)n + c] += h * vn;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
+  DevPack& d = eng.d;
+  ElemArgs a;
+  a.e0 = g.e0;
+  a.e1 = g.e1;
+  a.conn = d.conn;
+  a.elem_model = d.elem_model;
+  a.x = d.x;
+  a.invJ0 = d.invJ0;
+  a.invJ0_f = d.invJ0_f;
+  a.winvJ0 = d.winvJ0;
+  a.K0 = d.K0;
+  a.f0 = d.f0;
+  a.sidx = d.sidx;
+  a.mat = d.mat;
+  a.node_p = d.node_p;
+  a.elemK = fp32 ? (void*)d.elemK_f : (void*)d.elemK;
+  a.elemF = d.elemF;
+  a.flags = d.flags;
+  a.mindet = (long long*)d.dmin;
+  return a;
+}
+
+template <int TYPE, typename T>
+static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
+  ElemArgs a = elem_args(eng, g, fp32);
+  int ne = g.e1 - g.e0;
+  if (ne <= 0) return cudaSuccess;
+  if (g.mat_kind == B200FEM_MAT_LINEAR) {
+    constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 8;
+    a.elemK = (void*)eng.d.elemK;  // linear path stays FP64
+    elem_linear_kernel<TYPE, double><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
+    return cudaGetLastError();
+  }
+  constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 4;
+  const int threads = TYPE == B200FEM_ELEM_TET ? 256 : 192;
+  const int blocks = (ne + EPB - 1) / EPB;
+  if (g.mat_kind == B200FEM_MAT_NEOHOOKEAN) {
+    elem_nonlinear_kernel<TYPE, B200FEM_MAT_NEOHOOKEAN, false, T><<<blocks, threads, 0, eng.stream>>>(a);
+  } else if (g.nodal) {
+    elem_nonlinear_kernel<TYPE, B200FEM_MAT_MOONEYRIVLIN, true, T><<<blocks, threads, 0, eng.stream>>>(a);
+  } else {
+    elem_nonlinear_kernel<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T><<<blocks, threads, 0, eng.stream>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
+  (void)cK;
+  (void)cM;
+  cudaError_t e = ensure_constants(eng.device);
+  if (e != cudaSuccess) return e;
+  DevPack& d = eng.d;
+  // reset inverted-element counter and min detJ
+  if ((e = cudaMemsetAsync(d.flags + 1, 0, sizeof(int), eng.stream)) != cudaSuccess) return e;
+  long long big = 0x7fefffffffffffffll;  // ordered bits of DBL_MAX
+  if ((e = cudaMemcpyAsync(d.dmin, &big, sizeof(long long), cudaMemcpyHostToDevice, eng.stream)) != cudaSuccess)
+    return e;
+  const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  for (const ElemGroup& g : eng.groups) {
+    if (g.elem_type == B200FEM_ELEM_TET)
+      e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);
+    else
+      e = fp32 ? launch_group<B200FEM_ELEM_HEX, float>(eng, g, true) : launch_group<B200FEM_ELEM_HEX, double>(eng, g, false);
+    if (e != cudaSuccess) return e;
+  }
+  long long n9 = d.nnzb * 9;
+  int threads = 256;
+  long long blocks = (n9 + threads - 1) / threads;
+  if (want_K) {
+    gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
+        d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
+        d.step, 0, d.K);
+  } else {
+    gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
+        d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
+        d.step, 1, d.S);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rhs(Engine& eng) {
+  DevPack& d = eng.d;
+  int threads = 256;
+  rows_kernel<double><<<(d.n_nodes + threads - 1) / threads, threads, 0, eng.stream>>>(
+      d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx, d.node_model, d.mass, d.v, d.fext, d.step, d.fint, d.b,
+      d.sol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_forces_only(Engine& eng) {
+  DevPack& d = eng.d;
+  int threads = 256;
+  rows_kernel<double><<<(d.n_nodes + threads - 1) / threads, threads, 0, eng.stream>>>(
+      d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx, d.node_model, d.mass, d.v, d.fext, d.step, d.fint,
+      nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spmv(Engine& eng, const double* x, double* y) {
+  DevPack& d = eng.d;
+  int threads = 256;
+  long long blocks = ((long long)d.n_rows * 32 + threads - 1) / threads;
+  spmv_kernel<double><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.blk_rowptr, d.blk_col, d.S, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs) {
+  DevPack& d = eng.d;
+  long long n9 = d.nnzb * 9;
+  int threads = 256;
+  crs_export_kernel<<<(unsigned)((n9 + threads - 1) / threads), threads, 0, eng.stream>>>(d.nnzb, d.blk_row,
+                                                                                         d.blk_rowptr, vals, crs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero) {
+  DevPack& d = eng.d;
+  cudaError_t e;
+  if (init_zero) {
+    if ((e = cudaMemsetAsync(d.sol, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
+  }
+  if ((e = cudaMemsetAsync(d.unconv, 0, sizeof(int) * (size_t)(max_iter + 2), eng.stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(d.barrier, 0, 2 * sizeof(unsigned), eng.stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(d.p, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(d.q, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
+  PcgArgs a;
+  a.n_rows = d.n_rows;
+  a.rowptr = d.blk_rowptr;
+  a.col = d.blk_col;
+  a.blk_diag = d.blk_diag;
+  a.S = d.S;
+  a.Dinv = d.Dinv;
+  a.b = d.b;
+  a.x = d.sol;
+  a.r = d.r;
+  a.z = d.z;
+  a.p = d.p;
+  a.q = d.q;
+  a.piece_row = d.piece_row;
+  a.piece_model = d.piece_model;
+  a.model_piece = d.model_piece;
+  a.cta_piece = d.cta_piece;
+  a.partials = d.partials;
+  a.step = d.step;
+  a.model_out = d.model_scal;
+  a.barrier = d.barrier;
+  a.flags = d.flags;
+  a.unconv = d.unconv;
+  a.max_iter = max_iter;
+  a.update_state = update_state ? 1 : 0;
+  a.init_dinv = 1;
+  a.xpos = d.x;
+  a.vel = d.v;
+  a.act_node = d.act_node;
+  a.row_model = d.row_model;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(eng.pcg_grid);
+  cfg.blockDim = dim3(kPcgThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = eng.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
+}
+
+int pcg_threads() { return kPcgThreads; }
+int pcg_max_cta_pieces() { return kMaxCtaPieces; }
+
+int pcg_max_grid(int device) {
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<double>, kPcgThreads, 0);
+  return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+}  // namespace b200fem

@@ -1,0 +1,341 @@
+// setup.cpp -- host-side setup of the B200 FEM engine: grid factory, rest
+// data, lumped masses, linear stiffness cache, block pattern, CRS slot map
+// and the element-to-block scatter map.  Runs once per structure change
+// (the reference rebuilds these only when the solve-matrix structure
+// version changes, MechSystemSolver.updateSolveMatrixStructure,
+// MechSystemSolver.java:2484-2493).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "engine.h"
+
+namespace b200fem {
+
+namespace {
+
+// Shape-function derivatives dN/ds for the reference elements.
+// TetElement.getdNds (TetElement.java:204-215); one integration point, weight
+// 1/6 (TetElement.java:31-33).
+const double kTetGNs[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+// HexElement node natural coordinates (HexElement.java:119-129)
+const double kHexNode[8][3] = {{-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1},
+                               {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}};
+
+void hex_grad(double* g, int i, double s0, double s1, double s2) {
+  // HexElement.getdNds (HexElement.java:266-281)
+  double a = kHexNode[i][0] < 0 ? -1 : 1, b = kHexNode[i][1] < 0 ? -1 : 1,
+         c = kHexNode[i][2] < 0 ? -1 : 1;
+  g[0] = 0.125 * a * (1 + b * s1) * (1 + c * s2);
+  g[1] = 0.125 * (1 + a * s0) * b * (1 + c * s2);
+  g[2] = 0.125 * (1 + a * s0) * (1 + b * s1) * c;
+}
+
+double det33(const double* m) {
+  return m[0] * m[4] * m[8] + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] - m[6] * m[4] * m[2] -
+         m[0] * m[7] * m[5] - m[3] * m[1] * m[8];
+}
+
+// Matrix3dBase.fastInvert (Matrix3dBase.java:1615-1648)
+double invert33(double* inv, const double* d) {
+  double det = det33(d);
+  if (det != 0) {
+    double s = 1.0 / det;
+    inv[0] = s * (d[4] * d[8] - d[5] * d[7]);
+    inv[1] = s * (d[2] * d[7] - d[1] * d[8]);
+    inv[2] = s * (d[1] * d[5] - d[4] * d[2]);
+    inv[3] = s * (d[5] * d[6] - d[3] * d[8]);
+    inv[4] = s * (d[0] * d[8] - d[2] * d[6]);
+    inv[5] = s * (d[2] * d[3] - d[0] * d[5]);
+    inv[6] = s * (d[3] * d[7] - d[4] * d[6]);
+    inv[7] = s * (d[1] * d[6] - d[0] * d[7]);
+    inv[8] = s * (d[0] * d[4] - d[1] * d[3]);
+  }
+  return det;
+}
+
+// Shape gradients for integration point k (or the warping point, k = -1).
+void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
+  if (type == B200FEM_ELEM_TET) {
+    std::memcpy(g, kTetGNs, sizeof(kTetGNs));
+    *w = 1.0 / 6.0;
+  } else if (k < 0) {
+    // warping point: centre, weight 8 (HexElement.java:84-90)
+    for (int i = 0; i < 8; i++) hex_grad(g + 3 * i, i, 0, 0, 0);
+    *w = 8;
+  } else {
+    // INTEGRATION_COORDS_GAUSS_8 (HexElement.java:159-170): point k sits at
+    // the node-k corner scaled by 1/sqrt(3), weight 1
+    double q = 1 / std::sqrt(3.0);
+    for (int i = 0; i < 8; i++)
+      hex_grad(g + 3 * i, i, kHexNode[k][0] * q, kHexNode[k][1] * q, kHexNode[k][2] * q);
+    *w = 1;
+  }
+}
+
+// J = sum_n x_n (outer) dN_n/ds  (IntegrationPoint3d.computeJacobian,
+// IntegrationPoint3d.java:190-201)
+void jacobian(double* J, const double* g, int nen, const double* xyz, const int* nodes) {
+  for (int i = 0; i < 9; i++) J[i] = 0;
+  for (int n = 0; n < nen; n++) {
+    const double* p = xyz + 3 * (size_t)nodes[n];
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) J[3 * r + c] += p[r] * g[3 * n + c];
+  }
+}
+
+// LinearMaterial.getC (LinearMaterial.java:148-159), Voigt (xx,yy,zz,xy,yz,xz)
+void linear_tangent(double* C, double E, double nu) {
+  double a = E / (1 + nu);
+  double dia = (1 - nu) / (1 - 2 * nu) * a, mu = 0.5 * a, off = nu / (1 - 2 * nu) * a;
+  std::fill(C, C + 36, 0.0);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) C[6 * i + j] = i == j ? dia : off;
+  C[21] = C[28] = C[35] = mu;
+}
+
+// K += B_i^T D B_j dv  (FemUtilities.addMaterialStiffness, FemUtilities.java:78-129)
+void add_bdb(double* K, const double* gi, const double* D, const double* gj, double dv) {
+  double x = gj[0] * dv, y = gj[1] * dv, z = gj[2] * dv;
+  double t[6][3];
+  for (int r = 0; r < 6; r++) {
+    const double* d = D + 6 * r;
+    t[r][0] = d[0] * x + d[3] * y + d[5] * z;
+    t[r][1] = d[1] * y + d[3] * x + d[4] * z;
+    t[r][2] = d[2] * z + d[4] * y + d[5] * x;
+  }
+  for (int c = 0; c < 3; c++) {
+    K[c] += gi[0] * t[0][c] + gi[1] * t[3][c] + gi[2] * t[5][c];
+    K[3 + c] += gi[1] * t[1][c] + gi[0] * t[3][c] + gi[2] * t[4][c];
+    K[6 + c] += gi[2] * t[2][c] + gi[1] * t[4][c] + gi[0] * t[5][c];
+  }
+}
+
+}  // namespace
+
+int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
+  if (nx < 1 || ny < 1 || nz < 1) return B200FEM_ERR_INVALID_ARG;
+  if (type != B200FEM_ELEM_TET && type != B200FEM_ELEM_HEX) return B200FEM_ERR_INVALID_ARG;
+  *nn = (nx + 1) * (ny + 1) * (nz + 1);
+  *ne = (type == B200FEM_ELEM_TET ? 5 : 1) * nx * ny * nz;
+  return B200FEM_OK;
+}
+
+// FemFactory.createGridNodes (FemFactory.java:53-78); createTetGrid
+// (:86-126) splits each cell with Tetrahedralizer.subdivideHex(allOnX =
+// (i+j+k) odd) (Tetrahedralizer.java:135-141), whose parseCode /
+// getTetIndicesForHex (:203-300) reduce to the two 5-tet tables below;
+// createHexGrid (:203-255).
+void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
+                 int* conn) {
+  const double sx = 1.0 / nx, sy = 1.0 / ny, sz = 1.0 / nz;
+  size_t n = 0;
+  for (int k = 0; k <= nz; k++)
+    for (int j = 0; j <= ny; j++)
+      for (int i = 0; i <= nx; i++, n++) {
+        xyz[3 * n + 0] = wx * (-0.5 + i * sx);
+        xyz[3 * n + 1] = wy * (-0.5 + j * sy);
+        xyz[3 * n + 2] = wz * (-0.5 + k * sz);
+      }
+  // central tetrahedron {0,2,5,7} when allOnX, {1,6,4,3} otherwise
+  static const int kOdd[5][4] = {{1, 0, 2, 5}, {3, 0, 7, 2}, {4, 0, 5, 7}, {6, 2, 7, 5}, {0, 2, 5, 7}};
+  static const int kEven[5][4] = {{0, 1, 4, 3}, {2, 3, 6, 1}, {5, 4, 1, 6}, {7, 6, 3, 4}, {1, 6, 4, 3}};
+  const int wk = (nx + 1) * (ny + 1), wj = nx + 1;
+  size_t e = 0;
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        const int c[8] = {(k + 1) * wk + j * wj + i,       (k + 1) * wk + j * wj + i + 1,
+                          (k + 1) * wk + (j + 1) * wj + i + 1, (k + 1) * wk + (j + 1) * wj + i,
+                          k * wk + j * wj + i,             k * wk + j * wj + i + 1,
+                          k * wk + (j + 1) * wj + i + 1,   k * wk + (j + 1) * wj + i};
+        if (type == B200FEM_ELEM_HEX) {
+          std::memcpy(conn + 8 * e, c, sizeof(c));
+          e++;
+        } else {
+          const int(*t)[4] = ((i + j + k) % 2 != 0) ? kOdd : kEven;
+          for (int q = 0; q < 5; q++, e++)
+            for (int a = 0; a < 4; a++) conn[4 * e + a] = c[t[q][a]];
+        }
+      }
+}
+
+void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
+                 unsigned long long seed, double* xyz) {
+  unsigned long long s = seed;
+  auto next = [&s]() {
+    unsigned long long z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  const double sp[3] = {wx / nx, wy / ny, wz / nz};
+  size_t n = 0;
+  for (int k = 0; k <= nz; k++)
+    for (int j = 0; j <= ny; j++)
+      for (int i = 0; i <= nx; i++, n++) {
+        if (i == 0 || i == nx || j == 0 || j == ny || k == 0 || k == nz) continue;
+        for (int a = 0; a < 3; a++) xyz[3 * n + a] += (2 * next() - 1) * frac * sp[a];
+      }
+}
+
+int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
+  const int nen = m.elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  h.nen = nen;
+  h.nip = m.elem_type == B200FEM_ELEM_TET ? 1 : 8;
+  h.npair = nen * (nen + 1) / 2;
+  const int N = m.n_nodes, E = m.n_elems;
+  for (int q = 0; q < E * nen; q++)
+    if (m.conn[q] < 0 || m.conn[q] >= N) {
+      err = "connectivity index out of range";
+      return B200FEM_ERR_INVALID_ARG;
+    }
+  // solve indices in node order (MechSystemBase.updateDynamicComponentLists,
+  // MechSystemBase.java:689-760: active components numbered in tree order)
+  h.sidx.assign(N, -1);
+  h.act_node.clear();
+  for (int n = 0; n < N; n++)
+    if (!m.fixed[n]) {
+      h.sidx[n] = (int)h.act_node.size();
+      h.act_node.push_back(n);
+    }
+  h.n_active = (int)h.act_node.size();
+  // soft incompressibility: OFF for compressible materials
+  // (FemModel3d.java:3346-3348); AUTO -> NODAL if #elements > #active nodes
+  // else ELEMENT (getAllowedSoftIncompMethod, FemModel3d.java:462-481)
+  int method = m.incomp_request;
+  if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
+  else if (method == B200FEM_INCOMP_AUTO)
+    method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
+  if (method == B200FEM_INCOMP_ELEMENT) {
+    err = "ELEMENT soft incompressibility is not supported (use OFF or NODAL)";
+    return B200FEM_ERR_UNSUPPORTED;
+  }
+  h.incomp = method;
+
+  // rest data: IntegrationData3d.myInvJ0/myDetJ0 (IntegrationData3d.java:108-111)
+  h.invJ0.assign((size_t)E * h.nip * 9, 0);
+  h.detJ0.assign((size_t)E * h.nip, 0);
+  h.winvJ0.assign((size_t)E * 9, 0);
+  h.rest_vol.assign(E, 0);
+  double g[kMaxNen * 3], wgt, J[9];
+  for (int e = 0; e < E; e++) {
+    const int* nodes = &m.conn[(size_t)e * nen];
+    double vol = 0;
+    for (int k = 0; k < h.nip; k++) {
+      shape_grads(m.elem_type, k, g, &wgt);
+      jacobian(J, g, nen, m.rest.data(), nodes);
+      double d = invert33(&h.invJ0[((size_t)e * h.nip + k) * 9], J);
+      if (!(d > 0)) {
+        err = "element " + std::to_string(e) + " has non-positive rest volume";
+        return B200FEM_ERR_INVERTED;
+      }
+      h.detJ0[(size_t)e * h.nip + k] = d;
+      vol += d * wgt;
+    }
+    if (m.elem_type == B200FEM_ELEM_TET) {
+      // TetElement.computeRestVolumes = detJ0/6 (TetElement.java:247-254)
+      vol = h.detJ0[e] / 6;
+      std::memcpy(&h.winvJ0[(size_t)e * 9], &h.invJ0[(size_t)e * 9], 9 * sizeof(double));
+    } else {
+      shape_grads(m.elem_type, -1, g, &wgt);
+      jacobian(J, g, nen, m.rest.data(), nodes);
+      invert33(&h.winvJ0[(size_t)e * 9], J);
+    }
+    h.rest_vol[e] = vol;
+  }
+  // lumped masses (FemNode3d.computeMassFromDensity, FemNode3d.java:1030-1045)
+  h.mass.assign(N, 0);
+  for (int e = 0; e < E; e++) {
+    double share = h.rest_vol[e] * m.density / nen;
+    for (int a = 0; a < nen; a++) h.mass[m.conn[(size_t)e * nen + a]] += share;
+  }
+  // linear materials: rest stiffness K0 and f0 = K0 x_rest
+  // (LinearMaterialCache.addInitialStiffness, LinearMaterialCache.java:115-160)
+  h.K0.clear();
+  h.f0.clear();
+  if (m.mat_kind == B200FEM_MAT_LINEAR) {
+    double C[36];
+    linear_tangent(C, m.mat_params[0], m.mat_params[1]);
+    h.K0.assign((size_t)E * nen * nen * 9, 0);
+    h.f0.assign((size_t)E * nen * 3, 0);
+    double gx[kMaxNen * 3];
+    for (int e = 0; e < E; e++) {
+      double* K0 = &h.K0[(size_t)e * nen * nen * 9];
+      for (int k = 0; k < h.nip; k++) {
+        shape_grads(m.elem_type, k, g, &wgt);
+        const double* iJ = &h.invJ0[((size_t)e * h.nip + k) * 9];
+        double dv0 = h.detJ0[(size_t)e * h.nip + k] * wgt;
+        for (int n = 0; n < nen; n++)
+          for (int c = 0; c < 3; c++)
+            gx[3 * n + c] = iJ[c] * g[3 * n] + iJ[3 + c] * g[3 * n + 1] + iJ[6 + c] * g[3 * n + 2];
+        for (int i = 0; i < nen; i++)
+          for (int j = 0; j < nen; j++) add_bdb(&K0[(i * nen + j) * 9], &gx[3 * i], C, &gx[3 * j], dv0);
+      }
+      const int* nodes = &m.conn[(size_t)e * nen];
+      for (int i = 0; i < nen; i++)
+        for (int j = 0; j < nen; j++) {
+          const double* Kij = &K0[(i * nen + j) * 9];
+          const double* p = &m.rest[3 * (size_t)nodes[j]];
+          for (int r = 0; r < 3; r++)
+            h.f0[((size_t)e * nen + i) * 3 + r] += Kij[3 * r] * p[0] + Kij[3 * r + 1] * p[1] + Kij[3 * r + 2] * p[2];
+        }
+    }
+  }
+  // node neighbours: nodes sharing an element, self included
+  // (FemNodeNeighbor lists; FemModel3d.addSolveBlocks, FemModel3d.java:4099-4112)
+  std::vector<int> inc_ptr(N + 1, 0);
+  for (int q = 0; q < E * nen; q++) inc_ptr[m.conn[q] + 1]++;
+  for (int n = 0; n < N; n++) inc_ptr[n + 1] += inc_ptr[n];
+  std::vector<int> inc(E * nen), fill(inc_ptr.begin(), inc_ptr.end() - 1);
+  for (int e = 0; e < E; e++)
+    for (int a = 0; a < nen; a++) inc[fill[m.conn[(size_t)e * nen + a]]++] = e;
+  h.nbr.assign(N, {});
+  for (int n = 0; n < N; n++) {
+    auto& v = h.nbr[n];
+    for (int q = inc_ptr[n]; q < inc_ptr[n + 1]; q++) {
+      const int* nodes = &m.conn[(size_t)inc[q] * nen];
+      v.insert(v.end(), nodes, nodes + nen);
+    }
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  // block rows over active nodes; NODAL adds every pair of nodes that share
+  // a neighbour (indirect neighbours, FemModel3d.java:5397-5416)
+  h.rowptr.assign(h.n_active + 1, 0);
+  h.col.clear();
+  std::vector<int> cols;
+  for (int r = 0; r < h.n_active; r++) {
+    int n = h.act_node[r];
+    cols.clear();
+    if (h.incomp == B200FEM_INCOMP_NODAL) {
+      for (int a : h.nbr[n])
+        for (int b : h.nbr[a])
+          if (h.sidx[b] >= 0) cols.push_back(h.sidx[b]);
+    } else {
+      for (int b : h.nbr[n])
+        if (h.sidx[b] >= 0) cols.push_back(h.sidx[b]);
+    }
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    h.col.insert(h.col.end(), cols.begin(), cols.end());
+    h.rowptr[r + 1] = (int)h.col.size();
+  }
+  if (h.incomp == B200FEM_INCOMP_NODAL) {
+    // nodal rest volumes (updateNodalRestVolumes, FemModel3d.java:2594-2628)
+    h.node_rest_vol.assign(N, 0);
+    for (int e = 0; e < E; e++) {
+      const int* nodes = &m.conn[(size_t)e * nen];
+      if (m.elem_type == B200FEM_ELEM_TET) {
+        for (int a = 0; a < 4; a++) h.node_rest_vol[nodes[a]] += h.rest_vol[e] / 4;
+      } else {
+        for (int a = 0; a < 8; a++) h.node_rest_vol[nodes[a]] += h.detJ0[(size_t)e * 8 + a];
+      }
+    }
+  }
+  return B200FEM_OK;
+}
+
+}  // namespace b200fem

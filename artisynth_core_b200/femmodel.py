@@ -1,0 +1,389 @@
+"""Host-side mirror of the reference interface for the FEM hot path.
+
+Names follow ArtiSynth: ``FemFactory.createTetGrid/createHexGrid``,
+``FemModel3d`` (setMaterial, setDensity, setMassDamping,
+setStiffnessDamping, setGravity, updateStressAndStiffness, ...),
+``LinearMaterial`` / ``NeoHookeanMaterial`` / ``MooneyRivlinMaterial`` and
+``MechSystemSolver.backwardEuler``.  Every numerical operation is a call
+into libb200fem.so (sm_100a kernels); this module only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+# ---------------------------------------------------------------- materials
+@dataclass
+class LinearMaterial:
+    """LinearMaterial(E, nu) is corotated by default (LinearMaterial.java:53-55)."""
+
+    E: float = 500000.0
+    nu: float = 0.33
+    corotated: bool = True
+
+    kind = L.MAT_LINEAR
+
+    def params(self):
+        return [self.E, self.nu, 1.0 if self.corotated else 0.0]
+
+    def isIncompressible(self):
+        return False
+
+
+@dataclass
+class NeoHookeanMaterial:
+    E: float = 500000.0
+    nu: float = 0.33
+
+    kind = L.MAT_NEOHOOKEAN
+
+    def params(self):
+        return [self.E, self.nu]
+
+    def isIncompressible(self):
+        return False
+
+
+@dataclass
+class MooneyRivlinMaterial:
+    """MooneyRivlinMaterial(c10, c01, c11, c20, c02, kappa)
+    (MooneyRivlinMaterial.java:98-108); bulk potential QUADRATIC by default
+    (IncompressibleMaterialBase.java:13-14)."""
+
+    c10: float = 150000.0
+    c01: float = 0.0
+    c11: float = 0.0
+    c20: float = 0.0
+    c02: float = 0.0
+    kappa: float = 100000.0
+    jlimit: float = 0.0
+    bulk_potential: int = 0  # 0 QUADRATIC, 1 LOGARITHMIC
+
+    kind = L.MAT_MOONEYRIVLIN
+
+    def params(self):
+        return [self.c10, self.c01, self.c11, self.c20, self.c02, self.kappa, self.jlimit,
+                float(self.bulk_potential)]
+
+    def isIncompressible(self):
+        return True
+
+
+# ------------------------------------------------------------------ factory
+def grid_dims(elem_type, nx, ny, nz):
+    nn, ne = ctypes.c_int(), ctypes.c_int()
+    L.check(L.lib().b200fem_grid_dims(elem_type, nx, ny, nz, ctypes.byref(nn), ctypes.byref(ne)))
+    return nn.value, ne.value
+
+
+def create_grid(elem_type, wx, wy, wz, nx, ny, nz):
+    nn, ne = grid_dims(elem_type, nx, ny, nz)
+    nen = 4 if elem_type == L.ELEM_TET else 8
+    xyz = np.zeros(3 * nn)
+    conn = np.zeros(nen * ne, dtype=np.int32)
+    L.check(L.lib().b200fem_create_grid(elem_type, wx, wy, wz, nx, ny, nz, L.dptr(xyz), L.iptr(conn)))
+    return xyz.reshape(-1, 3), conn.reshape(-1, nen)
+
+
+def jitter_grid(xyz, nx, ny, nz, wx, wy, wz, frac, seed):
+    flat = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1).copy()
+    L.check(L.lib().b200fem_jitter_grid(nx, ny, nz, wx, wy, wz, float(frac), ctypes.c_ulonglong(seed),
+                                        L.dptr(flat)))
+    return flat.reshape(-1, 3)
+
+
+class FemFactory:
+    """FemFactory.createTetGrid / createHexGrid (FemFactory.java:86-255)."""
+
+    @staticmethod
+    def createTetGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_TET, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
+    def createHexGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_HEX, wx, wy, wz, nx, ny, nz)
+        return m
+
+
+# ------------------------------------------------------------------- engine
+class FemEngine:
+    """Owns one libb200fem handle (CuDssJNI-style opaque handle)."""
+
+    def __init__(self, device: int = 0, precision: int = L.PREC_FP64):
+        cfg = L.Config(device, precision)
+        h = L.lib().b200fem_create(ctypes.byref(cfg))
+        if not h:
+            msg = L.lib().b200fem_last_error(None)
+            raise L.B200FemError(L.ERR_CUDA, (msg or b"").decode())
+        self.h = ctypes.c_void_p(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            L.lib().b200fem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name, *args):
+        return L.check(getattr(L.lib(), name)(self.h, *args), self.h)
+
+
+# -------------------------------------------------------------------- model
+class FemModel3d:
+    """FemModel3d restricted to the hot path: one element type (tet or hex),
+    one material, lumped mass, fixed nodes and the BackwardEuler data."""
+
+    def __init__(self):
+        self.elem_type = L.ELEM_TET
+        self.rest = None
+        self.conn = None
+        self.fixed = None
+        self.material = LinearMaterial()
+        self.density = 1000.0
+        self.mass_damping = 2.0      # FemModel.DEFAULT_MASS_DAMPING (FemModel.java:304)
+        self.stiffness_damping = 0.0  # FemModel.DEFAULT_STIFFNESS_DAMPING (:303)
+        self.gravity = np.array([0.0, 0.0, -9.8])  # MechModel default (MechModel.java:125)
+        self.soft_incomp = L.INCOMP_AUTO  # FemModel3d.DEFAULT_SOFT_INCOMP (:196)
+        self.fext = None
+        self._grid = None
+        self._engine = None
+        self.precision = L.PREC_FP64
+        self.device = 0
+
+    # --- construction
+    def _set_grid(self, elem_type, wx, wy, wz, nx, ny, nz):
+        self.elem_type = elem_type
+        xyz, conn = create_grid(elem_type, wx, wy, wz, nx, ny, nz)
+        self.rest = xyz
+        self.conn = conn
+        self.fixed = np.zeros(xyz.shape[0], dtype=np.int32)
+        self._grid = (nx, ny, nz, wx, wy, wz)
+        self._invalidate()
+
+    def setMesh(self, elem_type, rest, conn, fixed=None):
+        self.elem_type = elem_type
+        self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1, 3)
+        nen = 4 if elem_type == L.ELEM_TET else 8
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, nen)
+        self.fixed = (np.zeros(self.rest.shape[0], dtype=np.int32) if fixed is None
+                      else np.ascontiguousarray(fixed, dtype=np.int32))
+        self._grid = None
+        self._invalidate()
+
+    def jitterInterior(self, frac, seed):
+        """Seeded jitter of interior grid nodes, applied to rest and current
+        positions before setup."""
+        if self._grid is None:
+            raise ValueError("jitter needs a grid built by FemFactory")
+        nx, ny, nz, wx, wy, wz = self._grid
+        self.rest = jitter_grid(self.rest, nx, ny, nz, wx, wy, wz, frac, seed)
+        self._invalidate()
+
+    def numNodes(self):
+        return self.rest.shape[0]
+
+    def numElements(self):
+        return self.conn.shape[0]
+
+    def setMaterial(self, mat):
+        self.material = mat
+        self._invalidate()
+
+    def setDensity(self, d):
+        self.density = float(d)
+        self._invalidate()
+
+    def setMassDamping(self, d):
+        self.mass_damping = float(d)
+
+    setParticleDamping = setMassDamping
+
+    def setStiffnessDamping(self, d):
+        self.stiffness_damping = float(d)
+
+    def setGravity(self, gx, gy=None, gz=None):
+        self.gravity = np.array([gx, gy, gz] if gy is not None else gx, dtype=np.float64).reshape(3)
+
+    def setSoftIncompMethod(self, method):
+        self.soft_incomp = int(method)
+        self._invalidate()
+
+    def fixNodes(self, mask):
+        """node.setDynamic(false) for every node where mask is true."""
+        self.fixed = np.ascontiguousarray(np.asarray(mask).astype(np.int32))
+        self._invalidate()
+
+    def setExternalForces(self, fext):
+        self.fext = None if fext is None else np.ascontiguousarray(fext, dtype=np.float64).reshape(-1, 3)
+        if self._engine is not None:
+            self._push_fext()
+
+    def setPrecision(self, precision):
+        self.precision = int(precision)
+        self._invalidate()
+
+    # --- engine
+    def _invalidate(self):
+        if self._engine is not None:
+            self._engine.close()
+        self._engine = None
+
+    def _push_fext(self):
+        f = self.fext.reshape(-1).copy() if self.fext is not None else None
+        self._engine.call("b200fem_set_external_forces", L.dptr(f))
+
+    def engine(self) -> FemEngine:
+        if self._engine is None:
+            eng = FemEngine(self.device, self.precision)
+            rest = np.ascontiguousarray(self.rest.reshape(-1))
+            conn = np.ascontiguousarray(self.conn.reshape(-1))
+            eng.call("b200fem_set_mesh", self.elem_type, self.numNodes(), L.dptr(rest), self.numElements(),
+                     L.iptr(conn), L.iptr(self.fixed))
+            prm = np.zeros(8)
+            p = self.material.params()
+            prm[: len(p)] = p
+            eng.call("b200fem_set_material", self.material.kind, L.dptr(prm), self.density, self.soft_incomp)
+            eng.call("b200fem_build")
+            self._engine = eng
+            if self.fext is not None:
+                self._push_fext()
+        return self._engine
+
+    # --- queries
+    def sizes(self):
+        e = self.engine()
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        e.call("b200fem_get_sizes", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d))
+        return dict(n_active=a.value, nnzb=b.value, crs_nnz_full=c.value, crs_nnz_upper=d.value)
+
+    def getSolveIndices(self):
+        out = np.zeros(self.numNodes(), dtype=np.int32)
+        self.engine().call("b200fem_get_solve_index", L.iptr(out))
+        return out
+
+    def getBlockPattern(self):
+        s = self.sizes()
+        rp = np.zeros(s["n_active"] + 1, dtype=np.int32)
+        col = np.zeros(s["nnzb"], dtype=np.int32)
+        self.engine().call("b200fem_get_pattern", L.iptr(rp), L.iptr(col))
+        return rp, col
+
+    def getCRSIndices(self, partition=L.PART_FULL):
+        s = self.sizes()
+        nnz = s["crs_nnz_full"] if partition == L.PART_FULL else s["crs_nnz_upper"]
+        ro = np.zeros(3 * s["n_active"] + 1, dtype=np.int32)
+        ci = np.zeros(nnz, dtype=np.int32)
+        self.engine().call("b200fem_get_crs_indices", partition, L.iptr(ro), L.iptr(ci))
+        return ro, ci
+
+    def createCrsBlockSlotMap(self, partition=L.PART_FULL):
+        s = self.sizes()
+        slots = np.zeros(9 * s["nnzb"], dtype=np.int32)
+        self.engine().call("b200fem_get_slot_map", partition, L.iptr(slots))
+        return slots
+
+    def getScatterMap(self):
+        nen = self.conn.shape[1]
+        out = np.zeros(self.numElements() * nen * nen, dtype=np.int32)
+        self.engine().call("b200fem_get_scatter_map", L.iptr(out))
+        return out.reshape(self.numElements(), nen, nen)
+
+    def getNodeMasses(self):
+        out = np.zeros(self.numNodes())
+        self.engine().call("b200fem_get_masses", L.dptr(out))
+        return out
+
+    def getSoftIncompMethod(self):
+        out = ctypes.c_int()
+        self.engine().call("b200fem_get_incomp_method", ctypes.byref(out))
+        return out.value
+
+    # --- state
+    def setState(self, x=None, v=None):
+        xe = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(-1).copy()
+        ve = None if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(-1).copy()
+        self.engine().call("b200fem_set_state", L.dptr(xe), L.dptr(ve))
+
+    def getState(self):
+        x = np.zeros(3 * self.numNodes())
+        v = np.zeros(3 * self.numNodes())
+        self.engine().call("b200fem_get_state", L.dptr(x), L.dptr(v))
+        return x.reshape(-1, 3), v.reshape(-1, 3)
+
+    # --- hot path
+    def updateStressAndStiffness(self, x=None, want_crs=False):
+        """Internal force (N,3), stiffness blocks (nnzb,3,3) in block-CSR
+        order and optionally the full-partition CRS values."""
+        s = self.sizes()
+        xe = None if x is None else np.ascontiguousarray(x, dtype=np.float64).reshape(-1).copy()
+        f = np.zeros(3 * self.numNodes())
+        K = np.zeros(9 * s["nnzb"])
+        crs = np.zeros(s["crs_nnz_full"]) if want_crs else None
+        self.engine().call("b200fem_update_stress_stiffness", L.dptr(xe), L.dptr(f), L.dptr(K), L.dptr(crs))
+        out = (f.reshape(-1, 3), K.reshape(-1, 3, 3))
+        return out + (crs,) if want_crs else out
+
+    def lastStats(self):
+        return None
+
+
+class MechSystemSolver:
+    """BackwardEuler integration of one FemModel3d on the device
+    (MechSystemSolver.backwardEuler, MechSystemSolver.java:2171-2476)."""
+
+    def __init__(self, model: FemModel3d, tol: float = 1e-10, max_iter: int = 10000):
+        self.model = model
+        self.tol = tol
+        self.max_iter = max_iter
+        self.abort_on_inverted = False
+        self.stats = L.Stats()
+
+    def params(self, h):
+        m = self.model
+        p = L.StepParams()
+        p.h = h
+        p.alpha_m = m.mass_damping
+        p.beta_k = m.stiffness_damping
+        for i in range(3):
+            p.gravity[i] = m.gravity[i]
+        p.tol = self.tol
+        p.max_iter = self.max_iter
+        p.abort_on_inverted = 1 if self.abort_on_inverted else 0
+        return p
+
+    def backwardEuler(self, h, nsteps=1):
+        p = self.params(h)
+        self.model.engine().call("b200fem_backward_euler_step", ctypes.byref(p), int(nsteps),
+                                 ctypes.byref(self.stats))
+        return self.stats
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1).copy()
+        y = np.zeros_like(x)
+        self.model.engine().call("b200fem_spmv", L.dptr(x), L.dptr(y))
+        return y
+
+    def pcg(self, b, x0=None, tol=1e-10, max_iter=10000):
+        b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1).copy()
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).reshape(-1).copy()
+        st = L.Stats()
+        self.model.engine().call("b200fem_pcg_solve", L.dptr(b), L.dptr(x), float(tol), int(max_iter),
+                                 ctypes.byref(st))
+        return x, st
+
+    def lastTiming(self):
+        a, s = ctypes.c_double(), ctypes.c_double()
+        self.model.engine().call("b200fem_last_timing", ctypes.byref(a), ctypes.byref(s))
+        return a.value, s.value

@@ -1,0 +1,175 @@
+/*
+ * b200fem.h -- C ABI of the B200 (sm_100a) FEM force/stiffness assembly and
+ * BackwardEuler step engine (libb200fem.so).
+ *
+ * The entry points mirror the operations of ArtiSynth's hot path and of the
+ * JNI bridge the reference already ships for its cuDSS solver:
+ *
+ *   handle lifecycle / errors  CuDssJNI.cc:15-747 (doInit, doDispose,
+ *                              doGetLastError), cudssBridge.h:39-52,187-189
+ *   pattern + CRS slot map     SparseNumberedBlockMatrix.createCrsBlockSlotMap
+ *                              (SparseNumberedBlockMatrix.java:389-498),
+ *                              SparseBlockMatrix.getCRSIndices (:1511-1532)
+ *   force/stiffness update     FemModel3d.updateStressAndStiffness
+ *                              (FemModel3d.java:2894-3051)
+ *   BackwardEuler step         MechSystemSolver.backwardEuler
+ *                              (MechSystemSolver.java:2171-2476)
+ *   SpMV / iterative solve     CuDssBridge::multiply / iterativeSolveBiCGStab
+ *                              (cudssBridge.cc:1419-1452,1705-2006)
+ *
+ * Conventions (same as the reference bridge): every function returns an int
+ * status, 0 on success and a negative B200FEM_ERR_* code on failure; the
+ * message of the last failure is available from b200fem_last_error().  The
+ * handle owns all device memory; caller arrays are borrowed for the duration
+ * of the call only.  Calls on one handle are synchronous and must not be
+ * made concurrently from several threads.  There is no CPU fallback: a
+ * handle cannot be created without a CUDA device.
+ *
+ * Array conventions: node positions/velocities/forces are (3*n_nodes)
+ * doubles in node order; connectivity is (nen*n_elems) int32 in the
+ * reference's local node order (TetElement, HexElement); stiffness blocks
+ * are 3x3 row-major, stored in block-CSR order over active nodes (block row
+ * = solve index), 9 doubles per block.
+ */
+#ifndef B200FEM_H
+#define B200FEM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (cf. CUDSS_BRIDGE_ERR_*, cudssBridge.h:39-52) */
+#define B200FEM_OK 0
+#define B200FEM_ERR_INVALID_ARG (-1)
+#define B200FEM_ERR_CUDA (-2)
+#define B200FEM_ERR_STATE (-3)
+#define B200FEM_ERR_UNSUPPORTED (-4)
+#define B200FEM_ERR_INVERTED (-5)
+#define B200FEM_ERR_BUDGET (-6)
+#define B200FEM_ERR_TIMEOUT (-7)
+#define B200FEM_ERR_NO_CONVERGE (-13)
+
+/* element types */
+#define B200FEM_ELEM_TET 0 /* TetElement, 4 nodes, 1 integration point */
+#define B200FEM_ELEM_HEX 1 /* HexElement, 8 nodes, 8 Gauss points */
+
+/* materials (parameter layout of b200fem_set_material) */
+#define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */
+#define B200FEM_MAT_NEOHOOKEAN 1   /* {E, nu}: NeoHookeanMaterial */
+#define B200FEM_MAT_MOONEYRIVLIN 2 /* {c10, c01, c11, c20, c02, kappa, jlimit,
+                                      bulk_potential(0 quadratic, 1 log)} */
+
+/* soft incompressibility (FemModel3d.IncompMethod) */
+#define B200FEM_INCOMP_OFF 0
+#define B200FEM_INCOMP_NODAL 1
+#define B200FEM_INCOMP_AUTO 2
+#define B200FEM_INCOMP_ELEMENT 3 /* resolved by AUTO; not supported */
+
+/* precision of the engine */
+#define B200FEM_PREC_FP64 0  /* plain FP64 drop-in */
+#define B200FEM_PREC_MIXED 1 /* FP32 element/SpMV, FP64 residual/dots/update */
+
+/* scalar CRS partitions (Matrix.Partition) */
+#define B200FEM_PART_FULL 0
+#define B200FEM_PART_UPPER 1
+
+typedef struct b200fem_engine* b200fem_handle;
+
+typedef struct {
+  int device;    /* CUDA device ordinal */
+  int precision; /* B200FEM_PREC_* */
+  int reserved[6];
+} b200fem_config;
+
+/* BackwardEuler parameters: FemModel.massDamping (default 2),
+   FemModel.stiffnessDamping (default 0), MechModel gravity, PCG controls. */
+typedef struct {
+  double h;          /* step size */
+  double alpha_m;    /* mass damping */
+  double beta_k;     /* stiffness damping */
+  double gravity[3]; /* gravity acceleration */
+  double tol;        /* PCG relative residual ||b - S v|| / ||b|| */
+  int max_iter;      /* PCG iteration cap (ERR_NO_CONVERGE beyond it) */
+  int abort_on_inverted; /* FemModel3d.abortOnInvertedElems */
+} b200fem_step_params;
+
+typedef struct {
+  int iterations;      /* PCG iterations of the last solve */
+  int num_inverted;    /* elements with detJ <= 0 at the last update */
+  double rel_residual; /* true relative residual of the last solve */
+  double min_detJ;     /* smallest Jacobian determinant seen */
+  int refinements;     /* iterative-refinement sweeps (mixed precision) */
+  int reserved[3];
+} b200fem_stats;
+
+/* ---- library / handle ---------------------------------------------------- */
+int b200fem_version(void);
+/* CuDssJNI doInit: returns NULL on failure (message via b200fem_last_error(NULL)) */
+b200fem_handle b200fem_create(const b200fem_config* cfg);
+/* CuDssJNI doDispose: idempotent; NULL is accepted */
+int b200fem_destroy(b200fem_handle h);
+/* CuDssJNI doGetLastError; h may be NULL for create failures */
+const char* b200fem_last_error(b200fem_handle h);
+
+/* ---- mesh factory (FemFactory.createTetGrid/createHexGrid, host only) ---- */
+int b200fem_grid_dims(int elem_type, int nx, int ny, int nz, int* n_nodes, int* n_elems);
+int b200fem_create_grid(int elem_type, double wx, double wy, double wz, int nx, int ny, int nz,
+                        double* xyz, int* conn);
+/* seeded interior-node jitter: (2u-1)*frac*spacing per axis, u from
+   splitmix64(seed) drawn in node order; boundary nodes stay put */
+int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
+                        unsigned long long seed, double* xyz);
+
+/* ---- model definition (FemModel3d nodes/elements/material) -------------- */
+/* fixed[n] != 0 marks a non-dynamic node (no solve index) */
+int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz,
+                     int n_elems, const int* conn, const int* fixed);
+int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, double density,
+                         int incomp_method);
+/* builds rest data, the block pattern, the element-to-block scatter map and
+   uploads everything (the reference's structure build + analyze) */
+int b200fem_build(b200fem_handle h);
+
+/* ---- pattern queries (bit-exact with the reference) ---------------------- */
+int b200fem_get_sizes(b200fem_handle h, int* n_active, int* nnzb, int* crs_nnz_full,
+                      int* crs_nnz_upper);
+/* solve index per node (-1 for fixed nodes), MechSystemBase numbering */
+int b200fem_get_solve_index(b200fem_handle h, int* sidx);
+int b200fem_get_pattern(b200fem_handle h, int* blk_rowptr, int* blk_col);
+/* 0-based scalar CRS row offsets (3*n_active+1) and column indices */
+int b200fem_get_crs_indices(b200fem_handle h, int partition, int* row_offs, int* col_idx);
+/* CrsBlockSlotMap: 9 slots per block in BSR order, -1 when excluded */
+int b200fem_get_slot_map(b200fem_handle h, int partition, int* slots);
+/* element-to-block scatter map: for every element and every local node pair
+   (i, j) (nen*nen per element) the BSR block index receiving K_ij, or -1 */
+int b200fem_get_scatter_map(b200fem_handle h, int* map);
+int b200fem_get_masses(b200fem_handle h, double* mass);
+int b200fem_get_incomp_method(b200fem_handle h, int* method);
+
+/* ---- state -------------------------------------------------------------- */
+int b200fem_set_state(b200fem_handle h, const double* x, const double* v);
+int b200fem_get_state(b200fem_handle h, double* x, double* v);
+int b200fem_set_external_forces(b200fem_handle h, const double* fext);
+
+/* ---- hot path ------------------------------------------------------------ */
+/* FemModel3d.updateStressAndStiffness at positions x (host, 3N): returns the
+   internal elastic force per node (3N; may be NULL), the stiffness blocks in
+   BSR order (9*nnzb; may be NULL) and/or the full-partition scalar CRS
+   values in the reference slot order (crs_nnz_full; may be NULL). */
+int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f_int,
+                                    double* k_blocks, double* crs_vals);
+/* nsteps BackwardEuler steps on the device-resident state */
+int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps,
+                                b200fem_stats* stats);
+/* y = S x with the solve matrix of the last step (host vectors, 3*n_active) */
+int b200fem_spmv(b200fem_handle h, const double* x, double* y);
+/* block-Jacobi PCG on the solve matrix of the last step (host vectors) */
+int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, int max_iter,
+                      b200fem_stats* stats);
+/* synchronise and report the device time of the last step/update call */
+int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200FEM_H */

@@ -1,0 +1,1346 @@
+// fem_oracle.cpp -- CPU FP64 restatement of ArtiSynth's FEM force/stiffness
+// assembly (FemModel3d.updateStressAndStiffness) and of the BackwardEuler
+// step (MechSystemSolver.backwardEuler).
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the correctness oracle: it may be
+// loaded by tests/, by __graft_entry__.smoke() and by the CPU-baseline leg of
+// bench.py, and only as the checker.  The product (artisynth_core_b200) never
+// links, loads or calls it.
+//
+// Every routine cites the reference file:line it restates (paths relative to
+// the artisynth_core source tree).  Arithmetic follows the reference
+// formulas; summation order follows the reference loops where practical.
+// The element loop runs over OpenMP threads but writes per-element buffers
+// that are reduced in a fixed order, so the result does not depend on the
+// thread count.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+enum { ELEM_TET = 0, ELEM_HEX = 1 };
+enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2 };
+enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
+
+// ---------------------------------------------------------------------------
+// small dense helpers (row-major 3x3)
+// ---------------------------------------------------------------------------
+
+static inline double det3(const double* m) {
+  // Matrix3dBase.determinant / fastInvert ordering (Matrix3dBase.java:1629)
+  return m[0] * m[4] * m[8] + m[3] * m[7] * m[2] + m[6] * m[1] * m[5] -
+         m[6] * m[4] * m[2] - m[0] * m[7] * m[5] - m[3] * m[1] * m[8];
+}
+
+// Matrix3dBase.fastInvert (Matrix3dBase.java:1615-1648): returns det, fills
+// inv only when det != 0.
+static double fast_invert(double* inv, const double* d) {
+  double det = det3(d);
+  if (det != 0) {
+    double deti = 1.0 / det;
+    inv[0] = deti * (d[4] * d[8] - d[5] * d[7]);
+    inv[3] = deti * (d[5] * d[6] - d[3] * d[8]);
+    inv[6] = deti * (d[3] * d[7] - d[4] * d[6]);
+    inv[1] = deti * (d[2] * d[7] - d[1] * d[8]);
+    inv[4] = deti * (d[0] * d[8] - d[2] * d[6]);
+    inv[7] = deti * (d[1] * d[6] - d[0] * d[7]);
+    inv[2] = deti * (d[1] * d[5] - d[4] * d[2]);
+    inv[5] = deti * (d[2] * d[3] - d[0] * d[5]);
+    inv[8] = deti * (d[0] * d[4] - d[1] * d[3]);
+  }
+  return det;
+}
+
+static inline void mul3(double* c, const double* a, const double* b) {
+  double t[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      t[3 * i + j] = a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j] + a[3 * i + 2] * b[6 + j];
+  std::memcpy(c, t, sizeof(t));
+}
+
+// ---------------------------------------------------------------------------
+// polar decomposition: R of F = R P with det(R) = +1
+// SVDecomposition3d.polarDecomposition (SVDecomposition3d.java:1418-1541):
+// R = U V^T, and when det(U) det(V) < 0 the column of U belonging to the
+// smallest singular value is negated.  Restated with a one-sided Jacobi
+// (Hestenes) SVD; the third column of U is formed as det(V) * (u1 x u2),
+// which is the same rotation for non-degenerate F and stays defined when the
+// smallest singular value vanishes.
+// ---------------------------------------------------------------------------
+static void polar_rotation(double* R, const double* F) {
+  double A[9], V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::memcpy(A, F, sizeof(A));
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0;
+    for (int p = 0; p < 2; p++) {
+      for (int q = p + 1; q < 3; q++) {
+        double al = 0, be = 0, ga = 0;
+        for (int r = 0; r < 3; r++) {
+          al += A[3 * r + p] * A[3 * r + p];
+          be += A[3 * r + q] * A[3 * r + q];
+          ga += A[3 * r + p] * A[3 * r + q];
+        }
+        if (ga == 0 || std::fabs(ga) <= 1e-300) continue;
+        double rel = std::fabs(ga) / std::sqrt(al * be);
+        off = std::max(off, rel);
+        if (rel < 1e-17) continue;
+        double zeta = (be - al) / (2 * ga);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+        double c = 1.0 / std::sqrt(1 + t * t), s = c * t;
+        for (int r = 0; r < 3; r++) {
+          double ap = A[3 * r + p], aq = A[3 * r + q];
+          A[3 * r + p] = c * ap - s * aq;
+          A[3 * r + q] = s * ap + c * aq;
+          double vp = V[3 * r + p], vq = V[3 * r + q];
+          V[3 * r + p] = c * vp - s * vq;
+          V[3 * r + q] = s * vp + c * vq;
+        }
+      }
+    }
+    if (off < 1e-16) break;
+  }
+  double sig[3];
+  int ord[3] = {0, 1, 2};
+  for (int k = 0; k < 3; k++)
+    sig[k] = std::sqrt(A[k] * A[k] + A[3 + k] * A[3 + k] + A[6 + k] * A[6 + k]);
+  std::sort(ord, ord + 3, [&](int a, int b) { return sig[a] > sig[b]; });
+  double U[9], Vs[9];
+  for (int kk = 0; kk < 3; kk++) {
+    int k = ord[kk];
+    for (int r = 0; r < 3; r++) {
+      Vs[3 * r + kk] = V[3 * r + k];
+      U[3 * r + kk] = sig[k] > 0 ? A[3 * r + k] / sig[k] : 0.0;
+    }
+  }
+  if (sig[ord[0]] == 0) {  // F == 0: reference falls back to identity
+    for (int i = 0; i < 9; i++) R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    return;
+  }
+  // re-orthonormalise u2 against u1 (protects rank-deficient F)
+  double d = U[0] * U[1] + U[3] * U[4] + U[6] * U[7];
+  for (int r = 0; r < 3; r++) U[3 * r + 1] -= d * U[3 * r];
+  double n2 = std::sqrt(U[1] * U[1] + U[4] * U[4] + U[7] * U[7]);
+  if (n2 < 1e-300) {
+    // pick any unit vector orthogonal to u1
+    double ax = std::fabs(U[0]), ay = std::fabs(U[3]), az = std::fabs(U[6]);
+    double e[3] = {0, 0, 0};
+    e[(ax <= ay && ax <= az) ? 0 : (ay <= az ? 1 : 2)] = 1;
+    double dd = e[0] * U[0] + e[1] * U[3] + e[2] * U[6];
+    for (int r = 0; r < 3; r++) U[3 * r + 1] = e[r] - dd * U[3 * r];
+    n2 = std::sqrt(U[1] * U[1] + U[4] * U[4] + U[7] * U[7]);
+  }
+  for (int r = 0; r < 3; r++) U[3 * r + 1] /= n2;
+  double detV = det3(Vs) >= 0 ? 1.0 : -1.0;
+  U[2] = detV * (U[3] * U[7] - U[6] * U[4]);
+  U[5] = detV * (U[6] * U[1] - U[0] * U[7]);
+  U[8] = detV * (U[0] * U[4] - U[3] * U[1]);
+  // R = U Vs^T
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      R[3 * i + j] = U[3 * i] * Vs[3 * j] + U[3 * i + 1] * Vs[3 * j + 1] + U[3 * i + 2] * Vs[3 * j + 2];
+}
+
+// ---------------------------------------------------------------------------
+// element shape data
+// ---------------------------------------------------------------------------
+
+// TetElement.getdNds (TetElement.java:204-215), one integration point at
+// (1/4,1/4,1/4) with weight 1/6 (TetElement.java:31-33).
+static const double TET_GNS[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+static const double TET_W = 1.0 / 6.0;
+
+// HexElement node coordinates (HexElement.java:119-129)
+static const double HEX_NODE[8][3] = {{-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1},
+                                      {-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}};
+
+// HexElement.getdNds (HexElement.java:266-281)
+static void hex_dNds(double* out, int i, double s0, double s1, double s2) {
+  double g0 = HEX_NODE[i][0] < 0 ? -1 : 1, g1 = HEX_NODE[i][1] < 0 ? -1 : 1,
+         g2 = HEX_NODE[i][2] < 0 ? -1 : 1;
+  out[0] = 0.125 * (g0) * (1 + g1 * s1) * (1 + g2 * s2);
+  out[1] = 0.125 * (1 + g0 * s0) * (g1) * (1 + g2 * s2);
+  out[2] = 0.125 * (1 + g0 * s0) * (1 + g1 * s1) * (g2);
+}
+
+struct ShapeTable {
+  int nen, nip;
+  std::vector<double> GNs;  // nip * nen * 3
+  std::vector<double> w;    // nip
+  std::vector<double> wGNs; // warping point: nen * 3
+  double ww;
+};
+
+static ShapeTable make_shape(int type) {
+  ShapeTable s;
+  if (type == ELEM_TET) {
+    s.nen = 4; s.nip = 1;
+    s.GNs.assign(&TET_GNS[0][0], &TET_GNS[0][0] + 12);
+    s.w = {TET_W};
+    s.wGNs = s.GNs;  // TetElement.getWarpingPoint == integration point 0
+    s.ww = TET_W;
+  } else {
+    s.nen = 8; s.nip = 8;
+    // INTEGRATION_COORDS_GAUSS_8 (HexElement.java:159-170)
+    double q = 1 / std::sqrt(3.0);
+    s.GNs.resize(8 * 8 * 3);
+    s.w.assign(8, 1.0);
+    for (int k = 0; k < 8; k++) {
+      double c0 = HEX_NODE[k][0] * q, c1 = HEX_NODE[k][1] * q, c2 = HEX_NODE[k][2] * q;
+      for (int i = 0; i < 8; i++) hex_dNds(&s.GNs[(k * 8 + i) * 3], i, c0, c1, c2);
+    }
+    // warping point at the centre with weight 8 (HexElement.java:84-90)
+    s.wGNs.resize(24);
+    for (int i = 0; i < 8; i++) hex_dNds(&s.wGNs[i * 3], i, 0, 0, 0);
+    s.ww = 8;
+  }
+  return s;
+}
+
+// IntegrationPoint3d.computeJacobian (IntegrationPoint3d.java:190-201):
+// J += pos (outer) dNds
+static void compute_jacobian(double* J, const double* GNs, int nen, const double* xyz,
+                             const int* nodes) {
+  for (int i = 0; i < 9; i++) J[i] = 0;
+  for (int n = 0; n < nen; n++) {
+    const double* p = xyz + 3 * nodes[n];
+    const double* g = GNs + 3 * n;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) J[3 * r + c] += p[r] * g[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// materials
+// ---------------------------------------------------------------------------
+
+struct Material {
+  int kind = MAT_LINEAR;
+  double E = 0, nu = 0;
+  int corotated = 1;
+  double c10 = 0, c01 = 0, c11 = 0, c20 = 0, c02 = 0, kappa = 0, jlimit = 0;
+  int bulk_potential = 0;  // 0 QUADRATIC, 1 LOGARITHMIC
+  bool incompressible() const { return kind == MAT_MOONEYRIVLIN; }
+  bool linear() const { return kind == MAT_LINEAR; }
+};
+
+// D is a 6x6 row-major Voigt matrix, order (xx, yy, zz, xy, yz, xz);
+// sigma is (s00, s11, s22, s01, s12, s02).
+
+// LinearMaterial.getC (LinearMaterial.java:148-159)
+static void linear_C(double* D, double E, double nu) {
+  double a = E / (1 + nu);
+  double dia = (1 - nu) / (1 - 2 * nu) * a;
+  double mu = 0.5 * a;
+  double off = nu / (1 - 2 * nu) * a;
+  for (int i = 0; i < 36; i++) D[i] = 0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D[6 * i + j] = (i == j) ? dia : off;
+  D[21] = mu; D[28] = mu; D[35] = mu;
+}
+
+// TensorUtils.addScaledIdentityProduct (TensorUtils.java:474-486)
+static void add_scaled_identity_product(double* D, double s) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D[6 * i + j] += s;
+}
+// TensorUtils.addScaledIdentity (TensorUtils.java:496-507)
+static void add_scaled_identity(double* D, double s) {
+  D[0] += s; D[7] += s; D[14] += s;
+  D[21] += 0.5 * s; D[28] += 0.5 * s; D[35] += 0.5 * s;
+}
+// Matrix6d.setLowerToUpper (Matrix6d.java:532-538): lower := upper
+static void set_lower_to_upper(double* D) {
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < i; j++) D[6 * i + j] = D[6 * j + i];
+}
+// sym 3x3 stored as (00,11,22,01,12,02) -> accessor
+static inline void sym_from6(double* m, const double* s) {
+  m[0] = s[0]; m[4] = s[1]; m[8] = s[2];
+  m[1] = m[3] = s[3]; m[5] = m[7] = s[4]; m[2] = m[6] = s[5];
+}
+// TensorUtils.addSymmetricTensorProduct(D, s, A, B) (TensorUtils.java:220-268):
+// upper part only
+static void add_sym_tensor_product(double* D, double s, const double* A6, const double* B6) {
+  double a00 = s * A6[0], a11 = s * A6[1], a22 = s * A6[2], a01 = s * A6[3], a12 = s * A6[4], a02 = s * A6[5];
+  double b00 = B6[0], b11 = B6[1], b22 = B6[2], b01 = B6[3], b12 = B6[4], b02 = B6[5];
+  D[0] += 2 * a00 * b00; D[1] += a00 * b11 + b00 * a11; D[2] += a00 * b22 + b00 * a22;
+  D[3] += a00 * b01 + b00 * a01; D[4] += a00 * b12 + b00 * a12; D[5] += a00 * b02 + b00 * a02;
+  D[7] += 2 * a11 * b11; D[8] += a11 * b22 + b11 * a22; D[9] += a11 * b01 + b11 * a01;
+  D[10] += a11 * b12 + b11 * a12; D[11] += a11 * b02 + b11 * a02;
+  D[14] += 2 * a22 * b22; D[15] += a22 * b01 + b22 * a01; D[16] += a22 * b12 + b22 * a12;
+  D[17] += a22 * b02 + b22 * a02;
+  D[21] += 2 * a01 * b01; D[22] += a01 * b12 + b01 * a12; D[23] += a01 * b02 + b01 * a02;
+  D[28] += 2 * a12 * b12; D[29] += a12 * b02 + b12 * a02;
+  D[35] += 2 * a02 * b02;
+}
+// TensorUtils.addTensorProduct(D, s, A) (TensorUtils.java:340-380): upper part
+static void add_tensor_product(double* D, double s, const double* A6) {
+  double a[6] = {A6[0], A6[1], A6[2], A6[3], A6[4], A6[5]};
+  for (int i = 0; i < 6; i++)
+    for (int j = i; j < 6; j++) D[6 * i + j] += (s * a[i]) * a[j];
+}
+// TensorUtils.addTensorProduct4 (TensorUtils.java:608-645): upper part
+static void add_tensor_product4(double* D, double s, const double* A6) {
+  double a00 = A6[0], a11 = A6[1], a22 = A6[2], a01 = A6[3], a12 = A6[4], a02 = A6[5];
+  double s00 = s * a00, s11 = s * a11, s22 = s * a22, s01 = s * a01, s02 = s * a02, s12 = s * a12;
+  D[0] += s00 * a00; D[1] += s01 * a01; D[2] += s02 * a02; D[3] += s00 * a01;
+  D[4] += s01 * a02; D[5] += s00 * a02;
+  D[7] += s11 * a11; D[8] += s12 * a12; D[9] += s01 * a11; D[10] += s11 * a12; D[11] += s01 * a12;
+  D[14] += s22 * a22; D[15] += s02 * a12; D[16] += s12 * a22; D[17] += s02 * a22;
+  D[21] += (s00 * a11 + s01 * a01) * 0.5; D[22] += (s01 * a12 + s02 * a11) * 0.5;
+  D[23] += (s00 * a12 + s02 * a01) * 0.5;
+  D[28] += (s11 * a22 + s12 * a12) * 0.5; D[29] += (s01 * a22 + s02 * a12) * 0.5;
+  D[35] += (s00 * a22 + s02 * a02) * 0.5;
+}
+
+// B = F F^T as (00,11,22,01,12,02)  (FemMaterial.computeLeftCauchyGreen,
+// FemMaterial.java:199-202)
+static void left_cauchy_green(double* B6, const double* F) {
+  double B[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      B[3 * i + j] = F[3 * i] * F[3 * j] + F[3 * i + 1] * F[3 * j + 1] + F[3 * i + 2] * F[3 * j + 2];
+  B6[0] = B[0]; B6[1] = B[4]; B6[2] = B[8]; B6[3] = B[1]; B6[4] = B[5]; B6[5] = B[2];
+}
+
+// NeoHookeanMaterial.computeStressAndTangent (NeoHookeanMaterial.java:113-139)
+static void neohookean(double* sig, double* D, const Material& m, const double* F, double J) {
+  double E = m.E, nu = m.nu;
+  double G = E / (2 * (1 + nu));
+  double lam = (E * nu) / ((1 - 2 * nu) * (1 + nu));
+  double mu = G;
+  double B6[6];
+  left_cauchy_green(B6, F);
+  for (int i = 0; i < 6; i++) sig[i] = (mu / J) * B6[i];
+  double diagTerm = (lam * std::log(J) - mu) / J;
+  sig[0] += diagTerm; sig[1] += diagTerm; sig[2] += diagTerm;
+  if (D) {
+    for (int i = 0; i < 36; i++) D[i] = 0;
+    add_scaled_identity_product(D, lam / J);
+    add_scaled_identity(D, 2 * (mu - lam * std::log(J)) / J);
+    set_lower_to_upper(D);
+  }
+}
+
+// MooneyRivlinMaterial.computePhiVals (MooneyRivlinMaterial.java:314-331)
+static void mr_phi(double* vals, const Material& m, double J) {
+  if (m.jlimit > 0 && J < m.jlimit) {
+    double phi0 = 1 / std::pow(m.jlimit, 2.0 / 3.0);
+    double dphi0 = -(2.0 / 3.0) * phi0 / m.jlimit;
+    double ddphi0 = -(5.0 / 3.0) * dphi0 / m.jlimit;
+    double delJ = J - m.jlimit;
+    vals[0] = (0.5 * ddphi0 * delJ + dphi0) * delJ + phi0;
+    vals[1] = ddphi0 * delJ + dphi0;
+    vals[2] = ddphi0;
+  } else {
+    double phi = 1 / std::pow(J, 2.0 / 3.0);
+    double dphi = -(2.0 / 3.0) * phi / J;
+    vals[0] = phi;
+    vals[1] = dphi;
+    vals[2] = -(5.0 / 3.0) * dphi / J;
+  }
+}
+
+// MooneyRivlinMaterial.computeDevStressAndTangent (MooneyRivlinMaterial.java:344-431)
+// followed by IncompressibleMaterialBase.computeStressAndTangent
+// (IncompressibleMaterialBase.java:249-260): add pressure stress/tangent.
+static void mooneyrivlin(double* sig, double* D, const Material& m, const double* F, double J,
+                         double p) {
+  double pv[3];
+  mr_phi(pv, m, J);
+  double phi = pv[0], dphi = pv[1];
+  double B6[6], B[9], B2[9], B26[6];
+  left_cauchy_green(B6, F);
+  for (int i = 0; i < 6; i++) B6[i] *= phi;
+  sym_from6(B, B6);
+  mul3(B2, B, B);  // myB2.mulTransposeLeft(myB) = B^T B = B B
+  B26[0] = B2[0]; B26[1] = B2[4]; B26[2] = B2[8]; B26[3] = B2[1]; B26[4] = B2[5]; B26[5] = B2[2];
+  double c10 = m.c10, c01 = m.c01, c11 = m.c11, c20 = m.c20, c02 = m.c02;
+  double I1 = B6[0] + B6[1] + B6[2];
+  double I2 = 0.5 * (I1 * I1 - (B26[0] + B26[1] + B26[2]));
+  double W1 = c10 + c11 * (I2 - 3) + c20 * 2 * (I1 - 3);
+  double W2 = c01 + c11 * (I1 - 3) + c02 * 2 * (I2 - 3);
+  for (int i = 0; i < 6; i++) sig[i] = (W1 + W2 * I1) * B6[i];
+  for (int i = 0; i < 6; i++) sig[i] += -W2 * B26[i];
+  double dev = (dphi / phi) * (sig[0] + sig[1] + sig[2]);
+  for (int i = 0; i < 6; i++) sig[i] *= 2.0 / J;
+  sig[0] += dev; sig[1] += dev; sig[2] += dev;
+  if (D) {
+    double Ji = 1.0 / J;
+    double ddphi = pv[2];
+    double W11 = 2 * c20, W12 = c11, W22 = 2 * c02;
+    double w1 = -W2;
+    double w2 = W11 + 2 * W12 * I1 + W2 + W22 * I2 * I2;
+    double w3 = W12 + W22 * I1;
+    double w4 = W22;
+    double wc1 = (w2 - W12 + W22 * I1) * I1;
+    double wc2 = -(W12 + W22 * I1 - W22 * I1 * I1 + 2 * W22 * I2 + W2);
+    double wcc = wc1 * I1 + wc2 * (I1 * I1 - 2 * I2);
+    double w0 = W1 * I1 + 2 * W2 * I2;
+    for (int i = 0; i < 36; i++) D[i] = 0;
+    double zeta = ((dphi + J * ddphi) * w0 + J * dphi * dphi / phi * (wcc - 2 * w0)) / phi;
+    double r = dphi / phi;
+    add_scaled_identity_product(D, zeta);
+    add_scaled_identity(D, -2 * r * w0);
+    static const double I6[6] = {1, 1, 1, 0, 0, 0};
+    add_sym_tensor_product(D, J * r, sig, I6);
+    add_tensor_product4(D, w1 * 4.0 * Ji, B6);
+    add_tensor_product(D, w2 * 4.0 * Ji, B6);
+    add_sym_tensor_product(D, w3 * 4.0 * Ji, B6, B26);
+    add_tensor_product(D, w4 * 4.0 * Ji, B26);
+    double T6[6];
+    for (int i = 0; i < 6; i++) T6[i] = wc1 * B6[i] + wc2 * B26[i];
+    add_sym_tensor_product(D, 2 * r, T6, I6);
+    set_lower_to_upper(D);
+    // IncompressibleMaterialBase.addPressureTangent (:218-224)
+    add_scaled_identity_product(D, p);
+    add_scaled_identity(D, -2 * p);
+  }
+  // IncompressibleMaterialBase.addPressureStress (:209-213)
+  sig[0] += p; sig[1] += p; sig[2] += p;
+}
+
+static void material_stress_tangent(double* sig, double* D, const Material& m, const double* F,
+                                    double J, double p) {
+  if (m.kind == MAT_NEOHOOKEAN) neohookean(sig, D, m, F, J);
+  else if (m.kind == MAT_MOONEYRIVLIN) mooneyrivlin(sig, D, m, F, J, p);
+  else {
+    // linear small-strain (non-corotated) stress, used only by point tests:
+    // LinearMaterialBase.computeStressAndTangent with R = null, corotated off
+    double eps[6] = {F[0] - 1, F[4] - 1, F[8] - 1, 0.5 * (F[1] + F[3]), 0.5 * (F[5] + F[7]),
+                     0.5 * (F[2] + F[6])};
+    double lam = m.E * m.nu / ((1 + m.nu) * (1 - 2 * m.nu));
+    double mu = m.E / (2 * (1 + m.nu));
+    double tr = lam * (eps[0] + eps[1] + eps[2]);
+    sig[0] = 2 * mu * eps[0] + tr; sig[1] = 2 * mu * eps[1] + tr; sig[2] = 2 * mu * eps[2] + tr;
+    sig[3] = 2 * mu * eps[3]; sig[4] = 2 * mu * eps[4]; sig[5] = 2 * mu * eps[5];
+    if (D) linear_C(D, m.E, m.nu);
+  }
+}
+
+// FemUtilities.addStressForce (FemUtilities.java:40-49)
+static inline void add_stress_force(double* f, const double* g, const double* s, double dv) {
+  double gx = g[0] * dv, gy = g[1] * dv, gz = g[2] * dv;
+  f[0] += gx * s[0] + gy * s[3] + gz * s[5];
+  f[1] += gy * s[1] + gx * s[3] + gz * s[4];
+  f[2] += gz * s[2] + gy * s[4] + gx * s[5];
+}
+
+// FemUtilities.addMaterialStiffness(K, gi, D, gj, dv) (FemUtilities.java:78-129)
+static void add_material_stiffness(double* K, const double* gi, const double* D, const double* gj,
+                                   double dv) {
+  double gjx = gj[0] * dv, gjy = gj[1] * dv, gjz = gj[2] * dv;
+#define DM(r, c) D[6 * (r) + (c)]
+  double dm[6][3];
+  for (int r = 0; r < 6; r++) {
+    dm[r][0] = DM(r, 0) * gjx + DM(r, 3) * gjy + DM(r, 5) * gjz;
+    dm[r][1] = DM(r, 1) * gjy + DM(r, 3) * gjx + DM(r, 4) * gjz;
+    dm[r][2] = DM(r, 2) * gjz + DM(r, 4) * gjy + DM(r, 5) * gjx;
+  }
+#undef DM
+  double gix = gi[0], giy = gi[1], giz = gi[2];
+  for (int c = 0; c < 3; c++) {
+    K[c] += gix * dm[0][c] + giy * dm[3][c] + giz * dm[5][c];
+    K[3 + c] += giy * dm[1][c] + gix * dm[3][c] + giz * dm[4][c];
+    K[6 + c] += giz * dm[2][c] + giy * dm[4][c] + gix * dm[5][c];
+  }
+}
+
+// FemUtilities.addGeometricStiffness (FemUtilities.java:131-144)
+static void add_geometric_stiffness(double* K, const double* gi, const double* s, const double* gj,
+                                    double dv) {
+  double Kg = gi[0] * (s[0] * gj[0] + s[3] * gj[1] + s[5] * gj[2]) +
+              gi[1] * (s[3] * gj[0] + s[1] * gj[1] + s[4] * gj[2]) +
+              gi[2] * (s[5] * gj[0] + s[4] * gj[1] + s[2] * gj[2]);
+  Kg = Kg * dv;
+  K[0] += Kg; K[4] += Kg; K[8] += Kg;
+}
+
+// ---------------------------------------------------------------------------
+// model
+// ---------------------------------------------------------------------------
+
+struct Model {
+  int type = ELEM_TET, N = 0, E = 0, nen = 4;
+  ShapeTable sh;
+  std::vector<double> rest;
+  std::vector<int> conn;
+  std::vector<int> sidx;  // solve index (block row) per node, -1 when fixed
+  int nact = 0;
+  Material mat;
+  double density = 1000;
+  int incomp = INCOMP_OFF;  // resolved method
+  // rest data
+  std::vector<double> invJ0, detJ0;  // per element per IP
+  std::vector<double> winvJ0;        // warping-point invJ0 per element
+  std::vector<double> restVol;       // per element
+  std::vector<double> mass;          // per node
+  std::vector<double> K0, f0;        // linear cache: E*nen*nen*9, E*nen*3
+  // node neighbours (direct: share an element), sorted by node index
+  std::vector<std::vector<int>> nbr;
+  std::vector<std::vector<int>> ind;  // indirect (NODAL 2-ring minus direct)
+  // BSR over active nodes
+  std::vector<int> rowptr, col;
+  // NODAL data
+  std::vector<double> nodeRestVol, nodeVol, nodePressure;
+  // results of the last update
+  std::vector<double> K;     // nnzb * 9
+  std::vector<double> fint;  // 3N
+  int numInverted = 0;
+  double minDetJ = 0;
+  std::string err;
+
+  int block_index(int bi, int bj) const {
+    auto b = col.begin() + rowptr[bi], e = col.begin() + rowptr[bi + 1];
+    auto it = std::lower_bound(b, e, bj);
+    if (it == e || *it != bj) return -1;
+    return (int)(it - col.begin());
+  }
+};
+
+static bool contains_sorted(const std::vector<int>& v, int x) {
+  return std::binary_search(v.begin(), v.end(), x);
+}
+
+static void build_rest_data(Model& m) {
+  const ShapeTable& s = m.sh;
+  m.invJ0.assign((size_t)m.E * s.nip * 9, 0);
+  m.detJ0.assign((size_t)m.E * s.nip, 0);
+  m.winvJ0.assign((size_t)m.E * 9, 0);
+  m.restVol.assign(m.E, 0);
+  for (int e = 0; e < m.E; e++) {
+    const int* nodes = &m.conn[(size_t)e * m.nen];
+    double J0[9];
+    double vol = 0;
+    for (int k = 0; k < s.nip; k++) {
+      compute_jacobian(J0, &s.GNs[k * m.nen * 3], m.nen, m.rest.data(), nodes);
+      // IntegrationData3d.setRestJacobian (IntegrationData3d.java:108-111)
+      double d = fast_invert(&m.invJ0[((size_t)e * s.nip + k) * 9], J0);
+      m.detJ0[(size_t)e * s.nip + k] = d;
+      vol += d * s.w[k];
+    }
+    if (m.type == ELEM_TET) {
+      // TetElement.computeRestVolumes (TetElement.java:247-254): signed
+      // volume of the rest tetrahedron
+      const double *p0 = &m.rest[3 * nodes[0]], *p1 = &m.rest[3 * nodes[1]],
+                   *p2 = &m.rest[3 * nodes[2]], *p3 = &m.rest[3 * nodes[3]];
+      double a[9] = {p1[0] - p0[0], p2[0] - p0[0], p3[0] - p0[0], p1[1] - p0[1], p2[1] - p0[1],
+                     p3[1] - p0[1], p1[2] - p0[2], p2[2] - p0[2], p3[2] - p0[2]};
+      vol = det3(a) / 6;
+      std::memcpy(&m.winvJ0[(size_t)e * 9], &m.invJ0[(size_t)e * 9], 9 * sizeof(double));
+    } else {
+      // FemElement3d.computeVolumes(rest) (FemElement3d.java:95-130)
+      compute_jacobian(J0, s.wGNs.data(), m.nen, m.rest.data(), nodes);
+      fast_invert(&m.winvJ0[(size_t)e * 9], J0);
+    }
+    m.restVol[e] = vol;
+  }
+  // lumped masses: FemNode3d.computeMassFromDensity (FemNode3d.java:1030-1045)
+  m.mass.assign(m.N, 0);
+  for (int e = 0; e < m.E; e++) {
+    double rm = m.restVol[e] * m.density;
+    for (int a = 0; a < m.nen; a++) m.mass[m.conn[(size_t)e * m.nen + a]] += rm / m.nen;
+  }
+}
+
+// LinearMaterialCache.addInitialStiffness (LinearMaterialCache.java:115-160)
+static void build_linear_cache(Model& m) {
+  const ShapeTable& s = m.sh;
+  int nen = m.nen;
+  m.K0.assign((size_t)m.E * nen * nen * 9, 0);
+  m.f0.assign((size_t)m.E * nen * 3, 0);
+  double C[36];
+  linear_C(C, m.mat.E, m.mat.nu);
+  for (int e = 0; e < m.E; e++) {
+    const int* nodes = &m.conn[(size_t)e * nen];
+    double* K0 = &m.K0[(size_t)e * nen * nen * 9];
+    for (int k = 0; k < s.nip; k++) {
+      const double* invJ0 = &m.invJ0[((size_t)e * s.nip + k) * 9];
+      double dv0 = m.detJ0[(size_t)e * s.nip + k] * 1.0 * s.w[k];
+      std::vector<double> GNx0(nen * 3);
+      for (int n = 0; n < nen; n++) {
+        const double* g = &s.GNs[(k * nen + n) * 3];
+        for (int c = 0; c < 3; c++)
+          GNx0[3 * n + c] = invJ0[c] * g[0] + invJ0[3 + c] * g[1] + invJ0[6 + c] * g[2];
+      }
+      for (int i = 0; i < nen; i++)
+        for (int j = 0; j < nen; j++)
+          add_material_stiffness(&K0[(i * nen + j) * 9], &GNx0[3 * i], C, &GNx0[3 * j], dv0);
+    }
+    for (int i = 0; i < nen; i++) {
+      double tmp[3] = {0, 0, 0};
+      for (int j = 0; j < nen; j++) {
+        const double* Kij = &K0[(i * nen + j) * 9];
+        const double* p = &m.rest[3 * nodes[j]];
+        for (int r = 0; r < 3; r++) tmp[r] += Kij[3 * r] * p[0] + Kij[3 * r + 1] * p[1] + Kij[3 * r + 2] * p[2];
+      }
+      for (int r = 0; r < 3; r++) m.f0[((size_t)e * nen + i) * 3 + r] = tmp[r];
+    }
+  }
+}
+
+static void build_pattern(Model& m) {
+  // FemNodeNeighbor lists: every pair of nodes sharing an element (self
+  // included); FemModel3d.addSolveBlocks (FemModel3d.java:4099-4112) makes a
+  // block for each pair with both solve indices != -1.
+  m.nbr.assign(m.N, {});
+  for (int e = 0; e < m.E; e++) {
+    const int* nodes = &m.conn[(size_t)e * m.nen];
+    for (int a = 0; a < m.nen; a++)
+      for (int b = 0; b < m.nen; b++) m.nbr[nodes[a]].push_back(nodes[b]);
+  }
+  for (auto& v : m.nbr) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  m.ind.assign(m.N, {});
+  if (m.incomp == INCOMP_NODAL) {
+    // FemModel3d.setNodalIncompBlocksAllocated (FemModel3d.java:5397-5416)
+    for (int n = 0; n < m.N; n++) {
+      const auto& nb = m.nbr[n];
+      for (int a : nb)
+        for (int b : nb)
+          if (!contains_sorted(m.nbr[a], b)) m.ind[a].push_back(b);
+    }
+    for (auto& v : m.ind) {
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+    }
+  }
+  m.rowptr.assign(m.nact + 1, 0);
+  std::vector<int> act_nodes(m.nact);
+  for (int n = 0; n < m.N; n++)
+    if (m.sidx[n] >= 0) act_nodes[m.sidx[n]] = n;
+  m.col.clear();
+  for (int bi = 0; bi < m.nact; bi++) {
+    int n = act_nodes[bi];
+    std::vector<int> cols;
+    for (int j : m.nbr[n])
+      if (m.sidx[j] >= 0) cols.push_back(m.sidx[j]);
+    for (int j : m.ind[n])
+      if (m.sidx[j] >= 0) cols.push_back(m.sidx[j]);
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    m.col.insert(m.col.end(), cols.begin(), cols.end());
+    m.rowptr[bi + 1] = (int)m.col.size();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FemModel3d.updateStressAndStiffness (FemModel3d.java:2894-3051) with
+// computeStressAndStiffness (:3333-3666) and the NODAL soft-incompressibility
+// terms (:2471-2515, :2594-2669).
+// ---------------------------------------------------------------------------
+
+struct ElemOut {
+  std::vector<double> f;     // nen*3
+  std::vector<double> K;     // nen*nen*9 (only (i,j) with bj >= bi valid)
+  std::vector<double> div;   // NODAL divBlk contributions: nen*nen*3, [i][j]
+  int inverted = 0;
+  double minDetJ = 1e300;
+};
+
+static void element_update(const Model& m, int e, const double* x, ElemOut& out) {
+  const ShapeTable& s = m.sh;
+  int nen = m.nen;
+  const int* nodes = &m.conn[(size_t)e * nen];
+  out.f.assign(nen * 3, 0);
+  out.K.assign(nen * nen * 9, 0);
+  out.div.assign(m.incomp == INCOMP_NODAL ? nen * nen * 3 : 0, 0);
+  out.inverted = 0;
+  out.minDetJ = 1e300;
+  if (m.mat.linear()) {
+    // linear cached path (FemModel3d.java:3359-3390)
+    const double* K0 = &m.K0[(size_t)e * nen * nen * 9];
+    const double* f0 = &m.f0[(size_t)e * nen * 3];
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (m.mat.corotated) {
+      // StiffnessWarper3d.computeWarpingRotation (StiffnessWarper3d.java:154-159)
+      double J[9], F[9];
+      compute_jacobian(J, s.wGNs.data(), nen, x, nodes);
+      mul3(F, J, &m.winvJ0[(size_t)e * 9]);
+      polar_rotation(R, F);
+    }
+    for (int i = 0; i < nen; i++) {
+      int bi = m.sidx[nodes[i]];
+      if (bi == -1) continue;
+      for (int j = 0; j < nen; j++) {
+        int bj = m.sidx[nodes[j]];
+        if (bj >= bi) {
+          const double* Kij = &K0[(i * nen + j) * 9];
+          double* Ko = &out.K[(i * nen + j) * 9];
+          if (m.mat.corotated) {
+            // StiffnessWarper3d.rotateStiffness: R K R^T (:219-222)
+            double T[9];
+            for (int a = 0; a < 3; a++)
+              for (int b = 0; b < 3; b++)
+                T[3 * a + b] = Kij[3 * a] * R[3 * b] + Kij[3 * a + 1] * R[3 * b + 1] + Kij[3 * a + 2] * R[3 * b + 2];
+            double U[9];
+            mul3(U, R, T);
+            for (int q = 0; q < 9; q++) Ko[q] += U[q];
+          } else {
+            for (int q = 0; q < 9; q++) Ko[q] += Kij[q];
+          }
+        }
+      }
+      // StiffnessWarper3d.addNodeForce (:278-307)
+      double tmp[3] = {0, 0, 0};
+      for (int j = 0; j < nen; j++) {
+        const double* p = &x[3 * nodes[j]];
+        double pos[3];
+        if (m.mat.corotated) {
+          for (int r = 0; r < 3; r++) pos[r] = R[r] * p[0] + R[3 + r] * p[1] + R[6 + r] * p[2];
+        } else {
+          pos[0] = p[0]; pos[1] = p[1]; pos[2] = p[2];
+        }
+        const double* Kij = &K0[(i * nen + j) * 9];
+        for (int r = 0; r < 3; r++) tmp[r] += Kij[3 * r] * pos[0] + Kij[3 * r + 1] * pos[1] + Kij[3 * r + 2] * pos[2];
+      }
+      for (int r = 0; r < 3; r++) tmp[r] -= f0[3 * i + r];
+      if (m.mat.corotated) {
+        double t2[3];
+        for (int r = 0; r < 3; r++) t2[r] = R[3 * r] * tmp[0] + R[3 * r + 1] * tmp[1] + R[3 * r + 2] * tmp[2];
+        for (int r = 0; r < 3; r++) out.f[3 * i + r] += t2[r];
+      } else {
+        for (int r = 0; r < 3; r++) out.f[3 * i + r] += tmp[r];
+      }
+    }
+    return;
+  }
+  // non-linear path (FemModel3d.java:3443-3631)
+  std::vector<double> GNx(nen * 3);
+  for (int k = 0; k < s.nip; k++) {
+    const double* GNs = &s.GNs[k * nen * 3];
+    double J[9], invJ[9], F[9];
+    compute_jacobian(J, GNs, nen, x, nodes);
+    mul3(F, J, &m.invJ0[((size_t)e * s.nip + k) * 9]);
+    double detF = det3(F);
+    double detJ = fast_invert(invJ, J);
+    out.minDetJ = std::min(out.minDetJ, detJ);
+    if (detJ <= 0) out.inverted = 1;
+    double dv = detJ * s.w[k];
+    for (int n = 0; n < nen; n++) {
+      const double* g = GNs + 3 * n;
+      for (int c = 0; c < 3; c++)
+        GNx[3 * n + c] = invJ[c] * g[0] + invJ[3 + c] * g[1] + invJ[6 + c] * g[2];
+    }
+    double pressure = 0;
+    if (m.incomp == INCOMP_NODAL) {
+      if (m.type == ELEM_TET) {
+        for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
+        pressure /= nen;
+      } else {
+        pressure = m.nodePressure[nodes[k]];
+      }
+    }
+    double sig[6], D[36];
+    material_stress_tangent(sig, D, m.mat, F, detF, pressure);
+    for (int i = 0; i < nen; i++) {
+      add_stress_force(&out.f[3 * i], &GNx[3 * i], sig, dv);
+      int bi = m.sidx[nodes[i]];
+      if (bi != -1) {
+        for (int j = 0; j < nen; j++) {
+          int bj = m.sidx[nodes[j]];
+          if (bj >= bi) {
+            double* Ko = &out.K[(i * nen + j) * 9];
+            add_material_stiffness(Ko, &GNx[3 * i], D, &GNx[3 * j], dv);
+            add_geometric_stiffness(Ko, &GNx[3 * i], sig, &GNx[3 * j], dv);
+            // FemNodeNeighbor.addPressureStiffness is a no-op unless
+            // noIncompressStiffnessDamping (FemNodeNeighbor.java:541-551)
+          }
+        }
+      }
+    }
+    if (m.incomp == INCOMP_NODAL && m.type != ELEM_TET) {
+      // integration points map to nodes (FemModel3d.java:3604-3614):
+      // divBlk(node_k, node_j) += dv * GNx_j
+      for (int j = 0; j < nen; j++)
+        for (int c = 0; c < 3; c++) out.div[(k * nen + j) * 3 + c] += dv * GNx[3 * j + c];
+    }
+  }
+  if (m.incomp == INCOMP_NODAL && m.type == ELEM_TET) {
+    // TetElement.getAreaWeightedNormals (TetElement.java:333-362) * (-1/12)
+    const double *p0 = &x[3 * nodes[0]], *p1 = &x[3 * nodes[1]], *p2 = &x[3 * nodes[2]],
+                 *p3 = &x[3 * nodes[3]];
+    const double* tri[4][3] = {{p1, p2, p3}, {p0, p3, p2}, {p0, p1, p3}, {p0, p2, p1}};
+    double c[4][3];
+    for (int a = 0; a < 4; a++) {
+      const double *q0 = tri[a][0], *q1 = tri[a][1], *q2 = tri[a][2];
+      double ux = q1[0] - q0[0], uy = q1[1] - q0[1], uz = q1[2] - q0[2];
+      double vx = q2[0] - q0[0], vy = q2[1] - q0[1], vz = q2[2] - q0[2];
+      c[a][0] = 0.5 * (uy * vz - uz * vy) * (-1 / 12.0);
+      c[a][1] = 0.5 * (uz * vx - ux * vz) * (-1 / 12.0);
+      c[a][2] = 0.5 * (ux * vy - uy * vx) * (-1 / 12.0);
+    }
+    // divBlk(node_i, node_j) += c_j for every element node i (:3632-3643)
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++)
+        for (int q = 0; q < 3; q++) out.div[(i * 4 + j) * 3 + q] += c[j][q];
+  }
+}
+
+static double current_volume(const Model& m, int e, const double* x) {
+  const int* nodes = &m.conn[(size_t)e * m.nen];
+  if (m.type == ELEM_TET) {
+    const double *p0 = &x[3 * nodes[0]], *p1 = &x[3 * nodes[1]], *p2 = &x[3 * nodes[2]],
+                 *p3 = &x[3 * nodes[3]];
+    double a[9] = {p1[0] - p0[0], p2[0] - p0[0], p3[0] - p0[0], p1[1] - p0[1], p2[1] - p0[1],
+                   p3[1] - p0[1], p1[2] - p0[2], p2[2] - p0[2], p3[2] - p0[2]};
+    return det3(a) / 6;
+  }
+  double vol = 0, J[9];
+  for (int k = 0; k < m.sh.nip; k++) {
+    compute_jacobian(J, &m.sh.GNs[k * m.nen * 3], m.nen, x, nodes);
+    vol += det3(J) * m.sh.w[k];
+  }
+  return vol;
+}
+
+static int update_stress_stiffness(Model& m, const double* x) {
+  int nen = m.nen;
+  size_t nnzb = m.col.size();
+  m.K.assign(nnzb * 9, 0);
+  m.fint.assign((size_t)3 * m.N, 0);
+  bool nodal = (m.incomp == INCOMP_NODAL);
+  if (nodal) {
+    // updateNodalRestVolumes (FemModel3d.java:2594-2628) -- rest volumes are
+    // constant; computed once in orc_create.
+    // updateNodalPressures (FemModel3d.java:2471-2515)
+    m.nodeVol.assign(m.N, 0);
+    for (int e = 0; e < m.E; e++) {
+      const int* nodes = &m.conn[(size_t)e * nen];
+      if (m.type == ELEM_TET) {
+        double vol = current_volume(m, e, x);
+        for (int i = 0; i < nen; i++) m.nodeVol[nodes[i]] += vol / 4;
+      } else {
+        double J[9];
+        for (int k = 0; k < m.sh.nip; k++) {
+          compute_jacobian(J, &m.sh.GNs[k * nen * 3], nen, x, nodes);
+          m.nodeVol[nodes[k]] += det3(J) * m.sh.w[k];
+        }
+      }
+    }
+    m.nodePressure.assign(m.N, 0);
+    for (int n = 0; n < m.N; n++) {
+      if (m.sidx[n] >= 0) {
+        double Jn = m.nodeVol[n] / m.nodeRestVol[n];
+        double K = m.mat.kappa;
+        m.nodePressure[n] = (m.mat.bulk_potential == 0) ? K * (Jn - 1) : K * std::log(Jn) / Jn;
+      }
+    }
+  }
+  std::vector<ElemOut> outs(m.E);
+#pragma omp parallel for schedule(static)
+  for (int e = 0; e < m.E; e++) element_update(m, e, x, outs[e]);
+
+  m.numInverted = 0;
+  m.minDetJ = 1e300;
+  // divBlk storage: per node n, one 3-vector per direct neighbour (sorted)
+  std::vector<std::vector<double>> div;
+  if (nodal) {
+    div.resize(m.N);
+    for (int n = 0; n < m.N; n++) div[n].assign(m.nbr[n].size() * 3, 0);
+  }
+  for (int e = 0; e < m.E; e++) {
+    const ElemOut& o = outs[e];
+    const int* nodes = &m.conn[(size_t)e * nen];
+    m.numInverted += o.inverted;
+    m.minDetJ = std::min(m.minDetJ, o.minDetJ);
+    for (int i = 0; i < nen; i++) {
+      for (int r = 0; r < 3; r++) m.fint[3 * nodes[i] + r] += o.f[3 * i + r];
+      int bi = m.sidx[nodes[i]];
+      if (bi == -1) continue;
+      for (int j = 0; j < nen; j++) {
+        int bj = m.sidx[nodes[j]];
+        if (bj >= bi) {
+          int b = m.block_index(bi, bj);
+          for (int q = 0; q < 9; q++) m.K[(size_t)b * 9 + q] += o.K[(i * nen + j) * 9 + q];
+        }
+      }
+    }
+    if (nodal) {
+      for (int i = 0; i < nen; i++) {
+        int n = nodes[i];
+        for (int j = 0; j < nen; j++) {
+          auto it = std::lower_bound(m.nbr[n].begin(), m.nbr[n].end(), nodes[j]);
+          size_t idx = it - m.nbr[n].begin();
+          for (int q = 0; q < 3; q++) div[n][idx * 3 + q] += o.div[(i * nen + j) * 3 + q];
+        }
+      }
+    }
+  }
+  if (nodal) {
+    // computeNodalIncompressibility (FemModel3d.java:2632-2669)
+    for (int n = 0; n < m.N; n++) {
+      if (m.sidx[n] < 0) continue;
+      double restVol = m.nodeRestVol[n];
+      double Jn = m.nodeVol[n] / restVol;
+      double K = m.mat.kappa;
+      double keff = (m.mat.bulk_potential == 0) ? K : K * (1 - std::log(Jn)) / (Jn * Jn);
+      double kp = keff / restVol;
+      if (kp == 0) continue;
+      const auto& nb = m.nbr[n];
+      for (size_t a = 0; a < nb.size(); a++) {
+        int bi = m.sidx[nb[a]];
+        if (bi < 0) continue;
+        for (size_t c = 0; c < nb.size(); c++) {
+          int bj = m.sidx[nb[c]];
+          if (bj < bi) continue;
+          int b = m.block_index(bi, bj);
+          const double* gi = &div[n][a * 3];
+          const double* gj = &div[n][c * 3];
+          // FemUtilities.addDilationalStiffness: K += kp * gi gj^T
+          for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) m.K[(size_t)b * 9 + 3 * r + q] += kp * gi[r] * gj[q];
+        }
+      }
+    }
+  }
+  // symmetrise: lower block := transpose of upper (FemModel3d.java:3003-3026)
+  for (int bi = 0; bi < m.nact; bi++) {
+    for (int p = m.rowptr[bi]; p < m.rowptr[bi + 1]; p++) {
+      int bj = m.col[p];
+      if (bj >= bi) continue;
+      int bu = m.block_index(bj, bi);
+      for (int r = 0; r < 3; r++)
+        for (int q = 0; q < 3; q++) m.K[(size_t)p * 9 + 3 * r + q] = m.K[(size_t)bu * 9 + 3 * q + r];
+    }
+  }
+  return 0;
+}
+
+// y = K x over active blocks (x, y indexed by block row / solve index)
+static void bsr_mul(const Model& m, const std::vector<double>& vals, const double* x, double* y) {
+#pragma omp parallel for schedule(static)
+  for (int bi = 0; bi < m.nact; bi++) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int p = m.rowptr[bi]; p < m.rowptr[bi + 1]; p++) {
+      const double* B = &vals[(size_t)p * 9];
+      const double* v = &x[3 * m.col[p]];
+      a0 += B[0] * v[0] + B[1] * v[1] + B[2] * v[2];
+      a1 += B[3] * v[0] + B[4] * v[1] + B[5] * v[2];
+      a2 += B[6] * v[0] + B[7] * v[1] + B[8] * v[2];
+    }
+    y[3 * bi] = a0; y[3 * bi + 1] = a1; y[3 * bi + 2] = a2;
+  }
+}
+
+static double dot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0;
+  for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+  return s;
+}
+
+// Jacobi-preconditioned CG to a relative residual ||b - A x|| / ||b|| <= tol
+// (CGSolver.solve, CGSolver.java:42-134, with a diagonal preconditioner).
+static int cg_solve(const Model& m, const std::vector<double>& S, const std::vector<double>& b,
+                    std::vector<double>& x, double tol, int maxit, int* iters, double* relres) {
+  size_t n = b.size();
+  std::vector<double> r(n), z(n), p(n), q(n), dinv(n);
+  for (int bi = 0; bi < m.nact; bi++) {
+    int d = m.block_index(bi, bi);
+    for (int c = 0; c < 3; c++) dinv[3 * bi + c] = 1.0 / S[(size_t)d * 9 + 4 * c];
+  }
+  bsr_mul(m, S, x.data(), q.data());
+  for (size_t i = 0; i < n; i++) r[i] = b[i] - q[i];
+  double bn = std::sqrt(dot(b, b));
+  if (bn == 0) bn = 1;
+  for (size_t i = 0; i < n; i++) z[i] = dinv[i] * r[i];
+  p = z;
+  double rho = dot(r, z);
+  int it = 0;
+  double rr = std::sqrt(dot(r, r));
+  while (rr / bn > tol && it < maxit) {
+    bsr_mul(m, S, p.data(), q.data());
+    double alpha = rho / dot(p, q);
+    for (size_t i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
+    for (size_t i = 0; i < n; i++) z[i] = dinv[i] * r[i];
+    double rho1 = dot(r, z);
+    double beta = rho1 / rho;
+    rho = rho1;
+    for (size_t i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+    rr = std::sqrt(dot(r, r));
+    it++;
+  }
+  if (iters) *iters = it;
+  if (relres) *relres = rr / bn;
+  return (rr / bn <= tol) ? 0 : 1;
+}
+
+// dense Cholesky for small systems (stands in for the reference's direct
+// PARDISO solve, MechSystemSolver.doDirectSolve, MechSystemSolver.java:2113)
+static int dense_solve(const Model& m, const std::vector<double>& S, const std::vector<double>& b,
+                       std::vector<double>& x) {
+  int n = 3 * m.nact;
+  std::vector<double> A((size_t)n * n, 0);
+  for (int bi = 0; bi < m.nact; bi++)
+    for (int p = m.rowptr[bi]; p < m.rowptr[bi + 1]; p++) {
+      int bj = m.col[p];
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[(size_t)(3 * bi + r) * n + 3 * bj + c] = S[(size_t)p * 9 + 3 * r + c];
+    }
+  for (int j = 0; j < n; j++) {
+    double d = A[(size_t)j * n + j];
+    for (int k = 0; k < j; k++) d -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
+    if (d <= 0) return 2;
+    d = std::sqrt(d);
+    A[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; i++) {
+      double s = A[(size_t)i * n + j];
+      for (int k = 0; k < j; k++) s -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
+      A[(size_t)i * n + j] = s / d;
+    }
+  }
+  x.assign(n, 0);
+  std::vector<double> y(n);
+  for (int i = 0; i < n; i++) {
+    double s = b[i];
+    for (int k = 0; k < i; k++) s -= A[(size_t)i * n + k] * y[k];
+    y[i] = s / A[(size_t)i * n + i];
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double s = y[i];
+    for (int k = i + 1; k < n; k++) s -= A[(size_t)k * n + i] * x[k];
+    x[i] = s / A[(size_t)i * n + i];
+  }
+  return 0;
+}
+
+static uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C API (ctypes)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int orc_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
+  *nnodes = (nx + 1) * (ny + 1) * (nz + 1);
+  *nelems = (type == ELEM_TET ? 5 : 1) * nx * ny * nz;
+}
+
+// FemFactory.createGridNodes (FemFactory.java:53-78), createTetGrid (:86-126)
+// with Tetrahedralizer.subdivideHex(..., allOnX) (Tetrahedralizer.java:135-141,
+// parseCode :203-263, getTetIndicesForHex :265-300), createHexGrid (:203-255).
+void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz,
+                     double* xyz, int* conn) {
+  double dx = 1.0 / nx, dy = 1.0 / ny, dz = 1.0 / nz;
+  int idx = 0;
+  for (int k = 0; k <= nz; k++)
+    for (int j = 0; j <= ny; j++)
+      for (int i = 0; i <= nx; i++) {
+        xyz[3 * idx] = wx * (-0.5 + i * dx);
+        xyz[3 * idx + 1] = wy * (-0.5 + j * dy);
+        xyz[3 * idx + 2] = wz * (-0.5 + k * dz);
+        idx++;
+      }
+  int wk = (nx + 1) * (ny + 1), wj = nx + 1;
+  static const int tetsA[5][4] = {{1, 0, 2, 5}, {3, 0, 7, 2}, {4, 0, 5, 7}, {6, 2, 7, 5}, {0, 2, 5, 7}};
+  static const int tetsB[5][4] = {{0, 1, 4, 3}, {2, 3, 6, 1}, {5, 4, 1, 6}, {7, 6, 3, 4}, {1, 6, 4, 3}};
+  int e = 0;
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        int h[8] = {(k + 1) * wk + j * wj + i,     (k + 1) * wk + j * wj + i + 1,
+                    (k + 1) * wk + (j + 1) * wj + i + 1, (k + 1) * wk + (j + 1) * wj + i,
+                    k * wk + j * wj + i,           k * wk + j * wj + i + 1,
+                    k * wk + (j + 1) * wj + i + 1, k * wk + (j + 1) * wj + i};
+        if (type == ELEM_HEX) {
+          for (int a = 0; a < 8; a++) conn[8 * e + a] = h[a];
+          e++;
+        } else {
+          bool allOnX = ((i + j + k) % 2) != 0;
+          const int(*t)[4] = allOnX ? tetsA : tetsB;
+          for (int q = 0; q < 5; q++) {
+            for (int a = 0; a < 4; a++) conn[4 * e + a] = h[t[q][a]];
+            e++;
+          }
+        }
+      }
+}
+
+// Seeded interior-node jitter: every node strictly inside the box moves by
+// (2u-1)*frac*spacing along each axis, u from splitmix64 in node order.
+void orc_jitter(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
+                uint64_t seed, double* xyz) {
+  uint64_t s = seed;
+  double sp[3] = {wx / nx, wy / ny, wz / nz};
+  int idx = 0;
+  for (int k = 0; k <= nz; k++)
+    for (int j = 0; j <= ny; j++)
+      for (int i = 0; i <= nx; i++, idx++) {
+        if (i == 0 || i == nx || j == 0 || j == ny || k == 0 || k == nz) continue;
+        for (int a = 0; a < 3; a++) {
+          double u = (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0);
+          xyz[3 * idx + a] += (2 * u - 1) * frac * sp[a];
+        }
+      }
+}
+
+// mat_params: LINEAR {E, nu, corotated}; NEOHOOKEAN {E, nu};
+// MOONEYRIVLIN {c10, c01, c11, c20, c02, kappa, jlimit, bulk_potential}
+void* orc_create(int type, int nnodes, const double* rest, int nelems, const int* conn,
+                 const int* fixed, int mat_kind, const double* mat_params, double density,
+                 int incomp_method) {
+  Model* m = new Model();
+  m->type = type;
+  m->sh = make_shape(type);
+  m->nen = m->sh.nen;
+  m->N = nnodes;
+  m->E = nelems;
+  m->rest.assign(rest, rest + 3 * (size_t)nnodes);
+  m->conn.assign(conn, conn + (size_t)nelems * m->nen);
+  m->sidx.assign(nnodes, -1);
+  m->nact = 0;
+  for (int n = 0; n < nnodes; n++)
+    if (!fixed[n]) m->sidx[n] = m->nact++;
+  m->mat.kind = mat_kind;
+  if (mat_kind == MAT_LINEAR) {
+    m->mat.E = mat_params[0]; m->mat.nu = mat_params[1]; m->mat.corotated = (int)mat_params[2];
+  } else if (mat_kind == MAT_NEOHOOKEAN) {
+    m->mat.E = mat_params[0]; m->mat.nu = mat_params[1];
+  } else {
+    m->mat.c10 = mat_params[0]; m->mat.c01 = mat_params[1]; m->mat.c11 = mat_params[2];
+    m->mat.c20 = mat_params[3]; m->mat.c02 = mat_params[4]; m->mat.kappa = mat_params[5];
+    m->mat.jlimit = mat_params[6]; m->mat.bulk_potential = (int)mat_params[7];
+  }
+  m->density = density;
+  // FemModel3d.computeStressAndStiffness forces OFF for compressible
+  // materials (:3346-3348); AUTO -> NODAL when #elements > #active nodes
+  // (getAllowedSoftIncompMethod, :462-481).
+  int method = incomp_method;
+  if (!m->mat.incompressible()) method = INCOMP_OFF;
+  else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
+  m->incomp = method;
+  build_rest_data(*m);
+  if (m->mat.linear()) build_linear_cache(*m);
+  build_pattern(*m);
+  if (m->incomp == INCOMP_NODAL) {
+    m->nodeRestVol.assign(m->N, 0);
+    for (int e = 0; e < m->E; e++) {
+      const int* nodes = &m->conn[(size_t)e * m->nen];
+      if (type == ELEM_TET) {
+        for (int i = 0; i < 4; i++) m->nodeRestVol[nodes[i]] += m->restVol[e] / 4;
+      } else {
+        for (int i = 0; i < 8; i++)
+          m->nodeRestVol[nodes[i]] += m->sh.w[i] * m->detJ0[(size_t)e * 8 + i];
+      }
+    }
+  }
+  return m;
+}
+
+void orc_destroy(void* h) { delete (Model*)h; }
+int orc_incomp_method(void* h) { return ((Model*)h)->incomp; }
+int orc_num_active(void* h) { return ((Model*)h)->nact; }
+int orc_nnzb(void* h) { return (int)((Model*)h)->col.size(); }
+void orc_solve_index(void* h, int* out) {
+  Model* m = (Model*)h;
+  std::copy(m->sidx.begin(), m->sidx.end(), out);
+}
+void orc_pattern(void* h, int* rowptr, int* col) {
+  Model* m = (Model*)h;
+  std::copy(m->rowptr.begin(), m->rowptr.end(), rowptr);
+  std::copy(m->col.begin(), m->col.end(), col);
+}
+void orc_masses(void* h, double* mass) {
+  Model* m = (Model*)h;
+  std::copy(m->mass.begin(), m->mass.end(), mass);
+}
+void orc_rest_volumes(void* h, double* vol) {
+  Model* m = (Model*)h;
+  std::copy(m->restVol.begin(), m->restVol.end(), vol);
+}
+
+// Scalar CRS view of the block pattern (SparseBlockMatrix.getCRSIndices,
+// SparseBlockMatrix.java:1511-1532, made 0-based as in
+// SparseNumberedBlockMatrix.createCrsBlockSlotMap :396-398).
+// partition 0 = Full, 1 = UpperTriangular.  Returns nnz.
+int orc_crs(void* h, int partition, int* row_offs, int* col_idx, int* slots) {
+  Model* m = (Model*)h;
+  int nnz = 0;
+  int nrows = 3 * m->nact;
+  std::vector<int> slot((size_t)m->col.size() * 9, -1);
+  for (int bi = 0; bi < m->nact; bi++) {
+    for (int r = 0; r < 3; r++) {
+      int row = 3 * bi + r;
+      if (row_offs) row_offs[row] = nnz;
+      for (int p = m->rowptr[bi]; p < m->rowptr[bi + 1]; p++) {
+        int bj = m->col[p];
+        for (int c = 0; c < 3; c++) {
+          int colg = 3 * bj + c;
+          if (partition == 1 && colg < row) continue;
+          if (col_idx) col_idx[nnz] = colg;
+          slot[(size_t)p * 9 + 3 * r + c] = nnz;
+          nnz++;
+        }
+      }
+    }
+  }
+  if (row_offs) row_offs[nrows] = nnz;
+  if (slots) std::copy(slot.begin(), slot.end(), slots);
+  return nnz;
+}
+
+// FemModel3d.updateStressAndStiffness at positions x (3N): returns the
+// internal force per node (3N) and the assembled stiffness blocks (9*nnzb,
+// BSR order, both triangles).  Returns the number of inverted elements.
+int orc_update_stress_stiffness(void* h, const double* x, double* fint, double* K) {
+  Model* m = (Model*)h;
+  update_stress_stiffness(*m, x);
+  if (fint) std::copy(m->fint.begin(), m->fint.end(), fint);
+  if (K) std::copy(m->K.begin(), m->K.end(), K);
+  return m->numInverted;
+}
+
+void orc_nodal_pressures(void* h, double* p) {
+  Model* m = (Model*)h;
+  if (m->nodePressure.empty()) std::fill(p, p + m->N, 0.0);
+  else std::copy(m->nodePressure.begin(), m->nodePressure.end(), p);
+}
+
+// One MechSystemSolver.backwardEuler step (MechSystemSolver.java:2171-2476).
+// prm = {alpha_m (massDamping), beta_k (stiffnessDamping), gx, gy, gz}.
+// fext: 3N external nodal forces (may be null).  x, v (3N) updated in place.
+// solver 0 = Jacobi-PCG to tol, 1 = dense Cholesky.
+// Returns 0, or 1 when CG did not converge, 2 when the dense solve failed.
+int orc_be_step(void* h, double hstep, const double* prm, const double* fext, double* x,
+                double* v, int solver, double tol, int maxit, int* iters, double* relres) {
+  Model* m = (Model*)h;
+  double am = prm[0], bk = prm[1];
+  const double* g = prm + 2;
+  update_stress_stiffness(*m, x);
+  int nv = 3 * m->nact;
+  // FemModel3d.updateNodeForces (FemModel3d.java:2740-2847): for each node
+  // f = fext + m g - f_int - (beta_k sum_j K_ij v_j + alpha_m m v)
+  std::vector<double> f((size_t)3 * m->N, 0);
+  std::vector<double> vact(nv), xact(nv);
+  for (int n = 0; n < m->N; n++)
+    if (m->sidx[n] >= 0)
+      for (int c = 0; c < 3; c++) {
+        vact[3 * m->sidx[n] + c] = v[3 * n + c];
+        xact[3 * m->sidx[n] + c] = x[3 * n + c];
+      }
+  std::vector<double> Kv(nv, 0);
+  if (bk != 0) bsr_mul(*m, m->K, vact.data(), Kv.data());
+  for (int n = 0; n < m->N; n++) {
+    for (int c = 0; c < 3; c++) {
+      double fi = fext ? fext[3 * n + c] : 0.0;
+      fi += m->mass[n] * g[c];
+      double fk = m->fint[3 * n + c];
+      double fd = 0;
+      int bi = m->sidx[n];
+      if (bi >= 0) fd = bk * Kv[3 * bi + c];
+      fd += am * m->mass[n] * v[3 * n + c];
+      fi -= fk;
+      fi -= fd;
+      f[3 * n + c] = fi;
+    }
+  }
+  // b = M v + h f   (:2194-2200)
+  std::vector<double> b(nv);
+  for (int n = 0; n < m->N; n++) {
+    int bi = m->sidx[n];
+    if (bi < 0) continue;
+    for (int c = 0; c < 3; c++) b[3 * bi + c] = m->mass[n] * v[3 * n + c] + hstep * f[3 * n + c];
+  }
+  // S = h(alpha_m M + beta_k K)  (addVelJacobian, s = -h)
+  size_t nnzb = m->col.size();
+  std::vector<double> S(nnzb * 9, 0);
+  for (size_t q = 0; q < nnzb * 9; q++) S[q] = (hstep * bk) * m->K[q];
+  for (int n = 0; n < m->N; n++) {
+    int bi = m->sidx[n];
+    if (bi < 0) continue;
+    int d = m->block_index(bi, bi);
+    for (int c = 0; c < 3; c++) S[(size_t)d * 9 + 4 * c] += hstep * am * m->mass[n];
+  }
+  // b += S v   (:2299-2301)
+  std::vector<double> Sv(nv);
+  bsr_mul(*m, S, vact.data(), Sv.data());
+  for (int i = 0; i < nv; i++) b[i] += Sv[i];
+  // S += h^2 K  (addPosJacobian, s = -h^2), then S += M (:2312, :2334)
+  for (size_t q = 0; q < nnzb * 9; q++) S[q] += (hstep * hstep) * m->K[q];
+  for (int n = 0; n < m->N; n++) {
+    int bi = m->sidx[n];
+    if (bi < 0) continue;
+    int d = m->block_index(bi, bi);
+    for (int c = 0; c < 3; c++) S[(size_t)d * 9 + 4 * c] += m->mass[n];
+  }
+  std::vector<double> vn = vact;
+  int status = 0;
+  if (solver == 1) {
+    status = dense_solve(*m, S, b, vn);
+    if (iters) *iters = 0;
+    if (relres) {
+      std::vector<double> r(nv);
+      bsr_mul(*m, S, vn.data(), r.data());
+      double rn = 0, bn = 0;
+      for (int i = 0; i < nv; i++) { rn += (b[i] - r[i]) * (b[i] - r[i]); bn += b[i] * b[i]; }
+      *relres = std::sqrt(rn / (bn > 0 ? bn : 1));
+    }
+  } else {
+    status = cg_solve(*m, S, b, vn, tol, maxit, iters, relres);
+  }
+  // setActiveVelState, x1 = x0 + h v1 (:2465-2475)
+  for (int n = 0; n < m->N; n++) {
+    int bi = m->sidx[n];
+    if (bi < 0) continue;
+    for (int c = 0; c < 3; c++) {
+      v[3 * n + c] = vn[3 * bi + c];
+      x[3 * n + c] = x[3 * n + c] + hstep * vn[3 * bi + c];
+    }
+  }
+  return status;
+}
+
+// point-level material evaluation for known-answer and finite-difference tests
+void orc_material_eval(int mat_kind, const double* mat_params, const double* F, double pressure,
+                       double* sig6, double* D36) {
+  Material mt;
+  mt.kind = mat_kind;
+  if (mat_kind == MAT_LINEAR) { mt.E = mat_params[0]; mt.nu = mat_params[1]; }
+  else if (mat_kind == MAT_NEOHOOKEAN) { mt.E = mat_params[0]; mt.nu = mat_params[1]; }
+  else {
+    mt.c10 = mat_params[0]; mt.c01 = mat_params[1]; mt.c11 = mat_params[2]; mt.c20 = mat_params[3];
+    mt.c02 = mat_params[4]; mt.kappa = mat_params[5]; mt.jlimit = mat_params[6];
+  }
+  material_stress_tangent(sig6, D36, mt, F, det3(F), pressure);
+}
+
+void orc_material_stiffness_block(const double* gi, const double* D36, const double* sig6,
+                                  const double* gj, double dv, double* K9) {
+  for (int i = 0; i < 9; i++) K9[i] = 0;
+  add_material_stiffness(K9, gi, D36, gj, dv);
+  if (sig6) add_geometric_stiffness(K9, gi, sig6, gj, dv);
+}
+
+void orc_linear_C(double E, double nu, double* D36) { linear_C(D36, E, nu); }
+
+void orc_polar(const double* F, double* R) { polar_rotation(R, F); }
+
+}  // extern "C"

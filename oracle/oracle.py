@@ -1,0 +1,205 @@
+"""ctypes front end of the CPU FP64 oracle (``oracle/fem_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY: tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use it as the checker.  The product package
+never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libfemoracle.so")
+_lib = None
+
+ELEM_TET, ELEM_HEX = 0, 1
+MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN = 0, 1, 2
+INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp = ctypes.c_void_p
+        L.orc_num_threads.argtypes = [ctypes.c_int]
+        L.orc_grid_dims.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
+        L.orc_create_grid.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [_dp, _ip]
+        L.orc_jitter.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_uint64, _dp]
+        L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip,
+                                 ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int]
+        L.orc_create.restype = vp
+        L.orc_destroy.argtypes = [vp]
+        for name in ("orc_incomp_method", "orc_num_active", "orc_nnzb"):
+            getattr(L, name).argtypes = [vp]
+            getattr(L, name).restype = ctypes.c_int
+        L.orc_solve_index.argtypes = [vp, _ip]
+        L.orc_pattern.argtypes = [vp, _ip, _ip]
+        L.orc_masses.argtypes = [vp, _dp]
+        L.orc_rest_volumes.argtypes = [vp, _dp]
+        L.orc_crs.argtypes = [vp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_crs.restype = ctypes.c_int
+        L.orc_update_stress_stiffness.argtypes = [vp, _dp, _dp, _dp]
+        L.orc_update_stress_stiffness.restype = ctypes.c_int
+        L.orc_nodal_pressures.argtypes = [vp, _dp]
+        L.orc_be_step.argtypes = [vp, ctypes.c_double, _dp, ctypes.c_void_p, _dp, _dp, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_double)]
+        L.orc_be_step.restype = ctypes.c_int
+        L.orc_material_eval.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, _dp, _dp]
+        L.orc_material_stiffness_block.argtypes = [_dp, _dp, ctypes.c_void_p, _dp, ctypes.c_double, _dp]
+        L.orc_linear_C.argtypes = [ctypes.c_double, ctypes.c_double, _dp]
+        L.orc_polar.argtypes = [_dp, _dp]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return lib().orc_num_threads(int(n))
+
+
+def grid(elem_type: int, widths, cells, jitter: float = 0.0, seed: int = 0):
+    """FemFactory.createTetGrid / createHexGrid plus seeded interior jitter."""
+    L = lib()
+    nx, ny, nz = (int(c) for c in cells)
+    nn, ne = ctypes.c_int(), ctypes.c_int()
+    L.orc_grid_dims(elem_type, nx, ny, nz, ctypes.byref(nn), ctypes.byref(ne))
+    nen = 4 if elem_type == ELEM_TET else 8
+    xyz = np.zeros(3 * nn.value)
+    conn = np.zeros(nen * ne.value, dtype=np.int32)
+    L.orc_create_grid(elem_type, float(widths[0]), float(widths[1]), float(widths[2]), nx, ny, nz, xyz, conn)
+    if jitter:
+        L.orc_jitter(nx, ny, nz, float(widths[0]), float(widths[1]), float(widths[2]), float(jitter),
+                     ctypes.c_uint64(seed), xyz)
+    return xyz.reshape(-1, 3), conn.reshape(-1, nen)
+
+
+class OracleModel:
+    """One FEM model inside the oracle."""
+
+    def __init__(self, elem_type, rest, conn, fixed, mat_kind, mat_params, density,
+                 incomp=INCOMP_AUTO):
+        self.L = lib()
+        self.elem_type = elem_type
+        self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1)
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
+        self.N = self.rest.size // 3
+        nen = 4 if elem_type == ELEM_TET else 8
+        self.E = self.conn.size // nen
+        fx = np.ascontiguousarray(fixed, dtype=np.int32)
+        mp = np.zeros(8)
+        mp[: len(mat_params)] = mat_params
+        self.h = self.L.orc_create(elem_type, self.N, self.rest, self.E, self.conn, fx, mat_kind, mp,
+                                   float(density), incomp)
+        self.nact = self.L.orc_num_active(self.h)
+        self.nnzb = self.L.orc_nnzb(self.h)
+        self.incomp = self.L.orc_incomp_method(self.h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.L.orc_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def solve_index(self):
+        out = np.zeros(self.N, dtype=np.int32)
+        self.L.orc_solve_index(self.h, out)
+        return out
+
+    def pattern(self):
+        rp = np.zeros(self.nact + 1, dtype=np.int32)
+        col = np.zeros(self.nnzb, dtype=np.int32)
+        self.L.orc_pattern(self.h, rp, col)
+        return rp, col
+
+    def masses(self):
+        out = np.zeros(self.N)
+        self.L.orc_masses(self.h, out)
+        return out
+
+    def rest_volumes(self):
+        out = np.zeros(self.E)
+        self.L.orc_rest_volumes(self.h, out)
+        return out
+
+    def crs(self, partition=0):
+        nnz = self.L.orc_crs(self.h, partition, None, None, None)
+        ro = np.zeros(3 * self.nact + 1, dtype=np.int32)
+        ci = np.zeros(nnz, dtype=np.int32)
+        sl = np.zeros(9 * self.nnzb, dtype=np.int32)
+        self.L.orc_crs(self.h, partition, ro.ctypes.data, ci.ctypes.data, sl.ctypes.data)
+        return ro, ci, sl
+
+    def update_stress_stiffness(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        f = np.zeros(3 * self.N)
+        K = np.zeros(9 * self.nnzb)
+        ninv = self.L.orc_update_stress_stiffness(self.h, x, f, K)
+        return f.reshape(-1, 3), K.reshape(-1, 3, 3), ninv
+
+    def nodal_pressures(self):
+        out = np.zeros(self.N)
+        self.L.orc_nodal_pressures(self.h, out)
+        return out
+
+    def be_step(self, h, x, v, alpha=2.0, beta=0.0, gravity=(0, 0, 0), fext=None, solver=0,
+                tol=1e-14, maxit=100000):
+        """One BackwardEuler step; x and v (N,3) float64 arrays updated in place."""
+        prm = np.array([alpha, beta, *gravity], dtype=np.float64)
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        fe = None
+        if fext is not None:
+            fe = np.ascontiguousarray(fext, dtype=np.float64).reshape(-1)
+        st = self.L.orc_be_step(self.h, float(h), prm, fe.ctypes.data if fe is not None else None,
+                                x.reshape(-1), v.reshape(-1), int(solver), float(tol), int(maxit),
+                                ctypes.byref(it), ctypes.byref(rr))
+        return st, it.value, rr.value
+
+
+def material_eval(mat_kind, params, F, pressure=0.0):
+    mp = np.zeros(8)
+    mp[: len(params)] = params
+    sig = np.zeros(6)
+    D = np.zeros(36)
+    lib().orc_material_eval(mat_kind, mp, np.ascontiguousarray(F, dtype=np.float64).reshape(-1),
+                            float(pressure), sig, D)
+    return sig, D.reshape(6, 6)
+
+
+def material_stiffness_block(gi, D, gj, dv, sig=None):
+    K = np.zeros(9)
+    s = None if sig is None else np.ascontiguousarray(sig, dtype=np.float64)
+    lib().orc_material_stiffness_block(np.asarray(gi, dtype=np.float64), np.ascontiguousarray(D, dtype=np.float64).reshape(-1),
+                                       s.ctypes.data if s is not None else None,
+                                       np.asarray(gj, dtype=np.float64), float(dv), K)
+    return K.reshape(3, 3)
+
+
+def linear_C(E, nu):
+    D = np.zeros(36)
+    lib().orc_linear_C(float(E), float(nu), D)
+    return D.reshape(6, 6)
+
+
+def polar(F):
+    R = np.zeros(9)
+    lib().orc_polar(np.ascontiguousarray(F, dtype=np.float64).reshape(-1), R)
+    return R.reshape(3, 3)

@@ -1,0 +1,180 @@
+"""Parity of the sm_100a engine (through the C ABI) with the CPU oracle.
+
+Bars (stated here, checked below):
+* pattern, CRS indices, slot map, scatter map, solve indices: bit-exact;
+* nodal forces and stiffness blocks: max |gpu - oracle| <= 1e-10 * max |oracle|;
+* positions after the stepped run: <= 1e-8 relative to the oracle's.
+"""
+import numpy as np
+import pytest
+
+from artisynth_core_b200 import _lib as L
+from artisynth_core_b200 import workloads as W
+from artisynth_core_b200.femmodel import (LinearMaterial, MechSystemSolver, MooneyRivlinMaterial,
+                                          NeoHookeanMaterial)
+
+from helpers import deformed, oracle_model, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-10
+POS_TOL = 1e-8
+
+
+def _cases():
+    return {
+        "linear_corotated_tet": W.linear_tet_beam(),
+        "linear_plain_tet": W.small_tet_beam(LinearMaterial(5e4, 0.33, False)),
+        "linear_corotated_hex": W.small_hex_beam(LinearMaterial(2e4, 0.3, True)),
+        "neohookean_tet": W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33)),
+        "neohookean_hex": W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "mooneyrivlin_tet_off": W.small_tet_beam(MooneyRivlinMaterial(1e4, 2e3, 0, 0, 0, 1e5)),
+        "mooneyrivlin_hex_full": W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 30, 486, 20, 10370)),
+    }
+
+
+def _incomp_off(wl):
+    wl.incomp = L.INCOMP_OFF
+    return wl
+
+
+@pytest.fixture(scope="module")
+def cases(b200):
+    cs = _cases()
+    for k in ("mooneyrivlin_tet_off", "mooneyrivlin_hex_full"):
+        _incomp_off(cs[k])
+    return cs
+
+
+def _gpu_model(wl):
+    m = wl.model()
+    if hasattr(wl, "incomp"):
+        m.setSoftIncompMethod(wl.incomp)
+    return m
+
+
+@pytest.mark.parametrize("name", list(_cases().keys()))
+def test_pattern_bit_exact(name, cases, oracle):
+    wl = cases[name]
+    m = _gpu_model(wl)
+    om = oracle_model(oracle, wl)
+    rp, col = m.getBlockPattern()
+    orp, ocol = om.pattern()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
+    assert np.array_equal(m.getSolveIndices(), om.solve_index())
+    for part in (L.PART_FULL, L.PART_UPPER):
+        ro, ci = m.getCRSIndices(part)
+        oro, oci, osl = om.crs(part)
+        assert np.array_equal(ro, oro) and np.array_equal(ci, oci)
+        assert np.array_equal(m.createCrsBlockSlotMap(part), osl)
+    # scatter map: element pair (i, j) -> block of (sidx_i, sidx_j)
+    smap = m.getScatterMap()
+    sidx = om.solve_index()
+    nen = wl.conn.shape[1]
+    ref = np.full_like(smap, -1)
+    for e in range(wl.conn.shape[0]):
+        for a in range(nen):
+            for b in range(nen):
+                ra, rb = sidx[wl.conn[e, a]], sidx[wl.conn[e, b]]
+                if ra >= 0 and rb >= 0:
+                    k = orp[ra] + np.searchsorted(ocol[orp[ra]:orp[ra + 1]], rb)
+                    ref[e, a, b] = k
+    assert np.array_equal(smap, ref)
+    assert rel_err(m.getNodeMasses(), om.masses()) <= 1e-14
+
+
+@pytest.mark.parametrize("name", list(_cases().keys()))
+def test_update_stress_stiffness(name, cases, oracle):
+    wl = cases[name]
+    m = _gpu_model(wl)
+    om = oracle_model(oracle, wl)
+    for seed, x in ((0, wl.rest), (1, deformed(wl.rest, seed=5))):
+        f, K, crs = m.updateStressAndStiffness(x, want_crs=True)
+        of, oK, _ = om.update_stress_stiffness(x)
+        if seed == 0:
+            # at rest the force is round-off of the cancelling terms
+            assert np.abs(f).max() <= 1e-9 * np.abs(oK).max() * np.ptp(wl.rest)
+        else:
+            assert rel_err(f, of) <= FORCE_TOL, (name, seed, rel_err(f, of))
+        assert rel_err(K, oK) <= FORCE_TOL, (name, seed, rel_err(K, oK))
+        # full-partition CRS export lands every block entry in its slot
+        slots = m.createCrsBlockSlotMap(L.PART_FULL)
+        assert np.array_equal(crs[slots], K.reshape(-1))
+
+
+def _run_pair(wl, oracle, steps, solver, tol_gpu):
+    m = _gpu_model(wl)
+    om = oracle_model(oracle, wl)
+    x = wl.rest.copy()
+    v = np.zeros_like(x)
+    fext = wl.fext if wl.traction is not None else None
+    for _ in range(steps):
+        st, it, rr = om.be_step(wl.h, x, v, alpha=wl.mass_damping, beta=wl.stiffness_damping,
+                                gravity=wl.gravity, fext=fext, solver=solver, tol=1e-14)
+        assert st == 0
+    ms = MechSystemSolver(m, tol=tol_gpu, max_iter=20000)
+    ms.backwardEuler(wl.h, steps)
+    xg, vg = m.getState()
+    return xg, vg, x, v, ms
+
+
+def test_backward_euler_linear_tet_beam(cases, oracle):
+    """Corotated linear tet beam, 100 BackwardEuler steps (dense oracle solve)."""
+    wl = cases["linear_corotated_tet"]
+    xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)
+    assert rel_err(xg, x) <= POS_TOL, rel_err(xg, x)
+    assert np.abs(xg - x).max() <= POS_TOL * np.abs(x).max()
+    assert x[:, 2].min() < -0.05  # the beam sags (FemModel3dTest.runCorotatedBeamStep)
+
+
+@pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex", "mooneyrivlin_tet_off",
+                                  "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full"])
+def test_backward_euler_small(name, cases, oracle):
+    wl = cases[name]
+    xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)
+    assert rel_err(xg, x) <= POS_TOL, (name, rel_err(xg, x))
+    assert rel_err(vg, v) <= 1e-6, (name, rel_err(vg, v))
+
+
+def test_backward_euler_neohookean_hex_beam_steps(oracle):
+    """The 40x10x10 NeoHookean hex beam with traction: 5 steps against the
+    oracle's tight CG, and PCG at the workload's 1e-10 tolerance."""
+    wl = W.neohookean_hex_beam()
+    wl.build_mesh()
+    xg, vg, x, v, ms = _run_pair(wl, oracle, 5, 0, wl.tol)
+    assert rel_err(xg - wl.rest, x - wl.rest) <= 1e-6
+    assert rel_err(xg, x) <= POS_TOL
+    assert ms.stats.rel_residual <= 1.5 * wl.tol
+
+
+def test_deterministic(cases):
+    wl = cases["neohookean_tet"]
+    out = []
+    for _ in range(2):
+        m = _gpu_model(wl)
+        MechSystemSolver(m, tol=1e-12).backwardEuler(wl.h, 5)
+        out.append(m.getState())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_no_convergence_reports_status(cases):
+    wl = cases["neohookean_hex"]
+    m = _gpu_model(wl)
+    ms = MechSystemSolver(m, tol=1e-14, max_iter=1)
+    with pytest.raises(L.B200FemError) as ei:
+        ms.backwardEuler(wl.h, 1)
+    assert ei.value.status == L.ERR_NO_CONVERGE
+
+
+def test_spmv_and_pcg_solve(cases):
+    wl = cases["neohookean_hex"]
+    m = _gpu_model(wl)
+    ms = MechSystemSolver(m, tol=1e-12)
+    ms.backwardEuler(wl.h, 2)
+    n = m.sizes()["n_active"] * 3
+    rng = np.random.default_rng(0)
+    xt = rng.standard_normal(n)
+    b = ms.spmv(xt)
+    x, st = ms.pcg(b, tol=1e-13, max_iter=5000)
+    assert rel_err(x, xt) <= 1e-9
+    assert st.rel_residual <= 1e-12

@@ -1,0 +1,238 @@
+"""Pins the CPU oracle against the reference's own known answers and
+consistency checks (no GPU needed).
+
+* CuDssSolverTest.testLinearElasticStiffness3ElementGeometryDeviceContribution
+  (CuDssSolverTest.java:691-760): E=4, nu=0, unit natural gradients ->
+  diagonal stiffness 4 per axis, so K x = (4, 8, 12) gives x = (1, 2, 3).
+* FemModel3dTest.testMaterialStiffness3ContextAssembly
+  (FemModel3dTest.java:599-670): D = diag entries 4, 5, 6 on unit gradients
+  assemble to the block {4,0,0, 0,5,0, 0,0,6}; solving with [4,10,18] gives
+  [1,2,3].
+* SparseNumberedBlockMatrixTest.testCrsBlockSlotMap
+  (SparseNumberedBlockMatrixTest.java:115-193): every CRS value slot is hit
+  exactly once and holds its block entry, for Full and UpperTriangular.
+* FemMaterialTest (FemMaterialTest.java:285-460): the tangent matches finite
+  differences of the stress for NeoHookean(1e4, 0.49) and
+  MooneyRivlin(1.2, 3.4, 0, 0, 0, 1000).
+* StiffnessTest (StiffnessTest.java:197-235): the assembled stiffness matches
+  finite differences of the nodal forces.
+* Pattern sizes of the benchmark meshes (788 blocks for the 10x2x2 tet beam,
+  113,398 for the 40x10x10 hex beam).
+"""
+import numpy as np
+import pytest
+
+from helpers import deformed, oracle_model, rel_err
+
+
+def test_linear_geometry_known_answer(oracle):
+    D = oracle.linear_C(4.0, 0.0)
+    K = np.zeros((3, 3))
+    for axis in range(3):
+        g = np.zeros(3)
+        g[axis] = 1.0
+        K += oracle.material_stiffness_block(g, D, g, 1.0)
+    # per node i the reference assembles only K[i,i] at CRS slot i
+    diag = np.array([oracle.material_stiffness_block(np.eye(3)[i], D, np.eye(3)[i], 1.0)[i, i]
+                     for i in range(3)])
+    assert np.array_equal(diag, [4.0, 4.0, 4.0])
+    x = np.array([4.0, 8.0, 12.0]) / diag
+    assert np.allclose(x, [1, 2, 3], rtol=0, atol=1e-15)
+
+
+def test_material_stiffness_context_known_answer(oracle):
+    blk = np.zeros((3, 3))
+    for axis, dval in enumerate((4.0, 5.0, 6.0)):
+        D = np.zeros((6, 6))
+        D[axis, axis] = dval
+        g = np.eye(3)[axis]
+        blk += oracle.material_stiffness_block(g, D, g, 1.0, sig=np.zeros(6))
+    assert np.array_equal(blk.reshape(-1), [4, 0, 0, 0, 5, 0, 0, 0, 6])
+    x = np.linalg.solve(blk, [4.0, 10.0, 18.0])
+    assert np.abs(x - [1, 2, 3]).max() <= 1e-10
+
+
+def _tiny_model(oracle, fixed0=True):
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (1.0, 0.8, 0.6), (1, 1, 1))
+    fixed = np.zeros(xyz.shape[0], dtype=np.int32)
+    if fixed0:
+        fixed[0] = 1
+    return oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_LINEAR, [1e4, 0.33, 1], 1000.0), xyz
+
+
+@pytest.mark.parametrize("partition", [0, 1])
+def test_crs_slot_map_property(oracle, partition):
+    m, xyz = _tiny_model(oracle)
+    rng = np.random.default_rng(0)
+    f, K, _ = m.update_stress_stiffness(xyz + 0.01 * rng.standard_normal(xyz.shape))
+    rp, col = m.pattern()
+    ro, ci, slots = m.crs(partition)
+    nnz = ci.size
+    vals = np.zeros(nnz)
+    # getCRSValues: walk rows, blocks by column
+    dense = np.zeros((3 * m.nact, 3 * m.nact))
+    for bi in range(m.nact):
+        for p in range(rp[bi], rp[bi + 1]):
+            dense[3 * bi:3 * bi + 3, 3 * col[p]:3 * col[p] + 3] = K[p]
+    for r in range(3 * m.nact):
+        for s in range(ro[r], ro[r + 1]):
+            vals[s] = dense[r, ci[s]]
+    seen = np.zeros(nnz, dtype=bool)
+    for p in range(col.size):
+        for q in range(9):
+            s = slots[9 * p + q]
+            if s == -1:
+                continue
+            assert 0 <= s < nnz and not seen[s]
+            seen[s] = True
+            assert vals[s] == K[p].reshape(-1)[q]
+    assert seen.all()
+    if partition == 1:
+        assert np.all(np.diff(ro) > 0) and all(ci[s] >= r for r in range(3 * m.nact) for s in range(ro[r], ro[r + 1]))
+
+
+def _fd_tangent(oracle, kind, params, F, p=0.0, h=1e-8):
+    """Spatial tangent check: for a perturbation dF = dU F (dU symmetric),
+    the Kirchhoff-type rate J(d sigma + sigma tr(dU)) - (dU sigma + sigma dU)
+    equals D:dU in Voigt form (FemMaterialTest's FD identity)."""
+    sig, D = oracle.material_eval(kind, params, F, p)
+    J = np.linalg.det(F)
+    err = 0.0
+    for k in range(6):
+        dU = np.zeros((3, 3))
+        i, j = [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)][k]
+        dU[i, j] = dU[j, i] = 1.0 if i == j else 0.5
+        Fp = (np.eye(3) + h * dU) @ F
+        Fm = (np.eye(3) - h * dU) @ F
+        sp, _ = oracle.material_eval(kind, params, Fp, p)
+        sm, _ = oracle.material_eval(kind, params, Fm, p)
+        ds = (sp - sm) / (2 * h)
+        S = np.array([[sig[0], sig[3], sig[5]], [sig[3], sig[1], sig[4]], [sig[5], sig[4], sig[2]]])
+        dS = np.array([[ds[0], ds[3], ds[5]], [ds[3], ds[1], ds[4]], [ds[5], ds[4], ds[2]]])
+        rate = dS + S * np.trace(dU) - (dU @ S + S @ dU)
+        v = np.array([rate[0, 0], rate[1, 1], rate[2, 2], rate[0, 1], rate[1, 2], rate[0, 2]])
+        eps = np.array([dU[0, 0], dU[1, 1], dU[2, 2], 2 * dU[0, 1], 2 * dU[1, 2], 2 * dU[0, 2]])
+        Dv = D @ eps
+        err = max(err, np.abs(v - Dv).max() / max(np.abs(D).max(), 1e-30))
+    return err
+
+
+@pytest.mark.parametrize("kind,params", [(1, [1e4, 0.49]), (2, [1.2, 3.4, 0, 0, 0, 1000, 0, 0]),
+                                         (2, [1037, 0, 0, 486, 0, 10370, 0, 0])])
+def test_material_tangent_matches_fd(oracle, kind, params):
+    # The reference's MooneyRivlin tangent is FD-consistent for c10, c01 and
+    # c20 (the terms its own tests and regression script use); its c11 and
+    # c02 terms are not exact derivatives and are reproduced as written.
+    rng = np.random.default_rng(1)
+    for _ in range(5):
+        F = np.eye(3) + 0.2 * rng.standard_normal((3, 3))
+        if np.linalg.det(F) <= 0.2:
+            continue
+        assert _fd_tangent(oracle, kind, params, F, p=0.0) <= 1e-6
+
+
+def test_polar_rotation(oracle):
+    rng = np.random.default_rng(2)
+    for _ in range(50):
+        F = rng.standard_normal((3, 3))
+        R = oracle.polar(F)
+        assert abs(np.linalg.det(R) - 1) <= 1e-12
+        assert np.abs(R.T @ R - np.eye(3)).max() <= 1e-12
+        U, s, Vt = np.linalg.svd(F)
+        Rref = U @ np.diag([1, 1, np.sign(np.linalg.det(U @ Vt))]) @ Vt
+        assert np.abs(R - Rref).max() <= 1e-10
+
+
+@pytest.mark.parametrize("kind,params,etype", [(0, [5e4, 0.3, 0], 0), (1, [5e4, 0.45], 0),
+                                               (1, [5e4, 0.45], 1), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1)])
+def test_stiffness_matches_force_fd(oracle, kind, params, etype):
+    # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
+    # exact derivative by design and is pinned by the GPU parity tests)
+    xyz, conn = oracle.grid(etype, (1.0, 0.4, 0.4), (3, 2, 2), jitter=0.04, seed=3)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(etype, xyz, conn, fixed, kind, params, 1000.0, oracle.INCOMP_OFF)
+    x = deformed(xyz, seed=1, rot_deg=15, bend=0.05, noise=0.01)
+    f0, K, _ = m.update_stress_stiffness(x)
+    sidx = m.solve_index()
+    rp, col = m.pattern()
+    act = np.where(sidx >= 0)[0]
+    h = 1e-7
+    rng = np.random.default_rng(4)
+    for trial in range(6):
+        n = act[rng.integers(act.size)]
+        c = rng.integers(3)
+        xp = x.copy(); xp[n, c] += h
+        xm = x.copy(); xm[n, c] -= h
+        fp, _, _ = m.update_stress_stiffness(xp)
+        fm, _, _ = m.update_stress_stiffness(xm)
+        df = (fp - fm) / (2 * h)
+        # K column of (n, c): rows bi, block (bi, sidx[n])
+        bj = sidx[n]
+        for bi in range(m.nact):
+            for p in range(rp[bi], rp[bi + 1]):
+                if col[p] == bj:
+                    node_i = act[bi]
+                    assert np.abs(K[p][:, c] - df[node_i]).max() <= 1e-5 * np.abs(K).max()
+
+
+def test_benchmark_pattern_sizes(oracle):
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (1.0, 0.2, 0.2), (10, 2, 2), 0.05, 0)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_LINEAR, [1e5, 0.33, 1], 1000.0)
+    assert (xyz.shape[0], conn.shape[0], m.nact, m.nnzb) == (99, 200, 90, 788)
+    assert abs(m.masses().sum() - 1000 * 1.0 * 0.2 * 0.2) <= 1e-10
+    xyz, conn = oracle.grid(oracle.ELEM_HEX, (1.0, 0.25, 0.25), (40, 10, 10), 0.03, 1)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_HEX, xyz, conn, fixed, oracle.MAT_NEOHOOKEAN, [5e4, 0.45], 1000.0)
+    assert (xyz.shape[0], conn.shape[0], m.nact, m.nnzb) == (4961, 4000, 4840, 113398)
+    assert abs(m.rest_volumes().sum() - 1.0 * 0.25 * 0.25) <= 1e-12
+
+
+def test_auto_resolves_to_nodal(oracle):
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (0.3, 0.15, 0.15), (6, 3, 3), 0.05, 2)
+    fixed = (xyz[:, 2] <= -0.075 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_MOONEYRIVLIN,
+                           [1000, 500, 0, 0, 0, 1e5, 0, 0], 1050.0, oracle.INCOMP_AUTO)
+    assert m.incomp == oracle.INCOMP_NODAL
+    m2 = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_NEOHOOKEAN, [1e4, 0.3], 1000.0,
+                            oracle.INCOMP_AUTO)
+    assert m2.incomp == oracle.INCOMP_OFF
+
+
+def test_corotated_beam_sags(oracle):
+    """FemModel3dTest.runCorotatedBeamStep (FemModel3dTest.java:802-868):
+    8x2x2 corotated beam, 25 steps h=0.01, gravity -9.8: tip sags below -0.05."""
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (1.0, 0.2, 0.2), (8, 2, 2))
+    fixed = (xyz[:, 0] <= -0.5 + 1e-6).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_LINEAR, [2e4, 0.33, 1], 1000.0)
+    x = xyz.copy()
+    v = np.zeros_like(x)
+    for _ in range(25):
+        st, _, _ = m.be_step(0.01, x, v, gravity=(0, 0, -9.8), solver=1)
+        assert st == 0
+    assert x[:, 2].min() < -0.05
+
+
+def test_be_dense_and_cg_agree(oracle):
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (1.0, 0.2, 0.2), (10, 2, 2), 0.05, 0)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-6).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, oracle.MAT_NEOHOOKEAN, [1e5, 0.33], 1000.0)
+    xa, va = xyz.copy(), np.zeros_like(xyz)
+    xb, vb = xyz.copy(), np.zeros_like(xyz)
+    for _ in range(10):
+        m.be_step(0.01, xa, va, gravity=(0, 0, -9.81), solver=1)
+        m.be_step(0.01, xb, vb, gravity=(0, 0, -9.81), solver=0, tol=1e-14)
+    assert rel_err(xa, xb) <= 1e-12
+
+
+def test_thread_count_does_not_change_results(oracle):
+    xyz, conn = oracle.grid(oracle.ELEM_HEX, (1.0, 0.25, 0.25), (8, 3, 3), 0.03, 1)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_HEX, xyz, conn, fixed, oracle.MAT_NEOHOOKEAN, [5e4, 0.45], 1000.0)
+    x = deformed(xyz)
+    prev = oracle.set_threads(1)
+    f1, K1, _ = m.update_stress_stiffness(x)
+    oracle.set_threads(4)
+    f4, K4, _ = m.update_stress_stiffness(x)
+    oracle.set_threads(prev)
+    assert np.array_equal(f1, f4) and np.array_equal(K1, K4)
