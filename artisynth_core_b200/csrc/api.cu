@@ -240,7 +240,8 @@ int build_pack(Engine& eng) {
 
   // ---- PCG work split: CTAs own contiguous row ranges balanced by blocks,
   // cut into pieces at model boundaries
-  int gmax = pcg_max_grid(eng.device);
+  // one 1024-thread CTA per SM at most, >= 32 rows (one per warp) each
+  int gmax = std::min(pcg_max_grid(eng.device), eng.num_sms);
   int G = std::max(1, std::min(gmax, (R + 31) / 32));
   std::vector<int> piece_row, piece_model, cta_piece, model_piece(M + 1, 0);
   for (;;) {
@@ -312,7 +313,7 @@ int build_pack(Engine& eng) {
   CK(dalloc(eng, &d.S, (size_t)NB * 9));
   CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
   CK(dalloc(eng, &d.fint, 3 * (size_t)N));
-  for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w}) {
+  for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w, &d.u, &d.s, &d.m0, &d.m1}) {
     CK(dalloc(eng, v, 3 * (size_t)R));
     CK(cudaMemset(*v, 0, 3 * sizeof(double) * (size_t)R));
   }
@@ -323,7 +324,7 @@ int build_pack(Engine& eng) {
     CK(dalloc(eng, &d.node_vol, (size_t)N));
     CK(dalloc(eng, &d.node_p, (size_t)N));
   }
-  CK(dalloc(eng, &d.partials, (size_t)d.n_pieces * 4));
+  CK(dalloc(eng, &d.partials, (size_t)d.n_pieces * 8));
   CK(upload(eng, &d.piece_row, piece_row));
   CK(upload(eng, &d.piece_model, piece_model));
   CK(upload(eng, &d.model_piece, model_piece));
@@ -424,6 +425,7 @@ int b200fem_destroy(b200fem_handle h) {
   free_pack(h->eng);
   for (auto& ev : h->eng.ev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& ev : h->eng.ev_pool) cudaEventDestroy(ev);
   if (h->eng.stream) cudaStreamDestroy(h->eng.stream);
   delete h;
   return B200FEM_OK;
@@ -721,10 +723,17 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
   }
   CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
   CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  while ((int)eng.ev_pool.size() < 3 * nsteps) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    eng.ev_pool.push_back(e);
+  }
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   for (int s = 0; s < nsteps; s++) {
+    CK(cudaEventRecord(eng.ev_pool[3 * s], eng.stream));
     CK(launch_assemble(eng, 0, 0, false));
     CK(launch_rhs(eng));
+    CK(cudaEventRecord(eng.ev_pool[3 * s + 1], eng.stream));
     if (p->abort_on_inverted) {
       int flags[4];
       CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
@@ -733,13 +742,23 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
         return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
     }
     CK(launch_pcg(eng, max_iter, true, 0));
+    CK(cudaEventRecord(eng.ev_pool[3 * s + 2], eng.stream));
   }
   CK(cudaEventRecord(eng.ev[1], eng.stream));
   eng.have_matrix = true;
   int st = read_step_status(eng, stats, max_iter);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]);
-  eng.last_solve_ms = ms;
+  // device time of the assembly (element, gather, RHS kernels) and of the
+  // PCG launches, summed over the steps of this call
+  double asm_ms = 0, pcg_ms = 0;
+  for (int s = 0; s < nsteps; s++) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, eng.ev_pool[3 * s], eng.ev_pool[3 * s + 1]);
+    cudaEventElapsedTime(&b, eng.ev_pool[3 * s + 1], eng.ev_pool[3 * s + 2]);
+    asm_ms += a;
+    pcg_ms += b;
+  }
+  eng.last_asm_ms = (float)asm_ms;
+  eng.last_solve_ms = (float)pcg_ms;
   return st;
 }
 

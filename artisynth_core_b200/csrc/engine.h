@@ -105,6 +105,10 @@ struct DevPack {
   double* p = nullptr;
   double* q = nullptr;
   double* w = nullptr;
+  double* u = nullptr;
+  double* s = nullptr;
+  double* m0 = nullptr;
+  double* m1 = nullptr;
   // per model tables
   double* mat = nullptr;       // n_models*kMatParams
   double* step = nullptr;      // n_models*8: h, alpha, beta, gx, gy, gz, tol, -
@@ -113,7 +117,7 @@ struct DevPack {
   double* node_vol = nullptr;
   double* node_p = nullptr;
   // reductions / PCG control
-  double* partials = nullptr;  // n_pieces*4
+  double* partials = nullptr;  // [2][n_pieces][4] (double-buffered by phase)
   int* piece_row = nullptr;    // n_pieces+1
   int* piece_model = nullptr;  // n_pieces
   int* model_piece = nullptr;  // n_models+1
@@ -143,6 +147,7 @@ struct Engine {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> ev_pool;  // 3 per step of a multi-step call
   std::string last_error;
   std::vector<ModelDesc> models;
   std::vector<ModelHost> hosts;

@@ -21,6 +21,7 @@
 #include <cstdio>
 
 #include "device_math.cuh"
+#include "spmv.cuh"
 #include "engine.h"
 
 namespace b200fem {
@@ -132,19 +133,34 @@ struct ElemArgs {
 // ---------------------------------------------------------------------------
 // non-linear materials (NeoHookean, MooneyRivlin), tet or hex
 // ---------------------------------------------------------------------------
-template <int TYPE, int MAT, bool NODAL, typename T>
-__global__ void __launch_bounds__(256) elem_nonlinear_kernel(ElemArgs a) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+// Shared-memory layout of the non-linear element kernel (one record per
+// integration point: shape gradients, dv, stress, tangent).
+template <int TYPE, int MAT, typename T, int EPB>
+struct ElemSmem {
+  static constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  static constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  static constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
+  static constexpr int NREC = EPB * NIP;
+  static constexpr size_t bytes() {
+    return sizeof(T) * ((size_t)EPB * NEN * 3 + (size_t)NREC * (NEN * 3 + 1 + 6 + DS)) + sizeof(int) * EPB * NEN;
+  }
+};
+
+template <int TYPE, int MAT, bool NODAL, typename T, int EPB>
+__global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
+  using SM = ElemSmem<TYPE, MAT, T, EPB>;
+  constexpr int NEN = SM::NEN;
+  constexpr int NIP = SM::NIP;
   constexpr int NPAIR = NEN * (NEN + 1) / 2;
-  constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 4;
-  constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
-  __shared__ T sx[EPB][NEN][3];
-  __shared__ T sg[EPB * NIP][NEN][3];
-  __shared__ T sdv[EPB * NIP];
-  __shared__ T ssig[EPB * NIP][6];
-  __shared__ T sD[EPB * NIP][DS];
-  __shared__ int snode[EPB][NEN];
+  constexpr int DS = SM::DS;
+  constexpr int NREC = SM::NREC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*sx)[NEN][3] = reinterpret_cast<T(*)[NEN][3]>(smem_raw);
+  T(*sg)[NEN][3] = reinterpret_cast<T(*)[NEN][3]>(smem_raw + sizeof(T) * EPB * NEN * 3);
+  T* sdv = reinterpret_cast<T*>(smem_raw + sizeof(T) * ((size_t)EPB * NEN * 3 + (size_t)NREC * NEN * 3));
+  T(*ssig)[6] = reinterpret_cast<T(*)[6]>(sdv + NREC);
+  T(*sD)[DS] = reinterpret_cast<T(*)[DS]>(sdv + NREC + NREC * 6);
+  int(*snode)[NEN] = reinterpret_cast<int(*)[NEN]>(sdv + NREC + NREC * 6 + NREC * DS);
   const int ebase = a.e0 + blockIdx.x * EPB;
   // stage 0: coalesced connectivity + coordinate loads.  In FP32 the
   // coordinates are taken relative to the element's first node in FP64 so
@@ -404,10 +420,18 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
   int q = (int)(t - p * 9);
   int qt = (q % 3) * 3 + q / 3;
   TK s = TK(0);
-  int c1 = cptr[p + 1];
-  for (int c = cptr[p]; c < c1; c++) {
-    int code = cidx[c];
-    s += elemK[(size_t)(code >> 1) * 9 + ((code & 1) ? qt : q)];
+  const int c0 = cptr[p], c1 = cptr[p + 1];
+  // four contributions per round (independent loads), summed in list order
+  for (int c = c0; c < c1; c += 4) {
+    int code[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) code[k] = (c + k < c1) ? cidx[c + k] : -1;
+    TK v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      v[k] = code[k] >= 0 ? elemK[(size_t)(code[k] >> 1) * 9 + ((code[k] & 1) ? qt : q)] : TK(0);
+#pragma unroll
+    for (int k = 0; k < 4; k++) s += v[k];
   }
   double val;
   if (mode == 0) {
@@ -442,12 +466,21 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double f[3] = {0, 0, 0};
-  int i1 = inc_ptr[n + 1];
-  for (int i = inc_ptr[n]; i < i1; i++) {
-    const TF* src = elemF + (size_t)inc_idx[i] * 3;
-    f[0] += (double)src[0];
-    f[1] += (double)src[1];
-    f[2] += (double)src[2];
+  const int i0 = inc_ptr[n], i1 = inc_ptr[n + 1];
+  // four incidences per round: their index and force loads are independent
+  for (int i = i0; i < i1; i += 4) {
+    int idx[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) idx[k] = (i + k < i1) ? inc_idx[i + k] : -1;
+    double g[4][3];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) g[k][c] = idx[k] >= 0 ? (double)elemF[(size_t)idx[k] * 3 + c] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) f[c] += g[k][c];
   }
   if (fint) {
     fint[3 * (size_t)n] = f[0];
@@ -471,32 +504,6 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
 // ---------------------------------------------------------------------------
 // block SpMV helpers
 // ---------------------------------------------------------------------------
-template <typename MT>
-__device__ __forceinline__ void warp_row_spmv(int row, const int* __restrict__ rowptr,
-                                              const int* __restrict__ col, const MT* __restrict__ S,
-                                              const double* __restrict__ x, int lane, double* y) {
-  int p0 = rowptr[row], p1 = rowptr[row + 1];
-  int nval = (p1 - p0) * 9;
-  const MT* base = S + (size_t)p0 * 9;
-  double a0 = 0, a1 = 0, a2 = 0;
-  for (int i = lane; i < nval; i += 32) {
-    int bk = i / 9, q = i - bk * 9, r = q / 3, c = q - r * 3;
-    double v = (double)base[i] * x[3 * (size_t)col[p0 + bk] + c];
-    if (r == 0) a0 += v;
-    else if (r == 1) a1 += v;
-    else a2 += v;
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-    a2 += __shfl_xor_sync(0xffffffffu, a2, off);
-  }
-  y[0] = a0;
-  y[1] = a1;
-  y[2] = a2;
-}
-
 template <typename MT>
 __global__ void spmv_kernel(int n_rows, const int* rowptr, const int* col, const MT* S, const double* x,
                             double* y) {
@@ -527,347 +534,6 @@ __global__ void crs_export_kernel(long long nnzb, const int* blk_row, const int*
 }
 
 // ---------------------------------------------------------------------------
-// persistent cooperative PCG
-// ---------------------------------------------------------------------------
-constexpr int kPcgThreads = 512;
-constexpr int kRowChunk = 512;
-constexpr int kMaxCtaPieces = 48;
-constexpr unsigned long long kBarrierTimeoutNs = 5000000000ull;
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Grid-wide barrier for a cooperative launch (all CTAs co-resident).  The
-// spin is bounded: after kBarrierTimeoutNs the CTA records
-// B200FEM_ERR_TIMEOUT in flags[0] and returns false; every CTA then leaves
-// the kernel at its next barrier.
-__device__ bool grid_barrier(unsigned* bar, int* flags) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned* gen = bar + 1;
-    volatile int* err = flags;
-    unsigned g = *gen;
-    __threadfence();
-    unsigned arrived = atomicAdd(bar, 1u);
-    int ok = 1;
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      unsigned long long t0 = global_ns();
-      while (*gen == g) {
-        if (*err != 0) { ok = 0; break; }
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
-          atomicExch(flags, B200FEM_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(40);
-      }
-    }
-    __threadfence();
-    if (*err != 0) ok = 0;
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-struct PcgArgs {
-  int n_rows;
-  const int* rowptr;
-  const int* col;
-  const int* blk_diag;
-  const void* S;
-  double* Dinv;
-  const double* b;
-  double* x;
-  double* r;
-  double* z;
-  double* p;
-  double* q;
-  const int* piece_row;
-  const int* piece_model;
-  const int* model_piece;
-  const int* cta_piece;
-  double* partials;  // n_pieces * 4
-  const double* step;
-  double* model_out;  // n_models * 4: iterations, rel residual, converged
-  unsigned* barrier;
-  int* flags;
-  int* unconv;
-  int max_iter;
-  int update_state;
-  int init_dinv;
-  double* xpos;
-  double* vel;
-  const int* act_node;
-  const int* row_model;
-};
-
-// Reduce per-row values (ND of them, produced by fn(row, lane, vals) in
-// warp-uniform fashion) over this CTA's pieces, in a fixed order, and write
-// partials[piece*4 + k].  fn may also update row data.
-template <int ND, bool WARP_ROWS, typename Fn>
-__device__ void cta_row_pass(const PcgArgs& a, int pc0, int pc1, double (*rowbuf)[3],
-                             double (*pacc)[3], Fn fn) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int npc = pc1 - pc0;
-  for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
-  const int r0 = a.piece_row[pc0], r1 = a.piece_row[pc1];
-  for (int c0 = r0; c0 < r1; c0 += kRowChunk) {
-    const int c1 = min(c0 + kRowChunk, r1);
-    __syncthreads();
-    if (WARP_ROWS) {
-      for (int row = c0 + warp; row < c1; row += nwarps) {
-        double vals[3] = {0, 0, 0};
-        fn(row, lane, vals);
-        if (lane == 0) {
-#pragma unroll
-          for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
-        }
-      }
-    } else {
-      for (int row = c0 + (int)threadIdx.x; row < c1; row += blockDim.x) {
-        double vals[3] = {0, 0, 0};
-        fn(row, 0, vals);
-#pragma unroll
-        for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
-      }
-    }
-    __syncthreads();
-    // piece j's rows inside this chunk, summed by warp (j % nwarps)
-    for (int j = warp; j < npc; j += nwarps) {
-      int pr0 = max(a.piece_row[pc0 + j], c0), pr1 = min(a.piece_row[pc0 + j + 1], c1);
-      if (pr0 >= pr1) continue;
-      double s[3] = {0, 0, 0};
-      for (int row = pr0 + lane; row < pr1; row += 32)
-#pragma unroll
-        for (int k = 0; k < ND; k++) s[k] += rowbuf[row - c0][k];
-#pragma unroll
-      for (int k = 0; k < ND; k++)
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
-      if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < ND; k++) pacc[j][k] += s[k];
-    }
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < npc; j += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < ND; k++) a.partials[(size_t)(pc0 + j) * 4 + k] = pacc[j][k];
-}
-
-// Sum slot k of the partials of each local piece's model (warp per piece,
-// fixed lane striding and butterfly order).
-template <int ND>
-__device__ void model_sums(const PcgArgs& a, int pc0, int pc1, double (*out)[3]) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (int j = warp; j < pc1 - pc0; j += nwarps) {
-    int m = a.piece_model[pc0 + j];
-    int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
-    double s[3] = {0, 0, 0};
-    for (int q = q0 + lane; q < q1; q += 32)
-#pragma unroll
-      for (int k = 0; k < ND; k++) s[k] += __ldcg(&a.partials[(size_t)q * 4 + k]);
-#pragma unroll
-    for (int k = 0; k < ND; k++)
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], off);
-    if (lane == 0)
-#pragma unroll
-      for (int k = 0; k < ND; k++) out[j][k] = s[k];
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ int piece_of_row(const PcgArgs& a, int pc0, int pc1, int row) {
-  int j = 0;
-  while (pc0 + j + 1 < pc1 && a.piece_row[pc0 + j + 1] <= row) j++;
-  return j;
-}
-
-template <typename MT>
-__global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
-  __shared__ double rowbuf[kRowChunk][3];
-  __shared__ double pacc[kMaxCtaPieces][3];
-  __shared__ double sums[kMaxCtaPieces][3];
-  __shared__ double s_rho[kMaxCtaPieces], s_bb[kMaxCtaPieces], s_alpha[kMaxCtaPieces],
-      s_beta[kMaxCtaPieces], s_tol[kMaxCtaPieces];
-  __shared__ int s_conv[kMaxCtaPieces], s_iters[kMaxCtaPieces];
-  const MT* S = (const MT*)a.S;
-  const int pc0 = a.cta_piece[blockIdx.x], pc1 = a.cta_piece[blockIdx.x + 1];
-  const int npc = pc1 - pc0;
-
-  // ---- init: r = b - S x, Dinv, z = Dinv r; dots r.z, r.r, b.b
-  cta_row_pass<3, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
-    double Ax[3];
-    warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
-    if (lane == 0) {
-      double* Di = a.Dinv + (size_t)row * 9;
-      if (a.init_dinv) {
-        const MT* Db = S + (size_t)a.blk_diag[row] * 9;
-        double d[9], inv[9];
-#pragma unroll
-        for (int i = 0; i < 9; i++) d[i] = (double)Db[i];
-        double det = invert3(inv, d);
-        if (det == 0.0) {
-          atomicExch(a.flags, B200FEM_ERR_INVALID_ARG);
-#pragma unroll
-          for (int i = 0; i < 9; i++) inv[i] = 0;
-        }
-#pragma unroll
-        for (int i = 0; i < 9; i++) Di[i] = inv[i];
-      }
-      double r[3], z[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) r[c] = a.b[3 * (size_t)row + c] - Ax[c];
-#pragma unroll
-      for (int c = 0; c < 3; c++) z[c] = Di[3 * c] * r[0] + Di[3 * c + 1] * r[1] + Di[3 * c + 2] * r[2];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        a.r[3 * (size_t)row + c] = r[c];
-        a.z[3 * (size_t)row + c] = z[c];
-      }
-      double bb = 0;
-#pragma unroll
-      for (int c = 0; c < 3; c++) bb += a.b[3 * (size_t)row + c] * a.b[3 * (size_t)row + c];
-      vals[0] = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
-      vals[1] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-      vals[2] = bb;
-    }
-  });
-  if (!grid_barrier(a.barrier, a.flags)) return;
-  model_sums<3>(a, pc0, pc1, sums);
-  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-    int m = a.piece_model[pc0 + j];
-    s_rho[j] = sums[j][0];
-    s_bb[j] = sums[j][2];
-    s_tol[j] = a.step[(size_t)m * 8 + 6];
-    s_conv[j] = (sums[j][1] == 0.0) || (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]));
-    s_iters[j] = 0;
-    s_beta[j] = 0;
-  }
-  __syncthreads();
-
-  int it = 0;
-  for (;;) {
-    // ---- phase A: p = z + beta p; q = S z + beta q; dot p.q
-    for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-      int m = a.piece_model[pc0 + j];
-      if (!s_conv[j] && pc0 + j == a.model_piece[m + 1] - 1) a.unconv[it] = 1;
-    }
-    cta_row_pass<1, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
-      int j = piece_of_row(a, pc0, pc1, row);
-      if (s_conv[j]) return;
-      double beta = s_beta[j];
-      double Az[3];
-      warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.z, lane, Az);
-      if (lane == 0) {
-        double pq = 0;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          size_t i = 3 * (size_t)row + c;
-          double pn = a.z[i] + beta * a.p[i];
-          double qn = Az[c] + beta * a.q[i];
-          a.p[i] = pn;
-          a.q[i] = qn;
-          pq += pn * qn;
-        }
-        vals[0] = pq;
-      }
-    });
-    if (!grid_barrier(a.barrier, a.flags)) return;
-    if (__ldcg(&a.unconv[it]) == 0) break;
-    model_sums<1>(a, pc0, pc1, sums);
-    for (int j = threadIdx.x; j < npc; j += blockDim.x)
-      s_alpha[j] = s_conv[j] ? 0.0 : s_rho[j] / sums[j][0];
-    __syncthreads();
-    // ---- phase B: x += alpha p; r -= alpha q; z = Dinv r; dots r.z, r.r
-    cta_row_pass<2, false>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
-      int j = piece_of_row(a, pc0, pc1, row);
-      if (s_conv[j]) return;
-      double al = s_alpha[j];
-      double r[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        size_t i = 3 * (size_t)row + c;
-        a.x[i] += al * a.p[i];
-        r[c] = a.r[i] - al * a.q[i];
-        a.r[i] = r[c];
-      }
-      const double* Di = a.Dinv + (size_t)row * 9;
-      double z[3];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        z[c] = Di[3 * c] * r[0] + Di[3 * c + 1] * r[1] + Di[3 * c + 2] * r[2];
-        a.z[3 * (size_t)row + c] = z[c];
-      }
-      vals[0] = r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
-      vals[1] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    });
-    if (!grid_barrier(a.barrier, a.flags)) return;
-    model_sums<2>(a, pc0, pc1, sums);
-    it++;
-    for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-      if (s_conv[j]) continue;
-      double rho1 = sums[j][0];
-      s_beta[j] = rho1 / s_rho[j];
-      s_rho[j] = rho1;
-      s_iters[j] = it;
-      if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j])) s_conv[j] = 1;
-    }
-    __syncthreads();
-    if (it >= a.max_iter) break;
-  }
-
-  // ---- final: true residual b - S x, and the state update
-  cta_row_pass<1, true>(a, pc0, pc1, rowbuf, pacc, [&](int row, int lane, double* vals) {
-    double Ax[3];
-    warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
-    if (lane == 0) {
-      double rr = 0;
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double d = a.b[3 * (size_t)row + c] - Ax[c];
-        rr += d * d;
-      }
-      vals[0] = rr;
-    }
-  });
-  if (!grid_barrier(a.barrier, a.flags)) return;
-  model_sums<1>(a, pc0, pc1, sums);
-  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-    int m = a.piece_model[pc0 + j];
-    if (pc0 + j == a.model_piece[m + 1] - 1) {
-      double* o = a.model_out + (size_t)m * 4;
-      o[0] = s_iters[j];
-      o[1] = s_bb[j] > 0 ? sqrt(sums[j][0] / s_bb[j]) : sqrt(sums[j][0]);
-      o[2] = s_conv[j];
-    }
-  }
-  if (a.update_state) {
-    const int r0 = a.piece_row[pc0], r1 = a.piece_row[pc1];
-    for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
-      int n = a.act_node[row];
-      double h = a.step[(size_t)a.row_model[row] * 8];
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double vn = a.x[3 * (size_t)row + c];
-        a.vel[3 * (size_t)n + c] = vn;
-        a.xpos[3 * (size_t)n + c] += h * vn;
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
 static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
@@ -893,6 +559,17 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   return a;
 }
 
+template <int TYPE, int MAT, bool NODAL, typename T, int EPB>
+static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) {
+  using SM = ElemSmem<TYPE, MAT, T, EPB>;
+  auto kern = elem_nonlinear_kernel<TYPE, MAT, NODAL, T, EPB>;
+  const size_t smem = SM::bytes();
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<(ne + EPB - 1) / EPB, 256, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
 template <int TYPE, typename T>
 static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   ElemArgs a = elem_args(eng, g, fp32);
@@ -904,17 +581,13 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
     elem_linear_kernel<TYPE, double><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
     return cudaGetLastError();
   }
-  constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 4;
-  const int threads = TYPE == B200FEM_ELEM_TET ? 256 : 192;
-  const int blocks = (ne + EPB - 1) / EPB;
-  if (g.mat_kind == B200FEM_MAT_NEOHOOKEAN) {
-    elem_nonlinear_kernel<TYPE, B200FEM_MAT_NEOHOOKEAN, false, T><<<blocks, threads, 0, eng.stream>>>(a);
-  } else if (g.nodal) {
-    elem_nonlinear_kernel<TYPE, B200FEM_MAT_MOONEYRIVLIN, true, T><<<blocks, threads, 0, eng.stream>>>(a);
-  } else {
-    elem_nonlinear_kernel<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T><<<blocks, threads, 0, eng.stream>>>(a);
-  }
-  return cudaGetLastError();
+  // elements per CTA: one thread per integration point in stage 1
+  constexpr int EPB_NH = TYPE == B200FEM_ELEM_TET ? 256 : 32;
+  constexpr int EPB_MR = TYPE == B200FEM_ELEM_TET ? 128 : 16;
+  if (g.mat_kind == B200FEM_MAT_NEOHOOKEAN)
+    return launch_nonlinear<TYPE, B200FEM_MAT_NEOHOOKEAN, false, T, EPB_NH>(a, ne, eng.stream);
+  if (g.nodal) return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, true, T, EPB_MR>(a, ne, eng.stream);
+  return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T, EPB_MR>(a, ne, eng.stream);
 }
 
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
@@ -984,69 +657,6 @@ cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs) {
   crs_export_kernel<<<(unsigned)((n9 + threads - 1) / threads), threads, 0, eng.stream>>>(d.nnzb, d.blk_row,
                                                                                          d.blk_rowptr, vals, crs);
   return cudaGetLastError();
-}
-
-cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero) {
-  DevPack& d = eng.d;
-  cudaError_t e;
-  if (init_zero) {
-    if ((e = cudaMemsetAsync(d.sol, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
-  }
-  if ((e = cudaMemsetAsync(d.unconv, 0, sizeof(int) * (size_t)(max_iter + 2), eng.stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(d.barrier, 0, 2 * sizeof(unsigned), eng.stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(d.p, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(d.q, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
-  PcgArgs a;
-  a.n_rows = d.n_rows;
-  a.rowptr = d.blk_rowptr;
-  a.col = d.blk_col;
-  a.blk_diag = d.blk_diag;
-  a.S = d.S;
-  a.Dinv = d.Dinv;
-  a.b = d.b;
-  a.x = d.sol;
-  a.r = d.r;
-  a.z = d.z;
-  a.p = d.p;
-  a.q = d.q;
-  a.piece_row = d.piece_row;
-  a.piece_model = d.piece_model;
-  a.model_piece = d.model_piece;
-  a.cta_piece = d.cta_piece;
-  a.partials = d.partials;
-  a.step = d.step;
-  a.model_out = d.model_scal;
-  a.barrier = d.barrier;
-  a.flags = d.flags;
-  a.unconv = d.unconv;
-  a.max_iter = max_iter;
-  a.update_state = update_state ? 1 : 0;
-  a.init_dinv = 1;
-  a.xpos = d.x;
-  a.vel = d.v;
-  a.act_node = d.act_node;
-  a.row_model = d.row_model;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(eng.pcg_grid);
-  cfg.blockDim = dim3(kPcgThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = eng.stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
-}
-
-int pcg_threads() { return kPcgThreads; }
-int pcg_max_cta_pieces() { return kMaxCtaPieces; }
-
-int pcg_max_grid(int device) {
-  int sms = 0, per_sm = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<double>, kPcgThreads, 0);
-  return sms * (per_sm > 0 ? per_sm : 1);
 }
 
 }  // namespace b200fem

@@ -1,0 +1,310 @@
+"""Benchmark: BackwardEuler steps/s of the NeoHookean hex beam (40x10x10
+hexes, 8 Gauss points, 4,961 nodes, 14,520 active DOF, PCG to 1e-10) on
+B200, next to the CPU oracle on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one BackwardEuler step (element kernel, block gather, RHS, PCG,
+state update) on device-resident state.  The model's working set (~30 MB)
+fits in L2, so a 256 MB buffer is written between timed steps to flush L2.
+Multi-GPU runs are independent replicas (one model per rank, weak scaling):
+the path has no cross-model exchange.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FEM BackwardEuler steps/s"
+UNIT = "steps/s"
+
+
+def algorithmic_bytes(wl, nnzb, n_active):
+    """Bytes per unit of work (per launch) used for the roofline.
+
+    assembly (element + gather + RHS kernels), one BackwardEuler system:
+      24 N (x read) + 4 nen E (connectivity) + 72 nip E (rest invJ0)
+      + 4 nen^2 E (scatter map) + 72 nnzb (S written) + 24 N (f / b)
+    PCG iteration:
+      76 nnzb (S + block column) + 4 (Na + 1) (row offsets)
+      + 24 Na (x) + 24 Na (y) + 72 Na (block-Jacobi inverse) + 9 * 24 Na
+    """
+    N = wl.rest.shape[0]
+    E = wl.conn.shape[0]
+    nen = wl.conn.shape[1]
+    nip = 8 if nen == 8 else 1
+    asm = 24 * N + 4 * nen * E + 72 * nip * E + 4 * nen * nen * E + 72 * nnzb + 24 * N
+    it = 76 * nnzb + 4 * (n_active + 1) + 48 * n_active + 72 * n_active + 9 * 24 * n_active
+    return asm, it
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n):
+    if n <= 1 or "RANK" not in os.environ:
+        return None, 0, 1, 0
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist, dist.get_rank(), dist.get_world_size(), local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_oracle_rate(wl, budget_s, threads, min_steps=2, max_steps=200):
+    """Times the CPU oracle (FP64 restatement of the Java path; Jacobi-PCG to
+    the workload tolerance) on the host: BackwardEuler steps/s."""
+    from oracle import oracle as O
+    O.build()
+    used = O.set_threads(threads)
+    om = O.OracleModel(wl.elem_type, wl.rest, wl.conn, wl.fixed, wl.material.kind, wl.material.params(),
+                       wl.density)
+    x = wl.rest.copy()
+    v = np.zeros_like(x)
+    fext = wl.fext if wl.traction is not None else None
+    om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=fext, tol=wl.tol)  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (n < min_steps or time.perf_counter() - t0 < budget_s):
+        st, _, _ = om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=fext, tol=wl.tol)
+        n += 1
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt, used
+
+
+def run_reference(args):
+    dist, rank, world, local = dist_setup(args.gpus)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    from artisynth_core_b200 import workloads as W
+    wl = W.neohookean_hex_beam().build_mesh()
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    O.build()
+    used = O.set_threads(threads)
+    om = O.OracleModel(wl.elem_type, wl.rest, wl.conn, wl.fixed, wl.material.kind, wl.material.params(),
+                       wl.density)
+    x = wl.rest.copy()
+    v = np.zeros_like(x)
+    for _ in range(args.warmup):
+        om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=wl.fext, tol=wl.tol)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=wl.fext, tol=wl.tol)
+    dt = time.perf_counter() - t0
+    val = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": dict(wl.describe(), solver="Jacobi-PCG 1e-10"),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": used, "kind": "port",
+                         "sample": f"{args.steps} full BackwardEuler steps of the 40x10x10 hex beam"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_b200(args):
+    import torch
+    dist, rank, world, local = dist_setup(args.gpus)
+    dev = local if dist is not None else 0
+    torch.cuda.set_device(dev)
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.femmodel import MechSystemSolver
+
+    wl = W.neohookean_hex_beam().build_mesh()
+    m = wl.model(device=dev)
+    sz = m.sizes()
+    ms = MechSystemSolver(m, tol=wl.tol, max_iter=20000)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+
+    for _ in range(args.warmup):
+        ms.backwardEuler(wl.h, 1)
+    # ---- timed region: device-resident state, L2 flushed between steps
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    asm_ms, pcg_ms, iters = 0.0, 0.0, []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms.backwardEuler(wl.h, 1)
+            a, s = ms.lastTiming()
+            asm_ms += a
+            pcg_ms += s
+            iters.append(ms.stats.iterations)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    step_ms = (asm_ms + pcg_ms) / args.steps
+    t = torch.tensor([step_ms], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms_max = float(t.item())
+    value = world * 1e3 / step_ms_max
+
+    # ---- end to end through the C ABI with host buffers: H2D state, step,
+    # D2H state, every step
+    x_h, v_h = m.getState()
+    e2e_steps = max(3, args.steps)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        m.setState(x_h, v_h)
+        ms.backwardEuler(wl.h, 1)
+        x_h, v_h = m.getState()
+    t1 = time.perf_counter()
+    e2e_ms = torch.tensor([1e3 * (t1 - t0) / e2e_steps], dtype=torch.float64, device=f"cuda:{dev}")
+    if dist is not None:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_val = world * 1e3 / float(e2e_ms.item())
+    state_bytes = 2 * 3 * wl.rest.shape[0] * 8
+
+    if rank == 0:
+        asm_b, it_b = algorithmic_bytes(wl, sz["nnzb"], sz["n_active"])
+        mean_it = float(np.mean(iters))
+        pcg_bytes = it_b * (mean_it + 2)  # iterations + the initial and final SpMV
+        asm_gbs = asm_b / (asm_ms / args.steps * 1e-3) / 1e9
+        pcg_gbs = pcg_bytes / (pcg_ms / args.steps * 1e-3) / 1e9
+        peak, kind = peaks()
+        dominant = "pcg_kernel" if pcg_ms >= asm_ms else "assembly (elem + gather + rows)"
+        achieved = pcg_gbs if pcg_ms >= asm_ms else asm_gbs
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(prof):
+            try:
+                traffic = json.load(open(prof)).get(dominant.split()[0])
+            except Exception:
+                traffic = None
+        cpu = None
+        if not args.no_cpu and world == 1:
+            rate, n, dt, used = cpu_oracle_rate(wl, args.cpu_budget, os.cpu_count() or 1)
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+                   "sample": f"{n} BackwardEuler steps of the 40x10x10 hex beam in {dt:.1f} s "
+                             f"(FP64 oracle, Jacobi-PCG 1e-10, OpenMP)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(wl.describe(), parallelism=f"replicas{world}", l2="flushed between steps (256 MB write)",
+                           tol=wl.tol, nnzb=sz["nnzb"], active_dof=3 * sz["n_active"]),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": 4 * args.steps,
+            "phases_ms_per_step": {"assembly": asm_ms / args.steps, "pcg": pcg_ms / args.steps,
+                                   "pcg_iterations": mean_it},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
+                         "bytes_per_launch": pcg_bytes if pcg_ms >= asm_ms else asm_b,
+                         "assembly_gbs": asm_gbs, "pcg_gbs": pcg_gbs},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    m._invalidate()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()
