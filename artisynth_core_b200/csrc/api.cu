@@ -17,6 +17,9 @@ namespace b200fem {
 cudaError_t launch_forces_only(Engine& eng);
 int pcg_max_grid(int device);
 int pcg_max_cta_pieces();
+void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached);
+cudaError_t prepare_pcg(Engine& eng);
+cudaError_t prepare_kernels(Engine& eng);
 
 namespace {
 
@@ -64,6 +67,13 @@ cudaError_t upload(Engine& eng, T** ptr, const std::vector<T>& v) {
 }  // namespace
 
 void free_pack(Engine& eng) {
+  for (cudaGraphExec_t* ex : {&eng.asm_exec, &eng.step_exec})
+    if (*ex) {
+      cudaGraphExecDestroy(*ex);
+      *ex = nullptr;
+    }
+  eng.step_exec_max_iter = -1;
+  eng.last_step_params.clear();
   for (void* p : eng.allocations) cudaFree(p);
   eng.allocations.clear();
   eng.d = DevPack();
@@ -279,6 +289,14 @@ int build_pack(Engine& eng) {
   for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
   eng.pcg_grid = G;
   d.n_pieces = (int)piece_model.size();
+  eng.pcg_nloc_max = 0;
+  eng.pcg_nb_max = 0;
+  for (int c = 0; c < G; c++) {
+    int ra = piece_row[cta_piece[c]], rb = piece_row[cta_piece[c + 1]];
+    eng.pcg_nloc_max = std::max(eng.pcg_nloc_max, rb - ra);
+    eng.pcg_nb_max = std::max(eng.pcg_nb_max, rowptr[rb] - rowptr[ra]);
+  }
+  pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached);
 
   // ---- device upload
   CK(upload(eng, &d.x, x));
@@ -347,6 +365,8 @@ int build_pack(Engine& eng) {
   eng.h_col = col;
   eng.h_sidx = sidx;
   eng.h_mass = mass;
+  CK(prepare_kernels(eng));
+  CK(prepare_pcg(eng));
   eng.built = true;
   return B200FEM_OK;
 }
@@ -425,6 +445,7 @@ int b200fem_destroy(b200fem_handle h) {
   free_pack(h->eng);
   for (auto& ev : h->eng.ev)
     if (ev) cudaEventDestroy(ev);
+
   for (auto& ev : h->eng.ev_pool) cudaEventDestroy(ev);
   if (h->eng.stream) cudaStreamDestroy(h->eng.stream);
   delete h;
@@ -641,7 +662,7 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
   NEED_BUILT();
   DevPack& d = eng.d;
   if (x) CK(cudaMemcpyAsync(d.x, x, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyHostToDevice, eng.stream));
-  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  CK(launch_reset_status(eng));
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   CK(launch_assemble(eng, 1.0, 0.0, true));
   CK(launch_forces_only(eng));
@@ -661,7 +682,7 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
   CK(cudaMemcpyAsync(&dmin, d.dmin, sizeof(dmin), cudaMemcpyDeviceToHost, eng.stream));
   CK(cudaStreamSynchronize(eng.stream));
   float ms = 0;
-  cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]);
+  CK(cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]));
   eng.last_asm_ms = ms;
   eng.last_solve_ms = 0;
   eng.last_stats.num_inverted = flags[1];
@@ -721,19 +742,54 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
     s[6] = p->tol;
     s[7] = 0;
   }
-  CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
-  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
-  while ((int)eng.ev_pool.size() < 3 * nsteps) {
+  if (step != eng.last_step_params) {
+    CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
+    eng.last_step_params = step;
+  }
+  CK(launch_reset_status(eng));
+  const bool graphs = eng.use_graphs && !p->abort_on_inverted;
+  if (graphs && (eng.asm_exec == nullptr || eng.step_exec == nullptr || eng.step_exec_max_iter != max_iter)) {
+    // two captured graphs per step -- assembly (element kernels, block
+    // gather, RHS) and solve (PCG) -- so stream events between the graph
+    // launches time each phase
+    for (cudaGraphExec_t* ex : {&eng.asm_exec, &eng.step_exec})
+      if (*ex) {
+        cudaGraphExecDestroy(*ex);
+        *ex = nullptr;
+      }
+    for (int g = 0; g < 2; g++) {
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(eng.stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t ce;
+      if (g == 0) {
+        ce = launch_assemble(eng, 0, 0, false);
+        if (ce == cudaSuccess) ce = launch_rhs(eng);
+      } else {
+        ce = launch_pcg(eng, max_iter, true, 0);
+      }
+      cudaError_t ee = cudaStreamEndCapture(eng.stream, &graph);
+      if (ce != cudaSuccess) return cuda_fail(&eng, ce, "capture of the BackwardEuler step");
+      if (ee != cudaSuccess) return cuda_fail(&eng, ee, "cudaStreamEndCapture");
+      ce = cudaGraphInstantiate(g == 0 ? &eng.asm_exec : &eng.step_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return cuda_fail(&eng, ce, "cudaGraphInstantiate");
+    }
+    eng.step_exec_max_iter = max_iter;
+  }
+  while ((int)eng.ev_pool.size() < 3) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
     eng.ev_pool.push_back(e);
   }
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   for (int s = 0; s < nsteps; s++) {
-    CK(cudaEventRecord(eng.ev_pool[3 * s], eng.stream));
-    CK(launch_assemble(eng, 0, 0, false));
-    CK(launch_rhs(eng));
-    CK(cudaEventRecord(eng.ev_pool[3 * s + 1], eng.stream));
+    CK(cudaEventRecord(eng.ev_pool[0], eng.stream));
+    if (graphs) CK(cudaGraphLaunch(eng.asm_exec, eng.stream));
+    else {
+      CK(launch_assemble(eng, 0, 0, false));
+      CK(launch_rhs(eng));
+    }
+    CK(cudaEventRecord(eng.ev_pool[1], eng.stream));
     if (p->abort_on_inverted) {
       int flags[4];
       CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
@@ -741,24 +797,24 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
       if (flags[1] > 0)
         return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
     }
-    CK(launch_pcg(eng, max_iter, true, 0));
-    CK(cudaEventRecord(eng.ev_pool[3 * s + 2], eng.stream));
+    if (graphs) CK(cudaGraphLaunch(eng.step_exec, eng.stream));
+    else CK(launch_pcg(eng, max_iter, true, 0));
+    CK(cudaEventRecord(eng.ev_pool[2], eng.stream));
   }
   CK(cudaEventRecord(eng.ev[1], eng.stream));
   eng.have_matrix = true;
   int st = read_step_status(eng, stats, max_iter);
-  // device time of the assembly (element, gather, RHS kernels) and of the
-  // PCG launches, summed over the steps of this call
-  double asm_ms = 0, pcg_ms = 0;
-  for (int s = 0; s < nsteps; s++) {
-    float a = 0, b = 0;
-    cudaEventElapsedTime(&a, eng.ev_pool[3 * s], eng.ev_pool[3 * s + 1]);
-    cudaEventElapsedTime(&b, eng.ev_pool[3 * s + 1], eng.ev_pool[3 * s + 2]);
-    asm_ms += a;
-    pcg_ms += b;
+  // device time of the last step's assembly (element, gather, RHS kernels)
+  // and PCG phases, and of the whole call
+  float a = 0, b = 0, t = 0;
+  if (nsteps > 0) {
+    CK(cudaEventElapsedTime(&a, eng.ev_pool[0], eng.ev_pool[1]));
+    CK(cudaEventElapsedTime(&b, eng.ev_pool[1], eng.ev_pool[2]));
   }
-  eng.last_asm_ms = (float)asm_ms;
-  eng.last_solve_ms = (float)pcg_ms;
+  CK(cudaEventElapsedTime(&t, eng.ev[0], eng.ev[1]));
+  eng.last_asm_ms = a;
+  eng.last_solve_ms = b;
+  eng.last_call_ms = t;
   return st;
 }
 
@@ -789,7 +845,7 @@ int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, 
   CK(cudaMemcpyAsync(d.step, step.data(), step.size() * sizeof(double), cudaMemcpyHostToDevice, eng.stream));
   CK(cudaMemcpyAsync(d.b, b, n, cudaMemcpyHostToDevice, eng.stream));
   CK(cudaMemcpyAsync(d.sol, x, n, cudaMemcpyHostToDevice, eng.stream));
-  CK(cudaMemsetAsync(d.flags, 0, 4 * sizeof(int), eng.stream));
+  CK(launch_reset_status(eng));
   CK(launch_pcg(eng, max_iter, false, 0));
   CK(cudaMemcpyAsync(x, d.sol, n, cudaMemcpyDeviceToHost, eng.stream));
   return read_step_status(eng, stats, max_iter);

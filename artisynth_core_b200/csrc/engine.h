@@ -166,8 +166,16 @@ struct Engine {
   std::vector<double> h_mass;
   // pcg launch geometry
   int pcg_grid = 0, pcg_block = 256;
+  int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
+  int pcg_attr_smem = -1;
+  // captured BackwardEuler step (element, gather, RHS, PCG) and its events
+  cudaGraphExec_t asm_exec = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  int step_exec_max_iter = -1;
+  bool use_graphs = true;
   // last timing
-  float last_asm_ms = 0, last_solve_ms = 0;
+  float last_asm_ms = 0, last_solve_ms = 0, last_call_ms = 0;
+  std::vector<double> last_step_params;
   b200fem_stats last_stats{};
   std::vector<void*> allocations;
 };
@@ -185,6 +193,7 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 // kernels.cu
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K);
 cudaError_t launch_rhs(Engine& eng);
+cudaError_t launch_reset_status(Engine& eng);
 cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero);
 cudaError_t launch_spmv(Engine& eng, const double* x, double* y);
 cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs);

@@ -564,8 +564,15 @@ static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) 
   using SM = ElemSmem<TYPE, MAT, T, EPB>;
   auto kern = elem_nonlinear_kernel<TYPE, MAT, NODAL, T, EPB>;
   const size_t smem = SM::bytes();
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  // the opt-in size is a per-function attribute: set it once per process
+  // (it is not a stream operation, so it must not run inside graph capture)
+  static bool attr_set = false;
+  if (ne < 0) {  // preparation call (outside any stream capture)
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) attr_set = true;
+    return e;
+  }
+  if (!attr_set) return cudaErrorInvalidConfiguration;
   kern<<<(ne + EPB - 1) / EPB, 256, smem, st>>>(a);
   return cudaGetLastError();
 }
@@ -574,8 +581,9 @@ template <int TYPE, typename T>
 static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   ElemArgs a = elem_args(eng, g, fp32);
   int ne = g.e1 - g.e0;
-  if (ne <= 0) return cudaSuccess;
+  if (ne == 0) return cudaSuccess;
   if (g.mat_kind == B200FEM_MAT_LINEAR) {
+    if (ne < 0) return cudaSuccess;
     constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 8;
     a.elemK = (void*)eng.d.elemK;  // linear path stays FP64
     elem_linear_kernel<TYPE, double><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
@@ -590,17 +598,28 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T, EPB_MR>(a, ne, eng.stream);
 }
 
+// One-time preparation before any stream capture: constant tables and the
+// shared-memory opt-in of every element kernel this pack launches.
+cudaError_t prepare_kernels(Engine& eng) {
+  cudaError_t e = ensure_constants(eng.device);
+  if (e != cudaSuccess) return e;
+  const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  for (ElemGroup g : eng.groups) {
+    g.e1 = g.e0 - 1;  // ne = -1: set attributes only
+    if (g.elem_type == B200FEM_ELEM_TET)
+      e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);
+    else
+      e = fp32 ? launch_group<B200FEM_ELEM_HEX, float>(eng, g, true) : launch_group<B200FEM_ELEM_HEX, double>(eng, g, false);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   (void)cK;
   (void)cM;
-  cudaError_t e = ensure_constants(eng.device);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
   DevPack& d = eng.d;
-  // reset inverted-element counter and min detJ
-  if ((e = cudaMemsetAsync(d.flags + 1, 0, sizeof(int), eng.stream)) != cudaSuccess) return e;
-  long long big = 0x7fefffffffffffffll;  // ordered bits of DBL_MAX
-  if ((e = cudaMemcpyAsync(d.dmin, &big, sizeof(long long), cudaMemcpyHostToDevice, eng.stream)) != cudaSuccess)
-    return e;
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
   for (const ElemGroup& g : eng.groups) {
     if (g.elem_type == B200FEM_ELEM_TET)
@@ -621,6 +640,18 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
         d.step, 1, d.S);
   }
+  return cudaGetLastError();
+}
+
+// per-call reset of the status words: error, inverted-element count, and
+// the smallest detJ (ordered-bits image of DBL_MAX)
+__global__ void reset_status_kernel(int* flags, long long* dmin) {
+  if (threadIdx.x < 4) flags[threadIdx.x] = 0;
+  if (threadIdx.x == 0) *dmin = 0x7fefffffffffffffll;
+}
+
+cudaError_t launch_reset_status(Engine& eng) {
+  reset_status_kernel<<<1, 32, 0, eng.stream>>>(eng.d.flags, (long long*)eng.d.dmin);
   return cudaGetLastError();
 }
 

@@ -97,6 +97,10 @@ struct PcgArgs {
   double* partials;  // [2][n_pieces][4]
   const double* step;
   double* model_out;  // n_models * 4: iterations, true rel residual, converged
+  int resident;       // row-local vectors and Dinv live in shared memory
+  int cached;         // the CTA's slice of S (values, columns, row offsets) is copied to shared memory
+  int nloc_max;       // max rows of one CTA
+  int nb_max;         // max blocks of one CTA
   unsigned* barrier;
   int* flags;
   int* unconv;  // per iteration: some model still unconverged
@@ -213,6 +217,97 @@ __device__ __forceinline__ double dot3(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
 
+// Row-local PCG state: the vectors x r u w z q s p and the block-Jacobi
+// inverse of the CTA's own rows.  In resident mode they live in shared
+// memory for the whole solve (only the owning CTA ever touches them); the
+// search-direction vectors read by neighbouring rows (u at the start, m in
+// the iteration, x for the true residual) are published to global memory.
+struct RowState {
+  double* v[9];
+  double* D;
+  int r0;
+  int res;
+  __device__ __forceinline__ double* at(int k, int row) const {
+    return res ? v[k] + 3 * (row - r0) : v[k] + 3 * (size_t)row;
+  }
+  __device__ __forceinline__ double* dinv(int row) const {
+    return res ? D + 9 * (row - r0) : D + 9 * (size_t)row;
+  }
+};
+enum { VX = 0, VR, VU, VW, VZ, VQ, VS, VP, VM };
+
+// The CTA's rows [r0, r1) own the contiguous block range [pbase, pend):
+// when it fits, the values, block columns and row offsets are copied to
+// shared memory once per solve and every SpMV of the solve reads them there.
+template <typename MT>
+struct MatView {
+  const int* rowptr;
+  const int* col;
+  const MT* S;
+  const int* ro_s;
+  const int* col_s;
+  const MT* S_s;
+  int r0;
+  int cached;
+};
+
+template <typename MT>
+__device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int row, const double* __restrict__ x,
+                                              int lane, double* y) {
+  int p0, p1;
+  const int* col;
+  const MT* S;
+  if (mv.cached) {
+    p0 = mv.ro_s[row - mv.r0];
+    p1 = mv.ro_s[row - mv.r0 + 1];
+    col = mv.col_s;
+    S = mv.S_s;
+  } else {
+    p0 = mv.rowptr[row];
+    p1 = mv.rowptr[row + 1];
+    col = mv.col;
+    S = mv.S;
+  }
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int p = p0 + lane; p < p1; p += 32) {
+    const int c = col[p];
+    const MT* B = S + (size_t)p * 9;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+    const double x0 = x[3 * (size_t)c], x1 = x[3 * (size_t)c + 1], x2 = x[3 * (size_t)c + 2];
+    a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+    a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+    a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+  }
+  y[0] = a0;
+  y[1] = a1;
+  y[2] = a2;
+}
+
+// dynamic shared memory layout of the PCG kernel
+__host__ __device__ inline size_t pcg_align16(size_t b) { return (b + 15) & ~(size_t)15; }
+template <typename MT>
+__host__ __device__ inline void pcg_smem_layout(int nloc_max, int nb_max, int res, int cached, size_t* off_vec,
+                                                size_t* off_ro, size_t* off_col, size_t* off_S, size_t* total) {
+  size_t o = 0;
+  *off_vec = o;
+  if (res) o += pcg_align16(sizeof(double) * (size_t)nloc_max * (9 * 3 + 9));
+  *off_ro = o;
+  if (cached) o += pcg_align16(sizeof(int) * (size_t)(nloc_max + 1));
+  *off_col = o;
+  if (cached) o += pcg_align16(sizeof(int) * (size_t)nb_max);
+  *off_S = o;
+  if (cached) o += pcg_align16(sizeof(MT) * (size_t)nb_max * 9);
+  *total = o;
+}
+
 template <typename MT>
 __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   __shared__ double rowbuf[kRowChunk][3];
@@ -223,19 +318,60 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       s_beta[kMaxCtaPieces], s_gold[kMaxCtaPieces], s_aold[kMaxCtaPieces];
   __shared__ int s_conv[kMaxCtaPieces], s_iters[kMaxCtaPieces], s_first[kMaxCtaPieces];
   __shared__ int s_restart;
-  const MT* S = (const MT*)a.S;
+  extern __shared__ __align__(16) unsigned char dyn[];
   CtaView cv{a.cta_piece[blockIdx.x], a.cta_piece[blockIdx.x + 1]};
   const int npc = cv.pc1 - cv.pc0;
+  const int r0 = a.piece_row[cv.pc0], r1 = a.piece_row[cv.pc1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ph = 0;
 
-  // ---- P0: block-Jacobi inverse, r = b - S x, u = Dinv r, ||b||^2
+  size_t off_vec, off_ro, off_col, off_S, total;
+  pcg_smem_layout<MT>(a.nloc_max, a.nb_max, a.resident, a.cached, &off_vec, &off_ro, &off_col, &off_S, &total);
+  RowState st;
+  st.r0 = r0;
+  st.res = a.resident;
+  if (a.resident) {
+    double* base = (double*)(dyn + off_vec);
+    for (int k = 0; k < 9; k++) st.v[k] = base + (size_t)k * a.nloc_max * 3;
+    st.D = base + (size_t)9 * a.nloc_max * 3;
+  } else {
+    st.v[VX] = a.x; st.v[VR] = a.r; st.v[VU] = a.u; st.v[VW] = a.w;
+    st.v[VZ] = a.z; st.v[VQ] = a.q; st.v[VS] = a.s; st.v[VP] = a.p;
+    st.v[VM] = nullptr;  // m is read from the published buffer
+    st.D = a.Dinv;
+  }
+  MatView<MT> mv;
+  mv.rowptr = a.rowptr;
+  mv.col = a.col;
+  mv.S = (const MT*)a.S;
+  mv.r0 = r0;
+  mv.cached = a.cached;
+  mv.ro_s = (const int*)(dyn + off_ro);
+  mv.col_s = (const int*)(dyn + off_col);
+  mv.S_s = (const MT*)(dyn + off_S);
+  const int pbase = a.rowptr[r0];
+  if (a.cached) {
+    const int nb = a.rowptr[r1] - pbase;
+    int* ro = (int*)(dyn + off_ro);
+    int* cs = (int*)(dyn + off_col);
+    MT* Ss = (MT*)(dyn + off_S);
+    for (int i = threadIdx.x; i <= r1 - r0; i += blockDim.x) ro[i] = a.rowptr[r0 + i] - pbase;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) cs[i] = a.col[pbase + i];
+    const MT* Sg = (const MT*)a.S + (size_t)pbase * 9;
+    for (int i = threadIdx.x; i < nb * 9; i += blockDim.x) Ss[i] = Sg[i];
+  }
   if (blockIdx.x == 0)
     for (int i = threadIdx.x; i <= a.max_iter + 1; i += blockDim.x) a.unconv[i] = 0;
-  cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+  __syncthreads();
+
+  // ---- P0: block-Jacobi inverse, r = b - S x0, u = Dinv r (published to
+  // m1 for the next SpMV), ||b||^2
+  cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
     double Ax[3];
-    warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
-    if (lane == 0) {
-      const MT* Db = S + (size_t)a.blk_diag[row] * 9;
+    view_row_spmv<MT>(mv, row, a.x, ln, Ax);
+    if (ln == 0) {
+      const MT* Db = (const MT*)a.S + (size_t)a.blk_diag[row] * 9;
+      if (a.cached) Db = mv.S_s + (size_t)(a.blk_diag[row] - pbase) * 9;
       double d[9], inv[9];
 #pragma unroll
       for (int i = 0; i < 9; i++) d[i] = (double)Db[i];
@@ -244,15 +380,19 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
 #pragma unroll
         for (int i = 0; i < 9; i++) inv[i] = 0;
       }
+      double* D = st.dinv(row);
 #pragma unroll
-      for (int i = 0; i < 9; i++) a.Dinv[(size_t)row * 9 + i] = inv[i];
-      double bv[3], r[3], u[3];
+      for (int i = 0; i < 9; i++) D[i] = inv[i];
+      double bv[3], r[3], u[3], x0[3];
       load3(bv, a.b, row);
+      load3(x0, a.x, row);
 #pragma unroll
       for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
       mul33(u, inv, r);
-      store3(a.r, row, r);
-      store3(a.u, row, u);
+      store3(st.at(VR, row), 0, r);
+      store3(st.at(VU, row), 0, u);
+      if (a.resident) store3(st.at(VX, row), 0, x0);
+      store3(a.m1, row, u);
       vals[0] = dot3(bv, bv);
     }
   });
@@ -269,23 +409,24 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
 
   int total_it = 0;
   for (int restart = 0;; restart++) {
-    // ---- P1: w = S u, m = Dinv w; dots gamma = r.u, delta = w.u, rho = r.r
+    // ---- P1: w = S u, m = Dinv w (published to m0); dots r.u, w.u, r.r
     for (int j = threadIdx.x; j < npc; j += blockDim.x) s_first[j] = 1;
-    cta_row_pass<3, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+    cta_row_pass<3, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
       if (s_conv[piece_of_row(a, cv, row)]) return;
       double Au[3];
-      warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.u, lane, Au);
-      if (lane == 0) {
+      view_row_spmv<MT>(mv, row, a.m1, ln, Au);
+      if (ln == 0) {
         double r[3], u[3], m[3], zero[3] = {0, 0, 0};
-        load3(r, a.r, row);
-        load3(u, a.u, row);
-        mul33(m, a.Dinv + (size_t)row * 9, Au);
-        store3(a.w, row, Au);
+        load3(r, st.at(VR, row), 0);
+        load3(u, st.at(VU, row), 0);
+        mul33(m, st.dinv(row), Au);
+        store3(st.at(VW, row), 0, Au);
         store3(a.m0, row, m);
-        store3(a.z, row, zero);
-        store3(a.q, row, zero);
-        store3(a.s, row, zero);
-        store3(a.p, row, zero);
+        if (a.resident) store3(st.at(VM, row), 0, m);
+        store3(st.at(VZ, row), 0, zero);
+        store3(st.at(VQ, row), 0, zero);
+        store3(st.at(VS, row), 0, zero);
+        store3(st.at(VP, row), 0, zero);
         vals[0] = dot3(r, u);
         vals[1] = dot3(Au, u);
         vals[2] = dot3(r, r);
@@ -302,8 +443,6 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       // runs on the first warps while the last warps reduce the scalars.
       const int nsumw = min(max(npc, 1), 8);
       const int nroww = (blockDim.x >> 5) - nsumw;
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      const int r0 = a.piece_row[cv.pc0], r1 = a.piece_row[cv.pc1];
       for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
       bool stop = false;
       for (int c0 = r0, first = 1; c0 < r1 || first; c0 += kRowChunk, first = 0) {
@@ -311,7 +450,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         if (warp < nroww) {
           for (int row = c0 + warp; row < c1; row += nroww) {
             double n[3];
-            warp_row_spmv<MT>(row, a.rowptr, a.col, S, mc, lane, n);
+            view_row_spmv<MT>(mv, row, mc, lane, n);
             if (lane == 0) {
               sn[row - c0][0] = n[0];
               sn[row - c0][1] = n[1];
@@ -319,6 +458,8 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             }
           }
         } else if (first) {
+          // reduce this iteration's scalars and form alpha, beta; the
+          // convergence test is on the recurrence residual
           const int sw = warp - nroww;
           const double* src = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
           for (int j = sw; j < npc; j += nsumw) {
@@ -332,44 +473,33 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             for (int k = 0; k < 3; k++)
 #pragma unroll
               for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
-            if (lane == 0) {
-              sums[j][0] = sm[0];
-              sums[j][1] = sm[1];
-              sums[j][2] = sm[2];
+            if (lane == 0 && !s_conv[j]) {
+              const double gam = sm[0], del = sm[1], rho = sm[2];
+              if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
+                s_conv[j] = 1;
+              } else {
+                double beta = 0, alpha;
+                if (s_first[j]) {
+                  alpha = gam / del;
+                  s_first[j] = 0;
+                } else {
+                  beta = gam / s_gold[j];
+                  alpha = gam / (del - beta * gam / s_aold[j]);
+                }
+                s_beta[j] = beta;
+                s_alpha[j] = alpha;
+                s_gold[j] = gam;
+                s_aold[j] = alpha;
+                s_iters[j]++;
+                if (cv.pc0 + j == a.model_piece[m + 1] - 1) a.unconv[idx] = 1;
+              }
             }
           }
         }
         __syncthreads();
-        if (first) {
-          // scalars; convergence on the recurrence residual
-          for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-            if (s_conv[j]) continue;
-            const double gam = sums[j][0], del = sums[j][1], rho = sums[j][2];
-            if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
-              s_conv[j] = 1;
-              continue;
-            }
-            double beta = 0, alpha;
-            if (s_first[j]) {
-              alpha = gam / del;
-              s_first[j] = 0;
-            } else {
-              beta = gam / s_gold[j];
-              alpha = gam / (del - beta * gam / s_aold[j]);
-            }
-            s_beta[j] = beta;
-            s_alpha[j] = alpha;
-            s_gold[j] = gam;
-            s_aold[j] = alpha;
-            s_iters[j]++;
-            const int m = a.piece_model[cv.pc0 + j];
-            if (cv.pc0 + j == a.model_piece[m + 1] - 1) a.unconv[idx] = 1;
-          }
-          __syncthreads();
-          if (idx >= a.max_iter) {
-            stop = true;
-            break;
-          }
+        if (first && idx >= a.max_iter) {
+          stop = true;
+          break;
         }
         // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
         // x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
@@ -378,40 +508,40 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           double v3[3] = {0, 0, 0};
           if (!s_conv[j]) {
             const double al = s_alpha[j], be = s_beta[j];
-            double x[3], r[3], u[3], w[3], z[3], q[3], sv[3], p[3], mm[3], D[9];
-            load3(x, a.x, row);
-            load3(r, a.r, row);
-            load3(u, a.u, row);
-            load3(w, a.w, row);
-            load3(z, a.z, row);
-            load3(q, a.q, row);
-            load3(sv, a.s, row);
-            load3(p, a.p, row);
-            load3(mm, mc, row);
-#pragma unroll
-            for (int i = 0; i < 9; i++) D[i] = a.Dinv[(size_t)row * 9 + i];
+            double* px = st.at(VX, row);
+            double* pr = st.at(VR, row);
+            double* pu = st.at(VU, row);
+            double* pw = st.at(VW, row);
+            double* pz = st.at(VZ, row);
+            double* pq = st.at(VQ, row);
+            double* ps = st.at(VS, row);
+            double* pp = st.at(VP, row);
+            const double* D = st.dinv(row);
+            double mm[3], w[3], r[3], u[3];
+            if (a.resident) load3(mm, st.at(VM, row), 0);
+            else load3(mm, mc, row);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-              z[c] = sn[row - c0][c] + be * z[c];
-              q[c] = mm[c] + be * q[c];
-              sv[c] = w[c] + be * sv[c];
-              p[c] = u[c] + be * p[c];
-              x[c] += al * p[c];
-              r[c] -= al * sv[c];
-              u[c] -= al * q[c];
-              w[c] -= al * z[c];
+              const double z = sn[row - c0][c] + be * pz[c];
+              const double q = mm[c] + be * pq[c];
+              const double sv = pw[c] + be * ps[c];
+              const double p = pu[c] + be * pp[c];
+              px[c] += al * p;
+              r[c] = pr[c] - al * sv;
+              u[c] = pu[c] - al * q;
+              w[c] = pw[c] - al * z;
+              pz[c] = z;
+              pq[c] = q;
+              ps[c] = sv;
+              pp[c] = p;
+              pr[c] = r[c];
+              pu[c] = u[c];
+              pw[c] = w[c];
             }
             double mnew[3];
             mul33(mnew, D, w);
-            store3(a.x, row, x);
-            store3(a.r, row, r);
-            store3(a.u, row, u);
-            store3(a.w, row, w);
-            store3(a.z, row, z);
-            store3(a.q, row, q);
-            store3(a.s, row, sv);
-            store3(a.p, row, p);
             store3(mn, row, mnew);
+            if (a.resident) store3(st.at(VM, row), 0, mnew);
             v3[0] = dot3(r, u);
             v3[1] = dot3(w, u);
             v3[2] = dot3(r, r);
@@ -421,6 +551,23 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           rowbuf[row - c0][2] = v3[2];
         }
         __syncthreads();
+        if (npc == 1 && c1 - c0 <= 32) {
+          // one piece, one warp of rows: reduce in warp 0 without a second pass
+          if (warp == 0) {
+            double sm[3] = {0, 0, 0};
+            if (c0 + lane < c1)
+#pragma unroll
+              for (int k = 0; k < 3; k++) sm[k] = rowbuf[lane][k];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+            if (lane == 0)
+#pragma unroll
+              for (int k = 0; k < 3; k++) pacc[0][k] += sm[k];
+          }
+          continue;
+        }
         for (int j = warp; j < npc; j += (blockDim.x >> 5)) {
           const int pr0 = max(a.piece_row[cv.pc0 + j], c0), pr1 = min(a.piece_row[cv.pc0 + j + 1], c1);
           if (pr0 >= pr1) continue;
@@ -458,12 +605,15 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     }
     ph++;
 
-    // ---- true residual r = b - S x; restart from it when it misses the
-    // tolerance although the recurrence converged
-    cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int lane, double* vals) {
+    // ---- publish x, then the true residual r = b - S x; restart from it
+    // when it misses the tolerance although the recurrence converged
+    if (a.resident)
+      for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) store3(a.x, row, st.at(VX, row));
+    if (!grid_barrier(a.barrier, a.flags)) return;
+    cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
       double Ax[3];
-      warp_row_spmv<MT>(row, a.rowptr, a.col, S, a.x, lane, Ax);
-      if (lane == 0) {
+      view_row_spmv<MT>(mv, row, a.x, ln, Ax);
+      if (ln == 0) {
         double bv[3], r[3];
         load3(bv, a.b, row);
 #pragma unroll
@@ -471,9 +621,10 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         vals[0] = dot3(r, r);
         if (!s_conv[piece_of_row(a, cv, row)]) return;
         double u[3];
-        mul33(u, a.Dinv + (size_t)row * 9, r);
-        store3(a.r, row, r);
-        store3(a.u, row, u);
+        mul33(u, st.dinv(row), r);
+        store3(st.at(VR, row), 0, r);
+        store3(st.at(VU, row), 0, u);
+        store3(a.m1, row, u);
       }
     });
     if (!grid_barrier(a.barrier, a.flags)) return;
@@ -504,7 +655,6 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   }
 
   if (a.update_state) {
-    const int r0 = a.piece_row[cv.pc0], r1 = a.piece_row[cv.pc1];
     for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
       const int n = a.act_node[row];
       const double h = a.step[(size_t)a.row_model[row] * 8];
@@ -560,10 +710,17 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.vel = d.v;
   a.act_node = d.act_node;
   a.row_model = d.row_model;
+  a.resident = eng.pcg_resident;
+  a.cached = eng.pcg_cached;
+  a.nloc_max = eng.pcg_nloc_max;
+  a.nb_max = eng.pcg_nb_max;
+  size_t ov, oro, oc, oS, total;
+  pcg_smem_layout<double>(a.nloc_max, a.nb_max, a.resident, a.cached, &ov, &oro, &oc, &oS, &total);
+  if ((int)total > eng.pcg_attr_smem) return cudaErrorInvalidConfiguration;  // prepare_pcg not run
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(eng.pcg_grid);
   cfg.blockDim = dim3(kPcgThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = total;
   cfg.stream = eng.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -574,6 +731,33 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
 }
 
 int pcg_threads() { return kPcgThreads; }
+
+cudaError_t prepare_pcg(Engine& eng) {
+  size_t ov, oro, oc, oS, total;
+  pcg_smem_layout<double>(eng.pcg_nloc_max, eng.pcg_nb_max, eng.pcg_resident, eng.pcg_cached, &ov, &oro, &oc, &oS,
+                          &total);
+  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
+  if (e == cudaSuccess) eng.pcg_attr_smem = (int)total;
+  return e;
+}
+
+// Decide shared-memory residency of the PCG row state and of the S slice
+// for the given per-CTA maxima (rows, blocks) within the device's opt-in
+// shared memory per block.
+void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached) {
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaFuncAttributes fa;
+  cudaFuncGetAttributes(&fa, pcg_kernel<double>);
+  const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
+  size_t ov, oro, oc, oS, total;
+  *resident = 0;
+  *cached = 0;
+  pcg_smem_layout<double>(nloc_max, nb_max, 1, 0, &ov, &oro, &oc, &oS, &total);
+  if ((long long)total <= budget) *resident = 1;
+  pcg_smem_layout<double>(nloc_max, nb_max, *resident, 1, &ov, &oro, &oc, &oS, &total);
+  if ((long long)total <= budget) *cached = 1;
+}
 int pcg_max_cta_pieces() { return kMaxCtaPieces; }
 
 int pcg_max_grid(int device) {
