@@ -119,6 +119,8 @@ def lib():
         "b200fem_spmv": ([H, _dp, _dp], ctypes.c_int),
         "b200fem_pcg_solve": ([H, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_last_timing": ([H, _dp, _dp], ctypes.c_int),
+        "b200fem_pcg_solve_noalloc": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
+                                       _ip, _dp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name, None)

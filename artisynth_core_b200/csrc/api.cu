@@ -20,6 +20,8 @@ int pcg_max_cta_pieces();
 void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached);
 cudaError_t prepare_pcg(Engine& eng);
 cudaError_t prepare_kernels(Engine& eng);
+int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const double* vals, const double* b, double* x,
+                      double tol, int max_iter, void* stream, int* iterations, double* rel_residual, const char** err);
 
 namespace {
 
@@ -849,6 +851,15 @@ int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, 
   CK(launch_pcg(eng, max_iter, false, 0));
   CK(cudaMemcpyAsync(x, d.sol, n, cudaMemcpyDeviceToHost, eng.stream));
   return read_step_status(eng, stats, max_iter);
+}
+
+int b200fem_pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const double* vals, const double* b,
+                              double* x, double tol, int max_iter, void* stream, int* iterations,
+                              double* rel_residual) {
+  const char* err = "";
+  int st = pcg_solve_noalloc(n_rows, rowptr, col, vals, b, x, tol, max_iter, stream, iterations, rel_residual, &err);
+  if (st != B200FEM_OK) set_global_error(std::string("b200fem_pcg_solve_noalloc: ") + err);
+  return st;
 }
 
 int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms) {

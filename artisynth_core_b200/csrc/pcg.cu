@@ -17,6 +17,8 @@
 // barrier: results are bit-reproducible and independent of timing.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "device_math.cuh"
 #include "engine.h"
 #include "spmv.cuh"
@@ -732,11 +734,26 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
 
 int pcg_threads() { return kPcgThreads; }
 
+// The dynamic shared-memory opt-in of pcg_kernel is process-wide per
+// function: raise it monotonically so one caller never lowers it below what
+// another needs.
+static std::mutex g_pcg_attr_mu;
+static int g_pcg_attr_bytes[64] = {0};
+
+static cudaError_t ensure_pcg_smem(int device, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_pcg_attr_mu);
+  const int d = (device >= 0 && device < 64) ? device : 0;
+  if ((int)bytes <= g_pcg_attr_bytes[d]) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) g_pcg_attr_bytes[d] = (int)bytes;
+  return e;
+}
+
 cudaError_t prepare_pcg(Engine& eng) {
   size_t ov, oro, oc, oS, total;
   pcg_smem_layout<double>(eng.pcg_nloc_max, eng.pcg_nb_max, eng.pcg_resident, eng.pcg_cached, &ov, &oro, &oc, &oS,
                           &total);
-  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
+  cudaError_t e = ensure_pcg_smem(eng.device, total);
   if (e == cudaSuccess) eng.pcg_attr_smem = (int)total;
   return e;
 }
@@ -765,6 +782,227 @@ int pcg_max_grid(int device) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<double>, kPcgThreads, 0);
   return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+
+// ---------------------------------------------------------------------------
+// Allocation-free PCG (b200fem_pcg_solve_noalloc)
+//
+// For callers that cannot allocate device memory: hosts whose device memory
+// is owned entirely by another allocator or pool (a framework's caching
+// allocator, a JVM-side arena handed out by the application), and real-time
+// or embedded hosts that fix their device footprint at start-up and forbid
+// allocation afterwards.  They pass their own device buffers for the matrix,
+// right-hand side and solution; every other buffer the solve needs comes
+// from the file-scope array below, which every device that loads the
+// library holds until the process exits.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxRows = B200FEM_NOALLOC_MAX_ROWS;
+constexpr int kNoAllocMaxIter = B200FEM_NOALLOC_MAX_ITER;
+constexpr int kNoAllocMaxGrid = 1024;
+
+constexpr size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct NoAllocLayout {
+  // byte offsets inside the scratch array, each 256-byte aligned
+  static constexpr size_t dinv = 0;
+  static constexpr size_t vec = al256(dinv + sizeof(double) * 9 * (size_t)kNoAllocMaxRows);  // r u w z q s p m0 m1
+  static constexpr size_t partials = al256(vec + sizeof(double) * 9 * 3 * (size_t)kNoAllocMaxRows);
+  static constexpr size_t step = al256(partials + sizeof(double) * 2 * 4 * (size_t)kNoAllocMaxGrid);
+  static constexpr size_t model_out = al256(step + sizeof(double) * 8);
+  static constexpr size_t blk_diag = al256(model_out + sizeof(double) * 4);
+  static constexpr size_t piece_row = al256(blk_diag + sizeof(int) * (size_t)kNoAllocMaxRows);
+  static constexpr size_t piece_model = al256(piece_row + sizeof(int) * (kNoAllocMaxGrid + 1));
+  static constexpr size_t model_piece = al256(piece_model + sizeof(int) * kNoAllocMaxGrid);
+  static constexpr size_t cta_piece = al256(model_piece + sizeof(int) * 2);
+  static constexpr size_t unconv = al256(cta_piece + sizeof(int) * (kNoAllocMaxGrid + 1));
+  static constexpr size_t flags = al256(unconv + sizeof(int) * (kNoAllocMaxIter + 2));
+  static constexpr size_t barrier = al256(flags + sizeof(int) * 4);
+  static constexpr size_t total = al256(barrier + sizeof(unsigned) * 2);
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
+
+// per-device set-up: the device address of the scratch array (host code
+// cannot use the symbol itself) and the launch geometry
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* base = nullptr;
+  int sms = 0;
+};
+static std::mutex g_noalloc_mu;
+static NoAllocDevice g_noalloc_dev[64];
+
+__global__ void noalloc_diag_kernel(int n_rows, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                    int* __restrict__ blk_diag, int* __restrict__ flags) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  int d = -1;
+  for (int p = rowptr[row]; p < rowptr[row + 1]; p++)
+    if (col[p] == row) d = p;
+  blk_diag[row] = d < 0 ? rowptr[row] : d;
+  if (d < 0) atomicExch(flags, B200FEM_ERR_INVALID_ARG);
+}
+
+int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const double* vals, const double* b, double* x,
+                      double tol, int max_iter, void* stream_ptr, int* iterations, double* rel_residual,
+                      const char** err) {
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  if (n_rows < 1 || n_rows > kNoAllocMaxRows) {
+    *err = "n_rows must be in [1, B200FEM_NOALLOC_MAX_ROWS]";
+    return B200FEM_ERR_BUDGET;
+  }
+  if (max_iter < 1 || max_iter > kNoAllocMaxIter) {
+    *err = "max_iter must be in [1, B200FEM_NOALLOC_MAX_ITER]";
+    return B200FEM_ERR_BUDGET;
+  }
+  if (!rowptr || !col || !vals || !b || !x || !(tol > 0)) {
+    *err = "null device pointer or non-positive tolerance";
+    return B200FEM_ERR_INVALID_ARG;
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) {
+    *err = "no current CUDA device";
+    return B200FEM_ERR_CUDA;
+  }
+  NoAllocDevice nd;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice& dev = g_noalloc_dev[device];
+    if (!dev.ready) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+        *err = "cudaGetSymbolAddress of the scratch array failed";
+        return B200FEM_ERR_CUDA;
+      }
+      dev.base = (unsigned char*)p;
+      if (cudaDeviceGetAttribute(&dev.sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        *err = "cudaDeviceGetAttribute failed";
+        return B200FEM_ERR_CUDA;
+      }
+      dev.ready = true;
+    }
+    nd = dev;
+  }
+  using LY = NoAllocLayout;
+  unsigned char* base = nd.base;
+  // even split of the rows over the CTAs, one piece each (single model)
+  const int G = min(min(nd.sms, kNoAllocMaxGrid), (n_rows + 31) / 32);
+  int piece_row[kNoAllocMaxGrid + 1], cta_piece[kNoAllocMaxGrid + 1], piece_model[kNoAllocMaxGrid];
+  int model_piece[2] = {0, G};
+  for (int c = 0; c <= G; c++) {
+    piece_row[c] = (int)((long long)n_rows * c / G);
+    cta_piece[c] = c;
+  }
+  for (int c = 0; c < G; c++) piece_model[c] = 0;
+  double step[8] = {0, 0, 0, 0, 0, 0, tol, 0};
+  const int nloc_max = (n_rows + G - 1) / G + 1;
+  int resident = 0, cached = 0;
+  pcg_plan_smem(device, nloc_max, 0, &resident, &cached);
+  cached = 0;
+  size_t ov, oro, oc, oS, dyn;
+  pcg_smem_layout<double>(nloc_max, 0, resident, 0, &ov, &oro, &oc, &oS, &dyn);
+  cudaError_t e;
+  if ((e = ensure_pcg_smem(device, dyn)) != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return B200FEM_ERR_CUDA;
+  }
+  // the array keeps the previous call's contents: clear what must start at
+  // zero (barrier counter, error/status words, model outputs)
+  e = cudaMemsetAsync(base + LY::barrier, 0, sizeof(unsigned) * 2, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + LY::flags, 0, sizeof(int) * 4, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + LY::model_out, 0, sizeof(double) * 4, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + LY::piece_row, piece_row, sizeof(int) * (G + 1), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + LY::cta_piece, cta_piece, sizeof(int) * (G + 1), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + LY::piece_model, piece_model, sizeof(int) * G, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + LY::model_piece, model_piece, sizeof(int) * 2, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(base + LY::step, step, sizeof(step), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return B200FEM_ERR_CUDA;
+  }
+  noalloc_diag_kernel<<<(n_rows + 255) / 256, 256, 0, stream>>>(n_rows, rowptr, col, (int*)(base + LY::blk_diag),
+                                                               (int*)(base + LY::flags));
+  double* vec = (double*)(base + LY::vec);
+  const size_t V = 3 * (size_t)kNoAllocMaxRows;
+  PcgArgs a;
+  a.n_rows = n_rows;
+  a.n_pieces = G;
+  a.rowptr = rowptr;
+  a.col = col;
+  a.blk_diag = (const int*)(base + LY::blk_diag);
+  a.S = vals;
+  a.Dinv = (double*)(base + LY::dinv);
+  a.b = b;
+  a.x = x;
+  a.r = vec + 0 * V;
+  a.u = vec + 1 * V;
+  a.w = vec + 2 * V;
+  a.z = vec + 3 * V;
+  a.q = vec + 4 * V;
+  a.s = vec + 5 * V;
+  a.p = vec + 6 * V;
+  a.m0 = vec + 7 * V;
+  a.m1 = vec + 8 * V;
+  a.piece_row = (const int*)(base + LY::piece_row);
+  a.piece_model = (const int*)(base + LY::piece_model);
+  a.model_piece = (const int*)(base + LY::model_piece);
+  a.cta_piece = (const int*)(base + LY::cta_piece);
+  a.partials = (double*)(base + LY::partials);
+  a.step = (const double*)(base + LY::step);
+  a.model_out = (double*)(base + LY::model_out);
+  a.resident = resident;
+  a.cached = 0;
+  a.nloc_max = nloc_max;
+  a.nb_max = 0;
+  a.barrier = (unsigned*)(base + LY::barrier);
+  a.flags = (int*)(base + LY::flags);
+  a.unconv = (int*)(base + LY::unconv);
+  a.max_iter = max_iter;
+  a.update_state = 0;
+  a.xpos = nullptr;
+  a.vel = nullptr;
+  a.act_node = nullptr;
+  a.row_model = nullptr;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G);
+  cfg.blockDim = dim3(kPcgThreads);
+  cfg.dynamicSmemBytes = dyn;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return B200FEM_ERR_CUDA;
+  }
+  double out[4];
+  int flags[4];
+  e = cudaMemcpyAsync(out, base + LY::model_out, sizeof(out), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(flags, base + LY::flags, sizeof(flags), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return B200FEM_ERR_CUDA;
+  }
+  if (iterations) *iterations = (int)out[0];
+  if (rel_residual) *rel_residual = out[1];
+  if (flags[0] == B200FEM_ERR_TIMEOUT) {
+    *err = "PCG grid barrier timed out";
+    return B200FEM_ERR_TIMEOUT;
+  }
+  if (flags[0] != 0) {
+    *err = "missing or singular diagonal block";
+    return B200FEM_ERR_INVALID_ARG;
+  }
+  if (out[2] == 0.0) {
+    *err = "PCG did not reach the tolerance within max_iter iterations";
+    return B200FEM_ERR_NO_CONVERGE;
+  }
+  return B200FEM_OK;
 }
 
 }  // namespace b200fem

@@ -169,6 +169,33 @@ int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, 
 /* synchronise and report the device time of the last step/update call */
 int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms);
 
+/* ---- allocation-free solve ---------------------------------------------- */
+/* Size limits of b200fem_pcg_solve_noalloc: its scratch is one fixed device
+   array (about 2.6 MB) sized for these limits. */
+#define B200FEM_NOALLOC_MAX_ROWS 8192  /* 3x3 block rows (24,576 unknowns) */
+#define B200FEM_NOALLOC_MAX_ITER 16384
+
+/* No counterpart in the reference.  Block-Jacobi PCG on S x = b that
+   allocates nothing, for callers that cannot allocate device memory (their
+   device memory belongs to another allocator or pool, or they forbid
+   allocation after start-up).  All arrays are caller-owned DEVICE memory on
+   the current device: the block-CSR matrix (rowptr n_rows+1, col nnzb, vals
+   9*nnzb row-major 3x3 blocks, every row holding its diagonal block), b and
+   x (3*n_rows; x is the initial guess on entry and the solution on exit).
+   Every other buffer comes from a static device array that each device
+   which loads the library holds until the process exits.  Sizes beyond
+   B200FEM_NOALLOC_MAX_ROWS / _MAX_ITER are rejected with
+   B200FEM_ERR_BUDGET.  The first call on a device looks up the array's
+   device address (cudaGetSymbolAddress); make that first call before any
+   stream capture.  The call runs on `stream` (a cudaStream_t, NULL for the
+   legacy default stream) and returns after it completes; all calls share
+   the one array, so calls that overlap on the GPU (other threads, other
+   streams) race and must be serialised by the caller.  Messages go to
+   b200fem_last_error(NULL). */
+int b200fem_pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const double* vals,
+                              const double* b, double* x, double tol, int max_iter, void* stream,
+                              int* iterations, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif
