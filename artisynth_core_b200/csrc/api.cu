@@ -246,7 +246,75 @@ int build_pack(Engine& eng) {
     }
     eng.groups.push_back(g);
   }
-  if (any_nodal) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "NODAL incompressibility is not built yet");
+  // ---- NODAL soft incompressibility: direct-neighbour lists, incidence
+  // slots, and per block the (divBlk i, divBlk j, node) triples of the
+  // dilational term, node-ascending
+  std::vector<int> nbr_ptr, nbr_idx, inc_slot, dptr, didx;
+  std::vector<double> mat_node;
+  if (any_nodal) {
+    nbr_ptr.assign(N + 1, 0);
+    mat_node.assign(2 * (size_t)N, 0.0);
+    for (int m = 0; m < M; m++) {
+      const int no = eng.node_off[m];
+      for (int n = 0; n < eng.models[m].n_nodes; n++) {
+        nbr_ptr[no + n + 1] = (int)eng.hosts[m].nbr[n].size();
+        mat_node[2 * (size_t)(no + n)] = eng.models[m].mat_params[5];
+        mat_node[2 * (size_t)(no + n) + 1] = eng.models[m].mat_params[7];
+      }
+    }
+    for (int n = 0; n < N; n++) nbr_ptr[n + 1] += nbr_ptr[n];
+    nbr_idx.resize(nbr_ptr[N]);
+    for (int m = 0; m < M; m++) {
+      const int no = eng.node_off[m];
+      for (int n = 0; n < eng.models[m].n_nodes; n++) {
+        const auto& v = eng.hosts[m].nbr[n];
+        for (size_t k = 0; k < v.size(); k++) nbr_idx[nbr_ptr[no + n] + k] = no + v[k];
+      }
+    }
+    auto slot_of = [&](int n, int node) -> int {
+      auto b = nbr_idx.begin() + nbr_ptr[n], e = nbr_idx.begin() + nbr_ptr[n + 1];
+      return (int)(std::lower_bound(b, e, node) - b);
+    };
+    inc_slot.resize(iidx.size() * nen);
+    for (int n = 0; n < N; n++)
+      for (int i = iptr[n]; i < iptr[n + 1]; i++) {
+        const int e = iidx[i] / nen;
+        for (int j = 0; j < nen; j++) inc_slot[(size_t)i * nen + j] = slot_of(n, conn[(size_t)e * nen + j]);
+      }
+    dptr.assign(NB + 1, 0);
+    for (int pass = 0; pass < 2; pass++) {
+      std::vector<int> fill;
+      if (pass == 1) {
+        for (long long p = 0; p < NB; p++) dptr[p + 1] += dptr[p];
+        didx.resize(3 * (size_t)dptr[NB]);
+        fill.assign(dptr.begin(), dptr.end() - 1);
+      }
+      for (int m = 0; m < M; m++) {
+        if (eng.hosts[m].incomp != B200FEM_INCOMP_NODAL) continue;
+        for (int n = eng.node_off[m]; n < eng.node_off[m + 1]; n++) {
+          if (sidx[n] < 0) continue;  // volumeIsControllable: active nodes only
+          for (int a = nbr_ptr[n]; a < nbr_ptr[n + 1]; a++) {
+            const int ra = sidx[nbr_idx[a]];
+            if (ra < 0) continue;
+            for (int b = nbr_ptr[n]; b < nbr_ptr[n + 1]; b++) {
+              const int rb = sidx[nbr_idx[b]];
+              if (rb < 0) continue;
+              const int p = block_of(ra, rb);
+              if (p < 0) return fail(&eng, B200FEM_ERR_STATE, "internal: dilational pair outside the pattern");
+              if (pass == 0) {
+                dptr[p + 1]++;
+              } else {
+                int* t = &didx[3 * (size_t)fill[p]++];
+                t[0] = a;
+                t[1] = b;
+                t[2] = n;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
   if (eng.precision != B200FEM_PREC_FP64)
     return fail(&eng, B200FEM_ERR_UNSUPPORTED, "mixed precision is not built yet");
 
@@ -340,9 +408,17 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.mat, mat));
   CK(upload(eng, &d.step, step));
   if (any_nodal) {
+    d.has_nodal = 1;
     CK(upload(eng, &d.node_rest_vol, node_rest_vol));
     CK(dalloc(eng, &d.node_vol, (size_t)N));
     CK(dalloc(eng, &d.node_p, (size_t)N));
+    CK(dalloc(eng, &d.node_kp, (size_t)N));
+    CK(upload(eng, &d.mat_node, mat_node));
+    CK(upload(eng, &d.nbr_ptr, nbr_ptr));
+    CK(upload(eng, &d.inc_slot, inc_slot));
+    CK(dalloc(eng, &d.divblk, 3 * (size_t)nbr_ptr[N]));
+    CK(upload(eng, &d.dil_ptr, dptr));
+    CK(upload(eng, &d.dil_idx, didx));
   }
   CK(dalloc(eng, &d.partials, (size_t)d.n_pieces * 8));
   CK(upload(eng, &d.piece_row, piece_row));

@@ -112,10 +112,18 @@ struct DevPack {
   // per model tables
   double* mat = nullptr;       // n_models*kMatParams
   double* step = nullptr;      // n_models*8: h, alpha, beta, gx, gy, gz, tol, -
-  // NODAL incompressibility
+  // NODAL incompressibility (FemModel3d.java:2471-2669)
   double* node_rest_vol = nullptr;
   double* node_vol = nullptr;
-  double* node_p = nullptr;
+  double* node_p = nullptr;    // nodal pressure
+  double* node_kp = nullptr;   // dilational modulus / rest volume
+  double* mat_node = nullptr;  // per node: kappa, bulk potential of its model
+  int* nbr_ptr = nullptr;      // N+1 direct neighbours (sorted node ids)
+  int* inc_slot = nullptr;     // per incidence (inc_idx order): nen slots in nbr(n)
+  double* divblk = nullptr;    // nbr_ptr[N] x 3: d V_n / d x_m
+  int* dil_ptr = nullptr;      // nnzb+1 dilational contributions per block
+  int* dil_idx = nullptr;      // (divblk row i, divblk row j, node n) triples
+  int has_nodal = 0;
   // reductions / PCG control
   double* partials = nullptr;  // [2][n_pieces][4] (double-buffered by phase)
   int* piece_row = nullptr;    // n_pieces+1

@@ -413,7 +413,9 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
                               const TK* __restrict__ elemK, const int* __restrict__ blk_row,
                               const int* __restrict__ blk_diag, const int* __restrict__ row_model,
                               const int* __restrict__ act_node, const double* __restrict__ mass,
-                              const double* __restrict__ step, int mode, TO* __restrict__ out) {
+                              const double* __restrict__ step, int mode, TO* __restrict__ out,
+                              const int* __restrict__ dptr, const int* __restrict__ didx,
+                              const double* __restrict__ divblk, const double* __restrict__ node_kp) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nnzb * 9) return;
   long long p = t / 9;
@@ -432,6 +434,18 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
       v[k] = code[k] >= 0 ? elemK[(size_t)(code[k] >> 1) * 9 + ((code[k] & 1) ? qt : q)] : TK(0);
 #pragma unroll
     for (int k = 0; k < 4; k++) s += v[k];
+  }
+  if (dptr) {
+    // NODAL dilational term sum_n kp_n divBlk(n,i) divBlk(n,j)^T, n ascending
+    // (FemModel3d.computeNodalIncompressibility, FemModel3d.java:2632-2669)
+    const int r = q / 3, c = q % 3;
+    const int d1 = dptr[p + 1];
+    double sd = 0;
+    for (int t = dptr[p]; t < d1; t++) {
+      const int* tr = didx + 3 * (size_t)t;
+      sd += node_kp[tr[2]] * divblk[3 * (size_t)tr[0] + r] * divblk[3 * (size_t)tr[1] + c];
+    }
+    s += (TK)sd;
   }
   double val;
   if (mode == 0) {
@@ -598,6 +612,148 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T, EPB_MR>(a, ne, eng.stream);
 }
 
+// ---------------------------------------------------------------------------
+// NODAL soft incompressibility
+// ---------------------------------------------------------------------------
+// Nodal volumes and pressures (updateNodalPressures, FemModel3d.java:2471-2515):
+// tets give V_e/4 to each node, hexes the dv of the integration point that
+// maps to the node; p_n = K(V_n/V0_n - 1) (QUADRATIC) or K ln(J)/J
+// (LOGARITHMIC) for active nodes, and kp_n = K_eff / V0_n
+// (computeNodalIncompressibility, :2632-2669).
+template <int TYPE>
+__global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                      const int* __restrict__ conn, const double* __restrict__ x,
+                                      const int* __restrict__ sidx, const double* __restrict__ rest_vol,
+                                      const double* __restrict__ mat_node, double* __restrict__ vol,
+                                      double* __restrict__ pres, double* __restrict__ kp) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double v = 0;
+  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+    const int e = inc_idx[i] / NEN, a = inc_idx[i] % NEN;
+    const int* nodes = conn + (size_t)e * NEN;
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < NEN; k++) {
+      const double* pk = x + 3 * (size_t)nodes[k];
+      double g0, g1, g2;
+      if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * k]; g1 = c_tet_gns[3 * k + 1]; g2 = c_tet_gns[3 * k + 2]; }
+      else { g0 = c_hex_gns[(a * 8 + k) * 3]; g1 = c_hex_gns[(a * 8 + k) * 3 + 1]; g2 = c_hex_gns[(a * 8 + k) * 3 + 2]; }
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        J[3 * r] += pk[r] * g0;
+        J[3 * r + 1] += pk[r] * g1;
+        J[3 * r + 2] += pk[r] * g2;
+      }
+    }
+    // tet: V_e = det(J)/6 shared by four nodes; hex: dv of point a (w = 1)
+    v += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 / 4 : det3(J);
+  }
+  vol[n] = v;
+  double p = 0, k = 0;
+  if (sidx[n] >= 0) {
+    const double K = mat_node[2 * (size_t)n], J = v / rest_vol[n];
+    if (mat_node[2 * (size_t)n + 1] == 0) {
+      p = K * (J - 1);
+      k = K;
+    } else {
+      p = K * log(J) / J;
+      k = K * (1 - log(J)) / (J * J);
+    }
+    k /= rest_vol[n];
+  }
+  pres[n] = p;
+  kp[n] = k;
+}
+
+// divBlk(n, m) = dV_n/dx_m, accumulated per node over its incidences in
+// element order (FemModel3d.java:3604-3648): tets add -1/12 of the
+// area-weighted normal of the face opposite m (TetElement.java:333-362);
+// hexes add dv_k GNx_m at the integration point k that maps to n.
+template <int TYPE>
+__global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                              const int* __restrict__ inc_slot, const int* __restrict__ conn,
+                              const double* __restrict__ x, const int* __restrict__ sidx,
+                              const int* __restrict__ nbr_ptr, double* __restrict__ divblk) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double* out = divblk + 3 * (size_t)nbr_ptr[n];
+  const int ns = nbr_ptr[n + 1] - nbr_ptr[n];
+  for (int s = 0; s < 3 * ns; s++) out[s] = 0;
+  if (sidx[n] < 0) return;
+  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+    const int e = inc_idx[i] / NEN, a = inc_idx[i] % NEN;
+    const int* nodes = conn + (size_t)e * NEN;
+    const int* slot = inc_slot + (size_t)i * NEN;
+    if (TYPE == B200FEM_ELEM_TET) {
+      const double* P[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) P[k] = x + 3 * (size_t)nodes[k];
+      // faces opposite nodes 0..3: (1,2,3), (0,3,2), (0,1,3), (0,2,1)
+      const int f[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const double *q0 = P[f[j][0]], *q1 = P[f[j][1]], *q2 = P[f[j][2]];
+        const double ux = q1[0] - q0[0], uy = q1[1] - q0[1], uz = q1[2] - q0[2];
+        const double vx = q2[0] - q0[0], vy = q2[1] - q0[1], vz = q2[2] - q0[2];
+        double* o = out + 3 * slot[j];
+        o[0] += 0.5 * (uy * vz - uz * vy) * (-1 / 12.0);
+        o[1] += 0.5 * (uz * vx - ux * vz) * (-1 / 12.0);
+        o[2] += 0.5 * (ux * vy - uy * vx) * (-1 / 12.0);
+      }
+    } else {
+      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const double* pk = x + 3 * (size_t)nodes[k];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * c_hex_gns[(a * 8 + k) * 3 + c];
+      }
+      const double dv = invert3(iJ, J);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const double g0 = c_hex_gns[(a * 8 + k) * 3], g1 = c_hex_gns[(a * 8 + k) * 3 + 1],
+                     g2 = c_hex_gns[(a * 8 + k) * 3 + 2];
+        double* o = out + 3 * slot[k];
+#pragma unroll
+        for (int c = 0; c < 3; c++) o[c] += dv * (iJ[c] * g0 + iJ[3 + c] * g1 + iJ[6 + c] * g2);
+      }
+    }
+  }
+}
+
+cudaError_t launch_nodal_pressure(Engine& eng) {
+  DevPack& d = eng.d;
+  if (!d.has_nodal) return cudaSuccess;
+  const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
+  if (eng.elem_type == B200FEM_ELEM_TET)
+    nodal_pressure_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+        d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
+        d.node_kp);
+  else
+    nodal_pressure_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
+        d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
+        d.node_kp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_divblk(Engine& eng) {
+  DevPack& d = eng.d;
+  if (!d.has_nodal) return cudaSuccess;
+  const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
+  if (eng.elem_type == B200FEM_ELEM_TET)
+    divblk_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+        d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
+  else
+    divblk_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
+        d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
+  return cudaGetLastError();
+}
+
 // One-time preparation before any stream capture: constant tables and the
 // shared-memory opt-in of every element kernel this pack launches.
 cudaError_t prepare_kernels(Engine& eng) {
@@ -621,6 +777,8 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   cudaError_t e = cudaSuccess;
   DevPack& d = eng.d;
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  if ((e = launch_nodal_pressure(eng)) != cudaSuccess) return e;
+  if ((e = launch_divblk(eng)) != cudaSuccess) return e;
   for (const ElemGroup& g : eng.groups) {
     if (g.elem_type == B200FEM_ELEM_TET)
       e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);
@@ -634,11 +792,11 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   if (want_K) {
     gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, 0, d.K);
+        d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
   } else {
     gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, 1, d.S);
+        d.step, 1, d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
   }
   return cudaGetLastError();
 }

@@ -30,6 +30,9 @@ def _cases():
         "neohookean_hex": W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45)),
         "mooneyrivlin_tet_off": W.small_tet_beam(MooneyRivlinMaterial(1e4, 2e3, 0, 0, 0, 1e5)),
         "mooneyrivlin_hex_full": W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 30, 486, 20, 10370)),
+        "mooneyrivlin_tet_nodal": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
+        "mooneyrivlin_hex_nodal": W.small_hex_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
+        "mooneyrivlin_tet_nodal_log": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5, 0.0, 1)),
     }
 
 
@@ -43,6 +46,8 @@ def cases(b200):
     cs = _cases()
     for k in ("mooneyrivlin_tet_off", "mooneyrivlin_hex_full"):
         _incomp_off(cs[k])
+    # more hexes than active nodes is needed for AUTO -> NODAL; request it
+    cs["mooneyrivlin_hex_nodal"].incomp = L.INCOMP_NODAL
     return cs
 
 
@@ -128,7 +133,9 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
 
 
 @pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex", "mooneyrivlin_tet_off",
-                                  "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full"])
+                                  "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full",
+                                  "mooneyrivlin_tet_nodal", "mooneyrivlin_hex_nodal",
+                                  "mooneyrivlin_tet_nodal_log"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)
@@ -178,3 +185,28 @@ def test_spmv_and_pcg_solve(cases):
     x, st = ms.pcg(b, tol=1e-13, max_iter=5000)
     assert rel_err(x, xt) <= 1e-9
     assert st.rel_residual <= 1e-12
+
+
+def test_nodal_resolution_and_pattern(cases, oracle):
+    """AUTO resolves to NODAL for the MooneyRivlin tet beam (more elements than
+    active nodes) and the 2-ring pattern is bit-exact."""
+    wl = cases["mooneyrivlin_tet_nodal"]
+    m = _gpu_model(wl)
+    om = oracle_model(oracle, wl)
+    assert m.getSoftIncompMethod() == L.INCOMP_NODAL == om.incomp
+    rp, col = m.getBlockPattern()
+    orp, ocol = om.pattern()
+    assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
+    direct = W.small_tet_beam(NeoHookeanMaterial(1e4, 0.3)).model()
+    assert col.size > direct.sizes()["nnzb"]  # the 2-ring adds blocks
+
+
+def test_mooneyrivlin_block_nodal_steps(oracle):
+    """The MooneyRivlin block workload's material and NODAL incompressibility
+    on a 12x6x6 block (z-min fixed, gravity): 5 steps against the oracle."""
+    wl = W.mooneyrivlin_tet_block()
+    wl.cells = (12, 6, 6)
+    wl.build_mesh()
+    xg, vg, x, v, ms = _run_pair(wl, oracle, 5, 0, 1e-12)
+    assert rel_err(xg, x) <= POS_TOL
+    assert rel_err(xg - wl.rest, x - wl.rest) <= 1e-6
