@@ -4,10 +4,10 @@ include/b200fem.h); this package is the host-side mirror of the reference
 interface around it."""
 from . import _lib
 from ._lib import B200FemError, lib
-from .femmodel import (FemEngine, FemFactory, FemModel3d, LinearMaterial, MechSystemSolver,
+from .femmodel import (FemEngine, FemFactory, FemModel3d, FemPack, LinearMaterial, MechSystemSolver,
                        MooneyRivlinMaterial, NeoHookeanMaterial, create_grid, jitter_grid)
 
 __all__ = [
-    "B200FemError", "FemEngine", "FemFactory", "FemModel3d", "LinearMaterial", "MechSystemSolver",
+    "B200FemError", "FemEngine", "FemFactory", "FemModel3d", "FemPack", "LinearMaterial", "MechSystemSolver",
     "MooneyRivlinMaterial", "NeoHookeanMaterial", "create_grid", "jitter_grid", "lib", "_lib",
 ]

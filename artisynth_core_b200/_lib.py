@@ -31,6 +31,7 @@ MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN = 0, 1, 2
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 PART_FULL, PART_UPPER = 0, 1
+PCG_AUTO, PCG_CLASSIC, PCG_PIPELINED = 0, 1, 2
 
 
 class B200FemError(RuntimeError):
@@ -55,6 +56,7 @@ class StepParams(ctypes.Structure):
         ("tol", ctypes.c_double),
         ("max_iter", ctypes.c_int),
         ("abort_on_inverted", ctypes.c_int),
+        ("pcg_variant", ctypes.c_int),
     ]
 
 
@@ -119,6 +121,12 @@ def lib():
         "b200fem_spmv": ([H, _dp, _dp], ctypes.c_int),
         "b200fem_pcg_solve": ([H, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_last_timing": ([H, _dp, _dp], ctypes.c_int),
+        "b200fem_add_model": ([H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.c_int, _dp,
+                               ctypes.c_double, ctypes.c_int, _ip], ctypes.c_int),
+        "b200fem_clear_models": ([H], ctypes.c_int),
+        "b200fem_num_models": ([H, _ip], ctypes.c_int),
+        "b200fem_model_range": ([H, ctypes.c_int, _ip, _ip, _ip], ctypes.c_int),
+        "b200fem_get_model_stats": ([H, _ip, _dp], ctypes.c_int),
         "b200fem_pcg_solve_noalloc": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
                                        _ip, _dp], ctypes.c_int),
     }

@@ -17,7 +17,7 @@ namespace b200fem {
 cudaError_t launch_forces_only(Engine& eng);
 int pcg_max_grid(int device);
 int pcg_max_cta_pieces();
-void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached);
+void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached, bool fp32);
 cudaError_t prepare_pcg(Engine& eng);
 cudaError_t prepare_kernels(Engine& eng);
 int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const double* vals, const double* b, double* x,
@@ -315,8 +315,6 @@ int build_pack(Engine& eng) {
       }
     }
   }
-  if (eng.precision != B200FEM_PREC_FP64)
-    return fail(&eng, B200FEM_ERR_UNSUPPORTED, "mixed precision is not built yet");
 
   // ---- PCG work split: CTAs own contiguous row ranges balanced by blocks,
   // cut into pieces at model boundaries
@@ -366,7 +364,8 @@ int build_pack(Engine& eng) {
     eng.pcg_nloc_max = std::max(eng.pcg_nloc_max, rb - ra);
     eng.pcg_nb_max = std::max(eng.pcg_nb_max, rowptr[rb] - rowptr[ra]);
   }
-  pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached);
+  pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
+                eng.precision == B200FEM_PREC_MIXED);
 
   // ---- device upload
   CK(upload(eng, &d.x, x));
@@ -395,10 +394,19 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.contrib_idx, cidx));
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));
-  CK(dalloc(eng, &d.elemK, (size_t)E * npair * 9));
-  CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
   CK(dalloc(eng, &d.K, (size_t)NB * 9));
-  CK(dalloc(eng, &d.S, (size_t)NB * 9));
+  if (eng.precision == B200FEM_PREC_MIXED) {
+    // mixed form: FP32 rest data, element outputs and solve matrix
+    std::vector<float> invJ0_f(invJ0.begin(), invJ0.end());
+    CK(upload(eng, &d.invJ0_f, invJ0_f));
+    CK(dalloc(eng, &d.elemK_f, (size_t)E * npair * 9));
+    CK(dalloc(eng, &d.elemF_f, (size_t)E * nen * 3));
+    CK(dalloc(eng, &d.S_f, (size_t)NB * 9));
+  } else {
+    CK(dalloc(eng, &d.elemK, (size_t)E * npair * 9));
+    CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
+    CK(dalloc(eng, &d.S, (size_t)NB * 9));
+  }
   CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
   CK(dalloc(eng, &d.fint, 3 * (size_t)N));
   for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w, &d.u, &d.s, &d.m0, &d.m1}) {
@@ -600,6 +608,73 @@ int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, d
   return B200FEM_OK;
 }
 
+int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz, int n_elems,
+                      const int* conn, const int* fixed, int mat_kind, const double* params, double density,
+                      int incomp, int* model_index) {
+  ENG(h);
+  if (elem_type != B200FEM_ELEM_TET && elem_type != B200FEM_ELEM_HEX)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
+  if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn) return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
+  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_MOONEYRIVLIN || !params)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
+  if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
+  ModelDesc m;
+  const int nen = elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  m.elem_type = elem_type;
+  m.n_nodes = n_nodes;
+  m.n_elems = n_elems;
+  m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
+  m.conn.assign(conn, conn + (size_t)nen * n_elems);
+  m.fixed.assign(n_nodes, 0);
+  if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
+  m.mat_kind = mat_kind;
+  const int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_NEOHOOKEAN ? 2 : 8;
+  std::copy(params, params + np, m.mat_params);
+  m.density = density;
+  m.incomp_request = incomp;
+  m.has_material = true;
+  if (eng.models.size() == 1 && eng.models[0].n_nodes == 0) eng.models[0] = std::move(m);
+  else eng.models.push_back(std::move(m));
+  if (model_index) *model_index = (int)eng.models.size() - 1;
+  free_pack(eng);
+  return B200FEM_OK;
+}
+
+int b200fem_clear_models(b200fem_handle h) {
+  ENG(h);
+  free_pack(eng);
+  eng.models.assign(1, ModelDesc());
+  return B200FEM_OK;
+}
+
+int b200fem_num_models(b200fem_handle h, int* n_models) {
+  ENG(h);
+  *n_models = (eng.models.size() == 1 && eng.models[0].n_nodes == 0) ? 0 : (int)eng.models.size();
+  return B200FEM_OK;
+}
+
+int b200fem_model_range(b200fem_handle h, int model, int* node_offset, int* n_nodes, int* n_active) {
+  ENG(h);
+  NEED_BUILT();
+  if (model < 0 || model >= (int)eng.models.size()) return fail(&eng, B200FEM_ERR_INVALID_ARG, "no such model");
+  if (node_offset) *node_offset = eng.node_off[model];
+  if (n_nodes) *n_nodes = eng.models[model].n_nodes;
+  if (n_active) *n_active = eng.hosts[model].n_active;
+  return B200FEM_OK;
+}
+
+int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_residual) {
+  ENG(h);
+  NEED_BUILT();
+  std::vector<double> ms((size_t)eng.d.n_models * 4);
+  CK(cudaMemcpy(ms.data(), eng.d.model_scal, ms.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int m = 0; m < eng.d.n_models; m++) {
+    if (iterations) iterations[m] = (int)ms[(size_t)m * 4];
+    if (rel_residual) rel_residual[m] = ms[(size_t)m * 4 + 1];
+  }
+  return B200FEM_OK;
+}
+
 int b200fem_build(b200fem_handle h) {
   ENG(h);
   return build_pack(eng);
@@ -749,16 +824,29 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
     CK(cudaMemcpyAsync(f_int, d.fint, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyDeviceToHost, eng.stream));
   if (k_blocks)
     CK(cudaMemcpyAsync(k_blocks, d.K, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
-  if (crs_vals) {
+  std::vector<double> kbsr;
+  if (crs_vals && d.S) {
     CK(launch_crs_export(eng, d.K, d.S));
     CK(cudaMemcpyAsync(crs_vals, d.S, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
     eng.have_matrix = false;  // S was used as scratch
+  } else if (crs_vals) {
+    // mixed form (no FP64 S buffer): permute to the CRS slot order on the host
+    kbsr.resize(9 * (size_t)d.nnzb);
+    CK(cudaMemcpyAsync(kbsr.data(), d.K, kbsr.size() * sizeof(double), cudaMemcpyDeviceToHost, eng.stream));
   }
   int flags[4];
   long long dmin;
   CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
   CK(cudaMemcpyAsync(&dmin, d.dmin, sizeof(dmin), cudaMemcpyDeviceToHost, eng.stream));
   CK(cudaStreamSynchronize(eng.stream));
+  if (!kbsr.empty()) {
+    for (int r = 0; r < d.n_rows; r++) {
+      const long long p0 = eng.h_rowptr[r], nb = eng.h_rowptr[r + 1] - p0;
+      for (long long p = p0; p < p0 + nb; p++)
+        for (int q = 0; q < 9; q++)
+          crs_vals[9 * p0 + (q / 3) * 3 * nb + 3 * (p - p0) + (q % 3)] = kbsr[9 * (size_t)p + q];
+    }
+  }
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, eng.ev[0], eng.ev[1]));
   eng.last_asm_ms = ms;
@@ -794,9 +882,12 @@ static int read_step_status(Engine& eng, b200fem_stats* stats, int max_iter) {
   if (stats) *stats = st;
   if (flags[0] == B200FEM_ERR_TIMEOUT) return fail(&eng, B200FEM_ERR_TIMEOUT, "PCG grid barrier timed out");
   if (flags[0] != 0) return fail(&eng, flags[0], "singular diagonal block in the solve matrix");
-  if (flags[2] != 0 || !all_conv)
-    return fail(&eng, B200FEM_ERR_NO_CONVERGE,
-                "PCG did not reach the tolerance within " + std::to_string(max_iter) + " iterations");
+  if (flags[2] != 0 || !all_conv) {
+    char buf[160];
+    snprintf(buf, sizeof(buf), "PCG did not reach the tolerance (worst true relative residual %.3e after %d iterations, cap %d)",
+             st.rel_residual, st.iterations, max_iter);
+    return fail(&eng, B200FEM_ERR_NO_CONVERGE, buf);
+  }
   return B200FEM_OK;
 }
 
@@ -808,6 +899,11 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "step size, tolerance and max_iter must be positive");
   DevPack& d = eng.d;
   int max_iter = std::min(p->max_iter, d.unconv_cap);
+  if (p->pcg_variant < 0 || p->pcg_variant > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown pcg_variant");
+  if (p->pcg_variant != eng.pcg_variant) {
+    eng.pcg_variant = p->pcg_variant;
+    eng.step_exec_max_iter = -1;  // recapture: the variant is a kernel argument
+  }
   std::vector<double> step((size_t)d.n_models * 8);
   for (int m = 0; m < d.n_models; m++) {
     double* s = &step[(size_t)m * 8];

@@ -91,6 +91,7 @@ struct DevPack {
   double* elemK = nullptr;     // E*npair*9
   double* elemF = nullptr;     // E*nen*3
   float* elemK_f = nullptr;
+  float* elemF_f = nullptr;
   // assembled values
   double* K = nullptr;         // nnzb*9 stiffness (drop-in output)
   double* S = nullptr;         // nnzb*9 solve matrix
@@ -176,6 +177,7 @@ struct Engine {
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_attr_smem = -1;
+  int pcg_variant = 0;
   // captured BackwardEuler step (element, gather, RHS, PCG) and its events
   cudaGraphExec_t asm_exec = nullptr;
   cudaGraphExec_t step_exec = nullptr;

@@ -421,17 +421,17 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
   long long p = t / 9;
   int q = (int)(t - p * 9);
   int qt = (q % 3) * 3 + q / 3;
-  TK s = TK(0);
+  double s = 0;
   const int c0 = cptr[p], c1 = cptr[p + 1];
   // four contributions per round (independent loads), summed in list order
   for (int c = c0; c < c1; c += 4) {
     int code[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) code[k] = (c + k < c1) ? cidx[c + k] : -1;
-    TK v[4];
+    double v[4];
 #pragma unroll
     for (int k = 0; k < 4; k++)
-      v[k] = code[k] >= 0 ? elemK[(size_t)(code[k] >> 1) * 9 + ((code[k] & 1) ? qt : q)] : TK(0);
+      v[k] = code[k] >= 0 ? (double)elemK[(size_t)(code[k] >> 1) * 9 + ((code[k] & 1) ? qt : q)] : 0.0;
 #pragma unroll
     for (int k = 0; k < 4; k++) s += v[k];
   }
@@ -445,7 +445,7 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
       const int* tr = didx + 3 * (size_t)t;
       sd += node_kp[tr[2]] * divblk[3 * (size_t)tr[0] + r] * divblk[3 * (size_t)tr[1] + c];
     }
-    s += (TK)sd;
+    s += sd;
   }
   double val;
   if (mode == 0) {
@@ -567,7 +567,7 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.mat = d.mat;
   a.node_p = d.node_p;
   a.elemK = fp32 ? (void*)d.elemK_f : (void*)d.elemK;
-  a.elemF = d.elemF;
+  a.elemF = fp32 ? (void*)d.elemF_f : (void*)d.elemF;
   a.flags = d.flags;
   a.mindet = (long long*)d.dmin;
   return a;
@@ -599,8 +599,9 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   if (g.mat_kind == B200FEM_MAT_LINEAR) {
     if (ne < 0) return cudaSuccess;
     constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 8;
-    a.elemK = (void*)eng.d.elemK;  // linear path stays FP64
-    elem_linear_kernel<TYPE, double><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
+    // the corotation and K0 products run in FP64; the mixed form stores
+    // the element outputs in FP32
+    elem_linear_kernel<TYPE, T><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
     return cudaGetLastError();
   }
   // elements per CTA: one thread per integration point in stage 1
@@ -788,15 +789,20 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   }
   long long n9 = d.nnzb * 9;
   int threads = 256;
-  long long blocks = (n9 + threads - 1) / threads;
-  if (want_K) {
-    gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
-        d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+  unsigned blocks = (unsigned)((n9 + threads - 1) / threads);
+  if (fp32) {
+    if (want_K)
+      gather_kernel<float, double><<<blocks, threads, 0, eng.stream>>>(
+          d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
+          d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+    else
+      gather_kernel<float, float><<<blocks, threads, 0, eng.stream>>>(
+          d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
+          d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
   } else {
-    gather_kernel<double, double><<<(unsigned)blocks, threads, 0, eng.stream>>>(
+    gather_kernel<double, double><<<blocks, threads, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, 1, d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+        d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
   }
   return cudaGetLastError();
 }
@@ -813,29 +819,31 @@ cudaError_t launch_reset_status(Engine& eng) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_rhs(Engine& eng) {
+static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   DevPack& d = eng.d;
-  int threads = 256;
-  rows_kernel<double><<<(d.n_nodes + threads - 1) / threads, threads, 0, eng.stream>>>(
-      d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx, d.node_model, d.mass, d.v, d.fext, d.step, d.fint, d.b,
-      d.sol);
+  const int threads = 64;
+  const int blocks = (d.n_nodes + threads - 1) / threads;
+  if (eng.precision == B200FEM_PREC_MIXED)
+    rows_kernel<float><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF_f, d.sidx,
+                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol);
+  else
+    rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
+                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forces_only(Engine& eng) {
-  DevPack& d = eng.d;
-  int threads = 256;
-  rows_kernel<double><<<(d.n_nodes + threads - 1) / threads, threads, 0, eng.stream>>>(
-      d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx, d.node_model, d.mass, d.v, d.fext, d.step, d.fint,
-      nullptr, nullptr);
-  return cudaGetLastError();
-}
+cudaError_t launch_rhs(Engine& eng) { return launch_rows(eng, eng.d.b, eng.d.sol); }
+
+cudaError_t launch_forces_only(Engine& eng) { return launch_rows(eng, nullptr, nullptr); }
 
 cudaError_t launch_spmv(Engine& eng, const double* x, double* y) {
   DevPack& d = eng.d;
   int threads = 256;
   long long blocks = ((long long)d.n_rows * 32 + threads - 1) / threads;
-  spmv_kernel<double><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.blk_rowptr, d.blk_col, d.S, x, y);
+  if (eng.precision == B200FEM_PREC_MIXED)
+    spmv_kernel<float><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.blk_rowptr, d.blk_col, d.S_f, x, y);
+  else
+    spmv_kernel<double><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.blk_rowptr, d.blk_col, d.S, x, y);
   return cudaGetLastError();
 }
 

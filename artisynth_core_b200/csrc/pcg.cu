@@ -28,7 +28,9 @@ namespace b200fem {
 constexpr int kPcgThreads = 1024;
 constexpr int kRowChunk = 512;
 constexpr int kMaxCtaPieces = 48;
-constexpr int kMaxRestarts = 3;
+constexpr int kMaxRestarts = 10;
+// auto variant: pipelined iterations allowed before switching to classic PCG
+constexpr int kPipelinedCap = 400;
 constexpr unsigned long long kBarrierTimeoutNs = 5000000000ull;
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -107,6 +109,7 @@ struct PcgArgs {
   int* flags;
   int* unconv;  // per iteration: some model still unconverged
   int max_iter;
+  int variant;  // 0 auto (pipelined, classic after a residual replacement), 1 classic, 2 pipelined
   int update_state;
   double* xpos;
   double* vel;
@@ -410,7 +413,113 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   ph++;
 
   int total_it = 0;
+  bool classic = a.variant == 1;
   for (int restart = 0;; restart++) {
+    if (classic) {
+      // ---- classic PCG (two grid barriers per iteration), from the state
+      // P0 or the true-residual pass left: r, z = Dinv r (resident) and z
+      // published in m1.  rho = r.z, ||r||^2 first.
+      cta_row_pass<2, false>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
+        if (s_conv[piece_of_row(a, cv, row)]) return;
+        double r[3], z[3], zero[3] = {0, 0, 0};
+        load3(r, st.at(VR, row), 0);
+        load3(z, st.at(VU, row), 0);
+        store3(st.at(VP, row), 0, zero);
+        store3(st.at(VQ, row), 0, zero);
+        vals[0] = dot3(r, z);
+        vals[1] = dot3(r, r);
+      });
+      if (!grid_barrier(a.barrier, a.flags)) return;
+      model_sums<2>(a, cv, ph & 1, sums);
+      ph++;
+      for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+        if (s_conv[j]) continue;
+        s_gold[j] = sums[j][0];  // rho
+        if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]) || sums[j][1] == 0.0) s_conv[j] = 1;
+        s_first[j] = 1;
+      }
+      __syncthreads();
+      for (int it = 0;; it++) {
+        const int idx = total_it + it;
+        // phase A: p = z + beta p; q = S z + beta q (z complete); p.q
+        for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+          if (s_conv[j]) continue;
+          s_beta[j] = s_first[j] ? 0.0 : s_gold[j] / s_aold[j];
+          s_first[j] = 0;
+          const int m = a.piece_model[cv.pc0 + j];
+          if (cv.pc0 + j == a.model_piece[m + 1] - 1) a.unconv[idx] = 1;
+        }
+        __syncthreads();
+        if (idx >= a.max_iter) {
+          total_it += it;
+          break;
+        }
+        cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
+          const int j = piece_of_row(a, cv, row);
+          if (s_conv[j]) return;
+          double Az[3];
+          view_row_spmv<MT>(mv, row, a.m1, ln, Az);
+          if (ln == 0) {
+            const double be = s_beta[j];
+            double* pz = st.at(VU, row);
+            double* pp = st.at(VP, row);
+            double* pq = st.at(VQ, row);
+            double pqv = 0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              pp[c] = pz[c] + be * pp[c];
+              pq[c] = Az[c] + be * pq[c];
+              pqv += pp[c] * pq[c];
+            }
+            vals[0] = pqv;
+          }
+        });
+        if (!grid_barrier(a.barrier, a.flags)) return;
+        if (__ldcg(&a.unconv[idx]) == 0) {
+          total_it += it;
+          break;
+        }
+        model_sums<1>(a, cv, ph & 1, sums);
+        ph++;
+        for (int j = threadIdx.x; j < npc; j += blockDim.x)
+          s_alpha[j] = s_conv[j] ? 0.0 : s_gold[j] / sums[j][0];
+        __syncthreads();
+        // phase B: x += alpha p; r -= alpha q; z = Dinv r (published); r.z, r.r
+        cta_row_pass<2, false>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
+          const int j = piece_of_row(a, cv, row);
+          if (s_conv[j]) return;
+          const double al = s_alpha[j];
+          double* px = st.at(VX, row);
+          double* pr = st.at(VR, row);
+          double* pz = st.at(VU, row);
+          const double* pp = st.at(VP, row);
+          const double* pq = st.at(VQ, row);
+          double r[3], z[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            px[c] += al * pp[c];
+            r[c] = pr[c] - al * pq[c];
+            pr[c] = r[c];
+          }
+          mul33(z, st.dinv(row), r);
+          store3(pz, 0, z);
+          store3(a.m1, row, z);
+          vals[0] = dot3(r, z);
+          vals[1] = dot3(r, r);
+        });
+        if (!grid_barrier(a.barrier, a.flags)) return;
+        model_sums<2>(a, cv, ph & 1, sums);
+        ph++;
+        for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+          if (s_conv[j]) continue;
+          s_aold[j] = s_gold[j];  // rho of the previous iteration
+          s_gold[j] = sums[j][0];
+          s_iters[j]++;
+          if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]) || sums[j][1] == 0.0) s_conv[j] = 1;
+        }
+        __syncthreads();
+      }
+    } else {
     // ---- P1: w = S u, m = Dinv w (published to m0); dots r.u, w.u, r.r
     for (int j = threadIdx.x; j < npc; j += blockDim.x) s_first[j] = 1;
     cta_row_pass<3, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
@@ -499,7 +608,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           }
         }
         __syncthreads();
-        if (first && idx >= a.max_iter) {
+        if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kPipelinedCap))) {
           stop = true;
           break;
         }
@@ -606,6 +715,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       }
     }
     ph++;
+    }  // pipelined
 
     // ---- publish x, then the true residual r = b - S x; restart from it
     // when it misses the tolerance although the recurrence converged
@@ -621,7 +731,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
 #pragma unroll
         for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
         vals[0] = dot3(r, r);
-        if (!s_conv[piece_of_row(a, cv, row)]) return;
+        // restart state for every row (used only by restarted models)
         double u[3];
         mul33(u, st.dinv(row), r);
         store3(st.at(VR, row), 0, r);
@@ -637,8 +747,12 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     for (int j = threadIdx.x; j < npc; j += blockDim.x) {
       const double rel = s_bb[j] > 0 ? sqrt(sums[j][0] / s_bb[j]) : sqrt(sums[j][0]);
       const bool ok = rel <= s_tol[j] || sums[j][0] == 0.0;
-      if (s_conv[j] && !ok && restart < kMaxRestarts && total_it < a.max_iter) {
-        s_conv[j] = 0;  // residual replacement for this model
+      // residual replacement when the recurrence converged but the true
+      // residual did not; in auto mode also when the pipelined phase hit its
+      // cap unconverged (classic PCG continues from the true residual)
+      const bool stalled = !s_conv[j] && !classic && a.variant == 0;
+      if (((s_conv[j] && !ok) || stalled) && restart < kMaxRestarts && total_it < a.max_iter) {
+        s_conv[j] = 0;
         s_restart = 1;
       }
       const int m = a.piece_model[cv.pc0 + j];
@@ -654,6 +768,9 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
     if (!grid_barrier(a.barrier, a.flags)) return;
     if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
+    // the pipelined recurrences drifted from the true residual: continue
+    // with classic PCG, whose attainable accuracy is better
+    if (a.variant == 0) classic = true;
   }
 
   if (a.update_state) {
@@ -707,6 +824,7 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.flags = d.flags;
   a.unconv = d.unconv;
   a.max_iter = max_iter;
+  a.variant = eng.pcg_variant;
   a.update_state = update_state ? 1 : 0;
   a.xpos = d.x;
   a.vel = d.v;
@@ -717,7 +835,10 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.nloc_max = eng.pcg_nloc_max;
   a.nb_max = eng.pcg_nb_max;
   size_t ov, oro, oc, oS, total;
-  pcg_smem_layout<double>(a.nloc_max, a.nb_max, a.resident, a.cached, &ov, &oro, &oc, &oS, &total);
+  if (eng.precision == B200FEM_PREC_MIXED)
+    pcg_smem_layout<float>(a.nloc_max, a.nb_max, a.resident, a.cached, &ov, &oro, &oc, &oS, &total);
+  else
+    pcg_smem_layout<double>(a.nloc_max, a.nb_max, a.resident, a.cached, &ov, &oro, &oc, &oS, &total);
   if ((int)total > eng.pcg_attr_smem) return cudaErrorInvalidConfiguration;  // prepare_pcg not run
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(eng.pcg_grid);
@@ -729,6 +850,10 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (eng.precision == B200FEM_PREC_MIXED) {
+    a.S = d.S_f;
+    return cudaLaunchKernelEx(&cfg, pcg_kernel<float>, a);
+  }
   return cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
 }
 
@@ -738,22 +863,29 @@ int pcg_threads() { return kPcgThreads; }
 // function: raise it monotonically so one caller never lowers it below what
 // another needs.
 static std::mutex g_pcg_attr_mu;
-static int g_pcg_attr_bytes[64] = {0};
+static int g_pcg_attr_bytes[2][64] = {{0}};
 
-static cudaError_t ensure_pcg_smem(int device, size_t bytes) {
+static cudaError_t ensure_pcg_smem(int device, size_t bytes, bool fp32 = false) {
   std::lock_guard<std::mutex> lk(g_pcg_attr_mu);
   const int d = (device >= 0 && device < 64) ? device : 0;
-  if ((int)bytes <= g_pcg_attr_bytes[d]) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) g_pcg_attr_bytes[d] = (int)bytes;
+  int& cur = g_pcg_attr_bytes[fp32 ? 1 : 0][d];
+  if ((int)bytes <= cur) return cudaSuccess;
+  cudaError_t e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
+                       : cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = (int)bytes;
   return e;
 }
 
 cudaError_t prepare_pcg(Engine& eng) {
   size_t ov, oro, oc, oS, total;
-  pcg_smem_layout<double>(eng.pcg_nloc_max, eng.pcg_nb_max, eng.pcg_resident, eng.pcg_cached, &ov, &oro, &oc, &oS,
-                          &total);
-  cudaError_t e = ensure_pcg_smem(eng.device, total);
+  const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  if (fp32)
+    pcg_smem_layout<float>(eng.pcg_nloc_max, eng.pcg_nb_max, eng.pcg_resident, eng.pcg_cached, &ov, &oro, &oc, &oS,
+                           &total);
+  else
+    pcg_smem_layout<double>(eng.pcg_nloc_max, eng.pcg_nb_max, eng.pcg_resident, eng.pcg_cached, &ov, &oro, &oc, &oS,
+                            &total);
+  cudaError_t e = ensure_pcg_smem(eng.device, total, fp32);
   if (e == cudaSuccess) eng.pcg_attr_smem = (int)total;
   return e;
 }
@@ -761,18 +893,23 @@ cudaError_t prepare_pcg(Engine& eng) {
 // Decide shared-memory residency of the PCG row state and of the S slice
 // for the given per-CTA maxima (rows, blocks) within the device's opt-in
 // shared memory per block.
-void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached) {
+void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached, bool fp32) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   cudaFuncAttributes fa;
-  cudaFuncGetAttributes(&fa, pcg_kernel<double>);
+  if (fp32) cudaFuncGetAttributes(&fa, pcg_kernel<float>);
+  else cudaFuncGetAttributes(&fa, pcg_kernel<double>);
   const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
   size_t ov, oro, oc, oS, total;
   *resident = 0;
   *cached = 0;
-  pcg_smem_layout<double>(nloc_max, nb_max, 1, 0, &ov, &oro, &oc, &oS, &total);
+  auto layout = [&](int res, int cac) {
+    if (fp32) pcg_smem_layout<float>(nloc_max, nb_max, res, cac, &ov, &oro, &oc, &oS, &total);
+    else pcg_smem_layout<double>(nloc_max, nb_max, res, cac, &ov, &oro, &oc, &oS, &total);
+  };
+  layout(1, 0);
   if ((long long)total <= budget) *resident = 1;
-  pcg_smem_layout<double>(nloc_max, nb_max, *resident, 1, &ov, &oro, &oc, &oS, &total);
+  layout(*resident, 1);
   if ((long long)total <= budget) *cached = 1;
 }
 int pcg_max_cta_pieces() { return kMaxCtaPieces; }
@@ -898,7 +1035,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   double step[8] = {0, 0, 0, 0, 0, 0, tol, 0};
   const int nloc_max = (n_rows + G - 1) / G + 1;
   int resident = 0, cached = 0;
-  pcg_plan_smem(device, nloc_max, 0, &resident, &cached);
+  pcg_plan_smem(device, nloc_max, 0, &resident, &cached, false);
   cached = 0;
   size_t ov, oro, oc, oS, dyn;
   pcg_smem_layout<double>(nloc_max, 0, resident, 0, &ov, &oro, &oc, &oS, &dyn);
@@ -959,6 +1096,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.flags = (int*)(base + LY::flags);
   a.unconv = (int*)(base + LY::unconv);
   a.max_iter = max_iter;
+  a.variant = 0;
   a.update_state = 0;
   a.xpos = nullptr;
   a.vel = nullptr;

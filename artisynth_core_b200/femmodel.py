@@ -343,10 +343,11 @@ class MechSystemSolver:
     """BackwardEuler integration of one FemModel3d on the device
     (MechSystemSolver.backwardEuler, MechSystemSolver.java:2171-2476)."""
 
-    def __init__(self, model: FemModel3d, tol: float = 1e-10, max_iter: int = 10000):
+    def __init__(self, model: FemModel3d, tol: float = 1e-10, max_iter: int = 10000, pcg_variant: int = 0):
         self.model = model
         self.tol = tol
         self.max_iter = max_iter
+        self.pcg_variant = pcg_variant
         self.abort_on_inverted = False
         self.stats = L.Stats()
 
@@ -361,6 +362,7 @@ class MechSystemSolver:
         p.tol = self.tol
         p.max_iter = self.max_iter
         p.abort_on_inverted = 1 if self.abort_on_inverted else 0
+        p.pcg_variant = self.pcg_variant
         return p
 
     def backwardEuler(self, h, nsteps=1):
@@ -386,4 +388,96 @@ class MechSystemSolver:
     def lastTiming(self):
         a, s = ctypes.c_double(), ctypes.c_double()
         self.model.engine().call("b200fem_last_timing", ctypes.byref(a), ctypes.byref(s))
+        return a.value, s.value
+
+
+class FemPack:
+    """Batched form: several independent models stepped together in one
+    engine (one pack).  Every kernel launch covers all models; each model
+    keeps its own material, PCG scalars and convergence test."""
+
+    def __init__(self, models, precision=L.PREC_MIXED, device=0):
+        self.models = list(models)
+        self.precision = precision
+        self.device = device
+        self._engine = None
+        self.offsets = None
+        self.stats = L.Stats()
+
+    def engine(self) -> FemEngine:
+        if self._engine is None:
+            eng = FemEngine(self.device, self.precision)
+            for m in self.models:
+                prm = np.zeros(8)
+                p = m.material.params()
+                prm[: len(p)] = p
+                rest = np.ascontiguousarray(m.rest.reshape(-1))
+                conn = np.ascontiguousarray(m.conn.reshape(-1))
+                idx = ctypes.c_int()
+                eng.call("b200fem_add_model", m.elem_type, m.numNodes(), L.dptr(rest), m.numElements(),
+                         L.iptr(conn), L.iptr(m.fixed), m.material.kind, L.dptr(prm), m.density, m.soft_incomp,
+                         ctypes.byref(idx))
+            eng.call("b200fem_build")
+            self._engine = eng
+            self.offsets = []
+            for i in range(len(self.models)):
+                o, n, a = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+                eng.call("b200fem_model_range", i, ctypes.byref(o), ctypes.byref(n), ctypes.byref(a))
+                self.offsets.append((o.value, n.value, a.value))
+            fext = [m.fext if m.fext is not None else np.zeros((m.numNodes(), 3)) for m in self.models]
+            if any(m.fext is not None for m in self.models):
+                f = np.ascontiguousarray(np.concatenate(fext).reshape(-1))
+                eng.call("b200fem_set_external_forces", L.dptr(f))
+        return self._engine
+
+    def close(self):
+        if self._engine is not None:
+            self._engine.close()
+            self._engine = None
+
+    def total_nodes(self):
+        return sum(m.numNodes() for m in self.models)
+
+    def setStates(self, xs=None, vs=None):
+        e = self.engine()
+        xe = None if xs is None else np.ascontiguousarray(np.concatenate([np.asarray(x).reshape(-1, 3) for x in xs]).reshape(-1))
+        ve = None if vs is None else np.ascontiguousarray(np.concatenate([np.asarray(v).reshape(-1, 3) for v in vs]).reshape(-1))
+        e.call("b200fem_set_state", L.dptr(xe), L.dptr(ve))
+
+    def getStates(self):
+        e = self.engine()
+        n = self.total_nodes()
+        x = np.zeros(3 * n)
+        v = np.zeros(3 * n)
+        e.call("b200fem_get_state", L.dptr(x), L.dptr(v))
+        x = x.reshape(-1, 3)
+        v = v.reshape(-1, 3)
+        return [(x[o:o + k], v[o:o + k]) for (o, k, _) in self.offsets]
+
+    def backwardEuler(self, h, nsteps=1, tol=1e-10, max_iter=20000, alpha=None, beta=None, gravity=None,
+                      pcg_variant=0):
+        m0 = self.models[0]
+        p = L.StepParams()
+        p.h = h
+        p.alpha_m = m0.mass_damping if alpha is None else alpha
+        p.beta_k = m0.stiffness_damping if beta is None else beta
+        g = m0.gravity if gravity is None else gravity
+        for i in range(3):
+            p.gravity[i] = g[i]
+        p.tol = tol
+        p.max_iter = max_iter
+        p.pcg_variant = pcg_variant
+        self.engine().call("b200fem_backward_euler_step", ctypes.byref(p), int(nsteps), ctypes.byref(self.stats))
+        return self.stats
+
+    def modelStats(self):
+        n = len(self.models)
+        it = np.zeros(n, dtype=np.int32)
+        rr = np.zeros(n)
+        self.engine().call("b200fem_get_model_stats", L.iptr(it), L.dptr(rr))
+        return it, rr
+
+    def lastTiming(self):
+        a, s = ctypes.c_double(), ctypes.c_double()
+        self.engine().call("b200fem_last_timing", ctypes.byref(a), ctypes.byref(s))
         return a.value, s.value

@@ -135,3 +135,25 @@ def small_hex_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.0
                    gravity=(0.0, 0.0, -9.81), h=0.005, steps=10) -> Workload:
     return Workload("small_hex_beam", L.ELEM_HEX, cells, widths, jitter, seed, material, 1000.0, "xmin",
                     gravity, h, steps, tol=1e-13)
+
+
+def batched_beams(count=256, seed=3, cell=0.05, jitter=0.05, large_frac=0.0, large_n=(80, 120)):
+    """Uneven NeoHookean tet beams: n x m x m cells of size `cell` (5 tets per
+    cell), n ~ U{4..60}, m ~ U{2..8}, E log-uniform in [1e3, 1e6] Pa, nu
+    uniform in [0.30, 0.49], density 1000, x-min face fixed, gravity; 20
+    steps of h = 0.01.  With large_frac > 0 that fraction of the beams draws
+    n ~ U{80..120} instead (the served-stream distribution)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(4, 61))
+        if large_frac and rng.random() < large_frac:
+            n = int(rng.integers(large_n[0], large_n[1] + 1))
+        m = int(rng.integers(2, 9))
+        E = float(10 ** rng.uniform(3, 6))
+        nu = float(rng.uniform(0.30, 0.49))
+        wl = Workload(f"beam{i}_{n}x{m}x{m}", L.ELEM_TET, (n, m, m), (n * cell, m * cell, m * cell), jitter,
+                      1000 + i, NeoHookeanMaterial(E, nu), 1000.0, "xmin", (0.0, 0.0, -9.81), 0.01, 20,
+                      tol=1e-10)
+        out.append(wl)
+    return out

@@ -91,6 +91,10 @@ typedef struct {
   double tol;        /* PCG relative residual ||b - S v|| / ||b|| */
   int max_iter;      /* PCG iteration cap (ERR_NO_CONVERGE beyond it) */
   int abort_on_inverted; /* FemModel3d.abortOnInvertedElems */
+  int pcg_variant;   /* 0 auto: pipelined CG (one grid barrier per iteration),
+                        switching to classic PCG after a residual replacement;
+                        1 classic PCG (two barriers, better attainable accuracy);
+                        2 pipelined only */
 } b200fem_step_params;
 
 typedef struct {
@@ -168,6 +172,25 @@ int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, 
                       b200fem_stats* stats);
 /* synchronise and report the device time of the last step/update call */
 int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms);
+
+/* ---- batched form: several independent models in one handle ------------- */
+/* The handle's models form one "pack": one element type, any mix of
+   materials; kernels run over all models at once (each PCG launch solves
+   every model, each with its own scalars and convergence test).
+   b200fem_set_mesh/_set_material define model 0; b200fem_add_model appends
+   (or fills model 0 while it is empty).  State arrays of set_state,
+   get_state and set_external_forces are the models' node arrays
+   concatenated in model order; b200fem_model_range gives each slice. */
+int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz,
+                      int n_elems, const int* conn, const int* fixed, int mat_kind,
+                      const double* params, double density, int incomp_method, int* model_index);
+int b200fem_clear_models(b200fem_handle h);
+int b200fem_num_models(b200fem_handle h, int* n_models);
+/* node offset and count of one model in the concatenated state arrays, and
+   its active block rows (DOF / 3) */
+int b200fem_model_range(b200fem_handle h, int model, int* node_offset, int* n_nodes, int* n_active);
+/* per-model PCG iterations and true relative residuals of the last solve */
+int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_residual);
 
 /* ---- allocation-free solve ---------------------------------------------- */
 /* Size limits of b200fem_pcg_solve_noalloc: its scratch is one fixed device

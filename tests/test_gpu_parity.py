@@ -210,3 +210,39 @@ def test_mooneyrivlin_block_nodal_steps(oracle):
     xg, vg, x, v, ms = _run_pair(wl, oracle, 5, 0, 1e-12)
     assert rel_err(xg, x) <= POS_TOL
     assert rel_err(xg - wl.rest, x - wl.rest) <= 1e-6
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_pcg_variants_agree_with_oracle(cases, oracle, variant):
+    """Classic (two barriers) and pipelined-only PCG both reach the oracle."""
+    wl = cases["neohookean_hex"]
+    m = _gpu_model(wl)
+    om = oracle_model(oracle, wl)
+    x = wl.rest.copy()
+    v = np.zeros_like(x)
+    for _ in range(wl.steps):
+        om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, solver=1)
+    MechSystemSolver(m, tol=1e-13, max_iter=20000, pcg_variant=variant).backwardEuler(wl.h, wl.steps)
+    xg, _ = m.getState()
+    assert rel_err(xg, x) <= POS_TOL
+
+
+def test_stiff_beam_reaches_tight_tolerance(b200, oracle):
+    """A stiff beam (E = 9.6e5 Pa at h = 0.01, Jacobi-PCG needs thousands of
+    iterations) at 1e-12: the auto variant falls back to classic PCG when the
+    pipelined recurrences stall, and matches the dense oracle."""
+    wl = W.batched_beams(count=6, seed=5)[4]
+    wl.cells = (12, wl.cells[1], wl.cells[2])
+    wl.widths = (12 * 0.05, wl.widths[1], wl.widths[2])
+    wl.build_mesh()
+    m = _gpu_model(wl)
+    ms = MechSystemSolver(m, tol=1e-12, max_iter=20000)
+    om = oracle_model(oracle, wl)
+    x = wl.rest.copy()
+    v = np.zeros_like(x)
+    for _ in range(3):
+        om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, solver=1)
+        ms.backwardEuler(wl.h, 1)
+        assert ms.stats.rel_residual <= 1e-12
+    xg, _ = m.getState()
+    assert rel_err(xg, x) <= POS_TOL
