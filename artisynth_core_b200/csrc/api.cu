@@ -366,6 +366,12 @@ int build_pack(Engine& eng) {
   }
   pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
                 eng.precision == B200FEM_PREC_MIXED);
+  // default SpMV row width: about one block per lane (tuned later by the
+  // autotuner): tets ~15 blocks per row -> 16 lanes, hexes ~27 -> 32
+  {
+    const double bpr = R > 0 ? (double)NB / R : 1.0;
+    eng.pcg_row_lanes = bpr <= 10 ? 8 : (bpr <= 20 ? 16 : 32);
+  }
 
   // ---- device upload
   CK(upload(eng, &d.x, x));

@@ -178,6 +178,7 @@ struct Engine {
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
+  int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)
   // captured BackwardEuler step (element, gather, RHS, PCG) and its events
   cudaGraphExec_t asm_exec = nullptr;
   cudaGraphExec_t step_exec = nullptr;

@@ -110,6 +110,7 @@ struct PcgArgs {
   int* unconv;  // per iteration: some model still unconverged
   int max_iter;
   int variant;  // 0 auto (pipelined, classic after a residual replacement), 1 classic, 2 pipelined
+  int row_lanes;  // lanes per block row in the iteration SpMV (8, 16, 32)
   int update_state;
   double* xpos;
   double* vel;
@@ -294,6 +295,73 @@ __device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int row, co
   y[0] = a0;
   y[1] = a1;
   y[2] = a2;
+}
+
+// Several rows per warp: lanes are split into groups of L (8, 16 or 32);
+// each group walks one row's blocks with stride L and reduces with
+// shuffles inside the group, so 32/L rows are in flight per warp.  The loop
+// runs a warp-uniform number of times; groups whose row is past the end
+// contribute nothing.
+template <typename MT, int L>
+__device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int row, bool valid,
+                                                     const double* __restrict__ x, int lane, double* y) {
+  int p0 = 0, p1 = 0;
+  const int* col;
+  const MT* S;
+  if (mv.cached) {
+    col = mv.col_s;
+    S = mv.S_s;
+    if (valid) {
+      p0 = mv.ro_s[row - mv.r0];
+      p1 = mv.ro_s[row - mv.r0 + 1];
+    }
+  } else {
+    col = mv.col;
+    S = mv.S;
+    if (valid) {
+      p0 = mv.rowptr[row];
+      p1 = mv.rowptr[row + 1];
+    }
+  }
+  const int gl = lane & (L - 1);
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int p = p0 + gl; p < p1; p += L) {
+    const int c = col[p];
+    const MT* B = S + (size_t)p * 9;
+    double b[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+    const double x0 = x[3 * (size_t)c], x1 = x[3 * (size_t)c + 1], x2 = x[3 * (size_t)c + 2];
+    a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
+    a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
+    a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
+  }
+#pragma unroll
+  for (int off = L / 2; off > 0; off >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+  }
+  y[0] = a0;
+  y[1] = a1;
+  y[2] = a2;
+}
+
+template <typename MT, int L>
+__device__ __forceinline__ void spmv_rows_to_smem(const MatView<MT>& mv, const double* __restrict__ x, int c0,
+                                                  int c1, int warp, int nroww, int lane, double (*sn)[3]) {
+  constexpr int G = 32 / L;
+  for (int base = c0 + warp * G; base < c1; base += nroww * G) {
+    const int row = base + lane / L;
+    const bool valid = row < c1;
+    double n[3];
+    view_rows_spmv_group<MT, L>(mv, row, valid, x, lane, n);
+    if (valid && (lane & (L - 1)) == 0) {
+      sn[row - c0][0] = n[0];
+      sn[row - c0][1] = n[1];
+      sn[row - c0][2] = n[2];
+    }
+  }
 }
 
 // dynamic shared memory layout of the PCG kernel
@@ -559,15 +627,9 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       for (int c0 = r0, first = 1; c0 < r1 || first; c0 += kRowChunk, first = 0) {
         const int c1 = min(c0 + kRowChunk, r1);
         if (warp < nroww) {
-          for (int row = c0 + warp; row < c1; row += nroww) {
-            double n[3];
-            view_row_spmv<MT>(mv, row, mc, lane, n);
-            if (lane == 0) {
-              sn[row - c0][0] = n[0];
-              sn[row - c0][1] = n[1];
-              sn[row - c0][2] = n[2];
-            }
-          }
+          if (a.row_lanes == 8) spmv_rows_to_smem<MT, 8>(mv, mc, c0, c1, warp, nroww, lane, sn);
+          else if (a.row_lanes == 16) spmv_rows_to_smem<MT, 16>(mv, mc, c0, c1, warp, nroww, lane, sn);
+          else spmv_rows_to_smem<MT, 32>(mv, mc, c0, c1, warp, nroww, lane, sn);
         } else if (first) {
           // reduce this iteration's scalars and form alpha, beta; the
           // convergence test is on the recurrence residual
@@ -825,6 +887,7 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.unconv = d.unconv;
   a.max_iter = max_iter;
   a.variant = eng.pcg_variant;
+  a.row_lanes = eng.pcg_row_lanes;
   a.update_state = update_state ? 1 : 0;
   a.xpos = d.x;
   a.vel = d.v;
@@ -1097,6 +1160,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.unconv = (int*)(base + LY::unconv);
   a.max_iter = max_iter;
   a.variant = 0;
+  a.row_lanes = 16;
   a.update_state = 0;
   a.xpos = nullptr;
   a.vel = nullptr;
