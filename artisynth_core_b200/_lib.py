@@ -32,6 +32,8 @@ INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 PART_FULL, PART_UPPER = 0, 1
 PCG_AUTO, PCG_CLASSIC, PCG_PIPELINED = 0, 1, 2
+OPT_PCG_SPLIT, OPT_ROW_LANES, OPT_PCG_CTAS, OPT_PIECE_ROWS = 1, 2, 3, 4
+SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED = 0, 1, 2
 
 
 class B200FemError(RuntimeError):
@@ -127,6 +129,8 @@ def lib():
         "b200fem_num_models": ([H, _ip], ctypes.c_int),
         "b200fem_model_range": ([H, ctypes.c_int, _ip, _ip, _ip], ctypes.c_int),
         "b200fem_get_model_stats": ([H, _ip, _dp], ctypes.c_int),
+        "b200fem_set_option": ([H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "b200fem_get_option": ([H, ctypes.c_int, _ip], ctypes.c_int),
         "b200fem_pcg_solve_noalloc": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
                                        _ip, _dp], ctypes.c_int),
     }

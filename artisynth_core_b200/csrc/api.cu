@@ -316,12 +316,14 @@ int build_pack(Engine& eng) {
     }
   }
 
-  // ---- PCG work split: CTAs own contiguous row ranges balanced by blocks,
-  // cut into pieces at model boundaries
-  // one 1024-thread CTA per SM at most, >= 32 rows (one per warp) each
+  // ---- PCG work split.  Contiguous: CTAs own contiguous row ranges
+  // balanced by blocks, cut into pieces at model boundaries.
+  // One 1024-thread CTA per SM at most, >= 32 rows (one per warp) each.
   int gmax = std::min(pcg_max_grid(eng.device), eng.num_sms);
+  if (eng.opt_ctas > 0) gmax = std::min(gmax, eng.opt_ctas);
   int G = std::max(1, std::min(gmax, (R + 31) / 32));
   std::vector<int> piece_row, piece_model, cta_piece, model_piece(M + 1, 0);
+  bool contiguous_ok = true;
   for (;;) {
     piece_row.clear();
     piece_model.clear();
@@ -350,13 +352,16 @@ int build_pack(Engine& eng) {
     cta_piece[G] = (int)piece_model.size();
     piece_row.push_back(R);
     if (maxp <= pcg_max_cta_pieces()) break;
-    if (G >= gmax) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for one PCG launch");
+    if (G >= gmax) {
+      // no contiguous split fits: the strided split below takes over
+      if (M <= 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many pieces for one PCG launch");
+      contiguous_ok = false;
+      break;
+    }
     G = std::min(gmax, G * 2);
   }
-  for (size_t k = 0; k < piece_model.size(); k++) model_piece[piece_model[k] + 1] = (int)k + 1;
-  for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
-  eng.pcg_grid = G;
-  d.n_pieces = (int)piece_model.size();
+  std::vector<int> cta_plist(piece_model.size());
+  for (size_t k = 0; k < cta_plist.size(); k++) cta_plist[k] = (int)k;
   eng.pcg_nloc_max = 0;
   eng.pcg_nb_max = 0;
   for (int c = 0; c < G; c++) {
@@ -366,9 +371,82 @@ int build_pack(Engine& eng) {
   }
   pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
                 eng.precision == B200FEM_PREC_MIXED);
+  eng.pcg_strided = 0;
+  if (!contiguous_ok) {
+    if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
+    eng.pcg_resident = eng.pcg_cached = 0;
+  }
+  if (eng.opt_split == 2 || (eng.opt_split == 0 && !eng.pcg_resident && M > 1)) {
+    // Strided split for packs too large for shared-memory residency: every
+    // model is cut into short pieces and each piece goes to the least-loaded
+    // CTA, so a model's rows are spread over many SMs.  When most models
+    // have converged, the iterations left for the slow ones then run on the
+    // whole GPU instead of on the few CTAs that would hold them.
+    G = std::max(1, std::min(gmax, (R + 31) / 32));
+    const double row_cost = 400.0, blk_cost = 9.0 * (eng.precision == B200FEM_PREC_MIXED ? 4 : 8) + 4 + 24;
+    for (int P = eng.opt_piece_rows > 0 ? eng.opt_piece_rows : 64;; P *= 2) {
+      piece_row.clear();
+      piece_model.clear();
+      for (int m = 0; m < M; m++) {
+        const int a = eng.row_off[m], n = eng.row_off[m + 1] - a;
+        if (n <= 0) continue;
+        const int k = (n + P - 1) / P;
+        for (int t = 0; t < k; t++) {
+          piece_row.push_back(a + (int)((long long)n * t / k));
+          piece_model.push_back(m);
+        }
+      }
+      piece_row.push_back(R);
+      const int np = (int)piece_model.size();
+      std::vector<int> owner(np), count(G, 0);
+      std::vector<std::pair<double, int>> heap;
+      for (int c = 0; c < G; c++) heap.push_back({0.0, c});
+      auto later = [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+        return x.first != y.first ? x.first > y.first : x.second > y.second;
+      };
+      std::make_heap(heap.begin(), heap.end(), later);
+      int maxp = 0;
+      for (int k = 0; k < np; k++) {
+        std::pop_heap(heap.begin(), heap.end(), later);
+        auto& top = heap.back();
+        const int ra = piece_row[k], rb = piece_row[k + 1];
+        owner[k] = top.second;
+        top.first += row_cost * (rb - ra) + blk_cost * (rowptr[rb] - rowptr[ra]);
+        maxp = std::max(maxp, ++count[top.second]);
+        std::push_heap(heap.begin(), heap.end(), later);
+      }
+      if (maxp > pcg_max_cta_pieces()) {
+        if (P >= R) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for one PCG launch");
+        continue;
+      }
+      cta_piece.assign(G + 1, 0);
+      for (int k = 0; k < np; k++) cta_piece[owner[k] + 1]++;
+      for (int c = 0; c < G; c++) cta_piece[c + 1] += cta_piece[c];
+      cta_plist.assign(np, 0);
+      std::vector<int> fill(cta_piece.begin(), cta_piece.end() - 1);
+      for (int k = 0; k < np; k++) cta_plist[fill[owner[k]]++] = k;
+      eng.pcg_nloc_max = 0;
+      for (int c = 0; c < G; c++) {
+        int rows = 0;
+        for (int q = cta_piece[c]; q < cta_piece[c + 1]; q++)
+          rows += piece_row[cta_plist[q] + 1] - piece_row[cta_plist[q]];
+        eng.pcg_nloc_max = std::max(eng.pcg_nloc_max, rows);
+      }
+      eng.pcg_nb_max = 0;
+      eng.pcg_resident = eng.pcg_cached = 0;
+      eng.pcg_strided = 1;
+      break;
+    }
+  }
+  for (size_t k = 0; k < piece_model.size(); k++) model_piece[piece_model[k] + 1] = (int)k + 1;
+  for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
+  eng.pcg_grid = G;
+  d.n_pieces = (int)piece_model.size();
   // default SpMV row width: about one block per lane (tuned later by the
   // autotuner): tets ~15 blocks per row -> 16 lanes, hexes ~27 -> 32
-  {
+  if (eng.opt_row_lanes > 0) {
+    eng.pcg_row_lanes = eng.opt_row_lanes;
+  } else {
     const double bpr = R > 0 ? (double)NB / R : 1.0;
     eng.pcg_row_lanes = bpr <= 10 ? 8 : (bpr <= 20 ? 16 : 32);
   }
@@ -439,6 +517,7 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.piece_model, piece_model));
   CK(upload(eng, &d.model_piece, model_piece));
   CK(upload(eng, &d.cta_piece, cta_piece));
+  CK(upload(eng, &d.cta_plist, cta_plist));
   d.unconv_cap = 200000;
   CK(dalloc(eng, &d.unconv, (size_t)d.unconv_cap + 2));
   {
@@ -684,6 +763,51 @@ int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_resid
 int b200fem_build(b200fem_handle h) {
   ENG(h);
   return build_pack(eng);
+}
+
+int b200fem_set_option(b200fem_handle h, int key, int value) {
+  ENG(h);
+  switch (key) {
+    case B200FEM_OPT_PCG_SPLIT:
+      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_SPLIT must be 0, 1 or 2");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_SPLIT is set before b200fem_build");
+      eng.opt_split = value;
+      return B200FEM_OK;
+    case B200FEM_OPT_PCG_CTAS:
+      if (value < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_CTAS must be >= 0");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_CTAS is set before b200fem_build");
+      eng.opt_ctas = value;
+      return B200FEM_OK;
+    case B200FEM_OPT_PIECE_ROWS:
+      if (value < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PIECE_ROWS must be >= 0");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PIECE_ROWS is set before b200fem_build");
+      eng.opt_piece_rows = value;
+      return B200FEM_OK;
+    case B200FEM_OPT_ROW_LANES:
+      if (value != 0 && value != 8 && value != 16 && value != 32)
+        return fail(&eng, B200FEM_ERR_INVALID_ARG, "ROW_LANES must be 0, 8, 16 or 32");
+      eng.opt_row_lanes = value;
+      if (eng.built && value != 0 && value != eng.pcg_row_lanes) {
+        eng.pcg_row_lanes = value;
+        eng.step_exec_max_iter = -1;  // recapture: the width is a kernel argument
+      }
+      return B200FEM_OK;
+    default:
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
+  }
+}
+
+int b200fem_get_option(b200fem_handle h, int key, int* value) {
+  ENG(h);
+  if (!value) return fail(&eng, B200FEM_ERR_INVALID_ARG, "null value");
+  switch (key) {
+    case B200FEM_OPT_PCG_SPLIT: *value = eng.built ? (eng.pcg_strided ? 2 : 1) : eng.opt_split; break;
+    case B200FEM_OPT_ROW_LANES: *value = eng.built ? eng.pcg_row_lanes : eng.opt_row_lanes; break;
+    case B200FEM_OPT_PCG_CTAS: *value = eng.built ? eng.pcg_grid : eng.opt_ctas; break;
+    case B200FEM_OPT_PIECE_ROWS: *value = eng.opt_piece_rows; break;
+    default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
+  }
+  return B200FEM_OK;
 }
 
 int b200fem_get_sizes(b200fem_handle h, int* n_active, int* nnzb, int* crs_full, int* crs_upper) {

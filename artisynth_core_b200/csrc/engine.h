@@ -131,6 +131,7 @@ struct DevPack {
   int* piece_model = nullptr;  // n_pieces
   int* model_piece = nullptr;  // n_models+1
   int* cta_piece = nullptr;    // pcg_grid+1
+  int* cta_plist = nullptr;    // n_pieces: global piece indices, CTA-major
   int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
   int unconv_cap = 0;
   int n_pieces = 0;
@@ -176,6 +177,9 @@ struct Engine {
   // pcg launch geometry
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
+  int pcg_strided = 0;  // pieces dealt to CTAs across models (large packs)
+  // tuning options (B200FEM_OPT_*): 0 = automatic
+  int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)

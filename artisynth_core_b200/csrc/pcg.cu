@@ -9,14 +9,19 @@
 // true residual b - S x is formed; if it exceeds the tolerance the
 // recurrences are restarted from it (residual replacement).
 //
-// Work split: every CTA owns a contiguous range of block rows, cut into
-// "pieces" at model boundaries (a pack may hold many models).  Dot products
+// Work split: every CTA owns a list of "pieces" (row ranges of one model).
+// In the contiguous split the pieces of a CTA are adjacent (a contiguous row
+// range cut at model boundaries), which lets the row state and the CTA's
+// slice of S live in shared memory; in the strided split, for packs too
+// large for that, every model is cut into short pieces dealt over all CTAs.
+// Passes over rows skip the models that have converged.  Dot products
 // are reduced per piece in a fixed order (warp shuffles, then shared
 // memory), partial sums are written to a double-buffered table, and each
 // model's scalars are summed from its pieces in a fixed order after the
 // barrier: results are bit-reproducible and independent of timing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "device_math.cuh"
@@ -29,8 +34,10 @@ constexpr int kPcgThreads = 1024;
 constexpr int kRowChunk = 512;
 constexpr int kMaxCtaPieces = 48;
 constexpr int kMaxRestarts = 10;
-// auto variant: pipelined iterations allowed before switching to classic PCG
-constexpr int kPipelinedCap = 400;
+// auto variant: iterations of one round (pipelined, then classic after the
+// first restart) before the true residual is checked and the recurrences
+// restart from it
+constexpr int kRoundCap = 400;
 constexpr unsigned long long kBarrierTimeoutNs = 5000000000ull;
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -97,7 +104,8 @@ struct PcgArgs {
   const int* piece_row;
   const int* piece_model;
   const int* model_piece;
-  const int* cta_piece;
+  const int* cta_piece;  // CTA c owns entries [cta_piece[c], cta_piece[c+1]) of cta_plist
+  const int* cta_plist;  // global piece indices, CTA-major
   double* partials;  // [2][n_pieces][4]
   const double* step;
   double* model_out;  // n_models * 4: iterations, true rel residual, converged
@@ -118,47 +126,76 @@ struct PcgArgs {
   const int* row_model;
 };
 
-struct CtaView {
-  int pc0, pc1;
+// The rows a CTA owns: its local pieces j = 0..npc-1 (global piece gp[j],
+// first global row grow[j]) laid end to end in a local row space
+// [0, nloc); local piece j covers local rows [lst0[j], lst0[j+1]).  In the
+// contiguous split the pieces are adjacent global row ranges (row = r0 + i);
+// in the strided split they are short row ranges of different models,
+// spread over the CTAs so that every model's rows are shared by many SMs.
+// A view may leave pieces out (those of converged models): its row space
+// lays only the remaining pieces end to end (lst), so passes over it cost
+// in proportion to the rows still iterating.
+struct CtaRows {
+  const int* gp;
+  const int* lst;   // start of piece j in this view's row space
+  const int* lst0;  // start of piece j in the local row space
+  const int* grow;
+  int npc, nloc;
+  // the piece holding view row i: the last j with lst[j] <= i (left-out
+  // pieces have zero length and are never returned for a valid row)
+  __device__ __forceinline__ int piece(int i) const {
+    int lo = 0, hi = npc - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (lst[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ int row(int i, int j) const { return grow[j] + (i - lst[j]); }
+  __device__ __forceinline__ int local(int i, int j) const { return lst0[j] + (i - lst[j]); }
 };
 
-// Reduce ND per-row values over this CTA's pieces in a fixed order and write
-// partials[buf][piece][k].  fn(row, lane, vals) runs per row, either by a
-// whole warp (WARP_ROWS) or by one thread.
+// Reduce ND per-row values over the view's pieces in a fixed order and write
+// partials[buf][piece][k] for every local piece (zero for pieces the view
+// leaves out).  fn(i, row, j, lane, vals) runs per row (local row i, global
+// row `row`, local piece j), either by a whole warp (WARP_ROWS) or by one
+// thread.
 template <int ND, bool WARP_ROWS, typename Fn>
-__device__ void cta_row_pass(const PcgArgs& a, CtaView cv, int buf, double (*rowbuf)[3], double (*pacc)[3],
-                             Fn fn) {
+__device__ void cta_row_pass(const PcgArgs& a, const CtaRows& cr, int buf, double (*rowbuf)[3],
+                             double (*pacc)[3], Fn fn) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int npc = cv.pc1 - cv.pc0;
+  const int npc = cr.npc;
   for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
-  const int r0 = a.piece_row[cv.pc0], r1 = a.piece_row[cv.pc1];
-  for (int c0 = r0; c0 < r1; c0 += kRowChunk) {
-    const int c1 = min(c0 + kRowChunk, r1);
+  for (int c0 = 0; c0 < cr.nloc; c0 += kRowChunk) {
+    const int c1 = min(c0 + kRowChunk, cr.nloc);
     __syncthreads();
     if (WARP_ROWS) {
-      for (int row = c0 + warp; row < c1; row += nwarps) {
+      for (int i = c0 + warp; i < c1; i += nwarps) {
+        const int j = cr.piece(i);
         double vals[3] = {0, 0, 0};
-        fn(row, lane, vals);
+        fn(cr.local(i, j), cr.row(i, j), j, lane, vals);
         if (lane == 0)
 #pragma unroll
-          for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
+          for (int k = 0; k < ND; k++) rowbuf[i - c0][k] = vals[k];
       }
     } else {
-      for (int row = c0 + (int)threadIdx.x; row < c1; row += blockDim.x) {
+      for (int i = c0 + (int)threadIdx.x; i < c1; i += blockDim.x) {
+        const int j = cr.piece(i);
         double vals[3] = {0, 0, 0};
-        fn(row, 0, vals);
+        fn(cr.local(i, j), cr.row(i, j), j, 0, vals);
 #pragma unroll
-        for (int k = 0; k < ND; k++) rowbuf[row - c0][k] = vals[k];
+        for (int k = 0; k < ND; k++) rowbuf[i - c0][k] = vals[k];
       }
     }
     __syncthreads();
     for (int j = warp; j < npc; j += nwarps) {
-      const int pr0 = max(a.piece_row[cv.pc0 + j], c0), pr1 = min(a.piece_row[cv.pc0 + j + 1], c1);
+      const int pr0 = max(cr.lst[j], c0), pr1 = min(cr.lst[j + 1], c1);
       if (pr0 >= pr1) continue;
       double sm[3] = {0, 0, 0};
-      for (int row = pr0 + lane; row < pr1; row += 32)
+      for (int i = pr0 + lane; i < pr1; i += 32)
 #pragma unroll
-        for (int k = 0; k < ND; k++) sm[k] += rowbuf[row - c0][k];
+        for (int k = 0; k < ND; k++) sm[k] += rowbuf[i - c0][k];
 #pragma unroll
       for (int k = 0; k < ND; k++)
 #pragma unroll
@@ -172,17 +209,18 @@ __device__ void cta_row_pass(const PcgArgs& a, CtaView cv, int buf, double (*row
   double* out = a.partials + (size_t)buf * a.n_pieces * 4;
   for (int j = threadIdx.x; j < npc; j += blockDim.x)
 #pragma unroll
-    for (int k = 0; k < ND; k++) out[(size_t)(cv.pc0 + j) * 4 + k] = pacc[j][k];
+    for (int k = 0; k < ND; k++) out[(size_t)cr.gp[j] * 4 + k] = pacc[j][k];
 }
 
 // Per local piece: sum of the partials of its model (warp per piece, fixed
-// lane striding and butterfly order).
+// lane striding and butterfly order); pieces with skip[j] set are left out.
 template <int ND>
-__device__ void model_sums(const PcgArgs& a, CtaView cv, int buf, double (*out)[3]) {
+__device__ void model_sums(const PcgArgs& a, const CtaRows& cr, int buf, double (*out)[3], const int* skip) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const double* src = a.partials + (size_t)buf * a.n_pieces * 4;
-  for (int j = warp; j < cv.pc1 - cv.pc0; j += nwarps) {
-    const int m = a.piece_model[cv.pc0 + j];
+  for (int j = warp; j < cr.npc; j += nwarps) {
+    if (skip && skip[j]) continue;
+    const int m = a.piece_model[cr.gp[j]];
     const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
     double sm[3] = {0, 0, 0};
     for (int qq = q0 + lane; qq < q1; qq += 32)
@@ -197,12 +235,6 @@ __device__ void model_sums(const PcgArgs& a, CtaView cv, int buf, double (*out)[
       for (int k = 0; k < ND; k++) out[j][k] = sm[k];
   }
   __syncthreads();
-}
-
-__device__ __forceinline__ int piece_of_row(const PcgArgs& a, CtaView cv, int row) {
-  int j = 0;
-  while (cv.pc0 + j + 1 < cv.pc1 && a.piece_row[cv.pc0 + j + 1] <= row) j++;
-  return j;
 }
 
 __device__ __forceinline__ void load3(double* d, const double* src, int row) {
@@ -225,26 +257,28 @@ __device__ __forceinline__ double dot3(const double* a, const double* b) {
 
 // Row-local PCG state: the vectors x r u w z q s p and the block-Jacobi
 // inverse of the CTA's own rows.  In resident mode they live in shared
-// memory for the whole solve (only the owning CTA ever touches them); the
-// search-direction vectors read by neighbouring rows (u at the start, m in
-// the iteration, x for the true residual) are published to global memory.
+// memory for the whole solve (only the owning CTA ever touches them) and
+// are indexed by local row; otherwise they are the global vectors indexed by
+// global row.  The search-direction vectors read by neighbouring rows (u at
+// the start, m in the iteration, x for the true residual) are published to
+// global memory.
 struct RowState {
   double* v[9];
   double* D;
-  int r0;
   int res;
-  __device__ __forceinline__ double* at(int k, int row) const {
-    return res ? v[k] + 3 * (row - r0) : v[k] + 3 * (size_t)row;
+  __device__ __forceinline__ double* at(int k, int i, int row) const {
+    return res ? v[k] + 3 * i : v[k] + 3 * (size_t)row;
   }
-  __device__ __forceinline__ double* dinv(int row) const {
-    return res ? D + 9 * (row - r0) : D + 9 * (size_t)row;
+  __device__ __forceinline__ double* dinv(int i, int row) const {
+    return res ? D + 9 * i : D + 9 * (size_t)row;
   }
 };
 enum { VX = 0, VR, VU, VW, VZ, VQ, VS, VP, VM };
 
-// The CTA's rows [r0, r1) own the contiguous block range [pbase, pend):
-// when it fits, the values, block columns and row offsets are copied to
-// shared memory once per solve and every SpMV of the solve reads them there.
+// In the contiguous split a CTA's rows own the contiguous block range
+// [pbase, pend): when it fits, the values, block columns and row offsets
+// are copied to shared memory once per solve and every SpMV of the solve
+// reads them there (indexed by local row).
 template <typename MT>
 struct MatView {
   const int* rowptr;
@@ -253,19 +287,22 @@ struct MatView {
   const int* ro_s;
   const int* col_s;
   const MT* S_s;
-  int r0;
   int cached;
 };
 
+// The vectors these SpMVs read (the search direction m, the iterate x) are
+// rewritten by other CTAs between grid barriers, so they are read with plain
+// coherent loads: no __restrict__/read-only-cache path, which is only valid
+// for data that stays unchanged for the whole launch.
 template <typename MT>
-__device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int row, const double* __restrict__ x,
-                                              int lane, double* y) {
+__device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int i, int row, const double* x, int lane,
+                                              double* y) {
   int p0, p1;
   const int* col;
   const MT* S;
   if (mv.cached) {
-    p0 = mv.ro_s[row - mv.r0];
-    p1 = mv.ro_s[row - mv.r0 + 1];
+    p0 = mv.ro_s[i];
+    p1 = mv.ro_s[i + 1];
     col = mv.col_s;
     S = mv.S_s;
   } else {
@@ -299,12 +336,11 @@ __device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int row, co
 
 // Several rows per warp: lanes are split into groups of L (8, 16 or 32);
 // each group walks one row's blocks with stride L and reduces with
-// shuffles inside the group, so 32/L rows are in flight per warp.  The loop
-// runs a warp-uniform number of times; groups whose row is past the end
-// contribute nothing.
+// shuffles inside the group, so 32/L rows are in flight per warp.  Groups
+// whose row is past the end contribute nothing.
 template <typename MT, int L>
-__device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int row, bool valid,
-                                                     const double* __restrict__ x, int lane, double* y) {
+__device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int i, int row, bool valid,
+                                                     const double* x, int lane, double* y) {
   int p0 = 0, p1 = 0;
   const int* col;
   const MT* S;
@@ -312,8 +348,8 @@ __device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int 
     col = mv.col_s;
     S = mv.S_s;
     if (valid) {
-      p0 = mv.ro_s[row - mv.r0];
-      p1 = mv.ro_s[row - mv.r0 + 1];
+      p0 = mv.ro_s[i];
+      p1 = mv.ro_s[i + 1];
     }
   } else {
     col = mv.col;
@@ -347,21 +383,50 @@ __device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int 
   y[2] = a2;
 }
 
+// n = S x for the rows [c0, c1) of the view `ar` into sn.
 template <typename MT, int L>
-__device__ __forceinline__ void spmv_rows_to_smem(const MatView<MT>& mv, const double* __restrict__ x, int c0,
-                                                  int c1, int warp, int nroww, int lane, double (*sn)[3]) {
+__device__ __forceinline__ void spmv_rows_to_smem(const MatView<MT>& mv, const CtaRows& ar, const double* x,
+                                                  int c0, int c1, int warp, int nroww, int lane,
+                                                  double (*sn)[3]) {
   constexpr int G = 32 / L;
   for (int base = c0 + warp * G; base < c1; base += nroww * G) {
-    const int row = base + lane / L;
-    const bool valid = row < c1;
+    const int ia = base + lane / L;
+    const bool valid = ia < c1;
+    int row = 0, i = 0;
+    if (valid) {
+      const int j = ar.piece(ia);
+      row = ar.row(ia, j);
+      i = ar.local(ia, j);
+    }
     double n[3];
-    view_rows_spmv_group<MT, L>(mv, row, valid, x, lane, n);
+    view_rows_spmv_group<MT, L>(mv, i, row, valid, x, lane, n);
     if (valid && (lane & (L - 1)) == 0) {
-      sn[row - c0][0] = n[0];
-      sn[row - c0][1] = n[1];
-      sn[row - c0][2] = n[2];
+      sn[ia - c0][0] = n[0];
+      sn[ia - c0][1] = n[1];
+      sn[ia - c0][2] = n[2];
     }
   }
+}
+
+// Warp 0 only: lay the rows of the pieces whose flag is clear end to end
+// (prefix sum over at most 64 pieces, two per lane).  The caller orders the
+// flag writes before this call and this call before any read of alst with
+// __syncthreads.
+static_assert(kMaxCtaPieces <= 64, "active_scan covers two pieces per lane");
+__device__ __forceinline__ void active_scan(int npc, int lane, const int* flag, const int* lst, int* alst) {
+  const int j0 = 2 * lane, j1 = 2 * lane + 1;
+  const int c0 = (j0 < npc && !flag[j0]) ? lst[j0 + 1] - lst[j0] : 0;
+  const int c1 = (j1 < npc && !flag[j1]) ? lst[j1 + 1] - lst[j1] : 0;
+  int incl = c0 + c1;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += t;
+  }
+  const int excl = incl - c0 - c1;
+  if (j0 < npc) alst[j0] = excl;
+  if (j1 < npc) alst[j1] = excl + c0;
+  if (lane == 31) alst[npc] = incl;
 }
 
 // dynamic shared memory layout of the PCG kernel
@@ -381,7 +446,10 @@ __host__ __device__ inline void pcg_smem_layout(int nloc_max, int nb_max, int re
   *total = o;
 }
 
-template <typename MT>
+// RES: compiled for shared-memory resident row state (the contiguous split
+// of packs that fit); otherwise residency is the runtime flag (zero in the
+// strided split), which keeps the register pressure of each form low.
+template <typename MT, bool RES>
 __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   __shared__ double rowbuf[kRowChunk][3];
   __shared__ double sn[kRowChunk][3];
@@ -390,20 +458,55 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   __shared__ double s_bb[kMaxCtaPieces], s_tol[kMaxCtaPieces], s_alpha[kMaxCtaPieces],
       s_beta[kMaxCtaPieces], s_gold[kMaxCtaPieces], s_aold[kMaxCtaPieces];
   __shared__ int s_conv[kMaxCtaPieces], s_iters[kMaxCtaPieces], s_first[kMaxCtaPieces];
+  // the model's solve is final (its true residual was checked and it was
+  // not restarted): later passes leave its rows alone
+  __shared__ int s_done[kMaxCtaPieces];
+  __shared__ int s_gp[kMaxCtaPieces], s_lst[kMaxCtaPieces + 1], s_grow[kMaxCtaPieces];
+  // row space of the pieces still iterating (see active_scan)
+  __shared__ int s_alst[kMaxCtaPieces + 1];
   __shared__ int s_restart;
   extern __shared__ __align__(16) unsigned char dyn[];
-  CtaView cv{a.cta_piece[blockIdx.x], a.cta_piece[blockIdx.x + 1]};
-  const int npc = cv.pc1 - cv.pc0;
-  const int r0 = a.piece_row[cv.pc0], r1 = a.piece_row[cv.pc1];
+  const bool res = RES || a.resident;
+  const int pc0 = a.cta_piece[blockIdx.x];
+  const int npc = a.cta_piece[blockIdx.x + 1] - pc0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ph = 0;
 
+  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+    const int g = a.cta_plist[pc0 + j];
+    s_gp[j] = g;
+    s_grow[j] = a.piece_row[g];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int j = 0; j < npc; j++) {
+      s_lst[j] = acc;
+      acc += a.piece_row[s_gp[j] + 1] - s_grow[j];
+    }
+    s_lst[npc] = acc;
+  }
+  __syncthreads();
+  const CtaRows cr{s_gp, s_lst, s_lst, s_grow, npc, s_lst[npc]};  // all local rows
+  const int nloc = cr.nloc;
+  // the rows of the pieces whose flag is clear, after rescan(flag)
+  auto active_view = [&]() { return CtaRows{s_gp, s_alst, s_lst, s_grow, npc, s_alst[npc]}; };
+  auto rescan = [&](const int* flag) {
+    __syncthreads();  // the flag writes of every thread come first
+    if (warp == 0) active_scan(npc, lane, flag, s_lst, s_alst);
+    __syncthreads();
+  };
+  // the last piece of a model owns the model's flags and outputs
+  auto owner = [&](int j) {
+    const int g = s_gp[j];
+    return g == a.model_piece[a.piece_model[g] + 1] - 1;
+  };
+
   size_t off_vec, off_ro, off_col, off_S, total;
-  pcg_smem_layout<MT>(a.nloc_max, a.nb_max, a.resident, a.cached, &off_vec, &off_ro, &off_col, &off_S, &total);
+  pcg_smem_layout<MT>(a.nloc_max, a.nb_max, res, a.cached, &off_vec, &off_ro, &off_col, &off_S, &total);
   RowState st;
-  st.r0 = r0;
-  st.res = a.resident;
-  if (a.resident) {
+  st.res = res;
+  if (res) {
     double* base = (double*)(dyn + off_vec);
     for (int k = 0; k < 9; k++) st.v[k] = base + (size_t)k * a.nloc_max * 3;
     st.D = base + (size_t)9 * a.nloc_max * 3;
@@ -417,18 +520,20 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   mv.rowptr = a.rowptr;
   mv.col = a.col;
   mv.S = (const MT*)a.S;
-  mv.r0 = r0;
   mv.cached = a.cached;
   mv.ro_s = (const int*)(dyn + off_ro);
   mv.col_s = (const int*)(dyn + off_col);
   mv.S_s = (const MT*)(dyn + off_S);
+  // residency and caching are planned only for the contiguous split, where
+  // local row i is global row r0 + i
+  const int r0 = npc > 0 ? s_grow[0] : 0;
   const int pbase = a.rowptr[r0];
   if (a.cached) {
-    const int nb = a.rowptr[r1] - pbase;
+    const int nb = a.rowptr[r0 + nloc] - pbase;
     int* ro = (int*)(dyn + off_ro);
     int* cs = (int*)(dyn + off_col);
     MT* Ss = (MT*)(dyn + off_S);
-    for (int i = threadIdx.x; i <= r1 - r0; i += blockDim.x) ro[i] = a.rowptr[r0 + i] - pbase;
+    for (int i = threadIdx.x; i <= nloc; i += blockDim.x) ro[i] = a.rowptr[r0 + i] - pbase;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) cs[i] = a.col[pbase + i];
     const MT* Sg = (const MT*)a.S + (size_t)pbase * 9;
     for (int i = threadIdx.x; i < nb * 9; i += blockDim.x) Ss[i] = Sg[i];
@@ -439,43 +544,44 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
 
   // ---- P0: block-Jacobi inverse, r = b - S x0, u = Dinv r (published to
   // m1 for the next SpMV), ||b||^2
-  cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
+  cta_row_pass<1, true>(a, cr, ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
     double Ax[3];
-    view_row_spmv<MT>(mv, row, a.x, ln, Ax);
+    view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
     if (ln == 0) {
       const MT* Db = (const MT*)a.S + (size_t)a.blk_diag[row] * 9;
       if (a.cached) Db = mv.S_s + (size_t)(a.blk_diag[row] - pbase) * 9;
       double d[9], inv[9];
 #pragma unroll
-      for (int i = 0; i < 9; i++) d[i] = (double)Db[i];
+      for (int k = 0; k < 9; k++) d[k] = (double)Db[k];
       if (invert3(inv, d) == 0.0) {
         atomicExch(a.flags, B200FEM_ERR_INVALID_ARG);
 #pragma unroll
-        for (int i = 0; i < 9; i++) inv[i] = 0;
+        for (int k = 0; k < 9; k++) inv[k] = 0;
       }
-      double* D = st.dinv(row);
+      double* D = st.dinv(i, row);
 #pragma unroll
-      for (int i = 0; i < 9; i++) D[i] = inv[i];
+      for (int k = 0; k < 9; k++) D[k] = inv[k];
       double bv[3], r[3], u[3], x0[3];
       load3(bv, a.b, row);
       load3(x0, a.x, row);
 #pragma unroll
       for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
       mul33(u, inv, r);
-      store3(st.at(VR, row), 0, r);
-      store3(st.at(VU, row), 0, u);
-      if (a.resident) store3(st.at(VX, row), 0, x0);
+      store3(st.at(VR, i, row), 0, r);
+      store3(st.at(VU, i, row), 0, u);
+      if (res) store3(st.at(VX, i, row), 0, x0);
       store3(a.m1, row, u);
       vals[0] = dot3(bv, bv);
     }
   });
   if (!grid_barrier(a.barrier, a.flags)) return;
-  model_sums<1>(a, cv, ph & 1, sums);
+  model_sums<1>(a, cr, ph & 1, sums, nullptr);
   for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-    const int m = a.piece_model[cv.pc0 + j];
+    const int m = a.piece_model[s_gp[j]];
     s_bb[j] = sums[j][0];
     s_tol[j] = a.step[(size_t)m * 8 + 6];
     s_conv[j] = 0;
+    s_done[j] = 0;
     s_iters[j] = 0;
   }
   ph++;
@@ -487,18 +593,19 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       // ---- classic PCG (two grid barriers per iteration), from the state
       // P0 or the true-residual pass left: r, z = Dinv r (resident) and z
       // published in m1.  rho = r.z, ||r||^2 first.
-      cta_row_pass<2, false>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
-        if (s_conv[piece_of_row(a, cv, row)]) return;
+      rescan(s_conv);
+      cta_row_pass<2, false>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int, double* vals) {
+        if (s_conv[j]) return;
         double r[3], z[3], zero[3] = {0, 0, 0};
-        load3(r, st.at(VR, row), 0);
-        load3(z, st.at(VU, row), 0);
-        store3(st.at(VP, row), 0, zero);
-        store3(st.at(VQ, row), 0, zero);
+        load3(r, st.at(VR, i, row), 0);
+        load3(z, st.at(VU, i, row), 0);
+        store3(st.at(VP, i, row), 0, zero);
+        store3(st.at(VQ, i, row), 0, zero);
         vals[0] = dot3(r, z);
         vals[1] = dot3(r, r);
       });
       if (!grid_barrier(a.barrier, a.flags)) return;
-      model_sums<2>(a, cv, ph & 1, sums);
+      model_sums<2>(a, cr, ph & 1, sums, s_conv);
       ph++;
       for (int j = threadIdx.x; j < npc; j += blockDim.x) {
         if (s_conv[j]) continue;
@@ -506,7 +613,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]) || sums[j][1] == 0.0) s_conv[j] = 1;
         s_first[j] = 1;
       }
-      __syncthreads();
+      rescan(s_conv);
       for (int it = 0;; it++) {
         const int idx = total_it + it;
         // phase A: p = z + beta p; q = S z + beta q (z complete); p.q
@@ -514,24 +621,22 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           if (s_conv[j]) continue;
           s_beta[j] = s_first[j] ? 0.0 : s_gold[j] / s_aold[j];
           s_first[j] = 0;
-          const int m = a.piece_model[cv.pc0 + j];
-          if (cv.pc0 + j == a.model_piece[m + 1] - 1) a.unconv[idx] = 1;
+          if (owner(j)) a.unconv[idx] = 1;
         }
         __syncthreads();
-        if (idx >= a.max_iter) {
+        if (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap)) {
           total_it += it;
           break;
         }
-        cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
-          const int j = piece_of_row(a, cv, row);
+        cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int ln, double* vals) {
           if (s_conv[j]) return;
           double Az[3];
-          view_row_spmv<MT>(mv, row, a.m1, ln, Az);
+          view_row_spmv<MT>(mv, i, row, a.m1, ln, Az);
           if (ln == 0) {
             const double be = s_beta[j];
-            double* pz = st.at(VU, row);
-            double* pp = st.at(VP, row);
-            double* pq = st.at(VQ, row);
+            double* pz = st.at(VU, i, row);
+            double* pp = st.at(VP, i, row);
+            double* pq = st.at(VQ, i, row);
             double pqv = 0;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -547,21 +652,20 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           total_it += it;
           break;
         }
-        model_sums<1>(a, cv, ph & 1, sums);
+        model_sums<1>(a, cr, ph & 1, sums, s_conv);
         ph++;
         for (int j = threadIdx.x; j < npc; j += blockDim.x)
           s_alpha[j] = s_conv[j] ? 0.0 : s_gold[j] / sums[j][0];
         __syncthreads();
         // phase B: x += alpha p; r -= alpha q; z = Dinv r (published); r.z, r.r
-        cta_row_pass<2, false>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
-          const int j = piece_of_row(a, cv, row);
+        cta_row_pass<2, false>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int, double* vals) {
           if (s_conv[j]) return;
           const double al = s_alpha[j];
-          double* px = st.at(VX, row);
-          double* pr = st.at(VR, row);
-          double* pz = st.at(VU, row);
-          const double* pp = st.at(VP, row);
-          const double* pq = st.at(VQ, row);
+          double* px = st.at(VX, i, row);
+          double* pr = st.at(VR, i, row);
+          double* pz = st.at(VU, i, row);
+          const double* pp = st.at(VP, i, row);
+          const double* pq = st.at(VQ, i, row);
           double r[3], z[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) {
@@ -569,14 +673,14 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             r[c] = pr[c] - al * pq[c];
             pr[c] = r[c];
           }
-          mul33(z, st.dinv(row), r);
+          mul33(z, st.dinv(i, row), r);
           store3(pz, 0, z);
           store3(a.m1, row, z);
           vals[0] = dot3(r, z);
           vals[1] = dot3(r, r);
         });
         if (!grid_barrier(a.barrier, a.flags)) return;
-        model_sums<2>(a, cv, ph & 1, sums);
+        model_sums<2>(a, cr, ph & 1, sums, s_conv);
         ph++;
         for (int j = threadIdx.x; j < npc; j += blockDim.x) {
           if (s_conv[j]) continue;
@@ -585,27 +689,28 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           s_iters[j]++;
           if (sqrt(sums[j][1]) <= s_tol[j] * sqrt(s_bb[j]) || sums[j][1] == 0.0) s_conv[j] = 1;
         }
-        __syncthreads();
+        rescan(s_conv);
       }
     } else {
     // ---- P1: w = S u, m = Dinv w (published to m0); dots r.u, w.u, r.r
     for (int j = threadIdx.x; j < npc; j += blockDim.x) s_first[j] = 1;
-    cta_row_pass<3, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
-      if (s_conv[piece_of_row(a, cv, row)]) return;
+    rescan(s_conv);
+    cta_row_pass<3, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int ln, double* vals) {
+      if (s_conv[j]) return;
       double Au[3];
-      view_row_spmv<MT>(mv, row, a.m1, ln, Au);
+      view_row_spmv<MT>(mv, i, row, a.m1, ln, Au);
       if (ln == 0) {
         double r[3], u[3], m[3], zero[3] = {0, 0, 0};
-        load3(r, st.at(VR, row), 0);
-        load3(u, st.at(VU, row), 0);
-        mul33(m, st.dinv(row), Au);
-        store3(st.at(VW, row), 0, Au);
+        load3(r, st.at(VR, i, row), 0);
+        load3(u, st.at(VU, i, row), 0);
+        mul33(m, st.dinv(i, row), Au);
+        store3(st.at(VW, i, row), 0, Au);
         store3(a.m0, row, m);
-        if (a.resident) store3(st.at(VM, row), 0, m);
-        store3(st.at(VZ, row), 0, zero);
-        store3(st.at(VQ, row), 0, zero);
-        store3(st.at(VS, row), 0, zero);
-        store3(st.at(VP, row), 0, zero);
+        if (res) store3(st.at(VM, i, row), 0, m);
+        store3(st.at(VZ, i, row), 0, zero);
+        store3(st.at(VQ, i, row), 0, zero);
+        store3(st.at(VS, i, row), 0, zero);
+        store3(st.at(VP, i, row), 0, zero);
         vals[0] = dot3(r, u);
         vals[1] = dot3(Au, u);
         vals[2] = dot3(r, r);
@@ -620,23 +725,28 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       double* mn = mbuf ? a.m0 : a.m1;
       // The SpMV n = S m does not depend on this iteration's scalars, so it
       // runs on the first warps while the last warps reduce the scalars.
+      // Both work on the rows of the models unconverged when the iteration
+      // began (the view laid out at the end of the previous iteration).
       const int nsumw = min(max(npc, 1), 8);
       const int nroww = (blockDim.x >> 5) - nsumw;
       for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
       bool stop = false;
-      for (int c0 = r0, first = 1; c0 < r1 || first; c0 += kRowChunk, first = 0) {
-        const int c1 = min(c0 + kRowChunk, r1);
+      const CtaRows ar = active_view();
+      const int nact = ar.nloc;
+      for (int c0 = 0, first = 1; c0 < nact || first; c0 += kRowChunk, first = 0) {
+        const int c1 = min(c0 + kRowChunk, nact);
         if (warp < nroww) {
-          if (a.row_lanes == 8) spmv_rows_to_smem<MT, 8>(mv, mc, c0, c1, warp, nroww, lane, sn);
-          else if (a.row_lanes == 16) spmv_rows_to_smem<MT, 16>(mv, mc, c0, c1, warp, nroww, lane, sn);
-          else spmv_rows_to_smem<MT, 32>(mv, mc, c0, c1, warp, nroww, lane, sn);
+          if (a.row_lanes == 8) spmv_rows_to_smem<MT, 8>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+          else if (a.row_lanes == 16) spmv_rows_to_smem<MT, 16>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+          else spmv_rows_to_smem<MT, 32>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
         } else if (first) {
           // reduce this iteration's scalars and form alpha, beta; the
           // convergence test is on the recurrence residual
           const int sw = warp - nroww;
           const double* src = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
           for (int j = sw; j < npc; j += nsumw) {
-            const int m = a.piece_model[cv.pc0 + j];
+            if (s_conv[j]) continue;
+            const int m = a.piece_model[s_gp[j]];
             const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
             double sm[3] = {0, 0, 0};
             for (int qq = q0 + lane; qq < q1; qq += 32)
@@ -646,7 +756,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             for (int k = 0; k < 3; k++)
 #pragma unroll
               for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
-            if (lane == 0 && !s_conv[j]) {
+            if (lane == 0) {
               const double gam = sm[0], del = sm[1], rho = sm[2];
               if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
                 s_conv[j] = 1;
@@ -664,38 +774,40 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
                 s_gold[j] = gam;
                 s_aold[j] = alpha;
                 s_iters[j]++;
-                if (cv.pc0 + j == a.model_piece[m + 1] - 1) a.unconv[idx] = 1;
+                if (owner(j)) a.unconv[idx] = 1;
               }
             }
           }
         }
         __syncthreads();
-        if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kPipelinedCap))) {
+        if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap))) {
           stop = true;
           break;
         }
         // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
         // x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
-        for (int row = c0 + (int)threadIdx.x; row < c1; row += blockDim.x) {
-          const int j = piece_of_row(a, cv, row);
+        for (int ia = c0 + (int)threadIdx.x; ia < c1; ia += blockDim.x) {
+          const int j = ar.piece(ia);
           double v3[3] = {0, 0, 0};
           if (!s_conv[j]) {
+            const int i = ar.local(ia, j);
+            const int row = ar.row(ia, j);
             const double al = s_alpha[j], be = s_beta[j];
-            double* px = st.at(VX, row);
-            double* pr = st.at(VR, row);
-            double* pu = st.at(VU, row);
-            double* pw = st.at(VW, row);
-            double* pz = st.at(VZ, row);
-            double* pq = st.at(VQ, row);
-            double* ps = st.at(VS, row);
-            double* pp = st.at(VP, row);
-            const double* D = st.dinv(row);
+            double* px = st.at(VX, i, row);
+            double* pr = st.at(VR, i, row);
+            double* pu = st.at(VU, i, row);
+            double* pw = st.at(VW, i, row);
+            double* pz = st.at(VZ, i, row);
+            double* pq = st.at(VQ, i, row);
+            double* ps = st.at(VS, i, row);
+            double* pp = st.at(VP, i, row);
+            const double* D = st.dinv(i, row);
             double mm[3], w[3], r[3], u[3];
-            if (a.resident) load3(mm, st.at(VM, row), 0);
+            if (res) load3(mm, st.at(VM, i, row), 0);
             else load3(mm, mc, row);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-              const double z = sn[row - c0][c] + be * pz[c];
+              const double z = sn[ia - c0][c] + be * pz[c];
               const double q = mm[c] + be * pq[c];
               const double sv = pw[c] + be * ps[c];
               const double p = pu[c] + be * pp[c];
@@ -714,14 +826,14 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             double mnew[3];
             mul33(mnew, D, w);
             store3(mn, row, mnew);
-            if (a.resident) store3(st.at(VM, row), 0, mnew);
+            if (res) store3(st.at(VM, i, row), 0, mnew);
             v3[0] = dot3(r, u);
             v3[1] = dot3(w, u);
             v3[2] = dot3(r, r);
           }
-          rowbuf[row - c0][0] = v3[0];
-          rowbuf[row - c0][1] = v3[1];
-          rowbuf[row - c0][2] = v3[2];
+          rowbuf[ia - c0][0] = v3[0];
+          rowbuf[ia - c0][1] = v3[1];
+          rowbuf[ia - c0][2] = v3[2];
         }
         __syncthreads();
         if (npc == 1 && c1 - c0 <= 32) {
@@ -742,12 +854,12 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           continue;
         }
         for (int j = warp; j < npc; j += (blockDim.x >> 5)) {
-          const int pr0 = max(a.piece_row[cv.pc0 + j], c0), pr1 = min(a.piece_row[cv.pc0 + j + 1], c1);
-          if (pr0 >= pr1) continue;
+          const int pr0 = max(s_alst[j], c0), pr1 = min(s_alst[j + 1], c1);
+          if (pr0 >= pr1 || s_conv[j]) continue;
           double sm[3] = {0, 0, 0};
-          for (int row = pr0 + lane; row < pr1; row += 32)
+          for (int i = pr0 + lane; i < pr1; i += 32)
 #pragma unroll
-            for (int k = 0; k < 3; k++) sm[k] += rowbuf[row - c0][k];
+            for (int k = 0; k < 3; k++) sm[k] += rowbuf[i - c0][k];
 #pragma unroll
           for (int k = 0; k < 3; k++)
 #pragma unroll
@@ -767,8 +879,10 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         double* out = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
         for (int j = threadIdx.x; j < npc; j += blockDim.x)
 #pragma unroll
-          for (int k = 0; k < 3; k++) out[(size_t)(cv.pc0 + j) * 4 + k] = pacc[j][k];
+          for (int k = 0; k < 3; k++) out[(size_t)s_gp[j] * 4 + k] = pacc[j][k];
       }
+      // the next iteration works on the models still unconverged
+      rescan(s_conv);
       if (!grid_barrier(a.barrier, a.flags)) return;
       mbuf ^= 1;
       if (__ldcg(&a.unconv[idx]) == 0) {
@@ -779,50 +893,57 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     ph++;
     }  // pipelined
 
-    // ---- publish x, then the true residual r = b - S x; restart from it
-    // when it misses the tolerance although the recurrence converged
-    if (a.resident)
-      for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) store3(a.x, row, st.at(VX, row));
+    // ---- publish x, then the true residual r = b - S x of the models not
+    // yet final; restart from it when it misses the tolerance
+    if (res)
+      for (int i = threadIdx.x; i < nloc; i += blockDim.x) store3(a.x, r0 + i, st.at(VX, i, r0 + i));
+    rescan(s_done);
     if (!grid_barrier(a.barrier, a.flags)) return;
-    cta_row_pass<1, true>(a, cv, ph & 1, rowbuf, pacc, [&](int row, int ln, double* vals) {
+    cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
       double Ax[3];
-      view_row_spmv<MT>(mv, row, a.x, ln, Ax);
+      view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
       if (ln == 0) {
         double bv[3], r[3];
         load3(bv, a.b, row);
 #pragma unroll
         for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
         vals[0] = dot3(r, r);
-        // restart state for every row (used only by restarted models)
+        // restart state (used only if the model restarts)
         double u[3];
-        mul33(u, st.dinv(row), r);
-        store3(st.at(VR, row), 0, r);
-        store3(st.at(VU, row), 0, u);
+        mul33(u, st.dinv(i, row), r);
+        store3(st.at(VR, i, row), 0, r);
+        store3(st.at(VU, i, row), 0, u);
         store3(a.m1, row, u);
       }
     });
     if (!grid_barrier(a.barrier, a.flags)) return;
-    model_sums<1>(a, cv, ph & 1, sums);
+    model_sums<1>(a, cr, ph & 1, sums, s_done);
     ph++;
     if (threadIdx.x == 0) s_restart = 0;
     __syncthreads();
     for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+      if (s_done[j]) continue;
       const double rel = s_bb[j] > 0 ? sqrt(sums[j][0] / s_bb[j]) : sqrt(sums[j][0]);
       const bool ok = rel <= s_tol[j] || sums[j][0] == 0.0;
-      // residual replacement when the recurrence converged but the true
-      // residual did not; in auto mode also when the pipelined phase hit its
-      // cap unconverged (classic PCG continues from the true residual)
-      const bool stalled = !s_conv[j] && !classic && a.variant == 0;
-      if (((s_conv[j] && !ok) || stalled) && restart < kMaxRestarts && total_it < a.max_iter) {
+      // the true residual decides: a model whose true residual meets the
+      // tolerance is done.  Otherwise residual replacement when the
+      // recurrence converged; in auto mode also when the round hit its cap
+      // unconverged (classic PCG continues from the true residual)
+      const bool capped = !s_conv[j] && a.variant == 0;
+      const bool again = !ok && (s_conv[j] || capped) && restart < kMaxRestarts && total_it < a.max_iter;
+      if (again) {
         s_conv[j] = 0;
         s_restart = 1;
       }
-      const int m = a.piece_model[cv.pc0 + j];
-      if (cv.pc0 + j == a.model_piece[m + 1] - 1) {
-        double* o = a.model_out + (size_t)m * 4;
+      if (owner(j)) {
+        double* o = a.model_out + (size_t)a.piece_model[s_gp[j]] * 4;
         o[0] = s_iters[j];
         o[1] = rel;
-        o[2] = (s_conv[j] && ok) ? 1.0 : 0.0;
+        o[2] = ok ? 1.0 : 0.0;
+      }
+      if (!again) {
+        s_done[j] = 1;
+        s_conv[j] = 1;  // no further iterations for this model
       }
     }
     __syncthreads();
@@ -830,13 +951,14 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
     if (!grid_barrier(a.barrier, a.flags)) return;
     if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
-    // the pipelined recurrences drifted from the true residual: continue
-    // with classic PCG, whose attainable accuracy is better
+    // continue with classic PCG, whose attainable accuracy is better than
+    // that of the pipelined recurrences
     if (a.variant == 0) classic = true;
   }
 
   if (a.update_state) {
-    for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+    for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
+      const int row = cr.row(i, cr.piece(i));
       const int n = a.act_node[row];
       const double h = a.step[(size_t)a.row_model[row] * 8];
 #pragma unroll
@@ -879,6 +1001,7 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.piece_model = d.piece_model;
   a.model_piece = d.model_piece;
   a.cta_piece = d.cta_piece;
+  a.cta_plist = d.cta_plist;
   a.partials = d.partials;
   a.step = d.step;
   a.model_out = d.model_scal;
@@ -915,9 +1038,11 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   cfg.numAttrs = 1;
   if (eng.precision == B200FEM_PREC_MIXED) {
     a.S = d.S_f;
-    return cudaLaunchKernelEx(&cfg, pcg_kernel<float>, a);
+    return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<float, true>, a)
+                      : cudaLaunchKernelEx(&cfg, pcg_kernel<float, false>, a);
   }
-  return cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
+  return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true>, a)
+                    : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false>, a);
 }
 
 int pcg_threads() { return kPcgThreads; }
@@ -933,8 +1058,12 @@ static cudaError_t ensure_pcg_smem(int device, size_t bytes, bool fp32 = false) 
   const int d = (device >= 0 && device < 64) ? device : 0;
   int& cur = g_pcg_attr_bytes[fp32 ? 1 : 0][d];
   if ((int)bytes <= cur) return cudaSuccess;
-  cudaError_t e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)
-                       : cudaFuncSetAttribute(pcg_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, false>, at, (int)bytes)
+                       : cudaFuncSetAttribute(pcg_kernel<double, false>, at, (int)bytes);
+  if (e == cudaSuccess)
+    e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, true>, at, (int)bytes)
+             : cudaFuncSetAttribute(pcg_kernel<double, true>, at, (int)bytes);
   if (e == cudaSuccess) cur = (int)bytes;
   return e;
 }
@@ -960,8 +1089,15 @@ void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cac
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   cudaFuncAttributes fa;
-  if (fp32) cudaFuncGetAttributes(&fa, pcg_kernel<float>);
-  else cudaFuncGetAttributes(&fa, pcg_kernel<double>);
+  cudaFuncAttributes fb;
+  if (fp32) {
+    cudaFuncGetAttributes(&fa, pcg_kernel<float, false>);
+    cudaFuncGetAttributes(&fb, pcg_kernel<float, true>);
+  } else {
+    cudaFuncGetAttributes(&fa, pcg_kernel<double, false>);
+    cudaFuncGetAttributes(&fb, pcg_kernel<double, true>);
+  }
+  fa.sharedSizeBytes = std::max(fa.sharedSizeBytes, fb.sharedSizeBytes);
   const long long budget = (long long)optin - (long long)fa.sharedSizeBytes - 1024;
   size_t ov, oro, oc, oS, total;
   *resident = 0;
@@ -980,7 +1116,7 @@ int pcg_max_cta_pieces() { return kMaxCtaPieces; }
 int pcg_max_grid(int device) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<double>, kPcgThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<double, false>, kPcgThreads, 0);
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
@@ -1148,6 +1284,9 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.piece_model = (const int*)(base + LY::piece_model);
   a.model_piece = (const int*)(base + LY::model_piece);
   a.cta_piece = (const int*)(base + LY::cta_piece);
+  // one piece per CTA, numbered like the CTAs: the identity table cta_piece
+  // doubles as the piece list
+  a.cta_plist = a.cta_piece;
   a.partials = (double*)(base + LY::partials);
   a.step = (const double*)(base + LY::step);
   a.model_out = (double*)(base + LY::model_out);
@@ -1176,7 +1315,8 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, pcg_kernel<double>, a);
+  e = resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true>, a)
+               : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false>, a);
   if (e != cudaSuccess) {
     *err = cudaGetErrorString(e);
     return B200FEM_ERR_CUDA;

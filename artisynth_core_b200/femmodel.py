@@ -396,10 +396,11 @@ class FemPack:
     engine (one pack).  Every kernel launch covers all models; each model
     keeps its own material, PCG scalars and convergence test."""
 
-    def __init__(self, models, precision=L.PREC_MIXED, device=0):
+    def __init__(self, models, precision=L.PREC_MIXED, device=0, options=None):
         self.models = list(models)
         self.precision = precision
         self.device = device
+        self.options = dict(options or {})  # B200FEM_OPT_* key -> value, applied before the build
         self._engine = None
         self.offsets = None
         self.stats = L.Stats()
@@ -417,6 +418,8 @@ class FemPack:
                 eng.call("b200fem_add_model", m.elem_type, m.numNodes(), L.dptr(rest), m.numElements(),
                          L.iptr(conn), L.iptr(m.fixed), m.material.kind, L.dptr(prm), m.density, m.soft_incomp,
                          ctypes.byref(idx))
+            for k, v in self.options.items():
+                eng.call("b200fem_set_option", int(k), int(v))
             eng.call("b200fem_build")
             self._engine = eng
             self.offsets = []
@@ -434,6 +437,18 @@ class FemPack:
         if self._engine is not None:
             self._engine.close()
             self._engine = None
+
+    def option(self, key) -> int:
+        """The value of a B200FEM_OPT_* option in force (resolved after the build)."""
+        v = ctypes.c_int()
+        self.engine().call("b200fem_get_option", int(key), ctypes.byref(v))
+        return v.value
+
+    def setOption(self, key, value):
+        """Options that may change after the build (ROW_LANES)."""
+        if self._engine is not None:
+            self._engine.call("b200fem_set_option", int(key), int(value))
+        self.options[key] = value
 
     def total_nodes(self):
         return sum(m.numNodes() for m in self.models)

@@ -192,6 +192,23 @@ int b200fem_model_range(b200fem_handle h, int model, int* node_offset, int* n_no
 /* per-model PCG iterations and true relative residuals of the last solve */
 int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_residual);
 
+/* ---- tuning options ------------------------------------------------------
+   No counterpart in the reference (its solves are a direct PARDISO/cuDSS
+   factorisation or an unpreconditioned CGSolver).  They choose how the
+   persistent PCG kernel lays the pack's rows over the GPU; results agree
+   across settings to rounding (each setting is bit-reproducible by itself).
+   SPLIT, CTAS and PIECE_ROWS take effect at b200fem_build; ROW_LANES also
+   afterwards (the step graph is re-captured). */
+#define B200FEM_OPT_PCG_SPLIT 1  /* 0 auto; 1 contiguous rows per CTA (shared-memory
+                                    resident when they fit); 2 strided: every model cut
+                                    into short pieces dealt over all CTAs */
+#define B200FEM_OPT_ROW_LANES 2  /* lanes per block row in the iteration SpMV: 0 auto, 8, 16, 32 */
+#define B200FEM_OPT_PCG_CTAS 3   /* CTAs of the persistent PCG kernel: 0 auto (one per SM) */
+#define B200FEM_OPT_PIECE_ROWS 4 /* block rows per piece in the strided split: 0 auto (64) */
+int b200fem_set_option(b200fem_handle h, int key, int value);
+/* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
+int b200fem_get_option(b200fem_handle h, int key, int* value);
+
 /* ---- allocation-free solve ---------------------------------------------- */
 /* Size limits of b200fem_pcg_solve_noalloc: its scratch is one fixed device
    array (about 2.6 MB) sized for these limits. */

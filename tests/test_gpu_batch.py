@@ -79,3 +79,82 @@ def test_pack_of_mixed_materials(b200, oracle):
         for _ in range(3):
             om.be_step(w.h, x, v, alpha=w.mass_damping, gravity=w.gravity, solver=1)
         assert rel_err(xg, x) <= 1e-8
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("variant", [L.PCG_AUTO, L.PCG_CLASSIC])
+def test_strided_split_equals_alone(beams, precision, variant):
+    """The strided split (models cut into short pieces dealt over the CTAs,
+    iterations compacted to the models still iterating) gives each model the
+    result it gets alone."""
+    steps = 4
+    opts = {L.OPT_PCG_SPLIT: L.SPLIT_STRIDED, L.OPT_PIECE_ROWS: 8, L.OPT_PCG_CTAS: 7}
+    pack = FemPack([b.model() for b in beams], precision=precision, options=opts)
+    assert pack.option(L.OPT_PCG_SPLIT) == L.SPLIT_STRIDED
+    assert pack.option(L.OPT_PCG_CTAS) == 7
+    pack.backwardEuler(beams[0].h, steps, tol=1e-12, pcg_variant=variant)
+    it, rr = pack.modelStats()
+    assert np.all(rr <= 1e-12)
+    assert len(set(it.tolist())) > 1  # models converge at different iterations
+    for b, (xg, _) in zip(beams, pack.getStates()):
+        m = b.model(precision=precision)
+        MechSystemSolver(m, tol=1e-12).backwardEuler(b.h, steps)
+        xa, _ = m.getState()
+        assert rel_err(xg, xa) <= 1e-9, (b.name, rel_err(xg, xa))
+
+
+def test_strided_many_pieces_per_cta(b200):
+    """More than one warp's worth of pieces on each CTA (the per-CTA piece
+    tables span two warps), on a pack whose models converge at different
+    iterations: every model matches its solve alone."""
+    bs = W.batched_beams(count=24, seed=9)
+    for b in bs:
+        b.cells = (min(b.cells[0], 10), b.cells[1], b.cells[2])
+        b.widths = (b.cells[0] * 0.05, b.widths[1], b.widths[2])
+        b.build_mesh()
+    steps = 3
+    # 40-row pieces over 6 CTAs: about 45 pieces per CTA (270 in all)
+    opts = {L.OPT_PCG_SPLIT: L.SPLIT_STRIDED, L.OPT_PIECE_ROWS: 40, L.OPT_PCG_CTAS: 6}
+    for precision in (L.PREC_FP64, L.PREC_MIXED):
+        pack = FemPack([b.model() for b in bs], precision=precision, options=opts)
+        pack.backwardEuler(bs[0].h, steps, tol=1e-12)
+        _, rr = pack.modelStats()
+        assert np.all(rr <= 1e-12)
+        for b, (xg, _) in zip(bs, pack.getStates()):
+            m = b.model(precision=precision)
+            MechSystemSolver(m, tol=1e-12).backwardEuler(b.h, steps)
+            xa, _ = m.getState()
+            assert rel_err(xg, xa) <= 1e-9, (b.name, precision, rel_err(xg, xa))
+        pack.close()
+
+
+def test_layout_options_agree(beams):
+    """Contiguous and strided splits, CTA counts and SpMV row widths change
+    only the rounding of the dot products."""
+    steps = 3
+    ref = None
+    for opts in ({}, {L.OPT_PCG_SPLIT: L.SPLIT_CONTIGUOUS, L.OPT_PCG_CTAS: 3},
+                 {L.OPT_PCG_SPLIT: L.SPLIT_STRIDED, L.OPT_ROW_LANES: 8},
+                 {L.OPT_PCG_SPLIT: L.SPLIT_STRIDED, L.OPT_ROW_LANES: 32, L.OPT_PIECE_ROWS: 5}):
+        pack = FemPack([b.model() for b in beams], precision=L.PREC_FP64, options=opts)
+        pack.backwardEuler(beams[0].h, steps, tol=1e-12)
+        x = np.concatenate([xg for xg, _ in pack.getStates()])
+        if L.OPT_ROW_LANES in opts:
+            assert pack.option(L.OPT_ROW_LANES) == opts[L.OPT_ROW_LANES]
+        pack.close()
+        if ref is None:
+            ref = x
+        else:
+            assert rel_err(x, ref) <= 1e-9, opts
+
+
+def test_row_lanes_change_after_build(beams):
+    pack = FemPack([b.model() for b in beams], precision=L.PREC_FP64)
+    pack.backwardEuler(beams[0].h, 2, tol=1e-12)
+    for lanes in (8, 32):
+        pack.setOption(L.OPT_ROW_LANES, lanes)
+        assert pack.option(L.OPT_ROW_LANES) == lanes
+    with pytest.raises(L.B200FemError):
+        pack.setOption(L.OPT_PCG_SPLIT, L.SPLIT_STRIDED)  # layout options precede the build
+    pack.backwardEuler(beams[0].h, 1, tol=1e-12)
+    assert np.all(np.isfinite(np.concatenate([xg for xg, _ in pack.getStates()])))
