@@ -130,6 +130,8 @@ def lib():
         "b200fem_model_range": ([H, ctypes.c_int, _ip, _ip, _ip], ctypes.c_int),
         "b200fem_get_model_stats": ([H, _ip, _dp], ctypes.c_int),
         "b200fem_set_option": ([H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "b200fem_set_active_models": ([H, _ip], ctypes.c_int),
+        "b200fem_memory_usage": ([H, ctypes.POINTER(ctypes.c_ulonglong)], ctypes.c_int),
         "b200fem_get_option": ([H, ctypes.c_int, _ip], ctypes.c_int),
         "b200fem_pcg_solve_noalloc": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
                                        _ip, _dp], ctypes.c_int),

@@ -54,7 +54,10 @@ cudaError_t dalloc(Engine& eng, T** ptr, size_t count) {
   *ptr = nullptr;
   if (count == 0) count = 1;
   cudaError_t e = cudaMalloc((void**)ptr, count * sizeof(T));
-  if (e == cudaSuccess) eng.allocations.push_back((void*)*ptr);
+  if (e == cudaSuccess) {
+    eng.allocations.push_back((void*)*ptr);
+    eng.device_bytes += count * sizeof(T);
+  }
   return e;
 }
 
@@ -78,6 +81,7 @@ void free_pack(Engine& eng) {
   eng.last_step_params.clear();
   for (void* p : eng.allocations) cudaFree(p);
   eng.allocations.clear();
+  eng.device_bytes = 0;
   eng.d = DevPack();
   eng.built = false;
   eng.have_matrix = false;
@@ -518,6 +522,8 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.model_piece, model_piece));
   CK(upload(eng, &d.cta_piece, cta_piece));
   CK(upload(eng, &d.cta_plist, cta_plist));
+  CK(upload(eng, &d.model_active, std::vector<int>(M, 1)));
+  eng.any_inactive = false;
   d.unconv_cap = 200000;
   CK(dalloc(eng, &d.unconv, (size_t)d.unconv_cap + 2));
   {
@@ -763,6 +769,33 @@ int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_resid
 int b200fem_build(b200fem_handle h) {
   ENG(h);
   return build_pack(eng);
+}
+
+int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes) {
+  ENG(h);
+  if (!bytes) return fail(&eng, B200FEM_ERR_INVALID_ARG, "null bytes");
+  *bytes = eng.device_bytes;
+  return B200FEM_OK;
+}
+
+int b200fem_set_active_models(b200fem_handle h, const int* active) {
+  ENG(h);
+  NEED_BUILT();
+  const int M = eng.d.n_models;
+  std::vector<int> a(M, 1);
+  bool any_off = false;
+  if (active)
+    for (int m = 0; m < M; m++) {
+      a[m] = active[m] != 0;
+      any_off |= a[m] == 0;
+    }
+  CK(cudaMemcpyAsync(eng.d.model_active, a.data(), sizeof(int) * M, cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  if (any_off != eng.any_inactive) {
+    eng.any_inactive = any_off;
+    eng.step_exec_max_iter = -1;  // recapture: the mask pointer is a kernel argument
+  }
+  return B200FEM_OK;
 }
 
 int b200fem_set_option(b200fem_handle h, int key, int value) {

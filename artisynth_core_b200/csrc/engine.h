@@ -132,6 +132,7 @@ struct DevPack {
   int* model_piece = nullptr;  // n_models+1
   int* cta_piece = nullptr;    // pcg_grid+1
   int* cta_plist = nullptr;    // n_pieces: global piece indices, CTA-major
+  int* model_active = nullptr; // n_models: 0 = left out of assembly and steps
   int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
   int unconv_cap = 0;
   int n_pieces = 0;
@@ -178,6 +179,7 @@ struct Engine {
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_strided = 0;  // pieces dealt to CTAs across models (large packs)
+  bool any_inactive = false;  // some model_active entry is 0 (kernels get the mask)
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
   int pcg_attr_smem = -1;
@@ -193,6 +195,7 @@ struct Engine {
   std::vector<double> last_step_params;
   b200fem_stats last_stats{};
   std::vector<void*> allocations;
+  size_t device_bytes = 0;  // sum of the allocations above
 };
 
 // setup.cpp

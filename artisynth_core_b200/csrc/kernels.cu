@@ -111,6 +111,9 @@ __device__ __forceinline__ long long dbl_order(double v) {
   return i >= 0 ? i : (i ^ 0x7fffffffffffffffll);
 }
 
+struct ElemArgs;
+__device__ bool block_inactive(const ElemArgs& a, int ebase, int epb);
+
 struct ElemArgs {
   int e0, e1;
   const int* conn;
@@ -124,11 +127,25 @@ struct ElemArgs {
   const int* sidx;
   const double* mat;       // per model kMatParams
   const double* node_p;    // NODAL pressures (or null)
+  const int* active;       // per model: 0 = left out of this assembly (or null: all)
   void* elemK;             // T* E*npair*9
   void* elemF;             // T* E*nen*3
   int* flags;              // [err, inverted]
   long long* mindet;       // ordered bits
 };
+
+// Whole-block exit when none of the block's elements belongs to an active
+// model (elements of a group are in model order, so blocks rarely mix).
+// Called before any shared-memory use; the block returns as a whole.
+__device__ bool block_inactive(const ElemArgs& a, int ebase, int epb) {
+  if (!a.active) return false;
+  bool mine = false;
+  for (int t = threadIdx.x; t < epb; t += blockDim.x) {
+    const int e = ebase + t;
+    mine |= e < a.e1 && a.active[a.elem_model[e]] != 0;
+  }
+  return !__syncthreads_or(mine);
+}
 
 // ---------------------------------------------------------------------------
 // non-linear materials (NeoHookean, MooneyRivlin), tet or hex
@@ -162,6 +179,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
   T(*sD)[DS] = reinterpret_cast<T(*)[DS]>(sdv + NREC + NREC * 6);
   int(*snode)[NEN] = reinterpret_cast<int(*)[NEN]>(sdv + NREC + NREC * 6 + NREC * DS);
   const int ebase = a.e0 + blockIdx.x * EPB;
+  if (block_inactive(a, ebase, EPB)) return;
   // stage 0: coalesced connectivity + coordinate loads.  In FP32 the
   // coordinates are taken relative to the element's first node in FP64 so
   // the Jacobian keeps full single precision.
@@ -300,6 +318,7 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
   __shared__ double sR[EPB][9];
   __shared__ int snode[EPB][NEN];
   const int ebase = a.e0 + blockIdx.x * EPB;
+  if (block_inactive(a, ebase, EPB)) return;
   for (int t = threadIdx.x; t < EPB * NEN; t += blockDim.x) {
     int el = t / NEN, n = t % NEN, e = ebase + el;
     if (e < a.e1) snode[el][n] = a.conn[(size_t)e * NEN + n];
@@ -415,10 +434,12 @@ __global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, cons
                               const int* __restrict__ act_node, const double* __restrict__ mass,
                               const double* __restrict__ step, int mode, TO* __restrict__ out,
                               const int* __restrict__ dptr, const int* __restrict__ didx,
-                              const double* __restrict__ divblk, const double* __restrict__ node_kp) {
+                              const double* __restrict__ divblk, const double* __restrict__ node_kp,
+                              const int* __restrict__ active) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nnzb * 9) return;
   long long p = t / 9;
+  if (active && !active[row_model[blk_row[p]]]) return;  // model left out of this step
   int q = (int)(t - p * 9);
   int qt = (q % 3) * 3 + q / 3;
   double s = 0;
@@ -476,9 +497,10 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
                             const int* __restrict__ node_model, const double* __restrict__ mass,
                             const double* __restrict__ v, const double* __restrict__ fext,
                             const double* __restrict__ step, double* __restrict__ fint,
-                            double* __restrict__ b, double* __restrict__ sol0) {
+                            double* __restrict__ b, double* __restrict__ sol0, const int* __restrict__ active) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
+  if (active && !active[node_model[n]]) return;  // model left out of this step
   double f[3] = {0, 0, 0};
   const int i0 = inc_ptr[n], i1 = inc_ptr[n + 1];
   // four incidences per round: their index and force loads are independent
@@ -557,6 +579,7 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.e1 = g.e1;
   a.conn = d.conn;
   a.elem_model = d.elem_model;
+  a.active = eng.any_inactive ? d.model_active : nullptr;
   a.x = d.x;
   a.invJ0 = d.invJ0;
   a.invJ0_f = d.invJ0_f;
@@ -788,21 +811,22 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
     if (e != cudaSuccess) return e;
   }
   long long n9 = d.nnzb * 9;
+  const int* act = eng.any_inactive ? d.model_active : nullptr;
   int threads = 256;
   unsigned blocks = (unsigned)((n9 + threads - 1) / threads);
   if (fp32) {
     if (want_K)
       gather_kernel<float, double><<<blocks, threads, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-          d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+          d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
     else
       gather_kernel<float, float><<<blocks, threads, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-          d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+          d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
   } else {
     gather_kernel<double, double><<<blocks, threads, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp);
+        d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
   }
   return cudaGetLastError();
 }
@@ -823,12 +847,13 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   DevPack& d = eng.d;
   const int threads = 64;
   const int blocks = (d.n_nodes + threads - 1) / threads;
+  const int* act = eng.any_inactive ? d.model_active : nullptr;
   if (eng.precision == B200FEM_PREC_MIXED)
     rows_kernel<float><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF_f, d.sidx,
-                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol);
+                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act);
   else
     rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
-                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol);
+                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act);
   return cudaGetLastError();
 }
 

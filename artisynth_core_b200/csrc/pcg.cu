@@ -124,6 +124,7 @@ struct PcgArgs {
   double* vel;
   const int* act_node;
   const int* row_model;
+  const int* model_active;  // per model: 0 = not solved in this call (or null: all)
 };
 
 // The rows a CTA owns: its local pieces j = 0..npc-1 (global piece gp[j],
@@ -540,11 +541,27 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   }
   if (blockIdx.x == 0)
     for (int i = threadIdx.x; i <= a.max_iter + 1; i += blockDim.x) a.unconv[i] = 0;
-  __syncthreads();
+  // models left out of this call are final from the start
+  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
+    const int m = a.piece_model[s_gp[j]];
+    const int off = a.model_active && !a.model_active[m];
+    s_tol[j] = a.step[(size_t)m * 8 + 6];
+    s_conv[j] = off;
+    s_done[j] = off;
+    s_iters[j] = 0;
+    s_bb[j] = 0;
+    if (off && owner(j)) {
+      double* o = a.model_out + (size_t)m * 4;
+      o[0] = 0;
+      o[1] = 0;
+      o[2] = 1.0;
+    }
+  }
+  rescan(s_done);
 
   // ---- P0: block-Jacobi inverse, r = b - S x0, u = Dinv r (published to
   // m1 for the next SpMV), ||b||^2
-  cta_row_pass<1, true>(a, cr, ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
+  cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
     double Ax[3];
     view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
     if (ln == 0) {
@@ -575,15 +592,9 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     }
   });
   if (!grid_barrier(a.barrier, a.flags)) return;
-  model_sums<1>(a, cr, ph & 1, sums, nullptr);
-  for (int j = threadIdx.x; j < npc; j += blockDim.x) {
-    const int m = a.piece_model[s_gp[j]];
-    s_bb[j] = sums[j][0];
-    s_tol[j] = a.step[(size_t)m * 8 + 6];
-    s_conv[j] = 0;
-    s_done[j] = 0;
-    s_iters[j] = 0;
-  }
+  model_sums<1>(a, cr, ph & 1, sums, s_done);
+  for (int j = threadIdx.x; j < npc; j += blockDim.x)
+    if (!s_done[j]) s_bb[j] = sums[j][0];
   ph++;
 
   int total_it = 0;
@@ -959,6 +970,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   if (a.update_state) {
     for (int i = threadIdx.x; i < nloc; i += blockDim.x) {
       const int row = cr.row(i, cr.piece(i));
+      if (a.model_active && !a.model_active[a.row_model[row]]) continue;
       const int n = a.act_node[row];
       const double h = a.step[(size_t)a.row_model[row] * 8];
 #pragma unroll
@@ -1016,6 +1028,7 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.vel = d.v;
   a.act_node = d.act_node;
   a.row_model = d.row_model;
+  a.model_active = eng.any_inactive ? d.model_active : nullptr;
   a.resident = eng.pcg_resident;
   a.cached = eng.pcg_cached;
   a.nloc_max = eng.pcg_nloc_max;
@@ -1305,6 +1318,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.vel = nullptr;
   a.act_node = nullptr;
   a.row_model = nullptr;
+  a.model_active = nullptr;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);
   cfg.blockDim = dim3(kPcgThreads);

@@ -438,6 +438,21 @@ class FemPack:
             self._engine.close()
             self._engine = None
 
+    def deviceBytes(self) -> int:
+        """Device memory held by the pack."""
+        v = ctypes.c_ulonglong()
+        self.engine().call("b200fem_memory_usage", ctypes.byref(v))
+        return v.value
+
+    def setActive(self, active=None):
+        """Mask of the models the next steps advance (None: all)."""
+        if active is None:
+            self.engine().call("b200fem_set_active_models", None)
+        else:
+            a = np.ascontiguousarray(np.asarray(active, dtype=np.int32))
+            assert a.shape == (len(self.models),)
+            self.engine().call("b200fem_set_active_models", L.iptr(a))
+
     def option(self, key) -> int:
         """The value of a B200FEM_OPT_* option in force (resolved after the build)."""
         v = ctypes.c_int()

@@ -191,6 +191,16 @@ int b200fem_num_models(b200fem_handle h, int* n_models);
 int b200fem_model_range(b200fem_handle h, int model, int* node_offset, int* n_nodes, int* n_active);
 /* per-model PCG iterations and true relative residuals of the last solve */
 int b200fem_get_model_stats(b200fem_handle h, int* iterations, double* rel_residual);
+/* Which models the following calls work on (continuous batching: one pack
+   step advances only the models that have work).  active[m] == 0 leaves
+   model m out of assembly, RHS, PCG and the state update: its positions and
+   velocities stay as they are and its stats read 0 iterations.  NULL makes
+   every model active again (the default after b200fem_build).  No
+   counterpart in the reference, which steps one model per MechModel. */
+int b200fem_set_active_models(b200fem_handle h, const int* active);
+/* device memory the handle's pack holds (bytes), for admission against a
+   device-memory budget */
+int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 
 /* ---- tuning options ------------------------------------------------------
    No counterpart in the reference (its solves are a direct PARDISO/cuDSS
