@@ -459,6 +459,8 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.x, x));
   CK(dalloc(eng, &d.v, 3 * (size_t)N));
   CK(cudaMemset(d.v, 0, 3 * sizeof(double) * (size_t)N));
+  CK(dalloc(eng, &d.vprev, 3 * (size_t)N));
+  CK(cudaMemset(d.vprev, 0, 3 * sizeof(double) * (size_t)N));
   CK(dalloc(eng, &d.fext, 3 * (size_t)N));
   CK(cudaMemset(d.fext, 0, 3 * sizeof(double) * (size_t)N));
   CK(upload(eng, &d.mass, mass));
@@ -816,6 +818,13 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PIECE_ROWS is set before b200fem_build");
       eng.opt_piece_rows = value;
       return B200FEM_OK;
+    case B200FEM_OPT_WARM_START:
+      if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "WARM_START must be 0 or 1");
+      if (value != eng.opt_warm_start) {
+        eng.opt_warm_start = value;
+        eng.step_exec_max_iter = -1;  // recapture: the RHS kernel's arguments change
+      }
+      return B200FEM_OK;
     case B200FEM_OPT_ROW_LANES:
       if (value != 0 && value != 8 && value != 16 && value != 32)
         return fail(&eng, B200FEM_ERR_INVALID_ARG, "ROW_LANES must be 0, 8, 16 or 32");
@@ -838,6 +847,7 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_ROW_LANES: *value = eng.built ? eng.pcg_row_lanes : eng.opt_row_lanes; break;
     case B200FEM_OPT_PCG_CTAS: *value = eng.built ? eng.pcg_grid : eng.opt_ctas; break;
     case B200FEM_OPT_PIECE_ROWS: *value = eng.opt_piece_rows; break;
+    case B200FEM_OPT_WARM_START: *value = eng.opt_warm_start; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
   return B200FEM_OK;
@@ -948,6 +958,9 @@ int b200fem_set_state(b200fem_handle h, const double* x, const double* v) {
   size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
   if (x) CK(cudaMemcpyAsync(eng.d.x, x, n, cudaMemcpyHostToDevice, eng.stream));
   if (v) CK(cudaMemcpyAsync(eng.d.v, v, n, cudaMemcpyHostToDevice, eng.stream));
+  // a state set from outside has no history: extrapolation starts at zero
+  // acceleration
+  if (v) CK(cudaMemcpyAsync(eng.d.vprev, v, n, cudaMemcpyHostToDevice, eng.stream));
   CK(cudaStreamSynchronize(eng.stream));
   return B200FEM_OK;
 }

@@ -133,6 +133,7 @@ struct DevPack {
   int* cta_piece = nullptr;    // pcg_grid+1
   int* cta_plist = nullptr;    // n_pieces: global piece indices, CTA-major
   int* model_active = nullptr; // n_models: 0 = left out of assembly and steps
+  double* vprev = nullptr;     // 3N: velocity before the last step (warm-start extrapolation)
   int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
   int unconv_cap = 0;
   int n_pieces = 0;
@@ -182,6 +183,7 @@ struct Engine {
   bool any_inactive = false;  // some model_active entry is 0 (kernels get the mask)
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
+  int opt_warm_start = 1;  // 0 previous velocity, 1 extrapolated from the last two
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)

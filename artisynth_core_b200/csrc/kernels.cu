@@ -497,7 +497,8 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
                             const int* __restrict__ node_model, const double* __restrict__ mass,
                             const double* __restrict__ v, const double* __restrict__ fext,
                             const double* __restrict__ step, double* __restrict__ fint,
-                            double* __restrict__ b, double* __restrict__ sol0, const int* __restrict__ active) {
+                            double* __restrict__ b, double* __restrict__ sol0, const int* __restrict__ active,
+                            const double* __restrict__ vprev) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   if (active && !active[node_model[n]]) return;  // model left out of this step
@@ -530,10 +531,14 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
 #pragma unroll
     for (int c = 0; c < 3; c++)
       b[3 * (size_t)r + c] = m * v[3 * (size_t)n + c] + h * (m * sp[3 + c] + fext[3 * (size_t)n + c] - f[c]);
-    // the PCG starts from the current velocity
+    // the PCG starts from the current velocity, or from its extrapolation
+    // v + (v - v_prev) over the last two steps
     if (sol0)
 #pragma unroll
-      for (int c = 0; c < 3; c++) sol0[3 * (size_t)r + c] = v[3 * (size_t)n + c];
+      for (int c = 0; c < 3; c++) {
+        const double vc = v[3 * (size_t)n + c];
+        sol0[3 * (size_t)r + c] = vprev ? 2.0 * vc - vprev[3 * (size_t)n + c] : vc;
+      }
   }
 }
 
@@ -848,12 +853,13 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   const int threads = 64;
   const int blocks = (d.n_nodes + threads - 1) / threads;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
+  const double* vp = eng.opt_warm_start == 1 ? d.vprev : nullptr;
   if (eng.precision == B200FEM_PREC_MIXED)
     rows_kernel<float><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF_f, d.sidx,
-                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act);
+                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
   else
     rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
-                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act);
+                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
   return cudaGetLastError();
 }
 

@@ -121,6 +121,7 @@ struct PcgArgs {
   int row_lanes;  // lanes per block row in the iteration SpMV (8, 16, 32)
   int update_state;
   double* xpos;
+  double* vprev;  // receives the velocity before the update
   double* vel;
   const int* act_node;
   const int* row_model;
@@ -976,6 +977,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vn = a.x[3 * (size_t)row + c];
+        a.vprev[3 * (size_t)n + c] = a.vel[3 * (size_t)n + c];
         a.vel[3 * (size_t)n + c] = vn;
         a.xpos[3 * (size_t)n + c] += h * vn;
       }
@@ -1026,6 +1028,7 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.update_state = update_state ? 1 : 0;
   a.xpos = d.x;
   a.vel = d.v;
+  a.vprev = d.vprev;
   a.act_node = d.act_node;
   a.row_model = d.row_model;
   a.model_active = eng.any_inactive ? d.model_active : nullptr;
@@ -1314,6 +1317,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.variant = 0;
   a.row_lanes = 16;
   a.update_state = 0;
+  a.vprev = nullptr;
   a.xpos = nullptr;
   a.vel = nullptr;
   a.act_node = nullptr;

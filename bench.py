@@ -9,6 +9,15 @@ state update) on device-resident state.  The model's working set (~30 MB)
 fits in L2, so a 256 MB buffer is written between timed steps to flush L2.
 Multi-GPU runs are independent replicas (one model per rank, weak scaling):
 the path has no cross-model exchange.
+
+On one GPU the line also carries the two other forms of the path:
+  "batched" -- 256 uneven NeoHookean tet beams in one pack (mixed FP32/FP64,
+               20 steps), model-steps/s next to the plain FP64 drop-in
+               stepping the models one at a time, and the position error
+               against that FP64 run;
+  "served"  -- a Poisson stream of 10-step requests (2000/s, 60 s) over a
+               pool of 512 beams with continuous batching and a 60 GB
+               device-memory budget: p50/p99 latency, throughput, error.
 """
 from __future__ import annotations
 
@@ -183,6 +192,124 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
+def _fp64_alone(w, steps, tol, dev):
+    """Positions of a model after `steps` steps of the plain FP64 drop-in."""
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200.femmodel import MechSystemSolver
+    m = w.model(precision=L.PREC_FP64, device=dev)
+    MechSystemSolver(m, tol=tol, max_iter=20000).backwardEuler(w.h, steps)
+    x, _ = m.getState()
+    m._invalidate()
+    return x
+
+
+def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
+    """Batched uneven models: 256 NeoHookean tet beams in one pack (mixed
+    FP32/FP64), `steps` BackwardEuler steps; next to the plain FP64 drop-in
+    stepping the models one at a time (every `sample_every`-th model)."""
+    import torch
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.femmodel import FemPack, MechSystemSolver
+    bs = W.batched_beams()
+    for b in bs:
+        b.build_mesh()
+    pack = FemPack([b.model(device=dev) for b in bs], precision=L.PREC_MIXED, device=dev)
+    t0 = time.perf_counter()
+    pack.engine()
+    build_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    asm = pcg = 0.0
+    its = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pack.backwardEuler(bs[0].h, 1, tol=tol)
+        a, p = pack.lastTiming()
+        asm += a
+        pcg += p
+        its.append(pack.stats.iterations)
+    wall = time.perf_counter() - t0
+    it_m, _ = pack.modelStats()
+    xs = [x for x, _ in pack.getStates()]
+    split = pack.option(L.OPT_PCG_SPLIT)
+    nbytes = pack.deviceBytes()
+    pack.close()
+    # plain FP64 drop-in, one model at a time, on a sample
+    sample = list(range(0, len(bs), sample_every))
+    t_single = 0.0
+    err = 0.0
+    for i in sample:
+        b = bs[i]
+        m = b.model(precision=L.PREC_FP64, device=dev)
+        ms = MechSystemSolver(m, tol=1e-10, max_iter=20000)
+        m.engine()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ms.backwardEuler(b.h, steps)
+        t_single += time.perf_counter() - t1
+        x, _ = m.getState()
+        m._invalidate()
+        err = max(err, _rel(xs[i], x))
+    single = len(sample) * steps / t_single
+    n = len(bs)
+    return {
+        "workload": "256 uneven NeoHookean tet beams (n 4-60, m 2-8, seed 3), 20 steps h=0.01",
+        "models": n, "tets": int(sum(b.conn.shape[0] for b in bs)), "steps": steps, "tol": tol,
+        "precision": "mixed FP32 element/SpMV, FP64 vectors", "pcg_split": "strided" if split == 2 else "contiguous",
+        "device_bytes": nbytes, "build_s": build_s,
+        "model_steps_per_s": n * steps / wall, "device_ms_per_step": (asm + pcg) / steps,
+        "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
+        "element_updates_per_s": sum(b.conn.shape[0] for b in bs) * steps / wall,
+        "pcg_iterations": {"max_per_step_mean": float(np.mean(its)), "model_median": float(np.median(it_m)),
+                           "model_p90": float(np.percentile(it_m, 90))},
+        "plain_fp64_single_model_steps_per_s": single,
+        "speedup_vs_plain_fp64": n * steps / wall / single,
+        "plain_fp64_sample": f"{len(sample)} of {n} models (every {sample_every}th), {steps} steps each",
+        "max_rel_position_error_vs_fp64": err,
+    }
+
+
+def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=10, tol=1e-10,
+               drain_s=30.0, err_sample=16):
+    """Served stream: Poisson arrivals (seed 4) of 10-step requests on models
+    of the config-4 distribution with 10% large (n 80-120) beams, 60 GB
+    device-memory budget, continuous batching."""
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.serve import FemServer, poisson_arrivals, run_stream
+    pool = W.batched_beams(count=pool_size, seed=4, large_frac=0.1)
+    for w in pool:
+        w.build_mesh()
+    srv = FemServer(pool, budget=60e9, tol=tol, device=dev)
+    t0 = time.perf_counter()
+    srv.preload()
+    preload_s = time.perf_counter() - t0
+    arrivals = poisson_arrivals(rate, seconds, pool_size, seed=4)
+    out = run_stream(srv, arrivals, steps_per_request, drain_s=drain_s)
+    # accuracy: served models against the plain FP64 drop-in for the same steps
+    steps_of = {}
+    for r in srv.done:
+        steps_of[r.model] = steps_of.get(r.model, 0) + r.steps
+    incomplete_models = {m for m, q in srv.queues.items() if q}
+    checked = [m for m in sorted(steps_of) if m not in incomplete_models and m not in srv.waiting][:err_sample]
+    err = 0.0
+    for m in checked:
+        x, _ = srv.state(m)
+        err = max(err, _rel(x, _fp64_alone(pool[m], steps_of[m], 1e-10, dev)))
+    srv.close()
+    out.update({
+        "workload": f"Poisson {rate:.0f} req/s (seed 4) for {seconds:.0f} s, {steps_per_request} steps/request, "
+                    f"pool of {pool_size} beams (config-4 distribution, 10% n 80-120)",
+        "pool_tets": int(sum(w.conn.shape[0] for w in pool)), "tol": tol, "budget_bytes": 60e9,
+        "preload_s": preload_s, "offered_model_steps_per_s": rate * steps_per_request,
+        "max_rel_position_error_vs_fp64": err, "error_sample_models": len(checked),
+    })
+    return out
+
+
 def run_b200(args):
     import torch
     dist, rank, world, local = dist_setup(args.gpus)
@@ -259,6 +386,15 @@ def run_b200(args):
                 traffic = json.load(open(prof)).get("pcg_kernel" if pcg_ms >= asm_ms else "assembly")
             except Exception:
                 traffic = None
+        batched = served = None
+        if world == 1 and not args.no_batched:
+            with ClockSampler(dev) as c:
+                batched = run_batched(dev, tol=args.batch_tol)
+            batched["clocks"] = c.summary()
+        if world == 1 and args.served_seconds > 0:
+            with ClockSampler(dev) as c:
+                served = run_served(dev, seconds=args.served_seconds, tol=args.batch_tol)
+            served["clocks"] = c.summary()
         cpu = None
         if not args.no_cpu and world == 1:
             rate, n, dt, used = cpu_oracle_rate(wl, args.cpu_budget, os.cpu_count() or 1)
@@ -282,6 +418,8 @@ def run_b200(args):
                          "assembly_gbs": asm_gbs, "pcg_gbs": pcg_gbs},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line), flush=True)
     m._invalidate()
@@ -297,6 +435,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-pack leg")
+    ap.add_argument("--served-seconds", type=float, default=60.0, help="length of the served stream (0: skip)")
+    ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched and served legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -207,14 +207,17 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
    factorisation or an unpreconditioned CGSolver).  They choose how the
    persistent PCG kernel lays the pack's rows over the GPU; results agree
    across settings to rounding (each setting is bit-reproducible by itself).
-   SPLIT, CTAS and PIECE_ROWS take effect at b200fem_build; ROW_LANES also
-   afterwards (the step graph is re-captured). */
+   SPLIT, CTAS and PIECE_ROWS take effect at b200fem_build; ROW_LANES and
+   WARM_START also afterwards (the step graph is re-captured). */
 #define B200FEM_OPT_PCG_SPLIT 1  /* 0 auto; 1 contiguous rows per CTA (shared-memory
                                     resident when they fit); 2 strided: every model cut
                                     into short pieces dealt over all CTAs */
 #define B200FEM_OPT_ROW_LANES 2  /* lanes per block row in the iteration SpMV: 0 auto, 8, 16, 32 */
 #define B200FEM_OPT_PCG_CTAS 3   /* CTAs of the persistent PCG kernel: 0 auto (one per SM) */
 #define B200FEM_OPT_PIECE_ROWS 4 /* block rows per piece in the strided split: 0 auto (64) */
+#define B200FEM_OPT_WARM_START 5 /* PCG start: 0 the previous velocity; 1 (default) its linear
+                                    extrapolation 2 v_n - v_(n-1) over the last two steps
+                                    (may be changed after the build) */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
