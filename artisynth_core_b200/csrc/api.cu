@@ -452,7 +452,9 @@ int build_pack(Engine& eng) {
     eng.pcg_row_lanes = eng.opt_row_lanes;
   } else {
     const double bpr = R > 0 ? (double)NB / R : 1.0;
-    eng.pcg_row_lanes = bpr <= 10 ? 8 : (bpr <= 20 ? 16 : 32);
+    // short rows do best with many rows in flight per warp: tets (~15
+    // blocks per row) -> 4, hexes (~27) -> 16, NODAL 2-ring rows -> 32
+    eng.pcg_row_lanes = bpr <= 18 ? 4 : (bpr <= 40 ? 16 : 32);
   }
 
   // ---- device upload
@@ -826,8 +828,8 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       }
       return B200FEM_OK;
     case B200FEM_OPT_ROW_LANES:
-      if (value != 0 && value != 8 && value != 16 && value != 32)
-        return fail(&eng, B200FEM_ERR_INVALID_ARG, "ROW_LANES must be 0, 8, 16 or 32");
+      if (value != 0 && value != 4 && value != 8 && value != 16 && value != 32)
+        return fail(&eng, B200FEM_ERR_INVALID_ARG, "ROW_LANES must be 0, 4, 8, 16 or 32");
       eng.opt_row_lanes = value;
       if (eng.built && value != 0 && value != eng.pcg_row_lanes) {
         eng.pcg_row_lanes = value;

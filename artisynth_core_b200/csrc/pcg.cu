@@ -118,7 +118,7 @@ struct PcgArgs {
   int* unconv;  // per iteration: some model still unconverged
   int max_iter;
   int variant;  // 0 auto (pipelined, classic after a residual replacement), 1 classic, 2 pipelined
-  int row_lanes;  // lanes per block row in the iteration SpMV (8, 16, 32)
+  int row_lanes;  // lanes per block row in the iteration SpMV (4, 8, 16, 32)
   int update_state;
   double* xpos;
   double* vprev;  // receives the velocity before the update
@@ -406,6 +406,92 @@ __device__ __forceinline__ void spmv_rows_to_smem(const MatView<MT>& mv, const C
       sn[ia - c0][0] = n[0];
       sn[ia - c0][1] = n[1];
       sn[ia - c0][2] = n[2];
+    }
+  }
+}
+
+// One pipelined-CG row update fused with the SpMV that feeds it, for the
+// rows [c0, c1) of the view: a group of L lanes forms n = S m for its row;
+// lanes 0..2 of the group then update the row's vector components
+//   z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
+//   x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
+// (one component each, w shared by shuffles for m'), and the group's dot
+// products r.u, w.u, r.r go to rowbuf[row - c0] (zero for converged rows).
+template <typename MT, int L>
+__device__ __forceinline__ void fused_rows(const PcgArgs& a, const MatView<MT>& mv, const CtaRows& ar,
+                                           const RowState& st, bool res, const double* mc, double* mn, int c0,
+                                           int c1, int warp, int nw, int lane, const int* conv,
+                                           const double* alpha, const double* beta, double (*rowbuf)[3]) {
+  static_assert(L >= 4, "three lanes per row update the vector components");
+  constexpr int G = 32 / L;
+  const int gl = lane & (L - 1);
+  const int g0 = lane & ~(L - 1);
+  for (int base = c0 + warp * G; base < c1; base += nw * G) {
+    const int ia = base + lane / L;
+    const bool valid = ia < c1;
+    int row = 0, i = 0, j = 0;
+    if (valid) {
+      j = ar.piece(ia);
+      row = ar.row(ia, j);
+      i = ar.local(ia, j);
+    }
+    double n[3];
+    view_rows_spmv_group<MT, L>(mv, i, row, valid, mc, lane, n);
+    const bool upd = valid && !conv[j] && gl < 3;
+    double wc = 0, ru = 0, wu = 0, rr = 0;
+    if (upd) {
+      const int c = gl;
+      const double al = alpha[j], be = beta[j];
+      double* px = st.at(VX, i, row) + c;
+      double* pr = st.at(VR, i, row) + c;
+      double* pu = st.at(VU, i, row) + c;
+      double* pw = st.at(VW, i, row) + c;
+      double* pz = st.at(VZ, i, row) + c;
+      double* pq = st.at(VQ, i, row) + c;
+      double* ps = st.at(VS, i, row) + c;
+      double* pp = st.at(VP, i, row) + c;
+      const double mm = res ? st.at(VM, i, row)[c] : mc[3 * (size_t)row + c];
+      const double nc = c == 0 ? n[0] : (c == 1 ? n[1] : n[2]);
+      const double z = nc + be * *pz;
+      const double q = mm + be * *pq;
+      const double sv = *pw + be * *ps;
+      const double p = *pu + be * *pp;
+      *px += al * p;
+      const double r = *pr - al * sv;
+      const double u = *pu - al * q;
+      const double w = *pw - al * z;
+      *pz = z;
+      *pq = q;
+      *ps = sv;
+      *pp = p;
+      *pr = r;
+      *pu = u;
+      *pw = w;
+      wc = w;
+      ru = r * u;
+      wu = w * u;
+      rr = r * r;
+    }
+    const double w0 = __shfl_sync(0xffffffffu, wc, g0);
+    const double w1 = __shfl_sync(0xffffffffu, wc, g0 + 1);
+    const double w2 = __shfl_sync(0xffffffffu, wc, g0 + 2);
+    if (upd) {
+      const int c = gl;
+      const double* D = st.dinv(i, row) + 3 * c;
+      const double mnew = D[0] * w0 + D[1] * w1 + D[2] * w2;
+      mn[3 * (size_t)row + c] = mnew;
+      if (res) st.at(VM, i, row)[c] = mnew;
+    }
+#pragma unroll
+    for (int off = 2; off > 0; off >>= 1) {
+      ru += __shfl_xor_sync(0xffffffffu, ru, off);
+      wu += __shfl_xor_sync(0xffffffffu, wu, off);
+      rr += __shfl_xor_sync(0xffffffffu, rr, off);
+    }
+    if (valid && gl == 0) {
+      rowbuf[ia - c0][0] = ru;
+      rowbuf[ia - c0][1] = wu;
+      rowbuf[ia - c0][2] = rr;
     }
   }
 }
@@ -747,105 +833,115 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       const int nact = ar.nloc;
       for (int c0 = 0, first = 1; c0 < nact || first; c0 += kRowChunk, first = 0) {
         const int c1 = min(c0 + kRowChunk, nact);
-        if (warp < nroww) {
-          if (a.row_lanes == 8) spmv_rows_to_smem<MT, 8>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
-          else if (a.row_lanes == 16) spmv_rows_to_smem<MT, 16>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
-          else spmv_rows_to_smem<MT, 32>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
-        } else if (first) {
-          // reduce this iteration's scalars and form alpha, beta; the
-          // convergence test is on the recurrence residual
-          const int sw = warp - nroww;
-          const double* src = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
-          for (int j = sw; j < npc; j += nsumw) {
-            if (s_conv[j]) continue;
-            const int m = a.piece_model[s_gp[j]];
-            const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
-            double sm[3] = {0, 0, 0};
-            for (int qq = q0 + lane; qq < q1; qq += 32)
+        if (first) {
+          if (warp < nroww) {
+            if (a.row_lanes == 4) spmv_rows_to_smem<MT, 4>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+            else if (a.row_lanes == 8) spmv_rows_to_smem<MT, 8>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+            else if (a.row_lanes == 16) spmv_rows_to_smem<MT, 16>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+            else spmv_rows_to_smem<MT, 32>(mv, ar, mc, c0, c1, warp, nroww, lane, sn);
+          } else if (first) {
+            // reduce this iteration's scalars and form alpha, beta; the
+            // convergence test is on the recurrence residual
+            const int sw = warp - nroww;
+            const double* src = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
+            for (int j = sw; j < npc; j += nsumw) {
+              if (s_conv[j]) continue;
+              const int m = a.piece_model[s_gp[j]];
+              const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
+              double sm[3] = {0, 0, 0};
+              for (int qq = q0 + lane; qq < q1; qq += 32)
 #pragma unroll
-              for (int k = 0; k < 3; k++) sm[k] += __ldcg(&src[(size_t)qq * 4 + k]);
+                for (int k = 0; k < 3; k++) sm[k] += __ldcg(&src[(size_t)qq * 4 + k]);
 #pragma unroll
-            for (int k = 0; k < 3; k++)
+              for (int k = 0; k < 3; k++)
 #pragma unroll
-              for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
-            if (lane == 0) {
-              const double gam = sm[0], del = sm[1], rho = sm[2];
-              if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
-                s_conv[j] = 1;
-              } else {
-                double beta = 0, alpha;
-                if (s_first[j]) {
-                  alpha = gam / del;
-                  s_first[j] = 0;
+                for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+              if (lane == 0) {
+                const double gam = sm[0], del = sm[1], rho = sm[2];
+                if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
+                  s_conv[j] = 1;
                 } else {
-                  beta = gam / s_gold[j];
-                  alpha = gam / (del - beta * gam / s_aold[j]);
+                  double beta = 0, alpha;
+                  if (s_first[j]) {
+                    alpha = gam / del;
+                    s_first[j] = 0;
+                  } else {
+                    beta = gam / s_gold[j];
+                    alpha = gam / (del - beta * gam / s_aold[j]);
+                  }
+                  s_beta[j] = beta;
+                  s_alpha[j] = alpha;
+                  s_gold[j] = gam;
+                  s_aold[j] = alpha;
+                  s_iters[j]++;
+                  if (owner(j)) a.unconv[idx] = 1;
                 }
-                s_beta[j] = beta;
-                s_alpha[j] = alpha;
-                s_gold[j] = gam;
-                s_aold[j] = alpha;
-                s_iters[j]++;
-                if (owner(j)) a.unconv[idx] = 1;
               }
             }
           }
-        }
-        __syncthreads();
-        if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap))) {
-          stop = true;
-          break;
-        }
-        // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
-        // x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
-        for (int ia = c0 + (int)threadIdx.x; ia < c1; ia += blockDim.x) {
-          const int j = ar.piece(ia);
-          double v3[3] = {0, 0, 0};
-          if (!s_conv[j]) {
-            const int i = ar.local(ia, j);
-            const int row = ar.row(ia, j);
-            const double al = s_alpha[j], be = s_beta[j];
-            double* px = st.at(VX, i, row);
-            double* pr = st.at(VR, i, row);
-            double* pu = st.at(VU, i, row);
-            double* pw = st.at(VW, i, row);
-            double* pz = st.at(VZ, i, row);
-            double* pq = st.at(VQ, i, row);
-            double* ps = st.at(VS, i, row);
-            double* pp = st.at(VP, i, row);
-            const double* D = st.dinv(i, row);
-            double mm[3], w[3], r[3], u[3];
-            if (res) load3(mm, st.at(VM, i, row), 0);
-            else load3(mm, mc, row);
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-              const double z = sn[ia - c0][c] + be * pz[c];
-              const double q = mm[c] + be * pq[c];
-              const double sv = pw[c] + be * ps[c];
-              const double p = pu[c] + be * pp[c];
-              px[c] += al * p;
-              r[c] = pr[c] - al * sv;
-              u[c] = pu[c] - al * q;
-              w[c] = pw[c] - al * z;
-              pz[c] = z;
-              pq[c] = q;
-              ps[c] = sv;
-              pp[c] = p;
-              pr[c] = r[c];
-              pu[c] = u[c];
-              pw[c] = w[c];
-            }
-            double mnew[3];
-            mul33(mnew, D, w);
-            store3(mn, row, mnew);
-            if (res) store3(st.at(VM, i, row), 0, mnew);
-            v3[0] = dot3(r, u);
-            v3[1] = dot3(w, u);
-            v3[2] = dot3(r, r);
+          __syncthreads();
+          if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap))) {
+            stop = true;
+            break;
           }
-          rowbuf[ia - c0][0] = v3[0];
-          rowbuf[ia - c0][1] = v3[1];
-          rowbuf[ia - c0][2] = v3[2];
+          // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
+          // x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
+          for (int ia = c0 + (int)threadIdx.x; ia < c1; ia += blockDim.x) {
+            const int j = ar.piece(ia);
+            double v3[3] = {0, 0, 0};
+            if (!s_conv[j]) {
+              const int i = ar.local(ia, j);
+              const int row = ar.row(ia, j);
+              const double al = s_alpha[j], be = s_beta[j];
+              double* px = st.at(VX, i, row);
+              double* pr = st.at(VR, i, row);
+              double* pu = st.at(VU, i, row);
+              double* pw = st.at(VW, i, row);
+              double* pz = st.at(VZ, i, row);
+              double* pq = st.at(VQ, i, row);
+              double* ps = st.at(VS, i, row);
+              double* pp = st.at(VP, i, row);
+              const double* D = st.dinv(i, row);
+              double mm[3], w[3], r[3], u[3];
+              if (res) load3(mm, st.at(VM, i, row), 0);
+              else load3(mm, mc, row);
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const double z = sn[ia - c0][c] + be * pz[c];
+                const double q = mm[c] + be * pq[c];
+                const double sv = pw[c] + be * ps[c];
+                const double p = pu[c] + be * pp[c];
+                px[c] += al * p;
+                r[c] = pr[c] - al * sv;
+                u[c] = pu[c] - al * q;
+                w[c] = pw[c] - al * z;
+                pz[c] = z;
+                pq[c] = q;
+                ps[c] = sv;
+                pp[c] = p;
+                pr[c] = r[c];
+                pu[c] = u[c];
+                pw[c] = w[c];
+              }
+              double mnew[3];
+              mul33(mnew, D, w);
+              store3(mn, row, mnew);
+              if (res) store3(st.at(VM, i, row), 0, mnew);
+              v3[0] = dot3(r, u);
+              v3[1] = dot3(w, u);
+              v3[2] = dot3(r, r);
+            }
+            rowbuf[ia - c0][0] = v3[0];
+            rowbuf[ia - c0][1] = v3[1];
+            rowbuf[ia - c0][2] = v3[2];
+          }
+        } else {
+          // later chunks: all warps, SpMV and update fused per row
+          const int nw = blockDim.x >> 5;
+          if (a.row_lanes == 4) fused_rows<MT, 4>(a, mv, ar, st, res, mc, mn, c0, c1, warp, nw, lane, s_conv, s_alpha, s_beta, rowbuf);
+          else if (a.row_lanes == 8) fused_rows<MT, 8>(a, mv, ar, st, res, mc, mn, c0, c1, warp, nw, lane, s_conv, s_alpha, s_beta, rowbuf);
+          else if (a.row_lanes == 16) fused_rows<MT, 16>(a, mv, ar, st, res, mc, mn, c0, c1, warp, nw, lane, s_conv, s_alpha, s_beta, rowbuf);
+          else fused_rows<MT, 32>(a, mv, ar, st, res, mc, mn, c0, c1, warp, nw, lane, s_conv, s_alpha, s_beta, rowbuf);
         }
         __syncthreads();
         if (npc == 1 && c1 - c0 <= 32) {
