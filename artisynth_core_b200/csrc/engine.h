@@ -184,6 +184,7 @@ struct Engine {
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
   int opt_warm_start = 1;  // 0 previous velocity, 1 extrapolated from the last two
+  bool elem_tile_small = false;  // element kernels: the small tile of each material
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)

@@ -632,13 +632,32 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
     elem_linear_kernel<TYPE, T><<<(ne + EPB - 1) / EPB, 256, 0, eng.stream>>>(a, g.corotated);
     return cudaGetLastError();
   }
-  // elements per CTA: one thread per integration point in stage 1
-  constexpr int EPB_NH = TYPE == B200FEM_ELEM_TET ? 256 : 32;
-  constexpr int EPB_MR = TYPE == B200FEM_ELEM_TET ? 128 : 16;
-  if (g.mat_kind == B200FEM_MAT_NEOHOOKEAN)
-    return launch_nonlinear<TYPE, B200FEM_MAT_NEOHOOKEAN, false, T, EPB_NH>(a, ne, eng.stream);
-  if (g.nodal) return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, true, T, EPB_MR>(a, ne, eng.stream);
-  return launch_nonlinear<TYPE, B200FEM_MAT_MOONEYRIVLIN, false, T, EPB_MR>(a, ne, eng.stream);
+  // elements per CTA (one thread per integration point in stage 1): a
+  // large and a small tile per material; the small one gives more CTAs
+  // per SM and fewer idle threads in the pair stage on small groups
+  constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : 32, NH_S = NH_L / 2;
+  constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : 16, MR_S = MR_L / 2;
+  constexpr int NH = B200FEM_MAT_NEOHOOKEAN, MR = B200FEM_MAT_MOONEYRIVLIN;
+  cudaStream_t st = eng.stream;
+  if (ne < 0) {  // preparation: both tiles
+    cudaError_t e;
+    if (g.mat_kind == NH) {
+      e = launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st);
+    }
+    if (g.nodal) {
+      e = launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st);
+    }
+    e = launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
+    return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st);
+  }
+  const bool small = eng.elem_tile_small;
+  if (g.mat_kind == NH)
+    return small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
+  if (g.nodal)
+    return small ? launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
+  return small ? launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
 }
 
 // ---------------------------------------------------------------------------

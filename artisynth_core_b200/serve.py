@@ -83,7 +83,7 @@ class FemServer:
     """
 
     def __init__(self, workloads, budget=60e9, precision=L.PREC_MIXED, pack_models=256, tol=1e-10,
-                 max_iter=20000, device=0, clock=time.perf_counter):
+                 max_iter=20000, device=0, clock=time.perf_counter, autotune=False, tune_cache=None):
         self.pool = list(workloads)
         self.budget = float(budget)
         self.precision = precision
@@ -92,6 +92,8 @@ class FemServer:
         self.max_iter = max_iter
         self.device = device
         self.clock = clock
+        self.autotune = autotune        # tune each new pack's run-time layout options
+        self.tune_cache = tune_cache
         self.slots: list[_Slot] = []
         self.where = {}                  # model -> (slot, index in pack)
         self.saved = {}                  # model -> (x, v) of an evicted model
@@ -196,9 +198,20 @@ class FemServer:
                 # nothing else can make room: try the first model by its real size
                 batch = [self.waiting[0]]
             t0 = self.clock()
-            pack = FemPack([self.pool[m].model(precision=self.precision, device=self.device) for m in batch],
-                           precision=self.precision, device=self.device)
-            pack.engine()
+            models = [self.pool[m].model(precision=self.precision, device=self.device) for m in batch]
+            if self.autotune:
+                from . import autotune as at
+
+                def make(opts):
+                    p = FemPack(models, precision=self.precision, device=self.device, options=opts)
+                    p.engine()
+                    return p
+
+                pack, _, _ = at.tune_pack(make, models, self.precision, self.h, self.tol,
+                                          cache=self.tune_cache or at.TuneCache(), piece_rows=False)
+            else:
+                pack = FemPack(models, precision=self.precision, device=self.device)
+                pack.engine()
             if any(m in self.saved for m in batch):
                 xs, vs = [], []
                 for i, m in enumerate(batch):

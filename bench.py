@@ -215,12 +215,23 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
     from artisynth_core_b200 import _lib as L
     from artisynth_core_b200 import workloads as W
     from artisynth_core_b200.femmodel import FemPack, MechSystemSolver
+    from artisynth_core_b200 import autotune
+    import tempfile
     bs = W.batched_beams()
     for b in bs:
         b.build_mesh()
-    pack = FemPack([b.model(device=dev) for b in bs], precision=L.PREC_MIXED, device=dev)
+    models = [b.model(device=dev) for b in bs]
+
+    def make(opts):
+        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options=opts)
+        p.engine()
+        return p
+
     t0 = time.perf_counter()
-    pack.engine()
+    # a fresh cache: the tuning cost is part of what is reported
+    with tempfile.TemporaryDirectory() as td:
+        pack, tuned, _ = autotune.tune_pack(make, models, L.PREC_MIXED, bs[0].h, tol,
+                                            cache=autotune.TuneCache(os.path.join(td, "tune.json")))
     build_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     asm = pcg = 0.0
@@ -260,7 +271,8 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
         "workload": "256 uneven NeoHookean tet beams (n 4-60, m 2-8, seed 3), 20 steps h=0.01",
         "models": n, "tets": int(sum(b.conn.shape[0] for b in bs)), "steps": steps, "tol": tol,
         "precision": "mixed FP32 element/SpMV, FP64 vectors", "pcg_split": "strided" if split == 2 else "contiguous",
-        "device_bytes": nbytes, "build_s": build_s,
+        "device_bytes": nbytes, "build_and_tune_s": build_s,
+        "tuned": {k: v for k, v in tuned.items() if not k.endswith("_ms") and not k.endswith("_it")},
         "model_steps_per_s": n * steps / wall, "device_ms_per_step": (asm + pcg) / steps,
         "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
         "element_updates_per_s": sum(b.conn.shape[0] for b in bs) * steps / wall,
@@ -273,8 +285,8 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
     }
 
 
-def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=10, tol=1e-10,
-               drain_s=30.0, err_sample=16):
+def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=10, tol=1e-6,
+               drain_s=30.0, err_sample=16, plain_sample=32):
     """Served stream: Poisson arrivals (seed 4) of 10-step requests on models
     of the config-4 distribution with 10% large (n 80-120) beams, 60 GB
     device-memory budget, continuous batching."""
@@ -283,7 +295,11 @@ def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=
     pool = W.batched_beams(count=pool_size, seed=4, large_frac=0.1)
     for w in pool:
         w.build_mesh()
-    srv = FemServer(pool, budget=60e9, tol=tol, device=dev)
+    import tempfile
+    from artisynth_core_b200 import autotune
+    td = tempfile.TemporaryDirectory()
+    srv = FemServer(pool, budget=60e9, tol=tol, device=dev, autotune=True,
+                    tune_cache=autotune.TuneCache(os.path.join(td.name, "tune.json")))
     t0 = time.perf_counter()
     srv.preload()
     preload_s = time.perf_counter() - t0
@@ -295,17 +311,41 @@ def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=
         steps_of[r.model] = steps_of.get(r.model, 0) + r.steps
     incomplete_models = {m for m, q in srv.queues.items() if q}
     checked = [m for m in sorted(steps_of) if m not in incomplete_models and m not in srv.waiting][:err_sample]
-    err = 0.0
+    err = derr = 0.0
     for m in checked:
         x, _ = srv.state(m)
-        err = max(err, _rel(x, _fp64_alone(pool[m], steps_of[m], 1e-10, dev)))
+        xr = _fp64_alone(pool[m], steps_of[m], 1e-10, dev)
+        err = max(err, _rel(x, xr))
+        derr = max(derr, _rel(x - pool[m].rest, xr - pool[m].rest))
     srv.close()
+    td.cleanup()
+    # the plain FP64 drop-in on the same distribution, one model at a time
+    import torch
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200.femmodel import MechSystemSolver
+    t_plain, n_plain = 0.0, 0
+    for i in range(0, pool_size, max(1, pool_size // plain_sample)):
+        w = pool[i]
+        mdl = w.model(precision=L.PREC_FP64, device=dev)
+        ms = MechSystemSolver(mdl, tol=1e-10, max_iter=20000)
+        mdl.engine()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ms.backwardEuler(w.h, steps_per_request)
+        t_plain += time.perf_counter() - t1
+        n_plain += steps_per_request
+        mdl._invalidate()
+    plain = n_plain / t_plain
     out.update({
         "workload": f"Poisson {rate:.0f} req/s (seed 4) for {seconds:.0f} s, {steps_per_request} steps/request, "
                     f"pool of {pool_size} beams (config-4 distribution, 10% n 80-120)",
         "pool_tets": int(sum(w.conn.shape[0] for w in pool)), "tol": tol, "budget_bytes": 60e9,
         "preload_s": preload_s, "offered_model_steps_per_s": rate * steps_per_request,
-        "max_rel_position_error_vs_fp64": err, "error_sample_models": len(checked),
+        "max_rel_position_error_vs_fp64": err, "max_rel_displacement_error_vs_fp64": derr,
+        "error_sample_models": len(checked),
+        "plain_fp64_single_model_steps_per_s": plain,
+        "speedup_vs_plain_fp64": out["model_steps_per_s"] / plain,
+        "plain_fp64_sample": f"{n_plain // steps_per_request} pool models, {steps_per_request} steps each, PCG 1e-10",
     })
     return out
 
@@ -393,7 +433,7 @@ def run_b200(args):
             batched["clocks"] = c.summary()
         if world == 1 and args.served_seconds > 0:
             with ClockSampler(dev) as c:
-                served = run_served(dev, seconds=args.served_seconds, tol=args.batch_tol)
+                served = run_served(dev, seconds=args.served_seconds, tol=args.served_tol)
             served["clocks"] = c.summary()
         cpu = None
         if not args.no_cpu and world == 1:
@@ -437,7 +477,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-pack leg")
     ap.add_argument("--served-seconds", type=float, default=60.0, help="length of the served stream (0: skip)")
-    ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched and served legs")
+    ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched leg")
+    ap.add_argument("--served-tol", type=float, default=1e-6,
+                    help="PCG tolerance of the served leg (the loosest that keeps positions within 1e-6 of FP64)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

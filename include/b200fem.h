@@ -207,8 +207,8 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
    factorisation or an unpreconditioned CGSolver).  They choose how the
    persistent PCG kernel lays the pack's rows over the GPU; results agree
    across settings to rounding (each setting is bit-reproducible by itself).
-   SPLIT, CTAS and PIECE_ROWS take effect at b200fem_build; ROW_LANES and
-   WARM_START also afterwards (the step graph is re-captured). */
+   SPLIT, CTAS and PIECE_ROWS take effect at b200fem_build; ROW_LANES,
+   WARM_START and ELEM_TILE also afterwards (the step graphs are re-captured). */
 #define B200FEM_OPT_PCG_SPLIT 1  /* 0 auto; 1 contiguous rows per CTA (shared-memory
                                     resident when they fit); 2 strided: every model cut
                                     into short pieces dealt over all CTAs */
@@ -218,6 +218,9 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 #define B200FEM_OPT_WARM_START 5 /* PCG start: 0 the previous velocity; 1 (default) its linear
                                     extrapolation 2 v_n - v_(n-1) over the last two steps
                                     (may be changed after the build) */
+#define B200FEM_OPT_ELEM_TILE 6  /* elements per CTA of the non-linear element kernels: 0 auto,
+                                    1 large tile (tet 256 / hex 32 NeoHookean, 128 / 16
+                                    MooneyRivlin), 2 half of it (may be changed after the build) */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);

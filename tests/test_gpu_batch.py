@@ -158,3 +158,27 @@ def test_row_lanes_change_after_build(beams):
         pack.setOption(L.OPT_PCG_SPLIT, L.SPLIT_STRIDED)  # layout options precede the build
     pack.backwardEuler(beams[0].h, 1, tol=1e-12)
     assert np.all(np.isfinite(np.concatenate([xg for xg, _ in pack.getStates()])))
+
+
+def test_autotune_sets_options_and_keeps_results(beams, tmp_path):
+    from artisynth_core_b200 import autotune
+    models = [b.model() for b in beams]
+
+    def make(opts):
+        o = dict(opts)
+        o[L.OPT_PCG_SPLIT] = L.SPLIT_STRIDED
+        p = FemPack(models, precision=L.PREC_FP64, options=o)
+        p.engine()
+        return p
+
+    cache = autotune.TuneCache(str(tmp_path / "tune.json"))
+    pack, res, hit = autotune.tune_pack(make, models, L.PREC_FP64, beams[0].h, 1e-12, cache=cache)
+    assert not hit and pack.option(L.OPT_ROW_LANES) == res["row_lanes"]
+    assert pack.option(L.OPT_ELEM_TILE) == res["elem_tile"]
+    for x, v in pack.getStates():
+        assert np.all(v == 0)  # the tuning steps were undone
+    pack.backwardEuler(beams[0].h, 3, tol=1e-12)
+    ref = FemPack([b.model() for b in beams], precision=L.PREC_FP64)
+    ref.backwardEuler(beams[0].h, 3, tol=1e-12)
+    for (xa, _), (xb, _) in zip(pack.getStates(), ref.getStates()):
+        assert rel_err(xa, xb) <= 1e-9
