@@ -488,17 +488,17 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.inc_idx, iidx));
   CK(dalloc(eng, &d.K, (size_t)NB * 9));
   if (eng.precision == B200FEM_PREC_MIXED) {
-    // mixed form: FP32 rest data, element outputs and solve matrix
+    // mixed form: FP32 rest data, tangent blocks and solve matrix; the
+    // nodal forces (the force residual) stay FP64
     std::vector<float> invJ0_f(invJ0.begin(), invJ0.end());
     CK(upload(eng, &d.invJ0_f, invJ0_f));
     CK(dalloc(eng, &d.elemK_f, (size_t)E * npair * 9));
-    CK(dalloc(eng, &d.elemF_f, (size_t)E * nen * 3));
     CK(dalloc(eng, &d.S_f, (size_t)NB * 9));
   } else {
     CK(dalloc(eng, &d.elemK, (size_t)E * npair * 9));
-    CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
     CK(dalloc(eng, &d.S, (size_t)NB * 9));
   }
+  CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
   CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
   CK(dalloc(eng, &d.fint, 3 * (size_t)N));
   for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w, &d.u, &d.s, &d.m0, &d.m1}) {

@@ -91,7 +91,6 @@ struct DevPack {
   double* elemK = nullptr;     // E*npair*9
   double* elemF = nullptr;     // E*nen*3
   float* elemK_f = nullptr;
-  float* elemF_f = nullptr;
   // assembled values
   double* K = nullptr;         // nnzb*9 stiffness (drop-in output)
   double* S = nullptr;         // nnzb*9 solve matrix

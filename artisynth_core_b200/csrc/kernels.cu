@@ -265,11 +265,13 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
     }
   }
   __syncthreads();
-  // stage 2: one thread per element pair block, then per node force
+  // stage 2: one thread per element pair block, then per node force (the
+  // FP32 form leaves the forces to the FP64 force kernel)
+  constexpr int NF = sizeof(T) == 8 ? NEN : 0;
   T* elemK = (T*)a.elemK;
-  T* elemF = (T*)a.elemF;
-  for (int t = threadIdx.x; t < EPB * (NPAIR + NEN); t += blockDim.x) {
-    int el = t / (NPAIR + NEN), w = t % (NPAIR + NEN), e = ebase + el;
+  double* elemF = (double*)a.elemF;
+  for (int t = threadIdx.x; t < EPB * (NPAIR + NF); t += blockDim.x) {
+    int el = t / (NPAIR + NF), w = t % (NPAIR + NF), e = ebase + el;
     if (e >= a.e1) continue;
     if (w < NPAIR) {
       int ia, ib;
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
         int s = el * NIP + k;
         add_stress_force(f, sg[s][n], ssig[s], sdv[s]);
       }
-      T* out = elemF + ((size_t)e * NEN + n) * 3;
+      double* out = elemF + ((size_t)e * NEN + n) * 3;
       out[0] = f[0];
       out[1] = f[1];
       out[2] = f[2];
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
   }
   __syncthreads();
   T* elemK = (T*)a.elemK;
-  T* elemF = (T*)a.elemF;
+  double* elemF = (double*)a.elemF;
   for (int t = threadIdx.x; t < EPB * (NPAIR + NEN); t += blockDim.x) {
     int el = t / (NPAIR + NEN), w = t % (NPAIR + NEN), e = ebase + el;
     if (e >= a.e1) continue;
@@ -416,10 +418,10 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
           acc[0] = t2[0]; acc[1] = t2[1]; acc[2] = t2[2];
         }
       }
-      T* out = elemF + ((size_t)e * NEN + n) * 3;
-      out[0] = (T)acc[0];
-      out[1] = (T)acc[1];
-      out[2] = (T)acc[2];
+      double* out = elemF + ((size_t)e * NEN + n) * 3;
+      out[0] = acc[0];
+      out[1] = acc[1];
+      out[2] = acc[2];
     }
   }
 }
@@ -595,7 +597,7 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.mat = d.mat;
   a.node_p = d.node_p;
   a.elemK = fp32 ? (void*)d.elemK_f : (void*)d.elemK;
-  a.elemF = fp32 ? (void*)d.elemF_f : (void*)d.elemF;
+  a.elemF = (void*)d.elemF;  // nodal forces are FP64 in both forms
   a.flags = d.flags;
   a.mindet = (long long*)d.dmin;
   return a;
@@ -616,6 +618,104 @@ static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) 
   }
   if (!attr_set) return cudaErrorInvalidConfiguration;
   kern<<<(ne + EPB - 1) / EPB, 256, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FP64 element forces of the mixed form (non-linear materials): the force
+// residual keeps FP64 -- coordinates, shape gradients, F, stress and the
+// nodal forces f_a = sum_ip sigma g_a dv -- while the tangent blocks come
+// from the FP32 element kernel.  Nodal forces nearly cancel the external
+// load, so their small net value needs FP64 terms.  One thread per element
+// (tets) or per integration point, the 8 points of a hex reduced over 8
+// consecutive lanes in a fixed butterfly order.
+// ---------------------------------------------------------------------------
+template <int TYPE, int MAT, bool NODAL>
+__global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = a.e0 + (int)(t / NIP);
+  const int k = (int)(t % NIP);
+  bool live = e < a.e1;
+  if (live && a.active && !a.active[a.elem_model[e]]) live = false;
+  if (NIP == 1 && !live) return;  // tets: no cross-lane reduction follows
+  double fl[NEN][3];
+#pragma unroll
+  for (int n = 0; n < NEN; n++) fl[n][0] = fl[n][1] = fl[n][2] = 0;
+  if (live) {
+    const int* nodes = a.conn + (size_t)e * NEN;
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const double* xn = a.x + 3 * (size_t)nodes[n];
+      const double g0 = gns<double, TYPE>(k, n, 0), g1 = gns<double, TYPE>(k, n, 1), g2 = gns<double, TYPE>(k, n, 2);
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const double xr = xn[r];
+        J[3 * r] += xr * g0;
+        J[3 * r + 1] += xr * g1;
+        J[3 * r + 2] += xr * g2;
+      }
+    }
+    double iJ0[9], F[9], invJ[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0[((size_t)e * NIP + k) * 9 + i];
+    matmul3(F, J, iJ0);
+    const double detF = det3(F);
+    const double detJ = invert3(invJ, J);
+    const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
+    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    double sig[6];
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
+      double aa, bb;
+      neohookean_point<double>(sig, &aa, &bb, mp[0], mp[1], F, detF);
+    } else {
+      double pr = 0;
+      if constexpr (NODAL) {
+        if (TYPE == B200FEM_ELEM_TET) {
+          double s = 0;
+#pragma unroll
+          for (int n = 0; n < NEN; n++) s += a.node_p[nodes[n]];
+          pr = s / NEN;
+        } else {
+          pr = a.node_p[nodes[k]];
+        }
+      }
+      double D[36];
+      mooneyrivlin_point<double>(sig, D, mp, F, detF, pr);
+    }
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const double g0 = gns<double, TYPE>(k, n, 0), g1 = gns<double, TYPE>(k, n, 1), g2 = gns<double, TYPE>(k, n, 2);
+      double g[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) g[c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
+      add_stress_force(fl[n], g, sig, dv);
+    }
+  }
+  if constexpr (NIP > 1) {
+    // sum the points of one element: lanes 8q..8q+7 hold its 8 points
+#pragma unroll
+    for (int n = 0; n < NEN; n++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) fl[n][c] += __shfl_xor_sync(0xffffffffu, fl[n][c], off);
+    if (!live || k != 0) return;
+  }
+  double* out = (double*)a.elemF + (size_t)e * NEN * 3;
+#pragma unroll
+  for (int n = 0; n < NEN; n++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[3 * n + c] = fl[n][c];
+}
+
+template <int TYPE, int MAT, bool NODAL>
+static cudaError_t launch_force(const ElemArgs& a, int ne, cudaStream_t st) {
+  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  const long long threads = (long long)ne * NIP;
+  elem_force_kernel<TYPE, MAT, NODAL><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -653,11 +753,18 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
     return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st);
   }
   const bool small = eng.elem_tile_small;
-  if (g.mat_kind == NH)
-    return small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
-  if (g.nodal)
-    return small ? launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
-  return small ? launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
+  cudaError_t e;
+  if (g.mat_kind == NH) {
+    e = small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, NH, false>(a, ne, st);
+  } else if (g.nodal) {
+    e = small ? launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, true>(a, ne, st);
+  } else {
+    e = small ? launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, false>(a, ne, st);
+  }
+  return e;
 }
 
 // ---------------------------------------------------------------------------
@@ -873,12 +980,9 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   const int blocks = (d.n_nodes + threads - 1) / threads;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
   const double* vp = eng.opt_warm_start == 1 ? d.vprev : nullptr;
-  if (eng.precision == B200FEM_PREC_MIXED)
-    rows_kernel<float><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF_f, d.sidx,
-                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
-  else
-    rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
-                                                           d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
+  // nodal forces are FP64 in both forms
+  rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
+                                                         d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
   return cudaGetLastError();
 }
 
