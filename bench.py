@@ -207,7 +207,7 @@ def _fp64_alone(w, steps, tol, dev):
     return x
 
 
-def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
+def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
     """Batched uneven models: 256 NeoHookean tet beams in one pack (mixed
     FP32/FP64), `steps` BackwardEuler steps; next to the plain FP64 drop-in
     stepping the models one at a time (every `sample_every`-th model)."""
@@ -228,10 +228,13 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4):
         return p
 
     t0 = time.perf_counter()
-    # a fresh cache: the tuning cost is part of what is reported
-    with tempfile.TemporaryDirectory() as td:
-        pack, tuned, _ = autotune.tune_pack(make, models, L.PREC_MIXED, bs[0].h, tol,
-                                            cache=autotune.TuneCache(os.path.join(td, "tune.json")))
+    if tune:
+        # a fresh cache: the tuning cost is part of what is reported
+        with tempfile.TemporaryDirectory() as td:
+            pack, tuned, _ = autotune.tune_pack(make, models, L.PREC_MIXED, bs[0].h, tol,
+                                                cache=autotune.TuneCache(os.path.join(td, "tune.json")))
+    else:
+        pack, tuned = make({}), {}
     build_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     asm = pcg = 0.0
@@ -429,7 +432,7 @@ def run_b200(args):
         batched = served = None
         if world == 1 and not args.no_batched:
             with ClockSampler(dev) as c:
-                batched = run_batched(dev, tol=args.batch_tol)
+                batched = run_batched(dev, steps=args.batch_steps, tol=args.batch_tol, tune=not args.no_tune)
             batched["clocks"] = c.summary()
         if world == 1 and args.served_seconds > 0:
             with ClockSampler(dev) as c:
@@ -476,6 +479,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-pack leg")
+    ap.add_argument("--only", choices=["batched"], default=None,
+                    help="run only this leg (for profiling): prints its JSON object")
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
     ap.add_argument("--served-seconds", type=float, default=60.0, help="length of the served stream (0: skip)")
     ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched leg")
     ap.add_argument("--served-tol", type=float, default=1e-6,
@@ -485,6 +492,11 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only == "batched":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_batched(0, steps=args.batch_steps, tol=args.batch_tol, sample_every=64,
+                                     tune=not args.no_tune)), flush=True)
     else:
         run_b200(args)
 
