@@ -17,6 +17,8 @@ namespace b200fem {
 cudaError_t launch_forces_only(Engine& eng);
 int pcg_max_grid(int device);
 int pcg_max_cta_pieces();
+size_t fused_elem_bytes(int elem_type, int mat_kind, bool fp32);
+size_t fused_smem_budget(int elem_type);
 void pcg_plan_smem(int device, int nloc_max, int nb_max, int* resident, int* cached, bool fp32);
 cudaError_t prepare_pcg(Engine& eng);
 cudaError_t prepare_kernels(Engine& eng);
@@ -250,6 +252,58 @@ int build_pack(Engine& eng) {
     }
     eng.groups.push_back(g);
   }
+  // ---- fused assembly: block-row chunks whose incident elements fit the
+  // chunk's shared memory, and the contribution lists re-indexed to them
+  std::vector<int> chunk_row, chunk_eptr, chunk_elem, contrib_loc;
+  eng.fused = false;
+  if (eng.opt_fused == 1 && eng.groups.size() == 1 && !eng.groups[0].nodal &&
+      (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN || eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN)) {
+    const size_t per = fused_elem_bytes(eng.elem_type, eng.groups[0].mat_kind, eng.precision == B200FEM_PREC_MIXED);
+    const int emax = (int)(fused_smem_budget(eng.elem_type) / per);
+    std::vector<int> stamp(E, -1), loc(E, 0);
+    contrib_loc.assign(cidx.size(), 0);
+    bool ok = true;
+    int cur = 0, nin = 0, rstart = 0;
+    chunk_row.push_back(0);
+    chunk_eptr.push_back(0);
+    auto close = [&](int rend) {
+      for (int p = rowptr[rstart]; p < rowptr[rend]; p++)
+        for (int q = cptr[p]; q < cptr[p + 1]; q++) {
+          const int code = cidx[q];
+          const int e = (code >> 1) / npair, w = (code >> 1) % npair;
+          contrib_loc[q] = ((loc[e] * npair + w) << 1) | (code & 1);
+        }
+      chunk_row.push_back(rend);
+      chunk_eptr.push_back((int)chunk_elem.size());
+      cur++;
+      nin = 0;
+      rstart = rend;
+    };
+    for (int r = 0; r < R && ok; r++) {
+      const int n = act_node[r];
+      int fresh = 0;
+      for (int i = iptr[n]; i < iptr[n + 1]; i++) fresh += stamp[iidx[i] / nen] != cur;
+      if (fresh > emax) ok = false;  // one row alone does not fit
+      if (nin + fresh > emax && r > rstart) {
+        close(r);
+        fresh = iptr[n + 1] - iptr[n];
+      }
+      for (int i = iptr[n]; i < iptr[n + 1]; i++) {
+        const int e = iidx[i] / nen;
+        if (stamp[e] == cur) continue;
+        stamp[e] = cur;
+        loc[e] = nin++;
+        chunk_elem.push_back(e);
+      }
+    }
+    if (ok && R > 0) close(R);
+    if (ok) {
+      eng.fused = true;
+      eng.fused_chunks = (int)chunk_row.size() - 1;
+      eng.fused_emax = emax;
+    }
+  }
+
   // ---- NODAL soft incompressibility: direct-neighbour lists, incidence
   // slots, and per block the (divBlk i, divBlk j, node) triples of the
   // dilational term, node-ascending
@@ -486,6 +540,12 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.contrib_idx, cidx));
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));
+  if (eng.fused) {
+    CK(upload(eng, &d.chunk_row, chunk_row));
+    CK(upload(eng, &d.chunk_eptr, chunk_eptr));
+    CK(upload(eng, &d.chunk_elem, chunk_elem));
+    CK(upload(eng, &d.contrib_loc, contrib_loc));
+  }
   CK(dalloc(eng, &d.K, (size_t)NB * 9));
   if (eng.precision == B200FEM_PREC_MIXED) {
     // mixed form: FP32 rest data, tangent blocks and solve matrix; the
@@ -820,6 +880,11 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PIECE_ROWS is set before b200fem_build");
       eng.opt_piece_rows = value;
       return B200FEM_OK;
+    case B200FEM_OPT_FUSED_ASSEMBLY:
+      if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "FUSED_ASSEMBLY must be 0 or 1");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "FUSED_ASSEMBLY is set before b200fem_build");
+      eng.opt_fused = value;
+      return B200FEM_OK;
     case B200FEM_OPT_ELEM_TILE:
       if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "ELEM_TILE must be 0, 1 or 2");
       if ((value == 2) != eng.elem_tile_small) {
@@ -858,6 +923,7 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_PIECE_ROWS: *value = eng.opt_piece_rows; break;
     case B200FEM_OPT_WARM_START: *value = eng.opt_warm_start; break;
     case B200FEM_OPT_ELEM_TILE: *value = eng.elem_tile_small ? 2 : 1; break;
+    case B200FEM_OPT_FUSED_ASSEMBLY: *value = eng.built ? (eng.fused ? 1 : 0) : eng.opt_fused; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
   return B200FEM_OK;

@@ -133,6 +133,12 @@ struct DevPack {
   int* cta_plist = nullptr;    // n_pieces: global piece indices, CTA-major
   int* model_active = nullptr; // n_models: 0 = left out of assembly and steps
   double* vprev = nullptr;     // 3N: velocity before the last step (warm-start extrapolation)
+  // fused assembly: block-row chunks, their incident elements, and the
+  // contribution lists re-indexed to chunk-local elements
+  int* chunk_row = nullptr;    // chunks+1
+  int* chunk_eptr = nullptr;   // chunks+1
+  int* chunk_elem = nullptr;
+  int* contrib_loc = nullptr;  // parallel to contrib_idx
   int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
   int unconv_cap = 0;
   int n_pieces = 0;
@@ -184,6 +190,9 @@ struct Engine {
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
   int opt_warm_start = 1;  // 0 previous velocity, 1 extrapolated from the last two
   bool elem_tile_small = false;  // element kernels: the small tile of each material
+  bool fused = false;            // BackwardEuler assembly on the fused row-chunk path
+  int fused_chunks = 0, fused_emax = 0;
+  int opt_fused = 0;             // 1: fused assembly where supported
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)

@@ -132,6 +132,7 @@ struct ElemArgs {
   void* elemF;             // T* E*nen*3
   int* flags;              // [err, inverted]
   long long* mindet;       // ordered bits
+  int det_stats;           // the FP64 force kernel records inverted elements / min detJ
 };
 
 // Whole-block exit when none of the block's elements belongs to an active
@@ -600,6 +601,7 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.elemF = (void*)d.elemF;  // nodal forces are FP64 in both forms
   a.flags = d.flags;
   a.mindet = (long long*)d.dmin;
+  a.det_stats = 0;
   return a;
 }
 
@@ -665,6 +667,10 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
     const double detF = det3(F);
     const double detJ = invert3(invJ, J);
     const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
+    if (a.det_stats) {
+      if (!(detJ > 0.0)) atomicAdd(&a.flags[1], 1);
+      atomicMin(a.mindet, dbl_order(detJ));
+    }
     const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
     double sig[6];
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
@@ -716,6 +722,192 @@ static cudaError_t launch_force(const ElemArgs& a, int ne, cudaStream_t st) {
   constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
   const long long threads = (long long)ne * NIP;
   elem_force_kernel<TYPE, MAT, NODAL><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Fused element-to-block assembly of the BackwardEuler matrix (non-linear
+// materials without NODAL incompressibility).  Each CTA owns a chunk of
+// consecutive block rows: it first computes, for every element incident to
+// those rows, the integration-point records (shape gradients, dv, stress,
+// tangent coefficients) into shared memory, then forms each of its blocks by
+// walking the block's contribution list in element order -- the same sums,
+// in the same order, as the element kernel + gather pair, without the element
+// blocks' round trip through HBM.  Elements on a chunk boundary are computed
+// by every chunk they touch.
+// ---------------------------------------------------------------------------
+struct FusedArgs {
+  const int* chunk_row;   // [chunks + 1] block-row range of each chunk
+  const int* chunk_eptr;  // [chunks + 1]
+  const int* chunk_elem;  // element ids of each chunk, ascending
+  const int* contrib_ptr;
+  const int* contrib_loc;  // (chunk-local element * npair + pair) << 1 | transposed
+  const int* rowptr;
+  const int* blk_row;
+  const int* blk_diag;
+  const int* row_model;
+  const int* act_node;
+  const double* mass;
+  const double* step;
+  const int* conn;
+  const int* elem_model;
+  const int* active;
+  const double* x;
+  const double* invJ0;
+  const float* invJ0_f;
+  const double* mat;
+  void* out;  // S (TO)
+};
+
+template <int TYPE, int MAT, typename T>
+struct FusedSmem {
+  static constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  static constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  static constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
+  static constexpr size_t per_elem() { return sizeof(T) * (size_t)NIP * (NEN * 3 + 1 + 6 + DS); }
+};
+
+template <int TYPE, int MAT, typename T, typename TO>
+__global__ void __launch_bounds__(256) fused_block_kernel(FusedArgs a) {
+  using SM = FusedSmem<TYPE, MAT, T>;
+  constexpr int NEN = SM::NEN, NIP = SM::NIP, DS = SM::DS;
+  constexpr int NPAIR = NEN * (NEN + 1) / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x;
+  const int e0 = a.chunk_eptr[c], ne = a.chunk_eptr[c + 1] - e0;
+  const int nrec = ne * NIP;
+  T(*sg)[NEN][3] = reinterpret_cast<T(*)[NEN][3]>(smem_raw);
+  T* sdv = reinterpret_cast<T*>(smem_raw + sizeof(T) * (size_t)nrec * NEN * 3);
+  T(*ssig)[6] = reinterpret_cast<T(*)[6]>(sdv + nrec);
+  T(*sD)[DS] = reinterpret_cast<T(*)[DS]>(sdv + nrec + (size_t)nrec * 6);
+  // stage 1: one thread per (element, integration point)
+  for (int t = threadIdx.x; t < nrec; t += blockDim.x) {
+    const int le = t / NIP, k = t % NIP;
+    const int e = a.chunk_elem[e0 + le];
+    if (a.active && !a.active[a.elem_model[e]]) continue;
+    const int* nodes = a.conn + (size_t)e * NEN;
+    T J[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) J[i] = T(0);
+    const int n0 = nodes[0];
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const int nd = nodes[n];
+      const T g0 = gns<T, TYPE>(k, n, 0), g1 = gns<T, TYPE>(k, n, 1), g2 = gns<T, TYPE>(k, n, 2);
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        double v = a.x[3 * (size_t)nd + r];
+        if constexpr (sizeof(T) == 4) v -= a.x[3 * (size_t)n0 + r];  // FP32: relative to node 0, in FP64
+        const T p = (T)v;
+        J[3 * r] += p * g0;
+        J[3 * r + 1] += p * g1;
+        J[3 * r + 2] += p * g2;
+      }
+    }
+    T iJ0[9];
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0[((size_t)e * NIP + k) * 9 + i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0_f[((size_t)e * NIP + k) * 9 + i];
+    }
+    T F[9], invJ[9];
+    matmul3(F, J, iJ0);
+    const T detF = det3(F);
+    const T detJ = invert3(invJ, J);
+    const T w = TYPE == B200FEM_ELEM_TET ? T(1.0 / 6.0) : T(1);
+    sdv[t] = detJ * w;
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const T g0 = gns<T, TYPE>(k, n, 0), g1 = gns<T, TYPE>(k, n, 1), g2 = gns<T, TYPE>(k, n, 2);
+#pragma unroll
+      for (int cc = 0; cc < 3; cc++) sg[t][n][cc] = invJ[cc] * g0 + invJ[3 + cc] * g1 + invJ[6 + cc] * g2;
+    }
+    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
+      T aa, bb;
+      neohookean_point<T>(ssig[t], &aa, &bb, (T)mp[0], (T)mp[1], F, detF);
+      sD[t][0] = aa;
+      sD[t][1] = bb;
+    } else {
+      T mpt[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) mpt[i] = (T)mp[i];
+      mooneyrivlin_point<T>(ssig[t], sD[t], mpt, F, detF, T(0));
+    }
+  }
+  __syncthreads();
+  // stage 2: one thread per block of the chunk's rows
+  const int r0 = a.chunk_row[c], r1 = a.chunk_row[c + 1];
+  const int pb0 = a.rowptr[r0], pb1 = a.rowptr[r1];
+  TO* out = (TO*)a.out;
+  for (int p = pb0 + threadIdx.x; p < pb1; p += blockDim.x) {
+    const int row = a.blk_row[p];
+    const int m = a.row_model[row];
+    if (a.active && !a.active[m]) continue;
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int q1 = a.contrib_ptr[p + 1];
+    for (int q = a.contrib_ptr[p]; q < q1; q++) {
+      const int code = a.contrib_loc[q];
+      const int lw = code >> 1;
+      const int le = lw / NPAIR, wp = lw - le * NPAIR;
+      int ia, ib;
+      pair_of<NEN>(wp, ia, ib);
+      T K[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) K[i] = T(0);
+#pragma unroll
+      for (int k = 0; k < NIP; k++) {
+        const int s = le * NIP + k;
+        if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN)
+          add_bdb_iso(K, sg[s][ia], sD[s][0], sD[s][1], sg[s][ib], sdv[s]);
+        else
+          add_bdb(K, sg[s][ia], sD[s], sg[s][ib], sdv[s]);
+        add_geometric(K, sg[s][ia], ssig[s], sg[s][ib], sdv[s]);
+      }
+      if (code & 1) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) acc[3 * i + j] += (double)K[3 * j + i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; i++) acc[i] += (double)K[i];
+      }
+    }
+    // S = (h^2 + h beta) K + (1 + h alpha) M  (addPosJacobian, addVelJacobian,
+    // addActiveMassMatrix; MechSystemSolver.java:2277,2312,2334)
+    const double* sp = a.step + (size_t)m * 8;
+    const double h = sp[0], al = sp[1], be = sp[2];
+    const double cm = p == a.blk_diag[row] ? (1.0 + h * al) * a.mass[a.act_node[row]] : 0.0;
+    TO* o = out + (size_t)p * 9;
+#pragma unroll
+    for (int i = 0; i < 9; i++) o[i] = (TO)((h * h + h * be) * acc[i] + ((i % 4 == 0) ? cm : 0.0));
+  }
+}
+
+// shared-memory budget of one chunk: tets two CTAs per SM, hexes (eight
+// integration points per element) one
+size_t fused_smem_budget(int elem_type) { return elem_type == B200FEM_ELEM_TET ? 100 * 1024 : 200 * 1024; }
+
+template <int TYPE, int MAT, typename T, typename TO>
+static cudaError_t launch_fused(const FusedArgs& fa, int chunks, int emax, cudaStream_t st) {
+  using SM = FusedSmem<TYPE, MAT, T>;
+  auto kern = fused_block_kernel<TYPE, MAT, T, TO>;
+  const size_t smem = SM::per_elem() * (size_t)emax;
+  static bool attr_set = false;
+  if (chunks < 0) {  // preparation call (outside any stream capture): the
+    // attribute is process-wide, so it is set to the full budget, which
+    // covers every engine's chunks
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fused_smem_budget(TYPE));
+    if (e == cudaSuccess) attr_set = true;
+    return e;
+  }
+  if (!attr_set) return cudaErrorInvalidConfiguration;
+  if (chunks == 0) return cudaSuccess;
+  kern<<<chunks, 256, smem, st>>>(fa);
   return cudaGetLastError();
 }
 
@@ -911,9 +1103,12 @@ cudaError_t launch_divblk(Engine& eng) {
 
 // One-time preparation before any stream capture: constant tables and the
 // shared-memory opt-in of every element kernel this pack launches.
+static cudaError_t launch_fused_blocks(Engine& eng, int chunks);
+
 cudaError_t prepare_kernels(Engine& eng) {
   cudaError_t e = ensure_constants(eng.device);
   if (e != cudaSuccess) return e;
+  if (eng.fused && (e = launch_fused_blocks(eng, -1)) != cudaSuccess) return e;
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
   for (ElemGroup g : eng.groups) {
     g.e1 = g.e0 - 1;  // ne = -1: set attributes only
@@ -926,12 +1121,86 @@ cudaError_t prepare_kernels(Engine& eng) {
   return cudaSuccess;
 }
 
+size_t fused_elem_bytes(int elem_type, int mat_kind, bool fp32) {
+  const bool tet = elem_type == B200FEM_ELEM_TET, nh = mat_kind == B200FEM_MAT_NEOHOOKEAN;
+  if (tet) {
+    if (nh) return fp32 ? FusedSmem<B200FEM_ELEM_TET, B200FEM_MAT_NEOHOOKEAN, float>::per_elem()
+                        : FusedSmem<B200FEM_ELEM_TET, B200FEM_MAT_NEOHOOKEAN, double>::per_elem();
+    return fp32 ? FusedSmem<B200FEM_ELEM_TET, B200FEM_MAT_MOONEYRIVLIN, float>::per_elem()
+                : FusedSmem<B200FEM_ELEM_TET, B200FEM_MAT_MOONEYRIVLIN, double>::per_elem();
+  }
+  if (nh) return fp32 ? FusedSmem<B200FEM_ELEM_HEX, B200FEM_MAT_NEOHOOKEAN, float>::per_elem()
+                      : FusedSmem<B200FEM_ELEM_HEX, B200FEM_MAT_NEOHOOKEAN, double>::per_elem();
+  return fp32 ? FusedSmem<B200FEM_ELEM_HEX, B200FEM_MAT_MOONEYRIVLIN, float>::per_elem()
+              : FusedSmem<B200FEM_ELEM_HEX, B200FEM_MAT_MOONEYRIVLIN, double>::per_elem();
+}
+
+// chunks < 0: set the kernel's shared-memory attribute only
+static cudaError_t launch_fused_blocks(Engine& eng, int chunks) {
+  DevPack& d = eng.d;
+  FusedArgs fa;
+  fa.chunk_row = d.chunk_row;
+  fa.chunk_eptr = d.chunk_eptr;
+  fa.chunk_elem = d.chunk_elem;
+  fa.contrib_ptr = d.contrib_ptr;
+  fa.contrib_loc = d.contrib_loc;
+  fa.rowptr = d.blk_rowptr;
+  fa.blk_row = d.blk_row;
+  fa.blk_diag = d.blk_diag;
+  fa.row_model = d.row_model;
+  fa.act_node = d.act_node;
+  fa.mass = d.mass;
+  fa.step = d.step;
+  fa.conn = d.conn;
+  fa.elem_model = d.elem_model;
+  fa.active = eng.any_inactive ? d.model_active : nullptr;
+  fa.x = d.x;
+  fa.invJ0 = d.invJ0;
+  fa.invJ0_f = d.invJ0_f;
+  fa.mat = d.mat;
+  const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  fa.out = fp32 ? (void*)d.S_f : (void*)d.S;
+  const int em = eng.fused_emax;
+  const bool tet = eng.elem_type == B200FEM_ELEM_TET;
+  const bool nh = eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN;
+  constexpr int TET = B200FEM_ELEM_TET, HEX = B200FEM_ELEM_HEX, NH = B200FEM_MAT_NEOHOOKEAN,
+                MR = B200FEM_MAT_MOONEYRIVLIN;
+  cudaStream_t st = eng.stream;
+  if (fp32) {
+    if (tet) return nh ? launch_fused<TET, NH, float, float>(fa, chunks, em, st) : launch_fused<TET, MR, float, float>(fa, chunks, em, st);
+    return nh ? launch_fused<HEX, NH, float, float>(fa, chunks, em, st) : launch_fused<HEX, MR, float, float>(fa, chunks, em, st);
+  }
+  if (tet) return nh ? launch_fused<TET, NH, double, double>(fa, chunks, em, st) : launch_fused<TET, MR, double, double>(fa, chunks, em, st);
+  return nh ? launch_fused<HEX, NH, double, double>(fa, chunks, em, st) : launch_fused<HEX, MR, double, double>(fa, chunks, em, st);
+}
+
+// BackwardEuler assembly on the fused path: FP64 nodal forces (and the
+// inverted-element statistics) per element, then the blocks of S per row chunk
+static cudaError_t launch_assemble_fused(Engine& eng) {
+  const ElemGroup& g = eng.groups[0];
+  ElemArgs a = elem_args(eng, g, eng.precision == B200FEM_PREC_MIXED);
+  a.det_stats = 1;
+  const int ne = g.e1 - g.e0;
+  cudaError_t e = cudaSuccess;
+  constexpr int TET = B200FEM_ELEM_TET, HEX = B200FEM_ELEM_HEX, NH = B200FEM_MAT_NEOHOOKEAN,
+                MR = B200FEM_MAT_MOONEYRIVLIN;
+  if (ne > 0) {
+    if (eng.elem_type == TET)
+      e = g.mat_kind == NH ? launch_force<TET, NH, false>(a, ne, eng.stream) : launch_force<TET, MR, false>(a, ne, eng.stream);
+    else
+      e = g.mat_kind == NH ? launch_force<HEX, NH, false>(a, ne, eng.stream) : launch_force<HEX, MR, false>(a, ne, eng.stream);
+  }
+  if (e != cudaSuccess) return e;
+  return launch_fused_blocks(eng, eng.fused_chunks);
+}
+
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   (void)cK;
   (void)cM;
   cudaError_t e = cudaSuccess;
   DevPack& d = eng.d;
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
+  if (!want_K && eng.fused) return launch_assemble_fused(eng);
   if ((e = launch_nodal_pressure(eng)) != cudaSuccess) return e;
   if ((e = launch_divblk(eng)) != cudaSuccess) return e;
   for (const ElemGroup& g : eng.groups) {

@@ -255,6 +255,8 @@ class FemModel3d:
             p = self.material.params()
             prm[: len(p)] = p
             eng.call("b200fem_set_material", self.material.kind, L.dptr(prm), self.density, self.soft_incomp)
+            for k, v in getattr(self, "options", {}).items():
+                eng.call("b200fem_set_option", int(k), int(v))
             eng.call("b200fem_build")
             self._engine = eng
             if self.fext is not None:

@@ -250,8 +250,20 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
     it_m, _ = pack.modelStats()
     xs = [x for x, _ in pack.getStates()]
     split = pack.option(L.OPT_PCG_SPLIT)
+    fused = pack.option(L.OPT_FUSED_ASSEMBLY) == 0
     nbytes = pack.deviceBytes()
+    import ctypes
+    na, nb = ctypes.c_int(), ctypes.c_int()
+    pack.engine().call("b200fem_get_sizes", ctypes.byref(na), ctypes.byref(nb), None, None)
     pack.close()
+    # algorithmic assembly bytes of one pack step (element data at the stored
+    # precision: f32 rest data and S in the mixed form)
+    N = sum(b.rest.shape[0] for b in bs)
+    E = sum(b.conn.shape[0] for b in bs)
+    nen, nip = 4, 1
+    asm_bytes = 24 * N + 4 * nen * E + 36 * nip * E + 4 * nen * nen * E + 36 * nb.value + 24 * N
+    peak, kind = peaks()
+    asm_gbs = asm_bytes / (asm / steps * 1e-3) / 1e9
     # plain FP64 drop-in, one model at a time, on a sample
     sample = list(range(0, len(bs), sample_every))
     t_single = 0.0
@@ -278,6 +290,9 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
         "tuned": {k: v for k, v in tuned.items() if not k.endswith("_ms") and not k.endswith("_it")},
         "model_steps_per_s": n * steps / wall, "device_ms_per_step": (asm + pcg) / steps,
         "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
+        "assembly": {"path": "fused row-chunk" if fused else "element kernel + gather",
+                     "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_gbs, "peak_gbs": peak,
+                     "frac": asm_gbs / peak, "peak_kind": kind, "nnzb": nb.value},
         "element_updates_per_s": sum(b.conn.shape[0] for b in bs) * steps / wall,
         "pcg_iterations": {"max_per_step_mean": float(np.mean(its)), "model_median": float(np.median(it_m)),
                            "model_p90": float(np.percentile(it_m, 90))},

@@ -221,6 +221,13 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 #define B200FEM_OPT_ELEM_TILE 6  /* elements per CTA of the non-linear element kernels: 0 auto,
                                     1 large tile (tet 256 / hex 32 NeoHookean, 128 / 16
                                     MooneyRivlin), 2 half of it (may be changed after the build) */
+#define B200FEM_OPT_FUSED_ASSEMBLY 7 /* BackwardEuler assembly: 0 (default) element kernel +
+                                        block gather; 1 fused row-chunk assembly for NeoHookean /
+                                        MooneyRivlin packs without NODAL incompressibility (after
+                                        the build: 1 when the fused path is in force).  The fused
+                                        path avoids the element blocks' HBM round trip but
+                                        recomputes boundary elements; it measured slower on the
+                                        benchmark meshes and is kept for larger chunks later. */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
