@@ -33,6 +33,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 PART_FULL, PART_UPPER = 0, 1
 PCG_AUTO, PCG_CLASSIC, PCG_PIPELINED = 0, 1, 2
 OPT_PCG_SPLIT, OPT_ROW_LANES, OPT_PCG_CTAS, OPT_PIECE_ROWS, OPT_WARM_START, OPT_ELEM_TILE, OPT_FUSED_ASSEMBLY = 1, 2, 3, 4, 5, 6, 7
+OPT_REFINE = 8
 SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED = 0, 1, 2
 
 

@@ -595,6 +595,16 @@ int build_pack(Engine& eng) {
     std::vector<double> ms((size_t)M * 4, 0.0);
     for (int m = 0; m < M; m++) ms[(size_t)m * 4 + 2] = 1.0;
     CK(upload(eng, &d.model_scal, ms));
+    // refinement sweeps (mixed form): FP64 residual, correction, and the
+    // correction solves' own per-model results
+    eng.refine_ok = eng.precision == B200FEM_PREC_MIXED && eng.groups.size() == 1 && !eng.groups[0].nodal &&
+                    (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN ||
+                     eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN);
+    if (eng.refine_ok) {
+      CK(dalloc(eng, &d.rref, 3 * (size_t)R));
+      CK(dalloc(eng, &d.dsol, 3 * (size_t)R));
+      CK(upload(eng, &d.model_scal2, ms));
+    }
   }
   CK(dalloc(eng, &d.barrier, 2));
   CK(cudaMemset(d.barrier, 0, 2 * sizeof(unsigned)));
@@ -880,6 +890,13 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PIECE_ROWS is set before b200fem_build");
       eng.opt_piece_rows = value;
       return B200FEM_OK;
+    case B200FEM_OPT_REFINE:
+      if (value < 0 || value > 4) return fail(&eng, B200FEM_ERR_INVALID_ARG, "REFINE must be 0..4");
+      if (value != eng.opt_refine) {
+        eng.opt_refine = value;
+        eng.step_exec_max_iter = -1;  // recapture the solve phase
+      }
+      return B200FEM_OK;
     case B200FEM_OPT_FUSED_ASSEMBLY:
       if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "FUSED_ASSEMBLY must be 0 or 1");
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "FUSED_ASSEMBLY is set before b200fem_build");
@@ -924,6 +941,7 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_WARM_START: *value = eng.opt_warm_start; break;
     case B200FEM_OPT_ELEM_TILE: *value = eng.elem_tile_small ? 2 : 1; break;
     case B200FEM_OPT_FUSED_ASSEMBLY: *value = eng.built ? (eng.fused ? 1 : 0) : eng.opt_fused; break;
+    case B200FEM_OPT_REFINE: *value = (eng.built && !eng.refine_ok) ? 0 : eng.opt_refine; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
   return B200FEM_OK;
@@ -1128,6 +1146,7 @@ static int read_step_status(Engine& eng, b200fem_stats* stats, int max_iter) {
     all_conv &= ms[(size_t)m * 4 + 2] != 0.0;
   }
   st.num_inverted = flags[1];
+  st.refinements = eng.refine_ok ? eng.opt_refine : 0;
   long long bits = dmin >= 0 ? dmin : (dmin ^ 0x7fffffffffffffffll);
   std::memcpy(&st.min_detJ, &bits, sizeof(double));
   eng.last_stats = st;
@@ -1191,7 +1210,7 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
         ce = launch_assemble(eng, 0, 0, false);
         if (ce == cudaSuccess) ce = launch_rhs(eng);
       } else {
-        ce = launch_pcg(eng, max_iter, true, 0);
+        ce = launch_solve(eng, max_iter);
       }
       cudaError_t ee = cudaStreamEndCapture(eng.stream, &graph);
       if (ce != cudaSuccess) return cuda_fail(&eng, ce, "capture of the BackwardEuler step");
@@ -1224,7 +1243,7 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
         return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
     }
     if (graphs) CK(cudaGraphLaunch(eng.step_exec, eng.stream));
-    else CK(launch_pcg(eng, max_iter, true, 0));
+    else CK(launch_solve(eng, max_iter));
     CK(cudaEventRecord(eng.ev_pool[2], eng.stream));
   }
   CK(cudaEventRecord(eng.ev[1], eng.stream));

@@ -139,6 +139,10 @@ struct DevPack {
   int* chunk_eptr = nullptr;   // chunks+1
   int* chunk_elem = nullptr;
   int* contrib_loc = nullptr;  // parallel to contrib_idx
+  // refinement sweeps: FP64 residual, correction, its PCG results
+  double* rref = nullptr;
+  double* dsol = nullptr;
+  double* model_scal2 = nullptr;
   int* unconv = nullptr;       // PCG per-iteration 'some model unconverged' words
   int unconv_cap = 0;
   int n_pieces = 0;
@@ -193,6 +197,9 @@ struct Engine {
   bool fused = false;            // BackwardEuler assembly on the fused row-chunk path
   int fused_chunks = 0, fused_emax = 0;
   int opt_fused = 0;             // 1: fused assembly where supported
+  int opt_refine = 0;            // refinement sweeps of the mixed form
+  bool refine_ok = false;        // supported by the pack (mixed, one NeoHookean/MooneyRivlin group, no NODAL)
+  double refine_tol = 1e-3;      // relative tolerance of a correction solve
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)
@@ -224,6 +231,9 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K);
 cudaError_t launch_rhs(Engine& eng);
 cudaError_t launch_reset_status(Engine& eng);
 cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero);
+cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const double* rhs, double* xsol,
+                          double tol_override, double* model_out);
+cudaError_t launch_solve(Engine& eng, int max_iter);
 cudaError_t launch_spmv(Engine& eng, const double* x, double* y);
 cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs);
 int read_pcg_result(Engine& eng, b200fem_stats* st);

@@ -1103,6 +1103,206 @@ cudaError_t launch_divblk(Engine& eng) {
 
 // One-time preparation before any stream capture: constant tables and the
 // shared-memory opt-in of every element kernel this pack launches.
+// ---------------------------------------------------------------------------
+// Iterative refinement of the mixed form against the FP64 operator.  The
+// mixed form solves with the FP32 matrix; a refinement sweep forms the FP64
+// residual r = b - S64 v matrix-free -- S64 v = (1 + h alpha) M v +
+// (h^2 + h beta) K v, with K v summed from the elements' FP64 tangents
+// (recomputed per integration point: material part B_a^T D (B v), geometric
+// part L sigma g_a with L = sum_b v_b g_b^T) -- solves S32 d = r loosely with
+// the same PCG and updates v += d.
+// ---------------------------------------------------------------------------
+template <int TYPE, int MAT>
+__global__ void __launch_bounds__(128) elem_kv_kernel(ElemArgs a, const double* __restrict__ v) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = a.e0 + (int)(t / NIP);
+  const int k = (int)(t % NIP);
+  bool live = e < a.e1;
+  if (live && a.active && !a.active[a.elem_model[e]]) live = false;
+  if (NIP == 1 && !live) return;
+  double fl[NEN][3];
+#pragma unroll
+  for (int n = 0; n < NEN; n++) fl[n][0] = fl[n][1] = fl[n][2] = 0;
+  if (live) {
+    const int* nodes = a.conn + (size_t)e * NEN;
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const double* xn = a.x + 3 * (size_t)nodes[n];
+      const double g0 = gns<double, TYPE>(k, n, 0), g1 = gns<double, TYPE>(k, n, 1), g2 = gns<double, TYPE>(k, n, 2);
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        J[3 * r] += xn[r] * g0;
+        J[3 * r + 1] += xn[r] * g1;
+        J[3 * r + 2] += xn[r] * g2;
+      }
+    }
+    double iJ0[9], F[9], invJ[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0[((size_t)e * NIP + k) * 9 + i];
+    matmul3(F, J, iJ0);
+    const double detF = det3(F);
+    const double detJ = invert3(invJ, J);
+    const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
+    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    double sig[6], D[36], ca = 0, cb = 0;
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) neohookean_point<double>(sig, &ca, &cb, mp[0], mp[1], F, detF);
+    else mooneyrivlin_point<double>(sig, D, mp, F, detF, 0.0);
+    // L = sum_b v_b g_b^T (velocities of fixed nodes are zero)
+    double g[NEN][3], L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      const double g0 = gns<double, TYPE>(k, n, 0), g1 = gns<double, TYPE>(k, n, 1), g2 = gns<double, TYPE>(k, n, 2);
+#pragma unroll
+      for (int c = 0; c < 3; c++) g[n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
+      const int r = a.sidx[nodes[n]];
+      if (r < 0) continue;
+      const double* vn = v + 3 * (size_t)r;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) L[3 * i + j] += vn[i] * g[n][j];
+    }
+    // engineering strain B v and tau = D (B v), Voigt xx yy zz xy yz xz
+    const double eps[6] = {L[0], L[4], L[8], L[1] + L[3], L[5] + L[7], L[2] + L[6]};
+    double tau[6];
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
+      const double tr = eps[0] + eps[1] + eps[2];
+#pragma unroll
+      for (int i = 0; i < 3; i++) tau[i] = ca * tr + 2.0 * cb * eps[i];
+#pragma unroll
+      for (int i = 3; i < 6; i++) tau[i] = cb * eps[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < 6; j++) s += D[6 * i + j] * eps[j];
+        tau[i] = s;
+      }
+    }
+#pragma unroll
+    for (int n = 0; n < NEN; n++) {
+      add_stress_force(fl[n], g[n], tau, dv);
+      // geometric part: L sigma g_a dv
+      const double sg0 = sig[0] * g[n][0] + sig[3] * g[n][1] + sig[5] * g[n][2];
+      const double sg1 = sig[3] * g[n][0] + sig[1] * g[n][1] + sig[4] * g[n][2];
+      const double sg2 = sig[5] * g[n][0] + sig[4] * g[n][1] + sig[2] * g[n][2];
+#pragma unroll
+      for (int i = 0; i < 3; i++) fl[n][i] += dv * (L[3 * i] * sg0 + L[3 * i + 1] * sg1 + L[3 * i + 2] * sg2);
+    }
+  }
+  if constexpr (NIP > 1) {
+#pragma unroll
+    for (int n = 0; n < NEN; n++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) fl[n][c] += __shfl_xor_sync(0xffffffffu, fl[n][c], off);
+    if (!live || k != 0) return;
+  }
+  double* out = (double*)a.elemF + (size_t)e * NEN * 3;
+#pragma unroll
+  for (int n = 0; n < NEN; n++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) out[3 * n + c] = fl[n][c];
+}
+
+// r = b - (1 + h alpha) m v - (h^2 + h beta) (K v), per active row (K v
+// summed from the element products in element order); the correction starts
+// at zero
+__global__ void refine_residual_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                       const double* __restrict__ ekv, const int* __restrict__ sidx,
+                                       const int* __restrict__ node_model, const double* __restrict__ mass,
+                                       const double* __restrict__ step, const double* __restrict__ b,
+                                       const double* __restrict__ v, double* __restrict__ r,
+                                       double* __restrict__ dsol, const int* __restrict__ active) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int row = sidx[n];
+  if (row < 0) return;
+  double kv[3] = {0, 0, 0};
+  const bool on = !active || active[node_model[n]];
+  if (on)
+    for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) kv[c] += ekv[(size_t)inc_idx[i] * 3 + c];
+  const double* sp = step + (size_t)node_model[n] * 8;
+  const double h = sp[0], al = sp[1], be = sp[2];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const size_t q = 3 * (size_t)row + c;
+    r[q] = on ? b[q] - (1.0 + h * al) * mass[n] * v[q] - (h * h + h * be) * kv[c] : 0.0;
+    dsol[q] = 0.0;
+  }
+}
+
+__global__ void refine_add_kernel(int R, double* __restrict__ v, const double* __restrict__ dv) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < 3LL * R) v[q] += dv[q];
+}
+
+// v_prev = v, v = v1, x += h v1 for the active rows (the PCG's own update,
+// done here after the refinement sweeps)
+__global__ void refine_state_kernel(int R, const int* __restrict__ act_node, const int* __restrict__ row_model,
+                                    const double* __restrict__ step, const double* __restrict__ sol,
+                                    double* __restrict__ x, double* __restrict__ vel, double* __restrict__ vprev,
+                                    const int* __restrict__ active) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= R) return;
+  const int m = row_model[row];
+  if (active && !active[m]) return;
+  const int n = act_node[row];
+  const double h = step[(size_t)m * 8];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double vn = sol[3 * (size_t)row + c];
+    vprev[3 * (size_t)n + c] = vel[3 * (size_t)n + c];
+    vel[3 * (size_t)n + c] = vn;
+    x[3 * (size_t)n + c] += h * vn;
+  }
+}
+
+// the solve phase of a BackwardEuler step: PCG, then the refinement sweeps
+// of the mixed form (when asked for and supported) and the state update
+cudaError_t launch_solve(Engine& eng, int max_iter) {
+  DevPack& d = eng.d;
+  const int sweeps = eng.refine_ok ? eng.opt_refine : 0;
+  if (sweeps == 0) return launch_pcg(eng, max_iter, true, 0);
+  cudaError_t e = launch_pcg(eng, max_iter, false, 0);
+  const int* act = eng.any_inactive ? d.model_active : nullptr;
+  const ElemGroup& g = eng.groups[0];
+  ElemArgs a = elem_args(eng, g, true);
+  const int ne = g.e1 - g.e0;
+  constexpr int TET = B200FEM_ELEM_TET, HEX = B200FEM_ELEM_HEX, NH = B200FEM_MAT_NEOHOOKEAN,
+                MR = B200FEM_MAT_MOONEYRIVLIN;
+  const int nip = eng.elem_type == TET ? 1 : 8;
+  const unsigned kb = (unsigned)(((long long)ne * nip + 127) / 128);
+  for (int s = 0; s < sweeps && e == cudaSuccess; s++) {
+    if (ne > 0) {
+      if (eng.elem_type == TET) {
+        if (g.mat_kind == NH) elem_kv_kernel<TET, NH><<<kb, 128, 0, eng.stream>>>(a, d.sol);
+        else elem_kv_kernel<TET, MR><<<kb, 128, 0, eng.stream>>>(a, d.sol);
+      } else {
+        if (g.mat_kind == NH) elem_kv_kernel<HEX, NH><<<kb, 128, 0, eng.stream>>>(a, d.sol);
+        else elem_kv_kernel<HEX, MR><<<kb, 128, 0, eng.stream>>>(a, d.sol);
+      }
+    }
+    refine_residual_kernel<<<(d.n_nodes + 127) / 128, 128, 0, eng.stream>>>(
+        d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx, d.node_model, d.mass, d.step, d.b, d.sol, d.rref,
+        d.dsol, act);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = launch_pcg_on(eng, max_iter, false, d.rref, d.dsol, eng.refine_tol, d.model_scal2);
+    if (e != cudaSuccess) return e;
+    refine_add_kernel<<<(unsigned)((3LL * d.n_rows + 255) / 256), 256, 0, eng.stream>>>(d.n_rows, d.sol, d.dsol);
+  }
+  refine_state_kernel<<<(d.n_rows + 127) / 128, 128, 0, eng.stream>>>(d.n_rows, d.act_node, d.row_model, d.step,
+                                                                      d.sol, d.x, d.v, d.vprev, act);
+  return cudaGetLastError();
+}
+
 static cudaError_t launch_fused_blocks(Engine& eng, int chunks);
 
 cudaError_t prepare_kernels(Engine& eng) {

@@ -108,6 +108,7 @@ struct PcgArgs {
   const int* cta_plist;  // global piece indices, CTA-major
   double* partials;  // [2][n_pieces][4]
   const double* step;
+  double tol_override;  // > 0: the tolerance of every model (refinement corrections)
   double* model_out;  // n_models * 4: iterations, true rel residual, converged
   int resident;       // row-local vectors and Dinv live in shared memory
   int cached;         // the CTA's slice of S (values, columns, row offsets) is copied to shared memory
@@ -632,7 +633,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   for (int j = threadIdx.x; j < npc; j += blockDim.x) {
     const int m = a.piece_model[s_gp[j]];
     const int off = a.model_active && !a.model_active[m];
-    s_tol[j] = a.step[(size_t)m * 8 + 6];
+    s_tol[j] = a.tol_override > 0 ? a.tol_override : a.step[(size_t)m * 8 + 6];
     s_conv[j] = off;
     s_done[j] = off;
     s_iters[j] = 0;
@@ -1081,12 +1082,13 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   }
 }
 
-cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero) {
+// Solve S x = b with the persistent PCG on the given right-hand side and
+// iterate (x in/out); tol_override > 0 replaces every model's tolerance;
+// per-model results go to model_out.
+cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const double* rhs, double* xsol,
+                          double tol_override, double* model_out) {
   DevPack& d = eng.d;
   cudaError_t e;
-  if (init_zero) {
-    if ((e = cudaMemsetAsync(d.sol, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream)) != cudaSuccess) return e;
-  }
   if ((e = cudaMemsetAsync(d.barrier, 0, sizeof(unsigned), eng.stream)) != cudaSuccess) return e;
   PcgArgs a;
   a.n_rows = d.n_rows;
@@ -1096,8 +1098,8 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.blk_diag = d.blk_diag;
   a.S = d.S;
   a.Dinv = d.Dinv;
-  a.b = d.b;
-  a.x = d.sol;
+  a.b = rhs;
+  a.x = xsol;
   a.r = d.r;
   a.u = d.u;
   a.w = d.w;
@@ -1114,7 +1116,8 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   a.cta_plist = d.cta_plist;
   a.partials = d.partials;
   a.step = d.step;
-  a.model_out = d.model_scal;
+  a.model_out = model_out;
+  a.tol_override = tol_override;
   a.barrier = d.barrier;
   a.flags = d.flags;
   a.unconv = d.unconv;
@@ -1155,6 +1158,15 @@ cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_ze
   }
   return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true>, a)
                     : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false>, a);
+}
+
+cudaError_t launch_pcg(Engine& eng, int max_iter, bool update_state, int init_zero) {
+  DevPack& d = eng.d;
+  if (init_zero) {
+    cudaError_t e = cudaMemsetAsync(d.sol, 0, sizeof(double) * 3 * (size_t)d.n_rows, eng.stream);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_pcg_on(eng, max_iter, update_state, d.b, d.sol, 0.0, d.model_scal);
 }
 
 int pcg_threads() { return kPcgThreads; }
@@ -1419,6 +1431,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.act_node = nullptr;
   a.row_model = nullptr;
   a.model_active = nullptr;
+  a.tol_override = 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);
   cfg.blockDim = dim3(kPcgThreads);

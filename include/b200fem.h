@@ -221,6 +221,12 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 #define B200FEM_OPT_ELEM_TILE 6  /* elements per CTA of the non-linear element kernels: 0 auto,
                                     1 large tile (tet 256 / hex 32 NeoHookean, 128 / 16
                                     MooneyRivlin), 2 half of it (may be changed after the build) */
+#define B200FEM_OPT_REFINE 8     /* refinement sweeps of the mixed form (0..4, default 0): each
+                                    forms the FP64 residual b - S64 v matrix-free from the
+                                    elements' FP64 tangents, solves the correction with the FP32
+                                    matrix to 1e-3 and adds it (one NeoHookean/MooneyRivlin
+                                    group without NODAL incompressibility; may be changed after
+                                    the build) */
 #define B200FEM_OPT_FUSED_ASSEMBLY 7 /* BackwardEuler assembly: 0 (default) element kernel +
                                         block gather; 1 fused row-chunk assembly for NeoHookean /
                                         MooneyRivlin packs without NODAL incompressibility (after

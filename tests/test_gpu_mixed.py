@@ -79,3 +79,51 @@ def test_mixed_mooneyrivlin_block_steps(oracle):
     MechSystemSolver(m, tol=1e-12, max_iter=20000).backwardEuler(wl.h, 5)
     xg, _ = m.getState()
     assert rel_err(xg, x) <= 1e-6, rel_err(xg, x)
+
+
+@pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex"])
+def test_refinement_recovers_fp64(name, cases):
+    """Refinement sweeps against the FP64 residual bring the mixed form's
+    positions to the plain FP64 result: the error falls by orders of
+    magnitude and the stats report the sweeps."""
+    wl = cases[name]
+    steps = 6
+    ref = wl.model(precision=L.PREC_FP64)
+    MechSystemSolver(ref, tol=1e-12).backwardEuler(wl.h, steps)
+    x64, _ = ref.getState()
+    errs = {}
+    for sweeps in (0, 2):
+        m = wl.model(precision=L.PREC_MIXED)
+        m.options = {L.OPT_REFINE: sweeps}
+        ms = MechSystemSolver(m, tol=1e-12)
+        ms.backwardEuler(wl.h, steps)
+        assert ms.stats.refinements == sweeps
+        x, _ = m.getState()
+        errs[sweeps] = rel_err(x - wl.rest, x64 - wl.rest)
+        m._invalidate()
+    assert errs[2] <= 1e-9 and errs[2] <= 1e-2 * errs[0], errs
+
+
+def test_refinement_in_a_pack_equals_alone(b200):
+    """A refined pack (strided split, masked models) gives each active model
+    its refined result alone and leaves the masked ones untouched."""
+    from artisynth_core_b200.femmodel import FemPack
+    bs = W.batched_beams(count=5, seed=6)
+    for b in bs:
+        b.cells = (min(b.cells[0], 8), b.cells[1], b.cells[2])
+        b.widths = (b.cells[0] * 0.05, b.widths[1], b.widths[2])
+        b.build_mesh()
+    pack = FemPack([b.model() for b in bs], precision=L.PREC_MIXED,
+                   options={L.OPT_REFINE: 2, L.OPT_PCG_SPLIT: L.SPLIT_STRIDED, L.OPT_PIECE_ROWS: 8})
+    mask = np.array([1, 0, 1, 1, 0], dtype=np.int32)
+    pack.setActive(mask)
+    pack.backwardEuler(bs[0].h, 3, tol=1e-12)
+    for i, (b, (x, v)) in enumerate(zip(bs, pack.getStates())):
+        if not mask[i]:
+            assert np.array_equal(x, b.rest) and not v.any()
+            continue
+        m = b.model(precision=L.PREC_MIXED)
+        m.options = {L.OPT_REFINE: 2}
+        MechSystemSolver(m, tol=1e-12).backwardEuler(b.h, 3)
+        xa, _ = m.getState()
+        assert rel_err(x, xa) <= 1e-9, (i, rel_err(x, xa))
