@@ -3,8 +3,8 @@
 What it chooses, by timing real BackwardEuler steps on the device:
   * ROW_LANES  -- lanes per block row in the PCG SpMV (4, 8, 16, 32): the
                   trade between rows in flight per warp and blocks per lane;
-  * ELEM_TILE  -- elements per CTA of the non-linear element kernels (the
-                  large or the half tile);
+  * ELEM_TILE  -- the non-linear element kernel: one thread per tetrahedron,
+                  or the shared-memory staged kernel with its large or half tile;
   * PIECE_ROWS -- (packs with the strided split) rows per piece, i.e. how
                   finely the models are dealt over the CTAs, which sets the
                   PCG schedule of the pack.
@@ -28,7 +28,7 @@ import numpy as np
 from . import _lib as L
 
 LANES = (4, 8, 16, 32)
-TILES = (1, 2)
+TILES = (0, 1, 2)
 PIECE_ROWS = (32, 64, 128)
 
 

@@ -904,8 +904,9 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       return B200FEM_OK;
     case B200FEM_OPT_ELEM_TILE:
       if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "ELEM_TILE must be 0, 1 or 2");
-      if ((value == 2) != eng.elem_tile_small) {
+      if ((value == 2) != eng.elem_tile_small || (value >= 1) != eng.elem_staged) {
         eng.elem_tile_small = value == 2;
+        eng.elem_staged = value >= 1 && value <= 2;
         eng.step_exec_max_iter = -1;  // recapture: another kernel instance
       }
       return B200FEM_OK;
@@ -939,7 +940,7 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_PCG_CTAS: *value = eng.built ? eng.pcg_grid : eng.opt_ctas; break;
     case B200FEM_OPT_PIECE_ROWS: *value = eng.opt_piece_rows; break;
     case B200FEM_OPT_WARM_START: *value = eng.opt_warm_start; break;
-    case B200FEM_OPT_ELEM_TILE: *value = eng.elem_tile_small ? 2 : 1; break;
+    case B200FEM_OPT_ELEM_TILE: *value = eng.elem_staged ? (eng.elem_tile_small ? 2 : 1) : 0; break;
     case B200FEM_OPT_FUSED_ASSEMBLY: *value = eng.built ? (eng.fused ? 1 : 0) : eng.opt_fused; break;
     case B200FEM_OPT_REFINE: *value = (eng.built && !eng.refine_ok) ? 0 : eng.opt_refine; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");

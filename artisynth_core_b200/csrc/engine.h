@@ -194,6 +194,7 @@ struct Engine {
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
   int opt_warm_start = 1;  // 0 previous velocity, 1 extrapolated from the last two
   bool elem_tile_small = false;  // element kernels: the small tile of each material
+  bool elem_staged = false;      // tets: the shared-memory staged kernel instead of one thread per element
   bool fused = false;            // BackwardEuler assembly on the fused row-chunk path
   int fused_chunks = 0, fused_emax = 0;
   int opt_fused = 0;             // 1: fused assembly where supported

@@ -1,19 +1,27 @@
 // kernels.cu -- sm_100a kernels of the FEM hot path:
 //
-//   elem_*_kernel     element-group kernels: node coordinates staged through
-//                     shared memory, per-integration-point kinematics and
-//                     material (F, sigma, D), then one thread per element node
-//                     pair forms the 3x3 tangent block and one per node the
-//                     stress force (FemModel3d.computeStressAndStiffness,
+//   elem_tet_kernel   tetrahedra, non-linear materials: one thread per
+//                     element in registers -- kinematics, stress and nodal
+//                     forces in FP64, the ten upper pair blocks in the
+//                     storage precision, warp-staged contiguous stores
+//   elem_nonlinear_kernel / elem_linear_kernel
+//                     hexahedra (and tets on request): coordinates staged
+//                     through shared memory, per-integration-point kinematics
+//                     and material (F, sigma, D), then one thread per element
+//                     node pair forms the 3x3 tangent block and one per node
+//                     the stress force (FemModel3d.computeStressAndStiffness,
 //                     FemModel3d.java:3333-3666)
-//   gather_kernel     deterministic, atomic-free scatter: every 3x3 block
-//                     entry sums its precomputed contribution list (element
-//                     pair, transposed flag) in element order and applies the
+//   elem_force_kernel FP64 nodal forces of the mixed form (hexes)
+//   gather_block_kernel
+//                     deterministic, atomic-free scatter: every 3x3 block sums
+//                     its precomputed contribution list (element pair,
+//                     transposed flag) in element order and applies the
 //                     BackwardEuler coefficients S = (h^2+h beta)K + (1+h alpha)M
+//   fused_block_kernel  optional fused row-chunk assembly (no element blocks
+//                     in HBM)
 //   rows_kernel       nodal internal force gather and BackwardEuler RHS
-//   pcg_kernel        persistent cooperative block-Jacobi PCG with
-//                     deterministic two-level dot products and a bounded grid
-//                     barrier; writes v1 and x1 = x0 + h v1 at the end
+//   elem_kv_kernel, refine_*  iterative refinement of the mixed form
+//   (pcg_kernel lives in pcg.cu)
 //
 // All reductions are in a fixed order: results are bit-reproducible run to run.
 #include <cuda_runtime.h>
@@ -111,6 +119,20 @@ __device__ __forceinline__ long long dbl_order(double v) {
   return i >= 0 ? i : (i ^ 0x7fffffffffffffffll);
 }
 
+// Inverted-element count and smallest detJ, aggregated over a warp before
+// the atomics: every element thread updating the same two words would
+// serialise on them.  All 32 lanes of the warp call it.
+__device__ __forceinline__ void warp_record_det(int* flags, long long* mindet, double det, int inv) {
+  const int tot = __reduce_add_sync(0xffffffffu, inv);
+  double d = det;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) d = fmin(d, __shfl_xor_sync(0xffffffffu, d, off));
+  if ((threadIdx.x & 31) == 0) {
+    if (tot) atomicAdd(&flags[1], tot);
+    if (d < 1.0e300) atomicMin(mindet, dbl_order(d));
+  }
+}
+
 struct ElemArgs;
 __device__ bool block_inactive(const ElemArgs& a, int ebase, int epb);
 
@@ -199,6 +221,8 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
   }
   __syncthreads();
   // stage 1: one thread per (element, integration point)
+  double mydet = 1.0e300;
+  int myinv = 0;
   for (int t = threadIdx.x; t < EPB * NIP; t += blockDim.x) {
     int el = t / NIP, k = t % NIP, e = ebase + el;
     if (e >= a.e1) continue;
@@ -228,10 +252,8 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
     matmul3(F, J, iJ0);
     T detF = det3(F);
     T detJ = invert3(invJ, J);
-    if (!(detJ > T(0))) {
-      atomicAdd(&a.flags[1], 1);
-    }
-    atomicMin(a.mindet, dbl_order((double)detJ));
+    myinv += !(detJ > T(0));
+    mydet = fmin(mydet, (double)detJ);
     const T w = TYPE == B200FEM_ELEM_TET ? T(1.0 / 6.0) : T(1);
     T dv = detJ * w;
     sdv[t] = dv;
@@ -265,6 +287,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
       mooneyrivlin_point<T>(ssig[t], sD[t], mpt, F, detF, pr);
     }
   }
+  warp_record_det(a.flags, a.mindet, mydet, myinv);
   __syncthreads();
   // stage 2: one thread per element pair block, then per node force (the
   // FP32 form leaves the forces to the FP64 force kernel)
@@ -428,62 +451,93 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
 }
 
 // ---------------------------------------------------------------------------
-// block gather: one thread per block entry
+// block gather: one thread per block (all nine entries), the warp's 32
+// consecutive blocks staged in shared memory and stored as contiguous lines.
+// Same sums in the same order as one thread per entry: the contribution list
+// in element order, then the NODAL dilational triples node-ascending.
 // ---------------------------------------------------------------------------
 template <typename TK, typename TO>
-__global__ void gather_kernel(long long nnzb, const int* __restrict__ cptr, const int* __restrict__ cidx,
-                              const TK* __restrict__ elemK, const int* __restrict__ blk_row,
-                              const int* __restrict__ blk_diag, const int* __restrict__ row_model,
-                              const int* __restrict__ act_node, const double* __restrict__ mass,
-                              const double* __restrict__ step, int mode, TO* __restrict__ out,
-                              const int* __restrict__ dptr, const int* __restrict__ didx,
-                              const double* __restrict__ divblk, const double* __restrict__ node_kp,
-                              const int* __restrict__ active) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nnzb * 9) return;
-  long long p = t / 9;
-  if (active && !active[row_model[blk_row[p]]]) return;  // model left out of this step
-  int q = (int)(t - p * 9);
-  int qt = (q % 3) * 3 + q / 3;
-  double s = 0;
-  const int c0 = cptr[p], c1 = cptr[p + 1];
-  // four contributions per round (independent loads), summed in list order
-  for (int c = c0; c < c1; c += 4) {
-    int code[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) code[k] = (c + k < c1) ? cidx[c + k] : -1;
-    double v[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      v[k] = code[k] >= 0 ? (double)elemK[(size_t)(code[k] >> 1) * 9 + ((code[k] & 1) ? qt : q)] : 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) s += v[k];
+__global__ void __launch_bounds__(256) gather_block_kernel(
+    long long nnzb, const int* __restrict__ cptr, const int* __restrict__ cidx, const TK* __restrict__ elemK,
+    const int* __restrict__ blk_row, const int* __restrict__ blk_diag, const int* __restrict__ row_model,
+    const int* __restrict__ act_node, const double* __restrict__ mass, const double* __restrict__ step, int mode,
+    TO* __restrict__ out, const int* __restrict__ dptr, const int* __restrict__ didx,
+    const double* __restrict__ divblk, const double* __restrict__ node_kp, const int* __restrict__ active) {
+  __shared__ TO stage[8][32 * 9];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long wbase = ((long long)blockIdx.x * 8 + warp) * 32;
+  const long long p = wbase + lane;
+  TO* my = stage[warp] + lane * 9;
+  bool live = p < nnzb;
+  int row = 0;
+  if (live) {
+    row = blk_row[p];
+    if (active && !active[row_model[row]]) live = false;
   }
-  if (dptr) {
-    // NODAL dilational term sum_n kp_n divBlk(n,i) divBlk(n,j)^T, n ascending
-    // (FemModel3d.computeNodalIncompressibility, FemModel3d.java:2632-2669)
-    const int r = q / 3, c = q % 3;
-    const int d1 = dptr[p + 1];
-    double sd = 0;
-    for (int t = dptr[p]; t < d1; t++) {
-      const int* tr = didx + 3 * (size_t)t;
-      sd += node_kp[tr[2]] * divblk[3 * (size_t)tr[0] + r] * divblk[3 * (size_t)tr[1] + c];
+  if (live) {
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int c1 = cptr[p + 1];
+    for (int c = cptr[p]; c < c1; c++) {
+      const int code = cidx[c];
+      const TK* B = elemK + (size_t)(code >> 1) * 9;
+      double b[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+      if (code & 1) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) s[3 * i + j] += b[3 * j + i];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; k++) s[k] += b[k];
+      }
     }
-    s += sd;
+    if (dptr) {
+      // NODAL dilational term sum_n kp_n divBlk(n,i) divBlk(n,j)^T, n ascending
+      // (FemModel3d.computeNodalIncompressibility, FemModel3d.java:2632-2669)
+      double sd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      const int d1 = dptr[p + 1];
+      for (int t = dptr[p]; t < d1; t++) {
+        const int* tr = didx + 3 * (size_t)t;
+        const double kp = node_kp[tr[2]];
+        const double* di = divblk + 3 * (size_t)tr[0];
+        const double* dj = divblk + 3 * (size_t)tr[1];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) sd[3 * r + c] += kp * di[r] * dj[c];
+      }
+#pragma unroll
+      for (int k = 0; k < 9; k++) s[k] += sd[k];
+    }
+    if (mode == 0) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) my[k] = (TO)s[k];  // plain stiffness K
+    } else {
+      const double* sp = step + (size_t)row_model[row] * 8;
+      const double h = sp[0], al = sp[1], be = sp[2];
+      // addPosJacobian (h^2 K), addVelJacobian (h beta K + h alpha M),
+      // addActiveMassMatrix (M)  (MechSystemSolver.java:2277,2312,2334)
+      const double cm = p == blk_diag[row] ? (1.0 + h * al) * mass[act_node[row]] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        double val = (h * h + h * be) * s[k];
+        if (k % 4 == 0) val += cm;
+        my[k] = (TO)val;
+      }
+    }
   }
-  double val;
-  if (mode == 0) {
-    val = (double)s;  // plain stiffness K
-  } else {
-    int row = blk_row[p];
-    const double* sp = step + (size_t)row_model[row] * 8;
-    double h = sp[0], al = sp[1], be = sp[2];
-    // addPosJacobian (h^2 K), addVelJacobian (h beta K + h alpha M),
-    // addActiveMassMatrix (M)  (MechSystemSolver.java:2277,2312,2334)
-    val = (h * h + h * be) * (double)s;
-    if (p == blk_diag[row] && (q == 0 || q == 4 || q == 8)) val += (1.0 + h * al) * mass[act_node[row]];
+  __syncwarp();
+  // contiguous stores of the warp's blocks (blocks of models left out stay)
+  const long long nv = nnzb - wbase < 32 ? nnzb - wbase : 32;
+  if (nv <= 0) return;
+  TO* o = out + (size_t)wbase * 9;
+  for (int i = lane; i < nv * 9; i += 32) {
+    const long long q = wbase + i / 9;
+    if (active && !active[row_model[blk_row[q]]]) continue;
+    o[i] = stage[warp][i];
   }
-  out[t] = (TO)val;
 }
 
 // ---------------------------------------------------------------------------
@@ -641,7 +695,8 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
   const int k = (int)(t % NIP);
   bool live = e < a.e1;
   if (live && a.active && !a.active[a.elem_model[e]]) live = false;
-  if (NIP == 1 && !live) return;  // tets: no cross-lane reduction follows
+  double mydet = 1.0e300;
+  int myinv = 0;
   double fl[NEN][3];
 #pragma unroll
   for (int n = 0; n < NEN; n++) fl[n][0] = fl[n][1] = fl[n][2] = 0;
@@ -667,10 +722,8 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
     const double detF = det3(F);
     const double detJ = invert3(invJ, J);
     const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
-    if (a.det_stats) {
-      if (!(detJ > 0.0)) atomicAdd(&a.flags[1], 1);
-      atomicMin(a.mindet, dbl_order(detJ));
-    }
+    myinv = !(detJ > 0.0);
+    mydet = detJ;
     const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
     double sig[6];
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
@@ -700,6 +753,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
       add_stress_force(fl[n], g, sig, dv);
     }
   }
+  if (a.det_stats) warp_record_det(a.flags, a.mindet, mydet, myinv);
   if constexpr (NIP > 1) {
     // sum the points of one element: lanes 8q..8q+7 hold its 8 points
 #pragma unroll
@@ -710,11 +764,147 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
         for (int off = 4; off > 0; off >>= 1) fl[n][c] += __shfl_xor_sync(0xffffffffu, fl[n][c], off);
     if (!live || k != 0) return;
   }
+  if (!live) return;
   double* out = (double*)a.elemF + (size_t)e * NEN * 3;
 #pragma unroll
   for (int n = 0; n < NEN; n++)
 #pragma unroll
     for (int c = 0; c < 3; c++) out[3 * n + c] = fl[n][c];
+}
+
+// ---------------------------------------------------------------------------
+// Tetrahedra, non-linear materials: one thread per element, everything in
+// registers.  Kinematics, stress and the nodal forces in FP64 (the force
+// residual); the ten upper pair blocks B_a^T D B_b + (g_a^T sigma g_b) I in
+// the storage precision T.  A warp stages its 32 element records in shared
+// memory and writes them as contiguous lines (records of consecutive
+// elements are adjacent in elemK / elemF).
+// ---------------------------------------------------------------------------
+// warps per CTA of elem_tet_kernel: the staging buffers (32 element records
+// per warp) stay within the static shared-memory limit
+template <typename T>
+__host__ __device__ constexpr int tet_wpb() { return sizeof(T) == 8 ? 1 : 2; }
+
+template <int MAT, bool NODAL, typename T>
+__global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
+  constexpr int NPAIR = 10, KW = NPAIR * 9, FW = 12, WPB = tet_wpb<T>();
+  __shared__ T sk[WPB][32 * KW];
+  __shared__ double sf[WPB][32 * FW];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wbase = a.e0 + (blockIdx.x * WPB + warp) * 32;
+  const int e = wbase + lane;
+  bool live = e < a.e1;
+  if (live && a.active && !a.active[a.elem_model[e]]) live = false;
+  T* kout = sk[warp] + lane * KW;
+  double* fout = sf[warp] + lane * FW;
+  double mydet = 1.0e300;
+  int myinv = 0;
+  if (live) {
+    const int* nodes = a.conn + (size_t)e * 4;
+    int nd[4];
+#pragma unroll
+    for (int n = 0; n < 4; n++) nd[n] = nodes[n];
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      const double g0 = c_tet_gns[3 * n], g1 = c_tet_gns[3 * n + 1], g2 = c_tet_gns[3 * n + 2];
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const double xr = a.x[3 * (size_t)nd[n] + r];
+        J[3 * r] += xr * g0;
+        J[3 * r + 1] += xr * g1;
+        J[3 * r + 2] += xr * g2;
+      }
+    }
+    double iJ0[9], F[9], invJ[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) iJ0[i] = a.invJ0[(size_t)e * 9 + i];
+    matmul3(F, J, iJ0);
+    const double detF = det3(F);
+    const double detJ = invert3(invJ, J);
+    myinv = !(detJ > 0.0);
+    mydet = detJ;
+    const double dv = detJ * (1.0 / 6.0);
+    double g[4][3];
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      const double g0 = c_tet_gns[3 * n], g1 = c_tet_gns[3 * n + 1], g2 = c_tet_gns[3 * n + 2];
+#pragma unroll
+      for (int c = 0; c < 3; c++) g[n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
+    }
+    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    double sig[6];
+    T Dt[MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36];
+    if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
+      double ca, cb;
+      neohookean_point<double>(sig, &ca, &cb, mp[0], mp[1], F, detF);
+      Dt[0] = (T)ca;
+      Dt[1] = (T)cb;
+    } else {
+      double pr = 0;
+      if constexpr (NODAL) pr = 0.25 * (a.node_p[nd[0]] + a.node_p[nd[1]] + a.node_p[nd[2]] + a.node_p[nd[3]]);
+      double D[36];
+      mooneyrivlin_point<double>(sig, D, mp, F, detF, pr);
+#pragma unroll
+      for (int i = 0; i < 36; i++) Dt[i] = (T)D[i];
+    }
+    // nodal forces (FP64)
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      double f[3] = {0, 0, 0};
+      add_stress_force(f, g[n], sig, dv);
+      fout[3 * n] = f[0];
+      fout[3 * n + 1] = f[1];
+      fout[3 * n + 2] = f[2];
+    }
+    // pair blocks (storage precision)
+    T gt[4][3], st[6];
+    const T dvt = (T)dv;
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) gt[n][c] = (T)g[n][c];
+#pragma unroll
+    for (int i = 0; i < 6; i++) st[i] = (T)sig[i];
+    int w = 0;
+#pragma unroll
+    for (int ia = 0; ia < 4; ia++)
+#pragma unroll
+      for (int ib = ia; ib < 4; ib++, w++) {
+        T K[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) K[i] = T(0);
+        if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) add_bdb_iso(K, gt[ia], Dt[0], Dt[1], gt[ib], dvt);
+        else add_bdb(K, gt[ia], Dt, gt[ib], dvt);
+        add_geometric(K, gt[ia], st, gt[ib], dvt);
+#pragma unroll
+        for (int i = 0; i < 9; i++) kout[9 * w + i] = K[i];
+      }
+  }
+  warp_record_det(a.flags, a.mindet, mydet, myinv);
+  __syncwarp();
+  // contiguous stores of the warp's element records
+  const int nv = min(32, a.e1 - wbase);
+  if (nv <= 0) return;
+  T* K = (T*)a.elemK + (size_t)wbase * KW;
+  for (int i = lane; i < nv * KW; i += 32) {
+    const int el = i / KW;
+    if (a.active && !a.active[a.elem_model[wbase + el]]) continue;
+    K[i] = sk[warp][i];
+  }
+  double* Fo = (double*)a.elemF + (size_t)wbase * FW;
+  for (int i = lane; i < nv * FW; i += 32) {
+    const int el = i / FW;
+    if (a.active && !a.active[a.elem_model[wbase + el]]) continue;
+    Fo[i] = sf[warp][i];
+  }
+}
+
+template <int MAT, bool NODAL, typename T>
+static cudaError_t launch_tet(const ElemArgs& a, int ne, cudaStream_t st) {
+  constexpr int TPB = 32 * tet_wpb<T>();
+  elem_tet_kernel<MAT, NODAL, T><<<(ne + TPB - 1) / TPB, TPB, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 template <int TYPE, int MAT, bool NODAL>
@@ -946,6 +1136,12 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   }
   const bool small = eng.elem_tile_small;
   cudaError_t e;
+  if (TYPE == B200FEM_ELEM_TET && !eng.elem_staged) {
+    // one thread per tetrahedron (FP64 forces in the same pass)
+    if (g.mat_kind == NH) return launch_tet<NH, false, T>(a, ne, st);
+    if (g.nodal) return launch_tet<MR, true, T>(a, ne, st);
+    return launch_tet<MR, false, T>(a, ne, st);
+  }
   if (g.mat_kind == NH) {
     e = small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
     if (e == cudaSuccess && fp32) e = launch_force<TYPE, NH, false>(a, ne, st);
@@ -1410,21 +1606,20 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
       e = fp32 ? launch_group<B200FEM_ELEM_HEX, float>(eng, g, true) : launch_group<B200FEM_ELEM_HEX, double>(eng, g, false);
     if (e != cudaSuccess) return e;
   }
-  long long n9 = d.nnzb * 9;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
-  int threads = 256;
-  unsigned blocks = (unsigned)((n9 + threads - 1) / threads);
+  // one thread per block, 8 warps of 32 blocks per CTA
+  const unsigned blocks = (unsigned)((d.nnzb + 255) / 256);
   if (fp32) {
     if (want_K)
-      gather_kernel<float, double><<<blocks, threads, 0, eng.stream>>>(
+      gather_block_kernel<float, double><<<blocks, 256, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
           d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
     else
-      gather_kernel<float, float><<<blocks, threads, 0, eng.stream>>>(
+      gather_block_kernel<float, float><<<blocks, 256, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
           d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
   } else {
-    gather_kernel<double, double><<<blocks, threads, 0, eng.stream>>>(
+    gather_block_kernel<double, double><<<blocks, 256, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
         d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
   }

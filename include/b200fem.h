@@ -218,9 +218,11 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 #define B200FEM_OPT_WARM_START 5 /* PCG start: 0 the previous velocity; 1 (default) its linear
                                     extrapolation 2 v_n - v_(n-1) over the last two steps
                                     (may be changed after the build) */
-#define B200FEM_OPT_ELEM_TILE 6  /* elements per CTA of the non-linear element kernels: 0 auto,
-                                    1 large tile (tet 256 / hex 32 NeoHookean, 128 / 16
-                                    MooneyRivlin), 2 half of it (may be changed after the build) */
+#define B200FEM_OPT_ELEM_TILE 6  /* non-linear element kernels: 0 (default) tets one thread per
+                                    element in registers, hexes the staged kernel's large tile;
+                                    1 the shared-memory staged kernel with its large tile (tet 256 /
+                                    hex 32 NeoHookean, 128 / 16 MooneyRivlin); 2 with half of it
+                                    (may be changed after the build) */
 #define B200FEM_OPT_REFINE 8     /* refinement sweeps of the mixed form (0..4, default 0): each
                                     forms the FP64 residual b - S64 v matrix-free from the
                                     elements' FP64 tangents, solves the correction with the FP32

@@ -42,7 +42,7 @@ class FakePack:
     def lastTiming(self):
         lanes = self.opts[L.OPT_ROW_LANES]
         pcg = {4: 3.0, 8: 2.0, 16: 4.0, 32: 5.0}[lanes] * (1.0 if self.opts[L.OPT_PIECE_ROWS] == 32 else 1.5)
-        asm = 1.0 if self.opts[L.OPT_ELEM_TILE] == 2 else 2.0
+        asm = {0: 1.5, 1: 2.0, 2: 1.0}[self.opts[L.OPT_ELEM_TILE]]
         return asm, pcg * self.stats.iterations
 
     def close(self):

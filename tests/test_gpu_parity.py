@@ -274,3 +274,23 @@ def test_fused_assembly_matches_gather(name, precision, cases):
     assert rel_err(xa, xb) <= (1e-11 if precision == L.PREC_FP64 else 1e-7), rel_err(xa, xb)
     assert ia == ib == 0
     assert abs(da - db) <= 1e-5 * abs(db)
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("name", ["neohookean_tet", "mooneyrivlin_tet_off", "mooneyrivlin_tet_nodal"])
+def test_tet_kernels_agree(name, precision, cases):
+    """The one-thread-per-tetrahedron kernel and the shared-memory staged
+    kernel give the same steps (same formulas; the former keeps kinematics
+    and stress in FP64 in both forms)."""
+    wl = cases[name]
+    xs = []
+    for tile in (0, 1):
+        m = _gpu_model(wl)
+        m.precision = precision
+        m.options = {L.OPT_ELEM_TILE: tile}
+        ms = MechSystemSolver(m, tol=1e-13)
+        ms.backwardEuler(wl.h, 4)
+        xs.append(m.getState()[0])
+        assert ms.stats.num_inverted == 0
+        m._invalidate()
+    assert rel_err(xs[0], xs[1]) <= (1e-11 if precision == L.PREC_FP64 else 1e-6), rel_err(xs[0], xs[1])
