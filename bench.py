@@ -389,6 +389,91 @@ def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=
     return out
 
 
+def run_batched_sharded(dist, rank, world, dev, steps=20, tol=1e-10):
+    """The batched leg on `world` GPUs: the 256 models dealt to ranks by LPT
+    on their element counts (strong scaling: the total work is fixed), one
+    tuned pack per rank, no collective on the data path; time = the slowest
+    rank's."""
+    import tempfile
+    import torch
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200 import autotune, shard
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.femmodel import FemPack
+    bs = W.batched_beams()
+    for b in bs:
+        b.build_mesh()
+    mine = shard.lpt_partition([b.conn.shape[0] for b in bs], world)[rank]
+    local = [bs[i] for i in mine]
+    models = [b.model(device=dev) for b in local]
+
+    def make(opts):
+        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options=opts)
+        p.engine()
+        return p
+
+    with tempfile.TemporaryDirectory() as td:
+        pack, tuned, _ = autotune.tune_pack(make, models, L.PREC_MIXED, bs[0].h, tol,
+                                            cache=autotune.TuneCache(os.path.join(td, "tune.json")))
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pack.backwardEuler(bs[0].h, 1, tol=tol)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    pack.close()
+    slowest = shard.max_over_ranks(dist, wall)
+    per_rank = shard.gather_to_root(dist, {"models": len(mine), "tets": int(sum(b.conn.shape[0] for b in local)),
+                                           "wall_s": wall})
+    if rank != 0:
+        return None
+    return {"workload": "256 uneven NeoHookean tet beams (seed 3), 20 steps, dealt to ranks by LPT on elements",
+            "ranks": world, "scaling": "strong", "steps": steps, "tol": tol,
+            "model_steps_per_s": len(bs) * steps / slowest, "per_rank": per_rank}
+
+
+def run_served_sharded(dist, rank, world, dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=10,
+                       tol=1e-6, drain_s=30.0):
+    """The served leg on `world` GPUs: pool models dealt to ranks by LPT;
+    every rank replays the same arrival stream and serves the requests for
+    its own models; latencies gathered to rank 0."""
+    import tempfile
+    import numpy as np
+    from artisynth_core_b200 import autotune, shard
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.serve import FemServer, poisson_arrivals, run_stream
+    pool = W.batched_beams(count=pool_size, seed=4, large_frac=0.1)
+    for w in pool:
+        w.build_mesh()
+    mine = shard.lpt_partition([w.conn.shape[0] for w in pool], world)[rank]
+    local_of = {m: i for i, m in enumerate(mine)}
+    td = tempfile.TemporaryDirectory()
+    srv = FemServer([pool[m] for m in mine], budget=60e9, tol=tol, device=dev, autotune=True,
+                    tune_cache=autotune.TuneCache(os.path.join(td.name, "tune.json")))
+    srv.preload()
+    times, models = poisson_arrivals(rate, seconds, pool_size, seed=4)
+    keep = np.array([int(m) in local_of for m in models], dtype=bool)
+    arr = (times[keep], np.array([local_of[int(m)] for m in models[keep]], dtype=np.int64))
+    dist.barrier()
+    out = run_stream(srv, arr, steps_per_request, drain_s=drain_s)
+    lat = [r.latency * 1e3 for r in srv.done]
+    srv.close()
+    td.cleanup()
+    gathered = shard.gather_to_root(dist, {"lat": lat, "out": out})
+    if rank != 0:
+        return None
+    alllat = np.concatenate([np.asarray(g["lat"]) for g in gathered]) if gathered else np.zeros(0)
+    wall = max(g["out"]["wall_s"] for g in gathered)
+    steps = sum(g["out"]["model_steps_per_s"] * g["out"]["wall_s"] for g in gathered)
+    return {"workload": f"Poisson {rate:.0f} req/s (seed 4), {seconds:.0f} s, pool of {pool_size} dealt to ranks by LPT",
+            "ranks": world, "requests": int(sum(g["out"]["requests"] for g in gathered)),
+            "completed": int(len(alllat)), "incomplete": int(sum(g["out"]["incomplete"] for g in gathered)),
+            "p50_ms": float(np.percentile(alllat, 50)) if len(alllat) else None,
+            "p99_ms": float(np.percentile(alllat, 99)) if len(alllat) else None,
+            "model_steps_per_s": steps / wall, "tol": tol}
+
+
 def run_b200(args):
     import torch
     dist, rank, world, local = dist_setup(args.gpus)
@@ -449,6 +534,13 @@ def run_b200(args):
     e2e_val = world * 1e3 / float(e2e_ms.item())
     state_bytes = 2 * 3 * wl.rest.shape[0] * 8
 
+    # multi-GPU forms of the batched and served legs (every rank takes part)
+    batched_sharded = served_sharded = None
+    if world > 1 and not args.no_batched:
+        batched_sharded = run_batched_sharded(dist, rank, world, dev, steps=args.batch_steps, tol=args.batch_tol)
+    if world > 1 and args.served_seconds > 0:
+        served_sharded = run_served_sharded(dist, rank, world, dev, seconds=args.served_seconds, tol=args.served_tol)
+
     if rank == 0:
         asm_b, it_b = algorithmic_bytes(wl, sz["nnzb"], sz["n_active"])
         mean_it = float(np.mean(iters))
@@ -466,6 +558,10 @@ def run_b200(args):
             except Exception:
                 traffic = None
         batched = served = None
+        if world > 1 and not args.no_batched:
+            batched = batched_sharded
+        if world > 1 and args.served_seconds > 0:
+            served = served_sharded
         if world == 1 and not args.no_batched:
             with ClockSampler(dev) as c:
                 batched = run_batched(dev, steps=args.batch_steps, tol=args.batch_tol, tune=not args.no_tune)
