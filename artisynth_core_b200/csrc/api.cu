@@ -538,6 +538,12 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.blk_row, blk_row));
   CK(upload(eng, &d.contrib_ptr, cptr));
   CK(upload(eng, &d.contrib_idx, cidx));
+  {
+    std::vector<int> mirror(NB);
+    for (int r = 0; r < R; r++)
+      for (int p = rowptr[r]; p < rowptr[r + 1]; p++) mirror[p] = block_of(col[p], r);
+    CK(upload(eng, &d.blk_mirror, mirror));
+  }
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));
   if (eng.fused) {

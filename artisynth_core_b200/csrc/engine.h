@@ -139,6 +139,7 @@ struct DevPack {
   int* chunk_eptr = nullptr;   // chunks+1
   int* chunk_elem = nullptr;
   int* contrib_loc = nullptr;  // parallel to contrib_idx
+  int* blk_mirror = nullptr;   // nnzb: the block at the transposed position
   // refinement sweeps: FP64 residual, correction, its PCG results
   double* rref = nullptr;
   double* dsol = nullptr;

@@ -451,10 +451,14 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
 }
 
 // ---------------------------------------------------------------------------
-// block gather: one thread per block (all nine entries), the warp's 32
+// block gather: one thread per upper block (all nine entries), the warp's 32
 // consecutive blocks staged in shared memory and stored as contiguous lines.
 // Same sums in the same order as one thread per entry: the contribution list
-// in element order, then the NODAL dilational triples node-ascending.
+// in element order, then the NODAL dilational triples node-ascending.  The
+// matrix is symmetric: a lower block's list holds the same contributions in
+// the same order, transposed, so each upper block also writes its transpose
+// to the mirror position (FemModel3d.java:3003-3026) and lower blocks are
+// not summed.
 // ---------------------------------------------------------------------------
 template <typename TK, typename TO>
 __global__ void __launch_bounds__(256) gather_block_kernel(
@@ -462,19 +466,22 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
     const int* __restrict__ blk_row, const int* __restrict__ blk_diag, const int* __restrict__ row_model,
     const int* __restrict__ act_node, const double* __restrict__ mass, const double* __restrict__ step, int mode,
     TO* __restrict__ out, const int* __restrict__ dptr, const int* __restrict__ didx,
-    const double* __restrict__ divblk, const double* __restrict__ node_kp, const int* __restrict__ active) {
+    const double* __restrict__ divblk, const double* __restrict__ node_kp, const int* __restrict__ active,
+    const int* __restrict__ mirror) {
   __shared__ TO stage[8][32 * 9];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long wbase = ((long long)blockIdx.x * 8 + warp) * 32;
   const long long p = wbase + lane;
   TO* my = stage[warp] + lane * 9;
   bool live = p < nnzb;
-  int row = 0;
+  int row = 0, mp = -1;
   if (live) {
     row = blk_row[p];
+    mp = mirror[p];
     if (active && !active[row_model[row]]) live = false;
   }
-  if (live) {
+  const bool lower = mp >= 0 && mp < p;  // written by its upper block
+  if (live && !lower) {
     double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int c1 = cptr[p + 1];
     for (int c = cptr[p]; c < c1; c++) {
@@ -514,6 +521,13 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
     if (mode == 0) {
 #pragma unroll
       for (int k = 0; k < 9; k++) my[k] = (TO)s[k];  // plain stiffness K
+      if (mp != p) {
+        TO* t = out + (size_t)mp * 9;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) t[3 * i + j] = (TO)s[3 * j + i];
+      }
     } else {
       const double* sp = step + (size_t)row_model[row] * 8;
       const double h = sp[0], al = sp[1], be = sp[2];
@@ -526,6 +540,14 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
         if (k % 4 == 0) val += cm;
         my[k] = (TO)val;
       }
+      if (mp != p) {
+        // off-diagonal: no mass term; the mirror is the transpose
+        TO* t = out + (size_t)mp * 9;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) t[3 * i + j] = my[3 * j + i];
+      }
     }
   }
   __syncwarp();
@@ -536,6 +558,8 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
   for (int i = lane; i < nv * 9; i += 32) {
     const long long q = wbase + i / 9;
     if (active && !active[row_model[blk_row[q]]]) continue;
+    const int mq = mirror[q];
+    if (mq >= 0 && mq < q) continue;  // lower block: written by its mirror
     o[i] = stage[warp][i];
   }
 }
@@ -1613,15 +1637,15 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
     if (want_K)
       gather_block_kernel<float, double><<<blocks, 256, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-          d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
+          d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror);
     else
       gather_block_kernel<float, float><<<blocks, 256, 0, eng.stream>>>(
           d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-          d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
+          d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror);
   } else {
     gather_block_kernel<double, double><<<blocks, 256, 0, eng.stream>>>(
         d.nnzb, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node, d.mass,
-        d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act);
+        d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror);
   }
   return cudaGetLastError();
 }
