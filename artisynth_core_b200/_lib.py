@@ -74,6 +74,15 @@ class Stats(ctypes.Structure):
     ]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("ticks", ctypes.c_longlong), ("model_steps", ctypes.c_longlong), ("slot_steps", ctypes.c_longlong),
+        ("builds", ctypes.c_longlong), ("evictions", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+        ("failed", ctypes.c_longlong), ("resident_bytes", ctypes.c_ulonglong), ("peak_bytes", ctypes.c_ulonglong),
+        ("pending", ctypes.c_int), ("resident_models", ctypes.c_int),
+    ]
+
+
 _lib = None
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -134,6 +143,20 @@ def lib():
         "b200fem_set_active_models": ([H, _ip], ctypes.c_int),
         "b200fem_memory_usage": ([H, ctypes.POINTER(ctypes.c_ulonglong)], ctypes.c_int),
         "b200fem_get_option": ([H, ctypes.c_int, _ip], ctypes.c_int),
+        "b200fem_server_create": ([ctypes.POINTER(Config), ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(StepParams)], H),
+        "b200fem_server_destroy": ([H], ctypes.c_int),
+        "b200fem_server_last_error": ([H], ctypes.c_char_p),
+        "b200fem_server_clock": ([H], ctypes.c_double),
+        "b200fem_server_set_option": ([H, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "b200fem_server_add_model": ([H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, ctypes.c_int,
+                                      _dp, ctypes.c_double, ctypes.c_int, _dp, _ip], ctypes.c_int),
+        "b200fem_server_submit": ([H, ctypes.c_int, ctypes.c_int, ctypes.c_double, _ip], ctypes.c_int),
+        "b200fem_server_preload": ([H], ctypes.c_int),
+        "b200fem_server_tick": ([H, _ip], ctypes.c_int),
+        "b200fem_server_poll": ([H, ctypes.c_int, _ip, _dp], ctypes.c_int),
+        "b200fem_server_get_state": ([H, ctypes.c_int, _dp, _dp], ctypes.c_int),
+        "b200fem_server_get_stats": ([H, ctypes.POINTER(ServerStats)], ctypes.c_int),
         "b200fem_pcg_solve_noalloc": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int, _vp,
                                        _ip, _dp], ctypes.c_int),
     }

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libb200fem.so")
-SOURCES = ["api.cu", "kernels.cu", "pcg.cu", "setup.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "pcg.cu", "setup.cpp", "serve.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -362,3 +362,137 @@ def run_stream(server: FemServer, arrivals, steps_per_request: int = 10, drain_s
         "gpu_step_s": st.step_s,
         "max_iterations": st.max_iterations,
     }
+
+
+class NativeServer:
+    """The same served form run by the library's native server
+    (b200fem_server_*, the entry points a Java host binds): admission,
+    eviction, ticks and request bookkeeping in C++; this class only forwards.
+    `options` (B200FEM_OPT_* -> value) apply to every pack it builds."""
+
+    def __init__(self, workloads, budget=60e9, precision=L.PREC_MIXED, pack_models=256, tol=1e-10,
+                 max_iter=20000, device=0, options=None):
+        import ctypes
+        self._c = ctypes
+        self.pool = list(workloads)
+        w0 = self.pool[0]
+        p = L.StepParams()
+        p.h = w0.h
+        p.alpha_m = w0.mass_damping
+        p.beta_k = w0.stiffness_damping
+        for i in range(3):
+            p.gravity[i] = w0.gravity[i]
+        p.tol = tol
+        p.max_iter = max_iter
+        cfg = L.Config()
+        cfg.device = device
+        cfg.precision = precision
+        self._lib = L.lib()
+        self.h = self._lib.b200fem_server_create(ctypes.byref(cfg), float(budget), int(pack_models), ctypes.byref(p))
+        if not self.h:
+            raise L.B200FemError(L.ERR_INVALID_ARG, "b200fem_server_create failed")
+        for k, v in (options or {}).items():
+            self._call("b200fem_server_set_option", int(k), int(v))
+        for w in self.pool:
+            if w.conn is None:
+                w.build_mesh()
+            m = w.model(precision=precision, device=device)
+            prm = np.zeros(8)
+            pp = m.material.params()
+            prm[: len(pp)] = pp
+            fext = None if m.fext is None else np.ascontiguousarray(m.fext.reshape(-1))
+            idx = ctypes.c_int()
+            self._call("b200fem_server_add_model", m.elem_type, m.numNodes(),
+                       L.dptr(np.ascontiguousarray(m.rest.reshape(-1))), m.numElements(),
+                       L.iptr(np.ascontiguousarray(m.conn.reshape(-1))), L.iptr(m.fixed), m.material.kind,
+                       L.dptr(prm), m.density, m.soft_incomp, L.dptr(fext), ctypes.byref(idx))
+
+    def _call(self, name, *args):
+        st = getattr(self._lib, name)(self.h, *args)
+        if st != 0:
+            raise L.B200FemError(st, (self._lib.b200fem_server_last_error(self.h) or b"").decode(errors="replace"))
+        return st
+
+    def clock(self) -> float:
+        return self._lib.b200fem_server_clock(self.h)
+
+    def submit(self, model: int, steps: int, t_arrive: float = -1.0) -> int:
+        rid = self._c.c_int()
+        self._call("b200fem_server_submit", int(model), int(steps), float(t_arrive), self._c.byref(rid))
+        return rid.value
+
+    def preload(self):
+        self._call("b200fem_server_preload")
+
+    def tick(self) -> int:
+        n = self._c.c_int()
+        self._call("b200fem_server_tick", self._c.byref(n))
+        return n.value
+
+    def poll(self, rid: int):
+        st, lat = self._c.c_int(), self._c.c_double()
+        self._call("b200fem_server_poll", int(rid), self._c.byref(st), self._c.byref(lat))
+        return st.value, lat.value
+
+    def state(self, model: int):
+        n = self.pool[model].rest.shape[0]
+        x, v = np.zeros(3 * n), np.zeros(3 * n)
+        self._call("b200fem_server_get_state", int(model), L.dptr(x), L.dptr(v))
+        return x.reshape(-1, 3), v.reshape(-1, 3)
+
+    def stats(self) -> dict:
+        s = L.ServerStats()
+        self._call("b200fem_server_get_stats", self._c.byref(s))
+        return {k: getattr(s, k) for k, _ in L.ServerStats._fields_}
+
+    def pending(self) -> int:
+        return self.stats()["pending"]
+
+    def close(self):
+        if self.h:
+            self._lib.b200fem_server_destroy(self.h)
+            self.h = None
+
+
+def run_stream_native(server: NativeServer, arrivals, steps_per_request: int = 10, drain_s: float = 30.0):
+    """run_stream for the native server: requests are submitted with their
+    scheduled arrival time on the server clock; latencies come from it."""
+    times, models = arrivals
+    t0 = server.clock()
+    nxt = 0
+    duration = float(times[-1]) if len(times) else 0.0
+    rids = []
+    pending = 0
+    while True:
+        now = server.clock() - t0
+        while nxt < len(times) and times[nxt] <= now:
+            rids.append(server.submit(int(models[nxt]), steps_per_request, t0 + float(times[nxt])))
+            nxt += 1
+            pending += 1
+        if nxt >= len(times) and server.pending() == 0:
+            break
+        if now > duration + drain_s:
+            break
+        if server.pending() == 0:
+            time.sleep(min(0.0005, max(0.0, float(times[nxt]) - now)))
+            continue
+        server.tick()
+    wall = server.clock() - t0
+    lat = []
+    for r in rids:
+        st, l = server.poll(r)
+        if st == 2:
+            lat.append(l * 1e3)
+    lat = np.array(lat)
+    s = server.stats()
+    done = len(lat)
+    return {
+        "requests": len(rids), "completed": done, "incomplete": len(rids) - done, "wall_s": wall,
+        "p50_ms": float(np.percentile(lat, 50)) if done else None,
+        "p99_ms": float(np.percentile(lat, 99)) if done else None,
+        "mean_ms": float(lat.mean()) if done else None,
+        "requests_per_s": done / wall if wall > 0 else 0.0,
+        "model_steps_per_s": s["model_steps"] / wall if wall > 0 else 0.0,
+        "ticks": s["ticks"], "slot_steps": s["slot_steps"], "builds": s["builds"], "evictions": s["evictions"],
+        "peak_bytes": s["peak_bytes"], "server": "native",
+    }

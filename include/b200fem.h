@@ -240,6 +240,52 @@ int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
 
+/* ---- served form: continuous-batching request server ---------------------
+   No counterpart in the reference (ArtiSynth steps one MechModel at a time).
+   The server keeps admitted models resident on the device in packs and
+   advances them in ticks: one tick is one BackwardEuler step of every
+   resident model with a pending request, all models of a pack in the same
+   launches; requests that arrive between ticks join at the next one, and a
+   model's requests run FIFO.  Admission is against budget_bytes of device
+   memory: idle packs are evicted (least recently used, states kept on the
+   host) to make room, and a model larger than the budget fails its requests.
+   Every pack steps with the parameters given at creation and the options set
+   with b200fem_server_set_option.  Times are seconds on the server's clock
+   (b200fem_server_clock).  Calls on one server are serialised. */
+typedef struct b200fem_server* b200fem_server_handle;
+typedef struct {
+  long long ticks, model_steps, slot_steps, builds, evictions, completed, failed;
+  unsigned long long resident_bytes, peak_bytes;
+  int pending;          /* requests not yet done */
+  int resident_models;
+} b200fem_server_stats;
+/* NULL on invalid arguments */
+b200fem_server_handle b200fem_server_create(const b200fem_config* cfg, double budget_bytes, int pack_models,
+                                            const b200fem_step_params* step);
+int b200fem_server_destroy(b200fem_server_handle s);
+const char* b200fem_server_last_error(b200fem_server_handle s);
+double b200fem_server_clock(b200fem_server_handle s);
+/* a B200FEM_OPT_* option for every pack the server builds */
+int b200fem_server_set_option(b200fem_server_handle s, int key, int value);
+/* a model of the pool (host copy; admitted on its first request or by preload);
+   params as b200fem_set_material (8 values), fext may be NULL */
+int b200fem_server_add_model(b200fem_server_handle s, int elem_type, int n_nodes, const double* rest_xyz,
+                             int n_elems, const int* conn, const int* fixed, int mat_kind,
+                             const double* params, double density, int incomp_method, const double* fext,
+                             int* model_id);
+/* a request of `steps` BackwardEuler steps of one model; t_arrive on the
+   server clock (a negative value: now) -- a caller replaying an arrival
+   stream passes the scheduled time so that queueing before the call counts */
+int b200fem_server_submit(b200fem_server_handle s, int model, int steps, double t_arrive, int* request_id);
+/* admit every pool model that fits the budget before any request */
+int b200fem_server_preload(b200fem_server_handle s);
+/* admission, then one step of every resident model with work */
+int b200fem_server_tick(b200fem_server_handle s, int* model_steps);
+/* state: 0 queued, 1 running, 2 done (latency = completion - arrival), -1 failed */
+int b200fem_server_poll(b200fem_server_handle s, int request_id, int* state, double* latency_s);
+int b200fem_server_get_state(b200fem_server_handle s, int model, double* x, double* v);
+int b200fem_server_get_stats(b200fem_server_handle s, b200fem_server_stats* out);
+
 /* ---- allocation-free solve ---------------------------------------------- */
 /* Size limits of b200fem_pcg_solve_noalloc: its scratch is one fixed device
    array (about 2.6 MB) sized for these limits. */

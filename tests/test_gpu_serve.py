@@ -110,3 +110,80 @@ def test_short_poisson_stream(b200):
     assert 0 < out["p50_ms"] <= out["p99_ms"]
     assert out["model_steps_per_s"] > 0
     srv.close()
+
+
+# ---- the native server (b200fem_server_*, what a Java host binds) --------
+from artisynth_core_b200.serve import NativeServer, run_stream_native  # noqa: E402
+
+
+def test_native_server_same_alone_and_in_the_mix(b200):
+    pool = _pool()
+    srv = NativeServer(pool, tol=1e-12, pack_models=4)
+    steps = {m: 0 for m in range(len(pool))}
+    rids = []
+
+    def submit(m, k):
+        rids.append(srv.submit(m, k))
+        steps[m] += k
+
+    for m in (0, 1, 2):
+        submit(m, 5)
+    srv.tick()
+    srv.tick()
+    submit(3, 4)
+    submit(0, 3)
+    srv.tick()
+    for m in (4, 5, 6, 7):
+        submit(m, 2)
+    for _ in range(1000):
+        if not srv.pending():
+            break
+        srv.tick()
+    assert srv.pending() == 0
+    st = srv.stats()
+    assert st["builds"] >= 2 and st["completed"] == len(rids) and st["failed"] == 0
+    for r in rids:
+        state, lat = srv.poll(r)
+        assert state == 2 and lat > 0
+    for m, w in enumerate(pool):
+        x, _ = srv.state(m)
+        xa = _alone(w, steps[m], L.PREC_MIXED)
+        assert rel_err(x, xa) <= 1e-9, (m, rel_err(x, xa))
+    srv.close()
+
+
+def test_native_server_budget_eviction(b200):
+    pool = _pool(count=6, seed=8)
+    probe = FemServer(pool[:2], tol=1e-12, pack_models=2)
+    for m in (0, 1):
+        probe.submit(m, 1)
+    probe.tick()
+    per_elem = probe.resident_bytes() / sum(w.conn.shape[0] for w in pool[:2])
+    probe.close()
+    biggest = max(w.conn.shape[0] for w in pool) * per_elem
+    srv = NativeServer(pool, budget=1.3 * biggest, tol=1e-12, pack_models=2)
+    steps = {m: 0 for m in range(len(pool))}
+    for rnd in range(2):
+        for m in range(len(pool)):
+            srv.submit(m, 2)
+            steps[m] += 2
+            for _ in range(1000):
+                if not srv.pending():
+                    break
+                srv.tick()
+    st = srv.stats()
+    assert st["evictions"] > 0 and st["failed"] == 0 and st["pending"] == 0
+    for m, w in enumerate(pool):
+        x, _ = srv.state(m)
+        assert rel_err(x, _alone(w, steps[m], L.PREC_MIXED)) <= 1e-9, m
+    srv.close()
+
+
+def test_native_short_poisson_stream(b200):
+    pool = _pool(count=12, seed=4)
+    srv = NativeServer(pool, tol=1e-10, options={L.OPT_ROW_LANES: 4})
+    srv.preload()
+    out = run_stream_native(srv, poisson_arrivals(200.0, 0.5, len(pool), seed=4), steps_per_request=3)
+    assert out["incomplete"] == 0 and out["requests"] > 0
+    assert 0 < out["p50_ms"] <= out["p99_ms"]
+    srv.close()
