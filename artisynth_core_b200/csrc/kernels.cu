@@ -68,11 +68,6 @@ static cudaError_t ensure_constants(int device) {
   int pa[36], pb[36], w = 0;
   for (int a = 0; a < 8; a++)
     for (int b = a; b < 8; b++) { pa[w] = a; pb[w] = b; w++; }
-  int pa4[10], pb4[10];
-  w = 0;
-  for (int a = 0; a < 4; a++)
-    for (int b = a; b < 4; b++) { pa4[w] = a; pb4[w] = b; w++; }
-  (void)pa4; (void)pb4;
   cudaError_t e;
   if ((e = cudaMemcpyToSymbol(c_tet_gns, tet, sizeof(tet))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_hex_gns, hex, sizeof(hex))) != cudaSuccess) return e;
