@@ -500,15 +500,15 @@ int build_pack(Engine& eng) {
   for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
   eng.pcg_grid = G;
   d.n_pieces = (int)piece_model.size();
-  // default SpMV row width: about one block per lane (tuned later by the
-  // autotuner): tets ~15 blocks per row -> 16 lanes, hexes ~27 -> 32
+  // default SpMV row width (the autotuner may change it later)
   if (eng.opt_row_lanes > 0) {
     eng.pcg_row_lanes = eng.opt_row_lanes;
   } else {
     const double bpr = R > 0 ? (double)NB / R : 1.0;
-    // short rows do best with many rows in flight per warp: tets (~15
-    // blocks per row) -> 4, hexes (~27) -> 16, NODAL 2-ring rows -> 32
-    eng.pcg_row_lanes = bpr <= 18 ? 4 : (bpr <= 40 ? 16 : 32);
+    // many rows in flight per warp do best up to hexes' ~27 blocks per row
+    // (measured: 40x10x10 hex beam 6.8 us per iteration at 4 lanes, 7.1
+    // at 16); NODAL 2-ring rows -> 32
+    eng.pcg_row_lanes = bpr <= 40 ? 4 : 32;
   }
 
   // ---- device upload

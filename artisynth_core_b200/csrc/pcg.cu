@@ -30,7 +30,15 @@
 
 namespace b200fem {
 
+// Threads per CTA: the strided split (every SM holds thousands of rows in
+// its bulk phase) wants many loads in flight; the resident form (a few
+// hundred rows per CTA at most, latency-bound) runs 512 threads with up to
+// 128 registers each, free of spills.  Measured on the 40x10x10 hex beam:
+// 4.7 us per iteration at 512 threads, 5.6 at 1024; on the 256-beam strided
+// pack 1024 threads stay faster (9.6 against 12.7 ms of PCG per step).
 constexpr int kPcgThreads = 1024;
+constexpr int kPcgThreadsResident = 512;
+__host__ __device__ constexpr int pcg_block(bool resident) { return resident ? kPcgThreadsResident : kPcgThreads; }
 constexpr int kRowChunk = 512;
 constexpr int kMaxCtaPieces = 48;
 constexpr int kMaxRestarts = 10;
@@ -50,28 +58,28 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ unsigned atom_add_release_u32(unsigned* p, unsigned v) {
-  unsigned o;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(o) : "l"(p), "r"(v) : "memory");
-  return o;
+__device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" : : "l"(p), "r"(v) : "memory");
 }
 
 // Grid-wide barrier of a cooperative launch (all CTAs co-resident) on a
-// monotonically increasing arrival counter: arrival k of a round sees
-// count = round*G + k and waits for count >= (round+1)*G.  Release on the
-// arrival and acquire on the poll order every CTA's prior global writes
-// before every CTA's later reads.  The wait is bounded: after
+// monotonically increasing arrival counter.  Every CTA passes the same
+// sequence of barriers and counts them in *round (shared memory, read and
+// written by thread 0 only, zero at kernel start), so barrier k is complete
+// when the counter reaches k*G: the arrival is a fire-and-forget reduction
+// (no round trip for its old value) and the poll starts at once.  Release
+// on the arrival and acquire on the poll order every CTA's prior global
+// writes before every CTA's later reads.  The wait is bounded: after
 // kBarrierTimeoutNs the CTA records B200FEM_ERR_TIMEOUT in flags[0] and
 // returns false, and every CTA leaves the kernel at its next barrier.
 // The counter must be zero when the kernel starts.
-__device__ bool grid_barrier(unsigned* count, int* flags) {
+__device__ bool grid_barrier(unsigned* count, int* flags, unsigned* round) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile int* err = flags;
-    const unsigned G = gridDim.x;
-    const unsigned arrived = atom_add_release_u32(count, 1u) + 1u;
-    const unsigned goal = ((arrived + G - 1u) / G) * G;
+    const unsigned goal = ++*round * gridDim.x;
+    red_add_release_u32(count, 1u);
     int ok = 1;
     const unsigned long long t0 = global_ns();
     while ((int)(ld_acquire_u32(count) - goal) < 0) {
@@ -159,6 +167,17 @@ struct CtaRows {
   __device__ __forceinline__ int local(int i, int j) const { return lst0[j] + (i - lst[j]); }
 };
 
+// Butterfly sum of ND values over the warp (every lane gets the sums).  The
+// levels are the outer loop, so the ND chains interleave: their shuffles
+// are in flight together instead of one chain after another.
+template <int ND>
+__device__ __forceinline__ void warp_sum(double* sm) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < ND; k++) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+}
+
 // Reduce ND per-row values over the view's pieces in a fixed order and write
 // partials[buf][piece][k] for every local piece (zero for pieces the view
 // leaves out).  fn(i, row, j, lane, vals) runs per row (local row i, global
@@ -199,10 +218,7 @@ __device__ void cta_row_pass(const PcgArgs& a, const CtaRows& cr, int buf, doubl
       for (int i = pr0 + lane; i < pr1; i += 32)
 #pragma unroll
         for (int k = 0; k < ND; k++) sm[k] += rowbuf[i - c0][k];
-#pragma unroll
-      for (int k = 0; k < ND; k++)
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+      warp_sum<ND>(sm);
       if (lane == 0)
 #pragma unroll
         for (int k = 0; k < ND; k++) pacc[j][k] += sm[k];
@@ -215,24 +231,42 @@ __device__ void cta_row_pass(const PcgArgs& a, const CtaRows& cr, int buf, doubl
     for (int k = 0; k < ND; k++) out[(size_t)cr.gp[j] * 4 + k] = pacc[j][k];
 }
 
-// Per local piece: sum of the partials of its model (warp per piece, fixed
-// lane striding and butterfly order); pieces with skip[j] set are left out.
+// One lane's share of a model's partials: the sum over pieces q = q0 + lane,
+// q0 + lane + 32, ... < q1 of src[q][0..ND), added in increasing q.  The
+// loads of U pieces are issued before their sums, so a lane waits for one
+// L2 round trip per U pieces instead of one per piece (U = 5 covers a
+// model cut into one piece per SM in a single round trip).
+template <int ND, int U = 5>
+__device__ __forceinline__ void lane_partials(const double* src, int q0, int q1, int lane, double* sm) {
+  for (int qq = q0 + lane; qq < q1; qq += 32 * U) {
+    double v[U][ND];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int q = qq + 32 * u;
+#pragma unroll
+      for (int k = 0; k < ND; k++) v[u][k] = q < q1 ? __ldcg(&src[(size_t)q * 4 + k]) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int k = 0; k < ND; k++) sm[k] += v[u][k];
+  }
+}
+
+// Per local piece: sum of the partials of its model, whose pieces are
+// [q0[j], q1[j]) (warp per piece, fixed lane striding and butterfly order);
+// pieces with skip[j] set are left out.
 template <int ND>
-__device__ void model_sums(const PcgArgs& a, const CtaRows& cr, int buf, double (*out)[3], const int* skip) {
+__device__ void model_sums(const PcgArgs& a, const CtaRows& cr, const int* q0s, const int* q1s, int buf,
+                           double (*out)[3], const int* skip) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const double* src = a.partials + (size_t)buf * a.n_pieces * 4;
   for (int j = warp; j < cr.npc; j += nwarps) {
     if (skip && skip[j]) continue;
-    const int m = a.piece_model[cr.gp[j]];
-    const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
+    const int q0 = q0s[j], q1 = q1s[j];
     double sm[3] = {0, 0, 0};
-    for (int qq = q0 + lane; qq < q1; qq += 32)
-#pragma unroll
-      for (int k = 0; k < ND; k++) sm[k] += __ldcg(&src[(size_t)qq * 4 + k]);
-#pragma unroll
-    for (int k = 0; k < ND; k++)
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+    lane_partials<ND>(src, q0, q1, lane, sm);
+    warp_sum<ND>(sm);
     if (lane == 0)
 #pragma unroll
       for (int k = 0; k < ND; k++) out[j][k] = sm[k];
@@ -293,6 +327,46 @@ struct MatView {
   int cached;
 };
 
+// One lane's walk over blocks p, p + stride, ... < p1 of a block row:
+// a += S_p x_col(p), blocks added in increasing p.  The x gathers of two
+// blocks are issued together, so a lane waits for one L2 round trip per
+// two blocks; a missing second block multiplies a zero x.
+template <typename MT>
+__device__ __forceinline__ void block_row_walk(const int* col, const MT* S, const double* x, int p, int p1,
+                                               int stride, double& a0, double& a1, double& a2) {
+  for (; p < p1; p += 2 * stride) {
+    const int pb = p + stride;
+    const bool hb = pb < p1;
+    const int ca = col[p];
+    const int cb = hb ? col[pb] : ca;
+    const double xa0 = x[3 * (size_t)ca], xa1 = x[3 * (size_t)ca + 1], xa2 = x[3 * (size_t)ca + 2];
+    double xb0 = 0, xb1 = 0, xb2 = 0;
+    if (hb) {
+      xb0 = x[3 * (size_t)cb];
+      xb1 = x[3 * (size_t)cb + 1];
+      xb2 = x[3 * (size_t)cb + 2];
+    }
+    {
+      const MT* B = S + (size_t)p * 9;
+      double b[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+      a0 += b[0] * xa0 + b[1] * xa1 + b[2] * xa2;
+      a1 += b[3] * xa0 + b[4] * xa1 + b[5] * xa2;
+      a2 += b[6] * xa0 + b[7] * xa1 + b[8] * xa2;
+    }
+    if (hb) {
+      const MT* B = S + (size_t)pb * 9;
+      double b[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+      a0 += b[0] * xb0 + b[1] * xb1 + b[2] * xb2;
+      a1 += b[3] * xb0 + b[4] * xb1 + b[5] * xb2;
+      a2 += b[6] * xb0 + b[7] * xb1 + b[8] * xb2;
+    }
+  }
+}
+
 // The vectors these SpMVs read (the search direction m, the iterate x) are
 // rewritten by other CTAs between grid barriers, so they are read with plain
 // coherent loads: no __restrict__/read-only-cache path, which is only valid
@@ -315,17 +389,7 @@ __device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int i, int 
     S = mv.S;
   }
   double a0 = 0, a1 = 0, a2 = 0;
-  for (int p = p0 + lane; p < p1; p += 32) {
-    const int c = col[p];
-    const MT* B = S + (size_t)p * 9;
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) b[k] = (double)B[k];
-    const double x0 = x[3 * (size_t)c], x1 = x[3 * (size_t)c + 1], x2 = x[3 * (size_t)c + 2];
-    a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
-    a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
-    a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
-  }
+  block_row_walk<MT>(col, S, x, p0 + lane, p1, 32, a0, a1, a2);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -364,17 +428,7 @@ __device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int 
   }
   const int gl = lane & (L - 1);
   double a0 = 0, a1 = 0, a2 = 0;
-  for (int p = p0 + gl; p < p1; p += L) {
-    const int c = col[p];
-    const MT* B = S + (size_t)p * 9;
-    double b[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) b[k] = (double)B[k];
-    const double x0 = x[3 * (size_t)c], x1 = x[3 * (size_t)c + 1], x2 = x[3 * (size_t)c + 2];
-    a0 += b[0] * x0 + b[1] * x1 + b[2] * x2;
-    a1 += b[3] * x0 + b[4] * x1 + b[5] * x2;
-    a2 += b[6] * x0 + b[7] * x1 + b[8] * x2;
-  }
+  block_row_walk<MT>(col, S, x, p0 + gl, p1, L, a0, a1, a2);
 #pragma unroll
   for (int off = L / 2; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -539,11 +593,13 @@ __host__ __device__ inline void pcg_smem_layout(int nloc_max, int nb_max, int re
 // of packs that fit); otherwise residency is the runtime flag (zero in the
 // strided split), which keeps the register pressure of each form low.
 template <typename MT, bool RES>
-__global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
+__global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   __shared__ double rowbuf[kRowChunk][3];
   __shared__ double sn[kRowChunk][3];
   __shared__ double pacc[kMaxCtaPieces][3];
   __shared__ double sums[kMaxCtaPieces][3];
+  // s_thr: the pipelined test's bound tol * ||b||, fixed for the solve
+  __shared__ double s_thr[kMaxCtaPieces];
   __shared__ double s_bb[kMaxCtaPieces], s_tol[kMaxCtaPieces], s_alpha[kMaxCtaPieces],
       s_beta[kMaxCtaPieces], s_gold[kMaxCtaPieces], s_aold[kMaxCtaPieces];
   __shared__ int s_conv[kMaxCtaPieces], s_iters[kMaxCtaPieces], s_first[kMaxCtaPieces];
@@ -551,20 +607,29 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
   // not restarted): later passes leave its rows alone
   __shared__ int s_done[kMaxCtaPieces];
   __shared__ int s_gp[kMaxCtaPieces], s_lst[kMaxCtaPieces + 1], s_grow[kMaxCtaPieces];
+  // the pieces [s_q0, s_q1) of each local piece's model (global piece numbers;
+  // read here once instead of from global memory in every reduction)
+  __shared__ int s_q0[kMaxCtaPieces], s_q1[kMaxCtaPieces];
   // row space of the pieces still iterating (see active_scan)
   __shared__ int s_alst[kMaxCtaPieces + 1];
   __shared__ int s_restart;
+  __shared__ int s_unc[2];  // see the pipelined iteration
   extern __shared__ __align__(16) unsigned char dyn[];
   const bool res = RES || a.resident;
   const int pc0 = a.cta_piece[blockIdx.x];
   const int npc = a.cta_piece[blockIdx.x + 1] - pc0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int ph = 0;
+  __shared__ unsigned s_bar_round;  // grid barriers passed (see grid_barrier)
+  if (threadIdx.x == 0) s_bar_round = 0;
 
   for (int j = threadIdx.x; j < npc; j += blockDim.x) {
     const int g = a.cta_plist[pc0 + j];
     s_gp[j] = g;
     s_grow[j] = a.piece_row[g];
+    const int m = a.piece_model[g];
+    s_q0[j] = a.model_piece[m];
+    s_q1[j] = a.model_piece[m + 1];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -586,10 +651,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     __syncthreads();
   };
   // the last piece of a model owns the model's flags and outputs
-  auto owner = [&](int j) {
-    const int g = s_gp[j];
-    return g == a.model_piece[a.piece_model[g] + 1] - 1;
-  };
+  auto owner = [&](int j) { return s_gp[j] == s_q1[j] - 1; };
 
   size_t off_vec, off_ro, off_col, off_S, total;
   pcg_smem_layout<MT>(a.nloc_max, a.nb_max, res, a.cached, &off_vec, &off_ro, &off_col, &off_S, &total);
@@ -679,10 +741,13 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       vals[0] = dot3(bv, bv);
     }
   });
-  if (!grid_barrier(a.barrier, a.flags)) return;
-  model_sums<1>(a, cr, ph & 1, sums, s_done);
+  if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+  model_sums<1>(a, cr, s_q0, s_q1, ph & 1, sums, s_done);
   for (int j = threadIdx.x; j < npc; j += blockDim.x)
-    if (!s_done[j]) s_bb[j] = sums[j][0];
+    if (!s_done[j]) {
+      s_bb[j] = sums[j][0];
+      s_thr[j] = s_tol[j] * sqrt(s_bb[j]);
+    }
   ph++;
 
   int total_it = 0;
@@ -703,8 +768,8 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         vals[0] = dot3(r, z);
         vals[1] = dot3(r, r);
       });
-      if (!grid_barrier(a.barrier, a.flags)) return;
-      model_sums<2>(a, cr, ph & 1, sums, s_conv);
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+      model_sums<2>(a, cr, s_q0, s_q1, ph & 1, sums, s_conv);
       ph++;
       for (int j = threadIdx.x; j < npc; j += blockDim.x) {
         if (s_conv[j]) continue;
@@ -746,12 +811,12 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             vals[0] = pqv;
           }
         });
-        if (!grid_barrier(a.barrier, a.flags)) return;
+        if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
         if (__ldcg(&a.unconv[idx]) == 0) {
           total_it += it;
           break;
         }
-        model_sums<1>(a, cr, ph & 1, sums, s_conv);
+        model_sums<1>(a, cr, s_q0, s_q1, ph & 1, sums, s_conv);
         ph++;
         for (int j = threadIdx.x; j < npc; j += blockDim.x)
           s_alpha[j] = s_conv[j] ? 0.0 : s_gold[j] / sums[j][0];
@@ -778,8 +843,8 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           vals[0] = dot3(r, z);
           vals[1] = dot3(r, r);
         });
-        if (!grid_barrier(a.barrier, a.flags)) return;
-        model_sums<2>(a, cr, ph & 1, sums, s_conv);
+        if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+        model_sums<2>(a, cr, s_q0, s_q1, ph & 1, sums, s_conv);
         ph++;
         for (int j = threadIdx.x; j < npc; j += blockDim.x) {
           if (s_conv[j]) continue;
@@ -815,7 +880,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         vals[2] = dot3(r, r);
       }
     });
-    if (!grid_barrier(a.barrier, a.flags)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
     int mbuf = 0;  // m0 holds the current m
 
     for (int it = 0;; it++) {
@@ -845,21 +910,25 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             // convergence test is on the recurrence residual
             const int sw = warp - nroww;
             const double* src = a.partials + (size_t)(ph & 1) * a.n_pieces * 4;
+            // unconv[idx - 1] is final (its barrier has passed); it is
+            // loaded here, next to the partials, and tested after this
+            // iteration's barrier instead of costing a round trip after
+            // every barrier.  Two slots: the next write to this one comes
+            // after the next barrier's __syncthreads.
+            const int unc = (sw == 0 && lane == 0 && it > 0) ? __ldcg(&a.unconv[idx - 1]) : 1;
             for (int j = sw; j < npc; j += nsumw) {
               if (s_conv[j]) continue;
-              const int m = a.piece_model[s_gp[j]];
-              const int q0 = a.model_piece[m], q1 = a.model_piece[m + 1];
+              const int q0 = s_q0[j], q1 = s_q1[j];
+              // the reciprocals of the previous gamma and alpha do not
+              // depend on the partials: they are formed while the loads are
+              // in flight, which leaves one division after the sums
+              const double rg = 1.0 / s_gold[j], ra = 1.0 / s_aold[j];
               double sm[3] = {0, 0, 0};
-              for (int qq = q0 + lane; qq < q1; qq += 32)
-#pragma unroll
-                for (int k = 0; k < 3; k++) sm[k] += __ldcg(&src[(size_t)qq * 4 + k]);
-#pragma unroll
-              for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+              lane_partials<3>(src, q0, q1, lane, sm);
+              warp_sum<3>(sm);
               if (lane == 0) {
                 const double gam = sm[0], del = sm[1], rho = sm[2];
-                if (sqrt(rho) <= s_tol[j] * sqrt(s_bb[j]) || rho == 0.0) {
+                if (sqrt(rho) <= s_thr[j] || rho == 0.0) {
                   s_conv[j] = 1;
                 } else {
                   double beta = 0, alpha;
@@ -867,8 +936,8 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
                     alpha = gam / del;
                     s_first[j] = 0;
                   } else {
-                    beta = gam / s_gold[j];
-                    alpha = gam / (del - beta * gam / s_aold[j]);
+                    beta = gam * rg;
+                    alpha = gam / (del - beta * gam * ra);
                   }
                   s_beta[j] = beta;
                   s_alpha[j] = alpha;
@@ -879,6 +948,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
                 }
               }
             }
+            if (sw == 0 && lane == 0) s_unc[it & 1] = unc;
           }
           __syncthreads();
           if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap))) {
@@ -952,10 +1022,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
             if (c0 + lane < c1)
 #pragma unroll
               for (int k = 0; k < 3; k++) sm[k] = rowbuf[lane][k];
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-              for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+            warp_sum<3>(sm);
             if (lane == 0)
 #pragma unroll
               for (int k = 0; k < 3; k++) pacc[0][k] += sm[k];
@@ -969,10 +1036,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
           for (int i = pr0 + lane; i < pr1; i += 32)
 #pragma unroll
             for (int k = 0; k < 3; k++) sm[k] += rowbuf[i - c0][k];
-#pragma unroll
-          for (int k = 0; k < 3; k++)
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) sm[k] += __shfl_xor_sync(0xffffffffu, sm[k], off);
+          warp_sum<3>(sm);
           if (lane == 0)
 #pragma unroll
             for (int k = 0; k < 3; k++) pacc[j][k] += sm[k];
@@ -992,10 +1056,12 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
       }
       // the next iteration works on the models still unconverged
       rescan(s_conv);
-      if (!grid_barrier(a.barrier, a.flags)) return;
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
       mbuf ^= 1;
-      if (__ldcg(&a.unconv[idx]) == 0) {
-        total_it += it;
+      // every model still iterating at idx - 1 converged there: iteration
+      // idx had no rows to work on and is not counted
+      if (s_unc[it & 1] == 0) {
+        total_it += it - 1;
         break;
       }
     }
@@ -1007,7 +1073,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     if (res)
       for (int i = threadIdx.x; i < nloc; i += blockDim.x) store3(a.x, r0 + i, st.at(VX, i, r0 + i));
     rescan(s_done);
-    if (!grid_barrier(a.barrier, a.flags)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
     cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
       double Ax[3];
       view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
@@ -1025,8 +1091,8 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
         store3(a.m1, row, u);
       }
     });
-    if (!grid_barrier(a.barrier, a.flags)) return;
-    model_sums<1>(a, cr, ph & 1, sums, s_done);
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+    model_sums<1>(a, cr, s_q0, s_q1, ph & 1, sums, s_done);
     ph++;
     if (threadIdx.x == 0) s_restart = 0;
     __syncthreads();
@@ -1058,7 +1124,7 @@ __global__ void __launch_bounds__(kPcgThreads) pcg_kernel(PcgArgs a) {
     __syncthreads();
     // every CTA must agree on a restart: publish and read after a barrier
     if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
-    if (!grid_barrier(a.barrier, a.flags)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
     if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
     // continue with classic PCG, whose attainable accuracy is better than
     // that of the pipelined recurrences
@@ -1143,7 +1209,7 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   if ((int)total > eng.pcg_attr_smem) return cudaErrorInvalidConfiguration;  // prepare_pcg not run
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(eng.pcg_grid);
-  cfg.blockDim = dim3(kPcgThreads);
+  cfg.blockDim = dim3(pcg_block(a.resident != 0));
   cfg.dynamicSmemBytes = total;
   cfg.stream = eng.stream;
   cudaLaunchAttribute attr[1];
@@ -1434,7 +1500,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.tol_override = 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);
-  cfg.blockDim = dim3(kPcgThreads);
+  cfg.blockDim = dim3(pcg_block(a.resident != 0));
   cfg.dynamicSmemBytes = dyn;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
