@@ -1318,6 +1318,47 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
   return status;
 }
 
+int orc_num_ip(void* h) { return ((Model*)h)->sh.nip; }
+
+// Integration point k of element e at positions x (3N), as the non-linear
+// element loop forms it (FemModel3d.java:3443-3470): shape gradients in the
+// current configuration GNx (nen x 3), dv = det J * w, and the material's
+// Cauchy stress sig (xx, yy, zz, xy, yz, xz) and tangent D (6x6 row-major,
+// same order), with the NODAL pressure of the last update_stress_stiffness
+// call where the model uses it.  These are the per-block descriptor inputs
+// of the reference's device assembly (FemModel3d.java:4613-4936).  Returns
+// nen, or -1 for linear materials (whose blocks come from the rest
+// stiffness) and out-of-range e or k.
+int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv, double* sig, double* D) {
+  const Model& m = *(const Model*)h;
+  const ShapeTable& s = m.sh;
+  if (m.mat.linear() || e < 0 || e >= m.E || k < 0 || k >= s.nip) return -1;
+  const int nen = m.nen;
+  const int* nodes = &m.conn[(size_t)e * nen];
+  const double* GNs = &s.GNs[k * nen * 3];
+  double J[9], invJ[9], F[9];
+  compute_jacobian(J, GNs, nen, x, nodes);
+  mul3(F, J, &m.invJ0[((size_t)e * s.nip + k) * 9]);
+  const double detF = det3(F);
+  const double detJ = fast_invert(invJ, J);
+  *dv = detJ * s.w[k];
+  for (int n = 0; n < nen; n++) {
+    const double* g = GNs + 3 * n;
+    for (int c = 0; c < 3; c++) GNx[3 * n + c] = invJ[c] * g[0] + invJ[3 + c] * g[1] + invJ[6 + c] * g[2];
+  }
+  double pressure = 0;
+  if (m.incomp == INCOMP_NODAL && !m.nodePressure.empty()) {
+    if (m.type == ELEM_TET) {
+      for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
+      pressure /= nen;
+    } else {
+      pressure = m.nodePressure[nodes[k]];
+    }
+  }
+  material_stress_tangent(sig, D, m.mat, F, detF, pressure);
+  return nen;
+}
+
 // point-level material evaluation for known-answer and finite-difference tests
 void orc_material_eval(int mat_kind, const double* mat_params, const double* F, double pressure,
                        double* sig6, double* D36) {

@@ -15,6 +15,10 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libfemoracle.so")
 _lib = None
+# the reference's device assembly kernels (cudssBridgeKernels.cu), compiled
+# from the reference tree by `make ref` where that tree is present
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
+REF_SOURCE_ROOT = "/root/reference"
 
 ELEM_TET, ELEM_HEX = 0, 1
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN = 0, 1, 2
@@ -28,6 +32,28 @@ def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
+
+
+def build_ref() -> str | None:
+    """Compile the reference's kernels into oracle/_ref/ when the reference
+    tree is present; elsewhere (a GPU box gets the prebuilt library) return
+    the library path if it exists, else None."""
+    if os.path.isdir(REF_SOURCE_ROOT):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + REF_SOURCE_ROOT], check=True)
+    return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
+
+
+def ref_kernels():
+    """ctypes handle of the reference kernels library, or None when it was
+    not built.  Entry points used: addMaterialStiffness3_launch
+    (cudssBridgeKernels.cu:244-253)."""
+    if not os.path.exists(REF_LIB_PATH):
+        return None
+    R = ctypes.CDLL(REF_LIB_PATH)
+    vp = ctypes.c_void_p
+    R.addMaterialStiffness3_launch.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_double, vp, vp]
+    R.addMaterialStiffness3_launch.restype = None
+    return R
 
 
 def lib():
@@ -65,6 +91,10 @@ def lib():
         L.orc_material_stiffness_block.argtypes = [_dp, _dp, ctypes.c_void_p, _dp, ctypes.c_double, _dp]
         L.orc_linear_C.argtypes = [ctypes.c_double, ctypes.c_double, _dp]
         L.orc_polar.argtypes = [_dp, _dp]
+        L.orc_num_ip.argtypes = [vp]
+        L.orc_num_ip.restype = ctypes.c_int
+        L.orc_ip_data.argtypes = [vp, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_double), _dp, _dp]
+        L.orc_ip_data.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -153,6 +183,22 @@ class OracleModel:
         K = np.zeros(9 * self.nnzb)
         ninv = self.L.orc_update_stress_stiffness(self.h, x, f, K)
         return f.reshape(-1, 3), K.reshape(-1, 3, 3), ninv
+
+    def num_ip(self):
+        return self.L.orc_num_ip(self.h)
+
+    def ip_data(self, x, e, k):
+        """(GNx (nen,3), dv, sig (6), D (6,6)) of integration point k of
+        element e at positions x (non-linear materials)."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        nen = 4 if self.elem_type == ELEM_TET else 8
+        g = np.zeros(3 * nen)
+        dv = ctypes.c_double()
+        sig = np.zeros(6)
+        D = np.zeros(36)
+        if self.L.orc_ip_data(self.h, x, int(e), int(k), g, ctypes.byref(dv), sig, D) != nen:
+            raise ValueError("no integration-point data for this element/point")
+        return g.reshape(nen, 3), dv.value, sig, D.reshape(6, 6)
 
     def nodal_pressures(self):
         out = np.zeros(self.N)

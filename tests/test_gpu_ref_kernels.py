@@ -1,0 +1,112 @@
+"""The reference's own device assembly kernel as a second checker.
+
+The reference's device assembly (FemModel3d.addMaterialStiffness3CrsValue-
+Contributions, FemModel3d.java:4613-4936) hands one descriptor per block
+contribution to addMaterialStiffness3Kernel (cudssBridgeKernels.cu:164-242):
+the current shape gradients g_i, g_j and dv of one integration point, the
+material tangent D (6x6) and Cauchy stress sigma there, and the nine CRS value
+slots of block (i, j).  The kernel forms B_i^T D B_j dv + (g_i . sigma g_j) dv I
+and adds it into the CRS values (FP64 atomics).
+
+That kernel, compiled from the reference source into oracle/_ref/ (`make -C
+oracle ref`), is fed the oracle's integration-point data for every (element,
+point, node pair) of NeoHookean tet and hex beams at deformed positions.  Its
+CRS values must equal
+* the engine's full-partition CRS export (b200fem_update_stress_stiffness)
+  within the parity bar, 1e-10 of the largest entry, and
+* the oracle's own assembly within 1e-12 (same arithmetic, summation order
+  differs through the atomics).
+This pins the element-tangent assembly (FemUtilities.addMaterialStiffness /
+addGeometricStiffness, FemUtilities.java:78-144) to the reference's code,
+not only to its restatement.
+"""
+import numpy as np
+import pytest
+
+from artisynth_core_b200.femmodel import NeoHookeanMaterial
+from artisynth_core_b200 import workloads as W
+from oracle import oracle as O
+
+from helpers import deformed, oracle_model, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_lib():
+    R = O.ref_kernels()
+    if R is None:
+        pytest.skip("reference kernels not built (make -C oracle ref needs the reference tree)")
+    return R
+
+
+def _descriptors(om, wl, x):
+    """Per block contribution: slots (9), g_i, g_j, D (36), sigma (6), dv."""
+    sidx = om.solve_index()
+    rp, col = om.pattern()
+    _, _, slots = om.crs(0)
+    nen = wl.conn.shape[1]
+    S, GI, GJ, DD, SG, DV = [], [], [], [], [], []
+    for e in range(wl.conn.shape[0]):
+        for k in range(om.num_ip()):
+            g, dv, sig, D = om.ip_data(x, e, k)
+            for a in range(nen):
+                ra = sidx[wl.conn[e, a]]
+                if ra < 0:
+                    continue
+                for b in range(nen):
+                    rb = sidx[wl.conn[e, b]]
+                    if rb < 0:
+                        continue
+                    p = rp[ra] + int(np.searchsorted(col[rp[ra]:rp[ra + 1]], rb))
+                    assert col[p] == rb
+                    S.append(slots[9 * p:9 * p + 9])
+                    GI.append(g[a])
+                    GJ.append(g[b])
+                    DD.append(D.reshape(-1))
+                    SG.append(sig)
+                    DV.append(dv)
+    return (np.ascontiguousarray(np.array(S, dtype=np.int32).reshape(-1)),
+            np.ascontiguousarray(np.array(GI).reshape(-1)), np.ascontiguousarray(np.array(GJ).reshape(-1)),
+            np.ascontiguousarray(np.array(DD).reshape(-1)), np.ascontiguousarray(np.array(SG).reshape(-1)),
+            np.ascontiguousarray(np.array(DV)))
+
+
+def _reference_crs(R, desc, nnz):
+    import torch
+    slots, gi, gj, D, sig, dv = desc
+    nb = dv.size
+    # every array the kernel indexes is sized for nb blocks, and every slot
+    # lies inside the CRS value array: checked before the launch
+    assert slots.size == 9 * nb and gi.size == 3 * nb and gj.size == 3 * nb
+    assert D.size == 36 * nb and sig.size == 6 * nb
+    assert slots.min() >= 0 and slots.max() < nnz
+    dev = torch.device("cuda:0")
+    t = [torch.from_numpy(a).to(dev) for a in (slots, gi, gj, D, sig, dv)]
+    crs = torch.zeros(nnz, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    R.addMaterialStiffness3_launch(nb, *(a.data_ptr() for a in t), 1.0, crs.data_ptr(), stream)
+    torch.cuda.synchronize()
+    return crs.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex"])
+def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
+    R = _ref_lib()
+    if case == "neohookean_tet":
+        wl = W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33))
+    else:
+        wl = W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45))
+    wl.build_mesh()
+    om = oracle_model(oracle, wl)
+    x = deformed(wl.rest, seed=5)
+    _, oK, ninv = om.update_stress_stiffness(x)
+    assert ninv == 0
+    m = wl.model()
+    _, K, crs = m.updateStressAndStiffness(x, want_crs=True)
+    ref = _reference_crs(R, _descriptors(om, wl, x), crs.size)
+    _, _, slots = om.crs(0)
+    ocrs = np.zeros(crs.size)
+    ocrs[slots] = oK.reshape(-1)
+    assert rel_err(ocrs, ref) <= 1e-12, rel_err(ocrs, ref)
+    assert rel_err(crs, ref) <= 1e-10, rel_err(crs, ref)
