@@ -46,13 +46,16 @@ def build_ref() -> str | None:
 def ref_kernels():
     """ctypes handle of the reference kernels library, or None when it was
     not built.  Entry points used: addMaterialStiffness3_launch
-    (cudssBridgeKernels.cu:244-253)."""
+    (cudssBridgeKernels.cu:244-253) and addLinearElasticStiffness3Element_launch
+    (:518-530)."""
     if not os.path.exists(REF_LIB_PATH):
         return None
     R = ctypes.CDLL(REF_LIB_PATH)
     vp = ctypes.c_void_p
     R.addMaterialStiffness3_launch.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp, ctypes.c_double, vp, vp]
     R.addMaterialStiffness3_launch.restype = None
+    R.addLinearElasticStiffness3Element_launch.argtypes = [ctypes.c_int] + [vp] * 9 + [ctypes.c_double, vp, vp]
+    R.addLinearElasticStiffness3Element_launch.restype = None
     return R
 
 

@@ -19,11 +19,18 @@ CRS values must equal
 This pins the element-tangent assembly (FemUtilities.addMaterialStiffness /
 addGeometricStiffness, FemUtilities.java:78-144) to the reference's code,
 not only to its restatement.
+
+The linear rest stiffness goes through addLinearElasticStiffness3ElementKernel
+(cudssBridgeKernels.cu:470-516), which builds D from (E, nu) itself
+(fillLinearElasticD) and sums B_i^T D B_j dv over the integration points of
+each element's node pairs, from rest shape gradients and dv: it must equal the
+engine's stiffness of a non-corotated LinearMaterial (K = K0 at any position)
+within 1e-10.
 """
 import numpy as np
 import pytest
 
-from artisynth_core_b200.femmodel import NeoHookeanMaterial
+from artisynth_core_b200.femmodel import LinearMaterial, NeoHookeanMaterial
 from artisynth_core_b200 import workloads as W
 from oracle import oracle as O
 
@@ -109,4 +116,82 @@ def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     ocrs = np.zeros(crs.size)
     ocrs[slots] = oK.reshape(-1)
     assert rel_err(ocrs, ref) <= 1e-12, rel_err(ocrs, ref)
+    assert rel_err(crs, ref) <= 1e-10, rel_err(crs, ref)
+
+
+def _linear_element_arrays(om_geom, wl, E, nu):
+    """Per-element arrays of addLinearElasticStiffness3Element_launch from the
+    rest kinematics (shape gradients, dv) of the oracle model om_geom."""
+    sidx = om_geom.solve_index()
+    rp, col = om_geom.pattern()
+    _, _, slots = om_geom.crs(0)
+    ne, nen = wl.conn.shape
+    nip = om_geom.num_ip()
+    counts = np.full(ne, nen, dtype=np.int32)
+    pair_off = [0]
+    pairs, bslots = [], []
+    grads = np.zeros((ne, nip, nen, 3))
+    dvs = np.zeros((ne, nip))
+    for e in range(ne):
+        for k in range(nip):
+            g, dv, _, _ = om_geom.ip_data(wl.rest, e, k)
+            grads[e, k] = g
+            dvs[e, k] = dv
+        for a in range(nen):
+            ra = sidx[wl.conn[e, a]]
+            if ra < 0:
+                continue
+            for b in range(nen):
+                rb = sidx[wl.conn[e, b]]
+                if rb < 0:
+                    continue
+                p = rp[ra] + int(np.searchsorted(col[rp[ra]:rp[ra + 1]], rb))
+                assert col[p] == rb
+                pairs.append((a, b))
+                bslots.append(slots[9 * p:9 * p + 9])
+        pair_off.append(len(pairs))
+    ip_off = np.arange(ne + 1, dtype=np.int32) * nip
+    grad_off = np.arange(ne, dtype=np.int32) * nip * nen
+    params = np.tile(np.array([E, nu]), ne)
+    return (counts, np.array(pair_off, dtype=np.int32), ip_off, grad_off,
+            np.array(pairs, dtype=np.int32).reshape(-1), np.array(bslots, dtype=np.int32).reshape(-1),
+            params, grads.reshape(-1), dvs.reshape(-1))
+
+
+@pytest.mark.parametrize("case", ["tet", "hex"])
+def test_reference_kernel_assembles_linear_rest_stiffness(b200, oracle, case):
+    import torch
+    R = _ref_lib()
+    E, nu = 5e4, 0.33
+    if case == "tet":
+        wl = W.small_tet_beam(LinearMaterial(E, nu, False))
+        geom = W.small_tet_beam(NeoHookeanMaterial(E, nu))
+    else:
+        wl = W.small_hex_beam(LinearMaterial(E, nu, False))
+        geom = W.small_hex_beam(NeoHookeanMaterial(E, nu))
+    wl.build_mesh()
+    geom.build_mesh()
+    assert np.array_equal(wl.rest, geom.rest) and np.array_equal(wl.conn, geom.conn)
+    om_geom = oracle_model(oracle, geom)
+    arrs = _linear_element_arrays(om_geom, wl, E, nu)
+    counts, pair_off, ip_off, grad_off, pairs, bslots, params, grads, dvs = arrs
+    m = wl.model()
+    _, K, crs = m.updateStressAndStiffness(deformed(wl.rest, seed=5), want_crs=True)
+    ne, nen = wl.conn.shape
+    nip = om_geom.num_ip()
+    # the kernel's indexing, checked before the launch: pair lists, local
+    # node indices, gradient and dv offsets, CRS slots
+    assert pair_off[-1] * 2 == pairs.size and pair_off[-1] * 9 == bslots.size
+    assert pairs.min() >= 0 and pairs.max() < nen
+    assert grads.size == 3 * ne * nip * nen and dvs.size == ne * nip and ip_off[-1] == dvs.size
+    assert bslots.min() >= 0 and bslots.max() < crs.size
+    dev = torch.device("cuda:0")
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (counts, pair_off, ip_off, grad_off, pairs, bslots, params, grads, dvs)]
+    out = torch.zeros(crs.size, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    R.addLinearElasticStiffness3Element_launch(ne, *(a.data_ptr() for a in t), 1.0, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    ref = out.cpu().numpy()
     assert rel_err(crs, ref) <= 1e-10, rel_err(crs, ref)
