@@ -130,6 +130,8 @@ def lib():
         "b200fem_set_external_forces": ([H, _dp], ctypes.c_int),
         "b200fem_update_stress_stiffness": ([H, _dp, _dp, _dp, _dp], ctypes.c_int),
         "b200fem_backward_euler_step": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
+        "b200fem_backward_euler_step_host": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_spmv": ([H, _dp, _dp], ctypes.c_int),
         "b200fem_pcg_solve": ([H, _dp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_last_timing": ([H, _dp, _dp], ctypes.c_int),

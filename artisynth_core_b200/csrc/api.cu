@@ -1169,9 +1169,13 @@ static int read_step_status(Engine& eng, b200fem_stats* stats, int max_iter) {
   return B200FEM_OK;
 }
 
-int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps, b200fem_stats* stats) {
-  ENG(h);
-  NEED_BUILT();
+namespace {
+// nsteps BackwardEuler steps.  With host buffers, the state is copied in
+// before the first step (after any graph capture, outside the timed events)
+// and back after the last, on the engine's stream, so the one
+// synchronisation that reads the step status also covers the copies.
+int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, b200fem_stats* stats,
+                         double* x_host, double* v_host) {
   if (!p || nsteps < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid step parameters");
   if (!(p->h > 0) || !(p->tol > 0) || p->max_iter <= 0)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "step size, tolerance and max_iter must be positive");
@@ -1233,6 +1237,9 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
     CK(cudaEventCreate(&e));
     eng.ev_pool.push_back(e);
   }
+  const size_t state_bytes = 3 * sizeof(double) * (size_t)d.n_nodes;
+  if (x_host) CK(cudaMemcpyAsync(d.x, x_host, state_bytes, cudaMemcpyHostToDevice, eng.stream));
+  if (v_host) CK(cudaMemcpyAsync(d.v, v_host, state_bytes, cudaMemcpyHostToDevice, eng.stream));
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   for (int s = 0; s < nsteps; s++) {
     CK(cudaEventRecord(eng.ev_pool[0], eng.stream));
@@ -1254,6 +1261,8 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
     CK(cudaEventRecord(eng.ev_pool[2], eng.stream));
   }
   CK(cudaEventRecord(eng.ev[1], eng.stream));
+  if (x_host) CK(cudaMemcpyAsync(x_host, d.x, state_bytes, cudaMemcpyDeviceToHost, eng.stream));
+  if (v_host) CK(cudaMemcpyAsync(v_host, d.v, state_bytes, cudaMemcpyDeviceToHost, eng.stream));
   eng.have_matrix = true;
   int st = read_step_status(eng, stats, max_iter);
   // device time of the last step's assembly (element, gather, RHS kernels)
@@ -1268,6 +1277,21 @@ int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, 
   eng.last_solve_ms = b;
   eng.last_call_ms = t;
   return st;
+}
+}  // namespace
+
+int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps, b200fem_stats* stats) {
+  ENG(h);
+  NEED_BUILT();
+  return backward_euler_steps(eng, p, nsteps, stats, nullptr, nullptr);
+}
+
+int b200fem_backward_euler_step_host(b200fem_handle h, const b200fem_step_params* p, int nsteps, double* x,
+                                     double* v, b200fem_stats* stats) {
+  ENG(h);
+  NEED_BUILT();
+  if (!x || !v) return fail(&eng, B200FEM_ERR_INVALID_ARG, "x and v are required");
+  return backward_euler_steps(eng, p, nsteps, stats, x, v);
 }
 
 int b200fem_spmv(b200fem_handle h, const double* x, double* y) {

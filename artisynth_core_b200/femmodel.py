@@ -373,6 +373,19 @@ class MechSystemSolver:
                                  ctypes.byref(self.stats))
         return self.stats
 
+    def backwardEulerHost(self, h, x, v, nsteps=1):
+        """nsteps steps from the host state x, v (float64 arrays of 3N
+        values, updated in place): the call a host that keeps the state makes
+        every step (b200fem_backward_euler_step_host)."""
+        for a in (x, v):
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size != 3 * self.model.numNodes():
+                raise ValueError("x and v must be C-contiguous float64 arrays of 3N values")
+        p = self.params(h)
+        self.model.engine().call("b200fem_backward_euler_step_host", ctypes.byref(p), int(nsteps),
+                                 ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(v.ctypes.data),
+                                 ctypes.byref(self.stats))
+        return self.stats
+
     def spmv(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1).copy()
         y = np.zeros_like(x)

@@ -530,18 +530,21 @@ def run_b200(args):
     step_ms_max = float(t.item())
     value = world * 1e3 / step_ms_max
 
-    # ---- end to end through the C ABI with host buffers: H2D state, step,
-    # D2H state, every step
-    x_h, v_h = m.getState()
+    # ---- end to end through the C ABI with host buffers: every step,
+    # b200fem_backward_euler_step_host copies x, v in from pinned host memory,
+    # steps, and copies the new x, v back (one synchronisation per call)
+    xs, vs = m.getState()
+    x_h = torch.empty(xs.size, dtype=torch.float64, pin_memory=True).numpy()
+    v_h = torch.empty(vs.size, dtype=torch.float64, pin_memory=True).numpy()
+    x_h[:] = xs.reshape(-1)
+    v_h[:] = vs.reshape(-1)
     e2e_steps = max(3, args.steps)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        m.setState(x_h, v_h)
-        ms.backwardEuler(wl.h, 1)
-        x_h, v_h = m.getState()
+        ms.backwardEulerHost(wl.h, x_h, v_h)
     t1 = time.perf_counter()
     e2e_ms = torch.tensor([1e3 * (t1 - t0) / e2e_steps], dtype=torch.float64, device=f"cuda:{dev}")
     if dist is not None:

@@ -165,6 +165,15 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
 /* nsteps BackwardEuler steps on the device-resident state */
 int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps,
                                 b200fem_stats* stats);
+/* MechSystemSolver.backwardEuler (MechSystemSolver.java:2171-2476) for a host
+   that keeps the state: x, v (3N each, host memory, in/out) are copied in,
+   nsteps steps run, and the new x, v are copied back, with one
+   synchronisation for the whole call.  The PCG's initial guess extrapolates
+   the engine's own last two velocities (the warm start); when the host hands
+   back the state it received, the result equals b200fem_backward_euler_step
+   on the device-resident state bit for bit. */
+int b200fem_backward_euler_step_host(b200fem_handle h, const b200fem_step_params* p, int nsteps,
+                                     double* x, double* v, b200fem_stats* stats);
 /* y = S x with the solve matrix of the last step (host vectors, 3*n_active) */
 int b200fem_spmv(b200fem_handle h, const double* x, double* y);
 /* block-Jacobi PCG on the solve matrix of the last step (host vectors) */
