@@ -5,9 +5,11 @@ interface around it."""
 from . import _lib
 from ._lib import B200FemError, lib
 from .femmodel import (FemEngine, FemFactory, FemModel3d, FemPack, LinearMaterial, MechSystemSolver,
-                       MooneyRivlinMaterial, NeoHookeanMaterial, create_grid, jitter_grid)
+                       MooneyRivlinMaterial, NeoHookeanMaterial, StVenantKirchoffMaterial, create_grid,
+                       jitter_grid)
 
 __all__ = [
     "B200FemError", "FemEngine", "FemFactory", "FemModel3d", "FemPack", "LinearMaterial", "MechSystemSolver",
-    "MooneyRivlinMaterial", "NeoHookeanMaterial", "create_grid", "jitter_grid", "lib", "_lib",
+    "MooneyRivlinMaterial", "NeoHookeanMaterial", "StVenantKirchoffMaterial", "create_grid", "jitter_grid",
+    "lib", "_lib",
 ]

@@ -27,7 +27,7 @@ ERR_TIMEOUT = -7
 ERR_NO_CONVERGE = -13
 
 ELEM_TET, ELEM_HEX = 0, 1
-MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN = 0, 1, 2
+MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 PART_FULL, PART_UPPER = 0, 1

@@ -764,12 +764,12 @@ int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double*
 
 int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, double density, int incomp) {
   ENG(h);
-  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_MOONEYRIVLIN || !params)
+  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_STVK || !params)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
   if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
   ModelDesc& m = eng.models[0];
   m.mat_kind = mat_kind;
-  int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_NEOHOOKEAN ? 2 : 8;
+  int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_MOONEYRIVLIN ? 8 : 2;
   std::fill(m.mat_params, m.mat_params + kMatParams, 0.0);
   std::copy(params, params + np, m.mat_params);
   m.density = density;
@@ -786,7 +786,7 @@ int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double
   if (elem_type != B200FEM_ELEM_TET && elem_type != B200FEM_ELEM_HEX)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
   if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn) return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
-  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_MOONEYRIVLIN || !params)
+  if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_STVK || !params)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
   if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
   ModelDesc m;
@@ -799,7 +799,7 @@ int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double
   m.fixed.assign(n_nodes, 0);
   if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
   m.mat_kind = mat_kind;
-  const int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_NEOHOOKEAN ? 2 : 8;
+  const int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_MOONEYRIVLIN ? 8 : 2;
   std::copy(params, params + np, m.mat_params);
   m.density = density;
   m.incomp_request = incomp;

@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/b200fem.h"
+
 namespace b200fem {
 
 template <typename T>
@@ -214,6 +216,58 @@ __device__ __forceinline__ void d_add_product4(T* D, T s, const T* A) {
   D[35] += (s00 * a22 + s02 * a02) * T(0.5);
 }
 
+// TensorUtils.addSymmetricTensorProduct4 (TensorUtils.java:674-716): upper
+// part; the caller mirrors it afterwards.
+template <typename T>
+__device__ __forceinline__ void d_add_sym_product4(T* D, T s, const T* A, const T* B) {
+  T a00 = s * A[0], a11 = s * A[1], a22 = s * A[2], a01 = s * A[3], a12 = s * A[4], a02 = s * A[5];
+  T b00 = B[0], b11 = B[1], b22 = B[2], b01 = B[3], b12 = B[4], b02 = B[5];
+  D[0] += T(2) * a00 * b00; D[1] += T(2) * a01 * b01; D[2] += T(2) * a02 * b02;
+  D[3] += a01 * b00 + a00 * b01; D[4] += a02 * b01 + a01 * b02; D[5] += a02 * b00 + a00 * b02;
+  D[7] += T(2) * a11 * b11; D[8] += T(2) * a12 * b12;
+  D[9] += a11 * b01 + a01 * b11; D[10] += a12 * b11 + a11 * b12; D[11] += a12 * b01 + a01 * b12;
+  D[14] += T(2) * a22 * b22;
+  D[15] += a12 * b02 + a02 * b12; D[16] += a22 * b12 + a12 * b22; D[17] += a22 * b02 + a02 * b22;
+  D[21] += T(0.5) * (a11 * b00 + T(2) * a01 * b01 + a00 * b11);
+  D[22] += T(0.5) * (a12 * b01 + a11 * b02 + a02 * b11 + a01 * b12);
+  D[23] += T(0.5) * (a12 * b00 + a02 * b01 + a01 * b02 + a00 * b12);
+  D[28] += T(0.5) * (a22 * b11 + T(2) * a12 * b12 + a11 * b22);
+  D[29] += T(0.5) * (a22 * b01 + a12 * b02 + a02 * b12 + a01 * b22);
+  D[35] += T(0.5) * (a22 * b00 + T(2) * a02 * b02 + a00 * b22);
+}
+
+// StVenantKirchoffMaterial.computeStressAndTangent
+// (StVenantKirchoffMaterial.java:136-164), the FEBio form:
+// sigma = ((lam tr E - mu)/J) B + (mu/J) B^2 with tr E = (tr B - 3)/2;
+// D = (lam/J) B(x)B + (mu/J) symmetric4(B, B).  D may be null.
+template <typename T>
+__device__ inline void stvk_point(T* sig, T* D, T E, T nu, const T* F, T J) {
+  const T mu = E / (T(2) * (T(1) + nu));
+  const T lam = (E * nu) / ((T(1) - T(2) * nu) * (T(1) + nu));
+  T B[6], B2[6];
+  left_cauchy_green(B, F);
+  const T tr = T(0.5) * (B[0] + B[1] + B[2] - T(3));
+  B2[0] = B[0] * B[0] + B[3] * B[3] + B[5] * B[5];
+  B2[1] = B[3] * B[3] + B[1] * B[1] + B[4] * B[4];
+  B2[2] = B[5] * B[5] + B[4] * B[4] + B[2] * B[2];
+  B2[3] = B[0] * B[3] + B[3] * B[1] + B[5] * B[4];
+  B2[4] = B[3] * B[5] + B[1] * B[4] + B[4] * B[2];
+  B2[5] = B[0] * B[5] + B[3] * B[4] + B[5] * B[2];
+  const T cb = (lam * tr - mu) / J, cb2 = mu / J;
+#pragma unroll
+  for (int i = 0; i < 6; i++) sig[i] = cb * B[i] + cb2 * B2[i];
+  if (D) {
+#pragma unroll
+    for (int i = 0; i < 36; i++) D[i] = T(0);
+    d_add_product(D, lam / J, B);
+    d_add_sym_product4(D, mu / J, B, B);
+#pragma unroll
+    for (int i = 1; i < 6; i++)
+#pragma unroll
+      for (int j = 0; j < i; j++) D[6 * i + j] = D[6 * j + i];
+  }
+}
+
 // MooneyRivlinMaterial.computeDevStressAndTangent (MooneyRivlinMaterial.java:344-431)
 // plus the pressure terms of IncompressibleMaterialBase.computeStressAndTangent
 // (IncompressibleMaterialBase.java:249-260).  mp = {c10, c01, c11, c20, c02,
@@ -368,6 +422,15 @@ __device__ __forceinline__ void add_stress_force(T* f, const T* g, const T* s, T
   f[0] += gx * s[0] + gy * s[3] + gz * s[5];
   f[1] += gy * s[1] + gx * s[3] + gz * s[4];
   f[2] += gz * s[2] + gy * s[4] + gx * s[5];
+}
+
+// Stress and full tangent of the general-tangent materials (MooneyRivlin
+// with its pressure p, StVenantKirchhoff) at one point; mp holds the model's
+// material parameters.
+template <int MAT, typename T>
+__device__ __forceinline__ void material_point(T* sig, T* D, const T* mp, const T* F, T J, T p) {
+  if constexpr (MAT == B200FEM_MAT_STVK) stvk_point<T>(sig, D, mp[0], mp[1], F, J);
+  else mooneyrivlin_point<T>(sig, D, mp, F, J, p);
 }
 
 }  // namespace b200fem

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
       T mpt[8];
 #pragma unroll
       for (int i = 0; i < 8; i++) mpt[i] = (T)mp[i];
-      mooneyrivlin_point<T>(ssig[t], sD[t], mpt, F, detF, pr);
+      material_point<MAT, T>(ssig[t], sD[t], mpt, F, detF, pr);
     }
   }
   warp_record_det(a.flags, a.mindet, mydet, myinv);
@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
         }
       }
       double D[36];
-      mooneyrivlin_point<double>(sig, D, mp, F, detF, pr);
+      material_point<MAT, double>(sig, D, mp, F, detF, pr);
     }
 #pragma unroll
     for (int n = 0; n < NEN; n++) {
@@ -863,7 +863,7 @@ __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
       double pr = 0;
       if constexpr (NODAL) pr = 0.25 * (a.node_p[nd[0]] + a.node_p[nd[1]] + a.node_p[nd[2]] + a.node_p[nd[3]]);
       double D[36];
-      mooneyrivlin_point<double>(sig, D, mp, F, detF, pr);
+      material_point<MAT, double>(sig, D, mp, F, detF, pr);
 #pragma unroll
       for (int i = 0; i < 36; i++) Dt[i] = (T)D[i];
     }
@@ -1043,7 +1043,7 @@ __global__ void __launch_bounds__(256) fused_block_kernel(FusedArgs a) {
       T mpt[8];
 #pragma unroll
       for (int i = 0; i < 8; i++) mpt[i] = (T)mp[i];
-      mooneyrivlin_point<T>(ssig[t], sD[t], mpt, F, detF, T(0));
+      material_point<MAT, T>(ssig[t], sD[t], mpt, F, detF, T(0));
     }
   }
   __syncthreads();
@@ -1138,13 +1138,18 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   // per SM and fewer idle threads in the pair stage on small groups
   constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : 32, NH_S = NH_L / 2;
   constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : 16, MR_S = MR_L / 2;
-  constexpr int NH = B200FEM_MAT_NEOHOOKEAN, MR = B200FEM_MAT_MOONEYRIVLIN;
+  // StVenantKirchhoff has the general 6x6 tangent: MooneyRivlin's tiles
+  constexpr int NH = B200FEM_MAT_NEOHOOKEAN, MR = B200FEM_MAT_MOONEYRIVLIN, SV = B200FEM_MAT_STVK;
   cudaStream_t st = eng.stream;
   if (ne < 0) {  // preparation: both tiles
     cudaError_t e;
     if (g.mat_kind == NH) {
       e = launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
       return e != cudaSuccess ? e : launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st);
+    }
+    if (g.mat_kind == SV) {
+      e = launch_nonlinear<TYPE, SV, false, T, MR_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, SV, false, T, MR_S>(a, ne, st);
     }
     if (g.nodal) {
       e = launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
@@ -1158,12 +1163,16 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   if (TYPE == B200FEM_ELEM_TET && !eng.elem_staged) {
     // one thread per tetrahedron (FP64 forces in the same pass)
     if (g.mat_kind == NH) return launch_tet<NH, false, T>(a, ne, st);
+    if (g.mat_kind == SV) return launch_tet<SV, false, T>(a, ne, st);
     if (g.nodal) return launch_tet<MR, true, T>(a, ne, st);
     return launch_tet<MR, false, T>(a, ne, st);
   }
   if (g.mat_kind == NH) {
     e = small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
     if (e == cudaSuccess && fp32) e = launch_force<TYPE, NH, false>(a, ne, st);
+  } else if (g.mat_kind == SV) {
+    e = small ? launch_nonlinear<TYPE, SV, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, SV, false, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, SV, false>(a, ne, st);
   } else if (g.nodal) {
     e = small ? launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
     if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, true>(a, ne, st);
@@ -1364,7 +1373,7 @@ __global__ void __launch_bounds__(128) elem_kv_kernel(ElemArgs a, const double* 
     const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
     double sig[6], D[36], ca = 0, cb = 0;
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) neohookean_point<double>(sig, &ca, &cb, mp[0], mp[1], F, detF);
-    else mooneyrivlin_point<double>(sig, D, mp, F, detF, 0.0);
+    else material_point<MAT, double>(sig, D, mp, F, detF, 0.0);
     // L = sum_b v_b g_b^T (velocities of fixed nodes are zero)
     double g[NEN][3], L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll

@@ -50,6 +50,22 @@ class NeoHookeanMaterial:
 
 
 @dataclass
+class StVenantKirchoffMaterial:
+    """StVenantKirchoffMaterial(E, nu) (StVenantKirchoffMaterial.java:60-64):
+    the reference's FEBio form, sigma = ((lam trE - mu)/J) B + (mu/J) B^2."""
+    E: float = 500000.0
+    nu: float = 0.33
+
+    kind = L.MAT_STVK
+
+    def params(self):
+        return [self.E, self.nu]
+
+    def isIncompressible(self):
+        return False
+
+
+@dataclass
 class MooneyRivlinMaterial:
     """MooneyRivlinMaterial(c10, c01, c11, c20, c02, kappa)
     (MooneyRivlinMaterial.java:98-108); bulk potential QUADRATIC by default

@@ -56,6 +56,8 @@ extern "C" {
 /* materials (parameter layout of b200fem_set_material) */
 #define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */
 #define B200FEM_MAT_NEOHOOKEAN 1   /* {E, nu}: NeoHookeanMaterial */
+#define B200FEM_MAT_STVK 3         /* {E, nu}: StVenantKirchoffMaterial (the reference's FEBio
+                                       form, StVenantKirchoffMaterial.java:136-164) */
 #define B200FEM_MAT_MOONEYRIVLIN 2 /* {c10, c01, c11, c20, c02, kappa, jlimit,
                                       bulk_potential(0 quadratic, 1 log)} */
 

@@ -27,7 +27,7 @@
 namespace {
 
 enum { ELEM_TET = 0, ELEM_HEX = 1 };
-enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2 };
+enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2, MAT_STVK = 3 };
 enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
 
 // ---------------------------------------------------------------------------
@@ -409,10 +409,67 @@ static void mooneyrivlin(double* sig, double* D, const Material& m, const double
   sig[0] += p; sig[1] += p; sig[2] += p;
 }
 
+// TensorUtils.addSymmetricTensorProduct4 (TensorUtils.java:674-716): upper part
+static void add_sym_tensor_product4(double* D, double s, const double* A6, const double* B6) {
+  const double a00 = s * A6[0], a11 = s * A6[1], a22 = s * A6[2], a01 = s * A6[3], a12 = s * A6[4],
+               a02 = s * A6[5];
+  const double b00 = B6[0], b11 = B6[1], b22 = B6[2], b01 = B6[3], b12 = B6[4], b02 = B6[5];
+  D[0] += 2 * a00 * b00;
+  D[1] += 2 * a01 * b01;
+  D[2] += 2 * a02 * b02;
+  D[3] += a01 * b00 + a00 * b01;
+  D[4] += a02 * b01 + a01 * b02;
+  D[5] += a02 * b00 + a00 * b02;
+  D[7] += 2 * a11 * b11;
+  D[8] += 2 * a12 * b12;
+  D[9] += a11 * b01 + a01 * b11;
+  D[10] += a12 * b11 + a11 * b12;
+  D[11] += a12 * b01 + a01 * b12;
+  D[14] += 2 * a22 * b22;
+  D[15] += a12 * b02 + a02 * b12;
+  D[16] += a22 * b12 + a12 * b22;
+  D[17] += a22 * b02 + a02 * b22;
+  D[21] += 0.5 * (a11 * b00 + 2 * a01 * b01 + a00 * b11);
+  D[22] += 0.5 * (a12 * b01 + a11 * b02 + a02 * b11 + a01 * b12);
+  D[23] += 0.5 * (a12 * b00 + a02 * b01 + a01 * b02 + a00 * b12);
+  D[28] += 0.5 * (a22 * b11 + 2 * a12 * b12 + a11 * b22);
+  D[29] += 0.5 * (a22 * b01 + a12 * b02 + a02 * b12 + a01 * b22);
+  D[35] += 0.5 * (a22 * b00 + 2 * a02 * b02 + a00 * b22);
+}
+
+// StVenantKirchoffMaterial.computeStressAndTangent
+// (StVenantKirchoffMaterial.java:136-164): FEBio's form
+// sigma = ((lam trE - mu)/J) B + (mu/J) B^2, trE = (tr B - 3)/2;
+// D = (lam/J) B(x)B (TensorUtils.addTensorProduct(D, s, B, B), :401-456) +
+// (mu/J) addSymmetricTensorProduct4(B, B), then setLowerToUpper.
+static void stvk(double* sig, double* D, const Material& m, const double* F, double J) {
+  const double G = m.E / (2 * (1 + m.nu));
+  const double lam = (m.E * m.nu) / ((1 - 2 * m.nu) * (1 + m.nu));
+  const double mu = G;
+  double B6[6];
+  left_cauchy_green(B6, F);
+  const double tr = 0.5 * (B6[0] + B6[1] + B6[2] - 3);
+  // myB2.mulTransposeLeft(myB): B^T B = B B for symmetric B
+  double Bf[9];
+  sym_from6(Bf, B6);
+  double B2f[9];
+  mul3(B2f, Bf, Bf);
+  const double B26[6] = {B2f[0], B2f[4], B2f[8], B2f[1], B2f[5], B2f[2]};
+  for (int i = 0; i < 6; i++) sig[i] = ((lam * tr - mu) / J) * B6[i];
+  for (int i = 0; i < 6; i++) sig[i] += (mu / J) * B26[i];
+  if (D) {
+    for (int i = 0; i < 36; i++) D[i] = 0;
+    add_tensor_product(D, lam / J, B6);
+    add_sym_tensor_product4(D, mu / J, B6, B6);
+    set_lower_to_upper(D);
+  }
+}
+
 static void material_stress_tangent(double* sig, double* D, const Material& m, const double* F,
                                     double J, double p) {
   if (m.kind == MAT_NEOHOOKEAN) neohookean(sig, D, m, F, J);
   else if (m.kind == MAT_MOONEYRIVLIN) mooneyrivlin(sig, D, m, F, J, p);
+  else if (m.kind == MAT_STVK) stvk(sig, D, m, F, J);
   else {
     // linear small-strain (non-corotated) stress, used only by point tests:
     // LinearMaterialBase.computeStressAndTangent with R = null, corotated off
@@ -1122,7 +1179,7 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   m->mat.kind = mat_kind;
   if (mat_kind == MAT_LINEAR) {
     m->mat.E = mat_params[0]; m->mat.nu = mat_params[1]; m->mat.corotated = (int)mat_params[2];
-  } else if (mat_kind == MAT_NEOHOOKEAN) {
+  } else if (mat_kind == MAT_NEOHOOKEAN || mat_kind == MAT_STVK) {
     m->mat.E = mat_params[0]; m->mat.nu = mat_params[1];
   } else {
     m->mat.c10 = mat_params[0]; m->mat.c01 = mat_params[1]; m->mat.c11 = mat_params[2];
@@ -1365,7 +1422,7 @@ void orc_material_eval(int mat_kind, const double* mat_params, const double* F, 
   Material mt;
   mt.kind = mat_kind;
   if (mat_kind == MAT_LINEAR) { mt.E = mat_params[0]; mt.nu = mat_params[1]; }
-  else if (mat_kind == MAT_NEOHOOKEAN) { mt.E = mat_params[0]; mt.nu = mat_params[1]; }
+  else if (mat_kind == MAT_NEOHOOKEAN || mat_kind == MAT_STVK) { mt.E = mat_params[0]; mt.nu = mat_params[1]; }
   else {
     mt.c10 = mat_params[0]; mt.c01 = mat_params[1]; mt.c11 = mat_params[2]; mt.c20 = mat_params[3];
     mt.c02 = mat_params[4]; mt.kappa = mat_params[5]; mt.jlimit = mat_params[6];

@@ -21,7 +21,7 @@ REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
 REF_SOURCE_ROOT = "/root/reference"
 
 ELEM_TET, ELEM_HEX = 0, 1
-MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN = 0, 1, 2
+MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

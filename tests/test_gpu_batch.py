@@ -64,10 +64,11 @@ def test_pack_result_equals_alone(beams, precision):
 
 def test_pack_of_mixed_materials(b200, oracle):
     """Models with different materials form element groups inside one pack."""
-    from artisynth_core_b200.femmodel import MooneyRivlinMaterial, NeoHookeanMaterial, LinearMaterial
+    from artisynth_core_b200.femmodel import (MooneyRivlinMaterial, NeoHookeanMaterial, LinearMaterial,
+                                              StVenantKirchoffMaterial)
     wls = [W.small_tet_beam(NeoHookeanMaterial(3e4, 0.4)), W.small_tet_beam(LinearMaterial(2e4, 0.3, True)),
            W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
-           W.small_tet_beam(NeoHookeanMaterial(8e4, 0.3))]
+           W.small_tet_beam(NeoHookeanMaterial(8e4, 0.3)), W.small_tet_beam(StVenantKirchoffMaterial(4e4, 0.3))]
     for w in wls:
         w.build_mesh()
     pack = FemPack([w.model() for w in wls], precision=L.PREC_FP64)

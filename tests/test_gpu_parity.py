@@ -13,7 +13,7 @@ import pytest
 from artisynth_core_b200 import _lib as L
 from artisynth_core_b200 import workloads as W
 from artisynth_core_b200.femmodel import (LinearMaterial, MechSystemSolver, MooneyRivlinMaterial,
-                                          NeoHookeanMaterial)
+                                          NeoHookeanMaterial, StVenantKirchoffMaterial)
 
 from helpers import deformed, oracle_model, rel_err
 
@@ -30,6 +30,8 @@ def _cases():
         "linear_corotated_hex": W.small_hex_beam(LinearMaterial(2e4, 0.3, True)),
         "neohookean_tet": W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33)),
         "neohookean_hex": W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "stvk_tet": W.small_tet_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "stvk_hex": W.small_hex_beam(StVenantKirchoffMaterial(5e4, 0.3)),
         "mooneyrivlin_tet_off": W.small_tet_beam(MooneyRivlinMaterial(1e4, 2e3, 0, 0, 0, 1e5)),
         "mooneyrivlin_hex_full": W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 30, 486, 20, 10370)),
         "mooneyrivlin_tet_nodal": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
@@ -134,7 +136,7 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
     assert x[:, 2].min() < -0.05  # the beam sags (FemModel3dTest.runCorotatedBeamStep)
 
 
-@pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex", "mooneyrivlin_tet_off",
+@pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex", "stvk_tet", "stvk_hex", "mooneyrivlin_tet_off",
                                   "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full",
                                   "mooneyrivlin_tet_nodal", "mooneyrivlin_hex_nodal",
                                   "mooneyrivlin_tet_nodal_log"])
@@ -277,7 +279,7 @@ def test_fused_assembly_matches_gather(name, precision, cases):
 
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
-@pytest.mark.parametrize("name", ["neohookean_tet", "mooneyrivlin_tet_off", "mooneyrivlin_tet_nodal"])
+@pytest.mark.parametrize("name", ["neohookean_tet", "stvk_tet", "mooneyrivlin_tet_off", "mooneyrivlin_tet_nodal"])
 def test_tet_kernels_agree(name, precision, cases):
     """The one-thread-per-tetrahedron kernel and the shared-memory staged
     kernel give the same steps (same formulas; the former keeps kinematics

@@ -10,7 +10,8 @@ and adds it into the CRS values (FP64 atomics).
 
 That kernel, compiled from the reference source into oracle/_ref/ (`make -C
 oracle ref`), is fed the oracle's integration-point data for every (element,
-point, node pair) of NeoHookean tet and hex beams at deformed positions.  Its
+point, node pair) of NeoHookean tet and hex and StVenantKirchhoff hex beams at
+deformed positions.  Its
 CRS values must equal
 * the engine's full-partition CRS export (b200fem_update_stress_stiffness)
   within the parity bar, 1e-10 of the largest entry, and
@@ -30,7 +31,7 @@ within 1e-10.
 import numpy as np
 import pytest
 
-from artisynth_core_b200.femmodel import LinearMaterial, NeoHookeanMaterial
+from artisynth_core_b200.femmodel import LinearMaterial, NeoHookeanMaterial, StVenantKirchoffMaterial
 from artisynth_core_b200 import workloads as W
 from oracle import oracle as O
 
@@ -97,13 +98,15 @@ def _reference_crs(R, desc, nnz):
     return crs.cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex"])
+@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex"])
 def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     R = _ref_lib()
     if case == "neohookean_tet":
         wl = W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33))
-    else:
+    elif case == "neohookean_hex":
         wl = W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45))
+    else:
+        wl = W.small_hex_beam(StVenantKirchoffMaterial(5e4, 0.3))
     wl.build_mesh()
     om = oracle_model(oracle, wl)
     x = deformed(wl.rest, seed=5)

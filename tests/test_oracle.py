@@ -118,7 +118,7 @@ def _fd_tangent(oracle, kind, params, F, p=0.0, h=1e-8):
 
 
 @pytest.mark.parametrize("kind,params", [(1, [1e4, 0.49]), (2, [1.2, 3.4, 0, 0, 0, 1000, 0, 0]),
-                                         (2, [1037, 0, 0, 486, 0, 10370, 0, 0])])
+                                         (2, [1037, 0, 0, 486, 0, 10370, 0, 0]), (3, [1e4, 0.3])])
 def test_material_tangent_matches_fd(oracle, kind, params):
     # The reference's MooneyRivlin tangent is FD-consistent for c10, c01 and
     # c20 (the terms its own tests and regression script use); its c11 and
@@ -144,7 +144,8 @@ def test_polar_rotation(oracle):
 
 
 @pytest.mark.parametrize("kind,params,etype", [(0, [5e4, 0.3, 0], 0), (1, [5e4, 0.45], 0),
-                                               (1, [5e4, 0.45], 1), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1)])
+                                               (1, [5e4, 0.45], 1), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1),
+                                               (3, [5e4, 0.3], 0), (3, [5e4, 0.3], 1)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
