@@ -242,10 +242,11 @@ int build_pack(Engine& eng) {
     g.mat_kind = eng.models[m].mat_kind;
     g.corotated = (g.mat_kind == B200FEM_MAT_LINEAR) ? (eng.models[m].mat_params[2] != 0) : 0;
     g.nodal = eng.hosts[m].incomp == B200FEM_INCOMP_NODAL;
+    g.elem_inc = eng.hosts[m].incomp == B200FEM_INCOMP_ELEMENT;
     if (!eng.groups.empty()) {
       ElemGroup& last = eng.groups.back();
       if (last.mat_kind == g.mat_kind && last.corotated == g.corotated && last.nodal == g.nodal &&
-          last.e1 == g.e0) {
+          last.elem_inc == g.elem_inc && last.e1 == g.e0) {
         last.e1 = g.e1;
         continue;
       }
@@ -256,7 +257,7 @@ int build_pack(Engine& eng) {
   // chunk's shared memory, and the contribution lists re-indexed to them
   std::vector<int> chunk_row, chunk_eptr, chunk_elem, contrib_loc;
   eng.fused = false;
-  if (eng.opt_fused == 1 && eng.groups.size() == 1 && !eng.groups[0].nodal &&
+  if (eng.opt_fused == 1 && eng.groups.size() == 1 && !eng.groups[0].nodal && !eng.groups[0].elem_inc &&
       (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN || eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN)) {
     const size_t per = fused_elem_bytes(eng.elem_type, eng.groups[0].mat_kind, eng.precision == B200FEM_PREC_MIXED);
     const int emax = (int)(fused_smem_budget(eng.elem_type) / per);
@@ -573,6 +574,21 @@ int build_pack(Engine& eng) {
   }
   CK(upload(eng, &d.mat, mat));
   CK(upload(eng, &d.step, step));
+  {
+    // ELEMENT soft incompressibility: rest volume per element of the pack
+    bool any_elem = false;
+    for (auto& h : eng.hosts) any_elem |= (h.incomp == B200FEM_INCOMP_ELEMENT);
+    if (any_elem) {
+      std::vector<double> erv((size_t)E, 1.0);
+      for (int m = 0; m < M; m++)
+        std::copy(eng.hosts[m].rest_vol.begin(), eng.hosts[m].rest_vol.end(), erv.begin() + eng.elem_off[m]);
+      CK(upload(eng, &d.elem_rest_vol, erv));
+      CK(dalloc(eng, &d.elem_p, (size_t)E));
+      CK(dalloc(eng, &d.elem_r, (size_t)E));
+      CK(cudaMemset(d.elem_p, 0, sizeof(double) * (size_t)E));
+      CK(cudaMemset(d.elem_r, 0, sizeof(double) * (size_t)E));
+    }
+  }
   if (any_nodal) {
     d.has_nodal = 1;
     CK(upload(eng, &d.node_rest_vol, node_rest_vol));
@@ -604,6 +620,7 @@ int build_pack(Engine& eng) {
     // refinement sweeps (mixed form): FP64 residual, correction, and the
     // correction solves' own per-model results
     eng.refine_ok = eng.precision == B200FEM_PREC_MIXED && eng.groups.size() == 1 && !eng.groups[0].nodal &&
+                    !eng.groups[0].elem_inc &&
                     (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN ||
                      eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN);
     if (eng.refine_ok) {

@@ -124,6 +124,11 @@ struct DevPack {
   int* dil_ptr = nullptr;      // nnzb+1 dilational contributions per block
   int* dil_idx = nullptr;      // (divblk row i, divblk row j, node n) triples
   int has_nodal = 0;
+  // ELEMENT soft incompressibility: per element rest volume, pressure and
+  // Rinv (effective modulus / rest volume)
+  double* elem_rest_vol = nullptr;
+  double* elem_p = nullptr;
+  double* elem_r = nullptr;
   // reductions / PCG control
   double* partials = nullptr;  // [2][n_pieces][4] (double-buffered by phase)
   int* piece_row = nullptr;    // n_pieces+1
@@ -161,6 +166,7 @@ struct ElemGroup {
   int mat_kind = B200FEM_MAT_LINEAR;
   int corotated = 1;
   int nodal = 0;
+  int elem_inc = 0;  // ELEMENT soft incompressibility (one pressure per element)
 };
 
 struct Engine {

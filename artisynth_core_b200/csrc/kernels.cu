@@ -128,6 +128,9 @@ __device__ __forceinline__ void warp_record_det(int* flags, long long* mindet, d
   }
 }
 
+// soft incompressibility of an element group (template argument INC)
+constexpr int kIncOff = 0, kIncNodal = 1, kIncElement = 2;
+
 struct ElemArgs;
 __device__ bool block_inactive(const ElemArgs& a, int ebase, int epb);
 
@@ -144,6 +147,8 @@ struct ElemArgs {
   const int* sidx;
   const double* mat;       // per model kMatParams
   const double* node_p;    // NODAL pressures (or null)
+  const double* elem_p;    // ELEMENT pressures (or null)
+  const double* elem_r;    // ELEMENT Rinv = effective modulus / rest volume (or null)
   const int* active;       // per model: 0 = left out of this assembly (or null: all)
   void* elemK;             // T* E*npair*9
   void* elemF;             // T* E*nen*3
@@ -181,7 +186,7 @@ struct ElemSmem {
   }
 };
 
-template <int TYPE, int MAT, bool NODAL, typename T, int EPB>
+template <int TYPE, int MAT, int INC, typename T, int EPB>
 __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
   using SM = ElemSmem<TYPE, MAT, T, EPB>;
   constexpr int NEN = SM::NEN;
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
       sD[t][1] = bb;
     } else {
       T pr = T(0);
-      if constexpr (NODAL) {
+      if constexpr (INC == kIncNodal) {
         if (TYPE == B200FEM_ELEM_TET) {
           double s = 0;
 #pragma unroll
@@ -275,6 +280,8 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
         } else {
           pr = (T)a.node_p[snode[el][k]];
         }
+      } else if constexpr (INC == kIncElement) {
+        pr = (T)a.elem_p[e];
       }
       T mpt[8];
 #pragma unroll
@@ -306,6 +313,25 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
         else
           add_bdb(K, sg[s][ia], sD[s], sg[s][ib], sdv[s]);
         add_geometric(K, sg[s][ia], ssig[s], sg[s][ib], sdv[s]);
+      }
+      if constexpr (INC == kIncElement) {
+        // ELEMENT dilational stiffness Rinv c_a c_b^T, c = sum_k GNx dv
+        // (FemModel3d.java:3650-3663, FemUtilities.addToIncompressConstraints)
+        T ca[3] = {T(0), T(0), T(0)}, cb[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int k = 0; k < NIP; k++) {
+          const int s = el * NIP + k;
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            ca[c] += sg[s][ia][c] * sdv[s];
+            cb[c] += sg[s][ib][c] * sdv[s];
+          }
+        }
+        const T r = (T)a.elem_r[e];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) K[3 * i + j] += r * ca[i] * cb[j];
       }
       T* out = elemK + ((size_t)e * NPAIR + w) * 9;
 #pragma unroll
@@ -670,6 +696,8 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.sidx = d.sidx;
   a.mat = d.mat;
   a.node_p = d.node_p;
+  a.elem_p = d.elem_p;
+  a.elem_r = d.elem_r;
   a.elemK = fp32 ? (void*)d.elemK_f : (void*)d.elemK;
   a.elemF = (void*)d.elemF;  // nodal forces are FP64 in both forms
   a.flags = d.flags;
@@ -678,10 +706,10 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   return a;
 }
 
-template <int TYPE, int MAT, bool NODAL, typename T, int EPB>
+template <int TYPE, int MAT, int INC, typename T, int EPB>
 static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) {
   using SM = ElemSmem<TYPE, MAT, T, EPB>;
-  auto kern = elem_nonlinear_kernel<TYPE, MAT, NODAL, T, EPB>;
+  auto kern = elem_nonlinear_kernel<TYPE, MAT, INC, T, EPB>;
   const size_t smem = SM::bytes();
   // the opt-in size is a per-function attribute: set it once per process
   // (it is not a stream operation, so it must not run inside graph capture)
@@ -705,7 +733,7 @@ static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) 
 // (tets) or per integration point, the 8 points of a hex reduced over 8
 // consecutive lanes in a fixed butterfly order.
 // ---------------------------------------------------------------------------
-template <int TYPE, int MAT, bool NODAL>
+template <int TYPE, int MAT, int INC>
 __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
   constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
   constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
@@ -750,7 +778,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
       neohookean_point<double>(sig, &aa, &bb, mp[0], mp[1], F, detF);
     } else {
       double pr = 0;
-      if constexpr (NODAL) {
+      if constexpr (INC == kIncNodal) {
         if (TYPE == B200FEM_ELEM_TET) {
           double s = 0;
 #pragma unroll
@@ -759,6 +787,8 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
         } else {
           pr = a.node_p[nodes[k]];
         }
+      } else if constexpr (INC == kIncElement) {
+        pr = a.elem_p[e];
       }
       double D[36];
       material_point<MAT, double>(sig, D, mp, F, detF, pr);
@@ -804,7 +834,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
 template <typename T>
 __host__ __device__ constexpr int tet_wpb() { return sizeof(T) == 8 ? 1 : 2; }
 
-template <int MAT, bool NODAL, typename T>
+template <int MAT, int INC, typename T>
 __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
   constexpr int NPAIR = 10, KW = NPAIR * 9, FW = 12, WPB = tet_wpb<T>();
   __shared__ T sk[WPB][32 * KW];
@@ -861,7 +891,8 @@ __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
       Dt[1] = (T)cb;
     } else {
       double pr = 0;
-      if constexpr (NODAL) pr = 0.25 * (a.node_p[nd[0]] + a.node_p[nd[1]] + a.node_p[nd[2]] + a.node_p[nd[3]]);
+      if constexpr (INC == kIncNodal) pr = 0.25 * (a.node_p[nd[0]] + a.node_p[nd[1]] + a.node_p[nd[2]] + a.node_p[nd[3]]);
+      else if constexpr (INC == kIncElement) pr = a.elem_p[e];
       double D[36];
       material_point<MAT, double>(sig, D, mp, F, detF, pr);
 #pragma unroll
@@ -896,6 +927,14 @@ __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
         if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) add_bdb_iso(K, gt[ia], Dt[0], Dt[1], gt[ib], dvt);
         else add_bdb(K, gt[ia], Dt, gt[ib], dvt);
         add_geometric(K, gt[ia], st, gt[ib], dvt);
+        if constexpr (INC == kIncElement) {
+          // ELEMENT dilational stiffness Rinv (g_a dv)(g_b dv)^T (one point)
+          const T r = (T)(a.elem_r[e] * dv * dv);
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) K[3 * i + j] += r * gt[ia][i] * gt[ib][j];
+        }
 #pragma unroll
         for (int i = 0; i < 9; i++) kout[9 * w + i] = K[i];
       }
@@ -919,18 +958,18 @@ __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
   }
 }
 
-template <int MAT, bool NODAL, typename T>
+template <int MAT, int INC, typename T>
 static cudaError_t launch_tet(const ElemArgs& a, int ne, cudaStream_t st) {
   constexpr int TPB = 32 * tet_wpb<T>();
-  elem_tet_kernel<MAT, NODAL, T><<<(ne + TPB - 1) / TPB, TPB, 0, st>>>(a);
+  elem_tet_kernel<MAT, INC, T><<<(ne + TPB - 1) / TPB, TPB, 0, st>>>(a);
   return cudaGetLastError();
 }
 
-template <int TYPE, int MAT, bool NODAL>
+template <int TYPE, int MAT, int INC>
 static cudaError_t launch_force(const ElemArgs& a, int ne, cudaStream_t st) {
   constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
   const long long threads = (long long)ne * NIP;
-  elem_force_kernel<TYPE, MAT, NODAL><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
+  elem_force_kernel<TYPE, MAT, INC><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1144,41 +1183,50 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   if (ne < 0) {  // preparation: both tiles
     cudaError_t e;
     if (g.mat_kind == NH) {
-      e = launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
-      return e != cudaSuccess ? e : launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st);
+      e = launch_nonlinear<TYPE, NH, kIncOff, T, NH_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, NH, kIncOff, T, NH_S>(a, ne, st);
     }
     if (g.mat_kind == SV) {
-      e = launch_nonlinear<TYPE, SV, false, T, MR_L>(a, ne, st);
-      return e != cudaSuccess ? e : launch_nonlinear<TYPE, SV, false, T, MR_S>(a, ne, st);
+      e = launch_nonlinear<TYPE, SV, kIncOff, T, MR_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, SV, kIncOff, T, MR_S>(a, ne, st);
     }
     if (g.nodal) {
-      e = launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
-      return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st);
+      e = launch_nonlinear<TYPE, MR, kIncNodal, T, MR_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, kIncNodal, T, MR_S>(a, ne, st);
     }
-    e = launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
-    return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st);
+    if (g.elem_inc) {
+      e = launch_nonlinear<TYPE, MR, kIncElement, T, MR_L>(a, ne, st);
+      return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, kIncElement, T, MR_S>(a, ne, st);
+    }
+    e = launch_nonlinear<TYPE, MR, kIncOff, T, MR_L>(a, ne, st);
+    return e != cudaSuccess ? e : launch_nonlinear<TYPE, MR, kIncOff, T, MR_S>(a, ne, st);
   }
   const bool small = eng.elem_tile_small;
   cudaError_t e;
   if (TYPE == B200FEM_ELEM_TET && !eng.elem_staged) {
     // one thread per tetrahedron (FP64 forces in the same pass)
-    if (g.mat_kind == NH) return launch_tet<NH, false, T>(a, ne, st);
-    if (g.mat_kind == SV) return launch_tet<SV, false, T>(a, ne, st);
-    if (g.nodal) return launch_tet<MR, true, T>(a, ne, st);
-    return launch_tet<MR, false, T>(a, ne, st);
+    if (g.mat_kind == NH) return launch_tet<NH, kIncOff, T>(a, ne, st);
+    if (g.mat_kind == SV) return launch_tet<SV, kIncOff, T>(a, ne, st);
+    if (g.nodal) return launch_tet<MR, kIncNodal, T>(a, ne, st);
+    if (g.elem_inc) return launch_tet<MR, kIncElement, T>(a, ne, st);
+    return launch_tet<MR, kIncOff, T>(a, ne, st);
   }
   if (g.mat_kind == NH) {
-    e = small ? launch_nonlinear<TYPE, NH, false, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, false, T, NH_L>(a, ne, st);
-    if (e == cudaSuccess && fp32) e = launch_force<TYPE, NH, false>(a, ne, st);
+    e = small ? launch_nonlinear<TYPE, NH, kIncOff, T, NH_S>(a, ne, st) : launch_nonlinear<TYPE, NH, kIncOff, T, NH_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, NH, kIncOff>(a, ne, st);
   } else if (g.mat_kind == SV) {
-    e = small ? launch_nonlinear<TYPE, SV, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, SV, false, T, MR_L>(a, ne, st);
-    if (e == cudaSuccess && fp32) e = launch_force<TYPE, SV, false>(a, ne, st);
+    e = small ? launch_nonlinear<TYPE, SV, kIncOff, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, SV, kIncOff, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, SV, kIncOff>(a, ne, st);
   } else if (g.nodal) {
-    e = small ? launch_nonlinear<TYPE, MR, true, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, true, T, MR_L>(a, ne, st);
-    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, true>(a, ne, st);
+    e = small ? launch_nonlinear<TYPE, MR, kIncNodal, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, kIncNodal, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, kIncNodal>(a, ne, st);
+  } else if (g.elem_inc) {
+    e = small ? launch_nonlinear<TYPE, MR, kIncElement, T, MR_S>(a, ne, st)
+              : launch_nonlinear<TYPE, MR, kIncElement, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, kIncElement>(a, ne, st);
   } else {
-    e = small ? launch_nonlinear<TYPE, MR, false, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, false, T, MR_L>(a, ne, st);
-    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, false>(a, ne, st);
+    e = small ? launch_nonlinear<TYPE, MR, kIncOff, T, MR_S>(a, ne, st) : launch_nonlinear<TYPE, MR, kIncOff, T, MR_L>(a, ne, st);
+    if (e == cudaSuccess && fp32) e = launch_force<TYPE, MR, kIncOff>(a, ne, st);
   }
   return e;
 }
@@ -1323,6 +1371,72 @@ cudaError_t launch_divblk(Engine& eng) {
     divblk_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
         d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
   return cudaGetLastError();
+}
+
+// ELEMENT soft incompressibility with one pressure value per element (tet
+// and hex), computePressuresAndRinv (FemModel3d.java:2517-2591, npvals == 1):
+// the current volume V (tet: det J / 6, TetElement.computeVolumes; hex: the
+// sum of det J w over the points, FemElement3d.computeVolumes), J = V/V0,
+// p = effectivePressure(kappa, J) and Rinv = effectiveModulus(kappa, J) / V0
+// (IncompressibleMaterialBase.java:116-152), per element of the group.
+template <int TYPE>
+__global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ conn,
+                                        const int* __restrict__ elem_model, const double* __restrict__ x,
+                                        const double* __restrict__ rest_vol, const double* __restrict__ mat,
+                                        double* __restrict__ elem_p, double* __restrict__ elem_r) {
+  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e1) return;
+  const int* nodes = conn + (size_t)e * NEN;
+  double V = 0;
+#pragma unroll
+  for (int q = 0; q < NIP; q++) {
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < NEN; k++) {
+      const double* pk = x + 3 * (size_t)nodes[k];
+      double g0, g1, g2;
+      if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * k]; g1 = c_tet_gns[3 * k + 1]; g2 = c_tet_gns[3 * k + 2]; }
+      else { g0 = c_hex_gns[(q * 8 + k) * 3]; g1 = c_hex_gns[(q * 8 + k) * 3 + 1]; g2 = c_hex_gns[(q * 8 + k) * 3 + 2]; }
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        J[3 * r] += pk[r] * g0;
+        J[3 * r + 1] += pk[r] * g1;
+        J[3 * r + 2] += pk[r] * g2;
+      }
+    }
+    V += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 : det3(J);
+  }
+  const double* mp = mat + (size_t)elem_model[e] * kMatParams;
+  const double K = mp[5], V0 = rest_vol[e], Jp = V / V0;
+  double p, keff;
+  if (mp[7] == 0) {
+    p = K * (Jp - 1);
+    keff = K;
+  } else {
+    p = K * log(Jp) / Jp;
+    keff = K * (1 - log(Jp)) / (Jp * Jp);
+  }
+  elem_p[e] = p;
+  elem_r[e] = keff / V0;
+}
+
+cudaError_t launch_element_pressure(Engine& eng) {
+  DevPack& d = eng.d;
+  for (const ElemGroup& g : eng.groups) {
+    if (!g.elem_inc || g.e1 <= g.e0) continue;
+    const int threads = 128, blocks = (g.e1 - g.e0 + threads - 1) / threads;
+    if (eng.elem_type == B200FEM_ELEM_TET)
+      element_pressure_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.elem_p, d.elem_r);
+    else
+      element_pressure_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
+          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.elem_p, d.elem_r);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // One-time preparation before any stream capture: constant tables and the
@@ -1610,9 +1724,9 @@ static cudaError_t launch_assemble_fused(Engine& eng) {
                 MR = B200FEM_MAT_MOONEYRIVLIN;
   if (ne > 0) {
     if (eng.elem_type == TET)
-      e = g.mat_kind == NH ? launch_force<TET, NH, false>(a, ne, eng.stream) : launch_force<TET, MR, false>(a, ne, eng.stream);
+      e = g.mat_kind == NH ? launch_force<TET, NH, kIncOff>(a, ne, eng.stream) : launch_force<TET, MR, kIncOff>(a, ne, eng.stream);
     else
-      e = g.mat_kind == NH ? launch_force<HEX, NH, false>(a, ne, eng.stream) : launch_force<HEX, MR, false>(a, ne, eng.stream);
+      e = g.mat_kind == NH ? launch_force<HEX, NH, kIncOff>(a, ne, eng.stream) : launch_force<HEX, MR, kIncOff>(a, ne, eng.stream);
   }
   if (e != cudaSuccess) return e;
   return launch_fused_blocks(eng, eng.fused_chunks);
@@ -1627,6 +1741,7 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   if (!want_K && eng.fused) return launch_assemble_fused(eng);
   if ((e = launch_nodal_pressure(eng)) != cudaSuccess) return e;
   if ((e = launch_divblk(eng)) != cudaSuccess) return e;
+  if ((e = launch_element_pressure(eng)) != cudaSuccess) return e;
   for (const ElemGroup& g : eng.groups) {
     if (g.elem_type == B200FEM_ELEM_TET)
       e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);

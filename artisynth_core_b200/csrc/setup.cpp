@@ -209,10 +209,6 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
-  if (method == B200FEM_INCOMP_ELEMENT) {
-    err = "ELEMENT soft incompressibility is not supported (use OFF or NODAL)";
-    return B200FEM_ERR_UNSUPPORTED;
-  }
   h.incomp = method;
 
   // rest data: IntegrationData3d.myInvJ0/myDetJ0 (IntegrationData3d.java:108-111)

@@ -65,7 +65,10 @@ extern "C" {
 #define B200FEM_INCOMP_OFF 0
 #define B200FEM_INCOMP_NODAL 1
 #define B200FEM_INCOMP_AUTO 2
-#define B200FEM_INCOMP_ELEMENT 3 /* resolved by AUTO; not supported */
+#define B200FEM_INCOMP_ELEMENT 3 /* one pressure value per element: p = effective pressure of
+                                    V/V0, dilational stiffness Rinv c_i c_j^T (FemModel3d.java:
+                                    2517-2591, 3650-3663); AUTO picks it when #elements <=
+                                    #active nodes */
 
 /* precision of the engine */
 #define B200FEM_PREC_FP64 0  /* plain FP64 drop-in */

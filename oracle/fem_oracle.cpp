@@ -706,6 +706,8 @@ struct ElemOut {
   double minDetJ = 1e300;
 };
 
+static double current_volume(const Model& m, int e, const double* x);
+
 static void element_update(const Model& m, int e, const double* x, ElemOut& out) {
   const ShapeTable& s = m.sh;
   int nen = m.nen;
@@ -775,6 +777,24 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
   }
   // non-linear path (FemModel3d.java:3443-3631)
   std::vector<double> GNx(nen * 3);
+  // ELEMENT soft incompressibility, one pressure value per element (tet and
+  // hex): computePressuresAndRinv (FemModel3d.java:2517-2591, npvals == 1):
+  // J = V/V0, p = effectivePressure(K, J), Rinv = effectiveModulus(K, J)/V0
+  // (IncompressibleMaterialBase.java:116-152); the constraint vectors
+  // c_i = sum_k GNx_i dv (FemUtilities.addToIncompressConstraints) and the
+  // dilational stiffness Rinv c_i c_j^T (:3650-3663)
+  const bool elem_inc = m.incomp == INCOMP_ELEMENT;
+  double elem_p = 0, elem_rinv = 0;
+  std::vector<double> cst;
+  if (elem_inc) {
+    const double V0 = m.restVol[e];
+    const double Jp = current_volume(m, e, x) / V0;
+    const double K = m.mat.kappa;
+    elem_p = (m.mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
+    const double keff = (m.mat.bulk_potential == 0) ? K : K * (1 - std::log(Jp)) / (Jp * Jp);
+    elem_rinv = keff / V0;
+    cst.assign(nen * 3, 0);
+  }
   for (int k = 0; k < s.nip; k++) {
     const double* GNs = &s.GNs[k * nen * 3];
     double J[9], invJ[9], F[9];
@@ -798,6 +818,10 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       } else {
         pressure = m.nodePressure[nodes[k]];
       }
+    } else if (elem_inc) {
+      pressure = elem_p;
+      for (int n = 0; n < nen; n++)
+        for (int c = 0; c < 3; c++) cst[3 * n + c] += GNx[3 * n + c] * dv;
     }
     double sig[6], D[36];
     material_stress_tangent(sig, D, m.mat, F, detF, pressure);
@@ -822,6 +846,19 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       // divBlk(node_k, node_j) += dv * GNx_j
       for (int j = 0; j < nen; j++)
         for (int c = 0; c < 3; c++) out.div[(k * nen + j) * 3 + c] += dv * GNx[3 * j + c];
+    }
+  }
+  if (elem_inc) {
+    for (int i = 0; i < nen; i++) {
+      int bi = m.sidx[nodes[i]];
+      if (bi == -1) continue;
+      for (int j = 0; j < nen; j++) {
+        int bj = m.sidx[nodes[j]];
+        if (bj < bi) continue;
+        double* Ko = &out.K[(i * nen + j) * 9];
+        for (int r = 0; r < 3; r++)
+          for (int q = 0; q < 3; q++) Ko[3 * r + q] += elem_rinv * cst[3 * i + r] * cst[3 * j + q];
+      }
     }
   }
   if (m.incomp == INCOMP_NODAL && m.type == ELEM_TET) {
@@ -1411,6 +1448,10 @@ int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv,
     } else {
       pressure = m.nodePressure[nodes[k]];
     }
+  } else if (m.incomp == INCOMP_ELEMENT) {
+    const double Jp = current_volume(m, e, x) / m.restVol[e];
+    const double K = m.mat.kappa;
+    pressure = (m.mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
   }
   material_stress_tangent(sig, D, m.mat, F, detF, pressure);
   return nen;

@@ -46,8 +46,8 @@ def build_ref() -> str | None:
 def ref_kernels():
     """ctypes handle of the reference kernels library, or None when it was
     not built.  Entry points used: addMaterialStiffness3_launch
-    (cudssBridgeKernels.cu:244-253) and addLinearElasticStiffness3Element_launch
-    (:518-530)."""
+    (cudssBridgeKernels.cu:244-253), addLinearElasticStiffness3Element_launch
+    (:518-530) and addDilationalStiffness3Element_launch (:725-739)."""
     if not os.path.exists(REF_LIB_PATH):
         return None
     R = ctypes.CDLL(REF_LIB_PATH)
@@ -56,6 +56,8 @@ def ref_kernels():
     R.addMaterialStiffness3_launch.restype = None
     R.addLinearElasticStiffness3Element_launch.argtypes = [ctypes.c_int] + [vp] * 9 + [ctypes.c_double, vp, vp]
     R.addLinearElasticStiffness3Element_launch.restype = None
+    R.addDilationalStiffness3Element_launch.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, vp, vp]
+    R.addDilationalStiffness3Element_launch.restype = None
     return R
 
 

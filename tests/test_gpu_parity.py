@@ -37,6 +37,11 @@ def _cases():
         "mooneyrivlin_tet_nodal": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
         "mooneyrivlin_hex_nodal": W.small_hex_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
         "mooneyrivlin_tet_nodal_log": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5, 0.0, 1)),
+        # ELEMENT soft incompressibility: AUTO picks it for the hex beam
+        # (16 elements <= 36 active nodes); requested for the tet beam
+        "mooneyrivlin_hex_element": W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_hex_element_log": W.small_hex_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
+        "mooneyrivlin_tet_element": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
     }
 
 
@@ -52,6 +57,7 @@ def cases(b200):
         _incomp_off(cs[k])
     # more hexes than active nodes is needed for AUTO -> NODAL; request it
     cs["mooneyrivlin_hex_nodal"].incomp = L.INCOMP_NODAL
+    cs["mooneyrivlin_tet_element"].incomp = L.INCOMP_ELEMENT
     return cs
 
 
@@ -139,7 +145,8 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
 @pytest.mark.parametrize("name", ["neohookean_tet", "neohookean_hex", "stvk_tet", "stvk_hex", "mooneyrivlin_tet_off",
                                   "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full",
                                   "mooneyrivlin_tet_nodal", "mooneyrivlin_hex_nodal",
-                                  "mooneyrivlin_tet_nodal_log"])
+                                  "mooneyrivlin_tet_nodal_log", "mooneyrivlin_hex_element",
+                                  "mooneyrivlin_hex_element_log", "mooneyrivlin_tet_element"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)
@@ -279,7 +286,8 @@ def test_fused_assembly_matches_gather(name, precision, cases):
 
 
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
-@pytest.mark.parametrize("name", ["neohookean_tet", "stvk_tet", "mooneyrivlin_tet_off", "mooneyrivlin_tet_nodal"])
+@pytest.mark.parametrize("name", ["neohookean_tet", "stvk_tet", "mooneyrivlin_tet_off", "mooneyrivlin_tet_nodal",
+                                  "mooneyrivlin_tet_element"])
 def test_tet_kernels_agree(name, precision, cases):
     """The one-thread-per-tetrahedron kernel and the shared-memory staged
     kernel give the same steps (same formulas; the former keeps kinematics

@@ -17,6 +17,10 @@ CRS values must equal
   within the parity bar, 1e-10 of the largest entry, and
 * the oracle's own assembly within 1e-12 (same arithmetic, summation order
   differs through the atomics).
+For a MooneyRivlin hex beam whose AUTO soft incompressibility resolves to
+ELEMENT, the descriptors carry the element pressure and the reference's
+addDilationalStiffness3ElementKernel (:658-723) adds Rinv c_i c_j^T from the
+element constraint vectors.
 This pins the element-tangent assembly (FemUtilities.addMaterialStiffness /
 addGeometricStiffness, FemUtilities.java:78-144) to the reference's code,
 not only to its restatement.
@@ -31,7 +35,8 @@ within 1e-10.
 import numpy as np
 import pytest
 
-from artisynth_core_b200.femmodel import LinearMaterial, NeoHookeanMaterial, StVenantKirchoffMaterial
+from artisynth_core_b200.femmodel import (LinearMaterial, MooneyRivlinMaterial, NeoHookeanMaterial,
+                                          StVenantKirchoffMaterial)
 from artisynth_core_b200 import workloads as W
 from oracle import oracle as O
 
@@ -79,7 +84,7 @@ def _descriptors(om, wl, x):
             np.ascontiguousarray(np.array(DV)))
 
 
-def _reference_crs(R, desc, nnz):
+def _reference_crs(R, desc, nnz, dilational=None):
     import torch
     slots, gi, gj, D, sig, dv = desc
     nb = dv.size
@@ -95,18 +100,92 @@ def _reference_crs(R, desc, nnz):
     stream = torch.cuda.current_stream(dev).cuda_stream
     R.addMaterialStiffness3_launch(nb, *(a.data_ptr() for a in t), 1.0, crs.data_ptr(), stream)
     torch.cuda.synchronize()
+    if dilational is not None:
+        _add_reference_dilational(R, dilational, crs, nnz)
     return crs.cpu().numpy()
 
 
-@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex"])
+def _dilational_arrays(om, wl, x):
+    """Arrays of addDilationalStiffness3Element_launch for ELEMENT soft
+    incompressibility with one pressure value per element: constraint
+    vectors c_i = sum_k GNx_i dv (FemUtilities.addToIncompressConstraints)
+    and Rinv = effectiveModulus(kappa, V/V0) / V0 (computePressuresAndRinv,
+    FemModel3d.java:2517-2591); every node free (dimension 3, identity
+    transform, the block's nine slots first in its 36-slot record)."""
+    sidx = om.solve_index()
+    rp, col = om.pattern()
+    _, _, slots = om.crs(0)
+    ne, nen = wl.conn.shape
+    mat = wl.material
+    V0 = om.rest_volumes()
+    cons = np.zeros((ne, nen, 3))
+    rinv = np.zeros(ne)
+    pair_off = [0]
+    pairs, bslots = [], []
+    for e in range(ne):
+        V = 0.0
+        for k in range(om.num_ip()):
+            g, dv, _, _ = om.ip_data(x, e, k)
+            cons[e] += g * dv
+            V += dv
+        J = V / V0[e]
+        keff = mat.kappa if mat.bulk_potential == 0 else mat.kappa * (1 - np.log(J)) / (J * J)
+        rinv[e] = keff / V0[e]
+        for a in range(nen):
+            ra = sidx[wl.conn[e, a]]
+            if ra < 0:
+                continue
+            for b in range(nen):
+                rb = sidx[wl.conn[e, b]]
+                if rb < 0:
+                    continue
+                p = rp[ra] + int(np.searchsorted(col[rp[ra]:rp[ra + 1]], rb))
+                assert col[p] == rb
+                pairs.append((a, b))
+                rec = np.full(36, -1, dtype=np.int32)
+                rec[:9] = slots[9 * p:9 * p + 9]
+                bslots.append(rec)
+        pair_off.append(len(pairs))
+    eye = np.zeros(18)
+    eye[[0, 4, 8]] = 1.0
+    return dict(counts=np.full(ne, nen, dtype=np.int32), node_off=np.arange(ne, dtype=np.int32) * nen,
+                pcount=np.ones(ne, dtype=np.int32), pair_off=np.array(pair_off, dtype=np.int32),
+                cons_off=np.arange(ne, dtype=np.int32) * nen, rinv_off=np.arange(ne, dtype=np.int32),
+                pairs=np.array(pairs, dtype=np.int32).reshape(-1), slots=np.array(bslots, dtype=np.int32).reshape(-1),
+                dims=np.full(ne * nen, 3, dtype=np.int32), transforms=np.tile(eye, ne * nen),
+                cons=cons.reshape(-1), rinv=rinv)
+
+
+def _add_reference_dilational(R, arr, crs_dev, nnz):
+    import torch
+    ne = arr["counts"].size
+    npair = arr["pair_off"][-1]
+    # the kernel's indexing, checked before the launch
+    assert arr["pairs"].size == 2 * npair and arr["slots"].size == 36 * npair
+    assert arr["slots"][arr["slots"] >= 0].max() < nnz
+    assert arr["dims"].size == arr["cons"].size // 3 == ne * arr["counts"][0]
+    assert arr["transforms"].size == 18 * arr["dims"].size and arr["rinv"].size == ne
+    dev = torch.device("cuda:0")
+    order = ("counts", "node_off", "pcount", "pair_off", "cons_off", "rinv_off", "pairs", "slots", "dims",
+             "transforms", "cons", "rinv")
+    t = [torch.from_numpy(np.ascontiguousarray(arr[k])).to(dev) for k in order]
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    R.addDilationalStiffness3Element_launch(ne, *(a.data_ptr() for a in t), 1.0, crs_dev.data_ptr(), stream)
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex", "mooneyrivlin_hex_element"])
 def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     R = _ref_lib()
     if case == "neohookean_tet":
         wl = W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33))
     elif case == "neohookean_hex":
         wl = W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45))
-    else:
+    elif case == "stvk_hex":
         wl = W.small_hex_beam(StVenantKirchoffMaterial(5e4, 0.3))
+    else:
+        wl = W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370))
     wl.build_mesh()
     om = oracle_model(oracle, wl)
     x = deformed(wl.rest, seed=5)
@@ -114,7 +193,8 @@ def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     assert ninv == 0
     m = wl.model()
     _, K, crs = m.updateStressAndStiffness(x, want_crs=True)
-    ref = _reference_crs(R, _descriptors(om, wl, x), crs.size)
+    dil = _dilational_arrays(om, wl, x) if om.incomp == O.INCOMP_ELEMENT else None
+    ref = _reference_crs(R, _descriptors(om, wl, x), crs.size, dil)
     _, _, slots = om.crs(0)
     ocrs = np.zeros(crs.size)
     ocrs[slots] = oK.reshape(-1)

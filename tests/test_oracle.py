@@ -143,15 +143,19 @@ def test_polar_rotation(oracle):
         assert np.abs(R - Rref).max() <= 1e-10
 
 
-@pytest.mark.parametrize("kind,params,etype", [(0, [5e4, 0.3, 0], 0), (1, [5e4, 0.45], 0),
-                                               (1, [5e4, 0.45], 1), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1),
-                                               (3, [5e4, 0.3], 0), (3, [5e4, 0.3], 1)])
-def test_stiffness_matches_force_fd(oracle, kind, params, etype):
+@pytest.mark.parametrize("kind,params,etype,incomp", [
+    (0, [5e4, 0.3, 0], 0, 0), (1, [5e4, 0.45], 0, 0), (1, [5e4, 0.45], 1, 0),
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1, 0), (3, [5e4, 0.3], 0, 0), (3, [5e4, 0.3], 1, 0),
+    # ELEMENT soft incompressibility (QUADRATIC and LOGARITHMIC bulk potentials)
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 0, 3), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1, 3),
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 1, 3)])
+def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
     xyz, conn = oracle.grid(etype, (1.0, 0.4, 0.4), (3, 2, 2), jitter=0.04, seed=3)
     fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
-    m = oracle.OracleModel(etype, xyz, conn, fixed, kind, params, 1000.0, oracle.INCOMP_OFF)
+    m = oracle.OracleModel(etype, xyz, conn, fixed, kind, params, 1000.0, incomp)
+    assert m.incomp == incomp
     x = deformed(xyz, seed=1, rot_deg=15, bend=0.05, noise=0.01)
     f0, K, _ = m.update_stress_stiffness(x)
     sidx = m.solve_index()
