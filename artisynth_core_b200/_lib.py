@@ -34,6 +34,7 @@ PART_FULL, PART_UPPER = 0, 1
 PCG_AUTO, PCG_CLASSIC, PCG_PIPELINED = 0, 1, 2
 OPT_PCG_SPLIT, OPT_ROW_LANES, OPT_PCG_CTAS, OPT_PIECE_ROWS, OPT_WARM_START, OPT_ELEM_TILE, OPT_FUSED_ASSEMBLY = 1, 2, 3, 4, 5, 6, 7
 OPT_REFINE = 8
+INTEGRATOR_BACKWARD_EULER, INTEGRATOR_CONSTRAINED_BACKWARD_EULER = 0, 1
 SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED = 0, 1, 2
 
 
@@ -60,6 +61,7 @@ class StepParams(ctypes.Structure):
         ("max_iter", ctypes.c_int),
         ("abort_on_inverted", ctypes.c_int),
         ("pcg_variant", ctypes.c_int),
+        ("integrator", ctypes.c_int),
     ]
 
 
@@ -130,6 +132,7 @@ def lib():
         "b200fem_set_external_forces": ([H, _dp], ctypes.c_int),
         "b200fem_update_stress_stiffness": ([H, _dp, _dp, _dp, _dp], ctypes.c_int),
         "b200fem_backward_euler_step": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
+        "b200fem_set_plane_constraints": ([H, ctypes.c_int, _ip, _dp, _dp], ctypes.c_int),
         "b200fem_backward_euler_step_host": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_spmv": ([H, _dp, _dp], ctypes.c_int),

@@ -1203,6 +1203,15 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
     eng.pcg_variant = p->pcg_variant;
     eng.step_exec_max_iter = -1;  // recapture: the variant is a kernel argument
   }
+  if (p->integrator < B200FEM_INTEGRATOR_BACKWARD_EULER || p->integrator > B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown integrator");
+  if (p->integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && !eng.cons_node.empty() && eng.refine_ok &&
+      eng.opt_refine > 0)
+    return fail(&eng, B200FEM_ERR_UNSUPPORTED, "refinement sweeps with plane constraints");
+  if (p->integrator != eng.integrator) {
+    eng.integrator = p->integrator;
+    eng.step_exec_max_iter = -1;  // recapture: the constraint arrays are kernel arguments
+  }
   std::vector<double> step((size_t)d.n_models * 8);
   for (int m = 0; m < d.n_models; m++) {
     double* s = &step[(size_t)m * 8];
@@ -1296,6 +1305,48 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
   return st;
 }
 }  // namespace
+
+int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, const double* normals,
+                                  const double* offsets) {
+  ENG(h);
+  NEED_BUILT();
+  DevPack& d = eng.d;
+  if (n < 0 || (n > 0 && (!nodes || !normals || !offsets)))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid plane constraints");
+  const int R = d.n_rows;
+  std::vector<double> nrm(3 * (size_t)R, 0.0), off((size_t)R, 0.0);
+  std::vector<int> seen((size_t)R, 0);
+  std::vector<int> cn;
+  std::vector<double> cq, co;
+  for (int k = 0; k < n; k++) {
+    const int node = nodes[k];
+    if (node < 0 || node >= (int)eng.h_sidx.size() || eng.h_sidx[node] < 0)
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "plane constraint on a missing or fixed node");
+    const int r = eng.h_sidx[node];
+    if (seen[r]) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "more than one plane constraint on a node");
+    seen[r] = 1;
+    const double* q = normals + 3 * (size_t)k;
+    const double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+    if (!(len > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "plane constraint with a zero normal");
+    for (int c = 0; c < 3; c++) nrm[3 * (size_t)r + c] = q[c] / len;
+    off[r] = offsets[k] / len;
+    cn.push_back(node);
+    for (int c = 0; c < 3; c++) cq.push_back(q[c] / len);
+    co.push_back(offsets[k] / len);
+  }
+  if (!d.row_nrm) {
+    CK(dalloc(eng, &d.row_nrm, 3 * (size_t)R));
+    CK(dalloc(eng, &d.row_off, (size_t)R));
+    eng.step_exec_max_iter = -1;  // recapture with the new arrays
+  }
+  CK(cudaMemcpyAsync(d.row_nrm, nrm.data(), sizeof(double) * nrm.size(), cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaMemcpyAsync(d.row_off, off.data(), sizeof(double) * off.size(), cudaMemcpyHostToDevice, eng.stream));
+  CK(cudaStreamSynchronize(eng.stream));
+  eng.cons_node = cn;
+  eng.cons_nrm = cq;
+  eng.cons_off = co;
+  return B200FEM_OK;
+}
 
 int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps, b200fem_stats* stats) {
   ENG(h);

@@ -145,6 +145,8 @@ struct DevPack {
   int* chunk_elem = nullptr;
   int* contrib_loc = nullptr;  // parallel to contrib_idx
   int* blk_mirror = nullptr;   // nnzb: the block at the transposed position
+  double* row_nrm = nullptr;   // 3 per row: unit normal of the row's plane constraint (zero: none)
+  double* row_off = nullptr;   // per row: the plane's offset
   // refinement sweeps: FP64 residual, correction, its PCG results
   double* rref = nullptr;
   double* dsol = nullptr;
@@ -196,6 +198,11 @@ struct Engine {
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_strided = 0;  // pieces dealt to CTAs across models (large packs)
+  // plane constraints (b200fem_set_plane_constraints): per constrained node
+  // its unit normal and offset; enforced by the ConstrainedBackwardEuler step
+  std::vector<int> cons_node;
+  std::vector<double> cons_nrm, cons_off;
+  int integrator = 0;  // of the captured step graph
   bool any_inactive = false;  // some model_active entry is 0 (kernels get the mask)
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;

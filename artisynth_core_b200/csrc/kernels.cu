@@ -600,7 +600,7 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
                             const double* __restrict__ v, const double* __restrict__ fext,
                             const double* __restrict__ step, double* __restrict__ fint,
                             double* __restrict__ b, double* __restrict__ sol0, const int* __restrict__ active,
-                            const double* __restrict__ vprev) {
+                            const double* __restrict__ vprev, const double* __restrict__ row_nrm) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   if (active && !active[node_model[n]]) return;  // model left out of this step
@@ -635,12 +635,23 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
       b[3 * (size_t)r + c] = m * v[3 * (size_t)n + c] + h * (m * sp[3 + c] + fext[3 * (size_t)n + c] - f[c]);
     // the PCG starts from the current velocity, or from its extrapolation
     // v + (v - v_prev) over the last two steps
-    if (sol0)
+    if (sol0) {
+      double s0[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vc = v[3 * (size_t)n + c];
-        sol0[3 * (size_t)r + c] = vprev ? 2.0 * vc - vprev[3 * (size_t)n + c] : vc;
+        s0[c] = vprev ? 2.0 * vc - vprev[3 * (size_t)n + c] : vc;
       }
+      if (row_nrm) {
+        // plane constraint: the initial guess lies on the plane
+        const double* q = row_nrm + 3 * (size_t)r;
+        const double d = q[0] * s0[0] + q[1] * s0[1] + q[2] * s0[2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) s0[c] -= q[c] * d;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) sol0[3 * (size_t)r + c] = s0[c];
+    }
   }
 }
 
@@ -1787,9 +1798,12 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   const int blocks = (d.n_nodes + threads - 1) / threads;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
   const double* vp = eng.opt_warm_start == 1 ? d.vprev : nullptr;
+  const double* nrm =
+      (sol && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && d.row_nrm) ? d.row_nrm : nullptr;
   // nodal forces are FP64 in both forms
   rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
-                                                         d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp);
+                                                         d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp,
+                                                         nrm);
   return cudaGetLastError();
 }
 

@@ -135,7 +135,25 @@ struct PcgArgs {
   const int* act_node;
   const int* row_model;
   const int* model_active;  // per model: 0 = not solved in this call (or null: all)
+  // plane constraints (ConstrainedBackwardEuler), or null: per row the unit
+  // normal (zero for rows without a constraint) and the plane's offset
+  const double* row_nrm;
+  const double* row_off;
 };
+
+// Plane constraints: the constrained velocities of a row lie on its plane,
+// so every residual and SpMV output is projected onto it (y -= n (n . y));
+// rows without a constraint have n = 0 and stay as they are.  With the
+// projected block-Jacobi inverse P D^-1 P every search direction stays on
+// the planes, and the PCG solves the KKT system [S G^T; G 0] for v.
+__device__ __forceinline__ void project_row(const double* nrm, int row, double* y) {
+  if (!nrm) return;
+  const double* q = nrm + 3 * (size_t)row;
+  const double d = q[0] * y[0] + q[1] * y[1] + q[2] * y[2];
+  y[0] -= q[0] * d;
+  y[1] -= q[1] * d;
+  y[2] -= q[2] * d;
+}
 
 // The rows a CTA owns: its local pieces j = 0..npc-1 (global piece gp[j],
 // first global row grow[j]) laid end to end in a local row space
@@ -492,6 +510,7 @@ __device__ __forceinline__ void fused_rows(const PcgArgs& a, const MatView<MT>& 
     }
     double n[3];
     view_rows_spmv_group<MT, L>(mv, i, row, valid, mc, lane, n);
+    if (valid) project_row(a.row_nrm, row, n);
     const bool upd = valid && !conv[j] && gl < 3;
     double wc = 0, ru = 0, wu = 0, rr = 0;
     if (upd) {
@@ -725,6 +744,21 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 #pragma unroll
         for (int k = 0; k < 9; k++) inv[k] = 0;
       }
+      if (a.row_nrm) {
+        // P D^-1 P with P = I - n n^T
+        const double* q = a.row_nrm + 3 * (size_t)row;
+        double t[9];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            t[3 * r + c] = inv[3 * r + c] - q[r] * (q[0] * inv[c] + q[1] * inv[3 + c] + q[2] * inv[6 + c]);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            inv[3 * r + c] = t[3 * r + c] - (t[3 * r] * q[0] + t[3 * r + 1] * q[1] + t[3 * r + 2] * q[2]) * q[c];
+      }
       double* D = st.dinv(i, row);
 #pragma unroll
       for (int k = 0; k < 9; k++) D[k] = inv[k];
@@ -733,6 +767,8 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       load3(x0, a.x, row);
 #pragma unroll
       for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
+      project_row(a.row_nrm, row, r);
+      project_row(a.row_nrm, row, bv);
       mul33(u, inv, r);
       store3(st.at(VR, i, row), 0, r);
       store3(st.at(VU, i, row), 0, u);
@@ -797,6 +833,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           double Az[3];
           view_row_spmv<MT>(mv, i, row, a.m1, ln, Az);
           if (ln == 0) {
+            project_row(a.row_nrm, row, Az);
             const double be = s_beta[j];
             double* pz = st.at(VU, i, row);
             double* pp = st.at(VP, i, row);
@@ -864,6 +901,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       double Au[3];
       view_row_spmv<MT>(mv, i, row, a.m1, ln, Au);
       if (ln == 0) {
+        project_row(a.row_nrm, row, Au);
         double r[3], u[3], m[3], zero[3] = {0, 0, 0};
         load3(r, st.at(VR, i, row), 0);
         load3(u, st.at(VU, i, row), 0);
@@ -976,9 +1014,11 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
               double mm[3], w[3], r[3], u[3];
               if (res) load3(mm, st.at(VM, i, row), 0);
               else load3(mm, mc, row);
+              double nn[3] = {sn[ia - c0][0], sn[ia - c0][1], sn[ia - c0][2]};
+              project_row(a.row_nrm, row, nn);
 #pragma unroll
               for (int c = 0; c < 3; c++) {
-                const double z = sn[ia - c0][c] + be * pz[c];
+                const double z = nn[c] + be * pz[c];
                 const double q = mm[c] + be * pq[c];
                 const double sv = pw[c] + be * ps[c];
                 const double p = pu[c] + be * pp[c];
@@ -1082,6 +1122,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         load3(bv, a.b, row);
 #pragma unroll
         for (int c = 0; c < 3; c++) r[c] = bv[c] - Ax[c];
+        project_row(a.row_nrm, row, r);
         vals[0] = dot3(r, r);
         // restart state (used only if the model restarts)
         double u[3];
@@ -1137,13 +1178,24 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       if (a.model_active && !a.model_active[a.row_model[row]]) continue;
       const int n = a.act_node[row];
       const double h = a.step[(size_t)a.row_model[row] * 8];
+      double xn[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vn = a.x[3 * (size_t)row + c];
         a.vprev[3 * (size_t)n + c] = a.vel[3 * (size_t)n + c];
         a.vel[3 * (size_t)n + c] = vn;
-        a.xpos[3 * (size_t)n + c] += h * vn;
+        xn[c] = a.xpos[3 * (size_t)n + c] + h * vn;
       }
+      if (a.row_nrm) {
+        // GlobalMass position correction of a single-particle plane
+        // constraint: the node moves onto its plane along the normal
+        const double* q = a.row_nrm + 3 * (size_t)row;
+        const double dist = q[0] * xn[0] + q[1] * xn[1] + q[2] * xn[2] - a.row_off[row];
+#pragma unroll
+        for (int c = 0; c < 3; c++) xn[c] -= q[c] * dist;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) a.xpos[3 * (size_t)n + c] = xn[c];
     }
   }
 }
@@ -1197,6 +1249,11 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.act_node = d.act_node;
   a.row_model = d.row_model;
   a.model_active = eng.any_inactive ? d.model_active : nullptr;
+  // constraints belong to the ConstrainedBackwardEuler step's solve only
+  a.row_nrm = (update_state && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && d.row_nrm)
+                  ? d.row_nrm
+                  : nullptr;
+  a.row_off = a.row_nrm ? d.row_off : nullptr;
   a.resident = eng.pcg_resident;
   a.cached = eng.pcg_cached;
   a.nloc_max = eng.pcg_nloc_max;
@@ -1497,6 +1554,8 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.act_node = nullptr;
   a.row_model = nullptr;
   a.model_active = nullptr;
+  a.row_nrm = nullptr;
+  a.row_off = nullptr;
   a.tol_override = 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);

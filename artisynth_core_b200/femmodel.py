@@ -340,6 +340,17 @@ class FemModel3d:
         self.engine().call("b200fem_get_state", L.dptr(x), L.dptr(v))
         return x.reshape(-1, 3), v.reshape(-1, 3)
 
+    def setPlaneConstraints(self, nodes, normals, offsets):
+        """ParticlePlaneConstraint on single nodes: node nodes[i] is held on
+        the plane normals[i] . x = offsets[i] by the ConstrainedBackwardEuler
+        integrator (b200fem_set_plane_constraints); empty lists remove them."""
+        nd = np.ascontiguousarray(nodes, dtype=np.int32).reshape(-1)
+        nr = np.ascontiguousarray(normals, dtype=np.float64).reshape(-1)
+        of = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1)
+        if nr.size != 3 * nd.size or of.size != nd.size:
+            raise ValueError("one normal (3 values) and one offset per node")
+        self.engine().call("b200fem_set_plane_constraints", int(nd.size), L.iptr(nd), L.dptr(nr), L.dptr(of))
+
     # --- hot path
     def updateStressAndStiffness(self, x=None, want_crs=False):
         """Internal force (N,3), stiffness blocks (nnzb,3,3) in block-CSR
@@ -361,11 +372,15 @@ class MechSystemSolver:
     """BackwardEuler integration of one FemModel3d on the device
     (MechSystemSolver.backwardEuler, MechSystemSolver.java:2171-2476)."""
 
-    def __init__(self, model: FemModel3d, tol: float = 1e-10, max_iter: int = 10000, pcg_variant: int = 0):
+    def __init__(self, model: FemModel3d, tol: float = 1e-10, max_iter: int = 10000, pcg_variant: int = 0,
+                 integrator: int = L.INTEGRATOR_BACKWARD_EULER):
         self.model = model
         self.tol = tol
         self.max_iter = max_iter
         self.pcg_variant = pcg_variant
+        # MechSystemSolver.setIntegrator: BackwardEuler ignores constraints,
+        # ConstrainedBackwardEuler enforces the model's plane constraints
+        self.integrator = integrator
         self.abort_on_inverted = False
         self.stats = L.Stats()
 
@@ -381,6 +396,7 @@ class MechSystemSolver:
         p.max_iter = self.max_iter
         p.abort_on_inverted = 1 if self.abort_on_inverted else 0
         p.pcg_variant = self.pcg_variant
+        p.integrator = self.integrator
         return p
 
     def backwardEuler(self, h, nsteps=1):

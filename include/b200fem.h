@@ -100,7 +100,13 @@ typedef struct {
                         switching to classic PCG after a residual replacement;
                         1 classic PCG (two barriers, better attainable accuracy);
                         2 pipelined only */
+  int integrator;    /* B200FEM_INTEGRATOR_*: BackwardEuler ignores constraints;
+                        ConstrainedBackwardEuler enforces the plane constraints */
 } b200fem_step_params;
+
+/* MechSystemSolver.Integrator */
+#define B200FEM_INTEGRATOR_BACKWARD_EULER 0
+#define B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER 1
 
 typedef struct {
   int iterations;      /* PCG iterations of the last solve */
@@ -167,6 +173,16 @@ int b200fem_set_external_forces(b200fem_handle h, const double* fext);
    values in the reference slot order (crs_nnz_full; may be NULL). */
 int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f_int,
                                     double* k_blocks, double* crs_vals);
+/* ParticlePlaneConstraint (ParticlePlaneConstraint.java:144-160) on single
+   nodes: node nodes[i] (not fixed, at most one constraint each) is held on the
+   plane normals[i] . x = offsets[i] (normals need not be unit length).  The
+   ConstrainedBackwardEuler integrator solves the KKT velocity system
+   [S G^T; G 0] (MechSystemSolver.KKTFactorAndSolve) by PCG on the constrained
+   velocities (every row's search directions projected onto its plane) and
+   then moves each constrained node onto its plane (the GlobalMass position
+   correction of a single-particle constraint).  n = 0 removes them. */
+int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, const double* normals,
+                                  const double* offsets);
 /* nsteps BackwardEuler steps on the device-resident state */
 int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps,
                                 b200fem_stats* stats);

@@ -1323,9 +1323,15 @@ void orc_nodal_pressures(void* h, double* p) {
 // fext: 3N external nodal forces (may be null).  x, v (3N) updated in place.
 // solver 0 = Jacobi-PCG to tol, 1 = dense Cholesky.
 // Returns 0, or 1 when CG did not converge, 2 when the dense solve failed.
-int orc_be_step(void* h, double hstep, const double* prm, const double* fext, double* x,
-                double* v, int solver, double tol, int maxit, int* iters, double* relres) {
-  Model* m = (Model*)h;
+// The BackwardEuler velocity system S v = b of MechSystemSolver.backwardEuler
+// (MechSystemSolver.java:2171-2476) at positions x and velocities v (3N):
+// S in BSR order (9*nnzb), b and the active velocities vact (3*nact).
+// ConstrainedBackwardEuler (MechSystemSolver.java:4804-4923) forms the same
+// M block and right-hand side (KKTFactorAndSolve with a0 = -h, a1 = -h^2,
+// a2 = -h, a3 = 0: the velocity-Jacobian term times v0, as here).
+static void be_system(Model* m, double hstep, const double* prm, const double* fext, const double* x,
+                      const double* v, std::vector<double>& S, std::vector<double>& b,
+                      std::vector<double>& vact) {
   double am = prm[0], bk = prm[1];
   const double* g = prm + 2;
   update_stress_stiffness(*m, x);
@@ -1333,7 +1339,8 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
   // FemModel3d.updateNodeForces (FemModel3d.java:2740-2847): for each node
   // f = fext + m g - f_int - (beta_k sum_j K_ij v_j + alpha_m m v)
   std::vector<double> f((size_t)3 * m->N, 0);
-  std::vector<double> vact(nv), xact(nv);
+  vact.assign(nv, 0);
+  std::vector<double> xact(nv);
   for (int n = 0; n < m->N; n++)
     if (m->sidx[n] >= 0)
       for (int c = 0; c < 3; c++) {
@@ -1357,7 +1364,7 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
     }
   }
   // b = M v + h f   (:2194-2200)
-  std::vector<double> b(nv);
+  b.assign(nv, 0);
   for (int n = 0; n < m->N; n++) {
     int bi = m->sidx[n];
     if (bi < 0) continue;
@@ -1365,7 +1372,7 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
   }
   // S = h(alpha_m M + beta_k K)  (addVelJacobian, s = -h)
   size_t nnzb = m->col.size();
-  std::vector<double> S(nnzb * 9, 0);
+  S.assign(nnzb * 9, 0);
   for (size_t q = 0; q < nnzb * 9; q++) S[q] = (hstep * bk) * m->K[q];
   for (int n = 0; n < m->N; n++) {
     int bi = m->sidx[n];
@@ -1385,6 +1392,14 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
     int d = m->block_index(bi, bi);
     for (int c = 0; c < 3; c++) S[(size_t)d * 9 + 4 * c] += m->mass[n];
   }
+}
+
+int orc_be_step(void* h, double hstep, const double* prm, const double* fext, double* x,
+                double* v, int solver, double tol, int maxit, int* iters, double* relres) {
+  Model* m = (Model*)h;
+  int nv = 3 * m->nact;
+  std::vector<double> S, b, vact;
+  be_system(m, hstep, prm, fext, x, v, S, b, vact);
   std::vector<double> vn = vact;
   int status = 0;
   if (solver == 1) {
@@ -1410,6 +1425,84 @@ int orc_be_step(void* h, double hstep, const double* prm, const double* fext, do
     }
   }
   return status;
+}
+
+// One MechSystemSolver.constrainedBackwardEuler step (MechSystemSolver.java:
+// 4804-4923) with bilateral particle-plane constraints
+// (ParticlePlaneConstraint.java:144-160, ParticleConstraintBase.java:163-200):
+// constraint i holds node nodes[i] on the plane nrm_i . x = off_i (nrm_i unit,
+// one constraint per node, nodes not fixed).  The velocity solve is the KKT
+// system [S G^T; G 0][v; lam] = [b; 0] with G_i = nrm_i^T on the node (a fixed
+// plane has no velocity offset: setBilateralOffsets, :2697-2721, with zero
+// compliance and gdot), solved densely (Gaussian elimination, partial
+// pivoting); then x1 = x0 + h v1 and the GlobalMass position correction,
+// which for one single-particle constraint moves the node onto its plane
+// along nrm_i (x -= nrm_i (nrm_i . x - off_i)).  Returns 0, or 2 when the
+// KKT matrix is singular.
+int orc_cbe_step(void* h, double hstep, const double* prm, const double* fext, double* x, double* v,
+                 int ncons, const int* nodes, const double* nrm, const double* off) {
+  Model* m = (Model*)h;
+  const int nv = 3 * m->nact;
+  std::vector<double> S, b, vact;
+  be_system(m, hstep, prm, fext, x, v, S, b, vact);
+  const int n = nv + ncons;
+  std::vector<double> A((size_t)n * n, 0), rhs(n, 0);
+  for (int bi = 0; bi < m->nact; bi++)
+    for (int p = m->rowptr[bi]; p < m->rowptr[bi + 1]; p++) {
+      int bj = m->col[p];
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[(size_t)(3 * bi + r) * n + 3 * bj + c] = S[(size_t)p * 9 + 3 * r + c];
+    }
+  for (int i = 0; i < nv; i++) rhs[i] = b[i];
+  for (int k = 0; k < ncons; k++) {
+    const int bi = m->sidx[nodes[k]];
+    if (bi < 0) return 2;
+    for (int c = 0; c < 3; c++) {
+      A[(size_t)(nv + k) * n + 3 * bi + c] = nrm[3 * k + c];
+      A[(size_t)(3 * bi + c) * n + nv + k] = nrm[3 * k + c];
+    }
+  }
+  // Gaussian elimination with partial pivoting
+  std::vector<int> piv(n);
+  for (int i = 0; i < n; i++) piv[i] = i;
+  for (int j = 0; j < n; j++) {
+    int best = j;
+    for (int i = j + 1; i < n; i++)
+      if (std::fabs(A[(size_t)i * n + j]) > std::fabs(A[(size_t)best * n + j])) best = i;
+    if (A[(size_t)best * n + j] == 0) return 2;
+    if (best != j) {
+      for (int c = 0; c < n; c++) std::swap(A[(size_t)j * n + c], A[(size_t)best * n + c]);
+      std::swap(rhs[j], rhs[best]);
+    }
+    const double d = A[(size_t)j * n + j];
+    for (int i = j + 1; i < n; i++) {
+      const double f = A[(size_t)i * n + j] / d;
+      if (f == 0) continue;
+      for (int c = j; c < n; c++) A[(size_t)i * n + c] -= f * A[(size_t)j * n + c];
+      rhs[i] -= f * rhs[j];
+    }
+  }
+  std::vector<double> sol(n);
+  for (int i = n - 1; i >= 0; i--) {
+    double t = rhs[i];
+    for (int c = i + 1; c < n; c++) t -= A[(size_t)i * n + c] * sol[c];
+    sol[i] = t / A[(size_t)i * n + i];
+  }
+  for (int nd = 0; nd < m->N; nd++) {
+    const int bi = m->sidx[nd];
+    if (bi < 0) continue;
+    for (int c = 0; c < 3; c++) {
+      v[3 * nd + c] = sol[3 * bi + c];
+      x[3 * nd + c] += hstep * sol[3 * bi + c];
+    }
+  }
+  for (int k = 0; k < ncons; k++) {
+    double* p = &x[3 * nodes[k]];
+    const double* q = &nrm[3 * k];
+    const double d = q[0] * p[0] + q[1] * p[1] + q[2] * p[2] - off[k];
+    for (int c = 0; c < 3; c++) p[c] -= q[c] * d;
+  }
+  return 0;
 }
 
 int orc_num_ip(void* h) { return ((Model*)h)->sh.nip; }

@@ -241,3 +241,36 @@ def test_thread_count_does_not_change_results(oracle):
     f4, K4, _ = m.update_stress_stiffness(x)
     oracle.set_threads(prev)
     assert np.array_equal(f1, f4) and np.array_equal(K1, K4)
+
+
+def _plane_beam(oracle):
+    xyz, conn = oracle.grid(oracle.ELEM_TET, (1.0, 0.3, 0.3), (6, 2, 2), jitter=0.04, seed=5)
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    m = oracle.OracleModel(oracle.ELEM_TET, xyz, conn, fixed, 1, [5e4, 0.33], 1000.0, oracle.INCOMP_OFF)
+    tip = np.where(xyz[:, 0] >= 0.5 - 1e-9)[0]
+    return xyz, m, tip
+
+
+def test_constrained_step_without_constraints_is_backward_euler(oracle):
+    xyz, m, _ = _plane_beam(oracle)
+    xa, va = xyz.copy(), np.zeros_like(xyz)
+    xb, vb = xyz.copy(), np.zeros_like(xyz)
+    for _ in range(3):
+        assert m.be_step(0.01, xa, va, gravity=(0, 0, -9.81), solver=1)[0] == 0
+        assert m.cbe_step(0.01, xb, vb, [], np.zeros(0), np.zeros(0), gravity=(0, 0, -9.81)) == 0
+    assert np.abs(xa - xb).max() <= 1e-12 * np.abs(xa).max()
+
+
+def test_constrained_step_holds_nodes_on_their_planes(oracle):
+    """Tip nodes on tilted planes through their rest positions: after each
+    ConstrainedBackwardEuler step n.v = 0 and n.x = offset (position
+    correction); the beam still deforms under gravity."""
+    xyz, m, tip = _plane_beam(oracle)
+    nrm = np.tile(np.array([0.0, 1.0, 1.0]) / np.sqrt(2), (tip.size, 1))
+    off = (nrm * xyz[tip]).sum(axis=1)
+    x, v = xyz.copy(), np.zeros_like(xyz)
+    for _ in range(4):
+        assert m.cbe_step(0.01, x, v, tip, nrm, off, gravity=(0, 0, -9.81)) == 0
+        assert np.abs((nrm * v[tip]).sum(axis=1)).max() <= 1e-10 * np.abs(v).max()
+        assert np.abs((nrm * x[tip]).sum(axis=1) - off).max() <= 1e-14
+    assert np.abs(x - xyz).max() > 1e-6
