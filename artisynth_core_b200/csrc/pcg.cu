@@ -633,6 +633,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   __shared__ int s_alst[kMaxCtaPieces + 1];
   __shared__ int s_restart;
   __shared__ int s_unc[2];  // see the pipelined iteration
+  // a model's convergence flag changed in this pipelined iteration: the
+  // active view is laid out again at its end (otherwise it stays as it is)
+  __shared__ int s_conv_dirty;
+  if (threadIdx.x == 0) s_conv_dirty = 0;
   extern __shared__ __align__(16) unsigned char dyn[];
   const bool res = RES || a.resident;
   const int pc0 = a.cta_piece[blockIdx.x];
@@ -968,6 +972,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
                 const double gam = sm[0], del = sm[1], rho = sm[2];
                 if (sqrt(rho) <= s_thr[j] || rho == 0.0) {
                   s_conv[j] = 1;
+                  s_conv_dirty = 1;
                 } else {
                   double beta = 0, alpha;
                   if (s_first[j]) {
@@ -995,6 +1000,11 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           }
           // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
           // x += alpha p; r -= alpha s; u -= alpha q; w -= alpha z; m' = Dinv w
+          // (resident form, one piece: each thread sums its rows' dot-product
+          // terms, each warp reduces them and the per-warp sums go to
+          // rowbuf[warp]; the 64-register strided form keeps rowbuf rows)
+          const bool regsum = RES && npc == 1;
+          double acc3[3] = {0, 0, 0};
           for (int ia = c0 + (int)threadIdx.x; ia < c1; ia += blockDim.x) {
             const int j = ar.piece(ia);
             double v3[3] = {0, 0, 0};
@@ -1042,9 +1052,20 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
               v3[1] = dot3(w, u);
               v3[2] = dot3(r, r);
             }
-            rowbuf[ia - c0][0] = v3[0];
-            rowbuf[ia - c0][1] = v3[1];
-            rowbuf[ia - c0][2] = v3[2];
+            if (regsum) {
+#pragma unroll
+              for (int k = 0; k < 3; k++) acc3[k] += v3[k];
+            } else {
+              rowbuf[ia - c0][0] = v3[0];
+              rowbuf[ia - c0][1] = v3[1];
+              rowbuf[ia - c0][2] = v3[2];
+            }
+          }
+          if (regsum) {
+            warp_sum<3>(acc3);
+            if (lane == 0)
+#pragma unroll
+              for (int k = 0; k < 3; k++) rowbuf[warp][k] = acc3[k];
           }
         } else {
           // later chunks: all warps, SpMV and update fused per row
@@ -1055,6 +1076,16 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           else fused_rows<MT, 32>(a, mv, ar, st, res, mc, mn, c0, c1, warp, nw, lane, s_conv, s_alpha, s_beta, rowbuf);
         }
         __syncthreads();
+        if (RES && npc == 1 && first) {
+          // one piece: the per-warp sums in warp order
+          if (threadIdx.x == 0) {
+            const int nw = blockDim.x >> 5;
+            for (int w = 0; w < nw; w++)
+#pragma unroll
+              for (int k = 0; k < 3; k++) pacc[0][k] += rowbuf[w][k];
+          }
+          continue;
+        }
         if (npc == 1 && c1 - c0 <= 32) {
           // one piece, one warp of rows: reduce in warp 0 without a second pass
           if (warp == 0) {
@@ -1094,8 +1125,14 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 #pragma unroll
           for (int k = 0; k < 3; k++) out[(size_t)s_gp[j] * 4 + k] = pacc[j][k];
       }
-      // the next iteration works on the models still unconverged
-      rescan(s_conv);
+      // the next iteration works on the models still unconverged; the
+      // resident form lays the view out again only when a flag changed
+      // (every thread read s_conv_dirty after the first chunk's barrier; it
+      // is cleared after the rescan's closing barrier)
+      if (!RES || s_conv_dirty) {
+        rescan(s_conv);
+        if (threadIdx.x == 0) s_conv_dirty = 0;
+      }
       if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
       mbuf ^= 1;
       // every model still iterating at idx - 1 converged there: iteration
