@@ -138,6 +138,7 @@ struct DevPack {
   int* cta_plist = nullptr;    // n_pieces: global piece indices, CTA-major
   int* model_active = nullptr; // n_models: 0 = left out of assembly and steps
   double* vprev = nullptr;     // 3N: velocity before the last step (warm-start extrapolation)
+  double* vprev2 = nullptr;    // 3N: velocity before that (quadratic extrapolation)
   // fused assembly: block-row chunks, their incident elements, and the
   // contribution lists re-indexed to chunk-local elements
   int* chunk_row = nullptr;    // chunks+1
@@ -206,7 +207,7 @@ struct Engine {
   bool any_inactive = false;  // some model_active entry is 0 (kernels get the mask)
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
-  int opt_warm_start = 1;  // 0 previous velocity, 1 extrapolated from the last two
+  int opt_warm_start = 2;  // 0 previous velocity, 1 linear from the last two, 2 quadratic from three
   bool elem_tile_small = false;  // element kernels: the small tile of each material
   bool elem_staged = false;      // tets: the shared-memory staged kernel instead of one thread per element
   bool fused = false;            // BackwardEuler assembly on the fused row-chunk path

@@ -131,6 +131,7 @@ struct PcgArgs {
   int update_state;
   double* xpos;
   double* vprev;  // receives the velocity before the update
+  double* vprev2;  // receives vprev before the update
   double* vel;
   const int* act_node;
   const int* row_model;
@@ -1219,6 +1220,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vn = a.x[3 * (size_t)row + c];
+        a.vprev2[3 * (size_t)n + c] = a.vprev[3 * (size_t)n + c];
         a.vprev[3 * (size_t)n + c] = a.vel[3 * (size_t)n + c];
         a.vel[3 * (size_t)n + c] = vn;
         xn[c] = a.xpos[3 * (size_t)n + c] + h * vn;
@@ -1283,6 +1285,7 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.xpos = d.x;
   a.vel = d.v;
   a.vprev = d.vprev;
+  a.vprev2 = d.vprev2;
   a.act_node = d.act_node;
   a.row_model = d.row_model;
   a.model_active = eng.any_inactive ? d.model_active : nullptr;
@@ -1586,6 +1589,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.row_lanes = 16;
   a.update_state = 0;
   a.vprev = nullptr;
+  a.vprev2 = nullptr;
   a.xpos = nullptr;
   a.vel = nullptr;
   a.act_node = nullptr;
