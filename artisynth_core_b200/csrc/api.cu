@@ -520,6 +520,10 @@ int build_pack(Engine& eng) {
   CK(cudaMemset(d.vprev, 0, 3 * sizeof(double) * (size_t)N));
   CK(dalloc(eng, &d.vprev2, 3 * (size_t)N));
   CK(cudaMemset(d.vprev2, 0, 3 * sizeof(double) * (size_t)N));
+  CK(dalloc(eng, &d.vprev3, 3 * (size_t)N));
+  CK(cudaMemset(d.vprev3, 0, 3 * sizeof(double) * (size_t)N));
+  CK(dalloc(eng, &d.vprev4, 3 * (size_t)N));
+  CK(cudaMemset(d.vprev4, 0, 3 * sizeof(double) * (size_t)N));
   CK(dalloc(eng, &d.fext, 3 * (size_t)N));
   CK(cudaMemset(d.fext, 0, 3 * sizeof(double) * (size_t)N));
   CK(upload(eng, &d.mass, mass));
@@ -936,7 +940,7 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       }
       return B200FEM_OK;
     case B200FEM_OPT_WARM_START:
-      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "WARM_START must be 0, 1 or 2");
+      if (value < 0 || value > 4) return fail(&eng, B200FEM_ERR_INVALID_ARG, "WARM_START must be 0 to 4");
       if (value != eng.opt_warm_start) {
         eng.opt_warm_start = value;
         eng.step_exec_max_iter = -1;  // recapture: the RHS kernel's arguments change
@@ -1082,6 +1086,8 @@ int b200fem_set_state(b200fem_handle h, const double* x, const double* v) {
   // acceleration
   if (v) CK(cudaMemcpyAsync(eng.d.vprev, v, n, cudaMemcpyHostToDevice, eng.stream));
   if (v) CK(cudaMemcpyAsync(eng.d.vprev2, v, n, cudaMemcpyHostToDevice, eng.stream));
+  if (v) CK(cudaMemcpyAsync(eng.d.vprev3, v, n, cudaMemcpyHostToDevice, eng.stream));
+  if (v) CK(cudaMemcpyAsync(eng.d.vprev4, v, n, cudaMemcpyHostToDevice, eng.stream));
   CK(cudaStreamSynchronize(eng.stream));
   return B200FEM_OK;
 }

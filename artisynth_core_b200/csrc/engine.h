@@ -139,6 +139,8 @@ struct DevPack {
   int* model_active = nullptr; // n_models: 0 = left out of assembly and steps
   double* vprev = nullptr;     // 3N: velocity before the last step (warm-start extrapolation)
   double* vprev2 = nullptr;    // 3N: velocity before that (quadratic extrapolation)
+  double* vprev3 = nullptr;    // 3N: and before that (cubic extrapolation)
+  double* vprev4 = nullptr;    // 3N: and before that (quartic extrapolation)
   // fused assembly: block-row chunks, their incident elements, and the
   // contribution lists re-indexed to chunk-local elements
   int* chunk_row = nullptr;    // chunks+1
@@ -207,7 +209,9 @@ struct Engine {
   bool any_inactive = false;  // some model_active entry is 0 (kernels get the mask)
   // tuning options (B200FEM_OPT_*): 0 = automatic
   int opt_split = 0, opt_row_lanes = 0, opt_ctas = 0, opt_piece_rows = 0;
-  int opt_warm_start = 2;  // 0 previous velocity, 1 linear from the last two, 2 quadratic from three
+  // PCG initial guess: the velocity extrapolated by a polynomial of this
+  // order through the last opt_warm_start + 1 velocities (0: v itself)
+  int opt_warm_start = 4;
   bool elem_tile_small = false;  // element kernels: the small tile of each material
   bool elem_staged = false;      // tets: the shared-memory staged kernel instead of one thread per element
   bool fused = false;            // BackwardEuler assembly on the fused row-chunk path

@@ -601,6 +601,7 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
                             const double* __restrict__ step, double* __restrict__ fint,
                             double* __restrict__ b, double* __restrict__ sol0, const int* __restrict__ active,
                             const double* __restrict__ vprev, const double* __restrict__ vprev2,
+                            const double* __restrict__ vprev3, const double* __restrict__ vprev4,
                             const double* __restrict__ row_nrm) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -641,7 +642,12 @@ __global__ void rows_kernel(int N, const int* __restrict__ inc_ptr, const int* _
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vc = v[3 * (size_t)n + c];
-        if (vprev2)  // quadratic through the last three velocities
+        if (vprev4)  // quartic through the last five velocities
+          s0[c] = 5.0 * (vc - vprev3[3 * (size_t)n + c]) + 10.0 * (vprev2[3 * (size_t)n + c] - vprev[3 * (size_t)n + c]) +
+                  vprev4[3 * (size_t)n + c];
+        else if (vprev3)  // cubic through the last four velocities
+          s0[c] = 4.0 * (vc + vprev2[3 * (size_t)n + c]) - 6.0 * vprev[3 * (size_t)n + c] - vprev3[3 * (size_t)n + c];
+        else if (vprev2)  // quadratic through the last three velocities
           s0[c] = 3.0 * (vc - vprev[3 * (size_t)n + c]) + vprev2[3 * (size_t)n + c];
         else
           s0[c] = vprev ? 2.0 * vc - vprev[3 * (size_t)n + c] : vc;
@@ -1602,7 +1608,8 @@ __global__ void refine_add_kernel(int R, double* __restrict__ v, const double* _
 __global__ void refine_state_kernel(int R, const int* __restrict__ act_node, const int* __restrict__ row_model,
                                     const double* __restrict__ step, const double* __restrict__ sol,
                                     double* __restrict__ x, double* __restrict__ vel, double* __restrict__ vprev,
-                                    double* __restrict__ vprev2, const int* __restrict__ active) {
+                                    double* __restrict__ vprev2, double* __restrict__ vprev3,
+                                    double* __restrict__ vprev4, const int* __restrict__ active) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= R) return;
   const int m = row_model[row];
@@ -1612,6 +1619,8 @@ __global__ void refine_state_kernel(int R, const int* __restrict__ act_node, con
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     const double vn = sol[3 * (size_t)row + c];
+    vprev4[3 * (size_t)n + c] = vprev3[3 * (size_t)n + c];
+    vprev3[3 * (size_t)n + c] = vprev2[3 * (size_t)n + c];
     vprev2[3 * (size_t)n + c] = vprev[3 * (size_t)n + c];
     vprev[3 * (size_t)n + c] = vel[3 * (size_t)n + c];
     vel[3 * (size_t)n + c] = vn;
@@ -1653,7 +1662,8 @@ cudaError_t launch_solve(Engine& eng, int max_iter) {
     refine_add_kernel<<<(unsigned)((3LL * d.n_rows + 255) / 256), 256, 0, eng.stream>>>(d.n_rows, d.sol, d.dsol);
   }
   refine_state_kernel<<<(d.n_rows + 127) / 128, 128, 0, eng.stream>>>(d.n_rows, d.act_node, d.row_model, d.step,
-                                                                      d.sol, d.x, d.v, d.vprev, d.vprev2, act);
+                                                                      d.sol, d.x, d.v, d.vprev, d.vprev2, d.vprev3,
+                                                                      d.vprev4, act);
   return cudaGetLastError();
 }
 
@@ -1803,13 +1813,15 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   const int blocks = (d.n_nodes + threads - 1) / threads;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
   const double* vp = eng.opt_warm_start >= 1 ? d.vprev : nullptr;
-  const double* vp2 = eng.opt_warm_start == 2 ? d.vprev2 : nullptr;
+  const double* vp2 = eng.opt_warm_start >= 2 ? d.vprev2 : nullptr;
+  const double* vp3 = eng.opt_warm_start >= 3 ? d.vprev3 : nullptr;
+  const double* vp4 = eng.opt_warm_start == 4 ? d.vprev4 : nullptr;
   const double* nrm =
       (sol && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && d.row_nrm) ? d.row_nrm : nullptr;
   // nodal forces are FP64 in both forms
   rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp,
-                                                         vp2, nrm);
+                                                         vp2, vp3, vp4, nrm);
   return cudaGetLastError();
 }
 

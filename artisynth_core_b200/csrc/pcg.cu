@@ -132,6 +132,8 @@ struct PcgArgs {
   double* xpos;
   double* vprev;  // receives the velocity before the update
   double* vprev2;  // receives vprev before the update
+  double* vprev3;  // receives vprev2 before the update
+  double* vprev4;  // receives vprev3 before the update
   double* vel;
   const int* act_node;
   const int* row_model;
@@ -1220,6 +1222,8 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const double vn = a.x[3 * (size_t)row + c];
+        a.vprev4[3 * (size_t)n + c] = a.vprev3[3 * (size_t)n + c];
+        a.vprev3[3 * (size_t)n + c] = a.vprev2[3 * (size_t)n + c];
         a.vprev2[3 * (size_t)n + c] = a.vprev[3 * (size_t)n + c];
         a.vprev[3 * (size_t)n + c] = a.vel[3 * (size_t)n + c];
         a.vel[3 * (size_t)n + c] = vn;
@@ -1286,6 +1290,8 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.vel = d.v;
   a.vprev = d.vprev;
   a.vprev2 = d.vprev2;
+  a.vprev3 = d.vprev3;
+  a.vprev4 = d.vprev4;
   a.act_node = d.act_node;
   a.row_model = d.row_model;
   a.model_active = eng.any_inactive ? d.model_active : nullptr;
@@ -1590,6 +1596,8 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.update_state = 0;
   a.vprev = nullptr;
   a.vprev2 = nullptr;
+  a.vprev3 = nullptr;
+  a.vprev4 = nullptr;
   a.xpos = nullptr;
   a.vel = nullptr;
   a.act_node = nullptr;

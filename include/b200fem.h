@@ -245,10 +245,13 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
 #define B200FEM_OPT_ROW_LANES 2  /* lanes per block row in the iteration SpMV: 0 auto, 4, 8, 16, 32 */
 #define B200FEM_OPT_PCG_CTAS 3   /* CTAs of the persistent PCG kernel: 0 auto (one per SM) */
 #define B200FEM_OPT_PIECE_ROWS 4 /* block rows per piece in the strided split: 0 auto (64) */
-#define B200FEM_OPT_WARM_START 5 /* PCG start: 0 the previous velocity; 1 its linear
-                                    extrapolation 2 v_n - v_(n-1) over the last two steps; 2
-                                    (default) the quadratic 3 (v_n - v_(n-1)) + v_(n-2) over
-                                    three (may be changed after the build) */
+#define B200FEM_OPT_WARM_START 5 /* PCG start: the velocity extrapolated by a polynomial of
+                                    order 0..4 through the last 1..5 velocities: 0 v_n; 1
+                                    2 v_n - v_(n-1); 2 3 (v_n - v_(n-1)) + v_(n-2); 3
+                                    4 (v_n + v_(n-2)) - 6 v_(n-1) - v_(n-3); 4 (default)
+                                    5 (v_n - v_(n-3)) + 10 (v_(n-2) - v_(n-1)) + v_(n-4).
+                                    Only the iteration count depends on it (may be changed
+                                    after the build) */
 #define B200FEM_OPT_ELEM_TILE 6  /* non-linear element kernels: 0 (default) tets one thread per
                                     element in registers, hexes the staged kernel's large tile;
                                     1 the shared-memory staged kernel with its large tile (tet 256 /
