@@ -501,6 +501,9 @@ int build_pack(Engine& eng) {
   for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
   eng.pcg_grid = G;
   d.n_pieces = (int)piece_model.size();
+  eng.pcg_every_cta_rows = 1;
+  for (int c = 0; c < G; c++)
+    if (cta_piece[c + 1] <= cta_piece[c]) eng.pcg_every_cta_rows = 0;
   // default SpMV row width (the autotuner may change it later)
   if (eng.opt_row_lanes > 0) {
     eng.pcg_row_lanes = eng.opt_row_lanes;

@@ -201,6 +201,7 @@ struct Engine {
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_strided = 0;  // pieces dealt to CTAs across models (large packs)
+  int pcg_every_cta_rows = 0;  // every CTA of the PCG split holds at least one piece
   // plane constraints (b200fem_set_plane_constraints): per constrained node
   // its unit normal and offset; enforced by the ConstrainedBackwardEuler step
   std::vector<int> cons_node;

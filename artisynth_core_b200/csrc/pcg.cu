@@ -138,6 +138,10 @@ struct PcgArgs {
   const int* act_node;
   const int* row_model;
   const int* model_active;  // per model: 0 = not solved in this call (or null: all)
+  // one model whose rows every CTA holds: every CTA computes the same
+  // scalars and takes the same decisions (loop exits, restarts) without
+  // agreeing through global memory
+  int single_model;
   // plane constraints (ConstrainedBackwardEuler), or null: per row the unit
   // normal (zero for rows without a constraint) and the plane's offset
   const double* row_nrm;
@@ -939,7 +943,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       const int nsumw = min(max(npc, 1), 8);
       const int nroww = (blockDim.x >> 5) - nsumw;
       for (int j = threadIdx.x; j < npc * 3; j += blockDim.x) pacc[j / 3][j % 3] = 0;
-      bool stop = false;
+      bool stop = false, conv_exit = false;
       const CtaRows ar = active_view();
       const int nact = ar.nloc;
       for (int c0 = 0, first = 1; c0 < nact || first; c0 += kRowChunk, first = 0) {
@@ -999,6 +1003,12 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           __syncthreads();
           if (first && (idx >= a.max_iter || (a.variant == 0 && it >= kRoundCap))) {
             stop = true;
+            break;
+          }
+          if (first && a.single_model && s_conv[0]) {
+            // the model met the recurrence test at this iteration: the
+            // iterate is final, and every CTA leaves here alike
+            conv_exit = true;
             break;
           }
           // z = n + beta z; q = m + beta q; s = w + beta s; p = u + beta p;
@@ -1117,7 +1127,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         }
         __syncthreads();
       }
-      if (stop) {
+      if (stop || conv_exit) {
         total_it += it;
         break;
       }
@@ -1204,9 +1214,14 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     }
     __syncthreads();
     // every CTA must agree on a restart: publish and read after a barrier
-    if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
-    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
-    if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
+    // (one model held by every CTA: each reached the same decision)
+    if (a.single_model) {
+      if (!s_restart) break;
+    } else {
+      if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+      if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
+    }
     // continue with classic PCG, whose attainable accuracy is better than
     // that of the pipelined recurrences
     if (a.variant == 0) classic = true;
@@ -1295,6 +1310,7 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.act_node = d.act_node;
   a.row_model = d.row_model;
   a.model_active = eng.any_inactive ? d.model_active : nullptr;
+  a.single_model = (d.n_models == 1 && eng.pcg_every_cta_rows) ? 1 : 0;
   // constraints belong to the ConstrainedBackwardEuler step's solve only
   a.row_nrm = (update_state && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && d.row_nrm)
                   ? d.row_nrm
@@ -1603,6 +1619,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.act_node = nullptr;
   a.row_model = nullptr;
   a.model_active = nullptr;
+  a.single_model = 0;
   a.row_nrm = nullptr;
   a.row_off = nullptr;
   a.tol_override = 0;
