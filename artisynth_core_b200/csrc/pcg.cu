@@ -40,6 +40,9 @@ constexpr int kPcgThreads = 1024;
 constexpr int kPcgThreadsResident = 512;
 __host__ __device__ constexpr int pcg_block(bool resident) { return resident ? kPcgThreadsResident : kPcgThreads; }
 constexpr int kRowChunk = 512;
+// lanes per row in the SpMV passes outside the iteration (P0, P1, classic
+// phase A, true residual): several rows per warp, a group leader per row
+constexpr int kPassLanes = 8;
 constexpr int kMaxCtaPieces = 48;
 constexpr int kMaxRestarts = 10;
 // auto variant: iterations of one round (pipelined, then classic after the
@@ -205,9 +208,11 @@ __device__ __forceinline__ void warp_sum(double* sm) {
 
 // Reduce ND per-row values over the view's pieces in a fixed order and write
 // partials[buf][piece][k] for every local piece (zero for pieces the view
-// leaves out).  fn(i, row, j, lane, vals) runs per row (local row i, global
-// row `row`, local piece j), either by a whole warp (WARP_ROWS) or by one
-// thread.
+// leaves out).  Per row (local row i, global row `row`, local piece j) either
+// fn(i, row, j, lane, valid, vals) runs on a group of kPassLanes lanes
+// (WARP_ROWS: every lane of the warp calls it, `valid` false for a group
+// without a row, and the group's first lane holds the row's values) or
+// fn(i, row, j, 0, vals) on one thread.
 template <int ND, bool WARP_ROWS, typename Fn>
 __device__ void cta_row_pass(const PcgArgs& a, const CtaRows& cr, int buf, double (*rowbuf)[3],
                              double (*pacc)[3], Fn fn) {
@@ -217,14 +222,22 @@ __device__ void cta_row_pass(const PcgArgs& a, const CtaRows& cr, int buf, doubl
   for (int c0 = 0; c0 < cr.nloc; c0 += kRowChunk) {
     const int c1 = min(c0 + kRowChunk, cr.nloc);
     __syncthreads();
-    if (WARP_ROWS) {
-      for (int i = c0 + warp; i < c1; i += nwarps) {
-        const int j = cr.piece(i);
+    if constexpr (WARP_ROWS) {
+      constexpr int G = 32 / kPassLanes;
+      for (int base = c0 + warp * G; base < c1; base += nwarps * G) {
+        const int ia = base + lane / kPassLanes;
+        const bool valid = ia < c1;
+        int j = 0, li = 0, row = 0;
+        if (valid) {
+          j = cr.piece(ia);
+          li = cr.local(ia, j);
+          row = cr.row(ia, j);
+        }
         double vals[3] = {0, 0, 0};
-        fn(cr.local(i, j), cr.row(i, j), j, lane, vals);
-        if (lane == 0)
+        fn(li, row, j, lane, valid, vals);
+        if (valid && (lane & (kPassLanes - 1)) == 0)
 #pragma unroll
-          for (int k = 0; k < ND; k++) rowbuf[i - c0][k] = vals[k];
+          for (int k = 0; k < ND; k++) rowbuf[ia - c0][k] = vals[k];
       }
     } else {
       for (int i = c0 + (int)threadIdx.x; i < c1; i += blockDim.x) {
@@ -717,10 +730,29 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     for (int i = threadIdx.x; i <= nloc; i += blockDim.x) ro[i] = a.rowptr[r0 + i] - pbase;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) cs[i] = a.col[pbase + i];
     const MT* Sg = (const MT*)a.S + (size_t)pbase * 9;
-    for (int i = threadIdx.x; i < nb * 9; i += blockDim.x) Ss[i] = Sg[i];
+    // resident form: eight loads in flight per thread before their stores
+    // (the 64-register form copies one value at a time)
+    const int nv = nb * 9, stride = blockDim.x;
+    constexpr int U = RES ? 8 : 1;
+    for (int i0 = threadIdx.x; i0 < nv; i0 += U * stride) {
+      MT v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u * stride;
+        v[u] = i < nv ? Sg[i] : MT(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int i = i0 + u * stride;
+        if (i < nv) Ss[i] = v[u];
+      }
+    }
   }
-  if (blockIdx.x == 0)
-    for (int i = threadIdx.x; i <= a.max_iter + 1; i += blockDim.x) a.unconv[i] = 0;
+  // the per-iteration flags are cleared two iterations ahead of their use
+  // (iteration idx clears idx + 2, ordered before any write to it by the
+  // barriers of iterations idx and idx + 1); the first two and the restart
+  // slot here, before the first barrier
+  if (blockIdx.x == 0 && threadIdx.x < 3) a.unconv[threadIdx.x < 2 ? threadIdx.x : a.max_iter + 1] = 0;
   // models left out of this call are final from the start
   for (int j = threadIdx.x; j < npc; j += blockDim.x) {
     const int m = a.piece_model[s_gp[j]];
@@ -741,10 +773,11 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 
   // ---- P0: block-Jacobi inverse, r = b - S x0, u = Dinv r (published to
   // m1 for the next SpMV), ||b||^2
-  cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
+  cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
+                        [&](int i, int row, int, int ln, bool valid, double* vals) {
     double Ax[3];
-    view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
-    if (ln == 0) {
+    view_rows_spmv_group<MT, kPassLanes>(mv, i, row, valid, a.x, ln, Ax);
+    if (valid && (ln & (kPassLanes - 1)) == 0) {
       const MT* Db = (const MT*)a.S + (size_t)a.blk_diag[row] * 9;
       if (a.cached) Db = mv.S_s + (size_t)(a.blk_diag[row] - pbase) * 9;
       double d[9], inv[9];
@@ -827,6 +860,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       rescan(s_conv);
       for (int it = 0;; it++) {
         const int idx = total_it + it;
+        if (blockIdx.x == 0 && threadIdx.x == 0 && idx + 2 <= a.max_iter) a.unconv[idx + 2] = 0;
         // phase A: p = z + beta p; q = S z + beta q (z complete); p.q
         for (int j = threadIdx.x; j < npc; j += blockDim.x) {
           if (s_conv[j]) continue;
@@ -839,11 +873,12 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           total_it += it;
           break;
         }
-        cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int ln, double* vals) {
-          if (s_conv[j]) return;
+        cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
+                              [&](int i, int row, int j, int ln, bool valid, double* vals) {
+          const bool act = valid && !s_conv[j];
           double Az[3];
-          view_row_spmv<MT>(mv, i, row, a.m1, ln, Az);
-          if (ln == 0) {
+          view_rows_spmv_group<MT, kPassLanes>(mv, i, row, act, a.m1, ln, Az);
+          if (act && (ln & (kPassLanes - 1)) == 0) {
             project_row(a.row_nrm, row, Az);
             const double be = s_beta[j];
             double* pz = st.at(VU, i, row);
@@ -907,11 +942,12 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     // ---- P1: w = S u, m = Dinv w (published to m0); dots r.u, w.u, r.r
     for (int j = threadIdx.x; j < npc; j += blockDim.x) s_first[j] = 1;
     rescan(s_conv);
-    cta_row_pass<3, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int j, int ln, double* vals) {
-      if (s_conv[j]) return;
+    cta_row_pass<3, true>(a, active_view(), ph & 1, rowbuf, pacc,
+                          [&](int i, int row, int j, int ln, bool valid, double* vals) {
+      const bool act = valid && !s_conv[j];
       double Au[3];
-      view_row_spmv<MT>(mv, i, row, a.m1, ln, Au);
-      if (ln == 0) {
+      view_rows_spmv_group<MT, kPassLanes>(mv, i, row, act, a.m1, ln, Au);
+      if (act && (ln & (kPassLanes - 1)) == 0) {
         project_row(a.row_nrm, row, Au);
         double r[3], u[3], m[3], zero[3] = {0, 0, 0};
         load3(r, st.at(VR, i, row), 0);
@@ -934,6 +970,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 
     for (int it = 0;; it++) {
       const int idx = total_it + it;
+      if (blockIdx.x == 0 && threadIdx.x == 0 && idx + 2 <= a.max_iter) a.unconv[idx + 2] = 0;
       const double* mc = mbuf ? a.m1 : a.m0;
       double* mn = mbuf ? a.m0 : a.m1;
       // The SpMV n = S m does not depend on this iteration's scalars, so it
@@ -1164,10 +1201,11 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       for (int i = threadIdx.x; i < nloc; i += blockDim.x) store3(a.x, r0 + i, st.at(VX, i, r0 + i));
     rescan(s_done);
     if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
-    cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc, [&](int i, int row, int, int ln, double* vals) {
+    cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
+                          [&](int i, int row, int, int ln, bool valid, double* vals) {
       double Ax[3];
-      view_row_spmv<MT>(mv, i, row, a.x, ln, Ax);
-      if (ln == 0) {
+      view_rows_spmv_group<MT, kPassLanes>(mv, i, row, valid, a.x, ln, Ax);
+      if (valid && (ln & (kPassLanes - 1)) == 0) {
         double bv[3], r[3];
         load3(bv, a.b, row);
 #pragma unroll
