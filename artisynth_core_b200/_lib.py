@@ -26,7 +26,8 @@ ERR_BUDGET = -6
 ERR_TIMEOUT = -7
 ERR_NO_CONVERGE = -13
 
-ELEM_TET, ELEM_HEX = 0, 1
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID = 0, 1, 2, 3
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1

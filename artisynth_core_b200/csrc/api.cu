@@ -257,7 +257,9 @@ int build_pack(Engine& eng) {
   // chunk's shared memory, and the contribution lists re-indexed to them
   std::vector<int> chunk_row, chunk_eptr, chunk_elem, contrib_loc;
   eng.fused = false;
+  // (tets and hexes: the fused kernel is instantiated for those two)
   if (eng.opt_fused == 1 && eng.groups.size() == 1 && !eng.groups[0].nodal && !eng.groups[0].elem_inc &&
+      (eng.elem_type == B200FEM_ELEM_TET || eng.elem_type == B200FEM_ELEM_HEX) &&
       (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN || eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN)) {
     const size_t per = fused_elem_bytes(eng.elem_type, eng.groups[0].mat_kind, eng.precision == B200FEM_PREC_MIXED);
     const int emax = (int)(fused_smem_budget(eng.elem_type) / per);
@@ -630,6 +632,7 @@ int build_pack(Engine& eng) {
     // correction solves' own per-model results
     eng.refine_ok = eng.precision == B200FEM_PREC_MIXED && eng.groups.size() == 1 && !eng.groups[0].nodal &&
                     !eng.groups[0].elem_inc &&
+                    (eng.elem_type == B200FEM_ELEM_TET || eng.elem_type == B200FEM_ELEM_HEX) &&
                     (eng.groups[0].mat_kind == B200FEM_MAT_NEOHOOKEAN ||
                      eng.groups[0].mat_kind == B200FEM_MAT_MOONEYRIVLIN);
     if (eng.refine_ok) {
@@ -771,11 +774,10 @@ int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz,
 int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz, int n_elems,
                      const int* conn, const int* fixed) {
   ENG(h);
-  if (elem_type != B200FEM_ELEM_TET && elem_type != B200FEM_ELEM_HEX)
-    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
+  if (elem_nen(elem_type) == 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
   if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
-  int nen = elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  int nen = elem_nen(elem_type);
   ModelDesc& m = eng.models[0];
   m.elem_type = elem_type;
   m.n_nodes = n_nodes;
@@ -809,14 +811,13 @@ int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double
                       const int* conn, const int* fixed, int mat_kind, const double* params, double density,
                       int incomp, int* model_index) {
   ENG(h);
-  if (elem_type != B200FEM_ELEM_TET && elem_type != B200FEM_ELEM_HEX)
-    return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
+  if (elem_nen(elem_type) == 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown element type");
   if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn) return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
   if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_STVK || !params)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
   if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
   ModelDesc m;
-  const int nen = elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  const int nen = elem_nen(elem_type);
   m.elem_type = elem_type;
   m.n_nodes = n_nodes;
   m.n_elems = n_elems;

@@ -21,6 +21,14 @@ constexpr int kMaxNen = 8;
 constexpr int kMaxIp = 8;
 constexpr int kMatParams = 8;
 
+// nodes and integration points per element type (0 for an unknown type);
+// wedges and pyramids, like hexes, have one integration point per node
+__host__ __device__ constexpr int elem_nen(int type) {
+  return type == B200FEM_ELEM_TET ? 4 : type == B200FEM_ELEM_HEX ? 8 : type == B200FEM_ELEM_WEDGE ? 6
+         : type == B200FEM_ELEM_PYRAMID ? 5 : 0;
+}
+__host__ __device__ constexpr int elem_nip(int type) { return type == B200FEM_ELEM_TET ? 1 : elem_nen(type); }
+
 // Model as given by the caller (host, FP64).
 struct ModelDesc {
   int elem_type = B200FEM_ELEM_TET;
@@ -242,6 +250,9 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err);
 int build_pack(Engine& eng);
 void free_pack(Engine& eng);
 int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne);
+// dN/ds of the element's nodes at integration point k (k = -1: the warping
+// point) and the point's weight
+void shape_grads(int type, int k, double* g /* nen * 3 */, double* w);
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn);
 void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,

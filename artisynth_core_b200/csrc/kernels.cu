@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <type_traits>
 
 #include "device_math.cuh"
 #include "spmv.cuh"
@@ -43,6 +44,10 @@ __constant__ double c_hex_wgns[8 * 3];     // warping point (centre)
 __constant__ float c_tet_gns_f[12];
 __constant__ float c_hex_gns_f[8 * 8 * 3];
 __constant__ int c_pair_a[36], c_pair_b[36];
+// wedges and pyramids: [ip][node][3] and the warping point [node][3]
+__constant__ double c_wed_gns[6 * 6 * 3], c_wed_wgns[6 * 3];
+__constant__ double c_pyr_gns[5 * 5 * 3], c_pyr_wgns[5 * 3];
+__constant__ float c_wed_gns_f[6 * 6 * 3], c_pyr_gns_f[5 * 5 * 3];
 
 static bool g_const_ready[64] = {false};
 
@@ -68,7 +73,22 @@ static cudaError_t ensure_constants(int device) {
   int pa[36], pb[36], w = 0;
   for (int a = 0; a < 8; a++)
     for (int b = a; b < 8; b++) { pa[w] = a; pb[w] = b; w++; }
+  // wedge and pyramid tables from the host shape functions
+  double wed[6 * 6 * 3], wedw[18], pyr[5 * 5 * 3], pyrw[15], wt;
+  float wedf[108], pyrf[75];
+  for (int k = 0; k < 6; k++) shape_grads(B200FEM_ELEM_WEDGE, k, &wed[k * 18], &wt);
+  shape_grads(B200FEM_ELEM_WEDGE, -1, wedw, &wt);
+  for (int k = 0; k < 5; k++) shape_grads(B200FEM_ELEM_PYRAMID, k, &pyr[k * 15], &wt);
+  shape_grads(B200FEM_ELEM_PYRAMID, -1, pyrw, &wt);
+  for (int i = 0; i < 108; i++) wedf[i] = (float)wed[i];
+  for (int i = 0; i < 75; i++) pyrf[i] = (float)pyr[i];
   cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_wed_gns, wed, sizeof(wed))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_wed_wgns, wedw, sizeof(wedw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_pyr_gns, pyr, sizeof(pyr))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_pyr_wgns, pyrw, sizeof(pyrw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_wed_gns_f, wedf, sizeof(wedf))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_pyr_gns_f, pyrf, sizeof(pyrf))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_tet_gns, tet, sizeof(tet))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_hex_gns, hex, sizeof(hex))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_hex_wgns, hexw, sizeof(hexw))) != cudaSuccess) return e;
@@ -84,26 +104,77 @@ static cudaError_t ensure_constants(int device) {
 // triangle of the nen x nen element matrix
 template <int NEN>
 __device__ __forceinline__ void pair_of(int w, int& a, int& b) {
-  if (NEN == 8) {
+  if constexpr (NEN == 8) {
     a = c_pair_a[w];
     b = c_pair_b[w];
-  } else {
+  } else if constexpr (NEN == 4) {
     // 4-node table: (0,0)(0,1)(0,2)(0,3)(1,1)(1,2)(1,3)(2,2)(2,3)(3,3)
     const int ta[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
     const int tb[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
     a = ta[w];
     b = tb[w];
+  } else {
+    // row a of the upper triangle holds NEN - a pairs
+    a = 0;
+    while (w >= NEN - a) {
+      w -= NEN - a;
+      a++;
+    }
+    b = a + w;
   }
 }
 
+// dN_n/ds component c at integration point k
 template <typename T, int TYPE>
 __device__ __forceinline__ T gns(int k, int n, int c) {
-  if (TYPE == B200FEM_ELEM_TET) {
+  if constexpr (TYPE == B200FEM_ELEM_TET) {
     if constexpr (sizeof(T) == 8) return c_tet_gns[3 * n + c];
     else return c_tet_gns_f[3 * n + c];
-  } else {
+  } else if constexpr (TYPE == B200FEM_ELEM_HEX) {
     if constexpr (sizeof(T) == 8) return c_hex_gns[(k * 8 + n) * 3 + c];
     else return c_hex_gns_f[(k * 8 + n) * 3 + c];
+  } else if constexpr (TYPE == B200FEM_ELEM_WEDGE) {
+    if constexpr (sizeof(T) == 8) return c_wed_gns[(k * 6 + n) * 3 + c];
+    else return c_wed_gns_f[(k * 6 + n) * 3 + c];
+  } else {
+    if constexpr (sizeof(T) == 8) return c_pyr_gns[(k * 5 + n) * 3 + c];
+    else return c_pyr_gns_f[(k * 5 + n) * 3 + c];
+  }
+}
+
+// dN_n/ds at the warping point (StiffnessWarper3d: TetElement integration
+// point 0, HexElement centre, WedgeElement (1/3, 1/3, 0), PyramidElement
+// (0, 0, -1/2))
+template <int TYPE>
+__device__ __forceinline__ double wgns(int n, int c) {
+  if constexpr (TYPE == B200FEM_ELEM_TET) return c_tet_gns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_HEX) return c_hex_wgns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_WEDGE) return c_wed_wgns[3 * n + c];
+  else return c_pyr_wgns[3 * n + c];
+}
+
+// integration weight of point k (TetElement 1/6; HexElement Gauss 1;
+// WedgeElement 1/6; PyramidElement 81/100 for the four base points, 125/27
+// for the fifth)
+template <typename T, int TYPE>
+__device__ __forceinline__ T ip_weight(int k) {
+  if constexpr (TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_WEDGE) return T(1.0 / 6.0);
+  else if constexpr (TYPE == B200FEM_ELEM_HEX) return T(1);
+  else return k < 4 ? T(81 / 100.0) : T(125 / 27.0);
+}
+
+// lanes per element in the FP64 force kernel
+__host__ __device__ constexpr int force_slot(int type) { return elem_nip(type) > 1 ? 8 : 1; }
+
+// calls f(std::integral_constant<int, TYPE>) for the run-time element type
+template <typename F>
+static cudaError_t by_elem_type(int type, F&& f) {
+  switch (type) {
+    case B200FEM_ELEM_TET: return f(std::integral_constant<int, B200FEM_ELEM_TET>{});
+    case B200FEM_ELEM_HEX: return f(std::integral_constant<int, B200FEM_ELEM_HEX>{});
+    case B200FEM_ELEM_WEDGE: return f(std::integral_constant<int, B200FEM_ELEM_WEDGE>{});
+    case B200FEM_ELEM_PYRAMID: return f(std::integral_constant<int, B200FEM_ELEM_PYRAMID>{});
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -177,8 +248,8 @@ __device__ bool block_inactive(const ElemArgs& a, int ebase, int epb) {
 // integration point: shape gradients, dv, stress, tangent).
 template <int TYPE, int MAT, typename T, int EPB>
 struct ElemSmem {
-  static constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  static constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  static constexpr int NEN = elem_nen(TYPE);
+  static constexpr int NIP = elem_nip(TYPE);
   static constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
   static constexpr int NREC = EPB * NIP;
   static constexpr size_t bytes() {
@@ -254,7 +325,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
     T detJ = invert3(invJ, J);
     myinv += !(detJ > T(0));
     mydet = fmin(mydet, (double)detJ);
-    const T w = TYPE == B200FEM_ELEM_TET ? T(1.0 / 6.0) : T(1);
+    const T w = ip_weight<T, TYPE>(k);
     T dv = detJ * w;
     sdv[t] = dv;
 #pragma unroll
@@ -358,7 +429,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
 // ---------------------------------------------------------------------------
 template <int TYPE, typename T>
 __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corotated) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NEN = elem_nen(TYPE);
   constexpr int NPAIR = NEN * (NEN + 1) / 2;
   constexpr int EPB = TYPE == B200FEM_ELEM_TET ? 32 : 8;
   __shared__ double sx[EPB][NEN][3];
@@ -388,9 +459,7 @@ __global__ void __launch_bounds__(256) elem_linear_kernel(ElemArgs a, int corota
       for (int i = 0; i < 9; i++) J[i] = 0;
 #pragma unroll
       for (int n = 0; n < NEN; n++) {
-        double g0, g1, g2;
-        if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * n]; g1 = c_tet_gns[3 * n + 1]; g2 = c_tet_gns[3 * n + 2]; }
-        else { g0 = c_hex_wgns[3 * n]; g1 = c_hex_wgns[3 * n + 1]; g2 = c_hex_wgns[3 * n + 2]; }
+        const double g0 = wgns<TYPE>(n, 0), g1 = wgns<TYPE>(n, 1), g2 = wgns<TYPE>(n, 2);
 #pragma unroll
         for (int r = 0; r < 3; r++) {
           J[3 * r] += sx[el][n][r] * g0;
@@ -751,17 +820,19 @@ static cudaError_t launch_nonlinear(const ElemArgs& a, int ne, cudaStream_t st) 
 // nodal forces f_a = sum_ip sigma g_a dv -- while the tangent blocks come
 // from the FP32 element kernel.  Nodal forces nearly cancel the external
 // load, so their small net value needs FP64 terms.  One thread per element
-// (tets) or per integration point, the 8 points of a hex reduced over 8
-// consecutive lanes in a fixed butterfly order.
+// (tets) or per integration point: an element of several points holds 8
+// consecutive lanes (lanes past its points idle), reduced in a fixed
+// butterfly order.
 // ---------------------------------------------------------------------------
 template <int TYPE, int MAT, int INC>
 __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  constexpr int NEN = elem_nen(TYPE);
+  constexpr int NIP = elem_nip(TYPE);
+  constexpr int SLOT = force_slot(TYPE);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = a.e0 + (int)(t / NIP);
-  const int k = (int)(t % NIP);
-  bool live = e < a.e1;
+  const int e = a.e0 + (int)(t / SLOT);
+  const int k = (int)(t % SLOT);
+  bool live = e < a.e1 && k < NIP;
   if (live && a.active && !a.active[a.elem_model[e]]) live = false;
   double mydet = 1.0e300;
   int myinv = 0;
@@ -789,7 +860,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
     matmul3(F, J, iJ0);
     const double detF = det3(F);
     const double detJ = invert3(invJ, J);
-    const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
+    const double dv = detJ * ip_weight<double, TYPE>(k);
     myinv = !(detJ > 0.0);
     mydet = detJ;
     const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
@@ -825,7 +896,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
   }
   if (a.det_stats) warp_record_det(a.flags, a.mindet, mydet, myinv);
   if constexpr (NIP > 1) {
-    // sum the points of one element: lanes 8q..8q+7 hold its 8 points
+    // sum the points of one element: lanes 8q..8q+7 hold its points
 #pragma unroll
     for (int n = 0; n < NEN; n++)
 #pragma unroll
@@ -988,8 +1059,7 @@ static cudaError_t launch_tet(const ElemArgs& a, int ne, cudaStream_t st) {
 
 template <int TYPE, int MAT, int INC>
 static cudaError_t launch_force(const ElemArgs& a, int ne, cudaStream_t st) {
-  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
-  const long long threads = (long long)ne * NIP;
+  const long long threads = (long long)ne * force_slot(TYPE);
   elem_force_kernel<TYPE, MAT, INC><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -1030,8 +1100,9 @@ struct FusedArgs {
 
 template <int TYPE, int MAT, typename T>
 struct FusedSmem {
-  static constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  static constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  static_assert(TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_HEX, "fused assembly: tets and hexes");
+  static constexpr int NEN = elem_nen(TYPE);
+  static constexpr int NIP = elem_nip(TYPE);
   static constexpr int DS = MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36;
   static constexpr size_t per_elem() { return sizeof(T) * (size_t)NIP * (NEN * 3 + 1 + 6 + DS); }
 };
@@ -1266,7 +1337,7 @@ __global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, co
                                       const int* __restrict__ sidx, const double* __restrict__ rest_vol,
                                       const double* __restrict__ mat_node, double* __restrict__ vol,
                                       double* __restrict__ pres, double* __restrict__ kp) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NEN = elem_nen(TYPE);
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double v = 0;
@@ -1277,9 +1348,7 @@ __global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, co
 #pragma unroll
     for (int k = 0; k < NEN; k++) {
       const double* pk = x + 3 * (size_t)nodes[k];
-      double g0, g1, g2;
-      if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * k]; g1 = c_tet_gns[3 * k + 1]; g2 = c_tet_gns[3 * k + 2]; }
-      else { g0 = c_hex_gns[(a * 8 + k) * 3]; g1 = c_hex_gns[(a * 8 + k) * 3 + 1]; g2 = c_hex_gns[(a * 8 + k) * 3 + 2]; }
+      const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1), g2 = gns<double, TYPE>(a, k, 2);
 #pragma unroll
       for (int r = 0; r < 3; r++) {
         J[3 * r] += pk[r] * g0;
@@ -1287,8 +1356,8 @@ __global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, co
         J[3 * r + 2] += pk[r] * g2;
       }
     }
-    // tet: V_e = det(J)/6 shared by four nodes; hex: dv of point a (w = 1)
-    v += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 / 4 : det3(J);
+    // tet: V_e = det(J)/6 shared by four nodes; otherwise the dv of point a
+    v += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 / 4 : det3(J) * ip_weight<double, TYPE>(a);
   }
   vol[n] = v;
   double p = 0, k = 0;
@@ -1316,7 +1385,7 @@ __global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int*
                               const int* __restrict__ inc_slot, const int* __restrict__ conn,
                               const double* __restrict__ x, const int* __restrict__ sidx,
                               const int* __restrict__ nbr_ptr, double* __restrict__ divblk) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
+  constexpr int NEN = elem_nen(TYPE);
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   double* out = divblk + 3 * (size_t)nbr_ptr[n];
@@ -1346,18 +1415,18 @@ __global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int*
     } else {
       double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
+      for (int k = 0; k < NEN; k++) {
         const double* pk = x + 3 * (size_t)nodes[k];
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
-          for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * c_hex_gns[(a * 8 + k) * 3 + c];
+          for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * gns<double, TYPE>(a, k, c);
       }
-      const double dv = invert3(iJ, J);
+      const double dv = invert3(iJ, J) * ip_weight<double, TYPE>(a);
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const double g0 = c_hex_gns[(a * 8 + k) * 3], g1 = c_hex_gns[(a * 8 + k) * 3 + 1],
-                     g2 = c_hex_gns[(a * 8 + k) * 3 + 2];
+      for (int k = 0; k < NEN; k++) {
+        const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1),
+                     g2 = gns<double, TYPE>(a, k, 2);
         double* o = out + 3 * slot[k];
 #pragma unroll
         for (int c = 0; c < 3; c++) o[c] += dv * (iJ[c] * g0 + iJ[3 + c] * g1 + iJ[6 + c] * g2);
@@ -1370,28 +1439,23 @@ cudaError_t launch_nodal_pressure(Engine& eng) {
   DevPack& d = eng.d;
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
-  if (eng.elem_type == B200FEM_ELEM_TET)
-    nodal_pressure_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+  return by_elem_type(eng.elem_type, [&](auto tag) {
+    nodal_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
         d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
         d.node_kp);
-  else
-    nodal_pressure_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
-        d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
-        d.node_kp);
-  return cudaGetLastError();
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_divblk(Engine& eng) {
   DevPack& d = eng.d;
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
-  if (eng.elem_type == B200FEM_ELEM_TET)
-    divblk_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+  return by_elem_type(eng.elem_type, [&](auto tag) {
+    divblk_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
         d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
-  else
-    divblk_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
-        d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
-  return cudaGetLastError();
+    return cudaGetLastError();
+  });
 }
 
 // ELEMENT soft incompressibility with one pressure value per element (tet
@@ -1405,8 +1469,8 @@ __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ 
                                         const int* __restrict__ elem_model, const double* __restrict__ x,
                                         const double* __restrict__ rest_vol, const double* __restrict__ mat,
                                         double* __restrict__ elem_p, double* __restrict__ elem_r) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  constexpr int NEN = elem_nen(TYPE);
+  constexpr int NIP = elem_nip(TYPE);
   const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= e1) return;
   const int* nodes = conn + (size_t)e * NEN;
@@ -1417,9 +1481,7 @@ __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ 
 #pragma unroll
     for (int k = 0; k < NEN; k++) {
       const double* pk = x + 3 * (size_t)nodes[k];
-      double g0, g1, g2;
-      if (TYPE == B200FEM_ELEM_TET) { g0 = c_tet_gns[3 * k]; g1 = c_tet_gns[3 * k + 1]; g2 = c_tet_gns[3 * k + 2]; }
-      else { g0 = c_hex_gns[(q * 8 + k) * 3]; g1 = c_hex_gns[(q * 8 + k) * 3 + 1]; g2 = c_hex_gns[(q * 8 + k) * 3 + 2]; }
+      const double g0 = gns<double, TYPE>(q, k, 0), g1 = gns<double, TYPE>(q, k, 1), g2 = gns<double, TYPE>(q, k, 2);
 #pragma unroll
       for (int r = 0; r < 3; r++) {
         J[3 * r] += pk[r] * g0;
@@ -1427,7 +1489,7 @@ __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ 
         J[3 * r + 2] += pk[r] * g2;
       }
     }
-    V += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 : det3(J);
+    V += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 : det3(J) * ip_weight<double, TYPE>(q);
   }
   const double* mp = mat + (size_t)elem_model[e] * kMatParams;
   const double K = mp[5], V0 = rest_vol[e], Jp = V / V0;
@@ -1448,13 +1510,11 @@ cudaError_t launch_element_pressure(Engine& eng) {
   for (const ElemGroup& g : eng.groups) {
     if (!g.elem_inc || g.e1 <= g.e0) continue;
     const int threads = 128, blocks = (g.e1 - g.e0 + threads - 1) / threads;
-    if (eng.elem_type == B200FEM_ELEM_TET)
-      element_pressure_kernel<B200FEM_ELEM_TET><<<blocks, threads, 0, eng.stream>>>(
+    cudaError_t e = by_elem_type(eng.elem_type, [&](auto tag) {
+      element_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
           g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.elem_p, d.elem_r);
-    else
-      element_pressure_kernel<B200FEM_ELEM_HEX><<<blocks, threads, 0, eng.stream>>>(
-          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.elem_p, d.elem_r);
-    cudaError_t e = cudaGetLastError();
+      return cudaGetLastError();
+    });
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1473,8 +1533,9 @@ cudaError_t launch_element_pressure(Engine& eng) {
 // ---------------------------------------------------------------------------
 template <int TYPE, int MAT>
 __global__ void __launch_bounds__(128) elem_kv_kernel(ElemArgs a, const double* __restrict__ v) {
-  constexpr int NEN = TYPE == B200FEM_ELEM_TET ? 4 : 8;
-  constexpr int NIP = TYPE == B200FEM_ELEM_TET ? 1 : 8;
+  static_assert(TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_HEX, "refinement: tets and hexes");
+  constexpr int NEN = elem_nen(TYPE);
+  constexpr int NIP = elem_nip(TYPE);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int e = a.e0 + (int)(t / NIP);
   const int k = (int)(t % NIP);
@@ -1504,7 +1565,7 @@ __global__ void __launch_bounds__(128) elem_kv_kernel(ElemArgs a, const double* 
     matmul3(F, J, iJ0);
     const double detF = det3(F);
     const double detJ = invert3(invJ, J);
-    const double dv = detJ * (TYPE == B200FEM_ELEM_TET ? 1.0 / 6.0 : 1.0);
+    const double dv = detJ * ip_weight<double, TYPE>(k);
     const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
     double sig[6], D[36], ca = 0, cb = 0;
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) neohookean_point<double>(sig, &ca, &cb, mp[0], mp[1], F, detF);
@@ -1676,10 +1737,10 @@ cudaError_t prepare_kernels(Engine& eng) {
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
   for (ElemGroup g : eng.groups) {
     g.e1 = g.e0 - 1;  // ne = -1: set attributes only
-    if (g.elem_type == B200FEM_ELEM_TET)
-      e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);
-    else
-      e = fp32 ? launch_group<B200FEM_ELEM_HEX, float>(eng, g, true) : launch_group<B200FEM_ELEM_HEX, double>(eng, g, false);
+    e = by_elem_type(g.elem_type, [&](auto tag) {
+      constexpr int TY = decltype(tag)::value;
+      return fp32 ? launch_group<TY, float>(eng, g, true) : launch_group<TY, double>(eng, g, false);
+    });
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1769,10 +1830,10 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   if ((e = launch_divblk(eng)) != cudaSuccess) return e;
   if ((e = launch_element_pressure(eng)) != cudaSuccess) return e;
   for (const ElemGroup& g : eng.groups) {
-    if (g.elem_type == B200FEM_ELEM_TET)
-      e = fp32 ? launch_group<B200FEM_ELEM_TET, float>(eng, g, true) : launch_group<B200FEM_ELEM_TET, double>(eng, g, false);
-    else
-      e = fp32 ? launch_group<B200FEM_ELEM_HEX, float>(eng, g, true) : launch_group<B200FEM_ELEM_HEX, double>(eng, g, false);
+    e = by_elem_type(g.elem_type, [&](auto tag) {
+      constexpr int TY = decltype(tag)::value;
+      return fp32 ? launch_group<TY, float>(eng, g, true) : launch_group<TY, double>(eng, g, false);
+    });
     if (e != cudaSuccess) return e;
   }
   const int* act = eng.any_inactive ? d.model_active : nullptr;

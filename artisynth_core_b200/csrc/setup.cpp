@@ -55,8 +55,74 @@ double invert33(double* inv, const double* d) {
   return det;
 }
 
+// WedgeElement.getdNds (WedgeElement.java:193-206): N_i = L_t(s1, s2) h_z(r)
+// with the triangle coordinates L = (1 - s1 - s2, s1, s2) of node t = i % 3
+// and the layer factor h = (1 -/+ r)/2 of z = i / 3
+void wedge_grad(double* g, int i, double s1, double s2, double r) {
+  const int t = i % 3;
+  const double sgn = i < 3 ? -1.0 : 1.0, h = 0.5 * (1 + sgn * r);
+  const double L = t == 0 ? 1 - s1 - s2 : (t == 1 ? s1 : s2);
+  const double dL1 = t == 0 ? -1.0 : (t == 1 ? 1.0 : 0.0), dL2 = t == 0 ? -1.0 : (t == 2 ? 1.0 : 0.0);
+  g[0] = dL1 * h;
+  g[1] = dL2 * h;
+  g[2] = L * 0.5 * sgn;
+}
+
+// PyramidElement.getdNds (PyramidElement.java:153-175): base nodes (a, b, -1)
+// with N = (1 + a s0)(1 + b s1)(1 - s2)/8, apex N = (1 + s2)/2
+const double kPyrBase[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+void pyramid_grad(double* g, int i, double s0, double s1, double s2) {
+  if (i == 4) {
+    g[0] = g[1] = 0;
+    g[2] = 0.5;
+    return;
+  }
+  const double a = kPyrBase[i][0], b = kPyrBase[i][1];
+  g[0] = 0.125 * a * (1 + b * s1) * (1 - s2);
+  g[1] = 0.125 * (1 + a * s0) * b * (1 - s2);
+  g[2] = -0.125 * (1 + a * s0) * (1 + b * s1);
+}
+
+}  // namespace
+
 // Shape gradients for integration point k (or the warping point, k = -1).
 void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
+  if (type == B200FEM_ELEM_WEDGE) {
+    // integration points (WedgeElement.java:36-49): (1/6, 1/6), (2/3, 1/6),
+    // (1/6, 2/3) on the layers r = -/+ 1/sqrt(3), weight 1/6; warping point
+    // (1/3, 1/3, 0), weight 1 (:128-133)
+    double s1 = 1.0 / 3.0, s2 = 1.0 / 3.0, r = 0;
+    *w = 1;
+    if (k >= 0) {
+      const double a = 1.0 / 6.0, b = 2.0 / 3.0, q = 1 / std::sqrt(3.0);
+      const int t = k % 3;
+      s1 = t == 1 ? b : a;
+      s2 = t == 2 ? b : a;
+      r = k < 3 ? -q : q;
+      *w = 1.0 / 6.0;
+    }
+    for (int i = 0; i < 6; i++) wedge_grad(g + 3 * i, i, s1, s2, r);
+    return;
+  }
+  if (type == B200FEM_ELEM_PYRAMID) {
+    // integration points (PyramidElement.java:69-83): (-/+a, -/+a, -2/3) in
+    // base-node order, weight 81/100, and (0, 0, 2/5), weight 125/27, with
+    // a = (8/5) sqrt(2/15); warping point (0, 0, -1/2), weight 128/27 (:38-44)
+    double s0 = 0, s1 = 0, s2 = -0.5;
+    *w = 128 / 27.0;
+    if (k >= 0 && k < 4) {
+      const double a = (8 / 5.0) * std::sqrt(2 / 15.0);
+      s0 = kPyrBase[k][0] * a;
+      s1 = kPyrBase[k][1] * a;
+      s2 = -2.0 / 3.0;
+      *w = 81 / 100.0;
+    } else if (k == 4) {
+      s2 = 2.0 / 5.0;
+      *w = 125 / 27.0;
+    }
+    for (int i = 0; i < 5; i++) pyramid_grad(g + 3 * i, i, s0, s1, s2);
+    return;
+  }
   if (type == B200FEM_ELEM_TET) {
     std::memcpy(g, kTetGNs, sizeof(kTetGNs));
     *w = 1.0 / 6.0;
@@ -73,6 +139,8 @@ void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
     *w = 1;
   }
 }
+
+namespace {
 
 // J = sum_n x_n (outer) dN_n/ds  (IntegrationPoint3d.computeJacobian,
 // IntegrationPoint3d.java:190-201)
@@ -116,9 +184,10 @@ void add_bdb(double* K, const double* gi, const double* D, const double* gj, dou
 
 int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
   if (nx < 1 || ny < 1 || nz < 1) return B200FEM_ERR_INVALID_ARG;
-  if (type != B200FEM_ELEM_TET && type != B200FEM_ELEM_HEX) return B200FEM_ERR_INVALID_ARG;
+  if (elem_nen(type) == 0) return B200FEM_ERR_INVALID_ARG;
   *nn = (nx + 1) * (ny + 1) * (nz + 1);
-  *ne = (type == B200FEM_ELEM_TET ? 5 : 1) * nx * ny * nz;
+  const int per_cell[4] = {5, 1, 2, 3};  // tet, hex, wedge, pyramid
+  *ne = per_cell[type] * nx * ny * nz;
   return B200FEM_OK;
 }
 
@@ -126,7 +195,12 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
 // (:86-126) splits each cell with Tetrahedralizer.subdivideHex(allOnX =
 // (i+j+k) odd) (Tetrahedralizer.java:135-141), whose parseCode /
 // getTetIndicesForHex (:203-300) reduce to the two 5-tet tables below;
-// createHexGrid (:203-255).
+// createHexGrid (:203-255); createWedgeGrid (:266-310): two wedges per cell;
+// createPyramidGrid (:137-195): three pyramids per cell sharing the apex
+// corner that the cell's (i, j, k) parities select (apexNodeTable, :128-129),
+// the bases being the three faces through the opposite corner in the order
+// and orientation of PyramidElement.createCubeTesselation
+// (PyramidElement.java:216-270).
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn) {
   const double sx = 1.0 / nx, sy = 1.0 / ny, sz = 1.0 / nz;
@@ -153,6 +227,23 @@ void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int 
         if (type == B200FEM_ELEM_HEX) {
           std::memcpy(conn + 8 * e, c, sizeof(c));
           e++;
+        } else if (type == B200FEM_ELEM_WEDGE) {
+          static const int kWedge[2][6] = {{0, 1, 4, 3, 2, 7}, {1, 5, 4, 2, 6, 7}};
+          for (int q = 0; q < 2; q++, e++)
+            for (int a = 0; a < 6; a++) conn[6 * e + a] = c[kWedge[q][a]];
+        } else if (type == B200FEM_ELEM_PYRAMID) {
+          static const int kApex[8] = {2, 3, 1, 0, 6, 7, 5, 4};
+          static const int kBase[8][3][4] = {
+              {{6, 2, 3, 7}, {6, 5, 1, 2}, {6, 7, 4, 5}}, {{7, 6, 2, 3}, {7, 3, 0, 4}, {7, 4, 5, 6}},
+              {{4, 5, 6, 7}, {4, 0, 1, 5}, {4, 7, 3, 0}}, {{5, 1, 2, 6}, {5, 4, 0, 1}, {5, 6, 7, 4}},
+              {{2, 3, 7, 6}, {2, 1, 0, 3}, {2, 6, 5, 1}}, {{3, 2, 1, 0}, {3, 0, 4, 7}, {3, 7, 6, 2}},
+              {{0, 3, 2, 1}, {0, 1, 5, 4}, {0, 4, 7, 3}}, {{1, 0, 3, 2}, {1, 2, 6, 5}, {1, 5, 4, 0}}};
+          const int code = (i % 2 == 0 ? 1 : 0) | (j % 2 == 0 ? 2 : 0) | (k % 2 == 0 ? 4 : 0);
+          const int apex = kApex[code];
+          for (int q = 0; q < 3; q++, e++) {
+            for (int a = 0; a < 4; a++) conn[5 * e + a] = c[kBase[apex][q][a]];
+            conn[5 * e + 4] = c[apex];
+          }
         } else {
           const int(*t)[4] = ((i + j + k) % 2 != 0) ? kOdd : kEven;
           for (int q = 0; q < 5; q++, e++)
@@ -182,9 +273,9 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 }
 
 int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
-  const int nen = m.elem_type == B200FEM_ELEM_TET ? 4 : 8;
+  const int nen = elem_nen(m.elem_type);
   h.nen = nen;
-  h.nip = m.elem_type == B200FEM_ELEM_TET ? 1 : 8;
+  h.nip = elem_nip(m.elem_type);
   h.npair = nen * (nen + 1) / 2;
   const int N = m.n_nodes, E = m.n_elems;
   for (int q = 0; q < E * nen; q++)
@@ -322,12 +413,15 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   if (h.incomp == B200FEM_INCOMP_NODAL) {
     // nodal rest volumes (updateNodalRestVolumes, FemModel3d.java:2594-2628)
     h.node_rest_vol.assign(N, 0);
+    double wts[kMaxNen], g[kMaxNen * 3];
+    for (int a = 0; a < nen; a++) shape_grads(m.elem_type, a, g, &wts[a]);
     for (int e = 0; e < E; e++) {
       const int* nodes = &m.conn[(size_t)e * nen];
       if (m.elem_type == B200FEM_ELEM_TET) {
         for (int a = 0; a < 4; a++) h.node_rest_vol[nodes[a]] += h.rest_vol[e] / 4;
       } else {
-        for (int a = 0; a < 8; a++) h.node_rest_vol[nodes[a]] += h.detJ0[(size_t)e * 8 + a];
+        // integration point a maps to node a: its rest dv = w_a detJ0_a
+        for (int a = 0; a < nen; a++) h.node_rest_vol[nodes[a]] += wts[a] * h.detJ0[(size_t)e * nen + a];
       }
     }
   }

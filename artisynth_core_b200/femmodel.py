@@ -99,7 +99,7 @@ def grid_dims(elem_type, nx, ny, nz):
 
 def create_grid(elem_type, wx, wy, wz, nx, ny, nz):
     nn, ne = grid_dims(elem_type, nx, ny, nz)
-    nen = 4 if elem_type == L.ELEM_TET else 8
+    nen = L.ELEM_NODES[elem_type]
     xyz = np.zeros(3 * nn)
     conn = np.zeros(nen * ne, dtype=np.int32)
     L.check(L.lib().b200fem_create_grid(elem_type, wx, wy, wz, nx, ny, nz, L.dptr(xyz), L.iptr(conn)))
@@ -114,7 +114,8 @@ def jitter_grid(xyz, nx, ny, nz, wx, wy, wz, frac, seed):
 
 
 class FemFactory:
-    """FemFactory.createTetGrid / createHexGrid (FemFactory.java:86-255)."""
+    """FemFactory.createTetGrid / createHexGrid / createWedgeGrid /
+    createPyramidGrid (FemFactory.java:86-310)."""
 
     @staticmethod
     def createTetGrid(model, wx, wy, wz, nx, ny, nz):
@@ -126,6 +127,18 @@ class FemFactory:
     def createHexGrid(model, wx, wy, wz, nx, ny, nz):
         m = model if model is not None else FemModel3d()
         m._set_grid(L.ELEM_HEX, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
+    def createWedgeGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_WEDGE, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
+    def createPyramidGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_PYRAMID, wx, wy, wz, nx, ny, nz)
         return m
 
 
@@ -191,7 +204,7 @@ class FemModel3d:
     def setMesh(self, elem_type, rest, conn, fixed=None):
         self.elem_type = elem_type
         self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1, 3)
-        nen = 4 if elem_type == L.ELEM_TET else 8
+        nen = L.ELEM_NODES[elem_type]
         self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, nen)
         self.fixed = (np.zeros(self.rest.shape[0], dtype=np.int32) if fixed is None
                       else np.ascontiguousarray(fixed, dtype=np.int32))

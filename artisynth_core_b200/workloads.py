@@ -137,6 +137,20 @@ def small_hex_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.0
                     gravity, h, steps, tol=1e-13)
 
 
+def small_wedge_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.03, seed=13,
+                     gravity=(0.0, 0.0, -9.81), h=0.005, steps=10) -> Workload:
+    """Small beam of wedges (FemFactory.createWedgeGrid: two per cell)."""
+    return Workload("small_wedge_beam", L.ELEM_WEDGE, cells, widths, jitter, seed, material, 1000.0, "xmin",
+                    gravity, h, steps, tol=1e-13)
+
+
+def small_pyramid_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.03, seed=17,
+                       gravity=(0.0, 0.0, -9.81), h=0.005, steps=10) -> Workload:
+    """Small beam of pyramids (FemFactory.createPyramidGrid: three per cell)."""
+    return Workload("small_pyramid_beam", L.ELEM_PYRAMID, cells, widths, jitter, seed, material, 1000.0, "xmin",
+                    gravity, h, steps, tol=1e-13)
+
+
 def batched_beams(count=256, seed=3, cell=0.05, jitter=0.05, large_frac=0.0, large_n=(80, 120)):
     """Uneven NeoHookean tet beams: n x m x m cells of size `cell` (5 tets per
     cell), n ~ U{4..60}, m ~ U{2..8}, E log-uniform in [1e3, 1e6] Pa, nu

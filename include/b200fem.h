@@ -52,6 +52,8 @@ extern "C" {
 /* element types */
 #define B200FEM_ELEM_TET 0 /* TetElement, 4 nodes, 1 integration point */
 #define B200FEM_ELEM_HEX 1 /* HexElement, 8 nodes, 8 Gauss points */
+#define B200FEM_ELEM_WEDGE 2   /* WedgeElement, 6 nodes, 6 integration points */
+#define B200FEM_ELEM_PYRAMID 3 /* PyramidElement, 5 nodes, 5 integration points */
 
 /* materials (parameter layout of b200fem_set_material) */
 #define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */

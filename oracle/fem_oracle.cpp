@@ -26,7 +26,7 @@
 
 namespace {
 
-enum { ELEM_TET = 0, ELEM_HEX = 1 };
+enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3 };
 enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2, MAT_STVK = 3 };
 enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
 
@@ -171,6 +171,26 @@ static void hex_dNds(double* out, int i, double s0, double s1, double s2) {
   out[2] = 0.125 * (1 + g0 * s0) * (1 + g1 * s1) * (g2);
 }
 
+// WedgeElement.getdNds (WedgeElement.java:193-206), node by node, at
+// (s1, s2, r)
+static void wedge_dNds(double* out, int i, double s1, double s2, double r) {
+  const double lo = 1 - r, hi = 1 + r, t = 1 - s1 - s2;
+  const double v[6][3] = {{-0.5 * lo, -0.5 * lo, -0.5 * t}, {0.5 * lo, 0, -0.5 * s1}, {0, 0.5 * lo, -0.5 * s2},
+                          {-0.5 * hi, -0.5 * hi, 0.5 * t},  {0.5 * hi, 0, 0.5 * s1},  {0, 0.5 * hi, 0.5 * s2}};
+  for (int c = 0; c < 3; c++) out[c] = v[i][c];
+}
+
+// PyramidElement.getdNds (PyramidElement.java:153-175), node by node
+static void pyramid_dNds(double* out, int i, double s0, double s1, double s2) {
+  const double v[5][3] = {
+      {-0.125 * (1 - s1) * (1 - s2), -0.125 * (1 - s0) * (1 - s2), -0.125 * (1 - s0) * (1 - s1)},
+      {+0.125 * (1 - s1) * (1 - s2), -0.125 * (1 + s0) * (1 - s2), -0.125 * (1 + s0) * (1 - s1)},
+      {+0.125 * (1 + s1) * (1 - s2), +0.125 * (1 + s0) * (1 - s2), -0.125 * (1 + s0) * (1 + s1)},
+      {-0.125 * (1 + s1) * (1 - s2), +0.125 * (1 - s0) * (1 - s2), -0.125 * (1 - s0) * (1 + s1)},
+      {0, 0, 0.5}};
+  for (int c = 0; c < 3; c++) out[c] = v[i][c];
+}
+
 struct ShapeTable {
   int nen, nip;
   std::vector<double> GNs;  // nip * nen * 3
@@ -187,6 +207,32 @@ static ShapeTable make_shape(int type) {
     s.w = {TET_W};
     s.wGNs = s.GNs;  // TetElement.getWarpingPoint == integration point 0
     s.ww = TET_W;
+  } else if (type == ELEM_WEDGE) {
+    s.nen = 6; s.nip = 6;
+    // myIntegrationCoords (WedgeElement.java:34-49)
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0, q = 1 / std::sqrt(3.0);
+    const double ip[6][3] = {{a, a, -q}, {b, a, -q}, {a, b, -q}, {a, a, q}, {b, a, q}, {a, b, q}};
+    s.GNs.resize(6 * 6 * 3);
+    s.w.assign(6, 1.0 / 6.0);
+    for (int k = 0; k < 6; k++)
+      for (int i = 0; i < 6; i++) wedge_dNds(&s.GNs[(k * 6 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // getWarpingPoint (WedgeElement.java:128-133): (1/3, 1/3, 0), weight 1
+    s.wGNs.resize(18);
+    for (int i = 0; i < 6; i++) wedge_dNds(&s.wGNs[i * 3], i, 1 / 3.0, 1 / 3.0, 0);
+    s.ww = 1;
+  } else if (type == ELEM_PYRAMID) {
+    s.nen = 5; s.nip = 5;
+    // myIntegrationCoords (PyramidElement.java:69-83)
+    const double a = (8 / 5.0) * std::sqrt(2 / 15.0), b = -2.0 / 3.0, c = 2.0 / 5.0;
+    const double ip[5][3] = {{-a, -a, b}, {a, -a, b}, {a, a, b}, {-a, a, b}, {0, 0, c}};
+    s.GNs.resize(5 * 5 * 3);
+    s.w = {81 / 100.0, 81 / 100.0, 81 / 100.0, 81 / 100.0, 125 / 27.0};
+    for (int k = 0; k < 5; k++)
+      for (int i = 0; i < 5; i++) pyramid_dNds(&s.GNs[(k * 5 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // getWarpingPoint (PyramidElement.java:38-44): (0, 0, -1/2), weight 128/27
+    s.wGNs.resize(15);
+    for (int i = 0; i < 5; i++) pyramid_dNds(&s.wGNs[i * 3], i, 0, 0, -0.5);
+    s.ww = 128 / 27.0;
   } else {
     s.nen = 8; s.nip = 8;
     // INTEGRATION_COORDS_GAUSS_8 (HexElement.java:159-170)
@@ -1135,7 +1181,8 @@ int orc_num_threads(int n) {
 
 void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
   *nnodes = (nx + 1) * (ny + 1) * (nz + 1);
-  *nelems = (type == ELEM_TET ? 5 : 1) * nx * ny * nz;
+  const int per_cell[4] = {5, 1, 2, 3};
+  *nelems = per_cell[type] * nx * ny * nz;
 }
 
 // FemFactory.createGridNodes (FemFactory.java:53-78), createTetGrid (:86-126)
@@ -1167,6 +1214,32 @@ void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, 
         if (type == ELEM_HEX) {
           for (int a = 0; a < 8; a++) conn[8 * e + a] = h[a];
           e++;
+        } else if (type == ELEM_WEDGE) {
+          // createWedgeGrid (FemFactory.java:266-310)
+          const int w[2][6] = {{h[0], h[1], h[4], h[3], h[2], h[7]}, {h[1], h[5], h[4], h[2], h[6], h[7]}};
+          for (int q = 0; q < 2; q++, e++)
+            for (int a = 0; a < 6; a++) conn[6 * e + a] = w[q][a];
+        } else if (type == ELEM_PYRAMID) {
+          // createPyramidGrid (FemFactory.java:137-195): apexNodeTable
+          // (:128-129) indexed by the parity code, then
+          // PyramidElement.createCubeTesselation (PyramidElement.java:216-270)
+          static const int apexTable[8] = {2, 3, 1, 0, 6, 7, 5, 4};
+          static const int tess[8][3][5] = {
+              {{6, 2, 3, 7, 0}, {6, 5, 1, 2, 0}, {6, 7, 4, 5, 0}},
+              {{7, 6, 2, 3, 1}, {7, 3, 0, 4, 1}, {7, 4, 5, 6, 1}},
+              {{4, 5, 6, 7, 2}, {4, 0, 1, 5, 2}, {4, 7, 3, 0, 2}},
+              {{5, 1, 2, 6, 3}, {5, 4, 0, 1, 3}, {5, 6, 7, 4, 3}},
+              {{2, 3, 7, 6, 4}, {2, 1, 0, 3, 4}, {2, 6, 5, 1, 4}},
+              {{3, 2, 1, 0, 5}, {3, 0, 4, 7, 5}, {3, 7, 6, 2, 5}},
+              {{0, 3, 2, 1, 6}, {0, 1, 5, 4, 6}, {0, 4, 7, 3, 6}},
+              {{1, 0, 3, 2, 7}, {1, 2, 6, 5, 7}, {1, 5, 4, 0, 7}}};
+          int code = 0;
+          if (i % 2 == 0) code |= 1;
+          if (j % 2 == 0) code |= 2;
+          if (k % 2 == 0) code |= 4;
+          const int apex = apexTable[code];
+          for (int q = 0; q < 3; q++, e++)
+            for (int a = 0; a < 5; a++) conn[5 * e + a] = h[tess[apex][q][a]];
         } else {
           bool allOnX = ((i + j + k) % 2) != 0;
           const int(*t)[4] = allOnX ? tetsA : tetsB;
@@ -1241,8 +1314,9 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
       if (type == ELEM_TET) {
         for (int i = 0; i < 4; i++) m->nodeRestVol[nodes[i]] += m->restVol[e] / 4;
       } else {
-        for (int i = 0; i < 8; i++)
-          m->nodeRestVol[nodes[i]] += m->sh.w[i] * m->detJ0[(size_t)e * 8 + i];
+        // integration points map to nodes (FemModel3d.java:2608-2614)
+        for (int i = 0; i < m->nen; i++)
+          m->nodeRestVol[nodes[i]] += m->sh.w[i] * m->detJ0[(size_t)e * m->nen + i];
       }
     }
   }

@@ -20,7 +20,8 @@ _lib = None
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
 REF_SOURCE_ROOT = "/root/reference"
 
-ELEM_TET, ELEM_HEX = 0, 1
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID = 0, 1, 2, 3
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 
@@ -116,7 +117,7 @@ def grid(elem_type: int, widths, cells, jitter: float = 0.0, seed: int = 0):
     nx, ny, nz = (int(c) for c in cells)
     nn, ne = ctypes.c_int(), ctypes.c_int()
     L.orc_grid_dims(elem_type, nx, ny, nz, ctypes.byref(nn), ctypes.byref(ne))
-    nen = 4 if elem_type == ELEM_TET else 8
+    nen = ELEM_NODES[elem_type]
     xyz = np.zeros(3 * nn.value)
     conn = np.zeros(nen * ne.value, dtype=np.int32)
     L.orc_create_grid(elem_type, float(widths[0]), float(widths[1]), float(widths[2]), nx, ny, nz, xyz, conn)
@@ -136,7 +137,7 @@ class OracleModel:
         self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1)
         self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
         self.N = self.rest.size // 3
-        nen = 4 if elem_type == ELEM_TET else 8
+        nen = ELEM_NODES[elem_type]
         self.E = self.conn.size // nen
         fx = np.ascontiguousarray(fixed, dtype=np.int32)
         mp = np.zeros(8)
@@ -215,7 +216,7 @@ class OracleModel:
         """(GNx (nen,3), dv, sig (6), D (6,6)) of integration point k of
         element e at positions x (non-linear materials)."""
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
-        nen = 4 if self.elem_type == ELEM_TET else 8
+        nen = ELEM_NODES[self.elem_type]
         g = np.zeros(3 * nen)
         dv = ctypes.c_double()
         sig = np.zeros(6)

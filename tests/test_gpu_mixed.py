@@ -25,6 +25,12 @@ def _cases():
         "neohookean_tet": W.small_tet_beam(NeoHookeanMaterial(5e4, 0.33)),
         "neohookean_hex": W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45)),
         "mooneyrivlin_tet_nodal": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
+        "neohookean_wedge": W.small_wedge_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "neohookean_pyramid": W.small_pyramid_beam(NeoHookeanMaterial(5e4, 0.45)),
+        # AUTO: ELEMENT on the wedge beam (32 elements <= 36 active nodes),
+        # NODAL on the pyramid beam (48 > 36)
+        "mooneyrivlin_wedge_auto": W.small_wedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_pyramid_auto": W.small_pyramid_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
     }
 
 

@@ -42,6 +42,18 @@ def _cases():
         "mooneyrivlin_hex_element": W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
         "mooneyrivlin_hex_element_log": W.small_hex_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
         "mooneyrivlin_tet_element": W.small_tet_beam(MooneyRivlinMaterial(1000.0, 500.0, 0, 0, 0, 1e5)),
+        # wedges (6 points) and pyramids (5 points, unequal weights)
+        "linear_corotated_wedge": W.small_wedge_beam(LinearMaterial(2e4, 0.3, True)),
+        "linear_corotated_pyramid": W.small_pyramid_beam(LinearMaterial(2e4, 0.3, True)),
+        "neohookean_wedge": W.small_wedge_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "neohookean_pyramid": W.small_pyramid_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "stvk_wedge": W.small_wedge_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "stvk_pyramid": W.small_pyramid_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "mooneyrivlin_wedge_nodal": W.small_wedge_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
+        "mooneyrivlin_pyramid_nodal": W.small_pyramid_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
+        "mooneyrivlin_wedge_element": W.small_wedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_pyramid_element_log": W.small_pyramid_beam(
+            MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
     }
 
 
@@ -58,6 +70,10 @@ def cases(b200):
     # more hexes than active nodes is needed for AUTO -> NODAL; request it
     cs["mooneyrivlin_hex_nodal"].incomp = L.INCOMP_NODAL
     cs["mooneyrivlin_tet_element"].incomp = L.INCOMP_ELEMENT
+    for k in ("mooneyrivlin_wedge_nodal", "mooneyrivlin_pyramid_nodal"):
+        cs[k].incomp = L.INCOMP_NODAL
+    for k in ("mooneyrivlin_wedge_element", "mooneyrivlin_pyramid_element_log"):
+        cs[k].incomp = L.INCOMP_ELEMENT
     return cs
 
 
@@ -146,7 +162,11 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
                                   "linear_plain_tet", "linear_corotated_hex", "mooneyrivlin_hex_full",
                                   "mooneyrivlin_tet_nodal", "mooneyrivlin_hex_nodal",
                                   "mooneyrivlin_tet_nodal_log", "mooneyrivlin_hex_element",
-                                  "mooneyrivlin_hex_element_log", "mooneyrivlin_tet_element"])
+                                  "mooneyrivlin_hex_element_log", "mooneyrivlin_tet_element",
+                                  "linear_corotated_wedge", "linear_corotated_pyramid", "neohookean_wedge",
+                                  "neohookean_pyramid", "stvk_wedge", "stvk_pyramid", "mooneyrivlin_wedge_nodal",
+                                  "mooneyrivlin_pyramid_nodal", "mooneyrivlin_wedge_element",
+                                  "mooneyrivlin_pyramid_element_log"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)

@@ -148,7 +148,11 @@ def test_polar_rotation(oracle):
     (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1, 0), (3, [5e4, 0.3], 0, 0), (3, [5e4, 0.3], 1, 0),
     # ELEMENT soft incompressibility (QUADRATIC and LOGARITHMIC bulk potentials)
     (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 0, 3), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1, 3),
-    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 1, 3)])
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 1, 3),
+    # wedges and pyramids (WedgeElement, PyramidElement)
+    (1, [5e4, 0.45], 2, 0), (1, [5e4, 0.45], 3, 0), (3, [5e4, 0.3], 2, 0), (3, [5e4, 0.3], 3, 0),
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 3),
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 3, 3)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
@@ -274,3 +278,29 @@ def test_constrained_step_holds_nodes_on_their_planes(oracle):
         assert np.abs((nrm * v[tip]).sum(axis=1)).max() <= 1e-10 * np.abs(v).max()
         assert np.abs((nrm * x[tip]).sum(axis=1) - off).max() <= 1e-14
     assert np.abs(x - xyz).max() > 1e-6
+
+
+@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3)])
+def test_grid_volumes_and_masses(oracle, etype, per_cell):
+    # createTetGrid / createHexGrid / createWedgeGrid / createPyramidGrid:
+    # every element positively oriented, rest volumes (sum of detJ0 w over
+    # the integration points; the pyramid's five-point rule integrates the
+    # collapsed-cube Jacobian exactly) add up to the box, and lumped masses
+    # to density x volume
+    widths, cells = (1.0, 0.5, 0.3), (3, 2, 2)
+    xyz, conn = oracle.grid(etype, widths, cells)
+    assert conn.shape[0] == per_cell * 12
+    m = oracle.OracleModel(etype, xyz, conn, np.zeros(len(xyz), np.int32), 1, [5e4, 0.3], 1000.0)
+    rv = m.rest_volumes()
+    assert rv.min() > 0
+    assert abs(rv.sum() - 0.15) <= 1e-14
+    assert abs(m.masses().sum() - 150.0) <= 1e-11
+
+
+@pytest.mark.parametrize("etype", [2, 3])
+def test_library_grid_matches_oracle(oracle, etype):
+    # the library's host-side mesh factory (no GPU needed) against the oracle's
+    from artisynth_core_b200 import femmodel as FM
+    xo, co = oracle.grid(etype, (1.0, 0.5, 0.3), (3, 2, 4))
+    xl, cl = FM.create_grid(etype, 1.0, 0.5, 0.3, 3, 2, 4)
+    assert np.array_equal(xo, xl) and np.array_equal(co, cl)
