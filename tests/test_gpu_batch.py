@@ -82,6 +82,29 @@ def test_pack_of_mixed_materials(b200, oracle):
         assert rel_err(xg, x) <= 1e-8
 
 
+@pytest.mark.parametrize("beam", ["wedge", "pyramid"])
+def test_pack_of_wedges_or_pyramids(b200, oracle, beam):
+    """A pack of one of the multi-point element types: uneven beams with
+    different materials (element groups), every model against its oracle run."""
+    from artisynth_core_b200.femmodel import (MooneyRivlinMaterial, NeoHookeanMaterial, LinearMaterial,
+                                              StVenantKirchoffMaterial)
+    mk = W.small_wedge_beam if beam == "wedge" else W.small_pyramid_beam
+    wls = [mk(NeoHookeanMaterial(3e4, 0.4)), mk(LinearMaterial(2e4, 0.3, True), cells=(6, 2, 2)),
+           mk(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370), cells=(3, 3, 2)),
+           mk(StVenantKirchoffMaterial(4e4, 0.3), cells=(5, 2, 3))]
+    for w in wls:
+        w.build_mesh()
+    pack = FemPack([w.model() for w in wls], precision=L.PREC_FP64)
+    pack.backwardEuler(wls[0].h, 3, tol=1e-12)
+    for w, (xg, _) in zip(wls, pack.getStates()):
+        om = oracle_model(oracle, w)
+        x = w.rest.copy()
+        v = np.zeros_like(x)
+        for _ in range(3):
+            om.be_step(w.h, x, v, alpha=w.mass_damping, gravity=w.gravity, solver=1)
+        assert rel_err(xg, x) <= 1e-8, (beam, w.material, rel_err(xg, x))
+
+
 @pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
 @pytest.mark.parametrize("variant", [L.PCG_AUTO, L.PCG_CLASSIC])
 def test_strided_split_equals_alone(beams, precision, variant):

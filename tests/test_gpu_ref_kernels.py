@@ -10,15 +10,15 @@ and adds it into the CRS values (FP64 atomics).
 
 That kernel, compiled from the reference source into oracle/_ref/ (`make -C
 oracle ref`), is fed the oracle's integration-point data for every (element,
-point, node pair) of NeoHookean tet and hex and StVenantKirchhoff hex beams at
-deformed positions.  Its
+point, node pair) of NeoHookean tet, hex, wedge and pyramid and
+StVenantKirchhoff hex and pyramid beams at deformed positions.  Its
 CRS values must equal
 * the engine's full-partition CRS export (b200fem_update_stress_stiffness)
   within the parity bar, 1e-10 of the largest entry, and
 * the oracle's own assembly within 1e-12 (same arithmetic, summation order
   differs through the atomics).
-For a MooneyRivlin hex beam whose AUTO soft incompressibility resolves to
-ELEMENT, the descriptors carry the element pressure and the reference's
+For MooneyRivlin hex and wedge beams whose AUTO soft incompressibility
+resolves to ELEMENT, the descriptors carry the element pressure and the reference's
 addDilationalStiffness3ElementKernel (:658-723) adds Rinv c_i c_j^T from the
 element constraint vectors.
 This pins the element-tangent assembly (FemUtilities.addMaterialStiffness /
@@ -175,7 +175,9 @@ def _add_reference_dilational(R, arr, crs_dev, nnz):
     torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex", "mooneyrivlin_hex_element"])
+@pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex", "mooneyrivlin_hex_element",
+                                  "neohookean_wedge", "neohookean_pyramid", "stvk_pyramid",
+                                  "mooneyrivlin_wedge_element"])
 def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     R = _ref_lib()
     if case == "neohookean_tet":
@@ -184,6 +186,15 @@ def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
         wl = W.small_hex_beam(NeoHookeanMaterial(5e4, 0.45))
     elif case == "stvk_hex":
         wl = W.small_hex_beam(StVenantKirchoffMaterial(5e4, 0.3))
+    elif case == "neohookean_wedge":
+        wl = W.small_wedge_beam(NeoHookeanMaterial(5e4, 0.45))
+    elif case == "neohookean_pyramid":
+        wl = W.small_pyramid_beam(NeoHookeanMaterial(5e4, 0.45))
+    elif case == "stvk_pyramid":
+        wl = W.small_pyramid_beam(StVenantKirchoffMaterial(5e4, 0.3))
+    elif case == "mooneyrivlin_wedge_element":
+        # AUTO resolves to ELEMENT: 32 wedges <= 36 active nodes
+        wl = W.small_wedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370))
     else:
         wl = W.small_hex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370))
     wl.build_mesh()
@@ -241,17 +252,15 @@ def _linear_element_arrays(om_geom, wl, E, nu):
             params, grads.reshape(-1), dvs.reshape(-1))
 
 
-@pytest.mark.parametrize("case", ["tet", "hex"])
+@pytest.mark.parametrize("case", ["tet", "hex", "wedge", "pyramid"])
 def test_reference_kernel_assembles_linear_rest_stiffness(b200, oracle, case):
     import torch
     R = _ref_lib()
     E, nu = 5e4, 0.33
-    if case == "tet":
-        wl = W.small_tet_beam(LinearMaterial(E, nu, False))
-        geom = W.small_tet_beam(NeoHookeanMaterial(E, nu))
-    else:
-        wl = W.small_hex_beam(LinearMaterial(E, nu, False))
-        geom = W.small_hex_beam(NeoHookeanMaterial(E, nu))
+    beam = {"tet": W.small_tet_beam, "hex": W.small_hex_beam, "wedge": W.small_wedge_beam,
+            "pyramid": W.small_pyramid_beam}[case]
+    wl = beam(LinearMaterial(E, nu, False))
+    geom = beam(NeoHookeanMaterial(E, nu))
     wl.build_mesh()
     geom.build_mesh()
     assert np.array_equal(wl.rest, geom.rest) and np.array_equal(wl.conn, geom.conn)
