@@ -26,8 +26,8 @@ ERR_BUDGET = -6
 ERR_TIMEOUT = -7
 ERR_NO_CONVERGE = -13
 
-ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID = 0, 1, 2, 3
-ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5}
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET = 0, 1, 2, 3, 4
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
@@ -117,6 +117,8 @@ def lib():
         "b200fem_grid_dims": ([ctypes.c_int] * 4 + [_ip, _ip], ctypes.c_int),
         "b200fem_create_grid": ([ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [_dp, _ip], ctypes.c_int),
         "b200fem_jitter_grid": ([ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_ulonglong, _dp], ctypes.c_int),
+        "b200fem_quadratic_tet_mesh": ([ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int), _dp, _ip],
+                                       ctypes.c_int),
         "b200fem_set_mesh": ([H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip], ctypes.c_int),
         "b200fem_set_material": ([H, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "b200fem_build": ([H], ctypes.c_int),

@@ -764,6 +764,21 @@ int b200fem_create_grid(int elem_type, double wx, double wy, double wz, int nx, 
   return B200FEM_OK;
 }
 
+int b200fem_quadratic_tet_mesh(int n_nodes, const double* xyz, int n_tets, const int* conn, int* n_nodes_out,
+                               double* xyz_out, int* conn_out) {
+  if (n_nodes <= 0 || n_tets <= 0 || !xyz || !conn || !n_nodes_out)
+    return fail(nullptr, B200FEM_ERR_INVALID_ARG, "invalid mesh arguments");
+  for (size_t q = 0; q < 4 * (size_t)n_tets; q++)
+    if (conn[q] < 0 || conn[q] >= n_nodes) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "connectivity index out of range");
+  std::vector<double> qx;
+  std::vector<int> qc;
+  quadratic_tets(n_nodes, xyz, n_tets, conn, qx, qc);
+  *n_nodes_out = (int)(qx.size() / 3);
+  if (xyz_out) std::copy(qx.begin(), qx.end(), xyz_out);
+  if (conn_out) std::copy(qc.begin(), qc.end(), conn_out);
+  return B200FEM_OK;
+}
+
 int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
                         unsigned long long seed, double* xyz) {
   if (nx < 1 || ny < 1 || nz < 1 || !xyz) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "invalid grid arguments");

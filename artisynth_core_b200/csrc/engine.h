@@ -17,7 +17,7 @@
 
 namespace b200fem {
 
-constexpr int kMaxNen = 8;
+constexpr int kMaxNen = 10;
 constexpr int kMaxIp = 8;
 constexpr int kMatParams = 8;
 
@@ -25,9 +25,15 @@ constexpr int kMatParams = 8;
 // wedges and pyramids, like hexes, have one integration point per node
 __host__ __device__ constexpr int elem_nen(int type) {
   return type == B200FEM_ELEM_TET ? 4 : type == B200FEM_ELEM_HEX ? 8 : type == B200FEM_ELEM_WEDGE ? 6
-         : type == B200FEM_ELEM_PYRAMID ? 5 : 0;
+         : type == B200FEM_ELEM_PYRAMID ? 5 : type == B200FEM_ELEM_QUADTET ? 10 : 0;
 }
-__host__ __device__ constexpr int elem_nip(int type) { return type == B200FEM_ELEM_TET ? 1 : elem_nen(type); }
+__host__ __device__ constexpr int elem_nip(int type) {
+  return type == B200FEM_ELEM_TET ? 1 : type == B200FEM_ELEM_QUADTET ? 4 : elem_nen(type);
+}
+// integration point k lies at node k (FemElement3d.integrationPointsMapToNodes)
+__host__ __device__ constexpr bool elem_ip_at_nodes(int type) {
+  return type == B200FEM_ELEM_HEX || type == B200FEM_ELEM_WEDGE || type == B200FEM_ELEM_PYRAMID;
+}
 
 // Model as given by the caller (host, FP64).
 struct ModelDesc {
@@ -250,6 +256,9 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err);
 int build_pack(Engine& eng);
 void free_pack(Engine& eng);
 int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne);
+// linear tets -> quadratic tets with shared edge nodes (createQuadraticModel)
+void quadratic_tets(int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
+                    std::vector<int>& out_conn);
 // dN/ds of the element's nodes at integration point k (k = -1: the warping
 // point) and the point's weight
 void shape_grads(int type, int k, double* g /* nen * 3 */, double* w);

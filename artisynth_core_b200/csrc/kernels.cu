@@ -48,6 +48,9 @@ __constant__ int c_pair_a[36], c_pair_b[36];
 __constant__ double c_wed_gns[6 * 6 * 3], c_wed_wgns[6 * 3];
 __constant__ double c_pyr_gns[5 * 5 * 3], c_pyr_wgns[5 * 3];
 __constant__ float c_wed_gns_f[6 * 6 * 3], c_pyr_gns_f[5 * 5 * 3];
+// quadratic tets: 4 points x 10 nodes, warping point
+__constant__ double c_qtet_gns[4 * 10 * 3], c_qtet_wgns[10 * 3];
+__constant__ float c_qtet_gns_f[4 * 10 * 3];
 
 static bool g_const_ready[64] = {false};
 
@@ -80,9 +83,17 @@ static cudaError_t ensure_constants(int device) {
   shape_grads(B200FEM_ELEM_WEDGE, -1, wedw, &wt);
   for (int k = 0; k < 5; k++) shape_grads(B200FEM_ELEM_PYRAMID, k, &pyr[k * 15], &wt);
   shape_grads(B200FEM_ELEM_PYRAMID, -1, pyrw, &wt);
+  double qt[120], qtw[30];
+  float qtf[120];
+  for (int k = 0; k < 4; k++) shape_grads(B200FEM_ELEM_QUADTET, k, &qt[k * 30], &wt);
+  shape_grads(B200FEM_ELEM_QUADTET, -1, qtw, &wt);
+  for (int i = 0; i < 120; i++) qtf[i] = (float)qt[i];
   for (int i = 0; i < 108; i++) wedf[i] = (float)wed[i];
   for (int i = 0; i < 75; i++) pyrf[i] = (float)pyr[i];
   cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_qtet_gns, qt, sizeof(qt))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qtet_wgns, qtw, sizeof(qtw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qtet_gns_f, qtf, sizeof(qtf))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_wed_gns, wed, sizeof(wed))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_wed_wgns, wedw, sizeof(wedw))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_pyr_gns, pyr, sizeof(pyr))) != cudaSuccess) return e;
@@ -136,6 +147,9 @@ __device__ __forceinline__ T gns(int k, int n, int c) {
   } else if constexpr (TYPE == B200FEM_ELEM_WEDGE) {
     if constexpr (sizeof(T) == 8) return c_wed_gns[(k * 6 + n) * 3 + c];
     else return c_wed_gns_f[(k * 6 + n) * 3 + c];
+  } else if constexpr (TYPE == B200FEM_ELEM_QUADTET) {
+    if constexpr (sizeof(T) == 8) return c_qtet_gns[(k * 10 + n) * 3 + c];
+    else return c_qtet_gns_f[(k * 10 + n) * 3 + c];
   } else {
     if constexpr (sizeof(T) == 8) return c_pyr_gns[(k * 5 + n) * 3 + c];
     else return c_pyr_gns_f[(k * 5 + n) * 3 + c];
@@ -144,21 +158,23 @@ __device__ __forceinline__ T gns(int k, int n, int c) {
 
 // dN_n/ds at the warping point (StiffnessWarper3d: TetElement integration
 // point 0, HexElement centre, WedgeElement (1/3, 1/3, 0), PyramidElement
-// (0, 0, -1/2))
+// (0, 0, -1/2), QuadtetElement the linear tet's gradients on its corners)
 template <int TYPE>
 __device__ __forceinline__ double wgns(int n, int c) {
   if constexpr (TYPE == B200FEM_ELEM_TET) return c_tet_gns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_HEX) return c_hex_wgns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_WEDGE) return c_wed_wgns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return c_qtet_wgns[3 * n + c];
   else return c_pyr_wgns[3 * n + c];
 }
 
 // integration weight of point k (TetElement 1/6; HexElement Gauss 1;
 // WedgeElement 1/6; PyramidElement 81/100 for the four base points, 125/27
-// for the fifth)
+// for the fifth; QuadtetElement 0.25/6)
 template <typename T, int TYPE>
 __device__ __forceinline__ T ip_weight(int k) {
   if constexpr (TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_WEDGE) return T(1.0 / 6.0);
+  else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return T(0.25 / 6.0);
   else if constexpr (TYPE == B200FEM_ELEM_HEX) return T(1);
   else return k < 4 ? T(81 / 100.0) : T(125 / 27.0);
 }
@@ -174,6 +190,7 @@ static cudaError_t by_elem_type(int type, F&& f) {
     case B200FEM_ELEM_HEX: return f(std::integral_constant<int, B200FEM_ELEM_HEX>{});
     case B200FEM_ELEM_WEDGE: return f(std::integral_constant<int, B200FEM_ELEM_WEDGE>{});
     case B200FEM_ELEM_PYRAMID: return f(std::integral_constant<int, B200FEM_ELEM_PYRAMID>{});
+    case B200FEM_ELEM_QUADTET: return f(std::integral_constant<int, B200FEM_ELEM_QUADTET>{});
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1440,10 +1457,16 @@ cudaError_t launch_nodal_pressure(Engine& eng) {
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
   return by_elem_type(eng.elem_type, [&](auto tag) {
-    nodal_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
-        d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
-        d.node_kp);
-    return cudaGetLastError();
+    constexpr int TY = decltype(tag)::value;
+    // NODAL: tets, or elements whose integration points sit at their nodes
+    if constexpr (TY != B200FEM_ELEM_TET && !elem_ip_at_nodes(TY)) {
+      return cudaErrorNotSupported;
+    } else {
+      nodal_pressure_kernel<TY><<<blocks, threads, 0, eng.stream>>>(
+          d.n_nodes, d.inc_ptr, d.inc_idx, d.conn, d.x, d.sidx, d.node_rest_vol, d.mat_node, d.node_vol, d.node_p,
+          d.node_kp);
+      return cudaGetLastError();
+    }
   });
 }
 
@@ -1452,9 +1475,14 @@ cudaError_t launch_divblk(Engine& eng) {
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
   return by_elem_type(eng.elem_type, [&](auto tag) {
-    divblk_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
-        d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
-    return cudaGetLastError();
+    constexpr int TY = decltype(tag)::value;
+    if constexpr (TY != B200FEM_ELEM_TET && !elem_ip_at_nodes(TY)) {
+      return cudaErrorNotSupported;
+    } else {
+      divblk_kernel<TY><<<blocks, threads, 0, eng.stream>>>(
+          d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
+      return cudaGetLastError();
+    }
   });
 }
 

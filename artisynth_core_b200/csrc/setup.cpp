@@ -5,7 +5,9 @@
 // version changes, MechSystemSolver.updateSolveMatrixStructure,
 // MechSystemSolver.java:2484-2493).
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
 #include <cstring>
 #include <numeric>
 
@@ -83,10 +85,45 @@ void pyramid_grad(double* g, int i, double s0, double s1, double s2) {
   g[2] = -0.125 * (1 + a * s0) * (1 + b * s1);
 }
 
+// QuadtetElement.getdNds (QuadtetElement.java:301-323) at (s1, s2, s3),
+// s0 = 1 - s1 - s2 - s3: corner n has N = s_n (2 s_n - 1), the edge node
+// between corners a and b N = 4 s_a s_b
+const int kQtetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+void quadtet_grad(double* g, int i, const double* s /* s0..s3 */) {
+  // ds_n/d(s1, s2, s3): s0 -> (-1, -1, -1), s_j -> unit j
+  auto ds = [](int n, int c) { return n == 0 ? -1.0 : (n == c + 1 ? 1.0 : 0.0); };
+  for (int c = 0; c < 3; c++) {
+    if (i < 4) {
+      g[c] = (4 * s[i] - 1) * ds(i, c);
+    } else {
+      const int a = kQtetEdge[i - 4][0], b = kQtetEdge[i - 4][1];
+      g[c] = 4 * (ds(a, c) * s[b] + s[a] * ds(b, c));
+    }
+  }
+}
+
 }  // namespace
 
 // Shape gradients for integration point k (or the warping point, k = -1).
 void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
+  if (type == B200FEM_ELEM_QUADTET) {
+    if (k < 0) {
+      // warping point (QuadtetElement.getWarpingPoint, :45-85): the linear
+      // tet's gradients on the corners, zero on the edge nodes, weight 1
+      std::memset(g, 0, 30 * sizeof(double));
+      std::memcpy(g, kTetGNs, sizeof(kTetGNs));
+      *w = 1;
+      return;
+    }
+    // myIntegrationCoords (QuadtetElement.java:22-23, 255-262): the
+    // reference's rounded alpha, beta; weight 0.25/6
+    const double alpha = 0.58541020, beta = 0.13819660;
+    const double c[3] = {k == 1 ? alpha : beta, k == 2 ? alpha : beta, k == 3 ? alpha : beta};
+    const double sv[4] = {1 - c[0] - c[1] - c[2], c[0], c[1], c[2]};
+    for (int i = 0; i < 10; i++) quadtet_grad(g + 3 * i, i, sv);
+    *w = 0.25 / 6.0;
+    return;
+  }
   if (type == B200FEM_ELEM_WEDGE) {
     // integration points (WedgeElement.java:36-49): (1/6, 1/6), (2/3, 1/6),
     // (1/6, 2/3) on the layers r = -/+ 1/sqrt(3), weight 1/6; warping point
@@ -186,9 +223,47 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
   if (nx < 1 || ny < 1 || nz < 1) return B200FEM_ERR_INVALID_ARG;
   if (elem_nen(type) == 0) return B200FEM_ERR_INVALID_ARG;
   *nn = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[4] = {5, 1, 2, 3};  // tet, hex, wedge, pyramid
+  const int per_cell[5] = {5, 1, 2, 3, 5};  // tet, hex, wedge, pyramid, quadtet
   *ne = per_cell[type] * nx * ny * nz;
+  if (type == B200FEM_ELEM_QUADTET) {
+    // the tet grid plus its edge nodes
+    std::vector<double> xyz(3 * (size_t)*nn);
+    std::vector<int> conn(4 * (size_t)*ne);
+    create_grid(B200FEM_ELEM_TET, 1, 1, 1, nx, ny, nz, xyz.data(), conn.data());
+    std::vector<double> qx;
+    std::vector<int> qc;
+    quadratic_tets(*nn, xyz.data(), *ne, conn.data(), qx, qc);
+    *nn = (int)(qx.size() / 3);
+  }
   return B200FEM_OK;
+}
+
+// FemFactory.createQuadraticModel for tets (FemFactory.java:5641-5710,
+// QuadtetElement.getQuadraticNodes :130-175): the linear nodes keep their
+// indices; each element in order adds the midpoints (a + b) * 0.5 of its edges
+// 01, 12, 02, 03, 13, 23 unless a node already sits at exactly that position
+void quadratic_tets(int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
+                    std::vector<int>& out_conn) {
+  std::map<std::array<double, 3>, int> at;
+  out_xyz.assign(xyz, xyz + 3 * (size_t)nn);
+  for (int n = 0; n < nn; n++) at.emplace(std::array<double, 3>{xyz[3 * n], xyz[3 * n + 1], xyz[3 * n + 2]}, n);
+  out_conn.assign(10 * (size_t)ne, 0);
+  for (int e = 0; e < ne; e++) {
+    const int* c = conn + 4 * (size_t)e;
+    int* q = &out_conn[10 * (size_t)e];
+    for (int a = 0; a < 4; a++) q[a] = c[a];
+    for (int j = 0; j < 6; j++) {
+      const double* pa = xyz + 3 * (size_t)c[kQtetEdge[j][0]];
+      const double* pb = xyz + 3 * (size_t)c[kQtetEdge[j][1]];
+      const std::array<double, 3> p{(pa[0] + pb[0]) * 0.5, (pa[1] + pb[1]) * 0.5, (pa[2] + pb[2]) * 0.5};
+      auto it = at.find(p);
+      if (it == at.end()) {
+        it = at.emplace(p, (int)(out_xyz.size() / 3)).first;
+        out_xyz.insert(out_xyz.end(), p.begin(), p.end());
+      }
+      q[4 + j] = it->second;
+    }
+  }
 }
 
 // FemFactory.createGridNodes (FemFactory.java:53-78); createTetGrid
@@ -203,6 +278,19 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
 // (PyramidElement.java:216-270).
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn) {
+  if (type == B200FEM_ELEM_QUADTET) {
+    // createQuadtetGrid (FemFactory.java:316-325): the tet grid made quadratic
+    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = 5 * nx * ny * nz;
+    std::vector<double> lx(3 * (size_t)nl);
+    std::vector<int> lc(4 * (size_t)ne);
+    create_grid(B200FEM_ELEM_TET, wx, wy, wz, nx, ny, nz, lx.data(), lc.data());
+    std::vector<double> qx;
+    std::vector<int> qc;
+    quadratic_tets(nl, lx.data(), ne, lc.data(), qx, qc);
+    std::copy(qx.begin(), qx.end(), xyz);
+    std::copy(qc.begin(), qc.end(), conn);
+    return;
+  }
   const double sx = 1.0 / nx, sy = 1.0 / ny, sz = 1.0 / nz;
   size_t n = 0;
   for (int k = 0; k <= nz; k++)
@@ -298,6 +386,11 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   // else ELEMENT (getAllowedSoftIncompMethod, FemModel3d.java:462-481)
   int method = m.incomp_request;
   if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
+  // NODAL needs tets or elements whose points map to nodes
+  // (softNodalIncompressAllowed, FemModel3d.java:400-405, 467-471)
+  else if (m.elem_type == B200FEM_ELEM_QUADTET &&
+           (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
+    method = B200FEM_INCOMP_ELEMENT;
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
   h.incomp = method;

@@ -106,6 +106,20 @@ def create_grid(elem_type, wx, wy, wz, nx, ny, nz):
     return xyz.reshape(-1, 3), conn.reshape(-1, nen)
 
 
+def quadratic_tet_mesh(xyz, conn):
+    """FemFactory.createQuadraticModel of a linear tet mesh (host only)."""
+    x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+    c = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
+    n = ctypes.c_int()
+    lib = L.lib()
+    L.check(lib.b200fem_quadratic_tet_mesh(x.size // 3, L.dptr(x), c.size // 4, L.iptr(c), ctypes.byref(n), None, None))
+    ox = np.zeros(3 * n.value)
+    oc = np.zeros(10 * (c.size // 4), dtype=np.int32)
+    L.check(lib.b200fem_quadratic_tet_mesh(x.size // 3, L.dptr(x), c.size // 4, L.iptr(c), ctypes.byref(n),
+                                           L.dptr(ox), L.iptr(oc)))
+    return ox.reshape(-1, 3), oc.reshape(-1, 10)
+
+
 def jitter_grid(xyz, nx, ny, nz, wx, wy, wz, frac, seed):
     flat = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1).copy()
     L.check(L.lib().b200fem_jitter_grid(nx, ny, nz, wx, wy, wz, float(frac), ctypes.c_ulonglong(seed),
@@ -127,6 +141,12 @@ class FemFactory:
     def createHexGrid(model, wx, wy, wz, nx, ny, nz):
         m = model if model is not None else FemModel3d()
         m._set_grid(L.ELEM_HEX, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
+    def createQuadtetGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_QUADTET, wx, wy, wz, nx, ny, nz)
         return m
 
     @staticmethod

@@ -54,6 +54,9 @@ extern "C" {
 #define B200FEM_ELEM_HEX 1 /* HexElement, 8 nodes, 8 Gauss points */
 #define B200FEM_ELEM_WEDGE 2   /* WedgeElement, 6 nodes, 6 integration points */
 #define B200FEM_ELEM_PYRAMID 3 /* PyramidElement, 5 nodes, 5 integration points */
+#define B200FEM_ELEM_QUADTET 4 /* QuadtetElement, 10 nodes (corners 0-3, then the midpoints
+                                  of edges 01, 12, 02, 03, 13, 23), 4 integration points;
+                                  soft incompressibility resolves to ELEMENT */
 
 /* materials (parameter layout of b200fem_set_material) */
 #define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */
@@ -132,6 +135,12 @@ const char* b200fem_last_error(b200fem_handle h);
 int b200fem_grid_dims(int elem_type, int nx, int ny, int nz, int* n_nodes, int* n_elems);
 int b200fem_create_grid(int elem_type, double wx, double wy, double wz, int nx, int ny, int nz,
                         double* xyz, int* conn);
+/* FemFactory.createQuadraticModel for a tet mesh: the n_nodes linear nodes
+   keep their indices, edge midpoints follow in element order (shared edges
+   once); conn_out holds 10 nodes per tet (B200FEM_ELEM_QUADTET order).
+   xyz_out / conn_out may be NULL to query *n_nodes_out first. */
+int b200fem_quadratic_tet_mesh(int n_nodes, const double* xyz, int n_tets, const int* conn, int* n_nodes_out,
+                               double* xyz_out, int* conn_out);
 /* seeded interior-node jitter: (2u-1)*frac*spacing per axis, u from
    splitmix64(seed) drawn in node order; boundary nodes stay put */
 int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,

@@ -26,7 +26,7 @@
 
 namespace {
 
-enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3 };
+enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3, ELEM_QUADTET = 4 };
 enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2, MAT_STVK = 3 };
 enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
 
@@ -191,6 +191,22 @@ static void pyramid_dNds(double* out, int i, double s0, double s1, double s2) {
   for (int c = 0; c < 3; c++) out[c] = v[i][c];
 }
 
+// QuadtetElement.getdNds (QuadtetElement.java:301-323), case by case
+static void quadtet_dNds(double* out, int i, double s1, double s2, double s3) {
+  const double s0 = 1 - s1 - s2 - s3;
+  const double v[10][3] = {{-4 * s0 + 1, -4 * s0 + 1, -4 * s0 + 1},
+                           {4 * s1 - 1, 0, 0},
+                           {0, 4 * s2 - 1, 0},
+                           {0, 0, 4 * s3 - 1},
+                           {4 * (s0 - s1), -4 * s1, -4 * s1},
+                           {4 * s2, 4 * s1, 0},
+                           {-4 * s2, 4 * (s0 - s2), -4 * s2},
+                           {-4 * s3, -4 * s3, 4 * (s0 - s3)},
+                           {4 * s3, 0, 4 * s1},
+                           {0, 4 * s3, 4 * s2}};
+  for (int c = 0; c < 3; c++) out[c] = v[i][c];
+}
+
 struct ShapeTable {
   int nen, nip;
   std::vector<double> GNs;  // nip * nen * 3
@@ -207,6 +223,22 @@ static ShapeTable make_shape(int type) {
     s.w = {TET_W};
     s.wGNs = s.GNs;  // TetElement.getWarpingPoint == integration point 0
     s.ww = TET_W;
+  } else if (type == ELEM_QUADTET) {
+    s.nen = 10; s.nip = 4;
+    // myIntegrationCoords with the reference's rounded constants
+    // (QuadtetElement.java:22-23, 255-262), weight 0.25/6
+    const double alpha = 0.58541020, beta = 0.13819660;
+    const double ip[4][3] = {{beta, beta, beta}, {alpha, beta, beta}, {beta, alpha, beta}, {beta, beta, alpha}};
+    s.GNs.resize(4 * 10 * 3);
+    s.w.assign(4, 0.25 / 6.0);
+    for (int k = 0; k < 4; k++)
+      for (int i = 0; i < 10; i++) quadtet_dNds(&s.GNs[(k * 10 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // getWarpingPoint (QuadtetElement.java:45-85): linear-tet gradients on the
+    // corner nodes, zero on the edge nodes, weight 1
+    s.wGNs.assign(30, 0.0);
+    for (int i = 0; i < 4; i++)
+      for (int c = 0; c < 3; c++) s.wGNs[i * 3 + c] = TET_GNS[i][c];
+    s.ww = 1;
   } else if (type == ELEM_WEDGE) {
     s.nen = 6; s.nip = 6;
     // myIntegrationCoords (WedgeElement.java:34-49)
@@ -1179,10 +1211,52 @@ int orc_num_threads(int n) {
 #endif
 }
 
+void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz, int* conn);
+
+// FemFactory.createQuadraticModel (FemFactory.java:5641-5710) for tets, as
+// the reference does it: for each element in order, the edge midpoints of
+// QuadtetElement.getQuadraticNodes (:130-175) are compared with every node so
+// far (exact position equality) and appended when new.  *nout = node count;
+// oxyz / oconn may be null.
+void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
+                        int* oconn) {
+  std::vector<double> P(xyz, xyz + 3 * (size_t)nn);
+  std::vector<int> Q(10 * (size_t)ne);
+  const int edges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  for (int e = 0; e < ne; e++) {
+    const int* c = conn + 4 * (size_t)e;
+    for (int a = 0; a < 4; a++) Q[10 * (size_t)e + a] = c[a];
+    for (int j = 0; j < 6; j++) {
+      const double* pa = xyz + 3 * (size_t)c[edges[j][0]];
+      const double* pb = xyz + 3 * (size_t)c[edges[j][1]];
+      double p[3];
+      for (int r = 0; r < 3; r++) p[r] = (pa[r] + pb[r]) * 0.5;  // Point3d.add, scale(0.5)
+      int found = -1;
+      const int cur = (int)(P.size() / 3);
+      for (int n = 0; n < cur && found < 0; n++)
+        if (P[3 * n] == p[0] && P[3 * n + 1] == p[1] && P[3 * n + 2] == p[2]) found = n;
+      if (found < 0) {
+        found = cur;
+        P.insert(P.end(), p, p + 3);
+      }
+      Q[10 * (size_t)e + 4 + j] = found;
+    }
+  }
+  *nout = (int)(P.size() / 3);
+  if (oxyz) std::copy(P.begin(), P.end(), oxyz);
+  if (oconn) std::copy(Q.begin(), Q.end(), oconn);
+}
+
 void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
   *nnodes = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[4] = {5, 1, 2, 3};
+  const int per_cell[5] = {5, 1, 2, 3, 5};
   *nelems = per_cell[type] * nx * ny * nz;
+  if (type == ELEM_QUADTET) {
+    std::vector<double> x(3 * (size_t)*nnodes);
+    std::vector<int> c(4 * (size_t)*nelems);
+    orc_create_grid(ELEM_TET, 1, 1, 1, nx, ny, nz, x.data(), c.data());
+    orc_quadratic_tets(*nnodes, x.data(), *nelems, c.data(), nnodes, nullptr, nullptr);
+  }
 }
 
 // FemFactory.createGridNodes (FemFactory.java:53-78), createTetGrid (:86-126)
@@ -1190,6 +1264,16 @@ void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
 // parseCode :203-263, getTetIndicesForHex :265-300), createHexGrid (:203-255).
 void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz,
                      double* xyz, int* conn) {
+  if (type == ELEM_QUADTET) {
+    // createQuadtetGrid (FemFactory.java:316-325)
+    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = 5 * nx * ny * nz;
+    std::vector<double> x(3 * (size_t)nl);
+    std::vector<int> c(4 * (size_t)ne);
+    orc_create_grid(ELEM_TET, wx, wy, wz, nx, ny, nz, x.data(), c.data());
+    int nout;
+    orc_quadratic_tets(nl, x.data(), ne, c.data(), &nout, xyz, conn);
+    return;
+  }
   double dx = 1.0 / nx, dy = 1.0 / ny, dz = 1.0 / nz;
   int idx = 0;
   for (int k = 0; k <= nz; k++)
@@ -1302,6 +1386,9 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   // (getAllowedSoftIncompMethod, :462-481).
   int method = incomp_method;
   if (!m->mat.incompressible()) method = INCOMP_OFF;
+  // NODAL only for tets and elements whose points map to nodes
+  // (softNodalIncompressAllowed, :400-405): quadratic tets take ELEMENT
+  else if (type == ELEM_QUADTET && (method == INCOMP_NODAL || method == INCOMP_AUTO)) method = INCOMP_ELEMENT;
   else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
   m->incomp = method;
   build_rest_data(*m);

@@ -20,8 +20,8 @@ _lib = None
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
 REF_SOURCE_ROOT = "/root/reference"
 
-ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID = 0, 1, 2, 3
-ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5}
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET = 0, 1, 2, 3, 4
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 
@@ -72,6 +72,8 @@ def lib():
         L.orc_num_threads.argtypes = [ctypes.c_int]
         L.orc_grid_dims.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
         L.orc_create_grid.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [_dp, _ip]
+        L.orc_quadratic_tets.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.c_void_p, ctypes.c_void_p]
         L.orc_jitter.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_uint64, _dp]
         L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip,
                                  ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int]
@@ -125,6 +127,19 @@ def grid(elem_type: int, widths, cells, jitter: float = 0.0, seed: int = 0):
         L.orc_jitter(nx, ny, nz, float(widths[0]), float(widths[1]), float(widths[2]), float(jitter),
                      ctypes.c_uint64(seed), xyz)
     return xyz.reshape(-1, 3), conn.reshape(-1, nen)
+
+
+def quadratic_tets(xyz, conn):
+    """FemFactory.createQuadraticModel of a linear tet mesh."""
+    L = lib()
+    x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+    c = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
+    n = ctypes.c_int()
+    L.orc_quadratic_tets(x.size // 3, x, c.size // 4, c, ctypes.byref(n), None, None)
+    ox = np.zeros(3 * n.value)
+    oc = np.zeros(10 * (c.size // 4), dtype=np.int32)
+    L.orc_quadratic_tets(x.size // 3, x, c.size // 4, c, ctypes.byref(n), ox.ctypes.data, oc.ctypes.data)
+    return ox.reshape(-1, 3), oc.reshape(-1, 10)
 
 
 class OracleModel:

@@ -31,6 +31,8 @@ def _cases():
         # NODAL on the pyramid beam (48 > 36)
         "mooneyrivlin_wedge_auto": W.small_wedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
         "mooneyrivlin_pyramid_auto": W.small_pyramid_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
+        "neohookean_quadtet": W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "mooneyrivlin_quadtet_auto": W.small_quadtet_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 

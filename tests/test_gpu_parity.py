@@ -54,6 +54,11 @@ def _cases():
         "mooneyrivlin_wedge_element": W.small_wedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
         "mooneyrivlin_pyramid_element_log": W.small_pyramid_beam(
             MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
+        # quadratic tets (10 nodes, 4 points; AUTO resolves to ELEMENT)
+        "linear_corotated_quadtet": W.small_quadtet_beam(LinearMaterial(2e4, 0.3, True)),
+        "neohookean_quadtet": W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "stvk_quadtet": W.small_quadtet_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "mooneyrivlin_quadtet_element": W.small_quadtet_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 
@@ -166,7 +171,8 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
                                   "linear_corotated_wedge", "linear_corotated_pyramid", "neohookean_wedge",
                                   "neohookean_pyramid", "stvk_wedge", "stvk_pyramid", "mooneyrivlin_wedge_nodal",
                                   "mooneyrivlin_pyramid_nodal", "mooneyrivlin_wedge_element",
-                                  "mooneyrivlin_pyramid_element_log"])
+                                  "mooneyrivlin_pyramid_element_log", "linear_corotated_quadtet",
+                                  "neohookean_quadtet", "stvk_quadtet", "mooneyrivlin_quadtet_element"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)

@@ -152,7 +152,9 @@ def test_polar_rotation(oracle):
     # wedges and pyramids (WedgeElement, PyramidElement)
     (1, [5e4, 0.45], 2, 0), (1, [5e4, 0.45], 3, 0), (3, [5e4, 0.3], 2, 0), (3, [5e4, 0.3], 3, 0),
     (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 3),
-    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 3, 3)])
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 3, 3),
+    # quadratic tets (QuadtetElement; soft incompressibility resolves to ELEMENT)
+    (1, [5e4, 0.45], 4, 0), (3, [5e4, 0.3], 4, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 4, 3)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
@@ -280,7 +282,7 @@ def test_constrained_step_holds_nodes_on_their_planes(oracle):
     assert np.abs(x - xyz).max() > 1e-6
 
 
-@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3)])
+@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3), (4, 5)])
 def test_grid_volumes_and_masses(oracle, etype, per_cell):
     # createTetGrid / createHexGrid / createWedgeGrid / createPyramidGrid:
     # every element positively oriented, rest volumes (sum of detJ0 w over
@@ -297,10 +299,39 @@ def test_grid_volumes_and_masses(oracle, etype, per_cell):
     assert abs(m.masses().sum() - 150.0) <= 1e-11
 
 
-@pytest.mark.parametrize("etype", [2, 3])
+@pytest.mark.parametrize("etype", [2, 3, 4])
 def test_library_grid_matches_oracle(oracle, etype):
     # the library's host-side mesh factory (no GPU needed) against the oracle's
     from artisynth_core_b200 import femmodel as FM
     xo, co = oracle.grid(etype, (1.0, 0.5, 0.3), (3, 2, 4))
     xl, cl = FM.create_grid(etype, 1.0, 0.5, 0.3, 3, 2, 4)
     assert np.array_equal(xo, xl) and np.array_equal(co, cl)
+
+
+def test_quadratic_tet_mesh(oracle):
+    # createQuadraticModel of a jittered tet grid: shared edges get one node,
+    # linear nodes keep their indices, library and oracle agree exactly
+    from artisynth_core_b200 import femmodel as FM
+    xyz, conn = oracle.grid(0, (1.0, 0.4, 0.4), (3, 2, 2), jitter=0.05, seed=2)
+    qx, qc = oracle.quadratic_tets(xyz, conn)
+    lx, lc = FM.quadratic_tet_mesh(xyz, conn)
+    assert np.array_equal(qx, lx) and np.array_equal(qc, lc)
+    assert np.array_equal(qx[:len(xyz)], xyz) and np.array_equal(qc[:, :4], conn)
+    edges = {tuple(sorted((a, b))) for t in conn for a, b in ((t[0], t[1]), (t[1], t[2]), (t[0], t[2]),
+                                                              (t[0], t[3]), (t[1], t[3]), (t[2], t[3]))}
+    assert len(qx) == len(xyz) + len(edges)
+    for t, q in zip(conn, qc):
+        assert np.array_equal(qx[q[4]], (xyz[t[0]] + xyz[t[1]]) * 0.5)
+        assert np.array_equal(qx[q[9]], (xyz[t[2]] + xyz[t[3]]) * 0.5)
+    # the quadratic tets of a straight-edged mesh span the same volume
+    m = oracle.OracleModel(4, qx, qc, np.zeros(len(qx), np.int32), 1, [5e4, 0.3], 1000.0)
+    l = oracle.OracleModel(0, xyz, conn, np.zeros(len(xyz), np.int32), 1, [5e4, 0.3], 1000.0)
+    assert abs(m.rest_volumes().sum() - l.rest_volumes().sum()) <= 1e-14
+
+
+def test_quadtet_incompressibility_resolves_to_element(oracle):
+    xyz, conn = oracle.grid(4, (1.0, 0.4, 0.4), (4, 2, 2))
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    for req in (oracle.INCOMP_AUTO, oracle.INCOMP_NODAL):
+        m = oracle.OracleModel(4, xyz, conn, fixed, 2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1000.0, req)
+        assert m.incomp == oracle.INCOMP_ELEMENT
