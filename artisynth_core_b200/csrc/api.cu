@@ -83,6 +83,7 @@ void free_pack(Engine& eng) {
   eng.last_step_params.clear();
   for (void* p : eng.allocations) cudaFree(p);
   eng.allocations.clear();
+  if (eng.d.status_host) cudaFreeHost(eng.d.status_host);
   eng.device_bytes = 0;
   eng.d = DevPack();
   eng.built = false;
@@ -628,6 +629,8 @@ int build_pack(Engine& eng) {
     std::vector<double> ms((size_t)M * 4, 0.0);
     for (int m = 0; m < M; m++) ms[(size_t)m * 4 + 2] = 1.0;
     CK(upload(eng, &d.model_scal, ms));
+    CK(cudaHostAlloc((void**)&d.status_host, sizeof(double) * (5 + ms.size()), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&d.status_dev, d.status_host, 0));
     // refinement sweeps (mixed form): FP64 residual, correction, and the
     // correction solves' own per-model results
     eng.refine_ok = eng.precision == B200FEM_PREC_MIXED && eng.groups.size() == 1 && !eng.groups[0].nodal &&
@@ -1183,13 +1186,14 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
 
 static int read_step_status(Engine& eng, b200fem_stats* stats, int max_iter) {
   DevPack& d = eng.d;
-  std::vector<double> ms((size_t)d.n_models * 4);
-  int flags[4];
-  long long dmin;
-  CK(cudaMemcpyAsync(ms.data(), d.model_scal, ms.size() * sizeof(double), cudaMemcpyDeviceToHost, eng.stream));
-  CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
-  CK(cudaMemcpyAsync(&dmin, d.dmin, sizeof(dmin), cudaMemcpyDeviceToHost, eng.stream));
+  CK(launch_status_pack(eng));
   CK(cudaStreamSynchronize(eng.stream));
+  const double* rec = d.status_host;
+  const double* ms = rec + 5;
+  int flags[4];
+  for (int i = 0; i < 4; i++) flags[i] = (int)rec[i];
+  long long dmin;
+  std::memcpy(&dmin, &rec[4], sizeof(dmin));
   b200fem_stats st{};
   bool all_conv = true;
   for (int m = 0; m < d.n_models; m++) {

@@ -172,6 +172,10 @@ struct DevPack {
   int unconv_cap = 0;
   int n_pieces = 0;
   double* model_scal = nullptr;  // n_models*8: rho, rr, bb, pq, conv, iters...
+  // mapped pinned host memory the status kernel fills after a step: flags[4]
+  // (as doubles), the smallest detJ's ordered bits, model_scal (n_models * 4)
+  double* status_host = nullptr;
+  double* status_dev = nullptr;
   unsigned* barrier = nullptr;   // [count, generation]
   int* flags = nullptr;          // [error, inverted count, ...]
   double* dmin = nullptr;        // min detJ (atomically reduced as ordered bits)
@@ -255,6 +259,7 @@ struct Engine {
 int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err);
 int build_pack(Engine& eng);
 void free_pack(Engine& eng);
+cudaError_t launch_status_pack(Engine& eng);
 int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne);
 // linear tets -> quadratic tets with shared edge nodes (createQuadraticModel)
 void quadratic_tets(int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,

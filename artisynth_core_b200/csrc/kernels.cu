@@ -1891,6 +1891,22 @@ __global__ void reset_status_kernel(int* flags, long long* dmin) {
   if (threadIdx.x == 0) *dmin = 0x7fefffffffffffffll;
 }
 
+// one record of the step's status for the host: flags, smallest detJ (the
+// ordered bits, moved as a double image) and the per-model results, written
+// into mapped pinned memory so that a single synchronisation delivers it
+__global__ void status_pack_kernel(const int* __restrict__ flags, const long long* __restrict__ dmin,
+                                   const double* __restrict__ ms, int n, double* __restrict__ out) {
+  if (threadIdx.x < 4) out[threadIdx.x] = (double)flags[threadIdx.x];
+  if (threadIdx.x == 4) out[4] = __longlong_as_double(*dmin);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) out[5 + i] = ms[i];
+}
+
+cudaError_t launch_status_pack(Engine& eng) {
+  status_pack_kernel<<<1, 256, 0, eng.stream>>>(eng.d.flags, (const long long*)eng.d.dmin, eng.d.model_scal,
+                                                4 * eng.d.n_models, eng.d.status_dev);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_reset_status(Engine& eng) {
   reset_status_kernel<<<1, 32, 0, eng.stream>>>(eng.d.flags, (long long*)eng.d.dmin);
   return cudaGetLastError();
