@@ -1262,38 +1262,34 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
   }
   CK(launch_reset_status(eng));
   const bool graphs = eng.use_graphs && !p->abort_on_inverted;
-  if (graphs && (eng.asm_exec == nullptr || eng.step_exec == nullptr || eng.step_exec_max_iter != max_iter)) {
-    // two captured graphs per step -- assembly (element kernels, block
-    // gather, RHS) and solve (PCG) -- so stream events between the graph
-    // launches time each phase
+  while ((int)eng.ev_pool.size() < 3) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    eng.ev_pool.push_back(e);
+  }
+  if (graphs && (eng.step_exec == nullptr || eng.step_exec_max_iter != max_iter)) {
+    // one captured graph per step: assembly (element kernels, block gather,
+    // RHS), an event record node between the phases (times each phase), and
+    // the solve (PCG); one launch per step leaves no gap between the phases
     for (cudaGraphExec_t* ex : {&eng.asm_exec, &eng.step_exec})
       if (*ex) {
         cudaGraphExecDestroy(*ex);
         *ex = nullptr;
       }
-    for (int g = 0; g < 2; g++) {
-      cudaGraph_t graph = nullptr;
-      CK(cudaStreamBeginCapture(eng.stream, cudaStreamCaptureModeThreadLocal));
-      cudaError_t ce;
-      if (g == 0) {
-        ce = launch_assemble(eng, 0, 0, false);
-        if (ce == cudaSuccess) ce = launch_rhs(eng);
-      } else {
-        ce = launch_solve(eng, max_iter);
-      }
-      cudaError_t ee = cudaStreamEndCapture(eng.stream, &graph);
-      if (ce != cudaSuccess) return cuda_fail(&eng, ce, "capture of the BackwardEuler step");
-      if (ee != cudaSuccess) return cuda_fail(&eng, ee, "cudaStreamEndCapture");
-      ce = cudaGraphInstantiate(g == 0 ? &eng.asm_exec : &eng.step_exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (ce != cudaSuccess) return cuda_fail(&eng, ce, "cudaGraphInstantiate");
-    }
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(eng.stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = launch_assemble(eng, 0, 0, false);
+    if (ce == cudaSuccess) ce = launch_rhs(eng);
+    // (an external record node: a plain record inside a capture only orders work)
+    if (ce == cudaSuccess) ce = cudaEventRecordWithFlags(eng.ev_pool[1], eng.stream, cudaEventRecordExternal);
+    if (ce == cudaSuccess) ce = launch_solve(eng, max_iter);
+    cudaError_t ee = cudaStreamEndCapture(eng.stream, &graph);
+    if (ce != cudaSuccess) return cuda_fail(&eng, ce, "capture of the BackwardEuler step");
+    if (ee != cudaSuccess) return cuda_fail(&eng, ee, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&eng.step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(&eng, ce, "cudaGraphInstantiate");
     eng.step_exec_max_iter = max_iter;
-  }
-  while ((int)eng.ev_pool.size() < 3) {
-    cudaEvent_t e;
-    CK(cudaEventCreate(&e));
-    eng.ev_pool.push_back(e);
   }
   const size_t state_bytes = 3 * sizeof(double) * (size_t)d.n_nodes;
   if (x_host) CK(cudaMemcpyAsync(d.x, x_host, state_bytes, cudaMemcpyHostToDevice, eng.stream));
@@ -1301,21 +1297,21 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   for (int s = 0; s < nsteps; s++) {
     CK(cudaEventRecord(eng.ev_pool[0], eng.stream));
-    if (graphs) CK(cudaGraphLaunch(eng.asm_exec, eng.stream));
-    else {
+    if (graphs) {
+      CK(cudaGraphLaunch(eng.step_exec, eng.stream));
+    } else {
       CK(launch_assemble(eng, 0, 0, false));
       CK(launch_rhs(eng));
+      CK(cudaEventRecord(eng.ev_pool[1], eng.stream));
+      if (p->abort_on_inverted) {
+        int flags[4];
+        CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
+        CK(cudaStreamSynchronize(eng.stream));
+        if (flags[1] > 0)
+          return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
+      }
+      CK(launch_solve(eng, max_iter));
     }
-    CK(cudaEventRecord(eng.ev_pool[1], eng.stream));
-    if (p->abort_on_inverted) {
-      int flags[4];
-      CK(cudaMemcpyAsync(flags, d.flags, sizeof(flags), cudaMemcpyDeviceToHost, eng.stream));
-      CK(cudaStreamSynchronize(eng.stream));
-      if (flags[1] > 0)
-        return fail(&eng, B200FEM_ERR_INVERTED, std::to_string(flags[1]) + " inverted elements");
-    }
-    if (graphs) CK(cudaGraphLaunch(eng.step_exec, eng.stream));
-    else CK(launch_solve(eng, max_iter));
     CK(cudaEventRecord(eng.ev_pool[2], eng.stream));
   }
   CK(cudaEventRecord(eng.ev[1], eng.stream));

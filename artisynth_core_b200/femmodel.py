@@ -442,13 +442,25 @@ class MechSystemSolver:
         """nsteps steps from the host state x, v (float64 arrays of 3N
         values, updated in place): the call a host that keeps the state makes
         every step (b200fem_backward_euler_step_host)."""
+        n3 = 3 * self.model.numNodes()
         for a in (x, v):
-            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size != 3 * self.model.numNodes():
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size != n3:
                 raise ValueError("x and v must be C-contiguous float64 arrays of 3N values")
-        p = self.params(h)
-        self.model.engine().call("b200fem_backward_euler_step_host", ctypes.byref(p), int(nsteps),
-                                 ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(v.ctypes.data),
-                                 ctypes.byref(self.stats))
+        # the step parameters and the bound entry point are kept between
+        # calls: this is the per-step call of a host that keeps the state
+        m = self.model
+        key = (h, m.mass_damping, m.stiffness_damping, tuple(m.gravity), self.tol, self.max_iter,
+               self.abort_on_inverted, self.pcg_variant, self.integrator)
+        cache = getattr(self, "_host_call", None)
+        eng = m.engine()
+        if cache is None or cache[0] != key or cache[1] is not eng:
+            p = self.params(h)
+            cache = (key, eng, p, ctypes.byref(p), ctypes.byref(self.stats),
+                     L.lib().b200fem_backward_euler_step_host)
+            self._host_call = cache
+        st = cache[5](eng.h, cache[3], int(nsteps), x.ctypes.data, v.ctypes.data, cache[4])
+        if st != L.OK:
+            L.check(st, eng.h)
         return self.stats
 
     def spmv(self, x):
