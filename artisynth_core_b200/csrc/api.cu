@@ -775,7 +775,7 @@ int b200fem_quadratic_tet_mesh(int n_nodes, const double* xyz, int n_tets, const
     if (conn[q] < 0 || conn[q] >= n_nodes) return fail(nullptr, B200FEM_ERR_INVALID_ARG, "connectivity index out of range");
   std::vector<double> qx;
   std::vector<int> qc;
-  quadratic_tets(n_nodes, xyz, n_tets, conn, qx, qc);
+  quadratic_mesh(B200FEM_ELEM_TET, n_nodes, xyz, n_tets, conn, qx, qc);
   *n_nodes_out = (int)(qx.size() / 3);
   if (xyz_out) std::copy(qx.begin(), qx.end(), xyz_out);
   if (conn_out) std::copy(qc.begin(), qc.end(), conn_out);

@@ -51,6 +51,9 @@ __constant__ float c_wed_gns_f[6 * 6 * 3], c_pyr_gns_f[5 * 5 * 3];
 // quadratic tets: 4 points x 10 nodes, warping point
 __constant__ double c_qtet_gns[4 * 10 * 3], c_qtet_wgns[10 * 3];
 __constant__ float c_qtet_gns_f[4 * 10 * 3];
+// quadratic hexes: 14 points x 20 nodes, warping point
+__constant__ double c_qhex_gns[14 * 20 * 3], c_qhex_wgns[20 * 3];
+__constant__ float c_qhex_gns_f[14 * 20 * 3];
 
 static bool g_const_ready[64] = {false};
 
@@ -88,9 +91,17 @@ static cudaError_t ensure_constants(int device) {
   for (int k = 0; k < 4; k++) shape_grads(B200FEM_ELEM_QUADTET, k, &qt[k * 30], &wt);
   shape_grads(B200FEM_ELEM_QUADTET, -1, qtw, &wt);
   for (int i = 0; i < 120; i++) qtf[i] = (float)qt[i];
+  static double qh[840], qhw[60];
+  static float qhf[840];
+  for (int k = 0; k < 14; k++) shape_grads(B200FEM_ELEM_QUADHEX, k, &qh[k * 60], &wt);
+  shape_grads(B200FEM_ELEM_QUADHEX, -1, qhw, &wt);
+  for (int i = 0; i < 840; i++) qhf[i] = (float)qh[i];
   for (int i = 0; i < 108; i++) wedf[i] = (float)wed[i];
   for (int i = 0; i < 75; i++) pyrf[i] = (float)pyr[i];
   cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_qhex_gns, qh, sizeof(qh))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qhex_wgns, qhw, sizeof(qhw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qhex_gns_f, qhf, sizeof(qhf))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qtet_gns, qt, sizeof(qt))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qtet_wgns, qtw, sizeof(qtw))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qtet_gns_f, qtf, sizeof(qtf))) != cudaSuccess) return e;
@@ -150,6 +161,9 @@ __device__ __forceinline__ T gns(int k, int n, int c) {
   } else if constexpr (TYPE == B200FEM_ELEM_QUADTET) {
     if constexpr (sizeof(T) == 8) return c_qtet_gns[(k * 10 + n) * 3 + c];
     else return c_qtet_gns_f[(k * 10 + n) * 3 + c];
+  } else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) {
+    if constexpr (sizeof(T) == 8) return c_qhex_gns[(k * 20 + n) * 3 + c];
+    else return c_qhex_gns_f[(k * 20 + n) * 3 + c];
   } else {
     if constexpr (sizeof(T) == 8) return c_pyr_gns[(k * 5 + n) * 3 + c];
     else return c_pyr_gns_f[(k * 5 + n) * 3 + c];
@@ -165,22 +179,27 @@ __device__ __forceinline__ double wgns(int n, int c) {
   else if constexpr (TYPE == B200FEM_ELEM_HEX) return c_hex_wgns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_WEDGE) return c_wed_wgns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return c_qtet_wgns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return c_qhex_wgns[3 * n + c];
   else return c_pyr_wgns[3 * n + c];
 }
 
 // integration weight of point k (TetElement 1/6; HexElement Gauss 1;
 // WedgeElement 1/6; PyramidElement 81/100 for the four base points, 125/27
-// for the fifth; QuadtetElement 0.25/6)
+// for the fifth; QuadtetElement 0.25/6; QuadhexElement 0.335180055401662 at
+// the eight corner points, 0.886426592797784 at the six face points)
 template <typename T, int TYPE>
 __device__ __forceinline__ T ip_weight(int k) {
   if constexpr (TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_WEDGE) return T(1.0 / 6.0);
   else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return T(0.25 / 6.0);
+  else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return k < 8 ? T(0.335180055401662) : T(0.886426592797784);
   else if constexpr (TYPE == B200FEM_ELEM_HEX) return T(1);
   else return k < 4 ? T(81 / 100.0) : T(125 / 27.0);
 }
 
 // lanes per element in the FP64 force kernel
-__host__ __device__ constexpr int force_slot(int type) { return elem_nip(type) > 1 ? 8 : 1; }
+__host__ __device__ constexpr int force_slot(int type) {
+  return elem_nip(type) > 8 ? 16 : (elem_nip(type) > 1 ? 8 : 1);
+}
 
 // calls f(std::integral_constant<int, TYPE>) for the run-time element type
 template <typename F>
@@ -191,6 +210,7 @@ static cudaError_t by_elem_type(int type, F&& f) {
     case B200FEM_ELEM_WEDGE: return f(std::integral_constant<int, B200FEM_ELEM_WEDGE>{});
     case B200FEM_ELEM_PYRAMID: return f(std::integral_constant<int, B200FEM_ELEM_PYRAMID>{});
     case B200FEM_ELEM_QUADTET: return f(std::integral_constant<int, B200FEM_ELEM_QUADTET>{});
+    case B200FEM_ELEM_QUADHEX: return f(std::integral_constant<int, B200FEM_ELEM_QUADHEX>{});
     default: return cudaErrorInvalidValue;
   }
 }
@@ -913,13 +933,13 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
   }
   if (a.det_stats) warp_record_det(a.flags, a.mindet, mydet, myinv);
   if constexpr (NIP > 1) {
-    // sum the points of one element: lanes 8q..8q+7 hold its points
+    // sum the points of one element: SLOT consecutive lanes hold its points
 #pragma unroll
     for (int n = 0; n < NEN; n++)
 #pragma unroll
       for (int c = 0; c < 3; c++)
 #pragma unroll
-        for (int off = 4; off > 0; off >>= 1) fl[n][c] += __shfl_xor_sync(0xffffffffu, fl[n][c], off);
+        for (int off = SLOT / 2; off > 0; off >>= 1) fl[n][c] += __shfl_xor_sync(0xffffffffu, fl[n][c], off);
     if (!live || k != 0) return;
   }
   if (!live) return;
@@ -1284,8 +1304,9 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   // elements per CTA (one thread per integration point in stage 1): a
   // large and a small tile per material; the small one gives more CTAs
   // per SM and fewer idle threads in the pair stage on small groups
-  constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : 32, NH_S = NH_L / 2;
-  constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : 16, MR_S = MR_L / 2;
+  // (quadratic hexes: 14 points of 20 gradients each per element)
+  constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : (TYPE == B200FEM_ELEM_QUADHEX ? 8 : 32), NH_S = NH_L / 2;
+  constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : (TYPE == B200FEM_ELEM_QUADHEX ? 8 : 16), MR_S = MR_L / 2;
   // StVenantKirchhoff has the general 6x6 tangent: MooneyRivlin's tiles
   constexpr int NH = B200FEM_MAT_NEOHOOKEAN, MR = B200FEM_MAT_MOONEYRIVLIN, SV = B200FEM_MAT_STVK;
   cudaStream_t st = eng.stream;

@@ -102,10 +102,64 @@ void quadtet_grad(double* g, int i, const double* s /* s0..s3 */) {
   }
 }
 
+// QuadhexElement node coordinates (QuadhexElement.java:117-142) and its
+// serendipity shape gradients (getdNds, :482-560): a corner (a, b, c) has
+// N = (1 + a s)(1 + b t)(1 + c r)(a s + b t + c r - 2)/8, an edge node with
+// a zero coordinate, e.g. (0, b, c), N = (1 - s^2)(1 + b t)(1 + c r)/4
+const double kQhexNode[20][3] = {{-1, -1, 1}, {1, -1, 1}, {1, 1, 1},  {-1, 1, 1},  {-1, -1, -1}, {1, -1, -1}, {1, 1, -1},
+                                 {-1, 1, -1}, {0, -1, 1}, {1, 0, 1},  {0, 1, 1},   {-1, 0, 1},   {0, -1, -1}, {1, 0, -1},
+                                 {0, 1, -1},  {-1, 0, -1}, {-1, -1, 0}, {1, -1, 0}, {1, 1, 0},   {-1, 1, 0}};
+void quadhex_grad(double* g, int i, const double* x /* s, t, r */) {
+  const double* c = kQhexNode[i];
+  double f[3];  // 1 + c_j x_j
+  for (int j = 0; j < 3; j++) f[j] = 1 + c[j] * x[j];
+  if (c[0] != 0 && c[1] != 0 && c[2] != 0) {
+    const double sum = c[0] * x[0] + c[1] * x[1] + c[2] * x[2];
+    for (int j = 0; j < 3; j++) {
+      const int a = (j + 1) % 3, b = (j + 2) % 3;
+      g[j] = 0.125 * c[j] * f[a] * f[b] * (sum - 2 + f[j]);
+    }
+    return;
+  }
+  const int z = c[0] == 0 ? 0 : (c[1] == 0 ? 1 : 2);  // the edge's own direction
+  for (int j = 0; j < 3; j++) {
+    const int a = (j + 1) % 3, b = (j + 2) % 3;
+    if (j == z) g[j] = -0.5 * x[z] * f[a] * f[b];
+    else {
+      const int o = (a == z) ? b : a;  // the other non-zero coordinate
+      g[j] = 0.25 * (1 - x[z] * x[z]) * c[j] * f[o];
+    }
+  }
+}
+
 }  // namespace
 
 // Shape gradients for integration point k (or the warping point, k = -1).
 void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
+  if (type == B200FEM_ELEM_QUADHEX) {
+    if (k < 0) {
+      // warping point (QuadhexElement.getWarpingPoint, :37-75): the linear
+      // hex's gradients at the centre on the corners, zero elsewhere, weight 1
+      std::memset(g, 0, 60 * sizeof(double));
+      for (int i = 0; i < 8; i++) hex_grad(g + 3 * i, i, 0, 0, 0);
+      *w = 1;
+      return;
+    }
+    // 14-point rule (myIntegrationCoords14, :159-182): the eight corners at
+    // +-q in node order with weight wc, then -+r on s, t, r with weight wf
+    const double q = 0.758686910639328, wc = 0.335180055401662;
+    const double r = 0.795822425754222, wf = 0.886426592797784;
+    double x[3] = {0, 0, 0};
+    if (k < 8) {
+      for (int j = 0; j < 3; j++) x[j] = kQhexNode[k][j] * q;
+      *w = wc;
+    } else {
+      x[(k - 8) / 2] = (k % 2 == 0) ? -r : r;
+      *w = wf;
+    }
+    for (int i = 0; i < 20; i++) quadhex_grad(g + 3 * i, i, x);
+    return;
+  }
   if (type == B200FEM_ELEM_QUADTET) {
     if (k < 0) {
       // warping point (QuadtetElement.getWarpingPoint, :45-85): the linear
@@ -223,45 +277,53 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
   if (nx < 1 || ny < 1 || nz < 1) return B200FEM_ERR_INVALID_ARG;
   if (elem_nen(type) == 0) return B200FEM_ERR_INVALID_ARG;
   *nn = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[5] = {5, 1, 2, 3, 5};  // tet, hex, wedge, pyramid, quadtet
+  const int per_cell[6] = {5, 1, 2, 3, 5, 1};  // tet, hex, wedge, pyramid, quadtet, quadhex
   *ne = per_cell[type] * nx * ny * nz;
-  if (type == B200FEM_ELEM_QUADTET) {
-    // the tet grid plus its edge nodes
+  if (type == B200FEM_ELEM_QUADTET || type == B200FEM_ELEM_QUADHEX) {
+    // the linear grid plus its edge nodes
+    const int lt = type == B200FEM_ELEM_QUADTET ? B200FEM_ELEM_TET : B200FEM_ELEM_HEX;
     std::vector<double> xyz(3 * (size_t)*nn);
-    std::vector<int> conn(4 * (size_t)*ne);
-    create_grid(B200FEM_ELEM_TET, 1, 1, 1, nx, ny, nz, xyz.data(), conn.data());
+    std::vector<int> conn(elem_nen(lt) * (size_t)*ne);
+    create_grid(lt, 1, 1, 1, nx, ny, nz, xyz.data(), conn.data());
     std::vector<double> qx;
     std::vector<int> qc;
-    quadratic_tets(*nn, xyz.data(), *ne, conn.data(), qx, qc);
+    quadratic_mesh(lt, *nn, xyz.data(), *ne, conn.data(), qx, qc);
     *nn = (int)(qx.size() / 3);
   }
   return B200FEM_OK;
 }
 
-// FemFactory.createQuadraticModel for tets (FemFactory.java:5641-5710,
-// QuadtetElement.getQuadraticNodes :130-175): the linear nodes keep their
-// indices; each element in order adds the midpoints (a + b) * 0.5 of its edges
-// 01, 12, 02, 03, 13, 23 unless a node already sits at exactly that position
-void quadratic_tets(int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
+// FemFactory.createQuadraticModel (FemFactory.java:5641-5710): the linear
+// nodes keep their indices; each element in order adds the midpoints
+// (a + b) * 0.5 of its edges (FemElement3dBase.createEdgeNode, :1591-1596)
+// unless a node already sits at exactly that position -- tets: edges 01, 12,
+// 02, 03, 13, 23 (QuadtetElement.getQuadraticNodes :130-175); hexes: 01 12 23
+// 30, 45 56 67 74, 04 15 26 37 (QuadhexElement.getQuadraticNodes :237-260)
+void quadratic_mesh(int lin_type, int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
                     std::vector<int>& out_conn) {
+  static const int kQhexEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                       {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  const bool hex = lin_type == B200FEM_ELEM_HEX;
+  const int nl = hex ? 8 : 4, nedge = hex ? 12 : 6, nq = nl + nedge;
+  const int(*edge)[2] = hex ? kQhexEdge : kQtetEdge;
   std::map<std::array<double, 3>, int> at;
   out_xyz.assign(xyz, xyz + 3 * (size_t)nn);
   for (int n = 0; n < nn; n++) at.emplace(std::array<double, 3>{xyz[3 * n], xyz[3 * n + 1], xyz[3 * n + 2]}, n);
-  out_conn.assign(10 * (size_t)ne, 0);
+  out_conn.assign(nq * (size_t)ne, 0);
   for (int e = 0; e < ne; e++) {
-    const int* c = conn + 4 * (size_t)e;
-    int* q = &out_conn[10 * (size_t)e];
-    for (int a = 0; a < 4; a++) q[a] = c[a];
-    for (int j = 0; j < 6; j++) {
-      const double* pa = xyz + 3 * (size_t)c[kQtetEdge[j][0]];
-      const double* pb = xyz + 3 * (size_t)c[kQtetEdge[j][1]];
+    const int* c = conn + nl * (size_t)e;
+    int* q = &out_conn[nq * (size_t)e];
+    for (int a = 0; a < nl; a++) q[a] = c[a];
+    for (int j = 0; j < nedge; j++) {
+      const double* pa = xyz + 3 * (size_t)c[edge[j][0]];
+      const double* pb = xyz + 3 * (size_t)c[edge[j][1]];
       const std::array<double, 3> p{(pa[0] + pb[0]) * 0.5, (pa[1] + pb[1]) * 0.5, (pa[2] + pb[2]) * 0.5};
       auto it = at.find(p);
       if (it == at.end()) {
         it = at.emplace(p, (int)(out_xyz.size() / 3)).first;
         out_xyz.insert(out_xyz.end(), p.begin(), p.end());
       }
-      q[4 + j] = it->second;
+      q[nl + j] = it->second;
     }
   }
 }
@@ -278,15 +340,17 @@ void quadratic_tets(int nn, const double* xyz, int ne, const int* conn, std::vec
 // (PyramidElement.java:216-270).
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn) {
-  if (type == B200FEM_ELEM_QUADTET) {
-    // createQuadtetGrid (FemFactory.java:316-325): the tet grid made quadratic
-    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = 5 * nx * ny * nz;
+  if (type == B200FEM_ELEM_QUADTET || type == B200FEM_ELEM_QUADHEX) {
+    // createQuadtetGrid / createQuadhexGrid (FemFactory.java:316-342): the
+    // linear grid made quadratic
+    const int lt = type == B200FEM_ELEM_QUADTET ? B200FEM_ELEM_TET : B200FEM_ELEM_HEX;
+    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = (lt == B200FEM_ELEM_TET ? 5 : 1) * nx * ny * nz;
     std::vector<double> lx(3 * (size_t)nl);
-    std::vector<int> lc(4 * (size_t)ne);
-    create_grid(B200FEM_ELEM_TET, wx, wy, wz, nx, ny, nz, lx.data(), lc.data());
+    std::vector<int> lc(elem_nen(lt) * (size_t)ne);
+    create_grid(lt, wx, wy, wz, nx, ny, nz, lx.data(), lc.data());
     std::vector<double> qx;
     std::vector<int> qc;
-    quadratic_tets(nl, lx.data(), ne, lc.data(), qx, qc);
+    quadratic_mesh(lt, nl, lx.data(), ne, lc.data(), qx, qc);
     std::copy(qx.begin(), qx.end(), xyz);
     std::copy(qc.begin(), qc.end(), conn);
     return;
@@ -391,6 +455,12 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   else if (m.elem_type == B200FEM_ELEM_QUADTET &&
            (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
     method = B200FEM_INCOMP_ELEMENT;
+  else if (m.elem_type == B200FEM_ELEM_QUADHEX && method != B200FEM_INCOMP_OFF) {
+    // QuadhexElement.numPressureVals() == 4 (:443-445): ELEMENT with a 4x4
+    // Rinv per element is not built
+    err = "soft incompressibility of quadratic hexes (four pressure values per element) is not supported";
+    return B200FEM_ERR_UNSUPPORTED;
+  }
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
   h.incomp = method;

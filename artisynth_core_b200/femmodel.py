@@ -150,6 +150,12 @@ class FemFactory:
         return m
 
     @staticmethod
+    def createQuadhexGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_QUADHEX, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
     def createWedgeGrid(model, wx, wy, wz, nx, ny, nz):
         m = model if model is not None else FemModel3d()
         m._set_grid(L.ELEM_WEDGE, wx, wy, wz, nx, ny, nz)

@@ -57,6 +57,10 @@ extern "C" {
 #define B200FEM_ELEM_QUADTET 4 /* QuadtetElement, 10 nodes (corners 0-3, then the midpoints
                                   of edges 01, 12, 02, 03, 13, 23), 4 integration points;
                                   soft incompressibility resolves to ELEMENT */
+#define B200FEM_ELEM_QUADHEX 5 /* QuadhexElement, 20 nodes (corners 0-7, then the midpoints of
+                                  edges 01 12 23 30, 45 56 67 74, 04 15 26 37), 14 points;
+                                  compressible materials (its soft incompressibility has four
+                                  pressure values per element: B200FEM_ERR_UNSUPPORTED) */
 
 /* materials (parameter layout of b200fem_set_material) */
 #define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */

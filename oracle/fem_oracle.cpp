@@ -26,7 +26,7 @@
 
 namespace {
 
-enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3, ELEM_QUADTET = 4 };
+enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3, ELEM_QUADTET = 4, ELEM_QUADHEX = 5 };
 enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2, MAT_STVK = 3 };
 enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
 
@@ -207,6 +207,37 @@ static void quadtet_dNds(double* out, int i, double s1, double s2, double s3) {
   for (int c = 0; c < 3; c++) out[c] = v[i][c];
 }
 
+// QuadhexElement.getdNds (QuadhexElement.java:482-560), case by case at
+// (s, t, r)
+static void quadhex_dNds(double* out, int i, double s, double t, double r) {
+  double u, a, b, c;
+  switch (i) {
+    case 0: u = (s + t - r + 1); a = (1 - t) * (1 + r) * (s + u); b = (1 - s) * (1 + r) * (t + u); c = (1 - s) * (1 - t) * (r - u); break;
+    case 1: u = (s - t + r - 1); a = (1 - t) * (1 + r) * (s + u); b = (1 + s) * (1 + r) * (t - u); c = (1 + s) * (1 - t) * (r + u); break;
+    case 2: u = (s + t + r - 1); a = (1 + t) * (1 + r) * (s + u); b = (1 + s) * (1 + r) * (t + u); c = (1 + s) * (1 + t) * (r + u); break;
+    case 3: u = (s - t - r + 1); a = (1 + t) * (1 + r) * (s + u); b = (1 - s) * (1 + r) * (t - u); c = (1 - s) * (1 + t) * (r - u); break;
+    case 4: u = (s + t + r + 1); a = (1 - t) * (1 - r) * (s + u); b = (1 - s) * (1 - r) * (t + u); c = (1 - s) * (1 - t) * (r + u); break;
+    case 5: u = (s - t - r - 1); a = (1 - t) * (1 - r) * (s + u); b = (1 + s) * (1 - r) * (t - u); c = (1 + s) * (1 - t) * (r - u); break;
+    case 6: u = (s + t - r - 1); a = (1 + t) * (1 - r) * (s + u); b = (1 + s) * (1 - r) * (t + u); c = (1 + s) * (1 + t) * (r - u); break;
+    case 7: u = (s - t + r + 1); a = (1 + t) * (1 - r) * (s + u); b = (1 - s) * (1 - r) * (t - u); c = (1 - s) * (1 + t) * (r + u); break;
+    case 8: out[0] = -.5 * s * (1 - t) * (1 + r); out[1] = -.25 * (1 - s * s) * (1 + r); out[2] = .25 * (1 - s * s) * (1 - t); return;
+    case 9: out[0] = .25 * (1 - t * t) * (1 + r); out[1] = -.5 * t * (1 + s) * (1 + r); out[2] = .25 * (1 + s) * (1 - t * t); return;
+    case 10: out[0] = -.5 * s * (1 + t) * (1 + r); out[1] = .25 * (1 - s * s) * (1 + r); out[2] = .25 * (1 - s * s) * (1 + t); return;
+    case 11: out[0] = -.25 * (1 - t * t) * (1 + r); out[1] = -.5 * t * (1 - s) * (1 + r); out[2] = .25 * (1 - s) * (1 - t * t); return;
+    case 12: out[0] = -.5 * s * (1 - t) * (1 - r); out[1] = -.25 * (1 - s * s) * (1 - r); out[2] = -.25 * (1 - s * s) * (1 - t); return;
+    case 13: out[0] = .25 * (1 - t * t) * (1 - r); out[1] = -.5 * t * (1 + s) * (1 - r); out[2] = -.25 * (1 + s) * (1 - t * t); return;
+    case 14: out[0] = -.5 * s * (1 + t) * (1 - r); out[1] = .25 * (1 - s * s) * (1 - r); out[2] = -.25 * (1 - s * s) * (1 + t); return;
+    case 15: out[0] = -.25 * (1 - t * t) * (1 - r); out[1] = -.5 * t * (1 - s) * (1 - r); out[2] = -.25 * (1 - s) * (1 - t * t); return;
+    case 16: out[0] = -.25 * (1 - t) * (1 - r * r); out[1] = -.25 * (1 - s) * (1 - r * r); out[2] = -.5 * r * (1 - s) * (1 - t); return;
+    case 17: out[0] = .25 * (1 - t) * (1 - r * r); out[1] = -.25 * (1 + s) * (1 - r * r); out[2] = -.5 * r * (1 + s) * (1 - t); return;
+    case 18: out[0] = .25 * (1 + t) * (1 - r * r); out[1] = .25 * (1 + s) * (1 - r * r); out[2] = -.5 * r * (1 + s) * (1 + t); return;
+    default: out[0] = -.25 * (1 + t) * (1 - r * r); out[1] = .25 * (1 - s) * (1 - r * r); out[2] = -.5 * r * (1 - s) * (1 + t); return;
+  }
+  out[0] = a * 0.125;  // Vector3d.scale(0.125)
+  out[1] = b * 0.125;
+  out[2] = c * 0.125;
+}
+
 struct ShapeTable {
   int nen, nip;
   std::vector<double> GNs;  // nip * nen * 3
@@ -223,6 +254,23 @@ static ShapeTable make_shape(int type) {
     s.w = {TET_W};
     s.wGNs = s.GNs;  // TetElement.getWarpingPoint == integration point 0
     s.ww = TET_W;
+  } else if (type == ELEM_QUADHEX) {
+    s.nen = 20; s.nip = 14;
+    // myIntegrationCoords14 (QuadhexElement.java:159-182)
+    const double q = 0.758686910639328, wc = 0.335180055401662;
+    const double r = 0.795822425754222, wf = 0.886426592797784;
+    const double ip[14][3] = {{-q, -q, q}, {q, -q, q}, {q, q, q}, {-q, q, q}, {-q, -q, -q}, {q, -q, -q}, {q, q, -q},
+                              {-q, q, -q}, {-r, 0, 0}, {r, 0, 0}, {0, -r, 0}, {0, r, 0},  {0, 0, -r},  {0, 0, r}};
+    s.GNs.resize(14 * 20 * 3);
+    s.w.assign(14, wf);
+    for (int k = 0; k < 8; k++) s.w[k] = wc;
+    for (int k = 0; k < 14; k++)
+      for (int i = 0; i < 20; i++) quadhex_dNds(&s.GNs[(k * 20 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // getWarpingPoint (:37-75): the linear hex's gradients at the centre on
+    // the corners, zero on the edge nodes, weight 1
+    s.wGNs.assign(60, 0.0);
+    for (int i = 0; i < 8; i++) hex_dNds(&s.wGNs[i * 3], i, 0, 0, 0);
+    s.ww = 1;
   } else if (type == ELEM_QUADTET) {
     s.nen = 10; s.nip = 4;
     // myIntegrationCoords with the reference's rounded constants
@@ -1218,15 +1266,19 @@ void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, 
 // QuadtetElement.getQuadraticNodes (:130-175) are compared with every node so
 // far (exact position equality) and appended when new.  *nout = node count;
 // oxyz / oconn may be null.
-void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
-                        int* oconn) {
+static void quadratic_model(int hex, int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
+                            int* oconn) {
   std::vector<double> P(xyz, xyz + 3 * (size_t)nn);
-  std::vector<int> Q(10 * (size_t)ne);
-  const int edges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  const int nl = hex ? 8 : 4, nedge = hex ? 12 : 6, nq = nl + nedge;
+  std::vector<int> Q(nq * (size_t)ne);
+  // QuadtetElement.getQuadraticNodes (:130-175), QuadhexElement's (:237-260)
+  const int tedges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+  const int hedges[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  const int(*edges)[2] = hex ? hedges : tedges;
   for (int e = 0; e < ne; e++) {
-    const int* c = conn + 4 * (size_t)e;
-    for (int a = 0; a < 4; a++) Q[10 * (size_t)e + a] = c[a];
-    for (int j = 0; j < 6; j++) {
+    const int* c = conn + nl * (size_t)e;
+    for (int a = 0; a < nl; a++) Q[nq * (size_t)e + a] = c[a];
+    for (int j = 0; j < nedge; j++) {
       const double* pa = xyz + 3 * (size_t)c[edges[j][0]];
       const double* pb = xyz + 3 * (size_t)c[edges[j][1]];
       double p[3];
@@ -1239,7 +1291,7 @@ void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int*
         found = cur;
         P.insert(P.end(), p, p + 3);
       }
-      Q[10 * (size_t)e + 4 + j] = found;
+      Q[nq * (size_t)e + nl + j] = found;
     }
   }
   *nout = (int)(P.size() / 3);
@@ -1247,15 +1299,26 @@ void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int*
   if (oconn) std::copy(Q.begin(), Q.end(), oconn);
 }
 
+void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
+                        int* oconn) {
+  quadratic_model(0, nn, xyz, ne, conn, nout, oxyz, oconn);
+}
+
+void orc_quadratic_hexes(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
+                         int* oconn) {
+  quadratic_model(1, nn, xyz, ne, conn, nout, oxyz, oconn);
+}
+
 void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
   *nnodes = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[5] = {5, 1, 2, 3, 5};
+  const int per_cell[6] = {5, 1, 2, 3, 5, 1};
   *nelems = per_cell[type] * nx * ny * nz;
-  if (type == ELEM_QUADTET) {
+  if (type == ELEM_QUADTET || type == ELEM_QUADHEX) {
+    const int hex = type == ELEM_QUADHEX;
     std::vector<double> x(3 * (size_t)*nnodes);
-    std::vector<int> c(4 * (size_t)*nelems);
-    orc_create_grid(ELEM_TET, 1, 1, 1, nx, ny, nz, x.data(), c.data());
-    orc_quadratic_tets(*nnodes, x.data(), *nelems, c.data(), nnodes, nullptr, nullptr);
+    std::vector<int> c((hex ? 8 : 4) * (size_t)*nelems);
+    orc_create_grid(hex ? ELEM_HEX : ELEM_TET, 1, 1, 1, nx, ny, nz, x.data(), c.data());
+    quadratic_model(hex, *nnodes, x.data(), *nelems, c.data(), nnodes, nullptr, nullptr);
   }
 }
 
@@ -1264,14 +1327,15 @@ void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
 // parseCode :203-263, getTetIndicesForHex :265-300), createHexGrid (:203-255).
 void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz,
                      double* xyz, int* conn) {
-  if (type == ELEM_QUADTET) {
-    // createQuadtetGrid (FemFactory.java:316-325)
-    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = 5 * nx * ny * nz;
+  if (type == ELEM_QUADTET || type == ELEM_QUADHEX) {
+    // createQuadtetGrid / createQuadhexGrid (FemFactory.java:316-342)
+    const int hex = type == ELEM_QUADHEX;
+    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = (hex ? 1 : 5) * nx * ny * nz;
     std::vector<double> x(3 * (size_t)nl);
-    std::vector<int> c(4 * (size_t)ne);
-    orc_create_grid(ELEM_TET, wx, wy, wz, nx, ny, nz, x.data(), c.data());
+    std::vector<int> c((hex ? 8 : 4) * (size_t)ne);
+    orc_create_grid(hex ? ELEM_HEX : ELEM_TET, wx, wy, wz, nx, ny, nz, x.data(), c.data());
     int nout;
-    orc_quadratic_tets(nl, x.data(), ne, c.data(), &nout, xyz, conn);
+    quadratic_model(hex, nl, x.data(), ne, c.data(), &nout, xyz, conn);
     return;
   }
   double dx = 1.0 / nx, dy = 1.0 / ny, dz = 1.0 / nz;
@@ -1389,6 +1453,12 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   // NODAL only for tets and elements whose points map to nodes
   // (softNodalIncompressAllowed, :400-405): quadratic tets take ELEMENT
   else if (type == ELEM_QUADTET && (method == INCOMP_NODAL || method == INCOMP_AUTO)) method = INCOMP_ELEMENT;
+  // QuadhexElement has four pressure values per element (:443-445): the
+  // restatement covers one, so its incompressible forms are refused
+  else if (type == ELEM_QUADHEX && method != INCOMP_OFF) {
+    delete m;
+    return nullptr;
+  }
   else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
   m->incomp = method;
   build_rest_data(*m);

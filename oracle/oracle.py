@@ -20,8 +20,8 @@ _lib = None
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
 REF_SOURCE_ROOT = "/root/reference"
 
-ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET = 0, 1, 2, 3, 4
-ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10}
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET, ELEM_QUADHEX = 0, 1, 2, 3, 4, 5
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10, ELEM_QUADHEX: 20}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 
@@ -72,8 +72,9 @@ def lib():
         L.orc_num_threads.argtypes = [ctypes.c_int]
         L.orc_grid_dims.argtypes = [ctypes.c_int] * 4 + [ctypes.POINTER(ctypes.c_int)] * 2
         L.orc_create_grid.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [_dp, _ip]
-        L.orc_quadratic_tets.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int),
-                                         ctypes.c_void_p, ctypes.c_void_p]
+        for fn in ("orc_quadratic_tets", "orc_quadratic_hexes"):
+            getattr(L, fn).argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.c_void_p, ctypes.c_void_p]
         L.orc_jitter.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_uint64, _dp]
         L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip,
                                  ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int]
@@ -159,6 +160,8 @@ class OracleModel:
         mp[: len(mat_params)] = mat_params
         self.h = self.L.orc_create(elem_type, self.N, self.rest, self.E, self.conn, fx, mat_kind, mp,
                                    float(density), incomp)
+        if not self.h:
+            raise ValueError("the oracle refuses this model (quadratic hexes with soft incompressibility)")
         self.nact = self.L.orc_num_active(self.h)
         self.nnzb = self.L.orc_nnzb(self.h)
         self.incomp = self.L.orc_incomp_method(self.h)

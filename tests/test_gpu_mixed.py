@@ -33,6 +33,7 @@ def _cases():
         "mooneyrivlin_pyramid_auto": W.small_pyramid_beam(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370)),
         "neohookean_quadtet": W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45)),
         "mooneyrivlin_quadtet_auto": W.small_quadtet_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
     }
 
 

@@ -59,6 +59,11 @@ def _cases():
         "neohookean_quadtet": W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45)),
         "stvk_quadtet": W.small_quadtet_beam(StVenantKirchoffMaterial(5e4, 0.3)),
         "mooneyrivlin_quadtet_element": W.small_quadtet_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        # quadratic hexes (20 nodes, 14 points; compressible forms)
+        "linear_corotated_quadhex": W.small_quadhex_beam(LinearMaterial(2e4, 0.3, True)),
+        "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "stvk_quadhex": W.small_quadhex_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "mooneyrivlin_quadhex_off": W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 
@@ -70,7 +75,7 @@ def _incomp_off(wl):
 @pytest.fixture(scope="module")
 def cases(b200):
     cs = _cases()
-    for k in ("mooneyrivlin_tet_off", "mooneyrivlin_hex_full"):
+    for k in ("mooneyrivlin_tet_off", "mooneyrivlin_hex_full", "mooneyrivlin_quadhex_off"):
         _incomp_off(cs[k])
     # more hexes than active nodes is needed for AUTO -> NODAL; request it
     cs["mooneyrivlin_hex_nodal"].incomp = L.INCOMP_NODAL
@@ -172,7 +177,9 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
                                   "neohookean_pyramid", "stvk_wedge", "stvk_pyramid", "mooneyrivlin_wedge_nodal",
                                   "mooneyrivlin_pyramid_nodal", "mooneyrivlin_wedge_element",
                                   "mooneyrivlin_pyramid_element_log", "linear_corotated_quadtet",
-                                  "neohookean_quadtet", "stvk_quadtet", "mooneyrivlin_quadtet_element"])
+                                  "neohookean_quadtet", "stvk_quadtet", "mooneyrivlin_quadtet_element",
+                                  "linear_corotated_quadhex", "neohookean_quadhex", "stvk_quadhex",
+                                  "mooneyrivlin_quadhex_off"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)
@@ -330,3 +337,12 @@ def test_tet_kernels_agree(name, precision, cases):
         assert ms.stats.num_inverted == 0
         m._invalidate()
     assert rel_err(xs[0], xs[1]) <= (1e-11 if precision == L.PREC_FP64 else 1e-6), rel_err(xs[0], xs[1])
+
+
+def test_quadhex_soft_incompressibility_refused(b200):
+    """QuadhexElement carries four pressure values per element; its soft
+    incompressibility is refused at build with B200FEM_ERR_UNSUPPORTED."""
+    wl = W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)).build_mesh()
+    with pytest.raises(L.B200FemError) as ei:
+        _gpu_model(wl).updateStressAndStiffness(wl.rest)
+    assert ei.value.status == L.ERR_UNSUPPORTED

@@ -178,7 +178,7 @@ def _add_reference_dilational(R, arr, crs_dev, nnz):
 @pytest.mark.parametrize("case", ["neohookean_tet", "neohookean_hex", "stvk_hex", "mooneyrivlin_hex_element",
                                   "neohookean_wedge", "neohookean_pyramid", "stvk_pyramid",
                                   "mooneyrivlin_wedge_element", "neohookean_quadtet",
-                                  "mooneyrivlin_quadtet_element"])
+                                  "mooneyrivlin_quadtet_element", "neohookean_quadhex"])
 def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
     R = _ref_lib()
     if case == "neohookean_tet":
@@ -193,6 +193,8 @@ def test_reference_kernel_assembles_engine_stiffness(b200, oracle, case):
         wl = W.small_pyramid_beam(NeoHookeanMaterial(5e4, 0.45))
     elif case == "stvk_pyramid":
         wl = W.small_pyramid_beam(StVenantKirchoffMaterial(5e4, 0.3))
+    elif case == "neohookean_quadhex":
+        wl = W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45))
     elif case == "neohookean_quadtet":
         wl = W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45))
     elif case == "mooneyrivlin_quadtet_element":
@@ -257,13 +259,14 @@ def _linear_element_arrays(om_geom, wl, E, nu):
             params, grads.reshape(-1), dvs.reshape(-1))
 
 
-@pytest.mark.parametrize("case", ["tet", "hex", "wedge", "pyramid", "quadtet"])
+@pytest.mark.parametrize("case", ["tet", "hex", "wedge", "pyramid", "quadtet", "quadhex"])
 def test_reference_kernel_assembles_linear_rest_stiffness(b200, oracle, case):
     import torch
     R = _ref_lib()
     E, nu = 5e4, 0.33
     beam = {"tet": W.small_tet_beam, "hex": W.small_hex_beam, "wedge": W.small_wedge_beam,
-            "pyramid": W.small_pyramid_beam, "quadtet": W.small_quadtet_beam}[case]
+            "pyramid": W.small_pyramid_beam, "quadtet": W.small_quadtet_beam,
+            "quadhex": W.small_quadhex_beam}[case]
     wl = beam(LinearMaterial(E, nu, False))
     geom = beam(NeoHookeanMaterial(E, nu))
     wl.build_mesh()

@@ -154,7 +154,9 @@ def test_polar_rotation(oracle):
     (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 2, 3),
     (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 1], 3, 3),
     # quadratic tets (QuadtetElement; soft incompressibility resolves to ELEMENT)
-    (1, [5e4, 0.45], 4, 0), (3, [5e4, 0.3], 4, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 4, 3)])
+    (1, [5e4, 0.45], 4, 0), (3, [5e4, 0.3], 4, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 4, 3),
+    # quadratic hexes (QuadhexElement, 14 points; compressible forms)
+    (1, [5e4, 0.45], 5, 0), (3, [5e4, 0.3], 5, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 5, 0)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
@@ -282,7 +284,7 @@ def test_constrained_step_holds_nodes_on_their_planes(oracle):
     assert np.abs(x - xyz).max() > 1e-6
 
 
-@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3), (4, 5)])
+@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3), (4, 5), (5, 1)])
 def test_grid_volumes_and_masses(oracle, etype, per_cell):
     # createTetGrid / createHexGrid / createWedgeGrid / createPyramidGrid:
     # every element positively oriented, rest volumes (sum of detJ0 w over
@@ -299,7 +301,7 @@ def test_grid_volumes_and_masses(oracle, etype, per_cell):
     assert abs(m.masses().sum() - 150.0) <= 1e-11
 
 
-@pytest.mark.parametrize("etype", [2, 3, 4])
+@pytest.mark.parametrize("etype", [2, 3, 4, 5])
 def test_library_grid_matches_oracle(oracle, etype):
     # the library's host-side mesh factory (no GPU needed) against the oracle's
     from artisynth_core_b200 import femmodel as FM
@@ -335,3 +337,16 @@ def test_quadtet_incompressibility_resolves_to_element(oracle):
     for req in (oracle.INCOMP_AUTO, oracle.INCOMP_NODAL):
         m = oracle.OracleModel(4, xyz, conn, fixed, 2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1000.0, req)
         assert m.incomp == oracle.INCOMP_ELEMENT
+
+
+def test_quadhex_shape_functions(oracle):
+    # the 14-point rule integrates the 20-node serendipity gradients of a unit
+    # cube exactly: rest volume 8 per element of the [-1, 1]^3 cube, and
+    # sum_n dN_n/ds = 0 at every point (partition of unity)
+    xyz, conn = oracle.grid(5, (2.0, 2.0, 2.0), (1, 1, 1))
+    assert xyz.shape == (20, 3) and conn.shape == (1, 20)
+    m = oracle.OracleModel(5, xyz, conn, np.zeros(20, np.int32), 1, [5e4, 0.3], 1000.0)
+    assert abs(m.rest_volumes().sum() - 8.0) <= 1e-13
+    with pytest.raises(ValueError):
+        oracle.OracleModel(5, xyz, conn, np.zeros(20, np.int32), 2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1000.0,
+                           oracle.INCOMP_AUTO)
