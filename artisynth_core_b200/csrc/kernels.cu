@@ -5,13 +5,15 @@
 //                     forces in FP64, the ten upper pair blocks in the
 //                     storage precision, warp-staged contiguous stores
 //   elem_nonlinear_kernel / elem_linear_kernel
-//                     hexahedra (and tets on request): coordinates staged
+//                     every element type (hex, wedge, pyramid, quadratic tet
+//                     and hex; tets on request) through the shape traits
+//                     below: coordinates staged
 //                     through shared memory, per-integration-point kinematics
 //                     and material (F, sigma, D), then one thread per element
 //                     node pair forms the 3x3 tangent block and one per node
 //                     the stress force (FemModel3d.computeStressAndStiffness,
 //                     FemModel3d.java:3333-3666)
-//   elem_force_kernel FP64 nodal forces of the mixed form (hexes)
+//   elem_force_kernel FP64 nodal forces of the mixed form (multi-point elements)
 //   gather_block_kernel
 //                     deterministic, atomic-free scatter: every 3x3 block sums
 //                     its precomputed contribution list (element pair,
