@@ -26,8 +26,9 @@ ERR_BUDGET = -6
 ERR_TIMEOUT = -7
 ERR_NO_CONVERGE = -13
 
-ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET, ELEM_QUADHEX = 0, 1, 2, 3, 4, 5
-ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10, ELEM_QUADHEX: 20}
+ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET, ELEM_QUADHEX, ELEM_QUADWEDGE, ELEM_QUADPYRAMID = range(8)
+ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10, ELEM_QUADHEX: 20,
+              ELEM_QUADWEDGE: 15, ELEM_QUADPYRAMID: 13}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1

@@ -25,11 +25,18 @@ constexpr int kMatParams = 8;
 // wedges and pyramids, like hexes, have one integration point per node
 __host__ __device__ constexpr int elem_nen(int type) {
   return type == B200FEM_ELEM_TET ? 4 : type == B200FEM_ELEM_HEX ? 8 : type == B200FEM_ELEM_WEDGE ? 6
-         : type == B200FEM_ELEM_PYRAMID ? 5 : type == B200FEM_ELEM_QUADTET ? 10 : type == B200FEM_ELEM_QUADHEX ? 20 : 0;
+         : type == B200FEM_ELEM_PYRAMID ? 5 : type == B200FEM_ELEM_QUADTET ? 10 : type == B200FEM_ELEM_QUADHEX ? 20
+         : type == B200FEM_ELEM_QUADWEDGE ? 15 : type == B200FEM_ELEM_QUADPYRAMID ? 13 : 0;
 }
 __host__ __device__ constexpr int elem_nip(int type) {
   return type == B200FEM_ELEM_TET ? 1 : type == B200FEM_ELEM_QUADTET ? 4 : type == B200FEM_ELEM_QUADHEX ? 14
-                                                                                                     : elem_nen(type);
+         : type == B200FEM_ELEM_QUADWEDGE ? 9 : type == B200FEM_ELEM_QUADPYRAMID ? 5 : elem_nen(type);
+}
+// the linear type a quadratic type is built from (createQuadraticModel)
+__host__ __device__ constexpr int elem_linear_base(int type) {
+  return type == B200FEM_ELEM_QUADTET ? B200FEM_ELEM_TET : type == B200FEM_ELEM_QUADHEX ? B200FEM_ELEM_HEX
+         : type == B200FEM_ELEM_QUADWEDGE ? B200FEM_ELEM_WEDGE : type == B200FEM_ELEM_QUADPYRAMID ? B200FEM_ELEM_PYRAMID
+         : -1;
 }
 // integration point k lies at node k (FemElement3d.integrationPointsMapToNodes)
 __host__ __device__ constexpr bool elem_ip_at_nodes(int type) {
@@ -262,8 +269,8 @@ int build_pack(Engine& eng);
 void free_pack(Engine& eng);
 cudaError_t launch_status_pack(Engine& eng);
 int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne);
-// linear tets or hexes -> quadratic tets or hexes with shared edge nodes
-// (createQuadraticModel); lin_type B200FEM_ELEM_TET or B200FEM_ELEM_HEX
+// linear -> quadratic elements with shared edge nodes (createQuadraticModel);
+// lin_type tet, hex, wedge or pyramid
 void quadratic_mesh(int lin_type, int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
                     std::vector<int>& out_conn);
 // dN/ds of the element's nodes at integration point k (k = -1: the warping

@@ -56,6 +56,10 @@ __constant__ float c_qtet_gns_f[4 * 10 * 3];
 // quadratic hexes: 14 points x 20 nodes, warping point
 __constant__ double c_qhex_gns[14 * 20 * 3], c_qhex_wgns[20 * 3];
 __constant__ float c_qhex_gns_f[14 * 20 * 3];
+// quadratic wedges (9 points x 15 nodes) and pyramids (5 points x 13 nodes)
+__constant__ double c_qwed_gns[9 * 15 * 3], c_qwed_wgns[15 * 3];
+__constant__ double c_qpyr_gns[5 * 13 * 3], c_qpyr_wgns[13 * 3];
+__constant__ float c_qwed_gns_f[9 * 15 * 3], c_qpyr_gns_f[5 * 13 * 3];
 
 static bool g_const_ready[64] = {false};
 
@@ -98,9 +102,23 @@ static cudaError_t ensure_constants(int device) {
   for (int k = 0; k < 14; k++) shape_grads(B200FEM_ELEM_QUADHEX, k, &qh[k * 60], &wt);
   shape_grads(B200FEM_ELEM_QUADHEX, -1, qhw, &wt);
   for (int i = 0; i < 840; i++) qhf[i] = (float)qh[i];
+  static double qw[405], qww[45], qp[195], qpw[39];
+  static float qwf[405], qpf[195];
+  for (int k = 0; k < 9; k++) shape_grads(B200FEM_ELEM_QUADWEDGE, k, &qw[k * 45], &wt);
+  shape_grads(B200FEM_ELEM_QUADWEDGE, -1, qww, &wt);
+  for (int k = 0; k < 5; k++) shape_grads(B200FEM_ELEM_QUADPYRAMID, k, &qp[k * 39], &wt);
+  shape_grads(B200FEM_ELEM_QUADPYRAMID, -1, qpw, &wt);
+  for (int i = 0; i < 405; i++) qwf[i] = (float)qw[i];
+  for (int i = 0; i < 195; i++) qpf[i] = (float)qp[i];
   for (int i = 0; i < 108; i++) wedf[i] = (float)wed[i];
   for (int i = 0; i < 75; i++) pyrf[i] = (float)pyr[i];
   cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_qwed_gns, qw, sizeof(qw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qwed_wgns, qww, sizeof(qww))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qwed_gns_f, qwf, sizeof(qwf))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qpyr_gns, qp, sizeof(qp))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qpyr_wgns, qpw, sizeof(qpw))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_qpyr_gns_f, qpf, sizeof(qpf))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qhex_gns, qh, sizeof(qh))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qhex_wgns, qhw, sizeof(qhw))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qhex_gns_f, qhf, sizeof(qhf))) != cudaSuccess) return e;
@@ -166,6 +184,12 @@ __device__ __forceinline__ T gns(int k, int n, int c) {
   } else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) {
     if constexpr (sizeof(T) == 8) return c_qhex_gns[(k * 20 + n) * 3 + c];
     else return c_qhex_gns_f[(k * 20 + n) * 3 + c];
+  } else if constexpr (TYPE == B200FEM_ELEM_QUADWEDGE) {
+    if constexpr (sizeof(T) == 8) return c_qwed_gns[(k * 15 + n) * 3 + c];
+    else return c_qwed_gns_f[(k * 15 + n) * 3 + c];
+  } else if constexpr (TYPE == B200FEM_ELEM_QUADPYRAMID) {
+    if constexpr (sizeof(T) == 8) return c_qpyr_gns[(k * 13 + n) * 3 + c];
+    else return c_qpyr_gns_f[(k * 13 + n) * 3 + c];
   } else {
     if constexpr (sizeof(T) == 8) return c_pyr_gns[(k * 5 + n) * 3 + c];
     else return c_pyr_gns_f[(k * 5 + n) * 3 + c];
@@ -182,6 +206,8 @@ __device__ __forceinline__ double wgns(int n, int c) {
   else if constexpr (TYPE == B200FEM_ELEM_WEDGE) return c_wed_wgns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return c_qtet_wgns[3 * n + c];
   else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return c_qhex_wgns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADWEDGE) return c_qwed_wgns[3 * n + c];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADPYRAMID) return c_qpyr_wgns[3 * n + c];
   else return c_pyr_wgns[3 * n + c];
 }
 
@@ -194,6 +220,8 @@ __device__ __forceinline__ T ip_weight(int k) {
   if constexpr (TYPE == B200FEM_ELEM_TET || TYPE == B200FEM_ELEM_WEDGE) return T(1.0 / 6.0);
   else if constexpr (TYPE == B200FEM_ELEM_QUADTET) return T(0.25 / 6.0);
   else if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return k < 8 ? T(0.335180055401662) : T(0.886426592797784);
+  else if constexpr (TYPE == B200FEM_ELEM_QUADWEDGE) return k < 6 ? T(5 / 54.0) : T(8 / 54.0);
+  else if constexpr (TYPE == B200FEM_ELEM_QUADPYRAMID) return k < 4 ? T(81 / 100.0) : T(125 / 27.0);
   else if constexpr (TYPE == B200FEM_ELEM_HEX) return T(1);
   else return k < 4 ? T(81 / 100.0) : T(125 / 27.0);
 }
@@ -213,6 +241,8 @@ static cudaError_t by_elem_type(int type, F&& f) {
     case B200FEM_ELEM_PYRAMID: return f(std::integral_constant<int, B200FEM_ELEM_PYRAMID>{});
     case B200FEM_ELEM_QUADTET: return f(std::integral_constant<int, B200FEM_ELEM_QUADTET>{});
     case B200FEM_ELEM_QUADHEX: return f(std::integral_constant<int, B200FEM_ELEM_QUADHEX>{});
+    case B200FEM_ELEM_QUADWEDGE: return f(std::integral_constant<int, B200FEM_ELEM_QUADWEDGE>{});
+    case B200FEM_ELEM_QUADPYRAMID: return f(std::integral_constant<int, B200FEM_ELEM_QUADPYRAMID>{});
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1306,9 +1336,9 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
   // elements per CTA (one thread per integration point in stage 1): a
   // large and a small tile per material; the small one gives more CTAs
   // per SM and fewer idle threads in the pair stage on small groups
-  // (quadratic hexes: 14 points of 20 gradients each per element)
-  constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : (TYPE == B200FEM_ELEM_QUADHEX ? 8 : 32), NH_S = NH_L / 2;
-  constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : (TYPE == B200FEM_ELEM_QUADHEX ? 8 : 16), MR_S = MR_L / 2;
+  // (elements of more than ten nodes: a point record holds 13-20 gradients)
+  constexpr int NH_L = TYPE == B200FEM_ELEM_TET ? 256 : (elem_nen(TYPE) > 10 ? 8 : 32), NH_S = NH_L / 2;
+  constexpr int MR_L = TYPE == B200FEM_ELEM_TET ? 128 : (elem_nen(TYPE) > 10 ? 8 : 16), MR_S = MR_L / 2;
   // StVenantKirchhoff has the general 6x6 tangent: MooneyRivlin's tiles
   constexpr int NH = B200FEM_MAT_NEOHOOKEAN, MR = B200FEM_MAT_MOONEYRIVLIN, SV = B200FEM_MAT_STVK;
   cudaStream_t st = eng.stream;

@@ -315,11 +315,12 @@ int b200fem_server_add_model(b200fem_server_handle s, int elem_type, int n_nodes
                              int n_elems, const int* conn, const int* fixed, int mat_kind, const double* params,
                              double density, int incomp_method, const double* fext, int* model_id) {
   SRV(s);
-  if (elem_type < B200FEM_ELEM_TET || elem_type > B200FEM_ELEM_QUADHEX || n_nodes <= 0 || n_elems <= 0 ||
+  if (elem_type < B200FEM_ELEM_TET || elem_type > B200FEM_ELEM_QUADPYRAMID || n_nodes <= 0 || n_elems <= 0 ||
       !rest_xyz || !conn || !params || !(density > 0))
     return S.fail(B200FEM_ERR_INVALID_ARG, "invalid model");
   PoolModel m;
-  static const int kNen[6] = {4, 8, 6, 5, 10, 20};  // tet, hex, wedge, pyramid, quadratic tet, quadratic hex
+  // tet, hex, wedge, pyramid and their quadratic forms
+  static const int kNen[8] = {4, 8, 6, 5, 10, 20, 15, 13};
   const int nen = kNen[elem_type];
   m.elem_type = elem_type;
   m.n_nodes = n_nodes;

@@ -132,10 +132,101 @@ void quadhex_grad(double* g, int i, const double* x /* s, t, r */) {
   }
 }
 
+// QuadwedgeElement (QuadwedgeElement.java:129-148, getdNds :301-333) at
+// (s1, s2, r), triangle coordinates L = (s0, s1, s2), layer z = -/+1:
+// corners N = L_t (1 + z r)(2 L_t + z r - 2)/2, triangle mid-edges
+// N = 2 L_a L_b (1 + z r), vertical mid-edges N = L_t (1 - r^2)
+void quadwedge_grad(double* g, int i, double s1, double s2, double r) {
+  const double L[3] = {1 - s1 - s2, s1, s2};
+  auto dL = [](int t, int c) { return t == 0 ? -1.0 : (t == c + 1 ? 1.0 : 0.0); };  // dL_t/ds_c, c = 0, 1
+  static const int tri[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+  if (i < 6) {
+    const int t = i % 3;
+    const double z = i < 3 ? -1.0 : 1.0, hz = 1 + z * r;
+    for (int c = 0; c < 2; c++) g[c] = dL(t, c) * hz * (4 * L[t] + z * r - 2) / 2;
+    g[2] = L[t] * z * (2 * L[t] + 2 * z * r - 1) / 2;
+  } else if (i < 12) {
+    const int a = tri[(i - 6) % 3][0], b = tri[(i - 6) % 3][1];
+    const double z = i < 9 ? -1.0 : 1.0, hz = 1 + z * r;
+    for (int c = 0; c < 2; c++) g[c] = 2 * (dL(a, c) * L[b] + L[a] * dL(b, c)) * hz;
+    g[2] = 2 * L[a] * L[b] * z;
+  } else {
+    const int t = i - 12;
+    for (int c = 0; c < 2; c++) g[c] = dL(t, c) * (1 - r * r);
+    g[2] = -2 * r * L[t];
+  }
+}
+
+// QuadpyramidElement.getdNds (QuadpyramidElement.java:260-319), the
+// reference's per-node expressions with q = (1 - r)/2
+void quadpyramid_grad(double* g, int i, double s, double t, double r) {
+  const double q = (1 - r) / 2;
+  double u;
+  switch (i) {
+    case 0: g[0] = q * (1 - t) * (1 + q * (2 * s + t - 1)) / 4; g[1] = q * (1 - s) * (1 + q * (2 * t + s - 1)) / 4;
+            g[2] = (1 - s) * (1 - t) * (1 + 2 * q * (s + t)) / 8; break;
+    case 1: g[0] = -q * (1 - t) * (1 + q * (-2 * s + t - 1)) / 4; g[1] = q * (1 + s) * (1 + q * (2 * t - s - 1)) / 4;
+            g[2] = (1 + s) * (1 - t) * (1 + 2 * q * (t - s)) / 8; break;
+    case 2: g[0] = -q * (1 + t) * (1 + q * (-2 * s - t - 1)) / 4; g[1] = -q * (1 + s) * (1 + q * (-2 * t - s - 1)) / 4;
+            g[2] = (1 + s) * (1 + t) * (1 - 2 * q * (t + s)) / 8; break;
+    case 3: g[0] = q * (1 + t) * (1 + q * (2 * s - t - 1)) / 4; g[1] = -q * (1 - s) * (1 + q * (-2 * t + s - 1)) / 4;
+            g[2] = (1 - s) * (1 + t) * (1 + 2 * q * (s - t)) / 8; break;
+    case 4: g[0] = 0; g[1] = 0; g[2] = 0.5 + r; break;
+    case 5: g[0] = -s * q * q * (1 - t); g[1] = -q * q * (1 - s * s) / 2; g[2] = -q * (1 - t) * (1 - s * s) / 2; break;
+    case 6: g[0] = q * q * (1 - t * t) / 2; g[1] = -t * q * q * (1 + s); g[2] = -q * (1 + s) * (1 - t * t) / 2; break;
+    case 7: g[0] = -s * q * q * (1 + t); g[1] = q * q * (1 - s * s) / 2; g[2] = -q * (1 + t) * (1 - s * s) / 2; break;
+    case 8: g[0] = -q * q * (1 - t * t) / 2; g[1] = -t * q * q * (1 - s); g[2] = -q * (1 - s) * (1 - t * t) / 2; break;
+    case 9: u = q * (1 - q); g[0] = u * (t - 1); g[1] = u * (s - 1); g[2] = (2 * q - 1) * (1 - s - t + s * t) / 2; break;
+    case 10: u = q * (1 - q); g[0] = u * (1 - t); g[1] = -u * (1 + s); g[2] = (2 * q - 1) * (1 + s - t - s * t) / 2; break;
+    case 11: u = q * (1 - q); g[0] = u * (1 + t); g[1] = u * (1 + s); g[2] = (2 * q - 1) * (1 + s + t + s * t) / 2; break;
+    default: u = q * (1 - q); g[0] = -u * (1 + t); g[1] = u * (1 - s); g[2] = (2 * q - 1) * (1 - s + t - s * t) / 2; break;
+  }
+}
+
 }  // namespace
 
 // Shape gradients for integration point k (or the warping point, k = -1).
 void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
+  if (type == B200FEM_ELEM_QUADWEDGE) {
+    if (k < 0) {
+      // warping point (QuadwedgeElement.getWarpingPoint): the linear wedge's
+      // gradients at (1/3, 1/3, 0) on the corners, zero elsewhere, weight 1
+      std::memset(g, 0, 45 * sizeof(double));
+      for (int i = 0; i < 6; i++) wedge_grad(g + 3 * i, i, 1.0 / 3.0, 1.0 / 3.0, 0);
+      *w = 1;
+      return;
+    }
+    // myIntegrationCoords (:151-170): the wedge's triangle points on the
+    // layers r = -q, +q (weight 5/54) and 0 (weight 8/54), q = sqrt(3/5)
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0, q = std::sqrt(3 / 5.0);
+    const int t = k % 3;
+    const double s1 = t == 1 ? b : a, s2 = t == 2 ? b : a, r = k < 3 ? -q : (k < 6 ? q : 0);
+    *w = k < 6 ? 5 / 54.0 : 8 / 54.0;
+    for (int i = 0; i < 15; i++) quadwedge_grad(g + 3 * i, i, s1, s2, r);
+    return;
+  }
+  if (type == B200FEM_ELEM_QUADPYRAMID) {
+    if (k < 0) {
+      // warping point (QuadpyramidElement.getWarpingPoint): the linear
+      // pyramid's gradients at (0, 0, -1/2) on the corners, weight 1
+      std::memset(g, 0, 39 * sizeof(double));
+      for (int i = 0; i < 5; i++) pyramid_grad(g + 3 * i, i, 0, 0, -0.5);
+      *w = 1;
+      return;
+    }
+    // the pyramid's five points (:151-165)
+    double s0 = 0, s1 = 0, s2 = 2.0 / 5.0;
+    *w = 125 / 27.0;
+    if (k < 4) {
+      const double a = (8 / 5.0) * std::sqrt(2 / 15.0);
+      s0 = kPyrBase[k][0] * a;
+      s1 = kPyrBase[k][1] * a;
+      s2 = -2.0 / 3.0;
+      *w = 81 / 100.0;
+    }
+    for (int i = 0; i < 13; i++) quadpyramid_grad(g + 3 * i, i, s0, s1, s2);
+    return;
+  }
   if (type == B200FEM_ELEM_QUADHEX) {
     if (k < 0) {
       // warping point (QuadhexElement.getWarpingPoint, :37-75): the linear
@@ -277,11 +368,11 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
   if (nx < 1 || ny < 1 || nz < 1) return B200FEM_ERR_INVALID_ARG;
   if (elem_nen(type) == 0) return B200FEM_ERR_INVALID_ARG;
   *nn = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[6] = {5, 1, 2, 3, 5, 1};  // tet, hex, wedge, pyramid, quadtet, quadhex
+  const int per_cell[8] = {5, 1, 2, 3, 5, 1, 2, 3};  // tet, hex, wedge, pyramid and quadratic forms
   *ne = per_cell[type] * nx * ny * nz;
-  if (type == B200FEM_ELEM_QUADTET || type == B200FEM_ELEM_QUADHEX) {
+  if (elem_linear_base(type) >= 0) {
     // the linear grid plus its edge nodes
-    const int lt = type == B200FEM_ELEM_QUADTET ? B200FEM_ELEM_TET : B200FEM_ELEM_HEX;
+    const int lt = elem_linear_base(type);
     std::vector<double> xyz(3 * (size_t)*nn);
     std::vector<int> conn(elem_nen(lt) * (size_t)*ne);
     create_grid(lt, 1, 1, 1, nx, ny, nz, xyz.data(), conn.data());
@@ -301,11 +392,18 @@ int grid_dims(int type, int nx, int ny, int nz, int* nn, int* ne) {
 // 30, 45 56 67 74, 04 15 26 37 (QuadhexElement.getQuadraticNodes :237-260)
 void quadratic_mesh(int lin_type, int nn, const double* xyz, int ne, const int* conn, std::vector<double>& out_xyz,
                     std::vector<int>& out_conn) {
+  // wedges: 01 12 20, 34 45 53, 03 14 25 (QuadwedgeElement.getQuadraticNodes);
+  // pyramids: 01 12 23 30, 04 14 24 34 (QuadpyramidElement.getQuadraticNodes)
   static const int kQhexEdge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
                                        {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-  const bool hex = lin_type == B200FEM_ELEM_HEX;
-  const int nl = hex ? 8 : 4, nedge = hex ? 12 : 6, nq = nl + nedge;
-  const int(*edge)[2] = hex ? kQhexEdge : kQtetEdge;
+  static const int kQwedEdge[9][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 4}, {4, 5}, {5, 3}, {0, 3}, {1, 4}, {2, 5}};
+  static const int kQpyrEdge[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 4}, {2, 4}, {3, 4}};
+  const int nl = elem_nen(lin_type);
+  const int nedge = lin_type == B200FEM_ELEM_HEX ? 12 : lin_type == B200FEM_ELEM_WEDGE ? 9
+                    : lin_type == B200FEM_ELEM_PYRAMID ? 8 : 6;
+  const int nq = nl + nedge;
+  const int(*edge)[2] = lin_type == B200FEM_ELEM_HEX ? kQhexEdge : lin_type == B200FEM_ELEM_WEDGE ? kQwedEdge
+                        : lin_type == B200FEM_ELEM_PYRAMID ? kQpyrEdge : kQtetEdge;
   std::map<std::array<double, 3>, int> at;
   out_xyz.assign(xyz, xyz + 3 * (size_t)nn);
   for (int n = 0; n < nn; n++) at.emplace(std::array<double, 3>{xyz[3 * n], xyz[3 * n + 1], xyz[3 * n + 2]}, n);
@@ -340,11 +438,13 @@ void quadratic_mesh(int lin_type, int nn, const double* xyz, int ne, const int* 
 // (PyramidElement.java:216-270).
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn) {
-  if (type == B200FEM_ELEM_QUADTET || type == B200FEM_ELEM_QUADHEX) {
-    // createQuadtetGrid / createQuadhexGrid (FemFactory.java:316-342): the
-    // linear grid made quadratic
-    const int lt = type == B200FEM_ELEM_QUADTET ? B200FEM_ELEM_TET : B200FEM_ELEM_HEX;
-    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = (lt == B200FEM_ELEM_TET ? 5 : 1) * nx * ny * nz;
+  if (elem_linear_base(type) >= 0) {
+    // createQuadtetGrid / createQuadhexGrid / createQuadwedgeGrid /
+    // createQuadpyramidGrid (FemFactory.java:316-376): the linear grid made
+    // quadratic
+    const int lt = elem_linear_base(type);
+    int nl, ne;
+    grid_dims(lt, nx, ny, nz, &nl, &ne);
     std::vector<double> lx(3 * (size_t)nl);
     std::vector<int> lc(elem_nen(lt) * (size_t)ne);
     create_grid(lt, wx, wy, wz, nx, ny, nz, lx.data(), lc.data());
@@ -452,13 +552,15 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
   // NODAL needs tets or elements whose points map to nodes
   // (softNodalIncompressAllowed, FemModel3d.java:400-405, 467-471)
-  else if (m.elem_type == B200FEM_ELEM_QUADTET &&
+  else if ((m.elem_type == B200FEM_ELEM_QUADTET || m.elem_type == B200FEM_ELEM_QUADPYRAMID) &&
            (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
     method = B200FEM_INCOMP_ELEMENT;
-  else if (m.elem_type == B200FEM_ELEM_QUADHEX && method != B200FEM_INCOMP_OFF) {
-    // QuadhexElement.numPressureVals() == 4 (:443-445): ELEMENT with a 4x4
-    // Rinv per element is not built
-    err = "soft incompressibility of quadratic hexes (four pressure values per element) is not supported";
+  else if ((m.elem_type == B200FEM_ELEM_QUADHEX || m.elem_type == B200FEM_ELEM_QUADWEDGE) &&
+           method != B200FEM_INCOMP_OFF) {
+    // QuadhexElement.numPressureVals() == 4 (:443-445), QuadwedgeElement's 2
+    // (:267-269): ELEMENT with an npvals x npvals Rinv per element is not built
+    err = "soft incompressibility of quadratic hexes and wedges (several pressure values per element) is not "
+          "supported";
     return B200FEM_ERR_UNSUPPORTED;
   }
   else if (method == B200FEM_INCOMP_AUTO)

@@ -150,6 +150,18 @@ class FemFactory:
         return m
 
     @staticmethod
+    def createQuadwedgeGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_QUADWEDGE, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
+    def createQuadpyramidGrid(model, wx, wy, wz, nx, ny, nz):
+        m = model if model is not None else FemModel3d()
+        m._set_grid(L.ELEM_QUADPYRAMID, wx, wy, wz, nx, ny, nz)
+        return m
+
+    @staticmethod
     def createQuadhexGrid(model, wx, wy, wz, nx, ny, nz):
         m = model if model is not None else FemModel3d()
         m._set_grid(L.ELEM_QUADHEX, wx, wy, wz, nx, ny, nz)

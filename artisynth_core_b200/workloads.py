@@ -167,6 +167,20 @@ def small_quadhex_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter
                     gravity, h, steps, tol=1e-13)
 
 
+def small_quadwedge_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.03, seed=29,
+                         gravity=(0.0, 0.0, -9.81), h=0.005, steps=10) -> Workload:
+    """Small beam of quadratic wedges (FemFactory.createQuadwedgeGrid)."""
+    return Workload("small_quadwedge_beam", L.ELEM_QUADWEDGE, cells, widths, jitter, seed, material, 1000.0, "xmin",
+                    gravity, h, steps, tol=1e-13)
+
+
+def small_quadpyramid_beam(material, cells=(4, 2, 2), widths=(1.0, 0.4, 0.4), jitter=0.03, seed=31,
+                           gravity=(0.0, 0.0, -9.81), h=0.005, steps=10) -> Workload:
+    """Small beam of quadratic pyramids (FemFactory.createQuadpyramidGrid)."""
+    return Workload("small_quadpyramid_beam", L.ELEM_QUADPYRAMID, cells, widths, jitter, seed, material, 1000.0,
+                    "xmin", gravity, h, steps, tol=1e-13)
+
+
 def batched_beams(count=256, seed=3, cell=0.05, jitter=0.05, large_frac=0.0, large_n=(80, 120)):
     """Uneven NeoHookean tet beams: n x m x m cells of size `cell` (5 tets per
     cell), n ~ U{4..60}, m ~ U{2..8}, E log-uniform in [1e3, 1e6] Pa, nu

@@ -61,6 +61,10 @@ extern "C" {
                                   edges 01 12 23 30, 45 56 67 74, 04 15 26 37), 14 points;
                                   compressible materials (its soft incompressibility has four
                                   pressure values per element: B200FEM_ERR_UNSUPPORTED) */
+#define B200FEM_ELEM_QUADWEDGE 6   /* QuadwedgeElement, 15 nodes (edges 01 12 20, 34 45 53, 03 14
+                                      25), 9 points; compressible (two pressure values) */
+#define B200FEM_ELEM_QUADPYRAMID 7 /* QuadpyramidElement, 13 nodes (edges 01 12 23 30, 04 14 24
+                                      34), 5 points; soft incompressibility resolves to ELEMENT */
 
 /* materials (parameter layout of b200fem_set_material) */
 #define B200FEM_MAT_LINEAR 0       /* {E, nu, corotated(0/1)}: LinearMaterial */

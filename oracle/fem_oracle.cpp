@@ -26,7 +26,8 @@
 
 namespace {
 
-enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3, ELEM_QUADTET = 4, ELEM_QUADHEX = 5 };
+enum { ELEM_TET = 0, ELEM_HEX = 1, ELEM_WEDGE = 2, ELEM_PYRAMID = 3, ELEM_QUADTET = 4, ELEM_QUADHEX = 5,
+       ELEM_QUADWEDGE = 6, ELEM_QUADPYRAMID = 7 };
 enum { MAT_LINEAR = 0, MAT_NEOHOOKEAN = 1, MAT_MOONEYRIVLIN = 2, MAT_STVK = 3 };
 enum { INCOMP_OFF = 0, INCOMP_NODAL = 1, INCOMP_AUTO = 2, INCOMP_ELEMENT = 3 };
 
@@ -238,6 +239,48 @@ static void quadhex_dNds(double* out, int i, double s, double t, double r) {
   out[2] = c * 0.125;
 }
 
+// QuadwedgeElement.getdNds (QuadwedgeElement.java:301-333), case by case
+static void quadwedge_dNds(double* o, int i, double s1, double s2, double r) {
+  const double s0 = 1 - s1 - s2;
+  const double v[15][3] = {
+      {(1 - r) * (4 * s1 + 4 * s2 + r - 2) / 2, (1 - r) * (4 * s1 + 4 * s2 + r - 2) / 2, s0 * (2 * s1 + 2 * s2 + 2 * r - 1) / 2},
+      {(1 - r) * (4 * s1 - r - 2) / 2, 0, -s1 * (2 * s1 - 2 * r - 1) / 2},
+      {0, (1 - r) * (4 * s2 - r - 2) / 2, -s2 * (2 * s2 - 2 * r - 1) / 2},
+      {(1 + r) * (4 * s1 + 4 * s2 - r - 2) / 2, (1 + r) * (4 * s1 + 4 * s2 - r - 2) / 2, s0 * (1 - 2 * s1 - 2 * s2 + 2 * r) / 2},
+      {(1 + r) * (4 * s1 + r - 2) / 2, 0, s1 * (2 * s1 + 2 * r - 1) / 2},
+      {0, (1 + r) * (4 * s2 + r - 2) / 2, s2 * (2 * s2 + 2 * r - 1) / 2},
+      {2 * (s0 - s1) * (1 - r), -2 * s1 * (1 - r), -2 * s1 * s0},
+      {2 * s2 * (1 - r), 2 * s1 * (1 - r), -2 * s1 * s2},
+      {-2 * s2 * (1 - r), 2 * (s0 - s2) * (1 - r), -2 * s2 * s0},
+      {2 * (s0 - s1) * (1 + r), -2 * s1 * (1 + r), 2 * s1 * s0},
+      {2 * s2 * (1 + r), 2 * s1 * (1 + r), 2 * s1 * s2},
+      {-2 * s2 * (1 + r), 2 * (s0 - s2) * (1 + r), 2 * s2 * s0},
+      {r * r - 1, r * r - 1, -2 * r * s0},
+      {1 - r * r, 0, -2 * r * s1},
+      {0, 1 - r * r, -2 * r * s2}};
+  for (int c = 0; c < 3; c++) o[c] = v[i][c];
+}
+
+// QuadpyramidElement.getdNds (QuadpyramidElement.java:260-319), q = (1 - r)/2
+static void quadpyramid_dNds(double* o, int i, double s, double t, double r) {
+  const double q = (1 - r) / 2, u = q * (1 - q);
+  const double v[13][3] = {
+      {q * (1 - t) * (1 + q * (2 * s + t - 1)) / 4, q * (1 - s) * (1 + q * (2 * t + s - 1)) / 4, (1 - s) * (1 - t) * (1 + 2 * q * (s + t)) / 8},
+      {-q * (1 - t) * (1 + q * (-2 * s + t - 1)) / 4, q * (1 + s) * (1 + q * (2 * t - s - 1)) / 4, (1 + s) * (1 - t) * (1 + 2 * q * (t - s)) / 8},
+      {-q * (1 + t) * (1 + q * (-2 * s - t - 1)) / 4, -q * (1 + s) * (1 + q * (-2 * t - s - 1)) / 4, (1 + s) * (1 + t) * (1 - 2 * q * (t + s)) / 8},
+      {q * (1 + t) * (1 + q * (2 * s - t - 1)) / 4, -q * (1 - s) * (1 + q * (-2 * t + s - 1)) / 4, (1 - s) * (1 + t) * (1 + 2 * q * (s - t)) / 8},
+      {0, 0, 0.5 + r},
+      {-s * q * q * (1 - t), -q * q * (1 - s * s) / 2, -q * (1 - t) * (1 - s * s) / 2},
+      {q * q * (1 - t * t) / 2, -t * q * q * (1 + s), -q * (1 + s) * (1 - t * t) / 2},
+      {-s * q * q * (1 + t), q * q * (1 - s * s) / 2, -q * (1 + t) * (1 - s * s) / 2},
+      {-q * q * (1 - t * t) / 2, -t * q * q * (1 - s), -q * (1 - s) * (1 - t * t) / 2},
+      {u * (t - 1), u * (s - 1), (2 * q - 1) * (1 - s - t + s * t) / 2},
+      {u * (1 - t), -u * (1 + s), (2 * q - 1) * (1 + s - t - s * t) / 2},
+      {u * (1 + t), u * (1 + s), (2 * q - 1) * (1 + s + t + s * t) / 2},
+      {-u * (1 + t), u * (1 - s), (2 * q - 1) * (1 - s + t - s * t) / 2}};
+  for (int c = 0; c < 3; c++) o[c] = v[i][c];
+}
+
 struct ShapeTable {
   int nen, nip;
   std::vector<double> GNs;  // nip * nen * 3
@@ -254,6 +297,33 @@ static ShapeTable make_shape(int type) {
     s.w = {TET_W};
     s.wGNs = s.GNs;  // TetElement.getWarpingPoint == integration point 0
     s.ww = TET_W;
+  } else if (type == ELEM_QUADWEDGE) {
+    s.nen = 15; s.nip = 9;
+    // myIntegrationCoords (QuadwedgeElement.java:151-170)
+    const double a = 1.0 / 6.0, b = 2.0 / 3.0, q = std::sqrt(3 / 5.0), w1 = 5 / 54.0, w2 = 8 / 54.0;
+    const double ip[9][3] = {{a, a, -q}, {b, a, -q}, {a, b, -q}, {a, a, q}, {b, a, q},
+                             {a, b, q},  {a, a, 0},  {b, a, 0},  {a, b, 0}};
+    s.GNs.resize(9 * 15 * 3);
+    s.w = {w1, w1, w1, w1, w1, w1, w2, w2, w2};
+    for (int k = 0; k < 9; k++)
+      for (int i = 0; i < 15; i++) quadwedge_dNds(&s.GNs[(k * 15 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // warping point: the linear wedge at (1/3, 1/3, 0) on the corners
+    s.wGNs.assign(45, 0.0);
+    for (int i = 0; i < 6; i++) wedge_dNds(&s.wGNs[i * 3], i, 1 / 3.0, 1 / 3.0, 0);
+    s.ww = 1;
+  } else if (type == ELEM_QUADPYRAMID) {
+    s.nen = 13; s.nip = 5;
+    // the pyramid's five points (QuadpyramidElement.java:151-165)
+    const double a = (8 / 5.0) * std::sqrt(2 / 15.0), b = -2.0 / 3.0, c = 2.0 / 5.0;
+    const double ip[5][3] = {{-a, -a, b}, {a, -a, b}, {a, a, b}, {-a, a, b}, {0, 0, c}};
+    s.GNs.resize(5 * 13 * 3);
+    s.w = {81 / 100.0, 81 / 100.0, 81 / 100.0, 81 / 100.0, 125 / 27.0};
+    for (int k = 0; k < 5; k++)
+      for (int i = 0; i < 13; i++) quadpyramid_dNds(&s.GNs[(k * 13 + i) * 3], i, ip[k][0], ip[k][1], ip[k][2]);
+    // warping point: the linear pyramid at (0, 0, -1/2) on the corners
+    s.wGNs.assign(39, 0.0);
+    for (int i = 0; i < 5; i++) pyramid_dNds(&s.wGNs[i * 3], i, 0, 0, -0.5);
+    s.ww = 1;
   } else if (type == ELEM_QUADHEX) {
     s.nen = 20; s.nip = 14;
     // myIntegrationCoords14 (QuadhexElement.java:159-182)
@@ -1266,15 +1336,19 @@ void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, 
 // QuadtetElement.getQuadraticNodes (:130-175) are compared with every node so
 // far (exact position equality) and appended when new.  *nout = node count;
 // oxyz / oconn may be null.
-static void quadratic_model(int hex, int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
+static void quadratic_model(int lin, int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
                             int* oconn) {
   std::vector<double> P(xyz, xyz + 3 * (size_t)nn);
-  const int nl = hex ? 8 : 4, nedge = hex ? 12 : 6, nq = nl + nedge;
-  std::vector<int> Q(nq * (size_t)ne);
-  // QuadtetElement.getQuadraticNodes (:130-175), QuadhexElement's (:237-260)
+  // getQuadraticNodes of QuadtetElement (:130-175), QuadhexElement
+  // (:237-260), QuadwedgeElement (:343-360), QuadpyramidElement (:336-350)
   const int tedges[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
   const int hedges[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-  const int(*edges)[2] = hex ? hedges : tedges;
+  const int wedges[9][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 4}, {4, 5}, {5, 3}, {0, 3}, {1, 4}, {2, 5}};
+  const int pedges[8][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 4}, {2, 4}, {3, 4}};
+  const int nls[4] = {4, 8, 6, 5}, nes[4] = {6, 12, 9, 8};
+  const int nl = nls[lin], nedge = nes[lin], nq = nl + nedge;
+  const int(*edges)[2] = lin == ELEM_HEX ? hedges : lin == ELEM_WEDGE ? wedges : lin == ELEM_PYRAMID ? pedges : tedges;
+  std::vector<int> Q(nq * (size_t)ne);
   for (int e = 0; e < ne; e++) {
     const int* c = conn + nl * (size_t)e;
     for (int a = 0; a < nl; a++) Q[nq * (size_t)e + a] = c[a];
@@ -1301,24 +1375,25 @@ static void quadratic_model(int hex, int nn, const double* xyz, int ne, const in
 
 void orc_quadratic_tets(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
                         int* oconn) {
-  quadratic_model(0, nn, xyz, ne, conn, nout, oxyz, oconn);
+  quadratic_model(ELEM_TET, nn, xyz, ne, conn, nout, oxyz, oconn);
 }
 
 void orc_quadratic_hexes(int nn, const double* xyz, int ne, const int* conn, int* nout, double* oxyz,
                          int* oconn) {
-  quadratic_model(1, nn, xyz, ne, conn, nout, oxyz, oconn);
+  quadratic_model(ELEM_HEX, nn, xyz, ne, conn, nout, oxyz, oconn);
 }
 
 void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
   *nnodes = (nx + 1) * (ny + 1) * (nz + 1);
-  const int per_cell[6] = {5, 1, 2, 3, 5, 1};
+  const int per_cell[8] = {5, 1, 2, 3, 5, 1, 2, 3};
   *nelems = per_cell[type] * nx * ny * nz;
-  if (type == ELEM_QUADTET || type == ELEM_QUADHEX) {
-    const int hex = type == ELEM_QUADHEX;
+  if (type >= ELEM_QUADTET) {
+    const int lin = type - ELEM_QUADTET;  // tet, hex, wedge, pyramid
+    const int nls[4] = {4, 8, 6, 5};
     std::vector<double> x(3 * (size_t)*nnodes);
-    std::vector<int> c((hex ? 8 : 4) * (size_t)*nelems);
-    orc_create_grid(hex ? ELEM_HEX : ELEM_TET, 1, 1, 1, nx, ny, nz, x.data(), c.data());
-    quadratic_model(hex, *nnodes, x.data(), *nelems, c.data(), nnodes, nullptr, nullptr);
+    std::vector<int> c(nls[lin] * (size_t)*nelems);
+    orc_create_grid(lin, 1, 1, 1, nx, ny, nz, x.data(), c.data());
+    quadratic_model(lin, *nnodes, x.data(), *nelems, c.data(), nnodes, nullptr, nullptr);
   }
 }
 
@@ -1327,15 +1402,17 @@ void orc_grid_dims(int type, int nx, int ny, int nz, int* nnodes, int* nelems) {
 // parseCode :203-263, getTetIndicesForHex :265-300), createHexGrid (:203-255).
 void orc_create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz,
                      double* xyz, int* conn) {
-  if (type == ELEM_QUADTET || type == ELEM_QUADHEX) {
-    // createQuadtetGrid / createQuadhexGrid (FemFactory.java:316-342)
-    const int hex = type == ELEM_QUADHEX;
-    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = (hex ? 1 : 5) * nx * ny * nz;
+  if (type >= ELEM_QUADTET) {
+    // createQuadtetGrid / createQuadhexGrid / createQuadwedgeGrid /
+    // createQuadpyramidGrid (FemFactory.java:316-376)
+    const int lin = type - ELEM_QUADTET;
+    const int nls[4] = {4, 8, 6, 5}, per[4] = {5, 1, 2, 3};
+    const int nl = (nx + 1) * (ny + 1) * (nz + 1), ne = per[lin] * nx * ny * nz;
     std::vector<double> x(3 * (size_t)nl);
-    std::vector<int> c((hex ? 8 : 4) * (size_t)ne);
-    orc_create_grid(hex ? ELEM_HEX : ELEM_TET, wx, wy, wz, nx, ny, nz, x.data(), c.data());
+    std::vector<int> c(nls[lin] * (size_t)ne);
+    orc_create_grid(lin, wx, wy, wz, nx, ny, nz, x.data(), c.data());
     int nout;
-    quadratic_model(hex, nl, x.data(), ne, c.data(), &nout, xyz, conn);
+    quadratic_model(lin, nl, x.data(), ne, c.data(), &nout, xyz, conn);
     return;
   }
   double dx = 1.0 / nx, dy = 1.0 / ny, dz = 1.0 / nz;
@@ -1452,10 +1529,12 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   if (!m->mat.incompressible()) method = INCOMP_OFF;
   // NODAL only for tets and elements whose points map to nodes
   // (softNodalIncompressAllowed, :400-405): quadratic tets take ELEMENT
-  else if (type == ELEM_QUADTET && (method == INCOMP_NODAL || method == INCOMP_AUTO)) method = INCOMP_ELEMENT;
+  else if ((type == ELEM_QUADTET || type == ELEM_QUADPYRAMID) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
+    method = INCOMP_ELEMENT;
   // QuadhexElement has four pressure values per element (:443-445): the
   // restatement covers one, so its incompressible forms are refused
-  else if (type == ELEM_QUADHEX && method != INCOMP_OFF) {
+  // (QuadwedgeElement: two, :267-269)
+  else if ((type == ELEM_QUADHEX || type == ELEM_QUADWEDGE) && method != INCOMP_OFF) {
     delete m;
     return nullptr;
   }

@@ -82,20 +82,21 @@ def test_pack_of_mixed_materials(b200, oracle):
         assert rel_err(xg, x) <= 1e-8
 
 
-@pytest.mark.parametrize("beam", ["wedge", "pyramid", "quadtet", "quadhex"])
+@pytest.mark.parametrize("beam", ["wedge", "pyramid", "quadtet", "quadhex", "quadwedge", "quadpyramid"])
 def test_pack_of_wedges_or_pyramids(b200, oracle, beam):
     """A pack of one of the multi-point element types: uneven beams with
     different materials (element groups), every model against its oracle run."""
     from artisynth_core_b200.femmodel import (MooneyRivlinMaterial, NeoHookeanMaterial, LinearMaterial,
                                               StVenantKirchoffMaterial)
     mk = {"wedge": W.small_wedge_beam, "pyramid": W.small_pyramid_beam, "quadtet": W.small_quadtet_beam,
-          "quadhex": W.small_quadhex_beam}[beam]
+          "quadhex": W.small_quadhex_beam, "quadwedge": W.small_quadwedge_beam,
+          "quadpyramid": W.small_quadpyramid_beam}[beam]
     wls = [mk(NeoHookeanMaterial(3e4, 0.4)), mk(LinearMaterial(2e4, 0.3, True), cells=(6, 2, 2)),
            mk(MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370), cells=(3, 3, 2)),
            mk(StVenantKirchoffMaterial(4e4, 0.3), cells=(5, 2, 3))]
     for w in wls:
         w.build_mesh()
-        if beam == "quadhex":  # quadratic hexes: compressible forms only
+        if beam in ("quadhex", "quadwedge"):  # several pressure values: compressible forms only
             w.incomp = L.INCOMP_OFF
     models = []
     for w in wls:

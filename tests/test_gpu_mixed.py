@@ -34,6 +34,8 @@ def _cases():
         "neohookean_quadtet": W.small_quadtet_beam(NeoHookeanMaterial(5e4, 0.45)),
         "mooneyrivlin_quadtet_auto": W.small_quadtet_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
         "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "neohookean_quadwedge": W.small_quadwedge_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "mooneyrivlin_quadpyramid_auto": W.small_quadpyramid_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 

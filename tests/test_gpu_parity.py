@@ -64,6 +64,13 @@ def _cases():
         "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
         "stvk_quadhex": W.small_quadhex_beam(StVenantKirchoffMaterial(5e4, 0.3)),
         "mooneyrivlin_quadhex_off": W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        # quadratic wedges (15 nodes, 9 points) and pyramids (13 nodes, 5 points)
+        "linear_corotated_quadwedge": W.small_quadwedge_beam(LinearMaterial(2e4, 0.3, True)),
+        "neohookean_quadwedge": W.small_quadwedge_beam(NeoHookeanMaterial(5e4, 0.45)),
+        "linear_corotated_quadpyramid": W.small_quadpyramid_beam(LinearMaterial(2e4, 0.3, True)),
+        "stvk_quadpyramid": W.small_quadpyramid_beam(StVenantKirchoffMaterial(5e4, 0.3)),
+        "mooneyrivlin_quadpyramid_element": W.small_quadpyramid_beam(
+            MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 
@@ -179,7 +186,9 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
                                   "mooneyrivlin_pyramid_element_log", "linear_corotated_quadtet",
                                   "neohookean_quadtet", "stvk_quadtet", "mooneyrivlin_quadtet_element",
                                   "linear_corotated_quadhex", "neohookean_quadhex", "stvk_quadhex",
-                                  "mooneyrivlin_quadhex_off"])
+                                  "mooneyrivlin_quadhex_off", "linear_corotated_quadwedge",
+                                  "neohookean_quadwedge", "linear_corotated_quadpyramid", "stvk_quadpyramid",
+                                  "mooneyrivlin_quadpyramid_element"])
 def test_backward_euler_small(name, cases, oracle):
     wl = cases[name]
     xg, vg, x, v, ms = _run_pair(wl, oracle, wl.steps, 1, 1e-13)

@@ -156,7 +156,10 @@ def test_polar_rotation(oracle):
     # quadratic tets (QuadtetElement; soft incompressibility resolves to ELEMENT)
     (1, [5e4, 0.45], 4, 0), (3, [5e4, 0.3], 4, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 4, 3),
     # quadratic hexes (QuadhexElement, 14 points; compressible forms)
-    (1, [5e4, 0.45], 5, 0), (3, [5e4, 0.3], 5, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 5, 0)])
+    (1, [5e4, 0.45], 5, 0), (3, [5e4, 0.3], 5, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 5, 0),
+    # quadratic wedges (compressible forms) and pyramids (ELEMENT)
+    (1, [5e4, 0.45], 6, 0), (3, [5e4, 0.3], 6, 0), (1, [5e4, 0.45], 7, 0), (3, [5e4, 0.3], 7, 0),
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 7, 3)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
@@ -284,7 +287,7 @@ def test_constrained_step_holds_nodes_on_their_planes(oracle):
     assert np.abs(x - xyz).max() > 1e-6
 
 
-@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3), (4, 5), (5, 1)])
+@pytest.mark.parametrize("etype,per_cell", [(0, 5), (1, 1), (2, 2), (3, 3), (4, 5), (5, 1), (6, 2), (7, 3)])
 def test_grid_volumes_and_masses(oracle, etype, per_cell):
     # createTetGrid / createHexGrid / createWedgeGrid / createPyramidGrid:
     # every element positively oriented, rest volumes (sum of detJ0 w over
@@ -301,7 +304,7 @@ def test_grid_volumes_and_masses(oracle, etype, per_cell):
     assert abs(m.masses().sum() - 150.0) <= 1e-11
 
 
-@pytest.mark.parametrize("etype", [2, 3, 4, 5])
+@pytest.mark.parametrize("etype", [2, 3, 4, 5, 6, 7])
 def test_library_grid_matches_oracle(oracle, etype):
     # the library's host-side mesh factory (no GPU needed) against the oracle's
     from artisynth_core_b200 import femmodel as FM
