@@ -311,7 +311,8 @@ __device__ bool block_inactive(const ElemArgs& a, int ebase, int epb) {
 }
 
 // ---------------------------------------------------------------------------
-// non-linear materials (NeoHookean, MooneyRivlin), tet or hex
+// non-linear materials (NeoHookean, MooneyRivlin, StVenantKirchhoff), every
+// element type
 // ---------------------------------------------------------------------------
 // Shared-memory layout of the non-linear element kernel (one record per
 // integration point: shape gradients, dv, stress, tangent).

@@ -209,7 +209,8 @@ class FemEngine:
 
 # -------------------------------------------------------------------- model
 class FemModel3d:
-    """FemModel3d restricted to the hot path: one element type (tet or hex),
+    """FemModel3d restricted to the hot path: one element type (tet, hex,
+    wedge or pyramid, linear or quadratic),
     one material, lumped mass, fixed nodes and the BackwardEuler data."""
 
     def __init__(self):
