@@ -36,6 +36,8 @@ PART_FULL, PART_UPPER = 0, 1
 PCG_AUTO, PCG_CLASSIC, PCG_PIPELINED = 0, 1, 2
 OPT_PCG_SPLIT, OPT_ROW_LANES, OPT_PCG_CTAS, OPT_PIECE_ROWS, OPT_WARM_START, OPT_ELEM_TILE, OPT_FUSED_ASSEMBLY = 1, 2, 3, 4, 5, 6, 7
 OPT_REFINE = 8
+OPT_BARRIER_TIMEOUT_MS, OPT_TEST_SKIP_ARRIVAL = 9, 10
+OPT_TET_ASSEMBLY = 11
 INTEGRATOR_BACKWARD_EULER, INTEGRATOR_CONSTRAINED_BACKWARD_EULER = 0, 1
 SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED = 0, 1, 2
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -253,6 +254,93 @@ int build_pack(Engine& eng) {
       }
     }
     eng.groups.push_back(g);
+  }
+  // ---- node-row tet assembly: tasks of consecutive block rows of one model
+  // whose node incidences fit rows_cap lanes, the rows' incidences (element
+  // order, the element's first active node records its statistics), and
+  // per contribution the stage entry (incidence in task * 4 + column node)
+  eng.tet_rows = false;
+  eng.rows_task_off.clear();
+  std::vector<int> task_row, row_incptr, row_inc;
+  std::vector<unsigned char> cbyte;
+  if (eng.opt_tet_assembly == 0 && eng.elem_type == B200FEM_ELEM_TET && eng.opt_fused == 0 && R > 0) {
+    bool ok = true;
+    for (const ElemGroup& g : eng.groups) ok &= g.mat_kind != B200FEM_MAT_LINEAR;
+    std::vector<int> first_active(E, -1);
+    for (int e = 0; ok && e < E; e++) {
+      for (int a = 0; a < nen && first_active[e] < 0; a++)
+        if (sidx[conn[(size_t)e * nen + a]] >= 0) first_active[e] = a;
+      ok &= first_active[e] >= 0;  // an element without an active node keeps the element path
+    }
+    int maxinc = 0;
+    for (int r = 0; ok && r < R; r++) maxinc = std::max(maxinc, iptr[act_node[r] + 1] - iptr[act_node[r]]);
+    ok &= maxinc <= 64;
+    if (ok) {
+      const int cap = maxinc <= 32 ? 32 : 64;
+      row_incptr.assign(R + 1, 0);
+      for (int r = 0; r < R; r++) row_incptr[r + 1] = row_incptr[r] + iptr[act_node[r] + 1] - iptr[act_node[r]];
+      row_inc.resize(row_incptr[R]);
+      for (int r = 0, k = 0; r < R; r++) {
+        const int n = act_node[r];
+        for (int i = iptr[n]; i < iptr[n + 1]; i++) {
+          const int e = iidx[i] / nen, a = iidx[i] % nen;
+          row_inc[k++] = (e << 3) | (a << 1) | (first_active[e] == a ? 1 : 0);
+        }
+      }
+      std::vector<int> task_of_row(R), model_task(M + 1, 0);
+      for (int m = 0; m < M; m++) {
+        model_task[m] = (int)task_row.size();
+        int r = eng.row_off[m];
+        while (r < eng.row_off[m + 1]) {
+          const int t = (int)task_row.size();
+          task_row.push_back(r);
+          int cnt = 0;
+          while (r < eng.row_off[m + 1] && cnt + (row_incptr[r + 1] - row_incptr[r]) <= cap) {
+            cnt += row_incptr[r + 1] - row_incptr[r];
+            task_of_row[r++] = t;
+          }
+        }
+      }
+      model_task[M] = (int)task_row.size();
+      task_row.push_back(R);
+      for (const ElemGroup& g : eng.groups) {
+        const int m0 = (int)(std::lower_bound(eng.elem_off.begin(), eng.elem_off.end(), g.e0) - eng.elem_off.begin());
+        const int m1 = (int)(std::lower_bound(eng.elem_off.begin(), eng.elem_off.end(), g.e1) - eng.elem_off.begin());
+        if (eng.rows_task_off.empty()) eng.rows_task_off.push_back(model_task[m0]);
+        eng.rows_task_off.push_back(model_task[m1]);
+      }
+      std::vector<int> pa, pb;
+      for (int x0 = 0; x0 < nen; x0++)
+        for (int x1 = x0; x1 < nen; x1++) {
+          pa.push_back(x0);
+          pb.push_back(x1);
+        }
+      cbyte.resize(cptr[NB]);
+      for (long long p = 0; p < NB; p++) {
+        const int r = blk_row[p];
+        const int rowpos = row_incptr[r] - row_incptr[task_row[task_of_row[r]]];
+        const int* rb = row_inc.data() + row_incptr[r];
+        const int rn = row_incptr[r + 1] - row_incptr[r];
+        for (int c = cptr[p]; c < cptr[p + 1]; c++) {
+          const int code = cidx[c];
+          const int e = (code >> 1) / npair, w = (code >> 1) % npair;
+          const int am = (code & 1) ? pb[w] : pa[w], bl = (code & 1) ? pa[w] : pb[w];
+          int lo = 0, hi = rn;
+          while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if ((rb[mid] >> 3) < e) lo = mid + 1;
+            else hi = mid;
+          }
+          if (lo >= rn || (rb[lo] >> 3) != e || ((rb[lo] >> 1) & 3) != am)
+            return fail(&eng, B200FEM_ERR_STATE, "internal: contribution without its row incidence");
+          const int q = rowpos + lo;
+          if (q >= cap) return fail(&eng, B200FEM_ERR_STATE, "internal: task incidence beyond its capacity");
+          cbyte[c] = (unsigned char)(q * 4 + bl);
+        }
+      }
+      eng.tet_rows = true;
+      eng.rows_cap = cap;
+    }
   }
   // ---- fused assembly: block-row chunks whose incident elements fit the
   // chunk's shared memory, and the contribution lists re-indexed to them
@@ -559,6 +647,12 @@ int build_pack(Engine& eng) {
   }
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));
+  if (eng.tet_rows) {
+    CK(upload(eng, &d.task_row, task_row));
+    CK(upload(eng, &d.row_incptr, row_incptr));
+    CK(upload(eng, &d.row_inc, row_inc));
+    CK(upload(eng, &d.contrib_byte, cbyte));
+  }
   if (eng.fused) {
     CK(upload(eng, &d.chunk_row, chunk_row));
     CK(upload(eng, &d.chunk_eptr, chunk_eptr));
@@ -663,6 +757,16 @@ int build_pack(Engine& eng) {
 }  // namespace b200fem
 
 using namespace b200fem;
+
+namespace {
+// true when every value is finite: a NaN or an infinity in a caller's array
+// is refused with B200FEM_ERR_INVALID_ARG before it reaches the device
+bool all_finite(const double* a, size_t n) {
+  bool ok = true;
+  for (size_t i = 0; i < n; i++) ok &= std::fabs(a[i]) <= DBL_MAX;
+  return ok;
+}
+}  // namespace
 
 struct b200fem_engine {
   Engine eng;
@@ -796,6 +900,8 @@ int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double*
   if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
   int nen = elem_nen(elem_type);
+  if (!all_finite(rest_xyz, 3 * (size_t)n_nodes))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite rest position");
   ModelDesc& m = eng.models[0];
   m.elem_type = elem_type;
   m.n_nodes = n_nodes;
@@ -812,10 +918,11 @@ int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, d
   ENG(h);
   if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_STVK || !params)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
-  if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
+  if (!(density > 0) || !(density <= DBL_MAX)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
   ModelDesc& m = eng.models[0];
-  m.mat_kind = mat_kind;
   int np = mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_MOONEYRIVLIN ? 8 : 2;
+  if (!all_finite(params, np)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite material parameter");
+  m.mat_kind = mat_kind;
   std::fill(m.mat_params, m.mat_params + kMatParams, 0.0);
   std::copy(params, params + np, m.mat_params);
   m.density = density;
@@ -833,7 +940,11 @@ int b200fem_add_model(b200fem_handle h, int elem_type, int n_nodes, const double
   if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn) return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
   if (mat_kind < B200FEM_MAT_LINEAR || mat_kind > B200FEM_MAT_STVK || !params)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown material");
-  if (!(density > 0)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
+  if (!(density > 0) || !(density <= DBL_MAX)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "density must be positive");
+  if (!all_finite(rest_xyz, 3 * (size_t)n_nodes))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite rest position");
+  if (!all_finite(params, mat_kind == B200FEM_MAT_LINEAR ? 3 : mat_kind == B200FEM_MAT_MOONEYRIVLIN ? 8 : 2))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite material parameter");
   ModelDesc m;
   const int nen = elem_nen(elem_type);
   m.elem_type = elem_type;
@@ -977,6 +1088,25 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
         eng.step_exec_max_iter = -1;  // recapture: the width is a kernel argument
       }
       return B200FEM_OK;
+    case B200FEM_OPT_TET_ASSEMBLY:
+      if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "TET_ASSEMBLY must be 0 or 1");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "TET_ASSEMBLY is set before b200fem_build");
+      eng.opt_tet_assembly = value;
+      return B200FEM_OK;
+    case B200FEM_OPT_BARRIER_TIMEOUT_MS:
+      if (value < 1 || value > 60000) return fail(&eng, B200FEM_ERR_INVALID_ARG, "BARRIER_TIMEOUT_MS must be 1..60000");
+      if (value != eng.barrier_timeout_ms) {
+        eng.barrier_timeout_ms = value;
+        eng.step_exec_max_iter = -1;  // recapture: the bound is a kernel argument
+      }
+      return B200FEM_OK;
+    case B200FEM_OPT_TEST_SKIP_ARRIVAL:
+      if (value < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "TEST_SKIP_ARRIVAL must be >= 0");
+      if (value != eng.test_skip_arrival) {
+        eng.test_skip_arrival = value;
+        eng.step_exec_max_iter = -1;  // recapture: the knob is a kernel argument
+      }
+      return B200FEM_OK;
     default:
       return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
@@ -994,6 +1124,9 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_ELEM_TILE: *value = eng.elem_staged ? (eng.elem_tile_small ? 2 : 1) : 0; break;
     case B200FEM_OPT_FUSED_ASSEMBLY: *value = eng.built ? (eng.fused ? 1 : 0) : eng.opt_fused; break;
     case B200FEM_OPT_REFINE: *value = (eng.built && !eng.refine_ok) ? 0 : eng.opt_refine; break;
+    case B200FEM_OPT_BARRIER_TIMEOUT_MS: *value = eng.barrier_timeout_ms; break;
+    case B200FEM_OPT_TET_ASSEMBLY: *value = eng.built ? (eng.tet_rows ? 0 : 1) : eng.opt_tet_assembly; break;
+    case B200FEM_OPT_TEST_SKIP_ARRIVAL: *value = eng.test_skip_arrival; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
   return B200FEM_OK;
@@ -1102,6 +1235,8 @@ int b200fem_set_state(b200fem_handle h, const double* x, const double* v) {
   ENG(h);
   NEED_BUILT();
   size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
+  if ((x && !all_finite(x, 3 * (size_t)eng.d.n_nodes)) || (v && !all_finite(v, 3 * (size_t)eng.d.n_nodes)))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite position or velocity");
   if (x) CK(cudaMemcpyAsync(eng.d.x, x, n, cudaMemcpyHostToDevice, eng.stream));
   if (v) CK(cudaMemcpyAsync(eng.d.v, v, n, cudaMemcpyHostToDevice, eng.stream));
   // a state set from outside has no history: extrapolation starts at zero
@@ -1128,6 +1263,8 @@ int b200fem_set_external_forces(b200fem_handle h, const double* fext) {
   ENG(h);
   NEED_BUILT();
   size_t n = 3 * (size_t)eng.d.n_nodes * sizeof(double);
+  if (fext && !all_finite(fext, 3 * (size_t)eng.d.n_nodes))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite external force");
   if (fext) CK(cudaMemcpyAsync(eng.d.fext, fext, n, cudaMemcpyHostToDevice, eng.stream));
   else CK(cudaMemsetAsync(eng.d.fext, 0, n, eng.stream));
   CK(cudaStreamSynchronize(eng.stream));
@@ -1139,6 +1276,7 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
   ENG(h);
   NEED_BUILT();
   DevPack& d = eng.d;
+  if (x && !all_finite(x, 3 * (size_t)d.n_nodes)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite position");
   if (x) CK(cudaMemcpyAsync(d.x, x, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyHostToDevice, eng.stream));
   CK(launch_reset_status(eng));
   CK(cudaEventRecord(eng.ev[0], eng.stream));
@@ -1228,6 +1366,10 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
   if (!p || nsteps < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid step parameters");
   if (!(p->h > 0) || !(p->tol > 0) || p->max_iter <= 0)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "step size, tolerance and max_iter must be positive");
+  {
+    const double sp[7] = {p->h, p->alpha_m, p->beta_k, p->gravity[0], p->gravity[1], p->gravity[2], p->tol};
+    if (!all_finite(sp, 7)) return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite step parameter");
+  }
   DevPack& d = eng.d;
   int max_iter = std::min(p->max_iter, d.unconv_cap);
   if (p->pcg_variant < 0 || p->pcg_variant > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown pcg_variant");
@@ -1387,6 +1529,8 @@ int b200fem_backward_euler_step_host(b200fem_handle h, const b200fem_step_params
   ENG(h);
   NEED_BUILT();
   if (!x || !v) return fail(&eng, B200FEM_ERR_INVALID_ARG, "x and v are required");
+  if (!all_finite(x, 3 * (size_t)eng.d.n_nodes) || !all_finite(v, 3 * (size_t)eng.d.n_nodes))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite position or velocity");
   return backward_euler_steps(eng, p, nsteps, stats, x, v);
 }
 

@@ -170,6 +170,12 @@ struct DevPack {
   int* chunk_elem = nullptr;
   int* contrib_loc = nullptr;  // parallel to contrib_idx
   int* blk_mirror = nullptr;   // nnzb: the block at the transposed position
+  // node-row tet assembly (tet_rows.cu): tasks of block rows, the rows'
+  // element incidences, and per contribution the stage entry it reads
+  int* task_row = nullptr;     // tasks+1
+  int* row_incptr = nullptr;   // rows+1
+  int* row_inc = nullptr;      // (element << 3) | (local node << 1) | records the element's statistics
+  unsigned char* contrib_byte = nullptr;  // parallel to contrib_idx
   double* row_nrm = nullptr;   // 3 per row: unit normal of the row's plane constraint (zero: none)
   double* row_off = nullptr;   // per row: the plane's offset
   // refinement sweeps: FP64 residual, correction, its PCG results
@@ -242,11 +248,22 @@ struct Engine {
   bool elem_tile_small = false;  // element kernels: the small tile of each material
   bool elem_staged = false;      // tets: the shared-memory staged kernel instead of one thread per element
   bool fused = false;            // BackwardEuler assembly on the fused row-chunk path
+  // BackwardEuler assembly of tet packs on the node-row path (tet_rows.cu):
+  // B200FEM_OPT_TET_ASSEMBLY 0 (default) where supported, 1 element kernel + gather
+  int opt_tet_assembly = 0;
+  bool tet_rows = false;
+  int rows_cap = 32;                   // incidences per task (32 or 64)
+  std::vector<int> rows_task_off;      // per element group: its task range
   int fused_chunks = 0, fused_emax = 0;
   int opt_fused = 0;             // 1: fused assembly where supported
   int opt_refine = 0;            // refinement sweeps of the mixed form
   bool refine_ok = false;        // supported by the pack (mixed, one NeoHookean/MooneyRivlin group, no NODAL)
   double refine_tol = 1e-3;      // relative tolerance of a correction solve
+  // bound of every PCG grid-barrier wait (B200FEM_OPT_BARRIER_TIMEOUT_MS)
+  int barrier_timeout_ms = 5000;
+  // B200FEM_OPT_TEST_SKIP_ARRIVAL: CTA index + 1 that skips its first
+  // barrier arrival (failure-detection tests; 0 off)
+  int test_skip_arrival = 0;
   int pcg_attr_smem = -1;
   int pcg_variant = 0;
   int pcg_row_lanes = 16;  // lanes per block row in the PCG SpMV (tunable)
@@ -280,6 +297,9 @@ void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int 
                  int* conn);
 void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
                  unsigned long long seed, double* xyz);
+
+// tet_rows.cu
+cudaError_t launch_tet_rows(Engine& eng, bool attr_only);
 
 // kernels.cu
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K);

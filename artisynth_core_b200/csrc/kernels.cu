@@ -1816,6 +1816,7 @@ cudaError_t prepare_kernels(Engine& eng) {
   cudaError_t e = ensure_constants(eng.device);
   if (e != cudaSuccess) return e;
   if (eng.fused && (e = launch_fused_blocks(eng, -1)) != cudaSuccess) return e;
+  if (eng.tet_rows && (e = launch_tet_rows(eng, true)) != cudaSuccess) return e;
   const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
   for (ElemGroup g : eng.groups) {
     g.e1 = g.e0 - 1;  // ne = -1: set attributes only
@@ -1911,6 +1912,9 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   if ((e = launch_nodal_pressure(eng)) != cudaSuccess) return e;
   if ((e = launch_divblk(eng)) != cudaSuccess) return e;
   if ((e = launch_element_pressure(eng)) != cudaSuccess) return e;
+  // the step on the node-row path: S, the nodal forces, b and the PCG's
+  // initial guess in one launch per group (launch_rhs then has nothing left)
+  if (!want_K && eng.tet_rows) return launch_tet_rows(eng, false);
   for (const ElemGroup& g : eng.groups) {
     e = by_elem_type(g.elem_type, [&](auto tag) {
       constexpr int TY = decltype(tag)::value;
@@ -1984,7 +1988,9 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_rhs(Engine& eng) { return launch_rows(eng, eng.d.b, eng.d.sol); }
+// follows launch_assemble(..., want_K = false) in the step; the node-row
+// path has formed b and the initial guess already
+cudaError_t launch_rhs(Engine& eng) { return eng.tet_rows ? cudaSuccess : launch_rows(eng, eng.d.b, eng.d.sol); }
 
 cudaError_t launch_forces_only(Engine& eng) { return launch_rows(eng, nullptr, nullptr); }
 

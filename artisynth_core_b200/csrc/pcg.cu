@@ -73,16 +73,21 @@ __device__ __forceinline__ void red_add_release_u32(unsigned* p, unsigned v) {
 // (no round trip for its old value) and the poll starts at once.  Release
 // on the arrival and acquire on the poll order every CTA's prior global
 // writes before every CTA's later reads.  The wait is bounded: after
-// kBarrierTimeoutNs the CTA records B200FEM_ERR_TIMEOUT in flags[0] and
-// returns false, and every CTA leaves the kernel at its next barrier.
-// The counter must be zero when the kernel starts.
-__device__ bool grid_barrier(unsigned* count, int* flags, unsigned* round) {
+// timeout_ns (B200FEM_OPT_BARRIER_TIMEOUT_MS, default kBarrierTimeoutNs)
+// the CTA records B200FEM_ERR_TIMEOUT in flags[0] and returns false, and
+// every CTA leaves the kernel at its next barrier.  skip_cta >= 0 is the
+// failure-detection test's knob: that CTA does not arrive at the first
+// barrier (it still waits, bounded like the others), so every wait of that
+// barrier runs out.  The counter must be zero when the kernel starts.
+__device__ bool grid_barrier(unsigned* count, int* flags, unsigned* round, unsigned long long timeout_ns,
+                             int skip_cta) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile int* err = flags;
-    const unsigned goal = ++*round * gridDim.x;
-    red_add_release_u32(count, 1u);
+    const unsigned r = ++*round;
+    const unsigned goal = r * gridDim.x;
+    if (!(r == 1u && (int)blockIdx.x == skip_cta)) red_add_release_u32(count, 1u);
     int ok = 1;
     const unsigned long long t0 = global_ns();
     while ((int)(ld_acquire_u32(count) - goal) < 0) {
@@ -90,7 +95,7 @@ __device__ bool grid_barrier(unsigned* count, int* flags, unsigned* round) {
         ok = 0;
         break;
       }
-      if (global_ns() - t0 > kBarrierTimeoutNs) {
+      if (global_ns() - t0 > timeout_ns) {
         atomicExch(flags, B200FEM_ERR_TIMEOUT);
         ok = 0;
         break;
@@ -127,6 +132,8 @@ struct PcgArgs {
   int nb_max;         // max blocks of one CTA
   unsigned* barrier;
   int* flags;
+  unsigned long long barrier_timeout_ns;  // bound of every grid-barrier wait
+  int skip_arrival_cta;  // test knob: this CTA skips its first arrival (-1: none)
   int* unconv;  // per iteration: some model still unconverged
   int max_iter;
   int variant;  // 0 auto (pipelined, classic after a residual replacement), 1 classic, 2 pipelined
@@ -821,7 +828,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       vals[0] = dot3(bv, bv);
     }
   });
-  if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+  if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
   model_sums<1>(a, cr, s_q0, s_q1, ph & 1, sums, s_done);
   for (int j = threadIdx.x; j < npc; j += blockDim.x)
     if (!s_done[j]) {
@@ -848,7 +855,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         vals[0] = dot3(r, z);
         vals[1] = dot3(r, r);
       });
-      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
       model_sums<2>(a, cr, s_q0, s_q1, ph & 1, sums, s_conv);
       ph++;
       for (int j = threadIdx.x; j < npc; j += blockDim.x) {
@@ -894,7 +901,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
             vals[0] = pqv;
           }
         });
-        if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+        if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
         if (__ldcg(&a.unconv[idx]) == 0) {
           total_it += it;
           break;
@@ -926,7 +933,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           vals[0] = dot3(r, z);
           vals[1] = dot3(r, r);
         });
-        if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+        if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
         model_sums<2>(a, cr, s_q0, s_q1, ph & 1, sums, s_conv);
         ph++;
         for (int j = threadIdx.x; j < npc; j += blockDim.x) {
@@ -965,7 +972,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         vals[2] = dot3(r, r);
       }
     });
-    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
     int mbuf = 0;  // m0 holds the current m
 
     for (int it = 0;; it++) {
@@ -1183,7 +1190,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         rescan(s_conv);
         if (threadIdx.x == 0) s_conv_dirty = 0;
       }
-      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
       mbuf ^= 1;
       // every model still iterating at idx - 1 converged there: iteration
       // idx had no rows to work on and is not counted
@@ -1200,7 +1207,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     if (res)
       for (int i = threadIdx.x; i < nloc; i += blockDim.x) store3(a.x, r0 + i, st.at(VX, i, r0 + i));
     rescan(s_done);
-    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
     cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
                           [&](int i, int row, int, int ln, bool valid, double* vals) {
       double Ax[3];
@@ -1220,7 +1227,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
         store3(a.m1, row, u);
       }
     });
-    if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
     model_sums<1>(a, cr, s_q0, s_q1, ph & 1, sums, s_done);
     ph++;
     if (threadIdx.x == 0) s_restart = 0;
@@ -1257,7 +1264,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       if (!s_restart) break;
     } else {
       if (s_restart && threadIdx.x == 0) a.unconv[a.max_iter + 1] = restart + 1;
-      if (!grid_barrier(a.barrier, a.flags, &s_bar_round)) return;
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
       if (__ldcg(&a.unconv[a.max_iter + 1]) != restart + 1) break;
     }
     // continue with classic PCG, whose attainable accuracy is better than
@@ -1334,6 +1341,8 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.tol_override = tol_override;
   a.barrier = d.barrier;
   a.flags = d.flags;
+  a.barrier_timeout_ns = 1000000ull * (unsigned long long)eng.barrier_timeout_ms;
+  a.skip_arrival_cta = eng.test_skip_arrival - 1;
   a.unconv = d.unconv;
   a.max_iter = max_iter;
   a.variant = eng.pcg_variant;
@@ -1531,12 +1540,16 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
                       double tol, int max_iter, void* stream_ptr, int* iterations, double* rel_residual,
                       const char** err) {
   cudaStream_t stream = (cudaStream_t)stream_ptr;
-  if (n_rows < 1 || n_rows > kNoAllocMaxRows) {
-    *err = "n_rows must be in [1, B200FEM_NOALLOC_MAX_ROWS]";
+  if (n_rows < 1 || max_iter < 1) {
+    *err = "n_rows and max_iter must be at least 1";
+    return B200FEM_ERR_INVALID_ARG;
+  }
+  if (n_rows > kNoAllocMaxRows) {
+    *err = "n_rows exceeds B200FEM_NOALLOC_MAX_ROWS";
     return B200FEM_ERR_BUDGET;
   }
-  if (max_iter < 1 || max_iter > kNoAllocMaxIter) {
-    *err = "max_iter must be in [1, B200FEM_NOALLOC_MAX_ITER]";
+  if (max_iter > kNoAllocMaxIter) {
+    *err = "max_iter exceeds B200FEM_NOALLOC_MAX_ITER";
     return B200FEM_ERR_BUDGET;
   }
   if (!rowptr || !col || !vals || !b || !x || !(tol > 0)) {
@@ -1606,6 +1619,23 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   }
   noalloc_diag_kernel<<<(n_rows + 255) / 256, 256, 0, stream>>>(n_rows, rowptr, col, (int*)(base + LY::blk_diag),
                                                                (int*)(base + LY::flags));
+  // a row without a diagonal block has no valid blk_diag entry (the
+  // stand-in rowptr[row] can lie past the caller's vals for an empty last
+  // row): refuse the matrix before the PCG reads any block
+  {
+    int diag_flag = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&diag_flag, base + LY::flags, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+      *err = cudaGetErrorString(e);
+      return B200FEM_ERR_CUDA;
+    }
+    if (diag_flag != 0) {
+      *err = "a block row has no diagonal block";
+      return B200FEM_ERR_INVALID_ARG;
+    }
+  }
   double* vec = (double*)(base + LY::vec);
   const size_t V = 3 * (size_t)kNoAllocMaxRows;
   PcgArgs a;
@@ -1643,6 +1673,8 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.nb_max = 0;
   a.barrier = (unsigned*)(base + LY::barrier);
   a.flags = (int*)(base + LY::flags);
+  a.barrier_timeout_ns = kBarrierTimeoutNs;
+  a.skip_arrival_cta = -1;
   a.unconv = (int*)(base + LY::unconv);
   a.max_iter = max_iter;
   a.variant = 0;

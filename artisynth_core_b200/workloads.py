@@ -45,12 +45,19 @@ class Workload:
     fixed: np.ndarray = field(default=None, repr=False)
     fext: np.ndarray = field(default=None, repr=False)
 
-    def build_mesh(self):
+    def build_mesh(self, mesher=None):
+        """Grid, jitter, fixed nodes and external forces.  `mesher(elem_type,
+        widths, cells, jitter, seed) -> (xyz, conn)` replaces the library's
+        grid factory (a caller that must not load the library, such as a CPU
+        baseline, passes a generator of its own that makes the same mesh)."""
         nx, ny, nz = self.cells
         wx, wy, wz = self.widths
-        xyz, conn = create_grid(self.elem_type, wx, wy, wz, nx, ny, nz)
-        if self.jitter:
-            xyz = jitter_grid(xyz, nx, ny, nz, wx, wy, wz, self.jitter, self.seed)
+        if mesher is not None:
+            xyz, conn = mesher(self.elem_type, self.widths, self.cells, self.jitter, self.seed)
+        else:
+            xyz, conn = create_grid(self.elem_type, wx, wy, wz, nx, ny, nz)
+            if self.jitter:
+                xyz = jitter_grid(xyz, nx, ny, nz, wx, wy, wz, self.jitter, self.seed)
         self.rest, self.conn = xyz, conn
         if self.fix == "xmin":
             self.fixed = (xyz[:, 0] <= -wx / 2 + 1e-9).astype(np.int32)

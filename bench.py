@@ -134,9 +134,35 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def cpu_oracle_rate(wl, budget_s, threads, min_steps=2, max_steps=200):
+def oracle_mesher(elem_type, widths, cells, jitter, seed):
+    """The oracle's own grid factory and jitter (bit-identical to the
+    library's): the CPU legs build their meshes without loading the
+    library."""
+    from oracle import oracle as O
+    O.build()
+    return O.grid(elem_type, widths, cells, jitter, seed)
+
+
+def cpu_info():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+def cpu_oracle_protocol(wl, threads, runs=5, warmup=3, budget_s=8.0, max_k=50):
     """Times the CPU oracle (FP64 restatement of the Java path; Jacobi-PCG to
-    the workload tolerance) on the host: BackwardEuler steps/s."""
+    the workload tolerance) on `threads` host threads: `warmup` untimed
+    steps, then `runs` timed runs of k consecutive BackwardEuler steps (k
+    sized from the warm-up so that the runs take about budget_s together);
+    returns the median steps/s over the runs, the runs, k and the threads
+    used."""
     from oracle import oracle as O
     O.build()
     used = O.set_threads(threads)
@@ -145,14 +171,42 @@ def cpu_oracle_rate(wl, budget_s, threads, min_steps=2, max_steps=200):
     x = wl.rest.copy()
     v = np.zeros_like(x)
     fext = wl.fext if wl.traction is not None else None
-    om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=fext, tol=wl.tol)  # warm-up
+
+    def step():
+        st, _, _ = om.be_step(wl.h, x, v, alpha=wl.mass_damping, beta=wl.stiffness_damping, gravity=wl.gravity,
+                              fext=fext, tol=wl.tol)
+        return st
+
     t0 = time.perf_counter()
-    n = 0
-    while n < max_steps and (n < min_steps or time.perf_counter() - t0 < budget_s):
-        st, _, _ = om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, fext=fext, tol=wl.tol)
-        n += 1
-    dt = time.perf_counter() - t0
-    return n / dt, n, dt, used
+    for _ in range(warmup):
+        step()
+    tw = (time.perf_counter() - t0) / max(warmup, 1)
+    k = int(max(1, min(max_k, budget_s / runs / max(tw, 1e-6))))
+    rates = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        for _ in range(k):
+            step()
+        rates.append(k / (time.perf_counter() - t0))
+    del om
+    return statistics.median(rates), rates, k, used
+
+
+def cpu_baseline_entry(wl, label, budget_s=8.0, runs=5, warmup=3):
+    """Both CPU variants of the baseline protocol: single thread (the Java
+    loop order) and OpenMP on every host core; `value` is the all-cores
+    median."""
+    allc = os.cpu_count() or 1
+    v1, r1, k1, _ = cpu_oracle_protocol(wl, 1, runs=runs, warmup=warmup, budget_s=budget_s)
+    va, ra, ka, used = cpu_oracle_protocol(wl, allc, runs=runs, warmup=warmup, budget_s=budget_s)
+    out = {"value": va, "unit": UNIT, "cores": used, "kind": "port",
+           "sample": f"median of {runs} runs of {ka} consecutive BackwardEuler steps of the {label} after "
+                     f"{warmup} warm-up steps (FP64 oracle, Jacobi-PCG {wl.tol:g}, OpenMP on {used} threads)",
+           "runs": ra,
+           "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "runs": r1,
+                             "sample": f"median of {runs} runs of {k1} steps after {warmup} warm-up steps"}}
+    out.update(cpu_info())
+    return out
 
 
 def run_reference(args):
@@ -162,7 +216,7 @@ def run_reference(args):
             dist.destroy_process_group()
         return
     from artisynth_core_b200 import workloads as W
-    wl = W.neohookean_hex_beam().build_mesh()
+    wl = W.neohookean_hex_beam().build_mesh(mesher=oracle_mesher)
     threads = os.cpu_count() or 1
     from oracle import oracle as O
     O.build()
@@ -183,8 +237,10 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": dict(wl.describe(), solver="Jacobi-PCG 1e-10"),
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": used, "kind": "port",
-                         "sample": f"{args.steps} full BackwardEuler steps of the 40x10x10 hex beam"},
+        "cpu_baseline": dict({"value": val, "unit": UNIT, "cores": used, "kind": "port",
+                              "sample": f"{args.steps} consecutive BackwardEuler steps of the 40x10x10 hex beam "
+                                        f"after {args.warmup} warm-up steps (FP64 oracle, Jacobi-PCG 1e-10, "
+                                        f"OpenMP on {used} threads)"}, **cpu_info()),
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -322,6 +378,86 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
                             "max_rel_position_error_vs_fp64": rerr,
                             "max_rel_displacement_error_vs_fp64": rderr},
     }
+
+
+def block_bytes(N, E, nnzb, n_active, s_bytes=72, rest_bytes=72):
+    """Algorithmic bytes of the MooneyRivlin block (4-node tets, one point):
+    assembly 24 N (x) + 16 E (connectivity) + rest_bytes E (invJ0) + 64 E
+    (scatter map) + s_bytes nnzb (S written, the NODAL 2-ring included) +
+    24 N (f / b); PCG iteration (s_bytes + 4) nnzb (S and block columns) +
+    4 (Na + 1) + 48 Na + 72 Na + 9 * 24 Na."""
+    asm = 24 * N + 16 * E + rest_bytes * E + 64 * E + s_bytes * nnzb + 24 * N
+    it = (s_bytes + 4) * nnzb + 4 * (n_active + 1) + 48 * n_active + 72 * n_active + 9 * 24 * n_active
+    return asm, it
+
+
+def run_block(dev, steps=50, tol=1e-10, cpu=True):
+    """The MooneyRivlin tet block (60x30x30 cells of a 0.3x0.15x0.15 m block,
+    270,000 tets, 58,621 nodes; AUTO soft incompressibility resolves to NODAL:
+    3,935,980 blocks), `steps` BackwardEuler steps from rest in the plain
+    FP64 form and in the mixed form, on device-resident state (S alone is
+    283 MB, above the 126 MB L2, so nothing is flushed); the mixed form's
+    position error against the FP64 run after the same steps."""
+    import torch
+    from artisynth_core_b200 import _lib as L
+    from artisynth_core_b200 import workloads as W
+    from artisynth_core_b200.femmodel import MechSystemSolver
+    wl = W.mooneyrivlin_tet_block().build_mesh()
+    peak, kind = peaks()
+    out = {"workload": "mooneyrivlin_tet_block_60x30x30 (270,000 tets, NODAL incompressibility, gravity, "
+                       f"z-min fixed), {steps} steps h=0.01 from rest, PCG {tol:g}",
+           "steps": steps, "tol": tol, "l2": "working set above L2 (S alone 283 MB f64)"}
+    xs = {}
+    for prec, name in ((L.PREC_FP64, "fp64"), (L.PREC_MIXED, "mixed")):
+        m = wl.model(precision=prec, device=dev)
+        ms = MechSystemSolver(m, tol=tol, max_iter=20000)
+        t0 = time.perf_counter()
+        m.engine()
+        sz = m.sizes()
+        ms.backwardEuler(wl.h, 1)  # captures the step graph
+        m.setState(wl.rest, np.zeros_like(wl.rest))
+        build_s = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        asm = pcg = 0.0
+        its = []
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ms.backwardEuler(wl.h, 1)
+            a, p = ms.lastTiming()
+            asm += a
+            pcg += p
+            its.append(ms.stats.iterations)
+        wall = time.perf_counter() - t0
+        xs[name], _ = m.getState()
+        m._invalidate()
+        sb = 72 if name == "fp64" else 36
+        asm_b, it_b = block_bytes(wl.rest.shape[0], wl.conn.shape[0], sz["nnzb"], sz["n_active"], s_bytes=sb,
+                                  rest_bytes=72 if name == "fp64" else 36)
+        mean_it = float(np.mean(its))
+        asm_gbs = asm_b / (asm / steps * 1e-3) / 1e9
+        pcg_gbs = it_b * (mean_it + 2) / (pcg / steps * 1e-3) / 1e9
+        out[name] = {"steps_per_s": steps / wall, "device_ms_per_step": (asm + pcg) / steps,
+                     "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
+                     "pcg_iterations_mean": mean_it, "build_s": build_s,
+                     "element_updates_per_s": wl.conn.shape[0] * steps / wall,
+                     "assembly_roofline": {"algorithmic_bytes": asm_b, "achieved_gbs": asm_gbs, "peak_gbs": peak,
+                                           "frac": asm_gbs / peak, "peak_kind": kind},
+                     "pcg_roofline": {"bytes_per_iteration": it_b, "achieved_gbs": pcg_gbs, "peak_gbs": peak,
+                                      "frac": pcg_gbs / peak, "peak_kind": kind}}
+        out["nnzb"] = sz["nnzb"]
+        out["active_dof"] = 3 * sz["n_active"]
+    out["mixed_max_rel_position_error_vs_fp64"] = _rel(xs["mixed"], xs["fp64"])
+    out["mixed_max_rel_displacement_error_vs_fp64"] = _rel(xs["mixed"] - wl.rest, xs["fp64"] - wl.rest)
+    if cpu:
+        # the oracle on every host core: a bounded sample of the same run
+        # (one warm-up step, then the median of 5 single-step runs)
+        cw = W.mooneyrivlin_tet_block().build_mesh(mesher=oracle_mesher)
+        v, runs, k, used = cpu_oracle_protocol(cw, os.cpu_count() or 1, runs=5, warmup=1, budget_s=1e-3, max_k=1)
+        out["cpu_baseline"] = dict({"value": v, "unit": UNIT, "cores": used, "kind": "port", "runs": runs,
+                                    "sample": f"median of 5 single BackwardEuler steps after 1 warm-up step "
+                                              f"(FP64 oracle, Jacobi-PCG {cw.tol:g}, OpenMP on {used} threads)"},
+                                   **cpu_info())
+    return out
 
 
 def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=10, tol=1e-6,
@@ -588,12 +724,14 @@ def run_b200(args):
             with ClockSampler(dev) as c:
                 served = run_served(dev, seconds=args.served_seconds, tol=args.served_tol)
             served["clocks"] = c.summary()
+        block = None
+        if world == 1 and not args.no_block:
+            with ClockSampler(dev) as c:
+                block = run_block(dev, steps=args.block_steps, cpu=not args.no_cpu)
+            block["clocks"] = c.summary()
         cpu = None
         if not args.no_cpu and world == 1:
-            rate, n, dt, used = cpu_oracle_rate(wl, args.cpu_budget, os.cpu_count() or 1)
-            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
-                   "sample": f"{n} BackwardEuler steps of the 40x10x10 hex beam in {dt:.1f} s "
-                             f"(FP64 oracle, Jacobi-PCG 1e-10, OpenMP)"}
+            cpu = cpu_baseline_entry(wl, "40x10x10 hex beam", budget_s=args.cpu_budget)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True,
@@ -612,6 +750,7 @@ def run_b200(args):
                          "assembly_gbs": asm_gbs, "pcg_gbs": pcg_gbs},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "block": block,
             "batched": batched,
             "served": served,
         }
@@ -628,9 +767,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds per CPU-baseline variant")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-pack leg")
-    ap.add_argument("--only", choices=["batched"], default=None,
+    ap.add_argument("--no-block", action="store_true", help="skip the MooneyRivlin block leg")
+    ap.add_argument("--block-steps", type=int, default=50)
+    ap.add_argument("--only", choices=["batched", "block"], default=None,
                     help="run only this leg (for profiling): prints its JSON object")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
@@ -648,6 +789,10 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(run_batched(0, steps=args.batch_steps, tol=args.batch_tol, sample_every=64,
                                      tune=not args.no_tune)), flush=True)
+    elif args.only == "block":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_block(0, steps=args.block_steps, cpu=not args.no_cpu)), flush=True)
     else:
         run_b200(args)
 

@@ -289,6 +289,21 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                         path avoids the element blocks' HBM round trip but
                                         recomputes boundary elements; it measured slower on the
                                         benchmark meshes and is kept for larger chunks later. */
+#define B200FEM_OPT_BARRIER_TIMEOUT_MS 9 /* bound of every wait at the PCG's grid barriers, in ms
+                                          (1..60000, default 5000): a wait that runs out ends
+                                          the solve with B200FEM_ERR_TIMEOUT and the device
+                                          context stays usable (may be changed after the build) */
+#define B200FEM_OPT_TEST_SKIP_ARRIVAL 10 /* failure-detection tests only: CTA index + 1 of the PCG
+                                           kernel that does not arrive at its first grid barrier,
+                                           so every wait there runs out after
+                                           B200FEM_OPT_BARRIER_TIMEOUT_MS; 0 (default) off */
+#define B200FEM_OPT_TET_ASSEMBLY 11 /* BackwardEuler assembly of tetrahedral packs with non-linear
+                                       materials: 0 (default) node-row kernel -- a warp per few block
+                                       rows recomputes each incident tetrahedron and sums the rows'
+                                       blocks, forces and right-hand side, with no element data in
+                                       HBM; 1 element kernel + block gather.  Both give the same S
+                                       and b bit for bit.  Set before b200fem_build; after it, 0
+                                       reads back as 1 where the node-row path does not apply */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
@@ -355,7 +370,10 @@ int b200fem_server_get_stats(b200fem_server_handle s, b200fem_server_stats* out)
    Every other buffer comes from a static device array that each device
    which loads the library holds until the process exits.  Sizes beyond
    B200FEM_NOALLOC_MAX_ROWS / _MAX_ITER are rejected with
-   B200FEM_ERR_BUDGET.  The first call on a device looks up the array's
+   B200FEM_ERR_BUDGET; n_rows or max_iter below 1, and a matrix with a row
+   that holds no diagonal block (checked before the solve reads any block),
+   with B200FEM_ERR_INVALID_ARG.  Running out of iterations returns
+   B200FEM_ERR_NO_CONVERGE with x holding the last iterate.  The first call on a device looks up the array's
    device address (cudaGetSymbolAddress); make that first call before any
    stream capture.  The call runs on `stream` (a cudaStream_t, NULL for the
    legacy default stream) and returns after it completes; all calls share

@@ -16,9 +16,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "libfemoracle.so")
 _lib = None
 # the reference's device assembly kernels (cudssBridgeKernels.cu), compiled
-# from the reference tree by `make ref` where that tree is present
+# from the reference tree by `make ref` where that tree is present; its
+# location comes from the caller or from $ARTISYNTH_REFERENCE
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libref_kernels.so")
-REF_SOURCE_ROOT = "/root/reference"
 
 ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET, ELEM_QUADHEX, ELEM_QUADWEDGE, ELEM_QUADPYRAMID = range(8)
 ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10, ELEM_QUADHEX: 20,
@@ -36,12 +36,14 @@ def build() -> str:
     return _LIB_PATH
 
 
-def build_ref() -> str | None:
-    """Compile the reference's kernels into oracle/_ref/ when the reference
-    tree is present; elsewhere (a GPU box gets the prebuilt library) return
-    the library path if it exists, else None."""
-    if os.path.isdir(REF_SOURCE_ROOT):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + REF_SOURCE_ROOT], check=True)
+def build_ref(source_root: str | None = None) -> str | None:
+    """Compile the reference's kernels into oracle/_ref/ from the reference
+    tree at `source_root` (default: $ARTISYNTH_REFERENCE) when that tree is
+    present; elsewhere (a GPU box gets the prebuilt library) return the
+    library path if it exists, else None."""
+    root = source_root or os.environ.get("ARTISYNTH_REFERENCE")
+    if root and os.path.isdir(root):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + root], check=True)
     return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
 
 
