@@ -526,6 +526,15 @@ int build_pack(Engine& eng) {
     if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
     eng.pcg_resident = eng.pcg_cached = 0;
   }
+  // cluster split: one thread-block cluster per model, models taken from a
+  // queue largest first (pcg_cluster.cu); for packs of many models that do
+  // not fit shared-memory residency
+  eng.pcg_cluster = false;
+  if (eng.opt_split == 3 || (eng.opt_split == 0 && !eng.pcg_resident && M > 1)) {
+    eng.cl_clusters = pcg_cluster_capacity(eng.precision == B200FEM_PREC_MIXED);
+    if (eng.cl_clusters > 0) eng.pcg_cluster = true;
+    else if (eng.opt_split == 3) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "thread-block clusters unavailable");
+  }
   if (eng.opt_split == 2 || (eng.opt_split == 0 && !eng.pcg_resident && M > 1)) {
     // Strided split for packs too large for shared-memory residency: every
     // model is cut into short pieces and each piece goes to the least-loaded
@@ -689,10 +698,18 @@ int build_pack(Engine& eng) {
       for (int m = 0; m < M; m++)
         std::copy(eng.hosts[m].rest_vol.begin(), eng.hosts[m].rest_vol.end(), erv.begin() + eng.elem_off[m]);
       CK(upload(eng, &d.elem_rest_vol, erv));
-      CK(dalloc(eng, &d.elem_p, (size_t)E));
-      CK(dalloc(eng, &d.elem_r, (size_t)E));
-      CK(cudaMemset(d.elem_p, 0, sizeof(double) * (size_t)E));
-      CK(cudaMemset(d.elem_r, 0, sizeof(double) * (size_t)E));
+      // one pressure value per element, or npv values and an npv x npv Rinv
+      const size_t npv = (size_t)elem_npv(eng.elem_type);
+      CK(dalloc(eng, &d.elem_p, (size_t)E * npv));
+      CK(dalloc(eng, &d.elem_r, (size_t)E * npv * npv));
+      CK(cudaMemset(d.elem_p, 0, sizeof(double) * (size_t)E * npv));
+      CK(cudaMemset(d.elem_r, 0, sizeof(double) * (size_t)E * npv * npv));
+      if (npv > 1) {
+        std::vector<double> dj0((size_t)E * nip, 1.0);
+        for (int m = 0; m < M; m++)
+          std::copy(eng.hosts[m].detJ0.begin(), eng.hosts[m].detJ0.end(), dj0.begin() + (size_t)eng.elem_off[m] * nip);
+        CK(upload(eng, &d.detJ0, dj0));
+      }
     }
   }
   if (any_nodal) {
@@ -715,6 +732,18 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.cta_piece, cta_piece));
   CK(upload(eng, &d.cta_plist, cta_plist));
   CK(upload(eng, &d.model_active, std::vector<int>(M, 1)));
+  {
+    // cluster split: model rows, the queue order (most blocks first) and the
+    // queue counter
+    std::vector<int> model_row(eng.row_off.begin(), eng.row_off.end()), order(M);
+    for (int m = 0; m < M; m++) order[m] = m;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+      return eng.blk_off[x + 1] - eng.blk_off[x] > eng.blk_off[y + 1] - eng.blk_off[y];
+    });
+    CK(upload(eng, &d.model_row, model_row));
+    CK(upload(eng, &d.cl_order, order));
+    CK(dalloc(eng, &d.cl_queue, 1));
+  }
   eng.any_inactive = false;
   d.unconv_cap = 200000;
   CK(dalloc(eng, &d.unconv, (size_t)d.unconv_cap + 2));
@@ -1038,7 +1067,7 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
   ENG(h);
   switch (key) {
     case B200FEM_OPT_PCG_SPLIT:
-      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_SPLIT must be 0, 1 or 2");
+      if (value < 0 || value > 3) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_SPLIT must be 0, 1, 2 or 3");
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_SPLIT is set before b200fem_build");
       eng.opt_split = value;
       return B200FEM_OK;
@@ -1116,7 +1145,9 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
   ENG(h);
   if (!value) return fail(&eng, B200FEM_ERR_INVALID_ARG, "null value");
   switch (key) {
-    case B200FEM_OPT_PCG_SPLIT: *value = eng.built ? (eng.pcg_strided ? 2 : 1) : eng.opt_split; break;
+    case B200FEM_OPT_PCG_SPLIT:
+      *value = eng.built ? (eng.pcg_cluster ? 3 : eng.pcg_strided ? 2 : 1) : eng.opt_split;
+      break;
     case B200FEM_OPT_ROW_LANES: *value = eng.built ? eng.pcg_row_lanes : eng.opt_row_lanes; break;
     case B200FEM_OPT_PCG_CTAS: *value = eng.built ? eng.pcg_grid : eng.opt_ctas; break;
     case B200FEM_OPT_PIECE_ROWS: *value = eng.opt_piece_rows; break;

@@ -38,6 +38,11 @@ __host__ __device__ constexpr int elem_linear_base(int type) {
          : type == B200FEM_ELEM_QUADWEDGE ? B200FEM_ELEM_WEDGE : type == B200FEM_ELEM_QUADPYRAMID ? B200FEM_ELEM_PYRAMID
          : -1;
 }
+// pressure values per element of ELEMENT soft incompressibility
+// (FemElement3d.numPressureVals: QuadhexElement 4, QuadwedgeElement 2)
+__host__ __device__ constexpr int elem_npv(int type) {
+  return type == B200FEM_ELEM_QUADHEX ? 4 : type == B200FEM_ELEM_QUADWEDGE ? 2 : 1;
+}
 // integration point k lies at node k (FemElement3d.integrationPointsMapToNodes)
 __host__ __device__ constexpr bool elem_ip_at_nodes(int type) {
   return type == B200FEM_ELEM_HEX || type == B200FEM_ELEM_WEDGE || type == B200FEM_ELEM_PYRAMID;
@@ -149,8 +154,9 @@ struct DevPack {
   // ELEMENT soft incompressibility: per element rest volume, pressure and
   // Rinv (effective modulus / rest volume)
   double* elem_rest_vol = nullptr;
-  double* elem_p = nullptr;
-  double* elem_r = nullptr;
+  double* elem_p = nullptr;    // E * npv pressure values
+  double* elem_r = nullptr;    // E * npv * npv: Rinv
+  double* detJ0 = nullptr;     // E * nip rest Jacobian determinants (several pressure values)
   // reductions / PCG control
   double* partials = nullptr;  // [2][n_pieces][4] (double-buffered by phase)
   int* piece_row = nullptr;    // n_pieces+1
@@ -176,6 +182,10 @@ struct DevPack {
   int* row_incptr = nullptr;   // rows+1
   int* row_inc = nullptr;      // (element << 3) | (local node << 1) | records the element's statistics
   unsigned char* contrib_byte = nullptr;  // parallel to contrib_idx
+  // cluster PCG split (pcg_cluster.cu)
+  int* model_row = nullptr;    // models+1: first block row of each model
+  int* cl_order = nullptr;     // models in queue order
+  int* cl_queue = nullptr;     // next queue position (cleared per solve)
   double* row_nrm = nullptr;   // 3 per row: unit normal of the row's plane constraint (zero: none)
   double* row_off = nullptr;   // per row: the plane's offset
   // refinement sweeps: FP64 residual, correction, its PCG results
@@ -233,6 +243,8 @@ struct Engine {
   int pcg_grid = 0, pcg_block = 256;
   int pcg_resident = 0, pcg_cached = 0, pcg_nloc_max = 0, pcg_nb_max = 0;
   int pcg_strided = 0;  // pieces dealt to CTAs across models (large packs)
+  bool pcg_cluster = false;  // one thread-block cluster per model (pcg_cluster.cu)
+  int cl_clusters = 0;       // clusters resident at once
   int pcg_every_cta_rows = 0;  // every CTA of the PCG split holds at least one piece
   // plane constraints (b200fem_set_plane_constraints): per constrained node
   // its unit normal and offset; enforced by the ConstrainedBackwardEuler step
@@ -293,6 +305,9 @@ void quadratic_mesh(int lin_type, int nn, const double* xyz, int ne, const int* 
 // dN/ds of the element's nodes at integration point k (k = -1: the warping
 // point) and the point's weight
 void shape_grads(int type, int k, double* g /* nen * 3 */, double* w);
+// pressure weights H of every integration point (nip * npv) and the weight
+// matrix W = (sum_k H H^T)^-1 (npv * npv) of a multi-pressure element type
+void pressure_tables(int type, double* H, double* W);
 void create_grid(int type, double wx, double wy, double wz, int nx, int ny, int nz, double* xyz,
                  int* conn);
 void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double frac,
@@ -300,6 +315,11 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 
 // tet_rows.cu
 cudaError_t launch_tet_rows(Engine& eng, bool attr_only);
+
+// pcg_cluster.cu
+int pcg_cluster_capacity(bool fp32);
+cudaError_t launch_pcg_cluster(Engine& eng, int max_iter, bool update_state, const double* rhs, double* xsol,
+                               double tol_override, double* model_out);
 
 // kernels.cu
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K);

@@ -61,6 +61,12 @@ __constant__ double c_qwed_gns[9 * 15 * 3], c_qwed_wgns[15 * 3];
 __constant__ double c_qpyr_gns[5 * 13 * 3], c_qpyr_wgns[13 * 3];
 __constant__ float c_qwed_gns_f[9 * 15 * 3], c_qpyr_gns_f[5 * 13 * 3];
 
+// ELEMENT soft incompressibility with several pressure values: pressure
+// weights H [ip][value] and the weight matrix W (quadratic hexes: 4 values,
+// quadratic wedges: 2)
+__constant__ double c_qhex_H[14 * 4], c_qhex_W[4 * 4];
+__constant__ double c_qwed_H[9 * 2], c_qwed_W[2 * 2];
+
 static bool g_const_ready[64] = {false};
 
 static cudaError_t ensure_constants(int device) {
@@ -119,6 +125,15 @@ static cudaError_t ensure_constants(int device) {
   if ((e = cudaMemcpyToSymbol(c_qpyr_gns, qp, sizeof(qp))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qpyr_wgns, qpw, sizeof(qpw))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qpyr_gns_f, qpf, sizeof(qpf))) != cudaSuccess) return e;
+  {
+    double hh[14 * 4], hw[16], wh[9 * 2], ww[4];
+    pressure_tables(B200FEM_ELEM_QUADHEX, hh, hw);
+    pressure_tables(B200FEM_ELEM_QUADWEDGE, wh, ww);
+    if ((e = cudaMemcpyToSymbol(c_qhex_H, hh, sizeof(hh))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_qhex_W, hw, sizeof(hw))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_qwed_H, wh, sizeof(wh))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_qwed_W, ww, sizeof(ww))) != cudaSuccess) return e;
+  }
   if ((e = cudaMemcpyToSymbol(c_qhex_gns, qh, sizeof(qh))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qhex_wgns, qhw, sizeof(qhw))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_qhex_gns_f, qhf, sizeof(qhf))) != cudaSuccess) return e;
@@ -232,6 +247,35 @@ __host__ __device__ constexpr int force_slot(int type) {
 }
 
 // calls f(std::integral_constant<int, TYPE>) for the run-time element type
+// pressure weight H_l at integration point k and weight-matrix entry W_ij
+// of a multi-pressure element type (1 for the one-pressure types)
+template <int TYPE>
+__device__ __forceinline__ double press_H(int k, int l) {
+  if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return c_qhex_H[k * 4 + l];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADWEDGE) return c_qwed_H[k * 2 + l];
+  else return 1.0;
+}
+template <int TYPE>
+__device__ __forceinline__ double press_W(int i, int j) {
+  if constexpr (TYPE == B200FEM_ELEM_QUADHEX) return c_qhex_W[i * 4 + j];
+  else if constexpr (TYPE == B200FEM_ELEM_QUADWEDGE) return c_qwed_W[i * 2 + j];
+  else return 1.0;
+}
+// the pressure at integration point k: sum_l H_l p_l over the element's
+// values (FemModel3d.java:3465-3471); one value: the element's pressure
+template <int TYPE>
+__device__ __forceinline__ double elem_point_pressure(const double* elem_p, int e, int k) {
+  constexpr int NPV = elem_npv(TYPE);
+  if constexpr (NPV == 1) {
+    return elem_p[e];
+  } else {
+    double pr = 0;
+#pragma unroll
+    for (int l = 0; l < NPV; l++) pr += press_H<TYPE>(k, l) * elem_p[(size_t)e * NPV + l];
+    return pr;
+  }
+}
+
 template <typename F>
 static cudaError_t by_elem_type(int type, F&& f) {
   switch (type) {
@@ -422,7 +466,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
           pr = (T)a.node_p[snode[el][k]];
         }
       } else if constexpr (INC == kIncElement) {
-        pr = (T)a.elem_p[e];
+        pr = (T)elem_point_pressure<TYPE>(a.elem_p, e, k);
       }
       T mpt[8];
 #pragma unroll
@@ -455,7 +499,7 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
           add_bdb(K, sg[s][ia], sD[s], sg[s][ib], sdv[s]);
         add_geometric(K, sg[s][ia], ssig[s], sg[s][ib], sdv[s]);
       }
-      if constexpr (INC == kIncElement) {
+      if constexpr (INC == kIncElement && elem_npv(TYPE) == 1) {
         // ELEMENT dilational stiffness Rinv c_a c_b^T, c = sum_k GNx dv
         // (FemModel3d.java:3650-3663, FemUtilities.addToIncompressConstraints)
         T ca[3] = {T(0), T(0), T(0)}, cb[3] = {T(0), T(0), T(0)};
@@ -473,6 +517,49 @@ __global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
         for (int i = 0; i < 3; i++)
 #pragma unroll
           for (int j = 0; j < 3; j++) K[3 * i + j] += r * ca[i] * cb[j];
+      } else if constexpr (INC == kIncElement) {
+        // several pressure values: constraints c^l = sum_k H_l GNx dv
+        // (3 x npv per node) and K_ab += c_a Rinv c_b^T, formed as
+        // X = Rinv c_b^T, K += c_a X (FemUtilities.addDilationalStiffness,
+        // FemUtilities.java:317-342)
+        constexpr int NPV = elem_npv(TYPE);
+        T ca[3][NPV], cb[3][NPV];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int l = 0; l < NPV; l++) ca[c][l] = cb[c][l] = T(0);
+#pragma unroll
+        for (int k = 0; k < NIP; k++) {
+          const int s = el * NIP + k;
+#pragma unroll
+          for (int l = 0; l < NPV; l++) {
+            const T hd = (T)press_H<TYPE>(k, l) * sdv[s];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              ca[c][l] += hd * sg[s][ia][c];
+              cb[c][l] += hd * sg[s][ib][c];
+            }
+          }
+        }
+        const double* Rv = a.elem_r + (size_t)e * NPV * NPV;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          T X[NPV];
+#pragma unroll
+          for (int l = 0; l < NPV; l++) {
+            T xq = T(0);
+#pragma unroll
+            for (int m = 0; m < NPV; m++) xq += (T)Rv[l * NPV + m] * cb[q][m];
+            X[l] = xq;
+          }
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            T acc = T(0);
+#pragma unroll
+            for (int l = 0; l < NPV; l++) acc += ca[r][l] * X[l];
+            K[3 * r + q] += acc;
+          }
+        }
       }
       T* out = elemK + ((size_t)e * NPAIR + w) * 9;
 #pragma unroll
@@ -950,7 +1037,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
           pr = a.node_p[nodes[k]];
         }
       } else if constexpr (INC == kIncElement) {
-        pr = a.elem_p[e];
+        pr = elem_point_pressure<TYPE>(a.elem_p, e, k);
       }
       double D[36];
       material_point<MAT, double>(sig, D, mp, F, detF, pr);
@@ -1550,12 +1637,91 @@ template <int TYPE>
 __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ conn,
                                         const int* __restrict__ elem_model, const double* __restrict__ x,
                                         const double* __restrict__ rest_vol, const double* __restrict__ mat,
-                                        double* __restrict__ elem_p, double* __restrict__ elem_r) {
+                                        const double* __restrict__ detJ0, double* __restrict__ elem_p,
+                                        double* __restrict__ elem_r) {
   constexpr int NEN = elem_nen(TYPE);
   constexpr int NIP = elem_nip(TYPE);
+  constexpr int NPV = elem_npv(TYPE);
   const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= e1) return;
   const int* nodes = conn + (size_t)e * NEN;
+  if constexpr (NPV > 1) {
+    // several pressure values (computePressuresAndRinv, FemModel3d.java:
+    // 2538-2581): per point J_k = detJ/detJ0 and dV = detJ0 w;
+    // pbuf = sum_k H p(K, J_k) dV, p = W pbuf / V0; Rinv = W K / V0 for the
+    // quadratic potential, else Wt R Wt with Wt = W / V0 and
+    // R = sum_k H H^T modulus(K, J_k) dV
+    const double* mp = mat + (size_t)elem_model[e] * kMatParams;
+    const double K = mp[5], V0 = rest_vol[e];
+    const bool quad = mp[7] == 0;
+    double pbuf[NPV], R[NPV * NPV];
+#pragma unroll
+    for (int i = 0; i < NPV; i++) pbuf[i] = 0;
+#pragma unroll
+    for (int i = 0; i < NPV * NPV; i++) R[i] = 0;
+    for (int k = 0; k < NIP; k++) {
+      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int n = 0; n < NEN; n++) {
+        const double* pn = x + 3 * (size_t)nodes[n];
+        const double g0 = gns<double, TYPE>(k, n, 0), g1 = gns<double, TYPE>(k, n, 1), g2 = gns<double, TYPE>(k, n, 2);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          J[3 * r] += pn[r] * g0;
+          J[3 * r + 1] += pn[r] * g1;
+          J[3 * r + 2] += pn[r] * g2;
+        }
+      }
+      const double dJ0 = detJ0[(size_t)e * NIP + k];
+      const double Jk = det3(J) / dJ0;
+      const double dV = dJ0 * ip_weight<double, TYPE>(k);
+      const double pv = (quad ? K * (Jk - 1) : K * log(Jk) / Jk) * dV;
+#pragma unroll
+      for (int i = 0; i < NPV; i++) pbuf[i] += press_H<TYPE>(k, i) * pv;
+      if (!quad) {
+        const double mod = K * (1 - log(Jk)) / (Jk * Jk);
+#pragma unroll
+        for (int i = 0; i < NPV; i++)
+#pragma unroll
+          for (int j = 0; j < NPV; j++) R[i * NPV + j] += press_H<TYPE>(k, i) * press_H<TYPE>(k, j) * mod * dV;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NPV; i++) {
+      double pi = 0;
+#pragma unroll
+      for (int j = 0; j < NPV; j++) pi += press_W<TYPE>(i, j) * pbuf[j];
+      elem_p[(size_t)e * NPV + i] = pi / V0;
+    }
+    double* Ro = elem_r + (size_t)e * NPV * NPV;
+    if (quad) {
+#pragma unroll
+      for (int i = 0; i < NPV; i++)
+#pragma unroll
+        for (int j = 0; j < NPV; j++) Ro[i * NPV + j] = press_W<TYPE>(i, j) * (K / V0);
+    } else {
+      double RW[NPV * NPV];
+#pragma unroll
+      for (int i = 0; i < NPV; i++)
+#pragma unroll
+        for (int j = 0; j < NPV; j++) {
+          double t = 0;
+#pragma unroll
+          for (int l = 0; l < NPV; l++) t += R[i * NPV + l] * (press_W<TYPE>(l, j) / V0);
+          RW[i * NPV + j] = t;
+        }
+#pragma unroll
+      for (int i = 0; i < NPV; i++)
+#pragma unroll
+        for (int j = 0; j < NPV; j++) {
+          double t = 0;
+#pragma unroll
+          for (int l = 0; l < NPV; l++) t += (press_W<TYPE>(i, l) / V0) * RW[l * NPV + j];
+          Ro[i * NPV + j] = t;
+        }
+    }
+    return;
+  }
   double V = 0;
 #pragma unroll
   for (int q = 0; q < NIP; q++) {
@@ -1594,7 +1760,7 @@ cudaError_t launch_element_pressure(Engine& eng) {
     const int threads = 128, blocks = (g.e1 - g.e0 + threads - 1) / threads;
     cudaError_t e = by_elem_type(eng.elem_type, [&](auto tag) {
       element_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
-          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.elem_p, d.elem_r);
+          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.detJ0, d.elem_p, d.elem_r);
       return cudaGetLastError();
     });
     if (e != cudaSuccess) return e;

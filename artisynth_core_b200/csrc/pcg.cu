@@ -1308,6 +1308,7 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
 // per-model results go to model_out.
 cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const double* rhs, double* xsol,
                           double tol_override, double* model_out) {
+  if (eng.pcg_cluster) return launch_pcg_cluster(eng, max_iter, update_state, rhs, xsol, tol_override, model_out);
   DevPack& d = eng.d;
   cudaError_t e;
   if ((e = cudaMemsetAsync(d.barrier, 0, sizeof(unsigned), eng.stream)) != cudaSuccess) return e;

@@ -185,6 +185,65 @@ void quadpyramid_grad(double* g, int i, double s, double t, double r) {
 
 }  // namespace
 
+// Pressure weights of the multi-pressure elements at their integration
+// points -- QuadhexElement.getH (1, s, t, r) (:451-470) and
+// QuadwedgeElement.getH ((1 - r)/2, (1 + r)/2) (:275-291) -- and the
+// weight matrix W = (sum_k H H^T)^-1 summed over the points without their
+// weights, as FemElement3d.createPressureWeightMatrix does (:226-255).
+void pressure_tables(int type, double* H, double* W) {
+  const int npv = elem_npv(type), nip = elem_nip(type);
+  for (int k = 0; k < nip; k++) {
+    double* h = H + (size_t)k * npv;
+    if (type == B200FEM_ELEM_QUADHEX) {
+      // the 14-point rule's coordinates (shape_grads)
+      const double q = 0.758686910639328, r = 0.795822425754222;
+      double x[3] = {0, 0, 0};
+      if (k < 8) {
+        for (int j = 0; j < 3; j++) x[j] = kQhexNode[k][j] * q;
+      } else {
+        x[(k - 8) / 2] = (k % 2 == 0) ? -r : r;
+      }
+      h[0] = 1;
+      h[1] = x[0];
+      h[2] = x[1];
+      h[3] = x[2];
+    } else {
+      const double q = std::sqrt(3 / 5.0), r = k < 3 ? -q : (k < 6 ? q : 0);
+      h[0] = 0.5 * (1 - r);
+      h[1] = 0.5 * (1 + r);
+    }
+  }
+  // M = sum_k H H^T, then W = M^-1 by Gauss-Jordan with partial pivoting
+  double M[16] = {0}, I[16] = {0};
+  for (int k = 0; k < nip; k++)
+    for (int i = 0; i < npv; i++)
+      for (int j = 0; j < npv; j++) M[i * npv + j] += H[k * npv + i] * H[k * npv + j];
+  for (int i = 0; i < npv; i++) I[i * npv + i] = 1;
+  for (int c = 0; c < npv; c++) {
+    int piv = c;
+    for (int r = c + 1; r < npv; r++)
+      if (std::fabs(M[r * npv + c]) > std::fabs(M[piv * npv + c])) piv = r;
+    for (int j = 0; j < npv; j++) {
+      std::swap(M[c * npv + j], M[piv * npv + j]);
+      std::swap(I[c * npv + j], I[piv * npv + j]);
+    }
+    const double d = M[c * npv + c];
+    for (int j = 0; j < npv; j++) {
+      M[c * npv + j] /= d;
+      I[c * npv + j] /= d;
+    }
+    for (int r = 0; r < npv; r++) {
+      if (r == c) continue;
+      const double f = M[r * npv + c];
+      for (int j = 0; j < npv; j++) {
+        M[r * npv + j] -= f * M[c * npv + j];
+        I[r * npv + j] -= f * I[c * npv + j];
+      }
+    }
+  }
+  for (int i = 0; i < npv * npv; i++) W[i] = I[i];
+}
+
 // Shape gradients for integration point k (or the warping point, k = -1).
 void shape_grads(int type, int k, double* g /* nen*3 */, double* w) {
   if (type == B200FEM_ELEM_QUADWEDGE) {
@@ -555,14 +614,12 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   else if ((m.elem_type == B200FEM_ELEM_QUADTET || m.elem_type == B200FEM_ELEM_QUADPYRAMID) &&
            (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
     method = B200FEM_INCOMP_ELEMENT;
+  // quadratic hexes and wedges: their points do not map to nodes either, so
+  // NODAL and AUTO resolve to ELEMENT with QuadhexElement's four and
+  // QuadwedgeElement's two pressure values (:443-445, :267-269)
   else if ((m.elem_type == B200FEM_ELEM_QUADHEX || m.elem_type == B200FEM_ELEM_QUADWEDGE) &&
-           method != B200FEM_INCOMP_OFF) {
-    // QuadhexElement.numPressureVals() == 4 (:443-445), QuadwedgeElement's 2
-    // (:267-269): ELEMENT with an npvals x npvals Rinv per element is not built
-    err = "soft incompressibility of quadratic hexes and wedges (several pressure values per element) is not "
-          "supported";
-    return B200FEM_ERR_UNSUPPORTED;
-  }
+           (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
+    method = B200FEM_INCOMP_ELEMENT;
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
   h.incomp = method;

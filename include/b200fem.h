@@ -260,7 +260,10 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
    WARM_START and ELEM_TILE also afterwards (the step graphs are re-captured). */
 #define B200FEM_OPT_PCG_SPLIT 1  /* 0 auto; 1 contiguous rows per CTA (shared-memory
                                     resident when they fit); 2 strided: every model cut
-                                    into short pieces dealt over all CTAs */
+                                    into short pieces dealt over all CTAs; 3 cluster: one
+                                    thread-block cluster per model, models taken from a
+                                    queue largest first (auto picks it for packs of several
+                                    models that do not fit shared-memory residency) */
 #define B200FEM_OPT_ROW_LANES 2  /* lanes per block row in the iteration SpMV: 0 auto, 4, 8, 16, 32 */
 #define B200FEM_OPT_PCG_CTAS 3   /* CTAs of the persistent PCG kernel: 0 auto (one per SM) */
 #define B200FEM_OPT_PIECE_ROWS 4 /* block rows per piece in the strided split: 0 auto (64) */

@@ -287,7 +287,69 @@ struct ShapeTable {
   std::vector<double> w;    // nip
   std::vector<double> wGNs; // warping point: nen * 3
   double ww;
+  // ELEMENT soft incompressibility: pressure values per element
+  // (FemElement3d.numPressureVals), the pressure weights H of every point
+  // (IntegrationPoint3d.getPressureWeights: nip * npv) and the pressure
+  // weight matrix W = (sum_k H H^T)^-1 (FemElement3d.createPressureWeightMatrix,
+  // FemElement3d.java:226-255)
+  int npv = 1;
+  std::vector<double> H;
+  std::vector<double> W;
 };
+
+// in-place Gauss-Jordan inverse of an n x n matrix (partial pivoting)
+static void invert_small(std::vector<double>& A, int n) {
+  std::vector<double> I((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) I[(size_t)i * n + i] = 1;
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++)
+      if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+    for (int k = 0; k < n; k++) {
+      std::swap(A[(size_t)c * n + k], A[(size_t)piv * n + k]);
+      std::swap(I[(size_t)c * n + k], I[(size_t)piv * n + k]);
+    }
+    const double d = A[(size_t)c * n + c];
+    for (int k = 0; k < n; k++) {
+      A[(size_t)c * n + k] /= d;
+      I[(size_t)c * n + k] /= d;
+    }
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      const double f = A[(size_t)r * n + c];
+      for (int k = 0; k < n; k++) {
+        A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+        I[(size_t)r * n + k] -= f * I[(size_t)c * n + k];
+      }
+    }
+  }
+  A = I;
+}
+
+// pressure weights and weight matrix of a multi-pressure element from its
+// integration-point coordinates: QuadhexElement.getH (1, s, t, r),
+// QuadwedgeElement.getH ((1 - r)/2, (1 + r)/2)
+static void set_pressure_weights(ShapeTable& s, int npv, const double (*ip)[3]) {
+  s.npv = npv;
+  s.H.assign((size_t)s.nip * npv, 0.0);
+  for (int k = 0; k < s.nip; k++) {
+    double* h = &s.H[(size_t)k * npv];
+    if (npv == 4) {
+      h[0] = 1;
+      h[1] = ip[k][0];
+      h[2] = ip[k][1];
+      h[3] = ip[k][2];
+    } else {
+      h[0] = 0.5 * (1 - ip[k][2]);
+      h[1] = 0.5 * (1 + ip[k][2]);
+    }
+  }
+  s.W.assign((size_t)npv * npv, 0.0);
+  for (int k = 0; k < s.nip; k++)
+    for (int i = 0; i < npv; i++)
+      for (int j = 0; j < npv; j++) s.W[(size_t)i * npv + j] += s.H[(size_t)k * npv + i] * s.H[(size_t)k * npv + j];
+  invert_small(s.W, npv);
+}
 
 static ShapeTable make_shape(int type) {
   ShapeTable s;
@@ -311,6 +373,7 @@ static ShapeTable make_shape(int type) {
     s.wGNs.assign(45, 0.0);
     for (int i = 0; i < 6; i++) wedge_dNds(&s.wGNs[i * 3], i, 1 / 3.0, 1 / 3.0, 0);
     s.ww = 1;
+    set_pressure_weights(s, 2, ip);  // QuadwedgeElement.numPressureVals (:267-269)
   } else if (type == ELEM_QUADPYRAMID) {
     s.nen = 13; s.nip = 5;
     // the pyramid's five points (QuadpyramidElement.java:151-165)
@@ -341,6 +404,7 @@ static ShapeTable make_shape(int type) {
     s.wGNs.assign(60, 0.0);
     for (int i = 0; i < 8; i++) hex_dNds(&s.wGNs[i * 3], i, 0, 0, 0);
     s.ww = 1;
+    set_pressure_weights(s, 4, ip);  // QuadhexElement.numPressureVals (:443-445)
   } else if (type == ELEM_QUADTET) {
     s.nen = 10; s.nip = 4;
     // myIntegrationCoords with the reference's rounded constants
@@ -904,6 +968,55 @@ struct ElemOut {
 
 static double current_volume(const Model& m, int e, const double* x);
 
+// ELEMENT soft incompressibility with several pressure values per element
+// (computePressuresAndRinv, FemModel3d.java:2538-2581): per point the
+// Jacobian ratio detJ/detJ0, dV = detJ0 w, pbuf_i = sum_k H_i p(K, J_k) dV,
+// p = W pbuf / V0; Rinv = W K / V0 for the quadratic potential, else
+// Wt R Wt with Wt = W / V0 and R_ij = sum_k H_i H_j modulus(K, J_k) dV
+static void multi_pressures(const Model& m, int e, const double* x, std::vector<double>& pvals,
+                            std::vector<double>& Rinv) {
+  const ShapeTable& s = m.sh;
+  const int nen = m.nen, npv = s.npv;
+  const int* nodes = &m.conn[(size_t)e * nen];
+  const double V0 = m.restVol[e], K = m.mat.kappa;
+  const bool quad = m.mat.bulk_potential == 0;
+  std::vector<double> pbuf(npv, 0.0), R((size_t)npv * npv, 0.0);
+  for (int k = 0; k < s.nip; k++) {
+    double J[9];
+    compute_jacobian(J, &s.GNs[k * nen * 3], nen, x, nodes);
+    const double detJ0 = m.detJ0[(size_t)e * s.nip + k];
+    const double Jk = det3(J) / detJ0;
+    const double dV = detJ0 * s.w[k];
+    const double* H = &s.H[(size_t)k * npv];
+    const double pv = (quad ? K * (Jk - 1) : K * std::log(Jk) / Jk) * dV;
+    for (int i = 0; i < npv; i++) pbuf[i] += H[i] * pv;
+    if (!quad) {
+      const double mod = K * (1 - std::log(Jk)) / (Jk * Jk);
+      for (int i = 0; i < npv; i++)
+        for (int j = 0; j < npv; j++) R[(size_t)i * npv + j] += H[i] * H[j] * mod * dV;
+    }
+  }
+  pvals.assign(npv, 0.0);
+  for (int i = 0; i < npv; i++) {
+    for (int j = 0; j < npv; j++) pvals[i] += s.W[(size_t)i * npv + j] * pbuf[j];
+    pvals[i] /= V0;
+  }
+  Rinv.assign((size_t)npv * npv, 0.0);
+  if (quad) {
+    for (int q = 0; q < npv * npv; q++) Rinv[q] = s.W[q] * (K / V0);
+  } else {
+    std::vector<double> Wt(s.W), RW((size_t)npv * npv, 0.0);
+    for (double& v : Wt) v /= V0;
+    for (int i = 0; i < npv; i++)
+      for (int j = 0; j < npv; j++)
+        for (int l = 0; l < npv; l++) RW[(size_t)i * npv + j] += R[(size_t)i * npv + l] * Wt[(size_t)l * npv + j];
+    for (int i = 0; i < npv; i++)
+      for (int j = 0; j < npv; j++)
+        for (int l = 0; l < npv; l++) Rinv[(size_t)i * npv + j] += Wt[(size_t)i * npv + l] * RW[(size_t)l * npv + j];
+  }
+}
+
+
 static void element_update(const Model& m, int e, const double* x, ElemOut& out) {
   const ShapeTable& s = m.sh;
   int nen = m.nen;
@@ -980,9 +1093,10 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
   // c_i = sum_k GNx_i dv (FemUtilities.addToIncompressConstraints) and the
   // dilational stiffness Rinv c_i c_j^T (:3650-3663)
   const bool elem_inc = m.incomp == INCOMP_ELEMENT;
+  const int npv = s.npv;
   double elem_p = 0, elem_rinv = 0;
-  std::vector<double> cst;
-  if (elem_inc) {
+  std::vector<double> cst, pvals, Rinv;
+  if (elem_inc && npv == 1) {
     const double V0 = m.restVol[e];
     const double Jp = current_volume(m, e, x) / V0;
     const double K = m.mat.kappa;
@@ -990,6 +1104,9 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
     const double keff = (m.mat.bulk_potential == 0) ? K : K * (1 - std::log(Jp)) / (Jp * Jp);
     elem_rinv = keff / V0;
     cst.assign(nen * 3, 0);
+  } else if (elem_inc) {
+    multi_pressures(m, e, x, pvals, Rinv);
+    cst.assign((size_t)nen * 3 * npv, 0);  // node i, row r, pressure value l
   }
   for (int k = 0; k < s.nip; k++) {
     const double* GNs = &s.GNs[k * nen * 3];
@@ -1014,10 +1131,20 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       } else {
         pressure = m.nodePressure[nodes[k]];
       }
-    } else if (elem_inc) {
+    } else if (elem_inc && npv == 1) {
       pressure = elem_p;
       for (int n = 0; n < nen; n++)
         for (int c = 0; c < 3; c++) cst[3 * n + c] += GNx[3 * n + c] * dv;
+    } else if (elem_inc) {
+      // pressure = sum_l H_l p_l at the point (FemModel3d.java:3465-3471);
+      // constraints += H dv GNx (FemUtilities.addToIncompressConstraints)
+      const double* H = &s.H[(size_t)k * npv];
+      for (int l = 0; l < npv; l++) pressure += H[l] * pvals[l];
+      for (int n = 0; n < nen; n++)
+        for (int l = 0; l < npv; l++) {
+          const double hd = H[l] * dv;
+          for (int c = 0; c < 3; c++) cst[((size_t)n * 3 + c) * npv + l] += hd * GNx[3 * n + c];
+        }
     }
     double sig[6], D[36];
     material_stress_tangent(sig, D, m.mat, F, detF, pressure);
@@ -1052,8 +1179,24 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         int bj = m.sidx[nodes[j]];
         if (bj < bi) continue;
         double* Ko = &out.K[(i * nen + j) * 9];
-        for (int r = 0; r < 3; r++)
-          for (int q = 0; q < 3; q++) Ko[3 * r + q] += elem_rinv * cst[3 * i + r] * cst[3 * j + q];
+        if (npv == 1) {
+          for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) Ko[3 * r + q] += elem_rinv * cst[3 * i + r] * cst[3 * j + q];
+        } else {
+          // FemUtilities.addDilationalStiffness (FemUtilities.java:317-342):
+          // X = Rinv GT_j^T, K_ij += GT_i X
+          for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) {
+              double acc = 0;
+              for (int l = 0; l < npv; l++) {
+                double xq = 0;
+                for (int mm = 0; mm < npv; mm++)
+                  xq += Rinv[(size_t)l * npv + mm] * cst[((size_t)j * 3 + q) * npv + mm];
+                acc += cst[((size_t)i * 3 + r) * npv + l] * xq;
+              }
+              Ko[3 * r + q] += acc;
+            }
+        }
       }
     }
   }
@@ -1531,13 +1674,10 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   // (softNodalIncompressAllowed, :400-405): quadratic tets take ELEMENT
   else if ((type == ELEM_QUADTET || type == ELEM_QUADPYRAMID) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
     method = INCOMP_ELEMENT;
-  // QuadhexElement has four pressure values per element (:443-445): the
-  // restatement covers one, so its incompressible forms are refused
-  // (QuadwedgeElement: two, :267-269)
-  else if ((type == ELEM_QUADHEX || type == ELEM_QUADWEDGE) && method != INCOMP_OFF) {
-    delete m;
-    return nullptr;
-  }
+  // quadratic hexes and wedges: their points do not map to nodes, so NODAL
+  // and AUTO resolve to ELEMENT (with four and two pressure values)
+  else if ((type == ELEM_QUADHEX || type == ELEM_QUADWEDGE) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
+    method = INCOMP_ELEMENT;
   else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
   m->incomp = method;
   build_rest_data(*m);
@@ -1851,10 +1991,14 @@ int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv,
     } else {
       pressure = m.nodePressure[nodes[k]];
     }
-  } else if (m.incomp == INCOMP_ELEMENT) {
+  } else if (m.incomp == INCOMP_ELEMENT && s.npv == 1) {
     const double Jp = current_volume(m, e, x) / m.restVol[e];
     const double K = m.mat.kappa;
     pressure = (m.mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
+  } else if (m.incomp == INCOMP_ELEMENT) {
+    std::vector<double> pvals, Rinv;
+    multi_pressures(m, e, x, pvals, Rinv);
+    for (int l = 0; l < s.npv; l++) pressure += s.H[(size_t)k * s.npv + l] * pvals[l];
   }
   material_stress_tangent(sig, D, m.mat, F, detF, pressure);
   return nen;

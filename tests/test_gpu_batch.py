@@ -96,8 +96,8 @@ def test_pack_of_wedges_or_pyramids(b200, oracle, beam):
            mk(StVenantKirchoffMaterial(4e4, 0.3), cells=(5, 2, 3))]
     for w in wls:
         w.build_mesh()
-        if beam in ("quadhex", "quadwedge"):  # several pressure values: compressible forms only
-            w.incomp = L.INCOMP_OFF
+        if beam in ("quadhex", "quadwedge"):  # several pressure values per element
+            w.incomp = L.INCOMP_ELEMENT
     models = []
     for w in wls:
         mdl = w.model()

@@ -36,6 +36,10 @@ def _cases():
         "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
         "neohookean_quadwedge": W.small_quadwedge_beam(NeoHookeanMaterial(5e4, 0.45)),
         "mooneyrivlin_quadpyramid_auto": W.small_quadpyramid_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        # AUTO resolves to ELEMENT with four (quadratic hex) and two
+        # (quadratic wedge) pressure values per element
+        "mooneyrivlin_quadhex_auto": W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_quadwedge_auto": W.small_quadwedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
     }
 
 

@@ -64,6 +64,14 @@ def _cases():
         "neohookean_quadhex": W.small_quadhex_beam(NeoHookeanMaterial(5e4, 0.45)),
         "stvk_quadhex": W.small_quadhex_beam(StVenantKirchoffMaterial(5e4, 0.3)),
         "mooneyrivlin_quadhex_off": W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        # ELEMENT with several pressure values (AUTO resolves to it): quadratic
+        # hexes 4, quadratic wedges 2; QUADRATIC and LOGARITHMIC potentials
+        "mooneyrivlin_quadhex_element": W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_quadhex_element_log": W.small_quadhex_beam(
+            MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
+        "mooneyrivlin_quadwedge_element": W.small_quadwedge_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)),
+        "mooneyrivlin_quadwedge_element_log": W.small_quadwedge_beam(
+            MooneyRivlinMaterial(1037, 0, 0, 486, 0, 10370, 0.0, 1)),
         # quadratic wedges (15 nodes, 9 points) and pyramids (13 nodes, 5 points)
         "linear_corotated_quadwedge": W.small_quadwedge_beam(LinearMaterial(2e4, 0.3, True)),
         "neohookean_quadwedge": W.small_quadwedge_beam(NeoHookeanMaterial(5e4, 0.45)),
@@ -186,7 +194,9 @@ def test_backward_euler_linear_tet_beam(cases, oracle):
                                   "mooneyrivlin_pyramid_element_log", "linear_corotated_quadtet",
                                   "neohookean_quadtet", "stvk_quadtet", "mooneyrivlin_quadtet_element",
                                   "linear_corotated_quadhex", "neohookean_quadhex", "stvk_quadhex",
-                                  "mooneyrivlin_quadhex_off", "linear_corotated_quadwedge",
+                                  "mooneyrivlin_quadhex_off", "mooneyrivlin_quadhex_element",
+                                  "mooneyrivlin_quadhex_element_log", "mooneyrivlin_quadwedge_element",
+                                  "mooneyrivlin_quadwedge_element_log", "linear_corotated_quadwedge",
                                   "neohookean_quadwedge", "linear_corotated_quadpyramid", "stvk_quadpyramid",
                                   "mooneyrivlin_quadpyramid_element"])
 def test_backward_euler_small(name, cases, oracle):
@@ -348,10 +358,13 @@ def test_tet_kernels_agree(name, precision, cases):
     assert rel_err(xs[0], xs[1]) <= (1e-11 if precision == L.PREC_FP64 else 1e-6), rel_err(xs[0], xs[1])
 
 
-def test_quadhex_soft_incompressibility_refused(b200):
-    """QuadhexElement carries four pressure values per element; its soft
-    incompressibility is refused at build with B200FEM_ERR_UNSUPPORTED."""
-    wl = W.small_quadhex_beam(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)).build_mesh()
-    with pytest.raises(L.B200FemError) as ei:
-        _gpu_model(wl).updateStressAndStiffness(wl.rest)
-    assert ei.value.status == L.ERR_UNSUPPORTED
+@pytest.mark.parametrize("maker", [W.small_quadhex_beam, W.small_quadwedge_beam])
+def test_multi_pressure_resolution(b200, oracle, maker):
+    """Quadratic hexes and wedges: AUTO and NODAL resolve to ELEMENT (their
+    points do not map to nodes, FemModel3d.java:462-481), as in the oracle."""
+    wl = maker(MooneyRivlinMaterial(1037, 120, 0, 486, 0, 10370)).build_mesh()
+    for req in (L.INCOMP_AUTO, L.INCOMP_NODAL):
+        wl.incomp = req
+        m = _gpu_model(wl)
+        assert m.getSoftIncompMethod() == L.INCOMP_ELEMENT == oracle_model(oracle, wl).incomp
+        m._invalidate()

@@ -159,7 +159,13 @@ def test_polar_rotation(oracle):
     (1, [5e4, 0.45], 5, 0), (3, [5e4, 0.3], 5, 0), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 5, 0),
     # quadratic wedges (compressible forms) and pyramids (ELEMENT)
     (1, [5e4, 0.45], 6, 0), (3, [5e4, 0.3], 6, 0), (1, [5e4, 0.45], 7, 0), (3, [5e4, 0.3], 7, 0),
-    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 7, 3)])
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 7, 3),
+    # ELEMENT with several pressure values: quadratic hexes (4) and wedges (2),
+    # QUADRATIC bulk potential (with the LOGARITHMIC one the reference's
+    # Rinv = Wt R Wt -- R summed with the point volumes, W without them -- is
+    # not the derivative of its pressures; the GPU parity tests pin it to the
+    # restatement)
+    (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 5, 3), (2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 6, 3)])
 def test_stiffness_matches_force_fd(oracle, kind, params, etype, incomp):
     # (the corotated warped stiffness R K0 R^T omits dR/dx, so it is not an
     # exact derivative by design and is pinned by the GPU parity tests)
@@ -350,6 +356,40 @@ def test_quadhex_shape_functions(oracle):
     assert xyz.shape == (20, 3) and conn.shape == (1, 20)
     m = oracle.OracleModel(5, xyz, conn, np.zeros(20, np.int32), 1, [5e4, 0.3], 1000.0)
     assert abs(m.rest_volumes().sum() - 8.0) <= 1e-13
-    with pytest.raises(ValueError):
-        oracle.OracleModel(5, xyz, conn, np.zeros(20, np.int32), 2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1000.0,
-                           oracle.INCOMP_AUTO)
+
+
+@pytest.mark.parametrize("etype", [5, 6])
+def test_multi_pressure_incompressibility_resolves_to_element(oracle, etype):
+    """Quadratic hexes and wedges: points that do not map to nodes, so AUTO
+    and NODAL resolve to ELEMENT (getAllowedSoftIncompMethod,
+    FemModel3d.java:462-481), with 4 and 2 pressure values."""
+    xyz, conn = oracle.grid(etype, (1.0, 0.4, 0.4), (3, 2, 2))
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    for req in (oracle.INCOMP_AUTO, oracle.INCOMP_NODAL, oracle.INCOMP_ELEMENT):
+        m = oracle.OracleModel(etype, xyz, conn, fixed, 2, [1e4, 2e3, 0, 0, 0, 1e5, 0, 0], 1000.0, req)
+        assert m.incomp == oracle.INCOMP_ELEMENT
+
+
+@pytest.mark.parametrize("etype,nip", [(5, 14), (6, 9)])
+def test_multi_pressure_uniform_dilation(oracle, etype, nip):
+    """A uniform dilation x = s X of one element: every point has J = s^3.
+    The reference's weight matrix W = (sum_k H H^T)^-1 sums the pressure
+    weights without the point weights (FemElement3d.createPressureWeightMatrix,
+    FemElement3d.java:226-255), while p = W (sum_k H p(J) dV) / V0 weights
+    them (FemModel3d.java:2545-2568); for these symmetric rules the pressure
+    at every point comes out as p(J) / nip.  The restatement keeps that, so
+    the virtual work of a uniform expansion d x = eps x is 3 eps V p(J)/nip,
+    and the element's forces sum to zero."""
+    xyz, conn = oracle.grid(etype, (1.0, 1.0, 1.0), (1, 1, 1))
+    kappa = 1e5
+    m = oracle.OracleModel(etype, xyz, conn, np.zeros(len(xyz), np.int32), 2,
+                           [0.0, 0.0, 0, 0, 0, kappa, 0, 0], 1000.0, oracle.INCOMP_ELEMENT)
+    s = 1.01
+    f, K, _ = m.update_stress_stiffness(xyz * s)
+    # MooneyRivlin with c10 = c01 = 0: the stress is the pressure alone
+    assert np.abs(f.sum(axis=0)).max() <= 1e-9 * np.abs(f).max()
+    eps = 1e-6
+    work = (f * (xyz * s * eps)).sum()
+    J = s ** 3
+    V = np.prod(np.ptp(xyz, axis=0)) * J
+    assert abs(work - 3 * eps * V * kappa * (J - 1) / nip) <= 1e-9 * abs(work)
