@@ -777,6 +777,11 @@ int build_pack(Engine& eng) {
   eng.h_col = col;
   eng.h_sidx = sidx;
   eng.h_mass = mass;
+  if (eng.att.active()) {
+    std::string err;
+    const int st = build_attachment_reduction(eng, err);
+    if (st != B200FEM_OK) return fail(&eng, st, err);
+  }
   CK(prepare_kernels(eng));
   CK(prepare_pcg(eng));
   eng.built = true;
@@ -939,6 +944,7 @@ int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double*
   m.conn.assign(conn, conn + (size_t)nen * n_elems);
   m.fixed.assign(n_nodes, 0);
   if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
+  eng.att = FrameAttach();  // attachments name nodes of the previous mesh
   free_pack(eng);
   return B200FEM_OK;
 }
@@ -1163,18 +1169,31 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
   return B200FEM_OK;
 }
 
+// The block pattern the queries report: the solve pattern, or with frame
+// attachments the reduced one (free nodes, then two block rows per frame)
+struct QueryPattern {
+  int rows;
+  const std::vector<int>& rowptr;
+  const std::vector<int>& col;
+};
+static QueryPattern query_pattern(const Engine& eng) {
+  if (eng.att.active()) return {eng.att.n_red, eng.att.rowptr, eng.att.col};
+  return {eng.d.n_rows, eng.h_rowptr, eng.h_col};
+}
+
 int b200fem_get_sizes(b200fem_handle h, int* n_active, int* nnzb, int* crs_full, int* crs_upper) {
   ENG(h);
   NEED_BUILT();
-  if (n_active) *n_active = eng.d.n_rows;
-  if (nnzb) *nnzb = (int)eng.d.nnzb;
-  if (crs_full) *crs_full = (int)(9 * eng.d.nnzb);
+  const QueryPattern qp = query_pattern(eng);
+  if (n_active) *n_active = qp.rows;
+  if (nnzb) *nnzb = (int)qp.col.size();
+  if (crs_full) *crs_full = (int)(9 * qp.col.size());
   if (crs_upper) {
     long long up = 0;
-    for (int r = 0; r < eng.d.n_rows; r++)
-      for (int p = eng.h_rowptr[r]; p < eng.h_rowptr[r + 1]; p++) {
-        if (eng.h_col[p] > r) up += 9;
-        else if (eng.h_col[p] == r) up += 6;
+    for (int r = 0; r < qp.rows; r++)
+      for (int p = qp.rowptr[r]; p < qp.rowptr[r + 1]; p++) {
+        if (qp.col[p] > r) up += 9;
+        else if (qp.col[p] == r) up += 6;
       }
     *crs_upper = (int)up;
   }
@@ -1184,28 +1203,31 @@ int b200fem_get_sizes(b200fem_handle h, int* n_active, int* nnzb, int* crs_full,
 int b200fem_get_solve_index(b200fem_handle h, int* sidx) {
   ENG(h);
   NEED_BUILT();
-  std::copy(eng.h_sidx.begin(), eng.h_sidx.end(), sidx);
+  const std::vector<int>& v = eng.att.active() ? eng.att.sidx : eng.h_sidx;
+  std::copy(v.begin(), v.end(), sidx);
   return B200FEM_OK;
 }
 
 int b200fem_get_pattern(b200fem_handle h, int* rowptr, int* col) {
   ENG(h);
   NEED_BUILT();
-  if (rowptr) std::copy(eng.h_rowptr.begin(), eng.h_rowptr.end(), rowptr);
-  if (col) std::copy(eng.h_col.begin(), eng.h_col.end(), col);
+  const QueryPattern qp = query_pattern(eng);
+  if (rowptr) std::copy(qp.rowptr.begin(), qp.rowptr.end(), rowptr);
+  if (col) std::copy(qp.col.begin(), qp.col.end(), col);
   return B200FEM_OK;
 }
 
 // SparseBlockMatrix.getCRSIndices (SparseBlockMatrix.java:1511-1532) and
 // SparseNumberedBlockMatrix.createCrsBlockSlotMap (:389-498), 0-based
 static int crs_walk(Engine& eng, int partition, int* row_offs, int* col_idx, int* slots) {
+  const QueryPattern qp = query_pattern(eng);
   int nnz = 0;
-  for (int r = 0; r < eng.d.n_rows; r++) {
+  for (int r = 0; r < qp.rows; r++) {
     for (int i = 0; i < 3; i++) {
       int row = 3 * r + i;
       if (row_offs) row_offs[row] = nnz;
-      for (int p = eng.h_rowptr[r]; p < eng.h_rowptr[r + 1]; p++) {
-        int bj = eng.h_col[p];
+      for (int p = qp.rowptr[r]; p < qp.rowptr[r + 1]; p++) {
+        int bj = qp.col[p];
         for (int c = 0; c < 3; c++) {
           int colg = 3 * bj + c;
           if (partition == B200FEM_PART_UPPER && colg < row) {
@@ -1219,7 +1241,7 @@ static int crs_walk(Engine& eng, int partition, int* row_offs, int* col_idx, int
       }
     }
   }
-  if (row_offs) row_offs[3 * eng.d.n_rows] = nnz;
+  if (row_offs) row_offs[3 * qp.rows] = nnz;
   return nnz;
 }
 
@@ -1244,6 +1266,8 @@ int b200fem_get_slot_map(b200fem_handle h, int partition, int* slots) {
 int b200fem_get_scatter_map(b200fem_handle h, int* map) {
   ENG(h);
   NEED_BUILT();
+  if (eng.att.active())
+    return fail(&eng, B200FEM_ERR_UNSUPPORTED, "an attached node's blocks go to several reduced blocks");
   std::copy(eng.h_scatter.begin(), eng.h_scatter.end(), map);
   return B200FEM_OK;
 }
@@ -1313,13 +1337,28 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   CK(launch_assemble(eng, 1.0, 0.0, true));
   CK(launch_forces_only(eng));
+  if (eng.att.active()) CK(launch_attach_reduce(eng));
   CK(cudaEventRecord(eng.ev[1], eng.stream));
   if (f_int)
     CK(cudaMemcpyAsync(f_int, d.fint, 3 * sizeof(double) * (size_t)d.n_nodes, cudaMemcpyDeviceToHost, eng.stream));
-  if (k_blocks)
-    CK(cudaMemcpyAsync(k_blocks, d.K, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
   std::vector<double> kbsr;
-  if (crs_vals && d.S) {
+  if (eng.att.active()) {
+    // the reduced stiffness and its scalar CRS export (reduced pattern)
+    const long long nbr = eng.att.nnzb;
+    if (k_blocks)
+      CK(cudaMemcpyAsync(k_blocks, d.K_red, 9 * sizeof(double) * (size_t)nbr, cudaMemcpyDeviceToHost, eng.stream));
+    if (crs_vals) {
+      if (nbr > 0) {
+        crs_export_kernel_launch(eng, nbr, d.red_row, d.red_rowptr, d.K_red, d.crs_red);
+        CK(cudaGetLastError());
+      }
+      CK(cudaMemcpyAsync(crs_vals, d.crs_red, 9 * sizeof(double) * (size_t)nbr, cudaMemcpyDeviceToHost, eng.stream));
+    }
+  } else if (k_blocks)
+    CK(cudaMemcpyAsync(k_blocks, d.K, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
+  if (eng.att.active()) {
+    // nothing more to export
+  } else if (crs_vals && d.S) {
     CK(launch_crs_export(eng, d.K, d.S));
     CK(cudaMemcpyAsync(crs_vals, d.S, 9 * sizeof(double) * (size_t)d.nnzb, cudaMemcpyDeviceToHost, eng.stream));
     eng.have_matrix = false;  // S was used as scratch
@@ -1395,6 +1434,9 @@ namespace {
 int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, b200fem_stats* stats,
                          double* x_host, double* v_host) {
   if (!p || nsteps < 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid step parameters");
+  if (eng.att.active())
+    return fail(&eng, B200FEM_ERR_UNSUPPORTED,
+                "BackwardEuler with frame attachments: the frames' rigid-body dynamics are not part of the engine");
   if (!(p->h > 0) || !(p->tol > 0) || p->max_iter <= 0)
     return fail(&eng, B200FEM_ERR_INVALID_ARG, "step size, tolerance and max_iter must be positive");
   {
@@ -1546,6 +1588,31 @@ int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, con
   eng.cons_node = cn;
   eng.cons_nrm = cq;
   eng.cons_off = co;
+  return B200FEM_OK;
+}
+
+int b200fem_set_frame_attachments(b200fem_handle h, int n_frames, int n_att, const int* nodes, const int* frames,
+                                  const double* H) {
+  ENG(h);
+  if (n_frames < 0 || n_att < 0 || (n_att > 0 && (!nodes || !frames || !H)) || (n_frames > 0) != (n_att > 0))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid frame attachments");
+  const int N = eng.models[0].n_nodes;
+  std::vector<char> seen(N > 0 ? N : 0, 0);
+  for (int k = 0; k < n_att; k++) {
+    if (nodes[k] < 0 || nodes[k] >= N || frames[k] < 0 || frames[k] >= n_frames)
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "attachment node or frame out of range");
+    if (seen[nodes[k]]) return fail(&eng, B200FEM_ERR_INVALID_ARG, "a node attached twice");
+    seen[nodes[k]] = 1;
+  }
+  if (n_att > 0 && !all_finite(H, 18 * (size_t)n_att))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite attachment block");
+  FrameAttach& A = eng.att;
+  A = FrameAttach();
+  A.n_frames = n_frames;
+  A.node.assign(nodes, nodes + n_att);
+  A.frame.assign(frames, frames + n_att);
+  A.H.assign(H, H + 18 * (size_t)n_att);
+  free_pack(eng);  // the reduced pattern is built with the pack
   return B200FEM_OK;
 }
 

@@ -187,6 +187,19 @@ struct DevPack {
   int* cl_order = nullptr;     // models in queue order
   int* cl_queue = nullptr;     // next queue position (cleared per solve)
   double* row_nrm = nullptr;   // 3 per row: unit normal of the row's plane constraint (zero: none)
+  // frame attachments (attach.cu): attachment of every extended row (-1
+  // free), the attachments' H, the reduced blocks' rows, row offsets and
+  // contribution lists (extended block, parts of T), the reduced K and its
+  // scalar CRS export
+  int* att_row = nullptr;
+  double* att_H = nullptr;
+  int* red_row = nullptr;
+  int* red_rowptr = nullptr;
+  int* red_eptr = nullptr;
+  int* red_ep = nullptr;
+  unsigned char* red_esel = nullptr;
+  double* K_red = nullptr;
+  double* crs_red = nullptr;
   double* row_off = nullptr;   // per row: the plane's offset
   // refinement sweeps: FP64 residual, correction, its PCG results
   double* rref = nullptr;
@@ -203,6 +216,20 @@ struct DevPack {
   unsigned* barrier = nullptr;   // [count, generation]
   int* flags = nullptr;          // [error, inverted count, ...]
   double* dmin = nullptr;        // min detJ (atomically reduced as ordered bits)
+};
+
+// FEM nodes attached to frames (PointFrameAttachment with an active master
+// frame): set by b200fem_set_frame_attachments, reduced by attach.cu
+struct FrameAttach {
+  int n_frames = 0;
+  std::vector<int> node, frame;  // per attachment: the node (model 0) and its frame
+  std::vector<double> H;         // per attachment: the 6x3 master block, row-major
+  bool active() const { return n_frames > 0; }
+  // the reduced system (built with the pack): free active nodes, then two
+  // block rows per frame
+  int n_free = 0, n_red = 0;
+  long long nnzb = 0;
+  std::vector<int> rowptr, col, sidx;
 };
 
 // One element group: contiguous element range with one element type and
@@ -248,6 +275,7 @@ struct Engine {
   int pcg_every_cta_rows = 0;  // every CTA of the PCG split holds at least one piece
   // plane constraints (b200fem_set_plane_constraints): per constrained node
   // its unit normal and offset; enforced by the ConstrainedBackwardEuler step
+  FrameAttach att;  // frame attachments of model 0
   std::vector<int> cons_node;
   std::vector<double> cons_nrm, cons_off;
   int integrator = 0;  // of the captured step graph
@@ -316,6 +344,10 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 // tet_rows.cu
 cudaError_t launch_tet_rows(Engine& eng, bool attr_only);
 
+// attach.cu
+int build_attachment_reduction(Engine& eng, std::string& err);
+cudaError_t launch_attach_reduce(Engine& eng);
+
 // pcg_cluster.cu
 int pcg_cluster_capacity(bool fp32);
 cudaError_t launch_pcg_cluster(Engine& eng, int max_iter, bool update_state, const double* rhs, double* xsol,
@@ -331,6 +363,8 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
 cudaError_t launch_solve(Engine& eng, int max_iter);
 cudaError_t launch_spmv(Engine& eng, const double* x, double* y);
 cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs);
+void crs_export_kernel_launch(Engine& eng, long long nnzb, const int* blk_row, const int* rowptr, const double* vals,
+                              double* crs);
 int read_pcg_result(Engine& eng, b200fem_stats* st);
 
 }  // namespace b200fem

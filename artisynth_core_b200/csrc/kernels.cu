@@ -2171,6 +2171,12 @@ cudaError_t launch_spmv(Engine& eng, const double* x, double* y) {
   return cudaGetLastError();
 }
 
+void crs_export_kernel_launch(Engine& eng, long long nnzb, const int* blk_row, const int* rowptr, const double* vals,
+                              double* crs) {
+  const long long n9 = nnzb * 9;
+  crs_export_kernel<<<(unsigned)((n9 + 255) / 256), 256, 0, eng.stream>>>(nnzb, blk_row, rowptr, vals, crs);
+}
+
 cudaError_t launch_crs_export(Engine& eng, const double* vals, double* crs) {
   DevPack& d = eng.d;
   long long n9 = d.nnzb * 9;

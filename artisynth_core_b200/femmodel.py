@@ -325,6 +325,10 @@ class FemModel3d:
             eng.call("b200fem_set_material", self.material.kind, L.dptr(prm), self.density, self.soft_incomp)
             for k, v in getattr(self, "options", {}).items():
                 eng.call("b200fem_set_option", int(k), int(v))
+            att = getattr(self, "attachments", None)
+            if att is not None:
+                nf, nd, fr, hb = att
+                eng.call("b200fem_set_frame_attachments", nf, int(nd.size), L.iptr(nd), L.iptr(fr), L.dptr(hb))
             eng.call("b200fem_build")
             self._engine = eng
             if self.fext is not None:
@@ -391,6 +395,19 @@ class FemModel3d:
         v = np.zeros(3 * self.numNodes())
         self.engine().call("b200fem_get_state", L.dptr(x), L.dptr(v))
         return x.reshape(-1, 3), v.reshape(-1, 3)
+
+    def setFrameAttachments(self, n_frames, nodes, frames, H):
+        """PointFrameAttachment of `nodes` to active frames (FemModel3d.
+        getGpuNodeReduction, FemModel3d.java:4356-4387): H holds each
+        attachment's 6x3 master block.  The stiffness and pattern queries
+        then describe the reduced system P^T K P over the free nodes and two
+        block rows per frame."""
+        nd = np.ascontiguousarray(np.asarray(nodes, dtype=np.int32).reshape(-1))
+        fr = np.ascontiguousarray(np.asarray(frames, dtype=np.int32).reshape(-1))
+        hb = np.ascontiguousarray(np.asarray(H, dtype=np.float64).reshape(-1))
+        assert hb.size == 18 * nd.size and fr.size == nd.size
+        self.attachments = (int(n_frames), nd, fr, hb)
+        self._invalidate()
 
     def setPlaneConstraints(self, nodes, normals, offsets):
         """ParticlePlaneConstraint on single nodes: node nodes[i] is held on

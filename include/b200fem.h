@@ -202,6 +202,27 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
    correction of a single-particle constraint).  n = 0 removes them. */
 int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, const double* normals,
                                   const double* offsets);
+/* PointFrameAttachment with an active master frame (FemModel3d.
+   getGpuNodeReduction, FemModel3d.java:4356-4387): node nodes[i] of the model
+   (set by b200fem_set_mesh first; not fixed; at most one attachment each)
+   follows frame frames[i] (0 .. n_frames - 1), its velocity v = H_i^T
+   [v_F; w_F] with H_i the attachment's 6x3 master block (18 doubles per
+   attachment, row-major; H = -PointFrameAttachment.getGT(0)).  Attached
+   nodes leave the solve: the stiffness of b200fem_update_stress_stiffness
+   is the reduced P^T K P -- each element block K_ij goes to T_i K_ij T_j^T,
+   T = I for a free node and H for an attached one (the reference's
+   scatterReduced3Block, cudssBridgeKernels.cu:325-365) -- over the free
+   active nodes in node order followed by two 3x3 block rows per frame
+   (translation, rotation: the frame's 6 scalar rows), and the pattern, CRS
+   and solve-index queries describe that reduced system (attached nodes have
+   solve index -1; frame f has block rows n_free + 2f and n_free + 2f + 1).
+   Every frame needs at least one attached node; single-model handles only.
+   The frames' own rigid-body dynamics are not part of the engine, so
+   BackwardEuler steps of a model with attachments return
+   B200FEM_ERR_UNSUPPORTED.  Takes effect at the next b200fem_build;
+   n_frames = n_att = 0 removes them; b200fem_set_mesh clears them. */
+int b200fem_set_frame_attachments(b200fem_handle h, int n_frames, int n_att, const int* nodes, const int* frames,
+                                  const double* H);
 /* nsteps BackwardEuler steps on the device-resident state */
 int b200fem_backward_euler_step(b200fem_handle h, const b200fem_step_params* p, int nsteps,
                                 b200fem_stats* stats);

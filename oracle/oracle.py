@@ -50,8 +50,9 @@ def build_ref(source_root: str | None = None) -> str | None:
 def ref_kernels():
     """ctypes handle of the reference kernels library, or None when it was
     not built.  Entry points used: addMaterialStiffness3_launch
-    (cudssBridgeKernels.cu:244-253), addLinearElasticStiffness3Element_launch
-    (:518-530) and addDilationalStiffness3Element_launch (:725-739)."""
+    (cudssBridgeKernels.cu:244-253), addMaterialStiffness3Element_launch
+    (:436-449), addLinearElasticStiffness3Element_launch (:518-530) and
+    addDilationalStiffness3Element_launch (:725-739)."""
     if not os.path.exists(REF_LIB_PATH):
         return None
     R = ctypes.CDLL(REF_LIB_PATH)
@@ -62,6 +63,8 @@ def ref_kernels():
     R.addLinearElasticStiffness3Element_launch.restype = None
     R.addDilationalStiffness3Element_launch.argtypes = [ctypes.c_int] + [vp] * 12 + [ctypes.c_double, vp, vp]
     R.addDilationalStiffness3Element_launch.restype = None
+    R.addMaterialStiffness3Element_launch.argtypes = [ctypes.c_int] + [vp] * 13 + [ctypes.c_double, vp, vp]
+    R.addMaterialStiffness3Element_launch.restype = None
     return R
 
 
@@ -295,3 +298,59 @@ def polar(F):
     R = np.zeros(9)
     lib().orc_polar(np.ascontiguousarray(F, dtype=np.float64).reshape(-1), R)
     return R.reshape(3, 3)
+
+
+def reduce_attachments(rowptr, col, K, act_node, n_nodes, n_frames, nodes, frames, H):
+    """Master-slave reduction of a stiffness assembled over free and attached
+    nodes (the extended system: rowptr/col/K over block rows whose nodes are
+    act_node) onto the free nodes followed by two block rows per frame
+    (translation, rotation): every block K_ij goes to T_i K_ij T_j^T, T = I
+    for a free node and the attachment's 6x3 master block H for an attached
+    one (scatterReduced3Block, cudssBridgeKernels.cu:325-365;
+    FemModel3d.getGpuNodeReduction, FemModel3d.java:4356-4387).  Blocks of a
+    reduced block are summed in extended-block order.  Returns the reduced
+    rowptr, col, blocks (nnzb, 3, 3) and the per-node reduced solve index
+    (-1 for fixed and attached nodes)."""
+    act_node = np.asarray(act_node)
+    R = act_node.size
+    att_of_node = {int(n): k for k, n in enumerate(nodes)}
+    att_row = np.array([att_of_node.get(int(n), -1) for n in act_node])
+    red_of_row = np.full(R, -1)
+    n_free = 0
+    for r in range(R):
+        if att_row[r] < 0:
+            red_of_row[r] = n_free
+            n_free += 1
+    Hb = np.asarray(H, dtype=np.float64).reshape(-1, 6, 3)
+
+    def targets(r):
+        k = att_row[r]
+        if k < 0:
+            return [(int(red_of_row[r]), np.eye(3))]
+        f = int(frames[k])
+        return [(n_free + 2 * f, Hb[k, 0:3]), (n_free + 2 * f + 1, Hb[k, 3:6])]
+
+    n_red = n_free + 2 * n_frames
+    rows = [dict() for _ in range(n_red)]
+    Kb = np.asarray(K).reshape(-1, 3, 3)
+    for ri in range(R):
+        for p in range(rowptr[ri], rowptr[ri + 1]):
+            rj = col[p]
+            for I, L in targets(ri):
+                T = L @ Kb[p]
+                for J, Rm in targets(rj):
+                    blk = T @ Rm.T
+                    acc = rows[I].get(J)
+                    rows[I][J] = blk if acc is None else acc + blk
+    rp = np.zeros(n_red + 1, dtype=np.int32)
+    cols, blocks = [], []
+    for I in range(n_red):
+        for J in sorted(rows[I]):
+            cols.append(J)
+            blocks.append(rows[I][J])
+        rp[I + 1] = len(cols)
+    sidx = np.full(n_nodes, -1, dtype=np.int32)
+    for r in range(R):
+        if red_of_row[r] >= 0:
+            sidx[act_node[r]] = red_of_row[r]
+    return rp, np.array(cols, dtype=np.int32), np.array(blocks).reshape(-1, 3, 3), sidx
