@@ -140,6 +140,7 @@ def lib():
         "b200fem_backward_euler_step": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_set_plane_constraints": ([H, ctypes.c_int, _ip, _dp, _dp], ctypes.c_int),
         "b200fem_set_frame_attachments": ([H, ctypes.c_int, ctypes.c_int, _ip, _ip, _dp], ctypes.c_int),
+        "b200fem_set_point_constraints": ([H, ctypes.c_int, _ip, _ip, _dp, _dp], ctypes.c_int),
         "b200fem_backward_euler_step_host": ([H, ctypes.POINTER(StepParams), ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.POINTER(Stats)], ctypes.c_int),
         "b200fem_spmv": ([H, _dp, _dp], ctypes.c_int),

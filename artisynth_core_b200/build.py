@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 LIB = os.path.join(HERE, "libb200fem.so")
-SOURCES = ["api.cu", "kernels.cu", "pcg.cu", "pcg_cluster.cu", "tet_rows.cu", "attach.cu", "setup.cpp", "serve.cpp"]
+SOURCES = ["api.cu", "kernels.cu", "pcg.cu", "pcg_cluster.cu", "tet_rows.cu", "attach.cu", "point_cons.cu", "setup.cpp", "serve.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1455,6 +1455,12 @@ int backward_euler_steps(Engine& eng, const b200fem_step_params* p, int nsteps, 
   if (p->integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && !eng.cons_node.empty() && eng.refine_ok &&
       eng.opt_refine > 0)
     return fail(&eng, B200FEM_ERR_UNSUPPORTED, "refinement sweeps with plane constraints");
+  if (p->integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && eng.pcons.active()) {
+    if (!eng.cons_node.empty())
+      return fail(&eng, B200FEM_ERR_UNSUPPORTED, "plane and point constraints in the same step");
+    if (eng.refine_ok && eng.opt_refine > 0)
+      return fail(&eng, B200FEM_ERR_UNSUPPORTED, "refinement sweeps with point constraints");
+  }
   if (p->integrator != eng.integrator) {
     eng.integrator = p->integrator;
     eng.step_exec_max_iter = -1;  // recapture: the constraint arrays are kernel arguments
@@ -1588,6 +1594,58 @@ int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, con
   eng.cons_node = cn;
   eng.cons_nrm = cq;
   eng.cons_off = co;
+  return B200FEM_OK;
+}
+
+int b200fem_set_point_constraints(b200fem_handle h, int n, const int* ptr, const int* nodes, const double* weights,
+                                  const double* targets) {
+  ENG(h);
+  NEED_BUILT();
+  constexpr int kMaxPointConstraints = 32;
+  if (n < 0 || n > kMaxPointConstraints || (n > 0 && (!ptr || !nodes || !weights || !targets)))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "invalid point constraints (at most 32)");
+  DevPack& d = eng.d;
+  PointCons pc;
+  pc.n = n;
+  if (n > 0) {
+    if (ptr[0] != 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "constraint offsets must start at 0");
+    for (int c = 0; c < n; c++)
+      if (ptr[c + 1] <= ptr[c]) return fail(&eng, B200FEM_ERR_INVALID_ARG, "a constraint without points");
+    const int ne = ptr[n];
+    pc.ptr.assign(ptr, ptr + n + 1);
+    pc.node.assign(nodes, nodes + ne);
+    pc.w.assign(weights, weights + ne);
+    pc.target.assign(targets, targets + 3 * (size_t)n);
+    for (int q = 0; q < ne; q++)
+      if (nodes[q] < 0 || nodes[q] >= d.n_nodes)
+        return fail(&eng, B200FEM_ERR_INVALID_ARG, "constraint point out of range");
+    if (!all_finite(weights, ne) || !all_finite(targets, 3 * (size_t)n))
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite constraint weight or target");
+    std::vector<int> row(ne);
+    for (int q = 0; q < ne; q++) row[q] = eng.h_sidx[nodes[q]];
+    if (!d.pc_Y || d.pc_cap < n) {
+      // the largest set so far: room for it once
+      const int m = 3 * n;
+      CK(dalloc(eng, &d.pc_Y, (size_t)m * 3 * d.n_rows));
+      CK(dalloc(eng, &d.pc_rhs, 3 * (size_t)d.n_rows));
+      CK(dalloc(eng, &d.pc_A, (size_t)m * m));
+      CK(dalloc(eng, &d.pc_lam, (size_t)m));
+      d.pc_cap = n;
+    }
+    // small per-set arrays: replaced with the set
+    CK(dalloc(eng, &d.pc_ptr, (size_t)n + 1));
+    CK(dalloc(eng, &d.pc_node, (size_t)ne));
+    CK(dalloc(eng, &d.pc_row, (size_t)ne));
+    CK(dalloc(eng, &d.pc_w, (size_t)ne));
+    CK(dalloc(eng, &d.pc_target, 3 * (size_t)n));
+    CK(cudaMemcpy(d.pc_ptr, ptr, sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.pc_node, nodes, sizeof(int) * ne, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.pc_row, row.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.pc_w, weights, sizeof(double) * ne, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.pc_target, targets, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  }
+  eng.pcons = pc;
+  eng.step_exec_max_iter = -1;  // recapture: the solve path and its arrays change
   return B200FEM_OK;
 }
 

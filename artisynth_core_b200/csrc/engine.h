@@ -193,6 +193,19 @@ struct DevPack {
   // scalar CRS export
   int* att_row = nullptr;
   double* att_H = nullptr;
+  // LinearPointConstraints: constraint offsets, points, their solve rows
+  // (-1 fixed), weights, targets; the Schur-complement solves Y (3 rows per
+  // constraint x 3R), their right-hand side, the dense matrix and vector
+  int* pc_ptr = nullptr;
+  int* pc_node = nullptr;
+  int* pc_row = nullptr;
+  double* pc_w = nullptr;
+  double* pc_target = nullptr;
+  double* pc_Y = nullptr;
+  double* pc_rhs = nullptr;
+  double* pc_A = nullptr;
+  double* pc_lam = nullptr;
+  int pc_cap = 0;  // constraints the device arrays hold
   int* red_row = nullptr;
   int* red_rowptr = nullptr;
   int* red_eptr = nullptr;
@@ -230,6 +243,15 @@ struct FrameAttach {
   int n_free = 0, n_red = 0;
   long long nnzb = 0;
   std::vector<int> rowptr, col, sidx;
+};
+
+// LinearPointConstraints (b200fem_set_point_constraints): constraint c holds
+// sum over q in [ptr[c], ptr[c+1]) of w[q] x[node[q]] at target[3c..3c+2]
+struct PointCons {
+  int n = 0;
+  std::vector<int> ptr, node;
+  std::vector<double> w, target;
+  bool active() const { return n > 0; }
 };
 
 // One element group: contiguous element range with one element type and
@@ -276,6 +298,7 @@ struct Engine {
   // plane constraints (b200fem_set_plane_constraints): per constrained node
   // its unit normal and offset; enforced by the ConstrainedBackwardEuler step
   FrameAttach att;  // frame attachments of model 0
+  PointCons pcons;  // LinearPointConstraints (ConstrainedBackwardEuler)
   std::vector<int> cons_node;
   std::vector<double> cons_nrm, cons_off;
   int integrator = 0;  // of the captured step graph
@@ -343,6 +366,11 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 
 // tet_rows.cu
 cudaError_t launch_tet_rows(Engine& eng, bool attr_only);
+
+// point_cons.cu
+cudaError_t launch_solve_points(Engine& eng, int max_iter);
+// kernels.cu: x += h v, v and its history shifted, for the active rows
+cudaError_t launch_state_update(Engine& eng, const double* vsol);
 
 // attach.cu
 int build_attachment_reduction(Engine& eng, std::string& err);

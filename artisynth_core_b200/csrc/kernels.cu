@@ -1939,7 +1939,18 @@ __global__ void refine_state_kernel(int R, const int* __restrict__ act_node, con
 
 // the solve phase of a BackwardEuler step: PCG, then the refinement sweeps
 // of the mixed form (when asked for and supported) and the state update
+cudaError_t launch_state_update(Engine& eng, const double* vsol) {
+  DevPack& d = eng.d;
+  const int* act = eng.any_inactive ? d.model_active : nullptr;
+  refine_state_kernel<<<(d.n_rows + 127) / 128, 128, 0, eng.stream>>>(d.n_rows, d.act_node, d.row_model, d.step,
+                                                                      vsol, d.x, d.v, d.vprev, d.vprev2, d.vprev3,
+                                                                      d.vprev4, act);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_solve(Engine& eng, int max_iter) {
+  if (eng.pcons.active() && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER)
+    return launch_solve_points(eng, max_iter);
   DevPack& d = eng.d;
   const int sweeps = eng.refine_ok ? eng.opt_refine : 0;
   if (sweeps == 0) return launch_pcg(eng, max_iter, true, 0);

@@ -396,6 +396,17 @@ class FemModel3d:
         self.engine().call("b200fem_get_state", L.dptr(x), L.dptr(v))
         return x.reshape(-1, 3), v.reshape(-1, 3)
 
+    def setPointConstraints(self, ptr, nodes, weights, targets):
+        """LinearPointConstraints: constraint c holds the weighted sum of the
+        positions of nodes[ptr[c]:ptr[c+1]] at targets[c] (enforced by the
+        ConstrainedBackwardEuler integrator)."""
+        pt = np.ascontiguousarray(np.asarray(ptr, dtype=np.int32).reshape(-1))
+        nd = np.ascontiguousarray(np.asarray(nodes, dtype=np.int32).reshape(-1))
+        wt = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+        tg = np.ascontiguousarray(np.asarray(targets, dtype=np.float64).reshape(-1))
+        self.engine().call("b200fem_set_point_constraints", int(pt.size - 1), L.iptr(pt), L.iptr(nd), L.dptr(wt),
+                           L.dptr(tg))
+
     def setFrameAttachments(self, n_frames, nodes, frames, H):
         """PointFrameAttachment of `nodes` to active frames (FemModel3d.
         getGpuNodeReduction, FemModel3d.java:4356-4387): H holds each

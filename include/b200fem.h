@@ -202,6 +202,19 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
    correction of a single-particle constraint).  n = 0 removes them. */
 int b200fem_set_plane_constraints(b200fem_handle h, int n, const int* nodes, const double* normals,
                                   const double* offsets);
+/* LinearPointConstraint (LinearPointConstraint.java), constraints that
+   couple several nodes: constraint c holds sum_q weights[q] x[nodes[q]] at
+   targets[3c .. 3c+2] over q in [ptr[c], ptr[c+1]) (n + 1 offsets from 0; at
+   most 32 constraints; fixed points count in the position but have no
+   velocity rows).  The ConstrainedBackwardEuler integrator solves the KKT
+   velocity system [S G^T; G 0][v; lam] = [b; 0] (zero compliance) by its
+   Schur complement on the device PCG -- 3n + 1 PCG solves per step -- and
+   then applies the GlobalMass position correction (dx = M^-1 G^T mu,
+   (G M^-1 G^T) mu = -(G x - target)); BackwardEuler ignores them.  Not
+   combined with plane constraints in one step.  n = 0 removes them.  Node
+   indices are the handle's (concatenated for a pack). */
+int b200fem_set_point_constraints(b200fem_handle h, int n, const int* ptr, const int* nodes, const double* weights,
+                                  const double* targets);
 /* PointFrameAttachment with an active master frame (FemModel3d.
    getGpuNodeReduction, FemModel3d.java:4356-4387): node nodes[i] of the model
    (set by b200fem_set_mesh first; not fixed; at most one attachment each)

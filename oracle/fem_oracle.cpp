@@ -1955,6 +1955,110 @@ int orc_cbe_step(void* h, double hstep, const double* prm, const double* fext, d
   return 0;
 }
 
+// dense Gaussian elimination with partial pivoting: solves A x = rhs (n x n,
+// row-major, destroyed); returns false for a singular matrix
+static bool dense_gauss(std::vector<double>& A, std::vector<double>& rhs, int n, std::vector<double>& sol) {
+  for (int j = 0; j < n; j++) {
+    int best = j;
+    for (int i = j + 1; i < n; i++)
+      if (std::fabs(A[(size_t)i * n + j]) > std::fabs(A[(size_t)best * n + j])) best = i;
+    if (A[(size_t)best * n + j] == 0) return false;
+    if (best != j) {
+      for (int c = 0; c < n; c++) std::swap(A[(size_t)j * n + c], A[(size_t)best * n + c]);
+      std::swap(rhs[j], rhs[best]);
+    }
+    const double d = A[(size_t)j * n + j];
+    for (int i = j + 1; i < n; i++) {
+      const double f = A[(size_t)i * n + j] / d;
+      if (f == 0) continue;
+      for (int c = j; c < n; c++) A[(size_t)i * n + c] -= f * A[(size_t)j * n + c];
+      rhs[i] -= f * rhs[j];
+    }
+  }
+  sol.assign(n, 0.0);
+  for (int i = n - 1; i >= 0; i--) {
+    double t = rhs[i];
+    for (int c = i + 1; c < n; c++) t -= A[(size_t)i * n + c] * sol[c];
+    sol[i] = t / A[(size_t)i * n + i];
+  }
+  return true;
+}
+
+// One ConstrainedBackwardEuler step (MechSystemSolver.java:4804-4923) with
+// LinearPointConstraints (LinearPointConstraint.java): constraint c holds
+// sum_i w_i x_i = target_c, three rows (x, y, z); the row of axis d carries
+// w_i on the d component of every point with a solve index
+// (addBilateralConstraints).  Velocity: the KKT system [S G^T; G 0][v; lam]
+// = [b; 0] (zero compliance and gdot, setBilateralOffsets :2697-2721),
+// solved densely; x1 = x0 + h v1; then the GlobalMass position correction
+// (applyPosCorrection): with dist = sum_i w_i x_i - target over all points
+// of each constraint (getBilateralInfo), dx = M^-1 G^T mu with
+// (G M^-1 G^T) mu = -dist, on the active nodes.  ptr (ncons + 1) indexes the
+// constraints' points in nodes / w; targets holds 3 values per constraint.
+// Returns 0, or 2 when a system is singular.
+int orc_cbe_step_points(void* h, double hstep, const double* prm, const double* fext, double* x, double* v,
+                        int ncons, const int* ptr, const int* nodes, const double* w, const double* targets) {
+  Model* m = (Model*)h;
+  const int nv = 3 * m->nact;
+  std::vector<double> S, b, vact;
+  be_system(m, hstep, prm, fext, x, v, S, b, vact);
+  const int mc = 3 * ncons, n = nv + mc;
+  std::vector<double> A((size_t)n * n, 0), rhs(n, 0);
+  for (int bi = 0; bi < m->nact; bi++)
+    for (int p = m->rowptr[bi]; p < m->rowptr[bi + 1]; p++) {
+      const int bj = m->col[p];
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) A[(size_t)(3 * bi + r) * n + 3 * bj + c] = S[(size_t)p * 9 + 3 * r + c];
+    }
+  for (int i = 0; i < nv; i++) rhs[i] = b[i];
+  for (int c = 0; c < ncons; c++)
+    for (int q = ptr[c]; q < ptr[c + 1]; q++) {
+      const int bi = m->sidx[nodes[q]];
+      if (bi < 0) continue;
+      for (int d = 0; d < 3; d++) {
+        A[(size_t)(nv + 3 * c + d) * n + 3 * bi + d] += w[q];
+        A[(size_t)(3 * bi + d) * n + nv + 3 * c + d] += w[q];
+      }
+    }
+  std::vector<double> sol;
+  if (!dense_gauss(A, rhs, n, sol)) return 2;
+  for (int nd = 0; nd < m->N; nd++) {
+    const int bi = m->sidx[nd];
+    if (bi < 0) continue;
+    for (int c = 0; c < 3; c++) {
+      v[3 * nd + c] = sol[3 * bi + c];
+      x[3 * nd + c] += hstep * sol[3 * bi + c];
+    }
+  }
+  // GlobalMass position correction
+  std::vector<double> P((size_t)mc * mc, 0), g(mc, 0);
+  for (int c = 0; c < ncons; c++)
+    for (int d = 0; d < 3; d++) {
+      double dist = -targets[3 * c + d];
+      for (int q = ptr[c]; q < ptr[c + 1]; q++) dist += w[q] * x[3 * nodes[q] + d];
+      g[3 * c + d] = -dist;
+    }
+  for (int c = 0; c < ncons; c++)
+    for (int c2 = 0; c2 < ncons; c2++)
+      for (int q = ptr[c]; q < ptr[c + 1]; q++) {
+        if (m->sidx[nodes[q]] < 0) continue;
+        for (int q2 = ptr[c2]; q2 < ptr[c2 + 1]; q2++) {
+          if (nodes[q2] != nodes[q]) continue;
+          const double s = w[q] * w[q2] / m->mass[nodes[q]];
+          for (int d = 0; d < 3; d++) P[(size_t)(3 * c + d) * mc + 3 * c2 + d] += s;
+        }
+      }
+  std::vector<double> mu;
+  if (!dense_gauss(P, g, mc, mu)) return 2;
+  for (int c = 0; c < ncons; c++)
+    for (int q = ptr[c]; q < ptr[c + 1]; q++) {
+      const int nd = nodes[q];
+      if (m->sidx[nd] < 0) continue;
+      for (int d = 0; d < 3; d++) x[3 * nd + d] += w[q] * mu[3 * c + d] / m->mass[nd];
+    }
+  return 0;
+}
+
 int orc_num_ip(void* h) { return ((Model*)h)->sh.nip; }
 
 // Integration point k of element e at positions x (3N), as the non-linear

@@ -108,6 +108,9 @@ def lib():
         L.orc_polar.argtypes = [_dp, _dp]
         L.orc_cbe_step.argtypes = [vp, ctypes.c_double, _dp, ctypes.c_void_p, _dp, _dp, ctypes.c_int, _ip, _dp, _dp]
         L.orc_cbe_step.restype = ctypes.c_int
+        L.orc_cbe_step_points.argtypes = [vp, ctypes.c_double, _dp, ctypes.c_void_p, _dp, _dp, ctypes.c_int, _ip,
+                                          _ip, _dp, _dp]
+        L.orc_cbe_step_points.restype = ctypes.c_int
         L.orc_num_ip.argtypes = [vp]
         L.orc_num_ip.restype = ctypes.c_int
         L.orc_ip_data.argtypes = [vp, _dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_double), _dp, _dp]
@@ -215,6 +218,27 @@ class OracleModel:
         K = np.zeros(9 * self.nnzb)
         ninv = self.L.orc_update_stress_stiffness(self.h, x, f, K)
         return f.reshape(-1, 3), K.reshape(-1, 3, 3), ninv
+
+    def cbe_step_points(self, h, x, v, ptr, nodes, weights, targets, alpha=2.0, beta=0.0, gravity=(0, 0, 0),
+                        fext=None):
+        """One ConstrainedBackwardEuler step with LinearPointConstraints
+        (constraint c: sum of weights[q] * x[nodes[q]] over q in
+        [ptr[c], ptr[c+1]) held at targets[c]); dense KKT velocity solve and
+        GlobalMass position correction; x, v (N,3) updated in place.
+        Returns the status (0 ok)."""
+        xf = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        vf = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        prm = np.array([alpha, beta, *gravity], dtype=np.float64)
+        fe = None if fext is None else np.ascontiguousarray(fext, dtype=np.float64).reshape(-1)
+        pt = np.ascontiguousarray(ptr, dtype=np.int32)
+        nd = np.ascontiguousarray(nodes, dtype=np.int32)
+        wt = np.ascontiguousarray(weights, dtype=np.float64)
+        tg = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        st = self.L.orc_cbe_step_points(self.h, float(h), prm, None if fe is None else fe.ctypes.data, xf, vf,
+                                        int(pt.size - 1), pt, nd, wt, tg)
+        x.reshape(-1)[:] = xf
+        v.reshape(-1)[:] = vf
+        return st
 
     def cbe_step(self, h, x, v, nodes, normals, offsets, alpha=2.0, beta=0.0, gravity=(0, 0, 0), fext=None):
         """One ConstrainedBackwardEuler step with particle-plane constraints
