@@ -243,9 +243,89 @@ def run_reference(args):
                                         f"OpenMP on {used} threads)"}, **cpu_info()),
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        line["reference_device_kernel"] = time_reference_kernel(O, om, wl, x)
+    except Exception as exc:  # no GPU, or the reference kernels were not built
+        line["reference_device_kernel"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def time_reference_kernel(O, om, wl, x, warmup=3, launches=20):
+    """The reference's own device assembly of the stiffness,
+    addMaterialStiffness3Element_launch (cudssBridgeKernels.cu:381-449:
+    one CTA per element, FP64 atomicAdd of B_i^T D B_j dv + (g_i . sigma g_j)
+    dv I into the CRS values), built from the reference source into
+    oracle/_ref, timed with CUDA events on the hex beam at the positions x.
+    Its per-point D, sigma, shape gradients and dv come from the host (here
+    the oracle), as the reference's Java path hands them over: the kernel time
+    covers the block products and the scatter only."""
+    import torch
+    R = O.ref_kernels()
+    if R is None or not torch.cuda.is_available():
+        raise RuntimeError("reference kernels not built or no CUDA device")
+    ne, nen = wl.conn.shape
+    nip = om.num_ip()
+    sidx = om.solve_index()
+    rp, col = om.pattern()
+    _, _, slots = om.crs(0)
+    nrow = rp.size - 1
+    blk_row = np.repeat(np.arange(nrow), np.diff(rp))
+    keys = blk_row.astype(np.int64) * nrow + col
+    grads = np.zeros((ne, nip, nen, 3))
+    Ds = np.zeros((ne, nip, 36))
+    sigs = np.zeros((ne, nip, 6))
+    dvs = np.zeros((ne, nip))
+    for e in range(ne):
+        for k in range(nip):
+            g, dv, sig, D = om.ip_data(x, e, k)
+            grads[e, k] = g
+            Ds[e, k] = D.reshape(-1)
+            sigs[e, k] = sig
+            dvs[e, k] = dv
+    a_idx, b_idx = np.meshgrid(np.arange(nen), np.arange(nen), indexing="ij")
+    pairs_e, pairs_a, pairs_b = [], [], []
+    for e in range(ne):
+        ra, rb = sidx[wl.conn[e, a_idx]], sidx[wl.conn[e, b_idx]]
+        ok = (ra >= 0) & (rb >= 0)
+        pairs_e.append(np.full(ok.sum(), e))
+        pairs_a.append(a_idx[ok])
+        pairs_b.append(b_idx[ok])
+    pe, pa, pb = (np.concatenate(v) for v in (pairs_e, pairs_a, pairs_b))
+    ra = sidx[wl.conn[pe, pa]].astype(np.int64)
+    rb = sidx[wl.conn[pe, pb]].astype(np.int64)
+    blk = np.searchsorted(keys, ra * nrow + rb)
+    assert np.all(keys[blk] == ra * nrow + rb)
+    bslots = np.full((pe.size, 36), -1, dtype=np.int32)
+    bslots[:, :9] = np.asarray(slots, dtype=np.int32).reshape(-1, 9)[blk]
+    poffs = np.concatenate([[0], np.cumsum(np.bincount(pe, minlength=ne))]).astype(np.int32)
+    ints = [np.full(ne, nen, np.int32), (np.arange(ne) * nen).astype(np.int32), poffs,
+            (np.arange(ne + 1) * nip).astype(np.int32), (np.arange(ne) * nip * nen).astype(np.int32),
+            np.stack([pa, pb], axis=1).astype(np.int32).reshape(-1), bslots.reshape(-1),
+            np.full(ne * nen, 3, np.int32)]
+    eye18 = np.tile(np.concatenate([np.eye(3).reshape(-1), np.zeros(9)]), ne * nen)
+    dbls = [eye18, grads.reshape(-1), Ds.reshape(-1), sigs.reshape(-1), dvs.reshape(-1)]
+    nnz = int(np.asarray(slots).max()) + 1
+    dev = torch.device("cuda:0")
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in ints + dbls]
+    out = torch.zeros(nnz, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    for i in range(warmup + launches):
+        out.zero_()
+        ev0.record(stream)
+        R.addMaterialStiffness3Element_launch(ne, *(a.data_ptr() for a in t), 1.0, out.data_ptr(),
+                                              stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if i >= warmup:
+            total += ev0.elapsed_time(ev1)
+    return {"kernel": "addMaterialStiffness3Element_launch (reference source, FP64 atomics)",
+            "workload": "neohookean_hex_beam_40x10x10 stiffness at the last stepped positions",
+            "ms_per_launch": total / launches, "launches": launches, "pairs": int(pe.size),
+            "includes": "block products and CRS scatter; D, sigma, gradients and dv precomputed on the host"}
 
 
 def _rel(a, b):
@@ -666,6 +746,17 @@ def run_b200(args):
     step_ms_max = float(t.item())
     value = world * 1e3 / step_ms_max
 
+    # ---- the drop-in FemModel3d.updateStressAndStiffness on the same beam
+    # (element kernel, FP64 stiffness gather, forces): device time per call,
+    # beside the reference's own device stiffness kernel timed by the
+    # reference arm on this mesh
+    xs_now, _ = m.getState()
+    uss = []
+    for i in range(3 + 20):
+        m.updateStressAndStiffness(xs_now)
+        if i >= 3:
+            uss.append(ms.lastTiming()[0])
+    uss_ms = float(np.mean(uss))
     # ---- end to end through the C ABI with host buffers: every step,
     # b200fem_backward_euler_step_host copies x, v in from pinned host memory,
     # steps, and copies the new x, v back (one synchronisation per call)
@@ -744,6 +835,9 @@ def run_b200(args):
             "gpu_launches": 5 * args.steps,
             "phases_ms_per_step": {"assembly": asm_ms / args.steps, "pcg": pcg_ms / args.steps,
                                    "pcg_iterations": mean_it},
+            "update_stress_stiffness_ms": {"value": uss_ms, "what": "b200fem_update_stress_stiffness device time "
+                                           "(element kernel computing F, sigma, D and blocks, FP64 stiffness "
+                                           "gather, nodal forces) on the hex beam"},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
                          "bytes_per_launch": pcg_bytes if pcg_ms >= asm_ms else asm_b,
