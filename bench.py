@@ -588,6 +588,22 @@ def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=
         err = max(err, _rel(x, xr))
         derr = max(derr, _rel(x - pool[m].rest, xr - pool[m].rest))
     srv.close()
+    # saturation: the same pool and server setup with arrivals at ten times the
+    # offered rate for 10 s -- the completed model steps per second of wall
+    # time is what the server sustains
+    opts = {L.OPT_ROW_LANES: tuned["row_lanes"], L.OPT_ELEM_TILE: tuned["elem_tile"]}
+    sat_srv = NativeServer(pool, budget=60e9, tol=tol, device=dev, options=opts)
+    sat_srv.preload()
+    sat = run_stream_native(sat_srv, poisson_arrivals(rate * 10, 10.0, pool_size, seed=5), steps_per_request,
+                            drain_s=10.0)
+    sat_srv.close()
+    # admission under budget pressure: packs of 64 models and a 1 GB budget
+    # (the pool needs about 3.5 GB), so idle packs are evicted and models
+    # re-admitted from their host-saved states while the stream runs
+    pr_srv = NativeServer(pool, budget=1e9, tol=tol, device=dev, pack_models=64, options=opts)
+    pres = run_stream_native(pr_srv, poisson_arrivals(rate, 10.0, pool_size, seed=6), steps_per_request,
+                             drain_s=20.0)
+    pr_srv.close()
     # the plain FP64 drop-in on the same distribution, one model at a time
     import torch
     from artisynth_core_b200 import _lib as L
@@ -616,6 +632,9 @@ def run_served(dev, seconds=60.0, pool_size=512, rate=2000.0, steps_per_request=
         "plain_fp64_single_model_steps_per_s": plain,
         "speedup_vs_plain_fp64": out["model_steps_per_s"] / plain,
         "plain_fp64_sample": f"{n_plain // steps_per_request} pool models, {steps_per_request} steps each, PCG 1e-10",
+        "saturation": dict({"offered_requests_per_s": rate * 10, "seconds": 10.0}, **sat),
+        "budget_pressure": dict({"budget_bytes": 1e9, "pack_models": 64, "offered_requests_per_s": rate,
+                                 "seconds": 10.0}, **pres),
     })
     return out
 
