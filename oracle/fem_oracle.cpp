@@ -787,8 +787,16 @@ static void add_geometric_stiffness(double* K, const double* gi, const double* s
 // ---------------------------------------------------------------------------
 
 struct Model {
-  int type = ELEM_TET, N = 0, E = 0, nen = 4;
-  ShapeTable sh;
+  int type = ELEM_TET, N = 0, E = 0, nen = 4;  // type and nen of the first element
+  ShapeTable sh;                               // its shape table
+  // per element (a mesh may mix element types): type, first connectivity
+  // entry, first integration point, first linear-cache block; one shape
+  // table per element type present
+  std::vector<int> etype, eoff, ipoff, k0off;
+  std::vector<ShapeTable> shapes;
+  const ShapeTable& shp(int e) const { return shapes[etype[e]]; }
+  int nen_of(int e) const { return shapes[etype[e]].nen; }
+  const int* nodes_of(int e) const { return &conn[eoff[e]]; }
   std::vector<double> rest;
   std::vector<int> conn;
   std::vector<int> sidx;  // solve index (block row) per node, -1 when fixed
@@ -829,23 +837,25 @@ static bool contains_sorted(const std::vector<int>& v, int x) {
 }
 
 static void build_rest_data(Model& m) {
-  const ShapeTable& s = m.sh;
-  m.invJ0.assign((size_t)m.E * s.nip * 9, 0);
-  m.detJ0.assign((size_t)m.E * s.nip, 0);
+  const size_t nips = (size_t)m.ipoff[m.E];
+  m.invJ0.assign(nips * 9, 0);
+  m.detJ0.assign(nips, 0);
   m.winvJ0.assign((size_t)m.E * 9, 0);
   m.restVol.assign(m.E, 0);
   for (int e = 0; e < m.E; e++) {
-    const int* nodes = &m.conn[(size_t)e * m.nen];
+    const ShapeTable& s = m.shp(e);
+    const int nen = s.nen;
+    const int* nodes = m.nodes_of(e);
     double J0[9];
     double vol = 0;
     for (int k = 0; k < s.nip; k++) {
-      compute_jacobian(J0, &s.GNs[k * m.nen * 3], m.nen, m.rest.data(), nodes);
+      compute_jacobian(J0, &s.GNs[k * nen * 3], nen, m.rest.data(), nodes);
       // IntegrationData3d.setRestJacobian (IntegrationData3d.java:108-111)
-      double d = fast_invert(&m.invJ0[((size_t)e * s.nip + k) * 9], J0);
-      m.detJ0[(size_t)e * s.nip + k] = d;
+      double d = fast_invert(&m.invJ0[((size_t)m.ipoff[e] + k) * 9], J0);
+      m.detJ0[(size_t)m.ipoff[e] + k] = d;
       vol += d * s.w[k];
     }
-    if (m.type == ELEM_TET) {
+    if (m.etype[e] == ELEM_TET) {
       // TetElement.computeRestVolumes (TetElement.java:247-254): signed
       // volume of the rest tetrahedron
       const double *p0 = &m.rest[3 * nodes[0]], *p1 = &m.rest[3 * nodes[1]],
@@ -853,10 +863,10 @@ static void build_rest_data(Model& m) {
       double a[9] = {p1[0] - p0[0], p2[0] - p0[0], p3[0] - p0[0], p1[1] - p0[1], p2[1] - p0[1],
                      p3[1] - p0[1], p1[2] - p0[2], p2[2] - p0[2], p3[2] - p0[2]};
       vol = det3(a) / 6;
-      std::memcpy(&m.winvJ0[(size_t)e * 9], &m.invJ0[(size_t)e * 9], 9 * sizeof(double));
+      std::memcpy(&m.winvJ0[(size_t)e * 9], &m.invJ0[(size_t)m.ipoff[e] * 9], 9 * sizeof(double));
     } else {
       // FemElement3d.computeVolumes(rest) (FemElement3d.java:95-130)
-      compute_jacobian(J0, s.wGNs.data(), m.nen, m.rest.data(), nodes);
+      compute_jacobian(J0, s.wGNs.data(), nen, m.rest.data(), nodes);
       fast_invert(&m.winvJ0[(size_t)e * 9], J0);
     }
     m.restVol[e] = vol;
@@ -865,24 +875,25 @@ static void build_rest_data(Model& m) {
   m.mass.assign(m.N, 0);
   for (int e = 0; e < m.E; e++) {
     double rm = m.restVol[e] * m.density;
-    for (int a = 0; a < m.nen; a++) m.mass[m.conn[(size_t)e * m.nen + a]] += rm / m.nen;
+    const int nen = m.nen_of(e);
+    for (int a = 0; a < nen; a++) m.mass[m.nodes_of(e)[a]] += rm / nen;
   }
 }
 
 // LinearMaterialCache.addInitialStiffness (LinearMaterialCache.java:115-160)
 static void build_linear_cache(Model& m) {
-  const ShapeTable& s = m.sh;
-  int nen = m.nen;
-  m.K0.assign((size_t)m.E * nen * nen * 9, 0);
-  m.f0.assign((size_t)m.E * nen * 3, 0);
+  m.K0.assign((size_t)m.k0off[m.E] * 9, 0);
+  m.f0.assign((size_t)m.eoff[m.E] * 3, 0);
   double C[36];
   linear_C(C, m.mat.E, m.mat.nu);
   for (int e = 0; e < m.E; e++) {
-    const int* nodes = &m.conn[(size_t)e * nen];
-    double* K0 = &m.K0[(size_t)e * nen * nen * 9];
+    const ShapeTable& s = m.shp(e);
+    const int nen = s.nen;
+    const int* nodes = m.nodes_of(e);
+    double* K0 = &m.K0[(size_t)m.k0off[e] * 9];
     for (int k = 0; k < s.nip; k++) {
-      const double* invJ0 = &m.invJ0[((size_t)e * s.nip + k) * 9];
-      double dv0 = m.detJ0[(size_t)e * s.nip + k] * 1.0 * s.w[k];
+      const double* invJ0 = &m.invJ0[((size_t)m.ipoff[e] + k) * 9];
+      double dv0 = m.detJ0[(size_t)m.ipoff[e] + k] * 1.0 * s.w[k];
       std::vector<double> GNx0(nen * 3);
       for (int n = 0; n < nen; n++) {
         const double* g = &s.GNs[(k * nen + n) * 3];
@@ -900,7 +911,7 @@ static void build_linear_cache(Model& m) {
         const double* p = &m.rest[3 * nodes[j]];
         for (int r = 0; r < 3; r++) tmp[r] += Kij[3 * r] * p[0] + Kij[3 * r + 1] * p[1] + Kij[3 * r + 2] * p[2];
       }
-      for (int r = 0; r < 3; r++) m.f0[((size_t)e * nen + i) * 3 + r] = tmp[r];
+      for (int r = 0; r < 3; r++) m.f0[((size_t)m.eoff[e] + i) * 3 + r] = tmp[r];
     }
   }
 }
@@ -911,9 +922,10 @@ static void build_pattern(Model& m) {
   // block for each pair with both solve indices != -1.
   m.nbr.assign(m.N, {});
   for (int e = 0; e < m.E; e++) {
-    const int* nodes = &m.conn[(size_t)e * m.nen];
-    for (int a = 0; a < m.nen; a++)
-      for (int b = 0; b < m.nen; b++) m.nbr[nodes[a]].push_back(nodes[b]);
+    const int* nodes = m.nodes_of(e);
+    const int nen = m.nen_of(e);
+    for (int a = 0; a < nen; a++)
+      for (int b = 0; b < nen; b++) m.nbr[nodes[a]].push_back(nodes[b]);
   }
   for (auto& v : m.nbr) {
     std::sort(v.begin(), v.end());
@@ -975,16 +987,16 @@ static double current_volume(const Model& m, int e, const double* x);
 // Wt R Wt with Wt = W / V0 and R_ij = sum_k H_i H_j modulus(K, J_k) dV
 static void multi_pressures(const Model& m, int e, const double* x, std::vector<double>& pvals,
                             std::vector<double>& Rinv) {
-  const ShapeTable& s = m.sh;
-  const int nen = m.nen, npv = s.npv;
-  const int* nodes = &m.conn[(size_t)e * nen];
+  const ShapeTable& s = m.shp(e);
+  const int nen = s.nen, npv = s.npv;
+  const int* nodes = m.nodes_of(e);
   const double V0 = m.restVol[e], K = m.mat.kappa;
   const bool quad = m.mat.bulk_potential == 0;
   std::vector<double> pbuf(npv, 0.0), R((size_t)npv * npv, 0.0);
   for (int k = 0; k < s.nip; k++) {
     double J[9];
     compute_jacobian(J, &s.GNs[k * nen * 3], nen, x, nodes);
-    const double detJ0 = m.detJ0[(size_t)e * s.nip + k];
+    const double detJ0 = m.detJ0[(size_t)m.ipoff[e] + k];
     const double Jk = det3(J) / detJ0;
     const double dV = detJ0 * s.w[k];
     const double* H = &s.H[(size_t)k * npv];
@@ -1018,9 +1030,9 @@ static void multi_pressures(const Model& m, int e, const double* x, std::vector<
 
 
 static void element_update(const Model& m, int e, const double* x, ElemOut& out) {
-  const ShapeTable& s = m.sh;
-  int nen = m.nen;
-  const int* nodes = &m.conn[(size_t)e * nen];
+  const ShapeTable& s = m.shp(e);
+  int nen = s.nen;
+  const int* nodes = m.nodes_of(e);
   out.f.assign(nen * 3, 0);
   out.K.assign(nen * nen * 9, 0);
   out.div.assign(m.incomp == INCOMP_NODAL ? nen * nen * 3 : 0, 0);
@@ -1028,8 +1040,8 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
   out.minDetJ = 1e300;
   if (m.mat.linear()) {
     // linear cached path (FemModel3d.java:3359-3390)
-    const double* K0 = &m.K0[(size_t)e * nen * nen * 9];
-    const double* f0 = &m.f0[(size_t)e * nen * 3];
+    const double* K0 = &m.K0[(size_t)m.k0off[e] * 9];
+    const double* f0 = &m.f0[(size_t)m.eoff[e] * 3];
     double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     if (m.mat.corotated) {
       // StiffnessWarper3d.computeWarpingRotation (StiffnessWarper3d.java:154-159)
@@ -1112,7 +1124,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
     const double* GNs = &s.GNs[k * nen * 3];
     double J[9], invJ[9], F[9];
     compute_jacobian(J, GNs, nen, x, nodes);
-    mul3(F, J, &m.invJ0[((size_t)e * s.nip + k) * 9]);
+    mul3(F, J, &m.invJ0[((size_t)m.ipoff[e] + k) * 9]);
     double detF = det3(F);
     double detJ = fast_invert(invJ, J);
     out.minDetJ = std::min(out.minDetJ, detJ);
@@ -1125,7 +1137,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
     }
     double pressure = 0;
     if (m.incomp == INCOMP_NODAL) {
-      if (m.type == ELEM_TET) {
+      if (m.etype[e] == ELEM_TET) {
         for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
         pressure /= nen;
       } else {
@@ -1164,7 +1176,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         }
       }
     }
-    if (m.incomp == INCOMP_NODAL && m.type != ELEM_TET) {
+    if (m.incomp == INCOMP_NODAL && m.etype[e] != ELEM_TET) {
       // integration points map to nodes (FemModel3d.java:3604-3614):
       // divBlk(node_k, node_j) += dv * GNx_j
       for (int j = 0; j < nen; j++)
@@ -1200,7 +1212,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       }
     }
   }
-  if (m.incomp == INCOMP_NODAL && m.type == ELEM_TET) {
+  if (m.incomp == INCOMP_NODAL && m.etype[e] == ELEM_TET) {
     // TetElement.getAreaWeightedNormals (TetElement.java:333-362) * (-1/12)
     const double *p0 = &x[3 * nodes[0]], *p1 = &x[3 * nodes[1]], *p2 = &x[3 * nodes[2]],
                  *p3 = &x[3 * nodes[3]];
@@ -1222,8 +1234,9 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
 }
 
 static double current_volume(const Model& m, int e, const double* x) {
-  const int* nodes = &m.conn[(size_t)e * m.nen];
-  if (m.type == ELEM_TET) {
+  const int* nodes = m.nodes_of(e);
+  const ShapeTable& s = m.shp(e);
+  if (m.etype[e] == ELEM_TET) {
     const double *p0 = &x[3 * nodes[0]], *p1 = &x[3 * nodes[1]], *p2 = &x[3 * nodes[2]],
                  *p3 = &x[3 * nodes[3]];
     double a[9] = {p1[0] - p0[0], p2[0] - p0[0], p3[0] - p0[0], p1[1] - p0[1], p2[1] - p0[1],
@@ -1231,15 +1244,14 @@ static double current_volume(const Model& m, int e, const double* x) {
     return det3(a) / 6;
   }
   double vol = 0, J[9];
-  for (int k = 0; k < m.sh.nip; k++) {
-    compute_jacobian(J, &m.sh.GNs[k * m.nen * 3], m.nen, x, nodes);
-    vol += det3(J) * m.sh.w[k];
+  for (int k = 0; k < s.nip; k++) {
+    compute_jacobian(J, &s.GNs[k * s.nen * 3], s.nen, x, nodes);
+    vol += det3(J) * s.w[k];
   }
   return vol;
 }
 
 static int update_stress_stiffness(Model& m, const double* x) {
-  int nen = m.nen;
   size_t nnzb = m.col.size();
   m.K.assign(nnzb * 9, 0);
   m.fint.assign((size_t)3 * m.N, 0);
@@ -1250,15 +1262,17 @@ static int update_stress_stiffness(Model& m, const double* x) {
     // updateNodalPressures (FemModel3d.java:2471-2515)
     m.nodeVol.assign(m.N, 0);
     for (int e = 0; e < m.E; e++) {
-      const int* nodes = &m.conn[(size_t)e * nen];
-      if (m.type == ELEM_TET) {
+      const int* nodes = m.nodes_of(e);
+      const ShapeTable& s = m.shp(e);
+      const int nen = s.nen;
+      if (m.etype[e] == ELEM_TET) {
         double vol = current_volume(m, e, x);
         for (int i = 0; i < nen; i++) m.nodeVol[nodes[i]] += vol / 4;
       } else {
         double J[9];
-        for (int k = 0; k < m.sh.nip; k++) {
-          compute_jacobian(J, &m.sh.GNs[k * nen * 3], nen, x, nodes);
-          m.nodeVol[nodes[k]] += det3(J) * m.sh.w[k];
+        for (int k = 0; k < s.nip; k++) {
+          compute_jacobian(J, &s.GNs[k * nen * 3], nen, x, nodes);
+          m.nodeVol[nodes[k]] += det3(J) * s.w[k];
         }
       }
     }
@@ -1285,7 +1299,8 @@ static int update_stress_stiffness(Model& m, const double* x) {
   }
   for (int e = 0; e < m.E; e++) {
     const ElemOut& o = outs[e];
-    const int* nodes = &m.conn[(size_t)e * nen];
+    const int* nodes = m.nodes_of(e);
+    const int nen = m.nen_of(e);
     m.numInverted += o.inverted;
     m.minDetJ = std::min(m.minDetJ, o.minDetJ);
     for (int i = 0; i < nen; i++) {
@@ -1639,17 +1654,41 @@ void orc_jitter(int nx, int ny, int nz, double wx, double wy, double wz, double 
 
 // mat_params: LINEAR {E, nu, corotated}; NEOHOOKEAN {E, nu};
 // MOONEYRIVLIN {c10, c01, c11, c20, c02, kappa, jlimit, bulk_potential}
-void* orc_create(int type, int nnodes, const double* rest, int nelems, const int* conn,
-                 const int* fixed, int mat_kind, const double* mat_params, double density,
-                 int incomp_method) {
+// A mesh of one element type per element (FemModel3d holds any mix of
+// FemElement3d types, FemModel3d.java:3333): types[e], and conn the
+// concatenation of every element's nodes in its type's local order.
+void* orc_create_mixed(int nnodes, const double* rest, int nelems, const int* types, const int* conn,
+                       const int* fixed, int mat_kind, const double* mat_params, double density,
+                       int incomp_method) {
   Model* m = new Model();
-  m->type = type;
-  m->sh = make_shape(type);
+  m->shapes.resize(8);
+  std::vector<char> have(8, 0);
+  m->etype.assign(types, types + nelems);
+  m->eoff.assign(nelems + 1, 0);
+  m->ipoff.assign(nelems + 1, 0);
+  m->k0off.assign(nelems + 1, 0);
+  for (int e = 0; e < nelems; e++) {
+    const int t = types[e];
+    if (t < 0 || t > 7) {
+      delete m;
+      return nullptr;
+    }
+    if (!have[t]) {
+      m->shapes[t] = make_shape(t);
+      have[t] = 1;
+    }
+    const ShapeTable& st = m->shapes[t];
+    m->eoff[e + 1] = m->eoff[e] + st.nen;
+    m->ipoff[e + 1] = m->ipoff[e] + st.nip;
+    m->k0off[e + 1] = m->k0off[e] + st.nen * st.nen;
+  }
+  m->type = nelems > 0 ? types[0] : ELEM_TET;
+  m->sh = m->shapes[m->type];
   m->nen = m->sh.nen;
   m->N = nnodes;
   m->E = nelems;
   m->rest.assign(rest, rest + 3 * (size_t)nnodes);
-  m->conn.assign(conn, conn + (size_t)nelems * m->nen);
+  m->conn.assign(conn, conn + (size_t)m->eoff[nelems]);
   m->sidx.assign(nnodes, -1);
   m->nact = 0;
   for (int n = 0; n < nnodes; n++)
@@ -1666,17 +1705,19 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   }
   m->density = density;
   // FemModel3d.computeStressAndStiffness forces OFF for compressible
-  // materials (:3346-3348); AUTO -> NODAL when #elements > #active nodes
-  // (getAllowedSoftIncompMethod, :462-481).
+  // materials (:3346-3348).  NODAL needs every element to be a tet or to
+  // have its points at its nodes (softNodalIncompressAllowed, :400-405); the
+  // quadratic types are not, so NODAL and AUTO resolve to ELEMENT
+  // (getAllowedSoftIncompMethod, :462-481); otherwise AUTO -> NODAL when
+  // #elements > #active nodes, else ELEMENT.
+  bool nodal_ok = true;
+  for (int e = 0; e < nelems; e++) {
+    const int t = types[e];
+    nodal_ok &= (t == ELEM_TET || t == ELEM_HEX || t == ELEM_WEDGE || t == ELEM_PYRAMID);
+  }
   int method = incomp_method;
   if (!m->mat.incompressible()) method = INCOMP_OFF;
-  // NODAL only for tets and elements whose points map to nodes
-  // (softNodalIncompressAllowed, :400-405): quadratic tets take ELEMENT
-  else if ((type == ELEM_QUADTET || type == ELEM_QUADPYRAMID) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
-    method = INCOMP_ELEMENT;
-  // quadratic hexes and wedges: their points do not map to nodes, so NODAL
-  // and AUTO resolve to ELEMENT (with four and two pressure values)
-  else if ((type == ELEM_QUADHEX || type == ELEM_QUADWEDGE) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
+  else if (!nodal_ok && (method == INCOMP_NODAL || method == INCOMP_AUTO))
     method = INCOMP_ELEMENT;
   else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
   m->incomp = method;
@@ -1686,17 +1727,26 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
   if (m->incomp == INCOMP_NODAL) {
     m->nodeRestVol.assign(m->N, 0);
     for (int e = 0; e < m->E; e++) {
-      const int* nodes = &m->conn[(size_t)e * m->nen];
-      if (type == ELEM_TET) {
+      const int* nodes = m->nodes_of(e);
+      const ShapeTable& st = m->shp(e);
+      if (m->etype[e] == ELEM_TET) {
         for (int i = 0; i < 4; i++) m->nodeRestVol[nodes[i]] += m->restVol[e] / 4;
       } else {
         // integration points map to nodes (FemModel3d.java:2608-2614)
-        for (int i = 0; i < m->nen; i++)
-          m->nodeRestVol[nodes[i]] += m->sh.w[i] * m->detJ0[(size_t)e * m->nen + i];
+        for (int i = 0; i < st.nen; i++)
+          m->nodeRestVol[nodes[i]] += st.w[i] * m->detJ0[(size_t)m->ipoff[e] + i];
       }
     }
   }
   return m;
+}
+
+void* orc_create(int type, int nnodes, const double* rest, int nelems, const int* conn,
+                 const int* fixed, int mat_kind, const double* mat_params, double density,
+                 int incomp_method) {
+  std::vector<int> types(nelems, type);
+  return orc_create_mixed(nnodes, rest, nelems, types.data(), conn, fixed, mat_kind, mat_params, density,
+                          incomp_method);
 }
 
 void orc_destroy(void* h) { delete (Model*)h; }
@@ -2060,6 +2110,7 @@ int orc_cbe_step_points(void* h, double hstep, const double* prm, const double* 
 }
 
 int orc_num_ip(void* h) { return ((Model*)h)->sh.nip; }
+int orc_elem_num_ip(void* h, int e) { return ((Model*)h)->shp(e).nip; }
 
 // Integration point k of element e at positions x (3N), as the non-linear
 // element loop forms it (FemModel3d.java:3443-3470): shape gradients in the
@@ -2072,14 +2123,15 @@ int orc_num_ip(void* h) { return ((Model*)h)->sh.nip; }
 // stiffness) and out-of-range e or k.
 int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv, double* sig, double* D) {
   const Model& m = *(const Model*)h;
-  const ShapeTable& s = m.sh;
-  if (m.mat.linear() || e < 0 || e >= m.E || k < 0 || k >= s.nip) return -1;
-  const int nen = m.nen;
-  const int* nodes = &m.conn[(size_t)e * nen];
+  if (m.mat.linear() || e < 0 || e >= m.E) return -1;
+  const ShapeTable& s = m.shp(e);
+  if (k < 0 || k >= s.nip) return -1;
+  const int nen = s.nen;
+  const int* nodes = m.nodes_of(e);
   const double* GNs = &s.GNs[k * nen * 3];
   double J[9], invJ[9], F[9];
   compute_jacobian(J, GNs, nen, x, nodes);
-  mul3(F, J, &m.invJ0[((size_t)e * s.nip + k) * 9]);
+  mul3(F, J, &m.invJ0[((size_t)m.ipoff[e] + k) * 9]);
   const double detF = det3(F);
   const double detJ = fast_invert(invJ, J);
   *dv = detJ * s.w[k];
@@ -2089,7 +2141,7 @@ int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv,
   }
   double pressure = 0;
   if (m.incomp == INCOMP_NODAL && !m.nodePressure.empty()) {
-    if (m.type == ELEM_TET) {
+    if (m.etype[e] == ELEM_TET) {
       for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
       pressure /= nen;
     } else {

@@ -85,6 +85,11 @@ def lib():
         L.orc_create.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip,
                                  ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int]
         L.orc_create.restype = vp
+        L.orc_create_mixed.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, ctypes.c_int, _dp,
+                                       ctypes.c_double, ctypes.c_int]
+        L.orc_create_mixed.restype = vp
+        L.orc_elem_num_ip.argtypes = [vp, ctypes.c_int]
+        L.orc_elem_num_ip.restype = ctypes.c_int
         L.orc_destroy.argtypes = [vp]
         for name in ("orc_incomp_method", "orc_num_active", "orc_nnzb"):
             getattr(L, name).argtypes = [vp]
@@ -157,20 +162,31 @@ class OracleModel:
 
     def __init__(self, elem_type, rest, conn, fixed, mat_kind, mat_params, density,
                  incomp=INCOMP_AUTO):
+        """elem_type: one type for every element (conn: E x nen), or a
+        sequence with each element's type (conn: the elements' nodes
+        concatenated) for a mesh that mixes element types."""
         self.L = lib()
-        self.elem_type = elem_type
         self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1)
         self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
         self.N = self.rest.size // 3
-        nen = ELEM_NODES[elem_type]
-        self.E = self.conn.size // nen
         fx = np.ascontiguousarray(fixed, dtype=np.int32)
         mp = np.zeros(8)
         mp[: len(mat_params)] = mat_params
-        self.h = self.L.orc_create(elem_type, self.N, self.rest, self.E, self.conn, fx, mat_kind, mp,
-                                   float(density), incomp)
+        if np.ndim(elem_type) == 0:
+            self.elem_type = int(elem_type)
+            self.types = None
+            self.E = self.conn.size // ELEM_NODES[self.elem_type]
+            self.h = self.L.orc_create(self.elem_type, self.N, self.rest, self.E, self.conn, fx, mat_kind, mp,
+                                       float(density), incomp)
+        else:
+            self.types = np.ascontiguousarray(elem_type, dtype=np.int32)
+            self.elem_type = int(self.types[0])
+            self.E = self.types.size
+            assert self.conn.size == sum(ELEM_NODES[int(t)] for t in self.types)
+            self.h = self.L.orc_create_mixed(self.N, self.rest, self.E, self.types, self.conn, fx, mat_kind, mp,
+                                             float(density), incomp)
         if not self.h:
-            raise ValueError("the oracle refuses this model (quadratic hexes with soft incompressibility)")
+            raise ValueError("the oracle refuses this model (unknown element type)")
         self.nact = self.L.orc_num_active(self.h)
         self.nnzb = self.L.orc_nnzb(self.h)
         self.incomp = self.L.orc_incomp_method(self.h)
@@ -257,14 +273,15 @@ class OracleModel:
         v.reshape(-1)[:] = vf
         return st
 
-    def num_ip(self):
-        return self.L.orc_num_ip(self.h)
+    def num_ip(self, e=None):
+        """Integration points of element e (default: of the first element)."""
+        return self.L.orc_num_ip(self.h) if e is None else self.L.orc_elem_num_ip(self.h, int(e))
 
     def ip_data(self, x, e, k):
         """(GNx (nen,3), dv, sig (6), D (6,6)) of integration point k of
         element e at positions x (non-linear materials)."""
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
-        nen = ELEM_NODES[self.elem_type]
+        nen = ELEM_NODES[self.elem_type if self.types is None else int(self.types[e])]
         g = np.zeros(3 * nen)
         dv = ctypes.c_double()
         sig = np.zeros(6)
@@ -378,3 +395,28 @@ def reduce_attachments(rowptr, col, K, act_node, n_nodes, n_frames, nodes, frame
         if red_of_row[r] >= 0:
             sidx[act_node[r]] = red_of_row[r]
     return rp, np.array(cols, dtype=np.int32), np.array(blocks).reshape(-1, 3, 3), sidx
+
+
+def mixed_grid(widths, cells, jitter=0.0, seed=0, split=(1 / 3, 2 / 3), kinds=(ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID)):
+    """A structured grid whose cells are hexes, wedges or pyramids by the x
+    position of the cell (FemFactory's hex, wedge and pyramid grids share
+    their node lattice): cells left of split[0] of the length take kinds[0],
+    cells up to split[1] kinds[1], the rest kinds[2].  Returns the nodes, the
+    per-element types and the concatenated connectivity (element order: the
+    first kind's elements, then the second's, then the third's, each in its
+    grid's order)."""
+    xyz = None
+    types, conn = [], []
+    x0 = -widths[0] / 2
+    bounds = [x0 + split[0] * widths[0], x0 + split[1] * widths[0]]
+    for idx, kind in enumerate(kinds):
+        g, c = grid(kind, widths, cells, jitter, seed)
+        if xyz is None:
+            xyz = g
+        cx = g[c, 0].mean(axis=1)
+        lo = -np.inf if idx == 0 else bounds[idx - 1]
+        hi = np.inf if idx == 2 else bounds[idx]
+        sel = (cx >= lo) & (cx < hi)
+        types += [kind] * int(sel.sum())
+        conn.append(c[sel].reshape(-1))
+    return xyz, np.array(types, dtype=np.int32), np.concatenate(conn).astype(np.int32)
