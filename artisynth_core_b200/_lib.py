@@ -123,6 +123,7 @@ def lib():
         "b200fem_quadratic_tet_mesh": ([ctypes.c_int, _dp, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_int), _dp, _ip],
                                        ctypes.c_int),
         "b200fem_set_mesh": ([H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip], ctypes.c_int),
+        "b200fem_set_mesh_mixed": ([H, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip], ctypes.c_int),
         "b200fem_set_material": ([H, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "b200fem_build": ([H], ctypes.c_int),
         "b200fem_get_sizes": ([H, _ip, _ip, _ip, _ip], ctypes.c_int),

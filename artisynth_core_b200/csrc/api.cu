@@ -95,10 +95,7 @@ int build_pack(Engine& eng) {
   free_pack(eng);
   const int M = (int)eng.models.size();
   if (M == 0) return fail(&eng, B200FEM_ERR_STATE, "no model defined");
-  eng.elem_type = eng.models[0].elem_type;
   for (auto& m : eng.models) {
-    if (m.elem_type != eng.elem_type)
-      return fail(&eng, B200FEM_ERR_UNSUPPORTED, "all models of a pack must use one element type");
     if (!m.has_material) return fail(&eng, B200FEM_ERR_STATE, "material not set");
     if (m.n_nodes <= 0 || m.n_elems <= 0) return fail(&eng, B200FEM_ERR_STATE, "mesh not set");
   }
@@ -108,7 +105,17 @@ int build_pack(Engine& eng) {
     int st = setup_model_host(eng.models[m], eng.hosts[m], err);
     if (st != B200FEM_OK) return fail(&eng, st, "model " + std::to_string(m) + ": " + err);
   }
-  const int nen = eng.hosts[0].nen, nip = eng.hosts[0].nip, npair = eng.hosts[0].npair;
+  // pack-wide element type: one type, or kElemMixed
+  eng.elem_type = eng.hosts[0].stype.empty() ? B200FEM_ELEM_TET : eng.hosts[0].stype[0];
+  eng.nen_max = 0;
+  for (auto& h : eng.hosts)
+    for (int t : h.stype) {
+      if (t != eng.elem_type) eng.elem_type = kElemMixed;
+      eng.nen_max = std::max(eng.nen_max, elem_nen(t));
+    }
+  const bool mixed = eng.elem_type == kElemMixed;
+  const int nen = mixed ? 0 : elem_nen(eng.elem_type), nip = mixed ? 0 : elem_nip(eng.elem_type);
+  const int npair = nen * (nen + 1) / 2;
   eng.nen = nen;
   eng.nip = nip;
   eng.npair = npair;
@@ -125,7 +132,31 @@ int build_pack(Engine& eng) {
   }
   const int N = eng.node_off[M], E = eng.elem_off[M], R = eng.row_off[M];
   const long long NB = eng.blk_off[M];
-  if (NB >= (1ll << 31) || (long long)E * npair * 2 >= (1ll << 31))
+  // element layout of the pack in storage order (each model's elements
+  // sorted by type): per element its type and the offsets of its node
+  // slots, integration points, upper-triangle pairs, nen x nen entries and
+  // pressure values; st_of maps the callers' element order to storage order
+  std::vector<int> etype(E), st_of(E);
+  std::vector<long long> coff(E + 1, 0), ipoff(E + 1, 0), proff(E + 1, 0), sqoff(E + 1, 0), pvoff(E + 1, 0),
+      pv2off(E + 1, 0);
+  for (int m = 0; m < M; m++) {
+    const ModelHost& h = eng.hosts[m];
+    const int eo = eng.elem_off[m];
+    for (int s = 0; s < eng.models[m].n_elems; s++) {
+      etype[eo + s] = h.stype[s];
+      st_of[eo + h.perm[s]] = eo + s;
+    }
+  }
+  for (int e = 0; e < E; e++) {
+    const int t = etype[e], k = elem_nen(t), v = elem_npv(t);
+    coff[e + 1] = coff[e] + k;
+    ipoff[e + 1] = ipoff[e] + elem_nip(t);
+    proff[e + 1] = proff[e] + k * (k + 1) / 2;
+    sqoff[e + 1] = sqoff[e] + (long long)k * k;
+    pvoff[e + 1] = pvoff[e] + v;
+    pv2off[e + 1] = pv2off[e] + v * v;
+  }
+  if (NB >= (1ll << 31) || proff[E] * 2 >= (1ll << 31) || coff[E] >= (1ll << 31))
     return fail(&eng, B200FEM_ERR_UNSUPPORTED, "pack too large for 32-bit block indices");
   DevPack& d = eng.d;
   d.n_models = M;
@@ -137,15 +168,15 @@ int build_pack(Engine& eng) {
   // ---- host arrays
   std::vector<double> x(3 * (size_t)N), mass(N), mat((size_t)M * kMatParams, 0.0), step((size_t)M * 8, 0.0);
   std::vector<int> node_model(N), sidx(N), act_node(R), row_model(R);
-  std::vector<int> conn((size_t)E * nen), elem_model(E);
-  std::vector<double> invJ0((size_t)E * nip * 9), winvJ0((size_t)E * 9);
+  std::vector<int> conn((size_t)coff[E]), elem_model(E);
+  std::vector<double> invJ0((size_t)ipoff[E] * 9), winvJ0((size_t)E * 9);
   bool any_linear = false, any_nodal = false;
   for (auto& m : eng.models) any_linear |= (m.mat_kind == B200FEM_MAT_LINEAR);
   for (auto& h : eng.hosts) any_nodal |= (h.incomp == B200FEM_INCOMP_NODAL);
   std::vector<double> K0, f0, node_rest_vol;
   if (any_linear) {
-    K0.assign((size_t)E * nen * nen * 9, 0.0);
-    f0.assign((size_t)E * nen * 3, 0.0);
+    K0.assign((size_t)sqoff[E] * 9, 0.0);
+    f0.assign((size_t)coff[E] * 3, 0.0);
   }
   if (any_nodal) node_rest_vol.assign(N, 1.0);
   std::vector<int> rowptr(R + 1, 0), col(NB), blk_diag(R), blk_row(NB);
@@ -170,13 +201,13 @@ int build_pack(Engine& eng) {
         if (h.col[p] == r) blk_diag[ro + r] = (int)(bo + p);
       }
     }
-    for (size_t q = 0; q < (size_t)md.n_elems * nen; q++) conn[(size_t)eo * nen + q] = no + md.conn[q];
+    for (size_t q = 0; q < h.sconn.size(); q++) conn[(size_t)coff[eo] + q] = no + h.sconn[q];
     for (int e = 0; e < md.n_elems; e++) elem_model[eo + e] = m;
-    std::copy(h.invJ0.begin(), h.invJ0.end(), invJ0.begin() + (size_t)eo * nip * 9);
+    std::copy(h.invJ0.begin(), h.invJ0.end(), invJ0.begin() + (size_t)ipoff[eo] * 9);
     std::copy(h.winvJ0.begin(), h.winvJ0.end(), winvJ0.begin() + (size_t)eo * 9);
     if (!h.K0.empty()) {
-      std::copy(h.K0.begin(), h.K0.end(), K0.begin() + (size_t)eo * nen * nen * 9);
-      std::copy(h.f0.begin(), h.f0.end(), f0.begin() + (size_t)eo * nen * 3);
+      std::copy(h.K0.begin(), h.K0.end(), K0.begin() + (size_t)sqoff[eo] * 9);
+      std::copy(h.f0.begin(), h.f0.end(), f0.begin() + (size_t)coff[eo] * 3);
     }
     if (!h.node_rest_vol.empty())
       std::copy(h.node_rest_vol.begin(), h.node_rest_vol.end(), node_rest_vol.begin() + no);
@@ -185,23 +216,26 @@ int build_pack(Engine& eng) {
     step[(size_t)m * 8 + 1] = 2.0;
     step[(size_t)m * 8 + 6] = 1e-10;
   }
-  // ---- element-to-block scatter map and per-block contribution lists
+  // ---- element-to-block scatter map (storage order, sqoff) and per-block
+  // contribution lists; the lists follow the callers' element order, the
+  // order in which the reference accumulates the element blocks
   auto block_of = [&](int r, int c) -> int {
     auto b = col.begin() + rowptr[r], e = col.begin() + rowptr[r + 1];
     auto it = std::lower_bound(b, e, c);
     return (it != e && *it == c) ? (int)(it - col.begin()) : -1;
   };
-  eng.h_scatter.assign((size_t)E * nen * nen, -1);
+  std::vector<int> scat((size_t)sqoff[E], -1);
   std::vector<int> cptr(NB + 1, 0);
   for (int e = 0; e < E; e++) {
-    const int* nodes = &conn[(size_t)e * nen];
-    for (int a = 0; a < nen; a++)
-      for (int b = 0; b < nen; b++) {
+    const int* nodes = &conn[(size_t)coff[e]];
+    const int k = elem_nen(etype[e]);
+    for (int a = 0; a < k; a++)
+      for (int b = 0; b < k; b++) {
         int ra = sidx[nodes[a]], rb = sidx[nodes[b]];
         if (ra < 0 || rb < 0) continue;
         int p = block_of(ra, rb);
         if (p < 0) return fail(&eng, B200FEM_ERR_STATE, "internal: element pair outside the pattern");
-        eng.h_scatter[((size_t)e * nen + a) * nen + b] = p;
+        scat[(size_t)sqoff[e] + a * k + b] = p;
         cptr[p + 1]++;
       }
   }
@@ -209,51 +243,86 @@ int build_pack(Engine& eng) {
   std::vector<int> cidx(cptr[NB]);
   {
     std::vector<int> fill(cptr.begin(), cptr.end() - 1);
-    for (int e = 0; e < E; e++) {
+    for (int o = 0; o < E; o++) {
+      const int e = st_of[o], k = elem_nen(etype[e]);
       int w = 0;
-      for (int a = 0; a < nen; a++)
-        for (int b = a; b < nen; b++, w++) {
-          int pab = eng.h_scatter[((size_t)e * nen + a) * nen + b];
+      for (int a = 0; a < k; a++)
+        for (int b = a; b < k; b++, w++) {
+          int pab = scat[(size_t)sqoff[e] + a * k + b];
           if (pab < 0) continue;
-          int code = (int)(((long long)e * npair + w) << 1);
+          int code = (int)((proff[e] + w) << 1);
           cidx[fill[pab]++] = code;  // K_ab at (a, b)
           if (a != b) {
-            int pba = eng.h_scatter[((size_t)e * nen + b) * nen + a];
+            int pba = scat[(size_t)sqoff[e] + b * k + a];
             cidx[fill[pba]++] = code | 1;  // K_ab^T at (b, a)
           }
         }
     }
   }
-  // node -> element incidences in element order
+  // the scatter map in the callers' element order (b200fem_get_scatter_map)
+  if (!mixed) {
+    eng.h_scatter.swap(scat);
+  } else {
+    eng.h_scatter.clear();
+    eng.h_scatter.reserve(scat.size());
+    for (int o = 0; o < E; o++) {
+      const int e = st_of[o];
+      eng.h_scatter.insert(eng.h_scatter.end(), scat.begin() + sqoff[e], scat.begin() + sqoff[e + 1]);
+    }
+    std::vector<int>().swap(scat);
+  }
+  // node -> element incidences in the callers' element order: the node slot
+  // (inc_idx), the storage element, and for mixed packs (type << 8) | local node
   std::vector<int> iptr(N + 1, 0);
   for (size_t q = 0; q < conn.size(); q++) iptr[conn[q] + 1]++;
   for (int n = 0; n < N; n++) iptr[n + 1] += iptr[n];
-  std::vector<int> iidx(conn.size());
+  std::vector<int> iidx(conn.size()), ielem(conn.size()), itl;
+  if (mixed) itl.resize(conn.size());
   {
     std::vector<int> fill(iptr.begin(), iptr.end() - 1);
-    for (int e = 0; e < E; e++)
-      for (int a = 0; a < nen; a++) iidx[fill[conn[(size_t)e * nen + a]]++] = e * nen + a;
-  }
-  // ---- element groups (runs of models with one material kind)
-  eng.groups.clear();
-  for (int m = 0; m < M; m++) {
-    ElemGroup g;
-    g.e0 = eng.elem_off[m];
-    g.e1 = eng.elem_off[m + 1];
-    g.elem_type = eng.elem_type;
-    g.mat_kind = eng.models[m].mat_kind;
-    g.corotated = (g.mat_kind == B200FEM_MAT_LINEAR) ? (eng.models[m].mat_params[2] != 0) : 0;
-    g.nodal = eng.hosts[m].incomp == B200FEM_INCOMP_NODAL;
-    g.elem_inc = eng.hosts[m].incomp == B200FEM_INCOMP_ELEMENT;
-    if (!eng.groups.empty()) {
-      ElemGroup& last = eng.groups.back();
-      if (last.mat_kind == g.mat_kind && last.corotated == g.corotated && last.nodal == g.nodal &&
-          last.elem_inc == g.elem_inc && last.e1 == g.e0) {
-        last.e1 = g.e1;
-        continue;
+    for (int o = 0; o < E; o++) {
+      const int e = st_of[o], k = elem_nen(etype[e]);
+      for (int a = 0; a < k; a++) {
+        const int q = fill[conn[(size_t)coff[e] + a]]++;
+        iidx[q] = (int)coff[e] + a;
+        ielem[q] = e;
+        if (mixed) itl[q] = (etype[e] << 8) | a;
       }
     }
-    eng.groups.push_back(g);
+  }
+  // ---- element groups: runs of one element type, material kind and soft
+  // incompressibility (a model of several types gives one run per type)
+  eng.groups.clear();
+  for (int m = 0; m < M; m++) {
+    const ModelHost& h = eng.hosts[m];
+    for (size_t k = 0; k + 1 < h.sec.size(); k++) {
+      ElemGroup g;
+      g.e0 = eng.elem_off[m] + h.sec[k];
+      g.e1 = eng.elem_off[m] + h.sec[k + 1];
+      if (g.e1 <= g.e0) continue;
+      g.elem_type = etype[g.e0];
+      g.mat_kind = eng.models[m].mat_kind;
+      g.corotated = (g.mat_kind == B200FEM_MAT_LINEAR) ? (eng.models[m].mat_params[2] != 0) : 0;
+      g.nodal = h.incomp == B200FEM_INCOMP_NODAL;
+      g.elem_inc = h.incomp == B200FEM_INCOMP_ELEMENT;
+      if (!eng.groups.empty()) {
+        ElemGroup& last = eng.groups.back();
+        if (last.elem_type == g.elem_type && last.mat_kind == g.mat_kind && last.corotated == g.corotated &&
+            last.nodal == g.nodal && last.elem_inc == g.elem_inc && last.e1 == g.e0) {
+          last.e1 = g.e1;
+          continue;
+        }
+      }
+      eng.groups.push_back(g);
+    }
+  }
+  for (ElemGroup& g : eng.groups) {
+    g.c0 = coff[g.e0];
+    g.ip0 = ipoff[g.e0];
+    g.pr0 = proff[g.e0];
+    g.sq0 = sqoff[g.e0];
+    g.pv0 = pvoff[g.e0];
+    g.pv20 = pv2off[g.e0];
   }
   // ---- node-row tet assembly: tasks of consecutive block rows of one model
   // whose node incidences fit rows_cap lanes, the rows' incidences (element
@@ -425,11 +494,13 @@ int build_pack(Engine& eng) {
       auto b = nbr_idx.begin() + nbr_ptr[n], e = nbr_idx.begin() + nbr_ptr[n + 1];
       return (int)(std::lower_bound(b, e, node) - b);
     };
-    inc_slot.resize(iidx.size() * nen);
+    // nen_max entries per incidence (the element's nen used)
+    const int nm = eng.nen_max;
+    inc_slot.assign(iidx.size() * nm, 0);
     for (int n = 0; n < N; n++)
       for (int i = iptr[n]; i < iptr[n + 1]; i++) {
-        const int e = iidx[i] / nen;
-        for (int j = 0; j < nen; j++) inc_slot[(size_t)i * nen + j] = slot_of(n, conn[(size_t)e * nen + j]);
+        const int e = ielem[i], k = elem_nen(etype[e]);
+        for (int j = 0; j < k; j++) inc_slot[(size_t)i * nm + j] = slot_of(n, conn[(size_t)coff[e] + j]);
       }
     dptr.assign(NB + 1, 0);
     for (int pass = 0; pass < 2; pass++) {
@@ -674,13 +745,13 @@ int build_pack(Engine& eng) {
     // nodal forces (the force residual) stay FP64
     std::vector<float> invJ0_f(invJ0.begin(), invJ0.end());
     CK(upload(eng, &d.invJ0_f, invJ0_f));
-    CK(dalloc(eng, &d.elemK_f, (size_t)E * npair * 9));
+    CK(dalloc(eng, &d.elemK_f, (size_t)proff[E] * 9));
     CK(dalloc(eng, &d.S_f, (size_t)NB * 9));
   } else {
-    CK(dalloc(eng, &d.elemK, (size_t)E * npair * 9));
+    CK(dalloc(eng, &d.elemK, (size_t)proff[E] * 9));
     CK(dalloc(eng, &d.S, (size_t)NB * 9));
   }
-  CK(dalloc(eng, &d.elemF, (size_t)E * nen * 3));
+  CK(dalloc(eng, &d.elemF, (size_t)coff[E] * 3));
   CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
   CK(dalloc(eng, &d.fint, 3 * (size_t)N));
   for (double** v : {&d.b, &d.sol, &d.r, &d.z, &d.p, &d.q, &d.w, &d.u, &d.s, &d.m0, &d.m1}) {
@@ -699,15 +770,15 @@ int build_pack(Engine& eng) {
         std::copy(eng.hosts[m].rest_vol.begin(), eng.hosts[m].rest_vol.end(), erv.begin() + eng.elem_off[m]);
       CK(upload(eng, &d.elem_rest_vol, erv));
       // one pressure value per element, or npv values and an npv x npv Rinv
-      const size_t npv = (size_t)elem_npv(eng.elem_type);
-      CK(dalloc(eng, &d.elem_p, (size_t)E * npv));
-      CK(dalloc(eng, &d.elem_r, (size_t)E * npv * npv));
-      CK(cudaMemset(d.elem_p, 0, sizeof(double) * (size_t)E * npv));
-      CK(cudaMemset(d.elem_r, 0, sizeof(double) * (size_t)E * npv * npv));
-      if (npv > 1) {
-        std::vector<double> dj0((size_t)E * nip, 1.0);
+      CK(dalloc(eng, &d.elem_p, (size_t)pvoff[E]));
+      CK(dalloc(eng, &d.elem_r, (size_t)pv2off[E]));
+      CK(cudaMemset(d.elem_p, 0, sizeof(double) * (size_t)pvoff[E]));
+      CK(cudaMemset(d.elem_r, 0, sizeof(double) * (size_t)pv2off[E]));
+      if (pvoff[E] > E) {
+        std::vector<double> dj0((size_t)ipoff[E], 1.0);
         for (int m = 0; m < M; m++)
-          std::copy(eng.hosts[m].detJ0.begin(), eng.hosts[m].detJ0.end(), dj0.begin() + (size_t)eng.elem_off[m] * nip);
+          std::copy(eng.hosts[m].detJ0.begin(), eng.hosts[m].detJ0.end(),
+                    dj0.begin() + (size_t)ipoff[eng.elem_off[m]]);
         CK(upload(eng, &d.detJ0, dj0));
       }
     }
@@ -721,6 +792,7 @@ int build_pack(Engine& eng) {
     CK(upload(eng, &d.mat_node, mat_node));
     CK(upload(eng, &d.nbr_ptr, nbr_ptr));
     CK(upload(eng, &d.inc_slot, inc_slot));
+    if (mixed) CK(upload(eng, &d.inc_tl, itl));
     CK(dalloc(eng, &d.divblk, 3 * (size_t)nbr_ptr[N]));
     CK(upload(eng, &d.dil_ptr, dptr));
     CK(upload(eng, &d.dil_idx, didx));
@@ -942,9 +1014,37 @@ int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double*
   m.n_elems = n_elems;
   m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
   m.conn.assign(conn, conn + (size_t)nen * n_elems);
+  m.etypes.clear();
   m.fixed.assign(n_nodes, 0);
   if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
   eng.att = FrameAttach();  // attachments name nodes of the previous mesh
+  free_pack(eng);
+  return B200FEM_OK;
+}
+
+int b200fem_set_mesh_mixed(b200fem_handle h, int n_nodes, const double* rest_xyz, int n_elems,
+                           const int* elem_types, const int* conn, const int* fixed) {
+  ENG(h);
+  if (n_nodes <= 0 || n_elems <= 0 || !rest_xyz || !conn || !elem_types)
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "empty mesh");
+  size_t total = 0;
+  for (int e = 0; e < n_elems; e++) {
+    const int k = elem_nen(elem_types[e]);
+    if (k == 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "element " + std::to_string(e) + ": unknown type");
+    total += (size_t)k;
+  }
+  if (!all_finite(rest_xyz, 3 * (size_t)n_nodes))
+    return fail(&eng, B200FEM_ERR_INVALID_ARG, "non-finite rest position");
+  ModelDesc& m = eng.models[0];
+  m.elem_type = kElemMixed;
+  m.n_nodes = n_nodes;
+  m.n_elems = n_elems;
+  m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
+  m.conn.assign(conn, conn + total);
+  m.etypes.assign(elem_types, elem_types + n_elems);
+  m.fixed.assign(n_nodes, 0);
+  if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
+  eng.att = FrameAttach();
   free_pack(eng);
   return B200FEM_OK;
 }

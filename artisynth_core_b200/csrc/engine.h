@@ -48,12 +48,16 @@ __host__ __device__ constexpr bool elem_ip_at_nodes(int type) {
   return type == B200FEM_ELEM_HEX || type == B200FEM_ELEM_WEDGE || type == B200FEM_ELEM_PYRAMID;
 }
 
+// element type of a model or pack whose elements are not all of one type
+constexpr int kElemMixed = -1;
+
 // Model as given by the caller (host, FP64).
 struct ModelDesc {
-  int elem_type = B200FEM_ELEM_TET;
+  int elem_type = B200FEM_ELEM_TET;  // kElemMixed: per element in etypes
   int n_nodes = 0, n_elems = 0;
   std::vector<double> rest;  // 3N
-  std::vector<int> conn;     // nen*E
+  std::vector<int> conn;     // every element's nodes, concatenated in element order
+  std::vector<int> etypes;   // per element (mixed meshes only)
   std::vector<int> fixed;    // N
   int mat_kind = B200FEM_MAT_LINEAR;
   double mat_params[kMatParams] = {0};
@@ -63,18 +67,30 @@ struct ModelDesc {
 };
 
 // Host-side derived data of one model (setup only).
+//
+// Element data are held in storage order: the caller's elements sorted by
+// type (stable), so that each type forms one contiguous section that the
+// type-specialised kernels run over.  A mesh of one type keeps the caller's
+// order.  Per storage element s, coff/ipoff/sqoff give the offsets of its
+// nodes (and force slots), integration points and nen x nen entries.
 struct ModelHost {
-  int nen = 4, nip = 1, npair = 10;
+  int nen = 4, nip = 1, npair = 10;  // of a single-type mesh (0 when mixed)
   int incomp = B200FEM_INCOMP_OFF;  // resolved method
   int n_active = 0;
   std::vector<int> sidx;      // per node, -1 when fixed
   std::vector<int> act_node;  // per active row -> node
-  std::vector<double> invJ0;  // E*nip*9
-  std::vector<double> detJ0;  // E*nip
+  std::vector<int> stype;     // per storage element: its type
+  std::vector<int> perm;      // storage element -> caller's element
+  std::vector<int> iperm;     // caller's element -> storage element
+  std::vector<int> sec;       // section bounds in storage order (type runs), sec.size() = runs + 1
+  std::vector<long long> coff, ipoff, sqoff;  // E+1 each
+  std::vector<int> sconn;     // nodes in storage order (coff)
+  std::vector<double> invJ0;  // ipoff[E]*9
+  std::vector<double> detJ0;  // ipoff[E]
   std::vector<double> winvJ0; // E*9 (warping point)
   std::vector<double> rest_vol;
   std::vector<double> mass;   // N
-  std::vector<double> K0, f0; // linear materials: E*nen*nen*9, E*nen*3
+  std::vector<double> K0, f0; // linear materials: sqoff[E]*9, coff[E]*3
   std::vector<double> node_rest_vol;  // NODAL
   // block pattern over active nodes
   std::vector<int> rowptr, col;
@@ -98,12 +114,12 @@ struct DevPack {
   int* act_node = nullptr;   // rows -> node
   int* row_model = nullptr;  // rows -> model
   // elements
-  int* conn = nullptr;       // nen*E global node indices
+  int* conn = nullptr;       // node slots (nen per element, storage order): global node indices
   int* elem_model = nullptr; // E
-  double* invJ0 = nullptr;   // E*nip*9
+  double* invJ0 = nullptr;   // 9 per integration point
   double* winvJ0 = nullptr;  // E*9
-  double* K0 = nullptr;      // linear: E*nen*nen*9
-  double* f0 = nullptr;      // linear: E*nen*3
+  double* K0 = nullptr;      // linear: nen*nen*9 per element
+  double* f0 = nullptr;      // linear: 3 per node slot
   float* invJ0_f = nullptr;  // mixed form copy
   // assembly maps
   int* blk_rowptr = nullptr; // n_rows+1 (global block index)
@@ -113,10 +129,10 @@ struct DevPack {
   int* contrib_ptr = nullptr;  // nnzb+1
   int* contrib_idx = nullptr;  // (elem*npair + pair) << 1 | transpose
   int* inc_ptr = nullptr;      // N+1 node -> element incidences
-  int* inc_idx = nullptr;      // elem*nen + local
+  int* inc_idx = nullptr;      // node slot of the incidence (element's first slot + local node)
   // element outputs
-  double* elemK = nullptr;     // E*npair*9
-  double* elemF = nullptr;     // E*nen*3
+  double* elemK = nullptr;     // 9 per upper-triangle node pair of each element
+  double* elemF = nullptr;     // 3 per node slot
   float* elemK_f = nullptr;
   // assembled values
   double* K = nullptr;         // nnzb*9 stiffness (drop-in output)
@@ -146,7 +162,8 @@ struct DevPack {
   double* node_kp = nullptr;   // dilational modulus / rest volume
   double* mat_node = nullptr;  // per node: kappa, bulk potential of its model
   int* nbr_ptr = nullptr;      // N+1 direct neighbours (sorted node ids)
-  int* inc_slot = nullptr;     // per incidence (inc_idx order): nen slots in nbr(n)
+  int* inc_slot = nullptr;     // per incidence (inc_idx order): nen_max slots in nbr(n)
+  int* inc_tl = nullptr;       // mixed packs: per incidence (element type << 8) | local node
   double* divblk = nullptr;    // nbr_ptr[N] x 3: d V_n / d x_m
   int* dil_ptr = nullptr;      // nnzb+1 dilational contributions per block
   int* dil_idx = nullptr;      // (divblk row i, divblk row j, node n) triples
@@ -154,9 +171,9 @@ struct DevPack {
   // ELEMENT soft incompressibility: per element rest volume, pressure and
   // Rinv (effective modulus / rest volume)
   double* elem_rest_vol = nullptr;
-  double* elem_p = nullptr;    // E * npv pressure values
-  double* elem_r = nullptr;    // E * npv * npv: Rinv
-  double* detJ0 = nullptr;     // E * nip rest Jacobian determinants (several pressure values)
+  double* elem_p = nullptr;    // npv pressure values per element
+  double* elem_r = nullptr;    // npv * npv per element: Rinv
+  double* detJ0 = nullptr;     // per integration point: rest Jacobian determinant (several pressure values)
   // reductions / PCG control
   double* partials = nullptr;  // [2][n_pieces][4] (double-buffered by phase)
   int* piece_row = nullptr;    // n_pieces+1
@@ -256,8 +273,14 @@ struct PointCons {
 
 // One element group: contiguous element range with one element type and
 // material kind (kernels are specialised on both).
+//
+// Kernels see a group's elements as 0 .. e1-e0-1: their per-element arrays
+// are offset to the group's first element (c0 node slots, ip0 integration
+// points, pr0 upper-triangle pairs, sq0 nen x nen entries, pv0 pressure
+// values, pv20 npv x npv entries), so one layout serves every element type.
 struct ElemGroup {
   int e0 = 0, e1 = 0;
+  long long c0 = 0, ip0 = 0, pr0 = 0, sq0 = 0, pv0 = 0, pv20 = 0;
   int elem_type = B200FEM_ELEM_TET;
   int mat_kind = B200FEM_MAT_LINEAR;
   int corotated = 1;
@@ -281,8 +304,9 @@ struct Engine {
   DevPack d;
   bool built = false;
   bool have_matrix = false;
-  int elem_type = B200FEM_ELEM_TET;  // pack-wide element type
-  int nen = 4, nip = 1, npair = 10;
+  int elem_type = B200FEM_ELEM_TET;  // pack-wide element type (kElemMixed: several)
+  int nen = 4, nip = 1, npair = 10;  // of a single-type pack
+  int nen_max = 4;                   // largest element of the pack
   // host copies for queries
   std::vector<int> h_rowptr, h_col;
   std::vector<int> h_scatter;  // E*nen*nen

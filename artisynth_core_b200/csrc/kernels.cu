@@ -926,27 +926,36 @@ __global__ void crs_export_kernel(long long nnzb, const int* blk_row, const int*
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+// p + off, or null for an array the pack does not hold
+template <typename T>
+static T* at(T* p, long long off) {
+  return p ? p + off : nullptr;
+}
+
+// The group's elements as 0 .. e1-e0-1: every per-element array starts at
+// the group's first element (ElemGroup offsets), so the type-specialised
+// kernels index them with their own constant strides.
 static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   DevPack& d = eng.d;
   ElemArgs a;
-  a.e0 = g.e0;
-  a.e1 = g.e1;
-  a.conn = d.conn;
-  a.elem_model = d.elem_model;
+  a.e0 = 0;
+  a.e1 = g.e1 - g.e0;
+  a.conn = at(d.conn, g.c0);
+  a.elem_model = at(d.elem_model, g.e0);
   a.active = eng.any_inactive ? d.model_active : nullptr;
   a.x = d.x;
-  a.invJ0 = d.invJ0;
-  a.invJ0_f = d.invJ0_f;
-  a.winvJ0 = d.winvJ0;
-  a.K0 = d.K0;
-  a.f0 = d.f0;
+  a.invJ0 = at(d.invJ0, 9 * g.ip0);
+  a.invJ0_f = at(d.invJ0_f, 9 * g.ip0);
+  a.winvJ0 = at(d.winvJ0, 9LL * g.e0);
+  a.K0 = at(d.K0, 9 * g.sq0);
+  a.f0 = at(d.f0, 3 * g.c0);
   a.sidx = d.sidx;
   a.mat = d.mat;
   a.node_p = d.node_p;
-  a.elem_p = d.elem_p;
-  a.elem_r = d.elem_r;
-  a.elemK = fp32 ? (void*)d.elemK_f : (void*)d.elemK;
-  a.elemF = (void*)d.elemF;  // nodal forces are FP64 in both forms
+  a.elem_p = at(d.elem_p, g.pv0);
+  a.elem_r = at(d.elem_r, g.pv20);
+  a.elemK = fp32 ? (void*)at(d.elemK_f, 9 * g.pr0) : (void*)at(d.elemK, 9 * g.pr0);
+  a.elemF = (void*)at(d.elemF, 3 * g.c0);  // nodal forces are FP64 in both forms
   a.flags = d.flags;
   a.mindet = (long long*)d.dmin;
   a.det_stats = 0;
@@ -1484,39 +1493,33 @@ static cudaError_t launch_group(Engine& eng, const ElemGroup& g, bool fp32) {
 // ---------------------------------------------------------------------------
 // NODAL soft incompressibility
 // ---------------------------------------------------------------------------
-// Nodal volumes and pressures (updateNodalPressures, FemModel3d.java:2471-2515):
-// tets give V_e/4 to each node, hexes the dv of the integration point that
-// maps to the node; p_n = K(V_n/V0_n - 1) (QUADRATIC) or K ln(J)/J
-// (LOGARITHMIC) for active nodes, and kp_n = K_eff / V0_n
-// (computeNodalIncompressibility, :2632-2669).
+// One incidence's share of its node's volume: tets give V_e/4 (det(J)/24),
+// other elements the dv of the integration point a that maps to the node.
 template <int TYPE>
-__global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
-                                      const int* __restrict__ conn, const double* __restrict__ x,
-                                      const int* __restrict__ sidx, const double* __restrict__ rest_vol,
-                                      const double* __restrict__ mat_node, double* __restrict__ vol,
-                                      double* __restrict__ pres, double* __restrict__ kp) {
+__device__ __forceinline__ double nodal_vol_share(const int* __restrict__ nodes, int a,
+                                                  const double* __restrict__ x) {
   constexpr int NEN = elem_nen(TYPE);
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  double v = 0;
-  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
-    const int e = inc_idx[i] / NEN, a = inc_idx[i] % NEN;
-    const int* nodes = conn + (size_t)e * NEN;
-    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-    for (int k = 0; k < NEN; k++) {
-      const double* pk = x + 3 * (size_t)nodes[k];
-      const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1), g2 = gns<double, TYPE>(a, k, 2);
+  for (int k = 0; k < NEN; k++) {
+    const double* pk = x + 3 * (size_t)nodes[k];
+    const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1), g2 = gns<double, TYPE>(a, k, 2);
 #pragma unroll
-      for (int r = 0; r < 3; r++) {
-        J[3 * r] += pk[r] * g0;
-        J[3 * r + 1] += pk[r] * g1;
-        J[3 * r + 2] += pk[r] * g2;
-      }
+    for (int r = 0; r < 3; r++) {
+      J[3 * r] += pk[r] * g0;
+      J[3 * r + 1] += pk[r] * g1;
+      J[3 * r + 2] += pk[r] * g2;
     }
-    // tet: V_e = det(J)/6 shared by four nodes; otherwise the dv of point a
-    v += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 / 4 : det3(J) * ip_weight<double, TYPE>(a);
   }
+  return TYPE == B200FEM_ELEM_TET ? det3(J) / 6 / 4 : det3(J) * ip_weight<double, TYPE>(a);
+}
+
+// p_n = K(V_n/V0_n - 1) (QUADRATIC) or K ln(J)/J (LOGARITHMIC) for active
+// nodes, and kp_n = K_eff / V0_n (computeNodalIncompressibility, :2632-2669)
+__device__ __forceinline__ void nodal_pressure_store(int n, double v, const int* __restrict__ sidx,
+                                                     const double* __restrict__ rest_vol,
+                                                     const double* __restrict__ mat_node, double* __restrict__ vol,
+                                                     double* __restrict__ pres, double* __restrict__ kp) {
   vol[n] = v;
   double p = 0, k = 0;
   if (sidx[n] >= 0) {
@@ -1534,10 +1537,96 @@ __global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, co
   kp[n] = k;
 }
 
-// divBlk(n, m) = dV_n/dx_m, accumulated per node over its incidences in
-// element order (FemModel3d.java:3604-3648): tets add -1/12 of the
-// area-weighted normal of the face opposite m (TetElement.java:333-362);
-// hexes add dv_k GNx_m at the integration point k that maps to n.
+// Nodal volumes and pressures (updateNodalPressures, FemModel3d.java:2471-2515),
+// one thread per node over its incidences in element order.
+template <int TYPE>
+__global__ void nodal_pressure_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                      const int* __restrict__ conn, const double* __restrict__ x,
+                                      const int* __restrict__ sidx, const double* __restrict__ rest_vol,
+                                      const double* __restrict__ mat_node, double* __restrict__ vol,
+                                      double* __restrict__ pres, double* __restrict__ kp) {
+  constexpr int NEN = elem_nen(TYPE);
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double v = 0;
+  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+    const int a = inc_idx[i] % NEN;
+    v += nodal_vol_share<TYPE>(conn + (inc_idx[i] - a), a, x);
+  }
+  nodal_pressure_store(n, v, sidx, rest_vol, mat_node, vol, pres, kp);
+}
+
+// the same for a pack of several element types: each incidence carries its
+// element's type and local node ((type << 8) | a), the node slot inc_idx
+// gives the element's first slot (inc_idx - a)
+__global__ void nodal_pressure_mixed_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                            const int* __restrict__ inc_tl, const int* __restrict__ conn,
+                                            const double* __restrict__ x, const int* __restrict__ sidx,
+                                            const double* __restrict__ rest_vol, const double* __restrict__ mat_node,
+                                            double* __restrict__ vol, double* __restrict__ pres,
+                                            double* __restrict__ kp) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double v = 0;
+  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+    const int t = inc_tl[i] >> 8, a = inc_tl[i] & 255;
+    const int* nodes = conn + (inc_idx[i] - a);
+    switch (t) {
+      case B200FEM_ELEM_TET: v += nodal_vol_share<B200FEM_ELEM_TET>(nodes, a, x); break;
+      case B200FEM_ELEM_HEX: v += nodal_vol_share<B200FEM_ELEM_HEX>(nodes, a, x); break;
+      case B200FEM_ELEM_WEDGE: v += nodal_vol_share<B200FEM_ELEM_WEDGE>(nodes, a, x); break;
+      default: v += nodal_vol_share<B200FEM_ELEM_PYRAMID>(nodes, a, x); break;
+    }
+  }
+  nodal_pressure_store(n, v, sidx, rest_vol, mat_node, vol, pres, kp);
+}
+
+// divBlk(n, m) = dV_n/dx_m, one incidence's terms (FemModel3d.java:3604-3648):
+// tets add -1/12 of the area-weighted normal of the face opposite m
+// (TetElement.java:333-362); other elements add dv_k GNx_m at the
+// integration point k that maps to n.  slot[j]: node j's entry in nbr(n).
+template <int TYPE>
+__device__ __forceinline__ void divblk_add(const int* __restrict__ nodes, int a, const int* __restrict__ slot,
+                                           const double* __restrict__ x, double* __restrict__ out) {
+  constexpr int NEN = elem_nen(TYPE);
+  if constexpr (TYPE == B200FEM_ELEM_TET) {
+    const double* P[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) P[k] = x + 3 * (size_t)nodes[k];
+    // faces opposite nodes 0..3: (1,2,3), (0,3,2), (0,1,3), (0,2,1)
+    const int f[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double *q0 = P[f[j][0]], *q1 = P[f[j][1]], *q2 = P[f[j][2]];
+      const double ux = q1[0] - q0[0], uy = q1[1] - q0[1], uz = q1[2] - q0[2];
+      const double vx = q2[0] - q0[0], vy = q2[1] - q0[1], vz = q2[2] - q0[2];
+      double* o = out + 3 * slot[j];
+      o[0] += 0.5 * (uy * vz - uz * vy) * (-1 / 12.0);
+      o[1] += 0.5 * (uz * vx - ux * vz) * (-1 / 12.0);
+      o[2] += 0.5 * (ux * vy - uy * vx) * (-1 / 12.0);
+    }
+  } else {
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
+#pragma unroll
+    for (int k = 0; k < NEN; k++) {
+      const double* pk = x + 3 * (size_t)nodes[k];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * gns<double, TYPE>(a, k, c);
+    }
+    const double dv = invert3(iJ, J) * ip_weight<double, TYPE>(a);
+#pragma unroll
+    for (int k = 0; k < NEN; k++) {
+      const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1), g2 = gns<double, TYPE>(a, k, 2);
+      double* o = out + 3 * slot[k];
+#pragma unroll
+      for (int c = 0; c < 3; c++) o[c] += dv * (iJ[c] * g0 + iJ[3 + c] * g1 + iJ[6 + c] * g2);
+    }
+  }
+}
+
+// divBlk per node, accumulated over its incidences in element order
 template <int TYPE>
 __global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
                               const int* __restrict__ inc_slot, const int* __restrict__ conn,
@@ -1551,44 +1640,32 @@ __global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int*
   for (int s = 0; s < 3 * ns; s++) out[s] = 0;
   if (sidx[n] < 0) return;
   for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
-    const int e = inc_idx[i] / NEN, a = inc_idx[i] % NEN;
-    const int* nodes = conn + (size_t)e * NEN;
-    const int* slot = inc_slot + (size_t)i * NEN;
-    if (TYPE == B200FEM_ELEM_TET) {
-      const double* P[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) P[k] = x + 3 * (size_t)nodes[k];
-      // faces opposite nodes 0..3: (1,2,3), (0,3,2), (0,1,3), (0,2,1)
-      const int f[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const double *q0 = P[f[j][0]], *q1 = P[f[j][1]], *q2 = P[f[j][2]];
-        const double ux = q1[0] - q0[0], uy = q1[1] - q0[1], uz = q1[2] - q0[2];
-        const double vx = q2[0] - q0[0], vy = q2[1] - q0[1], vz = q2[2] - q0[2];
-        double* o = out + 3 * slot[j];
-        o[0] += 0.5 * (uy * vz - uz * vy) * (-1 / 12.0);
-        o[1] += 0.5 * (uz * vx - ux * vz) * (-1 / 12.0);
-        o[2] += 0.5 * (ux * vy - uy * vx) * (-1 / 12.0);
-      }
-    } else {
-      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
-#pragma unroll
-      for (int k = 0; k < NEN; k++) {
-        const double* pk = x + 3 * (size_t)nodes[k];
-#pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-          for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * gns<double, TYPE>(a, k, c);
-      }
-      const double dv = invert3(iJ, J) * ip_weight<double, TYPE>(a);
-#pragma unroll
-      for (int k = 0; k < NEN; k++) {
-        const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1),
-                     g2 = gns<double, TYPE>(a, k, 2);
-        double* o = out + 3 * slot[k];
-#pragma unroll
-        for (int c = 0; c < 3; c++) o[c] += dv * (iJ[c] * g0 + iJ[3 + c] * g1 + iJ[6 + c] * g2);
-      }
+    const int a = inc_idx[i] % NEN;
+    divblk_add<TYPE>(conn + (inc_idx[i] - a), a, inc_slot + (size_t)i * NEN, x, out);
+  }
+}
+
+// the same for a pack of several element types (nm slots per incidence)
+__global__ void divblk_mixed_kernel(int N, int nm, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                    const int* __restrict__ inc_tl, const int* __restrict__ inc_slot,
+                                    const int* __restrict__ conn, const double* __restrict__ x,
+                                    const int* __restrict__ sidx, const int* __restrict__ nbr_ptr,
+                                    double* __restrict__ divblk) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double* out = divblk + 3 * (size_t)nbr_ptr[n];
+  const int ns = nbr_ptr[n + 1] - nbr_ptr[n];
+  for (int s = 0; s < 3 * ns; s++) out[s] = 0;
+  if (sidx[n] < 0) return;
+  for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+    const int t = inc_tl[i] >> 8, a = inc_tl[i] & 255;
+    const int* nodes = conn + (inc_idx[i] - a);
+    const int* slot = inc_slot + (size_t)i * nm;
+    switch (t) {
+      case B200FEM_ELEM_TET: divblk_add<B200FEM_ELEM_TET>(nodes, a, slot, x, out); break;
+      case B200FEM_ELEM_HEX: divblk_add<B200FEM_ELEM_HEX>(nodes, a, slot, x, out); break;
+      case B200FEM_ELEM_WEDGE: divblk_add<B200FEM_ELEM_WEDGE>(nodes, a, slot, x, out); break;
+      default: divblk_add<B200FEM_ELEM_PYRAMID>(nodes, a, slot, x, out); break;
     }
   }
 }
@@ -1597,6 +1674,12 @@ cudaError_t launch_nodal_pressure(Engine& eng) {
   DevPack& d = eng.d;
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
+  if (eng.elem_type == kElemMixed) {
+    nodal_pressure_mixed_kernel<<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_tl,
+                                                                    d.conn, d.x, d.sidx, d.node_rest_vol,
+                                                                    d.mat_node, d.node_vol, d.node_p, d.node_kp);
+    return cudaGetLastError();
+  }
   return by_elem_type(eng.elem_type, [&](auto tag) {
     constexpr int TY = decltype(tag)::value;
     // NODAL: tets, or elements whose integration points sit at their nodes
@@ -1615,6 +1698,11 @@ cudaError_t launch_divblk(Engine& eng) {
   DevPack& d = eng.d;
   if (!d.has_nodal) return cudaSuccess;
   const int threads = 128, blocks = (d.n_nodes + threads - 1) / threads;
+  if (eng.elem_type == kElemMixed) {
+    divblk_mixed_kernel<<<blocks, threads, 0, eng.stream>>>(d.n_nodes, eng.nen_max, d.inc_ptr, d.inc_idx, d.inc_tl,
+                                                            d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
+    return cudaGetLastError();
+  }
   return by_elem_type(eng.elem_type, [&](auto tag) {
     constexpr int TY = decltype(tag)::value;
     if constexpr (TY != B200FEM_ELEM_TET && !elem_ip_at_nodes(TY)) {
@@ -1758,9 +1846,10 @@ cudaError_t launch_element_pressure(Engine& eng) {
   for (const ElemGroup& g : eng.groups) {
     if (!g.elem_inc || g.e1 <= g.e0) continue;
     const int threads = 128, blocks = (g.e1 - g.e0 + threads - 1) / threads;
-    cudaError_t e = by_elem_type(eng.elem_type, [&](auto tag) {
+    cudaError_t e = by_elem_type(g.elem_type, [&](auto tag) {
       element_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
-          g.e0, g.e1, d.conn, d.elem_model, d.x, d.elem_rest_vol, d.mat, d.detJ0, d.elem_p, d.elem_r);
+          0, g.e1 - g.e0, at(d.conn, g.c0), at(d.elem_model, g.e0), d.x, at(d.elem_rest_vol, g.e0), d.mat,
+          at(d.detJ0, g.ip0), at(d.elem_p, g.pv0), at(d.elem_r, g.pv20));
       return cudaGetLastError();
     });
     if (e != cudaSuccess) return e;

@@ -584,16 +584,56 @@ void jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz, double
 }
 
 int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
-  const int nen = elem_nen(m.elem_type);
-  h.nen = nen;
-  h.nip = elem_nip(m.elem_type);
-  h.npair = nen * (nen + 1) / 2;
   const int N = m.n_nodes, E = m.n_elems;
-  for (int q = 0; q < E * nen; q++)
+  // element types in the caller's order, and the storage order: stable by
+  // type, so that every type is one contiguous section
+  std::vector<int> otype(E);
+  for (int e = 0; e < E; e++) {
+    otype[e] = m.elem_type == kElemMixed ? m.etypes[e] : m.elem_type;
+    if (elem_nen(otype[e]) == 0) {
+      err = "element " + std::to_string(e) + " has an unknown type";
+      return B200FEM_ERR_INVALID_ARG;
+    }
+  }
+  std::vector<long long> ooff(E + 1, 0);  // caller's node offsets
+  for (int e = 0; e < E; e++) ooff[e + 1] = ooff[e] + elem_nen(otype[e]);
+  if ((long long)m.conn.size() != ooff[E]) {
+    err = "connectivity size does not match the element types";
+    return B200FEM_ERR_INVALID_ARG;
+  }
+  for (long long q = 0; q < ooff[E]; q++)
     if (m.conn[q] < 0 || m.conn[q] >= N) {
       err = "connectivity index out of range";
       return B200FEM_ERR_INVALID_ARG;
     }
+  h.perm.resize(E);
+  for (int e = 0; e < E; e++) h.perm[e] = e;
+  std::stable_sort(h.perm.begin(), h.perm.end(), [&](int a, int b) { return otype[a] < otype[b]; });
+  h.iperm.assign(E, 0);
+  h.stype.assign(E, 0);
+  h.sec.assign(1, 0);
+  h.coff.assign(E + 1, 0);
+  h.ipoff.assign(E + 1, 0);
+  h.sqoff.assign(E + 1, 0);
+  for (int s = 0; s < E; s++) {
+    const int t = otype[h.perm[s]], nen = elem_nen(t);
+    h.iperm[h.perm[s]] = s;
+    h.stype[s] = t;
+    if (s > 0 && t != h.stype[s - 1]) h.sec.push_back(s);
+    h.coff[s + 1] = h.coff[s] + nen;
+    h.ipoff[s + 1] = h.ipoff[s] + elem_nip(t);
+    h.sqoff[s + 1] = h.sqoff[s] + (long long)nen * nen;
+  }
+  h.sec.push_back(E);
+  const bool single = h.sec.size() == 2;
+  h.nen = single ? elem_nen(h.stype[0]) : 0;
+  h.nip = single ? elem_nip(h.stype[0]) : 0;
+  h.npair = single ? h.nen * (h.nen + 1) / 2 : 0;
+  h.sconn.resize(h.coff[E]);
+  for (int s = 0; s < E; s++) {
+    const int o = h.perm[s];
+    std::copy(m.conn.begin() + ooff[o], m.conn.begin() + ooff[o + 1], h.sconn.begin() + h.coff[s]);
+  }
   // solve indices in node order (MechSystemBase.updateDynamicComponentLists,
   // MechSystemBase.java:689-760: active components numbered in tree order)
   h.sidx.assign(N, -1);
@@ -605,61 +645,61 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
     }
   h.n_active = (int)h.act_node.size();
   // soft incompressibility: OFF for compressible materials
-  // (FemModel3d.java:3346-3348); AUTO -> NODAL if #elements > #active nodes
-  // else ELEMENT (getAllowedSoftIncompMethod, FemModel3d.java:462-481)
+  // (FemModel3d.java:3346-3348).  NODAL needs every element to be a tet or
+  // to have its integration points at its nodes (softNodalIncompressAllowed,
+  // FemModel3d.java:400-405); the quadratic types are not, so NODAL and AUTO
+  // resolve to ELEMENT with QuadhexElement's four and QuadwedgeElement's two
+  // pressure values (getAllowedSoftIncompMethod, :462-481); otherwise AUTO ->
+  // NODAL if #elements > #active nodes, else ELEMENT
+  bool nodal_ok = true;
+  for (int s = 0; s < E; s++) nodal_ok &= h.stype[s] == B200FEM_ELEM_TET || elem_ip_at_nodes(h.stype[s]);
   int method = m.incomp_request;
   if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
-  // NODAL needs tets or elements whose points map to nodes
-  // (softNodalIncompressAllowed, FemModel3d.java:400-405, 467-471)
-  else if ((m.elem_type == B200FEM_ELEM_QUADTET || m.elem_type == B200FEM_ELEM_QUADPYRAMID) &&
-           (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
-    method = B200FEM_INCOMP_ELEMENT;
-  // quadratic hexes and wedges: their points do not map to nodes either, so
-  // NODAL and AUTO resolve to ELEMENT with QuadhexElement's four and
-  // QuadwedgeElement's two pressure values (:443-445, :267-269)
-  else if ((m.elem_type == B200FEM_ELEM_QUADHEX || m.elem_type == B200FEM_ELEM_QUADWEDGE) &&
-           (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
+  else if (!nodal_ok && (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
     method = B200FEM_INCOMP_ELEMENT;
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
   h.incomp = method;
 
   // rest data: IntegrationData3d.myInvJ0/myDetJ0 (IntegrationData3d.java:108-111)
-  h.invJ0.assign((size_t)E * h.nip * 9, 0);
-  h.detJ0.assign((size_t)E * h.nip, 0);
+  h.invJ0.assign((size_t)h.ipoff[E] * 9, 0);
+  h.detJ0.assign((size_t)h.ipoff[E], 0);
   h.winvJ0.assign((size_t)E * 9, 0);
   h.rest_vol.assign(E, 0);
   double g[kMaxNen * 3], wgt, J[9];
-  for (int e = 0; e < E; e++) {
-    const int* nodes = &m.conn[(size_t)e * nen];
+  for (int s = 0; s < E; s++) {
+    const int t = h.stype[s], nen = elem_nen(t), nip = elem_nip(t);
+    const int* nodes = &h.sconn[h.coff[s]];
     double vol = 0;
-    for (int k = 0; k < h.nip; k++) {
-      shape_grads(m.elem_type, k, g, &wgt);
+    for (int k = 0; k < nip; k++) {
+      shape_grads(t, k, g, &wgt);
       jacobian(J, g, nen, m.rest.data(), nodes);
-      double d = invert33(&h.invJ0[((size_t)e * h.nip + k) * 9], J);
+      double d = invert33(&h.invJ0[(size_t)(h.ipoff[s] + k) * 9], J);
       if (!(d > 0)) {
-        err = "element " + std::to_string(e) + " has non-positive rest volume";
+        err = "element " + std::to_string(h.perm[s]) + " has non-positive rest volume";
         return B200FEM_ERR_INVERTED;
       }
-      h.detJ0[(size_t)e * h.nip + k] = d;
+      h.detJ0[h.ipoff[s] + k] = d;
       vol += d * wgt;
     }
-    if (m.elem_type == B200FEM_ELEM_TET) {
+    if (t == B200FEM_ELEM_TET) {
       // TetElement.computeRestVolumes = detJ0/6 (TetElement.java:247-254)
-      vol = h.detJ0[e] / 6;
-      std::memcpy(&h.winvJ0[(size_t)e * 9], &h.invJ0[(size_t)e * 9], 9 * sizeof(double));
+      vol = h.detJ0[h.ipoff[s]] / 6;
+      std::memcpy(&h.winvJ0[(size_t)s * 9], &h.invJ0[(size_t)h.ipoff[s] * 9], 9 * sizeof(double));
     } else {
-      shape_grads(m.elem_type, -1, g, &wgt);
+      shape_grads(t, -1, g, &wgt);
       jacobian(J, g, nen, m.rest.data(), nodes);
-      invert33(&h.winvJ0[(size_t)e * 9], J);
+      invert33(&h.winvJ0[(size_t)s * 9], J);
     }
-    h.rest_vol[e] = vol;
+    h.rest_vol[s] = vol;
   }
-  // lumped masses (FemNode3d.computeMassFromDensity, FemNode3d.java:1030-1045)
+  // lumped masses (FemNode3d.computeMassFromDensity, FemNode3d.java:1030-1045),
+  // summed in the caller's element order
   h.mass.assign(N, 0);
-  for (int e = 0; e < E; e++) {
-    double share = h.rest_vol[e] * m.density / nen;
-    for (int a = 0; a < nen; a++) h.mass[m.conn[(size_t)e * nen + a]] += share;
+  for (int o = 0; o < E; o++) {
+    const int s = h.iperm[o], nen = elem_nen(h.stype[s]);
+    double share = h.rest_vol[s] * m.density / nen;
+    for (int a = 0; a < nen; a++) h.mass[h.sconn[h.coff[s] + a]] += share;
   }
   // linear materials: rest stiffness K0 and f0 = K0 x_rest
   // (LinearMaterialCache.addInitialStiffness, LinearMaterialCache.java:115-160)
@@ -668,45 +708,47 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   if (m.mat_kind == B200FEM_MAT_LINEAR) {
     double C[36];
     linear_tangent(C, m.mat_params[0], m.mat_params[1]);
-    h.K0.assign((size_t)E * nen * nen * 9, 0);
-    h.f0.assign((size_t)E * nen * 3, 0);
+    h.K0.assign((size_t)h.sqoff[E] * 9, 0);
+    h.f0.assign((size_t)h.coff[E] * 3, 0);
     double gx[kMaxNen * 3];
-    for (int e = 0; e < E; e++) {
-      double* K0 = &h.K0[(size_t)e * nen * nen * 9];
-      for (int k = 0; k < h.nip; k++) {
-        shape_grads(m.elem_type, k, g, &wgt);
-        const double* iJ = &h.invJ0[((size_t)e * h.nip + k) * 9];
-        double dv0 = h.detJ0[(size_t)e * h.nip + k] * wgt;
+    for (int s = 0; s < E; s++) {
+      const int t = h.stype[s], nen = elem_nen(t), nip = elem_nip(t);
+      double* K0 = &h.K0[(size_t)h.sqoff[s] * 9];
+      for (int k = 0; k < nip; k++) {
+        shape_grads(t, k, g, &wgt);
+        const double* iJ = &h.invJ0[(size_t)(h.ipoff[s] + k) * 9];
+        double dv0 = h.detJ0[h.ipoff[s] + k] * wgt;
         for (int n = 0; n < nen; n++)
           for (int c = 0; c < 3; c++)
             gx[3 * n + c] = iJ[c] * g[3 * n] + iJ[3 + c] * g[3 * n + 1] + iJ[6 + c] * g[3 * n + 2];
         for (int i = 0; i < nen; i++)
           for (int j = 0; j < nen; j++) add_bdb(&K0[(i * nen + j) * 9], &gx[3 * i], C, &gx[3 * j], dv0);
       }
-      const int* nodes = &m.conn[(size_t)e * nen];
+      const int* nodes = &h.sconn[h.coff[s]];
       for (int i = 0; i < nen; i++)
         for (int j = 0; j < nen; j++) {
           const double* Kij = &K0[(i * nen + j) * 9];
           const double* p = &m.rest[3 * (size_t)nodes[j]];
           for (int r = 0; r < 3; r++)
-            h.f0[((size_t)e * nen + i) * 3 + r] += Kij[3 * r] * p[0] + Kij[3 * r + 1] * p[1] + Kij[3 * r + 2] * p[2];
+            h.f0[(size_t)(h.coff[s] + i) * 3 + r] +=
+                Kij[3 * r] * p[0] + Kij[3 * r + 1] * p[1] + Kij[3 * r + 2] * p[2];
         }
     }
   }
   // node neighbours: nodes sharing an element, self included
   // (FemNodeNeighbor lists; FemModel3d.addSolveBlocks, FemModel3d.java:4099-4112)
   std::vector<int> inc_ptr(N + 1, 0);
-  for (int q = 0; q < E * nen; q++) inc_ptr[m.conn[q] + 1]++;
+  for (int n : h.sconn) inc_ptr[n + 1]++;
   for (int n = 0; n < N; n++) inc_ptr[n + 1] += inc_ptr[n];
-  std::vector<int> inc(E * nen), fill(inc_ptr.begin(), inc_ptr.end() - 1);
-  for (int e = 0; e < E; e++)
-    for (int a = 0; a < nen; a++) inc[fill[m.conn[(size_t)e * nen + a]]++] = e;
+  std::vector<int> inc(h.sconn.size()), fill(inc_ptr.begin(), inc_ptr.end() - 1);
+  for (int s = 0; s < E; s++)
+    for (long long q = h.coff[s]; q < h.coff[s + 1]; q++) inc[fill[h.sconn[q]]++] = s;
   h.nbr.assign(N, {});
   for (int n = 0; n < N; n++) {
     auto& v = h.nbr[n];
     for (int q = inc_ptr[n]; q < inc_ptr[n + 1]; q++) {
-      const int* nodes = &m.conn[(size_t)inc[q] * nen];
-      v.insert(v.end(), nodes, nodes + nen);
+      const int s = inc[q];
+      v.insert(v.end(), h.sconn.begin() + h.coff[s], h.sconn.begin() + h.coff[s + 1]);
     }
     std::sort(v.begin(), v.end());
     v.erase(std::unique(v.begin(), v.end()), v.end());
@@ -733,17 +775,21 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
     h.rowptr[r + 1] = (int)h.col.size();
   }
   if (h.incomp == B200FEM_INCOMP_NODAL) {
-    // nodal rest volumes (updateNodalRestVolumes, FemModel3d.java:2594-2628)
+    // nodal rest volumes (updateNodalRestVolumes, FemModel3d.java:2594-2628),
+    // summed in the caller's element order
     h.node_rest_vol.assign(N, 0);
-    double wts[kMaxNen], g[kMaxNen * 3];
-    for (int a = 0; a < nen; a++) shape_grads(m.elem_type, a, g, &wts[a]);
-    for (int e = 0; e < E; e++) {
-      const int* nodes = &m.conn[(size_t)e * nen];
-      if (m.elem_type == B200FEM_ELEM_TET) {
-        for (int a = 0; a < 4; a++) h.node_rest_vol[nodes[a]] += h.rest_vol[e] / 4;
+    double wts[kMaxNen];
+    for (int o = 0; o < E; o++) {
+      const int s = h.iperm[o], t = h.stype[s], nen = elem_nen(t);
+      const int* nodes = &h.sconn[h.coff[s]];
+      if (t == B200FEM_ELEM_TET) {
+        for (int a = 0; a < 4; a++) h.node_rest_vol[nodes[a]] += h.rest_vol[s] / 4;
       } else {
         // integration point a maps to node a: its rest dv = w_a detJ0_a
-        for (int a = 0; a < nen; a++) h.node_rest_vol[nodes[a]] += wts[a] * h.detJ0[(size_t)e * nen + a];
+        for (int a = 0; a < nen; a++) {
+          shape_grads(t, a, g, &wts[a]);
+          h.node_rest_vol[nodes[a]] += wts[a] * h.detJ0[h.ipoff[s] + a];
+        }
       }
     }
   }

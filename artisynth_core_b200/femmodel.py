@@ -209,9 +209,9 @@ class FemEngine:
 
 # -------------------------------------------------------------------- model
 class FemModel3d:
-    """FemModel3d restricted to the hot path: one element type (tet, hex,
-    wedge or pyramid, linear or quadratic),
-    one material, lumped mass, fixed nodes and the BackwardEuler data."""
+    """FemModel3d restricted to the hot path: tet, hex, wedge and pyramid
+    elements, linear or quadratic (one type, or any mix of them), one
+    material, lumped mass, fixed nodes and the BackwardEuler data."""
 
     def __init__(self):
         self.elem_type = L.ELEM_TET
@@ -241,10 +241,19 @@ class FemModel3d:
         self._invalidate()
 
     def setMesh(self, elem_type, rest, conn, fixed=None):
-        self.elem_type = elem_type
+        """elem_type: one B200FEM_ELEM_* type for every element (conn: E x nen),
+        or a sequence of one type per element (conn: every element's nodes
+        concatenated in element order)."""
         self.rest = np.ascontiguousarray(rest, dtype=np.float64).reshape(-1, 3)
-        nen = L.ELEM_NODES[elem_type]
-        self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, nen)
+        if np.ndim(elem_type) == 0:
+            self.elem_type = int(elem_type)
+            nen = L.ELEM_NODES[self.elem_type]
+            self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, nen)
+        else:
+            self.elem_type = np.ascontiguousarray(elem_type, dtype=np.int32).reshape(-1)
+            self.conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
+            if self.conn.size != sum(L.ELEM_NODES[int(t)] for t in self.elem_type):
+                raise ValueError("connectivity size does not match the element types")
         self.fixed = (np.zeros(self.rest.shape[0], dtype=np.int32) if fixed is None
                       else np.ascontiguousarray(fixed, dtype=np.int32))
         self._grid = None
@@ -263,7 +272,11 @@ class FemModel3d:
         return self.rest.shape[0]
 
     def numElements(self):
-        return self.conn.shape[0]
+        return self.elem_type.size if self.isMixed() else self.conn.shape[0]
+
+    def isMixed(self):
+        """True when the elements are of several types (one type per element)."""
+        return np.ndim(self.elem_type) > 0
 
     def setMaterial(self, mat):
         self.material = mat
@@ -317,8 +330,12 @@ class FemModel3d:
             eng = FemEngine(self.device, self.precision)
             rest = np.ascontiguousarray(self.rest.reshape(-1))
             conn = np.ascontiguousarray(self.conn.reshape(-1))
-            eng.call("b200fem_set_mesh", self.elem_type, self.numNodes(), L.dptr(rest), self.numElements(),
-                     L.iptr(conn), L.iptr(self.fixed))
+            if self.isMixed():
+                eng.call("b200fem_set_mesh_mixed", self.numNodes(), L.dptr(rest), self.numElements(),
+                         L.iptr(self.elem_type), L.iptr(conn), L.iptr(self.fixed))
+            else:
+                eng.call("b200fem_set_mesh", self.elem_type, self.numNodes(), L.dptr(rest), self.numElements(),
+                         L.iptr(conn), L.iptr(self.fixed))
             prm = np.zeros(8)
             p = self.material.params()
             prm[: len(p)] = p
@@ -369,6 +386,13 @@ class FemModel3d:
         return slots
 
     def getScatterMap(self):
+        """Block index of every element's (i, j) node pair: E x nen x nen, or
+        for a mesh of several types a flat array of nen_e * nen_e entries per
+        element in element order."""
+        if self.isMixed():
+            out = np.zeros(sum(L.ELEM_NODES[int(t)] ** 2 for t in self.elem_type), dtype=np.int32)
+            self.engine().call("b200fem_get_scatter_map", L.iptr(out))
+            return out
         nen = self.conn.shape[1]
         out = np.zeros(self.numElements() * nen * nen, dtype=np.int32)
         self.engine().call("b200fem_get_scatter_map", L.iptr(out))
@@ -548,6 +572,8 @@ class FemPack:
         if self._engine is None:
             eng = FemEngine(self.device, self.precision)
             for m in self.models:
+                if m.isMixed():
+                    raise ValueError("a pack takes models of one element type each")
                 prm = np.zeros(8)
                 p = m.material.params()
                 prm[: len(p)] = p

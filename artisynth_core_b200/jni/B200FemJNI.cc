@@ -128,6 +128,26 @@ JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doSetMesh(JNIEnv* env,
   return b200fem_set_mesh(H(h), type, r.size() / 3, r.p, c.size() / nen, c.p, f.p);
 }
 
+// a model whose elements are of several classes: types[e] per element, conn
+// every element's nodes concatenated in element order
+JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doSetMeshMixed(JNIEnv* env, jclass, jlong h,
+                                                                         jintArray types, jdoubleArray rest,
+                                                                         jintArray conn, jintArray fixed) {
+  if (!types || !rest || !conn) return B200FEM_ERR_INVALID_ARG;
+  Ints t(env, types, false);
+  Doubles r(env, rest, false);
+  Ints c(env, conn, false);
+  Ints f(env, fixed, false);
+  long long total = 0;
+  for (jsize e = 0; e < t.size(); e++) {
+    const int k = nodes_per_elem(t.p[e]);
+    if (!k) return B200FEM_ERR_INVALID_ARG;
+    total += k;
+  }
+  if (total != c.size()) return B200FEM_ERR_INVALID_ARG;
+  return b200fem_set_mesh_mixed(H(h), r.size() / 3, r.p, t.size(), t.p, c.p, f.p);
+}
+
 JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doSetMaterial(JNIEnv* env, jclass, jlong h, jint kind,
                                                                         jdoubleArray params, jdouble density,
                                                                         jint incomp) {

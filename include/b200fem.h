@@ -158,6 +158,16 @@ int b200fem_jitter_grid(int nx, int ny, int nz, double wx, double wy, double wz,
 /* fixed[n] != 0 marks a non-dynamic node (no solve index) */
 int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double* rest_xyz,
                      int n_elems, const int* conn, const int* fixed);
+/* A mesh whose elements are of several types (FemModel3d holds any mix of
+   FemElement3d subclasses; computeStressAndStiffness, FemModel3d.java:3333,
+   runs over each element by its own type): elem_types[e] is element e's
+   B200FEM_ELEM_* type and conn holds every element's nodes concatenated in
+   element order (elem_nen(type) entries each).  Pattern, masses, forces,
+   stiffness and steps are those of the same elements in this order; soft
+   incompressibility AUTO resolves over all elements (NODAL only when every
+   element is a tet, hex, wedge or pyramid). */
+int b200fem_set_mesh_mixed(b200fem_handle h, int n_nodes, const double* rest_xyz, int n_elems,
+                           const int* elem_types, const int* conn, const int* fixed);
 int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, double density,
                          int incomp_method);
 /* builds rest data, the block pattern, the element-to-block scatter map and
@@ -175,7 +185,8 @@ int b200fem_get_crs_indices(b200fem_handle h, int partition, int* row_offs, int*
 /* CrsBlockSlotMap: 9 slots per block in BSR order, -1 when excluded */
 int b200fem_get_slot_map(b200fem_handle h, int partition, int* slots);
 /* element-to-block scatter map: for every element and every local node pair
-   (i, j) (nen*nen per element) the BSR block index receiving K_ij, or -1 */
+   (i, j) (nen*nen per element, concatenated in element order) the BSR block
+   index receiving K_ij, or -1 */
 int b200fem_get_scatter_map(b200fem_handle h, int* map);
 int b200fem_get_masses(b200fem_handle h, double* mass);
 int b200fem_get_incomp_method(b200fem_handle h, int* method);
@@ -257,7 +268,7 @@ int b200fem_pcg_solve(b200fem_handle h, const double* b, double* x, double tol, 
 int b200fem_last_timing(b200fem_handle h, double* assemble_ms, double* solve_ms);
 
 /* ---- batched form: several independent models in one handle ------------- */
-/* The handle's models form one "pack": one element type, any mix of
+/* The handle's models form one "pack": any mix of element types and
    materials; kernels run over all models at once (each PCG launch solves
    every model, each with its own scalars and convergence test).
    b200fem_set_mesh/_set_material define model 0; b200fem_add_model appends
