@@ -468,9 +468,6 @@ class FemModel3d:
         out = (f.reshape(-1, 3), K.reshape(-1, 3, 3))
         return out + (crs,) if want_crs else out
 
-    def lastStats(self):
-        return None
-
 
 class MechSystemSolver:
     """BackwardEuler integration of one FemModel3d on the device

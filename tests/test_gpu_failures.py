@@ -19,7 +19,8 @@ import pytest
 
 from artisynth_core_b200 import _lib as L
 from artisynth_core_b200 import workloads as W
-from artisynth_core_b200.femmodel import LinearMaterial, MechSystemSolver, NeoHookeanMaterial
+from artisynth_core_b200.femmodel import (LinearMaterial, MechSystemSolver, NeoHookeanMaterial,
+                                          StVenantKirchoffMaterial)
 
 pytestmark = pytest.mark.gpu
 
@@ -85,7 +86,9 @@ def _invert_one_element(rest, conn, fixed):
 
 
 def test_abort_on_inverted_elements(b200):
-    wl = W.small_tet_beam(LinearMaterial(5e4, 0.33, True))
+    # a non-linear material: the reference counts inverted elements where it
+    # forms the Jacobian, which linear materials skip (below)
+    wl = W.small_tet_beam(StVenantKirchoffMaterial(5e4, 0.3))
     m = _model(wl)
     x_bad = _invert_one_element(wl.rest, wl.conn, wl.fixed)
     v0 = np.zeros_like(x_bad)
@@ -96,11 +99,27 @@ def test_abort_on_inverted_elements(b200):
     assert b"inverted" in L.lib().b200fem_last_error(m.engine().h)
     x, v = m.getState()
     assert np.array_equal(x, x_bad) and np.array_equal(v, v0)  # the step did not run
-    # without the abort the step runs (corotated linear elements stay solvable)
-    # and reports the inverted elements
+    # without the abort the step runs and reports the inverted elements in
+    # its statistics (filled also when the solve misses its tolerance)
     ms.abort_on_inverted = False
+    try:
+        ms.backwardEuler(wl.h, 1)
+    except L.B200FemError as err:
+        assert err.status == L.ERR_NO_CONVERGE
+    assert ms.stats.num_inverted >= 1 and ms.stats.min_detJ < 0
+
+
+def test_linear_material_counts_no_inverted_elements(b200):
+    """Linear materials leave computeStressAndStiffness before any Jacobian
+    (FemModel3d.java:3356-3394: the warper's cached stiffness, then the early
+    return), so an inverted element neither aborts the step nor is counted."""
+    wl = W.small_tet_beam(LinearMaterial(5e4, 0.33, True))
+    m = _model(wl)
+    m.setState(_invert_one_element(wl.rest, wl.conn, wl.fixed), np.zeros_like(wl.rest))
+    ms = MechSystemSolver(m, tol=1e-12)
+    ms.abort_on_inverted = True
     st = ms.backwardEuler(wl.h, 1)
-    assert st.num_inverted >= 1 and st.min_detJ < 0
+    assert st.num_inverted == 0
 
 
 def test_non_finite_inputs_rejected(b200):
