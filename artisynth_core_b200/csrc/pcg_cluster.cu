@@ -118,13 +118,16 @@ __device__ __forceinline__ void cl_dir(double* pv, const double* z, const double
 }
 
 // y = (S v)_row on a group of kClLanes lanes (all lanes get the sum); the
-// vector is formed per neighbour by vec(pv, j)
+// vector is formed per neighbour by vec(pv, j).  Every lane of the warp
+// calls it together (the group sums are warp shuffles over the full mask); a
+// group whose row is past its range passes valid = false and adds nothing.
 template <typename MT, typename Vec>
-__device__ __forceinline__ void cl_row_spmv(const ClusterPcgArgs& a, int row, int gl, Vec vec, double* y) {
+__device__ __forceinline__ void cl_row_spmv(const ClusterPcgArgs& a, int row, bool valid, int gl, Vec vec,
+                                            double* y) {
   const MT* S = (const MT*)a.S;
   double acc[3] = {0, 0, 0};
-  const int p1 = a.rowptr[row + 1];
-  for (int p = a.rowptr[row] + gl; p < p1; p += kClLanes) {
+  const int p0 = valid ? a.rowptr[row] : 0, p1 = valid ? a.rowptr[row + 1] : 0;
+  for (int p = p0 + gl; p < p1; p += kClLanes) {
     const int j = a.col[p];
     double v[3];
     vec(v, j);
@@ -197,6 +200,8 @@ __global__ void __launch_bounds__(kClThreads) pcg_cluster_kernel(ClusterPcgArgs 
   __shared__ double tot[4];
   __shared__ int s_next;
   const int grp = threadIdx.x / kClLanes, gl = threadIdx.x % kClLanes;
+  constexpr int kWarpGroups = 32 / kClLanes;
+  const int wgrp = grp % kWarpGroups, wbase = grp - wgrp;  // group within the warp, warp's first group
   const bool leader = gl == 0;
   int slot = 0;
   for (;;) {
@@ -227,10 +232,14 @@ __global__ void __launch_bounds__(kClThreads) pcg_cluster_kernel(ClusterPcgArgs 
 
     // ---- block-Jacobi inverse, r = b - S x0, z = D^-1 r; ||b||^2, r.z, r.r
     double v3[3] = {0, 0, 0};
-    for (int row = c0 + grp; row < c1; row += kClGroups) {
+    // (loops with a shuffle run over warp-uniform bases: the warp's four
+    // groups take rows base .. base + 3)
+    for (int base = c0 + wbase; base < c1; base += kClGroups) {
+      const int row = base + wgrp;
+      const bool valid = row < c1;
       double Ax[3];
-      cl_row_spmv<MT>(a, row, gl, [&](double* pv, int j) { cl_load3(pv, a.x, j); }, Ax);
-      if (leader) {
+      cl_row_spmv<MT>(a, row, valid, gl, [&](double* pv, int j) { cl_load3(pv, a.x, j); }, Ax);
+      if (leader && valid) {
         const MT* Db = (const MT*)a.S + (size_t)a.blk_diag[row] * 9;
         double d[9], inv[9];
 #pragma unroll
@@ -287,10 +296,13 @@ __global__ void __launch_bounds__(kClThreads) pcg_cluster_kernel(ClusterPcgArgs 
       bool conv = rr2 <= thr2;
       while (!conv && it < a.max_iter) {
         double v1[1] = {0};
-        for (int row = c0 + grp; row < c1; row += kClGroups) {
+        for (int base = c0 + wbase; base < c1; base += kClGroups) {
+          const int row = base + wgrp;
+          const bool valid = row < c1;
           double qv[3];
-          cl_row_spmv<MT>(a, row, gl, [&](double* pv, int j) { cl_dir(pv, a.z, pold, j, beta, first); }, qv);
-          if (leader) {
+          cl_row_spmv<MT>(a, row, valid, gl, [&](double* pv, int j) { cl_dir(pv, a.z, pold, j, beta, first); },
+                          qv);
+          if (leader && valid) {
             double pv[3];
             cl_dir(pv, a.z, pold, row, beta, first);
             cl_project(a.row_nrm, row, qv);
@@ -334,10 +346,12 @@ __global__ void __launch_bounds__(kClThreads) pcg_cluster_kernel(ClusterPcgArgs 
       }
       // ---- the true residual decides (restart state if it misses)
       double v1[2] = {0, 0};
-      for (int row = c0 + grp; row < c1; row += kClGroups) {
+      for (int base = c0 + wbase; base < c1; base += kClGroups) {
+        const int row = base + wgrp;
+        const bool valid = row < c1;
         double Ax[3];
-        cl_row_spmv<MT>(a, row, gl, [&](double* pv, int j) { cl_load3(pv, a.x, j); }, Ax);
-        if (leader) {
+        cl_row_spmv<MT>(a, row, valid, gl, [&](double* pv, int j) { cl_load3(pv, a.x, j); }, Ax);
+        if (leader && valid) {
           double bv[3], rv[3], zz[3];
           cl_load3(bv, a.b, row);
 #pragma unroll
