@@ -21,10 +21,11 @@
 // order) and forms the right-hand side b = M v + h (m g + f_ext - f_int)
 // and the PCG's initial guess.
 //
-// The arithmetic is the element-and-gather path's, operation for operation
-// (the same element code, blocks of the upper pair transposed for the lower
-// position, the same summation orders), so S and b are bit-identical to
-// that path's.
+// The arithmetic is the element-and-gather path's, expression for
+// expression (the same element code, blocks of the upper pair transposed
+// for the lower position, the same summation orders), so S and b agree with
+// that path's to rounding (the compiler may contract a different product of
+// an expression into an FMA in the two kernels).
 #include <cuda_runtime.h>
 
 #include "device_math.cuh"

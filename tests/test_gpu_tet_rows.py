@@ -1,9 +1,13 @@
 """The node-row assembly of tetrahedral packs (B200FEM_OPT_TET_ASSEMBLY 0,
-the default) against the element kernel + block gather (option 1): same
-BackwardEuler steps bit for bit -- the node-row kernel repeats the element
-path's arithmetic operation for operation -- and against the oracle where
-the element path has no counterpart run (a node with 48 incident tets,
-which takes the 64-lane tasks).
+the default) against the element kernel + block gather (option 1): the
+node-row kernel repeats the element path's arithmetic expression for
+expression and sums in the same orders, so the BackwardEuler steps agree to
+rounding (the two kernels are compiled apart, and the compiler may fuse a
+different product of an expression into an FMA: NeoHookean steps differ in
+the last bit, StVenantKirchhoff and MooneyRivlin ones do not) -- bar 1e-14
+relative on positions and velocities, same PCG iterations -- and against the
+oracle where the element path has no counterpart run (a node with 48
+incident tets, which takes the 64-lane tasks).
 """
 import numpy as np
 import pytest
@@ -16,6 +20,13 @@ from artisynth_core_b200.femmodel import (FemPack, LinearMaterial, MechSystemSol
 from helpers import oracle_model, rel_err
 
 pytestmark = pytest.mark.gpu
+
+AGREE = 1e-14
+
+
+def _agree(s0, s1):
+    (x0, v0), (x1, v1) = s0, s1
+    return rel_err(x0, x1) <= AGREE and rel_err(v0, v1) <= AGREE
 
 
 def _model(wl, path, precision=L.PREC_FP64, incomp=None):
@@ -59,10 +70,10 @@ def test_node_rows_equal_element_path(b200, name, precision):
         assert _path_in_force(m.engine()) == path
         out.append((m.getState(), ms.stats.iterations))
         m._invalidate()
-    (x0, v0), it0 = out[0]
-    (x1, v1), it1 = out[1]
+    s0, it0 = out[0]
+    s1, it1 = out[1]
     assert it0 == it1
-    assert np.array_equal(x0, x1) and np.array_equal(v0, v1), (name, rel_err(x0, x1))
+    assert _agree(s0, s1), (name, rel_err(s0[0], s1[0]), rel_err(s0[1], s1[1]))
 
 
 def test_linear_material_keeps_element_path(b200):
@@ -102,8 +113,8 @@ def test_pack_of_mixed_materials_and_masks(b200):
         assert pack.option(L.OPT_TET_ASSEMBLY) == path
         res.append(pack.getStates())
         pack.close()
-    for (x0, v0), (x1, v1) in zip(*res):
-        assert np.array_equal(x0, x1) and np.array_equal(v0, v1)
+    for s0, s1 in zip(*res):
+        assert _agree(s0, s1)
 
 
 def test_plane_constraints_on_node_rows(b200):
@@ -123,7 +134,7 @@ def test_plane_constraints_on_node_rows(b200):
         ms.backwardEuler(wl.h, 4)
         out.append(m.getState())
         m._invalidate()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert _agree(out[0], out[1])
 
 
 def _fan_mesh():
@@ -182,7 +193,7 @@ def test_high_valence_node_vs_oracle(b200, oracle):
         assert _path_in_force(m.engine()) == path
         states.append(m.getState())
         m._invalidate()
-    assert np.array_equal(states[0][0], states[1][0])
+    assert _agree(states[0], states[1])
     om = oracle_model(oracle, wl)
     x = xyz.copy()
     v = np.zeros_like(x)
