@@ -388,6 +388,7 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
     pack_lanes, pack_tile = pack.option(L.OPT_ROW_LANES), pack.option(L.OPT_ELEM_TILE)
     split = pack.option(L.OPT_PCG_SPLIT)
     fused = pack.option(L.OPT_FUSED_ASSEMBLY) == 1
+    node_rows = pack.option(L.OPT_TET_ASSEMBLY) == 0
     nbytes = pack.deviceBytes()
     import ctypes
     na, nb = ctypes.c_int(), ctypes.c_int()
@@ -438,12 +439,12 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
     return {
         "workload": "256 uneven NeoHookean tet beams (n 4-60, m 2-8, seed 3), 20 steps h=0.01",
         "models": n, "tets": int(sum(b.conn.shape[0] for b in bs)), "steps": steps, "tol": tol,
-        "precision": "mixed FP32 element/SpMV, FP64 vectors", "pcg_split": "strided" if split == 2 else "contiguous",
+        "precision": "mixed FP32 element/SpMV, FP64 vectors", "pcg_split": {1: "contiguous", 2: "strided", 3: "cluster"}.get(split, str(split)),
         "device_bytes": nbytes, "build_and_tune_s": build_s,
         "tuned": {k: v for k, v in tuned.items() if not k.endswith("_ms") and not k.endswith("_it")},
         "model_steps_per_s": n * steps / wall, "device_ms_per_step": (asm + pcg) / steps,
         "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
-        "assembly": {"path": "fused row-chunk" if fused else "element kernel + gather",
+        "assembly": {"path": "fused row-chunk" if fused else "node rows" if node_rows else "element kernel + gather",
                      "algorithmic_bytes": asm_bytes, "achieved_gbs": asm_gbs, "peak_gbs": peak,
                      "frac": asm_gbs / peak, "peak_kind": kind, "nnzb": nb.value},
         "element_updates_per_s": sum(b.conn.shape[0] for b in bs) * steps / wall,
