@@ -597,14 +597,13 @@ int build_pack(Engine& eng) {
     if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
     eng.pcg_resident = eng.pcg_cached = 0;
   }
-  // cluster split: one thread-block cluster per model, models taken from a
-  // queue largest first (pcg_cluster.cu); for packs of many models that do
-  // not fit shared-memory residency
+  // cluster split (on request): one thread-block cluster per model, models
+  // taken from a queue largest first (pcg_cluster.cu)
   eng.pcg_cluster = false;
-  if (eng.opt_split == 3 || (eng.opt_split == 0 && !eng.pcg_resident && M > 1)) {
+  if (eng.opt_split == 3) {
     eng.cl_clusters = pcg_cluster_capacity(eng.precision == B200FEM_PREC_MIXED);
     if (eng.cl_clusters > 0) eng.pcg_cluster = true;
-    else if (eng.opt_split == 3) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "thread-block clusters unavailable");
+    else return fail(&eng, B200FEM_ERR_UNSUPPORTED, "thread-block clusters unavailable");
   }
   if (eng.opt_split == 2 || (eng.opt_split == 0 && !eng.pcg_resident && M > 1)) {
     // Strided split for packs too large for shared-memory residency: every

@@ -343,10 +343,12 @@ def _fp64_alone(w, steps, tol, dev):
     return x
 
 
-def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
+def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True, layout=None):
     """Batched uneven models: 256 NeoHookean tet beams in one pack (mixed
     FP32/FP64), `steps` BackwardEuler steps; next to the plain FP64 drop-in
-    stepping the models one at a time (every `sample_every`-th model)."""
+    stepping the models one at a time (every `sample_every`-th model).
+    `layout`: build-time options fixed for the pack (e.g. the PCG split or
+    the tet assembly path, to compare the alternatives)."""
     import torch
     from artisynth_core_b200 import _lib as L
     from artisynth_core_b200 import workloads as W
@@ -359,7 +361,7 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True):
     models = [b.model(device=dev) for b in bs]
 
     def make(opts):
-        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options=opts)
+        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options=dict(layout or {}, **opts))
         p.engine()
         return p
 
@@ -889,6 +891,10 @@ def main():
                     help="run only this leg (for profiling): prints its JSON object")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-tune", action="store_true", help="batched leg without the autotuner")
+    ap.add_argument("--pcg-split", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="batched leg: B200FEM_OPT_PCG_SPLIT (0 auto, 2 strided, 3 cluster)")
+    ap.add_argument("--tet-assembly", type=int, default=1, choices=[0, 1],
+                    help="batched leg: B200FEM_OPT_TET_ASSEMBLY (0 node rows, 1 element kernel + gather)")
     ap.add_argument("--served-seconds", type=float, default=60.0, help="length of the served stream (0: skip)")
     ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched leg")
     ap.add_argument("--served-tol", type=float, default=1e-6,
@@ -901,8 +907,12 @@ def main():
     elif args.only == "batched":
         import torch
         torch.cuda.set_device(0)
+        from artisynth_core_b200 import _lib as L
+        layout = {L.OPT_TET_ASSEMBLY: args.tet_assembly}
+        if args.pcg_split:
+            layout[L.OPT_PCG_SPLIT] = args.pcg_split
         print(json.dumps(run_batched(0, steps=args.batch_steps, tol=args.batch_tol, sample_every=64,
-                                     tune=not args.no_tune)), flush=True)
+                                     tune=not args.no_tune, layout=layout)), flush=True)
     elif args.only == "block":
         import torch
         torch.cuda.set_device(0)

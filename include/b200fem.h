@@ -307,8 +307,11 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                     resident when they fit); 2 strided: every model cut
                                     into short pieces dealt over all CTAs; 3 cluster: one
                                     thread-block cluster per model, models taken from a
-                                    queue largest first (auto picks it for packs of several
-                                    models that do not fit shared-memory residency) */
+                                    queue largest first.  Auto: contiguous when the rows fit
+                                    shared-memory residency or the handle has one model,
+                                    else strided (on the 256-beam pack the strided split
+                                    measured 10.1 ms per step against the cluster split's
+                                    14.2: the slowest model is held to one cluster) */
 #define B200FEM_OPT_ROW_LANES 2  /* lanes per block row in the iteration SpMV: 0 auto, 4, 8, 16, 32 */
 #define B200FEM_OPT_PCG_CTAS 3   /* CTAs of the persistent PCG kernel: 0 auto (one per SM) */
 #define B200FEM_OPT_PIECE_ROWS 4 /* block rows per piece in the strided split: 0 auto (64) */
@@ -346,12 +349,15 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                            so every wait there runs out after
                                            B200FEM_OPT_BARRIER_TIMEOUT_MS; 0 (default) off */
 #define B200FEM_OPT_TET_ASSEMBLY 11 /* BackwardEuler assembly of tetrahedral packs with non-linear
-                                       materials: 0 (default) node-row kernel -- a warp per few block
-                                       rows recomputes each incident tetrahedron and sums the rows'
+                                       materials: 0 node-row kernel -- a warp per few block rows
+                                       recomputes each incident tetrahedron and sums the rows'
                                        blocks, forces and right-hand side, with no element data in
-                                       HBM; 1 element kernel + block gather.  Both give the same S
-                                       and b bit for bit.  Set before b200fem_build; after it, 0
-                                       reads back as 1 where the node-row path does not apply */
+                                       HBM; 1 (default) element kernel + block gather.  S and b
+                                       agree to rounding.  The node-row kernel evaluates every
+                                       tetrahedron four times and is compute-bound: 1.10 ms per
+                                       step on the 256-beam pack against 0.59 for the element
+                                       path.  Set before b200fem_build; after it, 0 reads back
+                                       as 1 where the node-row path does not apply */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
