@@ -361,7 +361,7 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True, layout=None
     models = [b.model(device=dev) for b in bs]
 
     def make(opts):
-        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options=dict(layout or {}, **opts))
+        p = FemPack(models, precision=L.PREC_MIXED, device=dev, options={**(layout or {}), **opts})
         p.engine()
         return p
 
