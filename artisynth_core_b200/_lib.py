@@ -38,6 +38,7 @@ OPT_PCG_SPLIT, OPT_ROW_LANES, OPT_PCG_CTAS, OPT_PIECE_ROWS, OPT_WARM_START, OPT_
 OPT_REFINE = 8
 OPT_BARRIER_TIMEOUT_MS, OPT_TEST_SKIP_ARRIVAL = 9, 10
 OPT_TET_ASSEMBLY = 11
+OPT_PCG_RESIDENT = 12
 INTEGRATOR_BACKWARD_EULER, INTEGRATOR_CONSTRAINED_BACKWARD_EULER = 0, 1
 SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED, SPLIT_CLUSTER = 0, 1, 2, 3
 

@@ -592,6 +592,7 @@ int build_pack(Engine& eng) {
   }
   pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
                 eng.precision == B200FEM_PREC_MIXED);
+  if (eng.opt_resident == 1) eng.pcg_resident = eng.pcg_cached = 0;
   eng.pcg_strided = 0;
   if (!contiguous_ok) {
     if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
@@ -1222,6 +1223,11 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
         eng.step_exec_max_iter = -1;  // recapture: the width is a kernel argument
       }
       return B200FEM_OK;
+    case B200FEM_OPT_PCG_RESIDENT:
+      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_RESIDENT must be 0, 1 or 2");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_RESIDENT is set before b200fem_build");
+      eng.opt_resident = value;
+      return B200FEM_OK;
     case B200FEM_OPT_TET_ASSEMBLY:
       if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "TET_ASSEMBLY must be 0 or 1");
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "TET_ASSEMBLY is set before b200fem_build");
@@ -1262,6 +1268,7 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_REFINE: *value = (eng.built && !eng.refine_ok) ? 0 : eng.opt_refine; break;
     case B200FEM_OPT_BARRIER_TIMEOUT_MS: *value = eng.barrier_timeout_ms; break;
     case B200FEM_OPT_TET_ASSEMBLY: *value = eng.built ? (eng.tet_rows ? 0 : 1) : eng.opt_tet_assembly; break;
+    case B200FEM_OPT_PCG_RESIDENT: *value = eng.built ? (eng.pcg_resident ? 2 : 1) : eng.opt_resident; break;
     case B200FEM_OPT_TEST_SKIP_ARRIVAL: *value = eng.test_skip_arrival; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }

@@ -338,6 +338,7 @@ struct Engine {
   // BackwardEuler assembly of tet packs on the node-row path (tet_rows.cu):
   // B200FEM_OPT_TET_ASSEMBLY 0 (default) where supported, 1 element kernel + gather
   int opt_tet_assembly = 1;  // element path (B200FEM_OPT_TET_ASSEMBLY)
+  int opt_resident = 0;      // B200FEM_OPT_PCG_RESIDENT
   bool tet_rows = false;
   int rows_cap = 32;                   // incidences per task (32 or 64)
   std::vector<int> rows_task_off;      // per element group: its task range
