@@ -592,7 +592,14 @@ int build_pack(Engine& eng) {
   }
   pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
                 eng.precision == B200FEM_PREC_MIXED);
-  if (eng.opt_resident == 1) eng.pcg_resident = eng.pcg_cached = 0;
+  // Shared-memory row state pays off while the solve matrix stays in L2
+  // (the 40x10x10 hex beam, 8 MB: 5.6 us per iteration resident, 9.6 with
+  // global vectors); a matrix streamed from HBM needs the non-resident
+  // form's 1024-thread CTAs, twice the warps for its loads (the 60x30x30
+  // MooneyRivlin block, 142 MB FP32: 60 us per iteration against 78
+  // resident).  Auto: resident up to 64 MB of S.
+  const double s_bytes = 9.0 * (eng.precision == B200FEM_PREC_MIXED ? 4 : 8) * (double)NB;
+  if (eng.opt_resident == 1 || (eng.opt_resident == 0 && s_bytes > 64e6)) eng.pcg_resident = eng.pcg_cached = 0;
   eng.pcg_strided = 0;
   if (!contiguous_ok) {
     if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
@@ -682,8 +689,10 @@ int build_pack(Engine& eng) {
     const double bpr = R > 0 ? (double)NB / R : 1.0;
     // many rows in flight per warp do best up to hexes' ~27 blocks per row
     // (measured: 40x10x10 hex beam 6.8 us per iteration at 4 lanes, 7.1
-    // at 16); NODAL 2-ring rows -> 32
-    eng.pcg_row_lanes = bpr <= 40 ? 4 : 32;
+    // at 16); NODAL 2-ring rows (~69 blocks) -> 16 (the 60x30x30
+    // MooneyRivlin block: 60.4 us per iteration mixed at 16 lanes, 62.9 at
+    // 32, 62.3 at 8)
+    eng.pcg_row_lanes = bpr <= 40 ? 4 : 16;
   }
 
   // ---- device upload
@@ -724,6 +733,12 @@ int build_pack(Engine& eng) {
     for (int r = 0; r < R; r++)
       for (int p = rowptr[r]; p < rowptr[r + 1]; p++) mirror[p] = block_of(col[p], r);
     CK(upload(eng, &d.blk_mirror, mirror));
+    std::vector<int> up;
+    up.reserve(NB / 2 + R);
+    for (long long p = 0; p < NB; p++)
+      if (!(mirror[p] >= 0 && mirror[p] < p)) up.push_back((int)p);
+    d.n_up = (long long)up.size();
+    CK(upload(eng, &d.up_blocks, up));
   }
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));

@@ -193,6 +193,8 @@ struct DevPack {
   int* chunk_elem = nullptr;
   int* contrib_loc = nullptr;  // parallel to contrib_idx
   int* blk_mirror = nullptr;   // nnzb: the block at the transposed position
+  int* up_blocks = nullptr;    // the upper blocks (column >= row), in BSR order
+  long long n_up = 0;
   // node-row tet assembly (tet_rows.cu): tasks of block rows, the rows'
   // element incidences, and per contribution the stage entry it reads
   int* task_row = nullptr;     // tasks+1

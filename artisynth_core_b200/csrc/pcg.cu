@@ -372,13 +372,9 @@ struct MatView {
   int cached;
 };
 
-// One lane's walk over blocks p, p + stride, ... < p1 of a block row:
-// a += S_p x_col(p), blocks added in increasing p.  The x gathers of two
-// blocks are issued together, so a lane waits for one L2 round trip per
-// two blocks; a missing second block multiplies a zero x.
-template <typename MT>
-__device__ __forceinline__ void block_row_walk(const int* col, const MT* S, const double* x, int p, int p1,
-                                               int stride, double& a0, double& a1, double& a2) {
+// the FP64-value walk of block_row_walk (below)
+__device__ __forceinline__ void block_row_walk_f64(const int* col, const double* S, const double* x, int p, int p1,
+                                                   int stride, double& a0, double& a1, double& a2) {
   for (; p < p1; p += 2 * stride) {
     const int pb = p + stride;
     const bool hb = pb < p1;
@@ -392,19 +388,71 @@ __device__ __forceinline__ void block_row_walk(const int* col, const MT* S, cons
       xb2 = x[3 * (size_t)cb + 2];
     }
     {
-      const MT* B = S + (size_t)p * 9;
-      double b[9];
-#pragma unroll
-      for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+      const double* b = S + (size_t)p * 9;
       a0 += b[0] * xa0 + b[1] * xa1 + b[2] * xa2;
       a1 += b[3] * xa0 + b[4] * xa1 + b[5] * xa2;
       a2 += b[6] * xa0 + b[7] * xa1 + b[8] * xa2;
     }
     if (hb) {
-      const MT* B = S + (size_t)pb * 9;
+      const double* b = S + (size_t)pb * 9;
+      a0 += b[0] * xb0 + b[1] * xb1 + b[2] * xb2;
+      a1 += b[3] * xb0 + b[4] * xb1 + b[5] * xb2;
+      a2 += b[6] * xb0 + b[7] * xb1 + b[8] * xb2;
+    }
+  }
+}
+__device__ __forceinline__ void block_row_walk_f64(const int*, const float*, const double*, int, int, int, double&,
+                                                   double&, double&) {}
+
+// One lane's walk over blocks p, p + stride, ... < p1 of a block row:
+// a += S_p x_col(p), blocks added in increasing p.  FP32 values: per step
+// of two blocks the column indices and both blocks' values are loaded
+// together (the values do not depend on the columns: streamed from HBM they
+// overlap the index loads), then the two x gathers, so a lane waits for one
+// HBM and one L2 round trip per two blocks; a missing second block reloads
+// the first block's values and is not added.  FP64 values (18 more
+// registers than the 1024-thread kernel has to spare): the x gathers of the
+// two blocks are issued together, then each block's values.
+template <typename MT>
+__device__ __forceinline__ void block_row_walk(const int* col, const MT* S, const double* x, int p, int p1,
+                                               int stride, double& a0, double& a1, double& a2) {
+  if constexpr (sizeof(MT) == 8) {
+    block_row_walk_f64(col, S, x, p, p1, stride, a0, a1, a2);
+    return;
+  }
+  for (; p < p1; p += 2 * stride) {
+    const int pb = p + stride;
+    const bool hb = pb < p1;
+    const int ca = col[p];
+    const int cb = hb ? col[pb] : ca;
+    MT ba[9], bb[9];
+    {
+      const MT* A = S + (size_t)p * 9;
+      const MT* B = S + (size_t)(hb ? pb : p) * 9;
+#pragma unroll
+      for (int k = 0; k < 9; k++) ba[k] = A[k];
+#pragma unroll
+      for (int k = 0; k < 9; k++) bb[k] = B[k];
+    }
+    const double xa0 = x[3 * (size_t)ca], xa1 = x[3 * (size_t)ca + 1], xa2 = x[3 * (size_t)ca + 2];
+    double xb0 = 0, xb1 = 0, xb2 = 0;
+    if (hb) {
+      xb0 = x[3 * (size_t)cb];
+      xb1 = x[3 * (size_t)cb + 1];
+      xb2 = x[3 * (size_t)cb + 2];
+    }
+    {
       double b[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) b[k] = (double)B[k];
+      for (int k = 0; k < 9; k++) b[k] = (double)ba[k];
+      a0 += b[0] * xa0 + b[1] * xa1 + b[2] * xa2;
+      a1 += b[3] * xa0 + b[4] * xa1 + b[5] * xa2;
+      a2 += b[6] * xa0 + b[7] * xa1 + b[8] * xa2;
+    }
+    if (hb) {
+      double b[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) b[k] = (double)bb[k];
       a0 += b[0] * xb0 + b[1] * xb1 + b[2] * xb2;
       a1 += b[3] * xb0 + b[4] * xb1 + b[5] * xb2;
       a2 += b[6] * xb0 + b[7] * xb1 + b[8] * xb2;

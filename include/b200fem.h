@@ -358,11 +358,12 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                        step on the 256-beam pack against 0.59 for the element
                                        path.  Set before b200fem_build; after it, 0 reads back
                                        as 1 where the node-row path does not apply */
-#define B200FEM_OPT_PCG_RESIDENT 12 /* row state of the contiguous split's PCG: 0 (auto) in shared
-                                       memory when the CTA's rows fit (512-thread CTAs, one per
-                                       SM); 1 never (1024-thread CTAs, global vectors: twice the
-                                       warps for the SpMV's loads); 2 when it fits.  Set before
-                                       b200fem_build; after it, 2 or 1 as in force */
+#define B200FEM_OPT_PCG_RESIDENT 12 /* row state of the contiguous split's PCG: 2 in shared memory
+                                       when the CTA's rows fit (512-thread CTAs, one per SM); 1
+                                       never (1024-thread CTAs, global vectors: twice the warps
+                                       for the SpMV's loads); 0 (auto) as 2 while the solve
+                                       matrix is at most 64 MB (it stays in L2), else as 1.  Set
+                                       before b200fem_build; after it, 2 or 1 as in force */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);

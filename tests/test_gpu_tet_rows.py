@@ -4,8 +4,10 @@ node-row kernel repeats the element path's arithmetic expression for
 expression and sums in the same orders, so the BackwardEuler steps agree to
 rounding (the two kernels are compiled apart, and the compiler may fuse a
 different product of an expression into an FMA: NeoHookean steps differ in
-the last bit, StVenantKirchhoff and MooneyRivlin ones do not) -- bar 1e-14
-relative on positions and velocities, same PCG iterations -- and against the
+the last bit, StVenantKirchhoff and MooneyRivlin ones do not) -- bars 1e-13
+relative on positions and 1e-11 on velocities (a last-bit change of S and b
+moves the PCG's iterates by round-off amplified by the condition number;
+measured 2e-16 and 2e-14), same PCG iterations -- and against the
 oracle where the element path has no counterpart run (a node with 48
 incident tets, which takes the 64-lane tasks).
 """
@@ -21,12 +23,12 @@ from helpers import oracle_model, rel_err
 
 pytestmark = pytest.mark.gpu
 
-AGREE = 1e-14
+AGREE_X, AGREE_V = 1e-13, 1e-11
 
 
 def _agree(s0, s1):
     (x0, v0), (x1, v1) = s0, s1
-    return rel_err(x0, x1) <= AGREE and rel_err(v0, v1) <= AGREE
+    return rel_err(x0, x1) <= AGREE_X and rel_err(v0, v1) <= AGREE_V
 
 
 def _model(wl, path, precision=L.PREC_FP64, incomp=None):
