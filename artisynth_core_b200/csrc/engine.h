@@ -361,6 +361,10 @@ struct Engine {
   cudaGraphExec_t asm_exec = nullptr;
   cudaGraphExec_t step_exec = nullptr;
   int step_exec_max_iter = -1;
+  // one step from page-locked host state as one graph (the buffers it holds)
+  cudaGraphExec_t host_exec = nullptr;
+  const double* host_x = nullptr;
+  const double* host_v = nullptr;
   bool use_graphs = true;
   // last timing
   float last_asm_ms = 0, last_solve_ms = 0, last_call_ms = 0;

@@ -62,3 +62,48 @@ def test_host_changed_state_solves_to_tolerance(b200):
         sb.backwardEulerHost(wl.h, x, v)
     xa, _ = a.getState()
     assert rel_err(x, xa.reshape(-1)) <= 1e-8
+
+
+def _pinned(a):
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    p = t.numpy()
+    p[:] = a
+    return t, p
+
+
+def test_page_locked_host_state_one_graph(b200):
+    """Page-locked x and v take the single-graph path (copies in, step, copies
+    out, status in one launch): bit-identical to device-resident steps and to
+    the pageable path, also when the host hands over other page-locked
+    buffers, or pageable ones, between calls."""
+    wl = _wl()
+    a = wl.model()
+    sa = MechSystemSolver(a, tol=1e-10)
+    b = wl.model()
+    sb = MechSystemSolver(b, tol=1e-10)
+    x0 = np.ascontiguousarray(wl.rest.reshape(-1).copy())
+    keep = []
+    tx, x = _pinned(x0)
+    tv, v = _pinned(np.zeros_like(x0))
+    keep += [tx, tv]
+    for step in range(8):
+        if step == 3:  # other page-locked buffers (captured again)
+            tx, x2 = _pinned(x)
+            tv, v2 = _pinned(v)
+            keep += [tx, tv]
+            x, v = x2, v2
+        if step == 5:  # pageable buffers (copies issued one by one)
+            x, v = np.ascontiguousarray(x.copy()), np.ascontiguousarray(v.copy())
+        if step == 7:  # page-locked again
+            tx, x2 = _pinned(x)
+            tv, v2 = _pinned(v)
+            keep += [tx, tv]
+            x, v = x2, v2
+        sa.backwardEuler(wl.h, 1)
+        sb.backwardEulerHost(wl.h, x, v)
+        assert sb.stats.iterations == sa.stats.iterations, step
+        xa, va = a.getState()
+        assert np.array_equal(x, xa.reshape(-1)) and np.array_equal(v, va.reshape(-1)), step
+        asm, solve = sb.lastTiming()
+        assert asm > 0 and solve > 0
