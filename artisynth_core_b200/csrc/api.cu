@@ -481,6 +481,9 @@ int build_pack(Engine& eng) {
         mat_node[2 * (size_t)(no + n) + 1] = eng.models[m].mat_params[7];
       }
     }
+    int max_nbr = 0;
+    for (int n = 0; n < N; n++) max_nbr = std::max(max_nbr, nbr_ptr[n + 1]);
+    eng.divblk_smem = max_nbr <= 32;  // kDivSmemSlots
     for (int n = 0; n < N; n++) nbr_ptr[n + 1] += nbr_ptr[n];
     nbr_idx.resize(nbr_ptr[N]);
     for (int m = 0; m < M; m++) {

@@ -1735,6 +1735,77 @@ __global__ void divblk_kernel(int N, const int* __restrict__ inc_ptr, const int*
   }
 }
 
+// divBlk per node with the node's sums in shared memory (nodes of at most
+// kDivSmemSlots direct neighbours): the same terms added in the same order as
+// divblk_kernel, but each += is a shared-memory update instead of a global
+// load-add-store chain.  Slot s, component c of thread t lives at
+// acc[(3 s + c) * blockDim + t], so a warp's threads touch consecutive words.
+constexpr int kDivSmemSlots = 32;
+constexpr int kDivSmemThreads = 64;
+template <int TYPE>
+__global__ void __launch_bounds__(kDivSmemThreads) divblk_smem_kernel(
+    int N, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx, const int* __restrict__ inc_slot,
+    const int* __restrict__ conn, const double* __restrict__ x, const int* __restrict__ sidx,
+    const int* __restrict__ nbr_ptr, double* __restrict__ divblk) {
+  constexpr int NEN = elem_nen(TYPE);
+  __shared__ double acc[3 * kDivSmemSlots * kDivSmemThreads];
+  const int t = threadIdx.x;
+  const int n = blockIdx.x * kDivSmemThreads + t;
+  if (n >= N) return;  // no block-wide barrier below
+  const int ns = nbr_ptr[n + 1] - nbr_ptr[n];
+  auto A = [&](int slot, int c) -> double& { return acc[(3 * slot + c) * kDivSmemThreads + t]; };
+  for (int q = 0; q < ns; q++) A(q, 0) = A(q, 1) = A(q, 2) = 0;
+  if (sidx[n] >= 0) {
+    for (int i = inc_ptr[n]; i < inc_ptr[n + 1]; i++) {
+      const int a = inc_idx[i] % NEN;
+      const int* nodes = conn + (inc_idx[i] - a);
+      const int* slot = inc_slot + (size_t)i * NEN;
+      if constexpr (TYPE == B200FEM_ELEM_TET) {
+        const double* P[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) P[k] = x + 3 * (size_t)nodes[k];
+        // faces opposite nodes 0..3: (1,2,3), (0,3,2), (0,1,3), (0,2,1)
+        const int f[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double *q0 = P[f[j][0]], *q1 = P[f[j][1]], *q2 = P[f[j][2]];
+          const double ux = q1[0] - q0[0], uy = q1[1] - q0[1], uz = q1[2] - q0[2];
+          const double vx = q2[0] - q0[0], vy = q2[1] - q0[1], vz = q2[2] - q0[2];
+          const int sj = slot[j];
+          A(sj, 0) += 0.5 * (uy * vz - uz * vy) * (-1 / 12.0);
+          A(sj, 1) += 0.5 * (uz * vx - ux * vz) * (-1 / 12.0);
+          A(sj, 2) += 0.5 * (ux * vy - uy * vx) * (-1 / 12.0);
+        }
+      } else {
+        double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
+#pragma unroll
+        for (int k = 0; k < NEN; k++) {
+          const double* pk = x + 3 * (size_t)nodes[k];
+#pragma unroll
+          for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) J[3 * r + c] += pk[r] * gns<double, TYPE>(a, k, c);
+        }
+        const double dv = invert3(iJ, J) * ip_weight<double, TYPE>(a);
+#pragma unroll
+        for (int k = 0; k < NEN; k++) {
+          const double g0 = gns<double, TYPE>(a, k, 0), g1 = gns<double, TYPE>(a, k, 1),
+                       g2 = gns<double, TYPE>(a, k, 2);
+          const int sk = slot[k];
+#pragma unroll
+          for (int c = 0; c < 3; c++) A(sk, c) += dv * (iJ[c] * g0 + iJ[3 + c] * g1 + iJ[6 + c] * g2);
+        }
+      }
+    }
+  }
+  double* out = divblk + 3 * (size_t)nbr_ptr[n];
+  for (int q = 0; q < ns; q++) {
+    out[3 * q] = A(q, 0);
+    out[3 * q + 1] = A(q, 1);
+    out[3 * q + 2] = A(q, 2);
+  }
+}
+
 // the same for a pack of several element types (nm slots per incidence)
 __global__ void divblk_mixed_kernel(int N, int nm, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
                                     const int* __restrict__ inc_tl, const int* __restrict__ inc_slot,
@@ -1798,8 +1869,13 @@ cudaError_t launch_divblk(Engine& eng) {
     if constexpr (TY != B200FEM_ELEM_TET && !elem_ip_at_nodes(TY)) {
       return cudaErrorNotSupported;
     } else {
-      divblk_kernel<TY><<<blocks, threads, 0, eng.stream>>>(
-          d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
+      if (eng.divblk_smem)
+        divblk_smem_kernel<TY><<<(d.n_nodes + kDivSmemThreads - 1) / kDivSmemThreads, kDivSmemThreads, 0,
+                                 eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx,
+                                               d.nbr_ptr, d.divblk);
+      else
+        divblk_kernel<TY><<<blocks, threads, 0, eng.stream>>>(
+            d.n_nodes, d.inc_ptr, d.inc_idx, d.inc_slot, d.conn, d.x, d.sidx, d.nbr_ptr, d.divblk);
       return cudaGetLastError();
     }
   });
