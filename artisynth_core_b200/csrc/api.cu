@@ -678,12 +678,6 @@ int build_pack(Engine& eng) {
       break;
     }
   }
-  // symmetric read of the solve matrix (lower blocks through their upper
-  // mirrors) where S streams from HBM in row order: one model per CTA range
-  // (contiguous split), above the 64 MB that stay in L2
-  eng.sym_spmv = eng.opt_sym == 2 ? !eng.pcg_cached
-                                  : eng.opt_sym == 0 && !eng.pcg_resident && !eng.pcg_cached && !eng.pcg_strided &&
-                                        !eng.pcg_cluster && s_bytes > 64e6;
   for (size_t k = 0; k < piece_model.size(); k++) model_piece[piece_model[k] + 1] = (int)k + 1;
   for (int m = 0; m < M; m++) model_piece[m + 1] = std::max(model_piece[m + 1], model_piece[m]);
   eng.pcg_grid = G;
@@ -1257,11 +1251,6 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
         eng.step_exec_max_iter = -1;  // recapture: the width is a kernel argument
       }
       return B200FEM_OK;
-    case B200FEM_OPT_SYM_SPMV:
-      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "SYM_SPMV must be 0, 1 or 2");
-      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "SYM_SPMV is set before b200fem_build");
-      eng.opt_sym = value;
-      return B200FEM_OK;
     case B200FEM_OPT_PCG_RESIDENT:
       if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "PCG_RESIDENT must be 0, 1 or 2");
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_RESIDENT is set before b200fem_build");
@@ -1308,7 +1297,6 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_BARRIER_TIMEOUT_MS: *value = eng.barrier_timeout_ms; break;
     case B200FEM_OPT_TET_ASSEMBLY: *value = eng.built ? (eng.tet_rows ? 0 : 1) : eng.opt_tet_assembly; break;
     case B200FEM_OPT_PCG_RESIDENT: *value = eng.built ? (eng.pcg_resident ? 2 : 1) : eng.opt_resident; break;
-    case B200FEM_OPT_SYM_SPMV: *value = eng.built ? (eng.sym_spmv ? 2 : 1) : eng.opt_sym; break;
     case B200FEM_OPT_TEST_SKIP_ARRIVAL: *value = eng.test_skip_arrival; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }

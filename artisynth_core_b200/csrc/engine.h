@@ -342,8 +342,6 @@ struct Engine {
   // B200FEM_OPT_TET_ASSEMBLY 0 (default) where supported, 1 element kernel + gather
   int opt_tet_assembly = 1;  // element path (B200FEM_OPT_TET_ASSEMBLY)
   int opt_resident = 0;      // B200FEM_OPT_PCG_RESIDENT
-  int opt_sym = 0;           // B200FEM_OPT_SYM_SPMV
-  bool sym_spmv = false;     // the PCG reads lower blocks through their upper mirrors
   bool tet_rows = false;
   int rows_cap = 32;                   // incidences per task (32 or 64)
   std::vector<int> rows_task_off;      // per element group: its task range

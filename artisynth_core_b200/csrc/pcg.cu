@@ -138,7 +138,6 @@ struct PcgArgs {
   int max_iter;
   int variant;  // 0 auto (pipelined, classic after a residual replacement), 1 classic, 2 pipelined
   int row_lanes;  // lanes per block row in the iteration SpMV (4, 8, 16, 32)
-  const int* mirror;  // the block at the transposed position, for the symmetric read (or null)
   int update_state;
   double* xpos;
   double* vprev;  // receives the velocity before the update
@@ -367,7 +366,6 @@ struct MatView {
   const int* rowptr;
   const int* col;
   const MT* S;
-  const int* mirror;  // symmetric read of lower blocks (null: every block read in place)
   const int* ro_s;
   const int* col_s;
   const MT* S_s;
@@ -375,16 +373,13 @@ struct MatView {
 };
 
 // the FP64-value walk of block_row_walk (below)
-__device__ __forceinline__ void block_row_walk_f64(const int* col, const double* S, const int* mirror, int row,
-                                                   const double* x, int p, int p1, int stride, double& a0,
-                                                   double& a1, double& a2) {
+__device__ __forceinline__ void block_row_walk_f64(const int* col, const double* S, const double* x, int p, int p1,
+                                                   int stride, double& a0, double& a1, double& a2) {
   for (; p < p1; p += 2 * stride) {
     const int pb = p + stride;
     const bool hb = pb < p1;
     const int ca = col[p];
     const int cb = hb ? col[pb] : ca;
-    const bool ta = mirror && ca < row, tb = mirror && hb && cb < row;
-    const int qa = ta ? mirror[p] : p, qb = tb ? mirror[pb] : pb;
     const double xa0 = x[3 * (size_t)ca], xa1 = x[3 * (size_t)ca + 1], xa2 = x[3 * (size_t)ca + 2];
     double xb0 = 0, xb1 = 0, xb2 = 0;
     if (hb) {
@@ -393,24 +388,21 @@ __device__ __forceinline__ void block_row_walk_f64(const int* col, const double*
       xb2 = x[3 * (size_t)cb + 2];
     }
     {
-      const double* b = S + (size_t)qa * 9;
-      // entry (r, c) of the block: b[3r + c], or b[3c + r] of its upper mirror
-      const int s1 = ta ? 3 : 1, s3 = ta ? 1 : 3;
-      a0 += b[0] * xa0 + b[s1] * xa1 + b[2 * s1] * xa2;
-      a1 += b[s3] * xa0 + b[s3 + s1] * xa1 + b[s3 + 2 * s1] * xa2;
-      a2 += b[2 * s3] * xa0 + b[2 * s3 + s1] * xa1 + b[2 * s3 + 2 * s1] * xa2;
+      const double* b = S + (size_t)p * 9;
+      a0 += b[0] * xa0 + b[1] * xa1 + b[2] * xa2;
+      a1 += b[3] * xa0 + b[4] * xa1 + b[5] * xa2;
+      a2 += b[6] * xa0 + b[7] * xa1 + b[8] * xa2;
     }
     if (hb) {
-      const double* b = S + (size_t)qb * 9;
-      const int s1 = tb ? 3 : 1, s3 = tb ? 1 : 3;
-      a0 += b[0] * xb0 + b[s1] * xb1 + b[2 * s1] * xb2;
-      a1 += b[s3] * xb0 + b[s3 + s1] * xb1 + b[s3 + 2 * s1] * xb2;
-      a2 += b[2 * s3] * xb0 + b[2 * s3 + s1] * xb1 + b[2 * s3 + 2 * s1] * xb2;
+      const double* b = S + (size_t)pb * 9;
+      a0 += b[0] * xb0 + b[1] * xb1 + b[2] * xb2;
+      a1 += b[3] * xb0 + b[4] * xb1 + b[5] * xb2;
+      a2 += b[6] * xb0 + b[7] * xb1 + b[8] * xb2;
     }
   }
 }
-__device__ __forceinline__ void block_row_walk_f64(const int*, const float*, const int*, int, const double*, int, int,
-                                                   int, double&, double&, double&) {}
+__device__ __forceinline__ void block_row_walk_f64(const int*, const float*, const double*, int, int, int, double&,
+                                                   double&, double&) {}
 
 // One lane's walk over blocks p, p + stride, ... < p1 of a block row:
 // a += S_p x_col(p), blocks added in increasing p.  FP32 values: per step
@@ -421,19 +413,11 @@ __device__ __forceinline__ void block_row_walk_f64(const int*, const float*, con
 // the first block's values and is not added.  FP64 values (18 more
 // registers than the 1024-thread kernel has to spare): the x gathers of the
 // two blocks are issued together, then each block's values.
-//
-// mirror (or null): the symmetric read of a matrix streamed from HBM.  A
-// lower block (column < row) is read as the transpose of its upper mirror,
-// which another row of the same sweep loads from HBM at about the same time,
-// so the lower half comes from L2 and HBM carries the upper half of S (plus
-// four bytes of mirror index per lower block).  The values are the bits the
-// block gather stores at the lower position, so the sums are unchanged.
 template <typename MT>
-__device__ __forceinline__ void block_row_walk(const int* col, const MT* S, const int* mirror, int row,
-                                               const double* x, int p, int p1, int stride, double& a0, double& a1,
-                                               double& a2) {
+__device__ __forceinline__ void block_row_walk(const int* col, const MT* S, const double* x, int p, int p1,
+                                               int stride, double& a0, double& a1, double& a2) {
   if constexpr (sizeof(MT) == 8) {
-    block_row_walk_f64(col, S, mirror, row, x, p, p1, stride, a0, a1, a2);
+    block_row_walk_f64(col, S, x, p, p1, stride, a0, a1, a2);
     return;
   }
   for (; p < p1; p += 2 * stride) {
@@ -442,15 +426,7 @@ __device__ __forceinline__ void block_row_walk(const int* col, const MT* S, cons
     const int ca = col[p];
     const int cb = hb ? col[pb] : ca;
     MT ba[9], bb[9];
-    if (mirror) {
-      const bool ta = ca < row, tb = hb && cb < row;
-      const MT* A = S + (size_t)(ta ? mirror[p] : p) * 9;
-      const MT* B = S + (size_t)(hb ? (tb ? mirror[pb] : pb) : p) * 9;
-#pragma unroll
-      for (int k = 0; k < 9; k++) ba[k] = A[ta ? 3 * (k % 3) + k / 3 : k];
-#pragma unroll
-      for (int k = 0; k < 9; k++) bb[k] = B[tb ? 3 * (k % 3) + k / 3 : k];
-    } else {
+    {
       const MT* A = S + (size_t)p * 9;
       const MT* B = S + (size_t)(hb ? pb : p) * 9;
 #pragma unroll
@@ -506,7 +482,7 @@ __device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int i, int 
     S = mv.S;
   }
   double a0 = 0, a1 = 0, a2 = 0;
-  block_row_walk<MT>(col, S, mv.cached ? nullptr : mv.mirror, row, x, p0 + lane, p1, 32, a0, a1, a2);
+  block_row_walk<MT>(col, S, x, p0 + lane, p1, 32, a0, a1, a2);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -545,7 +521,7 @@ __device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int 
   }
   const int gl = lane & (L - 1);
   double a0 = 0, a1 = 0, a2 = 0;
-  block_row_walk<MT>(col, S, mv.cached ? nullptr : mv.mirror, row, x, p0 + gl, p1, L, a0, a1, a2);
+  block_row_walk<MT>(col, S, x, p0 + gl, p1, L, a0, a1, a2);
 #pragma unroll
   for (int off = L / 2; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -710,9 +686,7 @@ __host__ __device__ inline void pcg_smem_layout(int nloc_max, int nb_max, int re
 // RES: compiled for shared-memory resident row state (the contiguous split
 // of packs that fit); otherwise residency is the runtime flag (zero in the
 // strided split), which keeps the register pressure of each form low.
-// SYM: the instance with the symmetric read of lower blocks (non-resident
-// only); the others compile the in-place read alone.
-template <typename MT, bool RES, bool SYM = false>
+template <typename MT, bool RES>
 __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   __shared__ double rowbuf[kRowChunk][3];
   __shared__ double sn[kRowChunk][3];
@@ -795,7 +769,6 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   mv.rowptr = a.rowptr;
   mv.col = a.col;
   mv.S = (const MT*)a.S;
-  mv.mirror = SYM ? a.mirror : nullptr;
   mv.cached = a.cached;
   mv.ro_s = (const int*)(dyn + off_ro);
   mv.col_s = (const int*)(dyn + off_col);
@@ -1423,7 +1396,6 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   a.max_iter = max_iter;
   a.variant = eng.pcg_variant;
   a.row_lanes = eng.pcg_row_lanes;
-  a.mirror = eng.sym_spmv ? d.blk_mirror : nullptr;
   a.update_state = update_state ? 1 : 0;
   a.xpos = d.x;
   a.vel = d.v;
@@ -1463,11 +1435,9 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   if (eng.precision == B200FEM_PREC_MIXED) {
     a.S = d.S_f;
     return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<float, true>, a)
-           : a.mirror ? cudaLaunchKernelEx(&cfg, pcg_kernel<float, false, true>, a)
                       : cudaLaunchKernelEx(&cfg, pcg_kernel<float, false>, a);
   }
   return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true>, a)
-         : a.mirror ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, false, true>, a)
                     : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false>, a);
 }
 
@@ -1496,9 +1466,6 @@ static cudaError_t ensure_pcg_smem(int device, size_t bytes, bool fp32 = false) 
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, false>, at, (int)bytes)
                        : cudaFuncSetAttribute(pcg_kernel<double, false>, at, (int)bytes);
-  if (e == cudaSuccess)
-    e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, false, true>, at, (int)bytes)
-             : cudaFuncSetAttribute(pcg_kernel<double, false, true>, at, (int)bytes);
   if (e == cudaSuccess)
     e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, true>, at, (int)bytes)
              : cudaFuncSetAttribute(pcg_kernel<double, true>, at, (int)bytes);
@@ -1761,7 +1728,6 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.max_iter = max_iter;
   a.variant = 0;
   a.row_lanes = 16;
-  a.mirror = nullptr;
   a.update_state = 0;
   a.vprev = nullptr;
   a.vprev2 = nullptr;

@@ -364,13 +364,6 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                        for the SpMV's loads); 0 (auto) as 2 while the solve
                                        matrix is at most 64 MB (it stays in L2), else as 1.  Set
                                        before b200fem_build; after it, 2 or 1 as in force */
-#define B200FEM_OPT_SYM_SPMV 13 /* the PCG's block SpMV: 2 reads each lower block (column < row)
-                                   as the transpose of its upper mirror, so HBM carries the
-                                   upper half of the solve matrix and the lower half comes from
-                                   L2 (the mirror is loaded by another row of the same sweep); 1
-                                   reads every block in place; 0 (auto) as 2 for a matrix above
-                                   64 MB on the contiguous split, else as 1.  Same sums either
-                                   way.  Set before b200fem_build; after it, 2 or 1 as in force */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
