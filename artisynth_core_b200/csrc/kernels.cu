@@ -371,8 +371,20 @@ struct ElemSmem {
   }
 };
 
+// two CTAs per SM (128 registers) except for FP64 quadratic hexes and
+// wedges (20 and 15 nodes), whose point records and pair sums spilled 100 to
+// 1,000 bytes at 128: one CTA per SM and up to 255 registers (update of a
+// 24x6x6 beam, B200: quadratic hex MooneyRivlin with four pressure values
+// 138 -> 108 us, NeoHookean 61 -> 57 us, quadratic wedge 92 -> 89 us).  The
+// 10- and 13-node elements keep two CTAs: quadratic tets measured the same
+// either way, quadratic pyramids 53 us at two CTAs against 58 at one.
+template <int TYPE, int MAT, int INC, typename T>
+constexpr int elem_min_ctas() {
+  return (elem_nen(TYPE) >= 15 && sizeof(T) == 8) ? 1 : 2;
+}
+
 template <int TYPE, int MAT, int INC, typename T, int EPB>
-__global__ void __launch_bounds__(256, 2) elem_nonlinear_kernel(ElemArgs a) {
+__global__ void __launch_bounds__(256, (elem_min_ctas<TYPE, MAT, INC, T>())) elem_nonlinear_kernel(ElemArgs a) {
   using SM = ElemSmem<TYPE, MAT, T, EPB>;
   constexpr int NEN = SM::NEN;
   constexpr int NIP = SM::NIP;
