@@ -961,21 +961,6 @@ b200fem_handle b200fem_create(const b200fem_config* cfg) {
     return nullptr;
   }
   for (auto& ev : h->eng.ev) cudaEventCreate(&ev);
-  {
-    // the assembly's side stream (optional: without it the RHS kernel runs
-    // after the gather on the main stream)
-    Engine& g = h->eng;
-    if (cudaStreamCreateWithFlags(&g.aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming) != cudaSuccess) {
-      cudaGetLastError();
-      if (g.aux_stream) cudaStreamDestroy(g.aux_stream);
-      if (g.ev_fork) cudaEventDestroy(g.ev_fork);
-      if (g.ev_join) cudaEventDestroy(g.ev_join);
-      g.aux_stream = nullptr;
-      g.ev_fork = g.ev_join = nullptr;
-    }
-  }
   h->eng.models.assign(1, ModelDesc());
   return h;
 }
@@ -984,11 +969,7 @@ int b200fem_destroy(b200fem_handle h) {
   if (!h) return B200FEM_OK;
   cudaSetDevice(h->eng.device);
   if (h->eng.stream) cudaStreamSynchronize(h->eng.stream);
-  if (h->eng.aux_stream) cudaStreamSynchronize(h->eng.aux_stream);
   free_pack(h->eng);
-  if (h->eng.aux_stream) cudaStreamDestroy(h->eng.aux_stream);
-  if (h->eng.ev_fork) cudaEventDestroy(h->eng.ev_fork);
-  if (h->eng.ev_join) cudaEventDestroy(h->eng.ev_join);
   for (auto& ev : h->eng.ev)
     if (ev) cudaEventDestroy(ev);
 

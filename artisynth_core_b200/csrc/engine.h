@@ -295,11 +295,6 @@ struct Engine {
   int precision = B200FEM_PREC_FP64;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
-  // side stream of the step's assembly: the RHS kernel beside the block
-  // gather (fork and join events); null when it could not be created
-  cudaStream_t aux_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  bool rows_forked = false;  // launch_assemble ran the RHS kernel: launch_rhs has nothing left
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> ev_pool;  // 3 per step of a multi-step call
   std::string last_error;

@@ -2346,9 +2346,6 @@ static cudaError_t launch_assemble_fused(Engine& eng) {
   return launch_fused_blocks(eng, eng.fused_chunks);
 }
 
-static cudaError_t launch_rows(Engine& eng, double* b, double* sol, cudaStream_t st);
-static cudaError_t launch_gather(Engine& eng, bool want_K);
-
 cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   (void)cK;
   (void)cM;
@@ -2369,26 +2366,6 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
     });
     if (e != cudaSuccess) return e;
   }
-  // the step: the nodal forces, b and the PCG's initial guess (rows_kernel)
-  // run on the side stream beside the block gather -- they read the element
-  // forces, the gather the element blocks -- and join before the solve
-  // (launch_rhs then has nothing left)
-  if (!want_K && eng.aux_stream) {
-    if ((e = cudaEventRecord(eng.ev_fork, eng.stream)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(eng.aux_stream, eng.ev_fork, 0)) != cudaSuccess) return e;
-    if ((e = launch_rows(eng, d.b, d.sol, eng.aux_stream)) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(eng.ev_join, eng.aux_stream)) != cudaSuccess) return e;
-    if ((e = launch_gather(eng, want_K)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(eng.stream, eng.ev_join, 0)) != cudaSuccess) return e;
-    eng.rows_forked = true;
-    return cudaSuccess;
-  }
-  return launch_gather(eng, want_K);
-}
-
-static cudaError_t launch_gather(Engine& eng, bool want_K) {
-  DevPack& d = eng.d;
-  const bool fp32 = eng.precision == B200FEM_PREC_MIXED;
   const int* act = eng.any_inactive ? d.model_active : nullptr;
   if (d.n_up == 0) return cudaSuccess;
   // Matrices that stay in L2 (up to 64 MB of blocks): one thread per block
@@ -2463,7 +2440,7 @@ cudaError_t launch_reset_status(Engine& eng) {
   return cudaGetLastError();
 }
 
-static cudaError_t launch_rows(Engine& eng, double* b, double* sol, cudaStream_t st) {
+static cudaError_t launch_rows(Engine& eng, double* b, double* sol) {
   DevPack& d = eng.d;
   const int threads = 64;
   const int blocks = (d.n_nodes + threads - 1) / threads;
@@ -2475,7 +2452,7 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol, cudaStream_t
   const double* nrm =
       (sol && eng.integrator == B200FEM_INTEGRATOR_CONSTRAINED_BACKWARD_EULER && d.row_nrm) ? d.row_nrm : nullptr;
   // nodal forces are FP64 in both forms
-  rows_kernel<double><<<blocks, threads, 0, st>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
+  rows_kernel<double><<<blocks, threads, 0, eng.stream>>>(d.n_nodes, d.inc_ptr, d.inc_idx, d.elemF, d.sidx,
                                                          d.node_model, d.mass, d.v, d.fext, d.step, d.fint, b, sol, act, vp,
                                                          vp2, vp3, vp4, nrm);
   return cudaGetLastError();
@@ -2483,16 +2460,9 @@ static cudaError_t launch_rows(Engine& eng, double* b, double* sol, cudaStream_t
 
 // follows launch_assemble(..., want_K = false) in the step; the node-row
 // path has formed b and the initial guess already
-cudaError_t launch_rhs(Engine& eng) {
-  if (eng.tet_rows) return cudaSuccess;
-  if (eng.rows_forked) {  // ran beside the gather in launch_assemble
-    eng.rows_forked = false;
-    return cudaSuccess;
-  }
-  return launch_rows(eng, eng.d.b, eng.d.sol, eng.stream);
-}
+cudaError_t launch_rhs(Engine& eng) { return eng.tet_rows ? cudaSuccess : launch_rows(eng, eng.d.b, eng.d.sol); }
 
-cudaError_t launch_forces_only(Engine& eng) { return launch_rows(eng, nullptr, nullptr, eng.stream); }
+cudaError_t launch_forces_only(Engine& eng) { return launch_rows(eng, nullptr, nullptr); }
 
 cudaError_t launch_spmv(Engine& eng, const double* x, double* y) {
   DevPack& d = eng.d;
