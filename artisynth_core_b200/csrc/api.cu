@@ -116,9 +116,6 @@ int build_pack(Engine& eng) {
   const bool mixed = eng.elem_type == kElemMixed;
   const int nen = mixed ? 0 : elem_nen(eng.elem_type), nip = mixed ? 0 : elem_nip(eng.elem_type);
   const int npair = nen * (nen + 1) / 2;
-  eng.nen = nen;
-  eng.nip = nip;
-  eng.npair = npair;
   // offsets
   eng.node_off.assign(M + 1, 0);
   eng.elem_off.assign(M + 1, 0);

@@ -307,7 +307,6 @@ struct Engine {
   bool built = false;
   bool have_matrix = false;
   int elem_type = B200FEM_ELEM_TET;  // pack-wide element type (kElemMixed: several)
-  int nen = 4, nip = 1, npair = 10;  // of a single-type pack
   int nen_max = 4;                   // largest element of the pack
   bool divblk_smem = false;          // NODAL divBlk sums in shared memory (every node <= 32 neighbours)
   // host copies for queries
