@@ -853,8 +853,9 @@ def run_b200(args):
                            tol=wl.tol, nnzb=sz["nnzb"], active_dof=3 * sz["n_active"]),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes},
-            # per timed step: status reset, element kernel, block gather, RHS rows, PCG
-            "gpu_launches": 5 * args.steps,
+            # per timed step: status reset, element kernel, block gather, RHS rows,
+            # PCG, and the status record the call reads back
+            "gpu_launches": 6 * args.steps,
             "phases_ms_per_step": {"assembly": asm_ms / args.steps, "pcg": pcg_ms / args.steps,
                                    "pcg_iterations": mean_it},
             "update_stress_stiffness_ms": {"value": uss_ms, "what": "b200fem_update_stress_stiffness device time "
