@@ -140,3 +140,30 @@ def test_pack_of_different_types(b200, oracle):
             st, _, _ = om.be_step(wl.h, x, v, alpha=wl.mass_damping, gravity=wl.gravity, solver=1, tol=1e-14)
             assert st == 0
         assert rel_err(xg, x) <= 1e-8, rel_err(xg, x)
+
+
+def test_mixed_mesh_rejects_bad_input(b200, oracle):
+    """An unknown element type or a connectivity index out of range is refused
+    (ERR_INVALID_ARG at b200fem_set_mesh_mixed or at the build)."""
+    import ctypes
+    xyz, types, conn, fixed = _mesh(oracle, HEX_WEDGE_PYR)
+    lib = L.lib()
+    h = lib.b200fem_create(ctypes.byref(L.Config(0, L.PREC_FP64)))
+    assert h
+    try:
+        rest = np.ascontiguousarray(xyz.reshape(-1))
+        bad = types.copy()
+        bad[3] = 42
+        assert lib.b200fem_set_mesh_mixed(h, xyz.shape[0], L.dptr(rest), types.size, L.iptr(bad), L.iptr(conn),
+                                          L.iptr(fixed)) == L.ERR_INVALID_ARG
+        c2 = conn.copy()
+        c2[7] = xyz.shape[0] + 5
+        assert lib.b200fem_set_mesh_mixed(h, xyz.shape[0], L.dptr(rest), types.size, L.iptr(types), L.iptr(c2),
+                                          L.iptr(fixed)) == L.OK
+        prm = np.zeros(8)
+        prm[:2] = (5e4, 0.45)
+        assert lib.b200fem_set_material(h, L.MAT_NEOHOOKEAN, L.dptr(prm), 1000.0, L.INCOMP_AUTO) == L.OK
+        assert lib.b200fem_build(h) == L.ERR_INVALID_ARG
+        assert b"out of range" in lib.b200fem_last_error(h)
+    finally:
+        lib.b200fem_destroy(h)
