@@ -30,6 +30,7 @@ ELEM_TET, ELEM_HEX, ELEM_WEDGE, ELEM_PYRAMID, ELEM_QUADTET, ELEM_QUADHEX, ELEM_Q
 ELEM_NODES = {ELEM_TET: 4, ELEM_HEX: 8, ELEM_WEDGE: 6, ELEM_PYRAMID: 5, ELEM_QUADTET: 10, ELEM_QUADHEX: 20,
               ELEM_QUADWEDGE: 15, ELEM_QUADPYRAMID: 13}
 MAT_LINEAR, MAT_NEOHOOKEAN, MAT_MOONEYRIVLIN, MAT_STVK = 0, 1, 2, 3
+MAT_MODEL = -1  # b200fem_set_element_materials: the element keeps the model's material
 INCOMP_OFF, INCOMP_NODAL, INCOMP_AUTO, INCOMP_ELEMENT = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 PART_FULL, PART_UPPER = 0, 1
@@ -126,6 +127,8 @@ def lib():
         "b200fem_set_mesh": ([H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip], ctypes.c_int),
         "b200fem_set_mesh_mixed": ([H, ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip], ctypes.c_int),
         "b200fem_set_material": ([H, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+        "b200fem_set_element_materials": ([H, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+                                          ctypes.c_int),
         "b200fem_build": ([H], ctypes.c_int),
         "b200fem_get_sizes": ([H, _ip, _ip, _ip, _ip], ctypes.c_int),
         "b200fem_get_solve_index": ([H, _ip], ctypes.c_int),

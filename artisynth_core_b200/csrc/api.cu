@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -163,12 +164,17 @@ int build_pack(Engine& eng) {
   d.nnzb = NB;
 
   // ---- host arrays
-  std::vector<double> x(3 * (size_t)N), mass(N), mat((size_t)M * kMatParams, 0.0), step((size_t)M * 8, 0.0);
+  // material table: one row per model, then the models' element materials
+  std::vector<int> mat_row(M + 1, M);
+  for (int m = 0; m < M; m++) mat_row[m + 1] = mat_row[m] + (int)eng.models[m].emat_kind.size();
+  const bool own_mats = mat_row[M] > M;
+  std::vector<double> x(3 * (size_t)N), mass(N), mat((size_t)mat_row[M] * kMatParams, 0.0),
+      step((size_t)M * 8, 0.0);
   std::vector<int> node_model(N), sidx(N), act_node(R), row_model(R);
-  std::vector<int> conn((size_t)coff[E]), elem_model(E);
+  std::vector<int> conn((size_t)coff[E]), elem_model(E), elem_mat(own_mats ? E : 0);
   std::vector<double> invJ0((size_t)ipoff[E] * 9), winvJ0((size_t)E * 9);
-  bool any_linear = false, any_nodal = false;
-  for (auto& m : eng.models) any_linear |= (m.mat_kind == B200FEM_MAT_LINEAR);
+  bool any_linear = false, any_nodal = false, permuted = false;
+  for (auto& h : eng.hosts) any_linear |= !h.K0.empty();
   for (auto& h : eng.hosts) any_nodal |= (h.incomp == B200FEM_INCOMP_NODAL);
   std::vector<double> K0, f0, node_rest_vol;
   if (any_linear) {
@@ -199,7 +205,11 @@ int build_pack(Engine& eng) {
       }
     }
     for (size_t q = 0; q < h.sconn.size(); q++) conn[(size_t)coff[eo] + q] = no + h.sconn[q];
-    for (int e = 0; e < md.n_elems; e++) elem_model[eo + e] = m;
+    for (int e = 0; e < md.n_elems; e++) {
+      elem_model[eo + e] = m;
+      if (own_mats) elem_mat[eo + e] = h.smat[e] == 0 ? m : mat_row[m] + h.smat[e] - 1;
+      permuted |= h.perm[e] != e;
+    }
     std::copy(h.invJ0.begin(), h.invJ0.end(), invJ0.begin() + (size_t)ipoff[eo] * 9);
     std::copy(h.winvJ0.begin(), h.winvJ0.end(), winvJ0.begin() + (size_t)eo * 9);
     if (!h.K0.empty()) {
@@ -209,6 +219,7 @@ int build_pack(Engine& eng) {
     if (!h.node_rest_vol.empty())
       std::copy(h.node_rest_vol.begin(), h.node_rest_vol.end(), node_rest_vol.begin() + no);
     std::copy(md.mat_params, md.mat_params + kMatParams, mat.begin() + (size_t)m * kMatParams);
+    std::copy(md.emat_params.begin(), md.emat_params.end(), mat.begin() + (size_t)mat_row[m] * kMatParams);
     step[(size_t)m * 8 + 0] = 0.01;
     step[(size_t)m * 8 + 1] = 2.0;
     step[(size_t)m * 8 + 6] = 1e-10;
@@ -257,7 +268,7 @@ int build_pack(Engine& eng) {
     }
   }
   // the scatter map in the callers' element order (b200fem_get_scatter_map)
-  if (!mixed) {
+  if (!permuted) {
     eng.h_scatter.swap(scat);
   } else {
     eng.h_scatter.clear();
@@ -287,8 +298,9 @@ int build_pack(Engine& eng) {
       }
     }
   }
-  // ---- element groups: runs of one element type, material kind and soft
-  // incompressibility (a model of several types gives one run per type)
+  // ---- element groups: runs of one element type, material kind, corotation
+  // and soft incompressibility (a model of several types or element materials
+  // gives one run per section)
   eng.groups.clear();
   for (int m = 0; m < M; m++) {
     const ModelHost& h = eng.hosts[m];
@@ -298,10 +310,12 @@ int build_pack(Engine& eng) {
       g.e1 = eng.elem_off[m] + h.sec[k + 1];
       if (g.e1 <= g.e0) continue;
       g.elem_type = etype[g.e0];
-      g.mat_kind = eng.models[m].mat_kind;
-      g.corotated = (g.mat_kind == B200FEM_MAT_LINEAR) ? (eng.models[m].mat_params[2] != 0) : 0;
-      g.nodal = h.incomp == B200FEM_INCOMP_NODAL;
-      g.elem_inc = h.incomp == B200FEM_INCOMP_ELEMENT;
+      g.mat_kind = h.skind[h.sec[k]];
+      g.corotated = h.scorot[h.sec[k]];
+      // elements of compressible materials run with OFF (FemModel3d.java:3346-3348)
+      const bool inc = g.mat_kind == B200FEM_MAT_MOONEYRIVLIN;
+      g.nodal = inc && h.incomp == B200FEM_INCOMP_NODAL;
+      g.elem_inc = inc && h.incomp == B200FEM_INCOMP_ELEMENT;
       if (!eng.groups.empty()) {
         ElemGroup& last = eng.groups.back();
         if (last.elem_type == g.elem_type && last.mat_kind == g.mat_kind && last.corotated == g.corotated &&
@@ -331,7 +345,11 @@ int build_pack(Engine& eng) {
   std::vector<unsigned char> cbyte;
   if (eng.opt_tet_assembly == 0 && eng.elem_type == B200FEM_ELEM_TET && eng.opt_fused == 0 && R > 0) {
     bool ok = true;
-    for (const ElemGroup& g : eng.groups) ok &= g.mat_kind != B200FEM_MAT_LINEAR;
+    // (its tasks are runs of one model's rows: every group must cover whole models)
+    for (const ElemGroup& g : eng.groups)
+      ok &= g.mat_kind != B200FEM_MAT_LINEAR &&
+            std::binary_search(eng.elem_off.begin(), eng.elem_off.end(), g.e0) &&
+            std::binary_search(eng.elem_off.begin(), eng.elem_off.end(), g.e1);
     std::vector<int> first_active(E, -1);
     for (int e = 0; ok && e < E; e++) {
       for (int a = 0; a < nen && first_active[e] < 0; a++)
@@ -716,6 +734,8 @@ int build_pack(Engine& eng) {
   CK(upload(eng, &d.row_model, row_model));
   CK(upload(eng, &d.conn, conn));
   CK(upload(eng, &d.elem_model, elem_model));
+  if (own_mats) CK(upload(eng, &d.elem_mat, elem_mat));
+  else d.elem_mat = d.elem_model;
   CK(upload(eng, &d.invJ0, invJ0));
   CK(upload(eng, &d.winvJ0, winvJ0));
   if (any_linear) {
@@ -1040,6 +1060,9 @@ int b200fem_set_mesh(b200fem_handle h, int elem_type, int n_nodes, const double*
   m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
   m.conn.assign(conn, conn + (size_t)nen * n_elems);
   m.etypes.clear();
+  m.emat.clear();  // element materials name elements of the previous mesh
+  m.emat_kind.clear();
+  m.emat_params.clear();
   m.fixed.assign(n_nodes, 0);
   if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
   eng.att = FrameAttach();  // attachments name nodes of the previous mesh
@@ -1067,9 +1090,63 @@ int b200fem_set_mesh_mixed(b200fem_handle h, int n_nodes, const double* rest_xyz
   m.rest.assign(rest_xyz, rest_xyz + 3 * (size_t)n_nodes);
   m.conn.assign(conn, conn + total);
   m.etypes.assign(elem_types, elem_types + n_elems);
+  m.emat.clear();
+  m.emat_kind.clear();
+  m.emat_params.clear();
   m.fixed.assign(n_nodes, 0);
   if (fixed) std::copy(fixed, fixed + n_nodes, m.fixed.begin());
   eng.att = FrameAttach();
+  free_pack(eng);
+  return B200FEM_OK;
+}
+
+int b200fem_set_element_materials(b200fem_handle h, int model, int n_elems, const int* mat_kinds,
+                                  const double* params) {
+  ENG(h);
+  if (model < 0 || model >= (int)eng.models.size()) return fail(&eng, B200FEM_ERR_INVALID_ARG, "no such model");
+  ModelDesc& m = eng.models[model];
+  if (!mat_kinds) {
+    m.emat.clear();
+    m.emat_kind.clear();
+    m.emat_params.clear();
+    free_pack(eng);
+    return B200FEM_OK;
+  }
+  if (n_elems != m.n_elems || n_elems <= 0) return fail(&eng, B200FEM_ERR_INVALID_ARG, "element count mismatch");
+  // distinct materials, each once (equal kind and parameter values)
+  std::vector<int> emat(n_elems, -1), kinds;
+  std::vector<double> prm;
+  std::map<std::pair<int, std::vector<double>>, int> seen;
+  bool any = false;
+  for (int e = 0; e < n_elems; e++) {
+    const int k = mat_kinds[e];
+    if (k == B200FEM_MAT_MODEL) continue;
+    if (k < B200FEM_MAT_LINEAR || k > B200FEM_MAT_STVK || !params)
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "element " + std::to_string(e) + ": unknown material");
+    const int np = k == B200FEM_MAT_LINEAR ? 3 : k == B200FEM_MAT_MOONEYRIVLIN ? 8 : 2;
+    const double* p = params + (size_t)e * kMatParams;
+    if (!all_finite(p, np))
+      return fail(&eng, B200FEM_ERR_INVALID_ARG, "element " + std::to_string(e) + ": non-finite material parameter");
+    std::vector<double> key(p, p + np);
+    key.resize(kMatParams, 0.0);
+    auto it = seen.find({k, key});
+    if (it == seen.end()) {
+      it = seen.emplace(std::make_pair(k, key), (int)kinds.size()).first;
+      kinds.push_back(k);
+      prm.insert(prm.end(), key.begin(), key.end());
+    }
+    emat[e] = it->second;
+    any = true;
+  }
+  if (any) {
+    m.emat.swap(emat);
+    m.emat_kind.swap(kinds);
+    m.emat_params.swap(prm);
+  } else {
+    m.emat.clear();
+    m.emat_kind.clear();
+    m.emat_params.clear();
+  }
   free_pack(eng);
   return B200FEM_OK;
 }

@@ -64,17 +64,23 @@ struct ModelDesc {
   double density = 1000;
   int incomp_request = B200FEM_INCOMP_AUTO;
   bool has_material = false;
+  // per-element materials (FemElement.setMaterial; FemModel3d.getElementMaterial,
+  // FemModel3d.java:608-614): per caller element -1 (the model's material) or
+  // an index into the distinct element materials emat_kind / emat_params
+  std::vector<int> emat;
+  std::vector<int> emat_kind;
+  std::vector<double> emat_params;  // kMatParams each
 };
 
 // Host-side derived data of one model (setup only).
 //
 // Element data are held in storage order: the caller's elements sorted by
-// type (stable), so that each type forms one contiguous section that the
-// type-specialised kernels run over.  A mesh of one type keeps the caller's
-// order.  Per storage element s, coff/ipoff/sqoff give the offsets of its
-// nodes (and force slots), integration points and nen x nen entries.
+// type, then material kind and corotation (stable), so that each such class
+// forms one contiguous section that the specialised kernels run over.  A
+// mesh of one type and one material keeps the caller's order.  Per storage
+// element s, coff/ipoff/sqoff give the offsets of its nodes (and force
+// slots), integration points and nen x nen entries.
 struct ModelHost {
-  int nen = 4, nip = 1, npair = 10;  // of a single-type mesh (0 when mixed)
   int incomp = B200FEM_INCOMP_OFF;  // resolved method
   int n_active = 0;
   std::vector<int> sidx;      // per node, -1 when fixed
@@ -82,7 +88,11 @@ struct ModelHost {
   std::vector<int> stype;     // per storage element: its type
   std::vector<int> perm;      // storage element -> caller's element
   std::vector<int> iperm;     // caller's element -> storage element
-  std::vector<int> sec;       // section bounds in storage order (type runs), sec.size() = runs + 1
+  std::vector<int> smat;      // per storage element: 0 the model's material, k + 1 element material k
+  std::vector<int> skind;     // per storage element: its material kind
+  std::vector<char> scorot;   // per storage element: corotated linear material
+  std::vector<int> sec;       // section bounds in storage order (runs of one type, kind and
+                              // corotation), sec.size() = runs + 1
   std::vector<long long> coff, ipoff, sqoff;  // E+1 each
   std::vector<int> sconn;     // nodes in storage order (coff)
   std::vector<double> invJ0;  // ipoff[E]*9
@@ -116,6 +126,8 @@ struct DevPack {
   // elements
   int* conn = nullptr;       // node slots (nen per element, storage order): global node indices
   int* elem_model = nullptr; // E
+  int* elem_mat = nullptr;   // E: row of mat (the model's row unless the element has its own
+                             // material); aliases elem_model when no element has one
   double* invJ0 = nullptr;   // 9 per integration point
   double* winvJ0 = nullptr;  // E*9
   double* K0 = nullptr;      // linear: nen*nen*9 per element
@@ -153,7 +165,7 @@ struct DevPack {
   double* m0 = nullptr;
   double* m1 = nullptr;
   // per model tables
-  double* mat = nullptr;       // n_models*kMatParams
+  double* mat = nullptr;       // kMatParams per row: the models' materials, then element materials
   double* step = nullptr;      // n_models*8: h, alpha, beta, gx, gy, gz, tol, -
   // NODAL incompressibility (FemModel3d.java:2471-2669)
   double* node_rest_vol = nullptr;

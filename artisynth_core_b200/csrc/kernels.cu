@@ -322,6 +322,7 @@ struct ElemArgs {
   int e0, e1;
   const int* conn;
   const int* elem_model;
+  const int* elem_mat;     // per element: its row of mat
   const double* x;
   const double* invJ0;
   const float* invJ0_f;
@@ -329,7 +330,7 @@ struct ElemArgs {
   const double* K0;
   const double* f0;
   const int* sidx;
-  const double* mat;       // per model kMatParams
+  const double* mat;       // kMatParams per row
   const double* node_p;    // NODAL pressures (or null)
   const double* elem_p;    // ELEMENT pressures (or null)
   const double* elem_r;    // ELEMENT Rinv = effective modulus / rest volume (or null)
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(256, (elem_min_ctas<TYPE, MAT, INC, T>())) ele
 #pragma unroll
       for (int c = 0; c < 3; c++) sg[t][n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
     }
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
       T aa, bb;
       neohookean_point<T>(ssig[t], &aa, &bb, (T)mp[0], (T)mp[1], F, detF);
@@ -1044,6 +1045,7 @@ static ElemArgs elem_args(Engine& eng, const ElemGroup& g, bool fp32) {
   a.e1 = g.e1 - g.e0;
   a.conn = at(d.conn, g.c0);
   a.elem_model = at(d.elem_model, g.e0);
+  a.elem_mat = at(d.elem_mat, g.e0);
   a.active = eng.any_inactive ? d.model_active : nullptr;
   a.x = d.x;
   a.invJ0 = at(d.invJ0, 9 * g.ip0);
@@ -1131,7 +1133,7 @@ __global__ void __launch_bounds__(128) elem_force_kernel(ElemArgs a) {
     const double dv = detJ * ip_weight<double, TYPE>(k);
     myinv = !(detJ > 0.0);
     mydet = detJ;
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     double sig[6];
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
       double aa, bb;
@@ -1241,7 +1243,7 @@ __global__ void __launch_bounds__(64) elem_tet_kernel(ElemArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; c++) g[n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
     }
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     double sig[6];
     T Dt[MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36];
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
@@ -1358,6 +1360,7 @@ struct FusedArgs {
   const double* step;
   const int* conn;
   const int* elem_model;
+  const int* elem_mat;
   const int* active;
   const double* x;
   const double* invJ0;
@@ -1432,7 +1435,7 @@ __global__ void __launch_bounds__(256) fused_block_kernel(FusedArgs a) {
 #pragma unroll
       for (int cc = 0; cc < 3; cc++) sg[t][n][cc] = invJ[cc] * g0 + invJ[3 + cc] * g1 + invJ[6 + cc] * g2;
     }
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
       T aa, bb;
       neohookean_point<T>(ssig[t], &aa, &bb, (T)mp[0], (T)mp[1], F, detF);
@@ -1901,7 +1904,7 @@ cudaError_t launch_divblk(Engine& eng) {
 // (IncompressibleMaterialBase.java:116-152), per element of the group.
 template <int TYPE>
 __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ conn,
-                                        const int* __restrict__ elem_model, const double* __restrict__ x,
+                                        const int* __restrict__ elem_mat, const double* __restrict__ x,
                                         const double* __restrict__ rest_vol, const double* __restrict__ mat,
                                         const double* __restrict__ detJ0, double* __restrict__ elem_p,
                                         double* __restrict__ elem_r) {
@@ -1917,7 +1920,7 @@ __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ 
     // pbuf = sum_k H p(K, J_k) dV, p = W pbuf / V0; Rinv = W K / V0 for the
     // quadratic potential, else Wt R Wt with Wt = W / V0 and
     // R = sum_k H H^T modulus(K, J_k) dV
-    const double* mp = mat + (size_t)elem_model[e] * kMatParams;
+    const double* mp = mat + (size_t)elem_mat[e] * kMatParams;
     const double K = mp[5], V0 = rest_vol[e];
     const bool quad = mp[7] == 0;
     double pbuf[NPV], R[NPV * NPV];
@@ -2005,7 +2008,7 @@ __global__ void element_pressure_kernel(int e0, int e1, const int* __restrict__ 
     }
     V += TYPE == B200FEM_ELEM_TET ? det3(J) / 6 : det3(J) * ip_weight<double, TYPE>(q);
   }
-  const double* mp = mat + (size_t)elem_model[e] * kMatParams;
+  const double* mp = mat + (size_t)elem_mat[e] * kMatParams;
   const double K = mp[5], V0 = rest_vol[e], Jp = V / V0;
   double p, keff;
   if (mp[7] == 0) {
@@ -2026,7 +2029,7 @@ cudaError_t launch_element_pressure(Engine& eng) {
     const int threads = 128, blocks = (g.e1 - g.e0 + threads - 1) / threads;
     cudaError_t e = by_elem_type(g.elem_type, [&](auto tag) {
       element_pressure_kernel<decltype(tag)::value><<<blocks, threads, 0, eng.stream>>>(
-          0, g.e1 - g.e0, at(d.conn, g.c0), at(d.elem_model, g.e0), d.x, at(d.elem_rest_vol, g.e0), d.mat,
+          0, g.e1 - g.e0, at(d.conn, g.c0), at(d.elem_mat, g.e0), d.x, at(d.elem_rest_vol, g.e0), d.mat,
           at(d.detJ0, g.ip0), at(d.elem_p, g.pv0), at(d.elem_r, g.pv20));
       return cudaGetLastError();
     });
@@ -2081,7 +2084,7 @@ __global__ void __launch_bounds__(128) elem_kv_kernel(ElemArgs a, const double* 
     const double detF = det3(F);
     const double detJ = invert3(invJ, J);
     const double dv = detJ * ip_weight<double, TYPE>(k);
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     double sig[6], D[36], ca = 0, cb = 0;
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) neohookean_point<double>(sig, &ca, &cb, mp[0], mp[1], F, detF);
     else material_point<MAT, double>(sig, D, mp, F, detF, 0.0);
@@ -2305,6 +2308,7 @@ static cudaError_t launch_fused_blocks(Engine& eng, int chunks) {
   fa.step = d.step;
   fa.conn = d.conn;
   fa.elem_model = d.elem_model;
+  fa.elem_mat = d.elem_mat;
   fa.active = eng.any_inactive ? d.model_active : nullptr;
   fa.x = d.x;
   fa.invJ0 = d.invJ0;

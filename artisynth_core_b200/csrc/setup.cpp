@@ -606,29 +606,44 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
       err = "connectivity index out of range";
       return B200FEM_ERR_INVALID_ARG;
     }
+  // each element's material: its own, else the model's
+  // (FemModel3d.getElementMaterial, FemModel3d.java:608-614)
+  const bool own = !m.emat.empty();
+  if (own && (int)m.emat.size() != E) {
+    err = "element materials do not match the element count";
+    return B200FEM_ERR_INVALID_ARG;
+  }
+  auto kind_of = [&](int o) { return own && m.emat[o] >= 0 ? m.emat_kind[m.emat[o]] : m.mat_kind; };
+  auto params_of = [&](int o) {
+    return own && m.emat[o] >= 0 ? &m.emat_params[(size_t)m.emat[o] * kMatParams] : m.mat_params;
+  };
+  auto corot_of = [&](int o) { return kind_of(o) == B200FEM_MAT_LINEAR && params_of(o)[2] != 0; };
+  auto class_of = [&](int o) { return (otype[o] * 8 + kind_of(o)) * 2 + (corot_of(o) ? 1 : 0); };
   h.perm.resize(E);
   for (int e = 0; e < E; e++) h.perm[e] = e;
-  std::stable_sort(h.perm.begin(), h.perm.end(), [&](int a, int b) { return otype[a] < otype[b]; });
+  std::stable_sort(h.perm.begin(), h.perm.end(), [&](int a, int b) { return class_of(a) < class_of(b); });
   h.iperm.assign(E, 0);
   h.stype.assign(E, 0);
+  h.smat.assign(E, 0);
+  h.skind.assign(E, 0);
+  h.scorot.assign(E, 0);
   h.sec.assign(1, 0);
   h.coff.assign(E + 1, 0);
   h.ipoff.assign(E + 1, 0);
   h.sqoff.assign(E + 1, 0);
   for (int s = 0; s < E; s++) {
-    const int t = otype[h.perm[s]], nen = elem_nen(t);
-    h.iperm[h.perm[s]] = s;
+    const int o = h.perm[s], t = otype[o], nen = elem_nen(t);
+    h.iperm[o] = s;
     h.stype[s] = t;
-    if (s > 0 && t != h.stype[s - 1]) h.sec.push_back(s);
+    h.smat[s] = own && m.emat[o] >= 0 ? m.emat[o] + 1 : 0;
+    h.skind[s] = kind_of(o);
+    h.scorot[s] = corot_of(o) ? 1 : 0;
+    if (s > 0 && class_of(o) != class_of(h.perm[s - 1])) h.sec.push_back(s);
     h.coff[s + 1] = h.coff[s] + nen;
     h.ipoff[s + 1] = h.ipoff[s] + elem_nip(t);
     h.sqoff[s + 1] = h.sqoff[s] + (long long)nen * nen;
   }
   h.sec.push_back(E);
-  const bool single = h.sec.size() == 2;
-  h.nen = single ? elem_nen(h.stype[0]) : 0;
-  h.nip = single ? elem_nip(h.stype[0]) : 0;
-  h.npair = single ? h.nen * (h.nen + 1) / 2 : 0;
   h.sconn.resize(h.coff[E]);
   for (int s = 0; s < E; s++) {
     const int o = h.perm[s];
@@ -644,21 +659,34 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
       h.act_node.push_back(n);
     }
   h.n_active = (int)h.act_node.size();
-  // soft incompressibility: OFF for compressible materials
-  // (FemModel3d.java:3346-3348).  NODAL needs every element to be a tet or
-  // to have its integration points at its nodes (softNodalIncompressAllowed,
-  // FemModel3d.java:400-405); the quadratic types are not, so NODAL and AUTO
-  // resolve to ELEMENT with QuadhexElement's four and QuadwedgeElement's two
-  // pressure values (getAllowedSoftIncompMethod, :462-481); otherwise AUTO ->
-  // NODAL if #elements > #active nodes, else ELEMENT
-  bool nodal_ok = true;
-  for (int s = 0; s < E; s++) nodal_ok &= h.stype[s] == B200FEM_ELEM_TET || elem_ip_at_nodes(h.stype[s]);
+  // soft incompressibility.  NODAL needs the model's material to be
+  // incompressible and every element to be a tet or to have its integration
+  // points at its nodes (softNodalIncompressAllowed, FemModel3d.java:400-405);
+  // otherwise NODAL and AUTO resolve to ELEMENT (QuadhexElement's four and
+  // QuadwedgeElement's two pressure values), and AUTO -> NODAL if #elements >
+  // #active nodes, else ELEMENT (getAllowedSoftIncompMethod, :462-481).  An
+  // element of a compressible material runs with OFF (:3346-3348), so a model
+  // none of whose elements is incompressible resolves to OFF.
+  bool nodal_ok = true, any_incomp = false, all_incomp = true;
+  for (int s = 0; s < E; s++) {
+    nodal_ok &= h.stype[s] == B200FEM_ELEM_TET || elem_ip_at_nodes(h.stype[s]);
+    any_incomp |= h.skind[s] == B200FEM_MAT_MOONEYRIVLIN;
+    all_incomp &= h.skind[s] == B200FEM_MAT_MOONEYRIVLIN;
+  }
   int method = m.incomp_request;
-  if (m.mat_kind != B200FEM_MAT_MOONEYRIVLIN) method = B200FEM_INCOMP_OFF;
-  else if (!nodal_ok && (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
+  if (!any_incomp) method = B200FEM_INCOMP_OFF;
+  else if ((m.mat_kind != B200FEM_MAT_MOONEYRIVLIN || !nodal_ok) &&
+           (method == B200FEM_INCOMP_NODAL || method == B200FEM_INCOMP_AUTO))
     method = B200FEM_INCOMP_ELEMENT;
   else if (method == B200FEM_INCOMP_AUTO)
     method = (E > h.n_active) ? B200FEM_INCOMP_NODAL : B200FEM_INCOMP_ELEMENT;
+  if (method == B200FEM_INCOMP_NODAL && !all_incomp) {
+    // the reference sums nodal volumes over the incompressible elements only
+    // (updateNodalPressures, :2471-2503) and divides by a zero rest volume at a
+    // node that only compressible elements touch
+    err = "NODAL soft incompressibility with elements of compressible materials";
+    return B200FEM_ERR_UNSUPPORTED;
+  }
   h.incomp = method;
 
   // rest data: IntegrationData3d.myInvJ0/myDetJ0 (IntegrationData3d.java:108-111)
@@ -703,15 +731,20 @@ int setup_model_host(const ModelDesc& m, ModelHost& h, std::string& err) {
   }
   // linear materials: rest stiffness K0 and f0 = K0 x_rest
   // (LinearMaterialCache.addInitialStiffness, LinearMaterialCache.java:115-160)
+  // (each linear element with its own E and nu)
   h.K0.clear();
   h.f0.clear();
-  if (m.mat_kind == B200FEM_MAT_LINEAR) {
+  bool any_linear = false;
+  for (int s = 0; s < E; s++) any_linear |= h.skind[s] == B200FEM_MAT_LINEAR;
+  if (any_linear) {
     double C[36];
-    linear_tangent(C, m.mat_params[0], m.mat_params[1]);
     h.K0.assign((size_t)h.sqoff[E] * 9, 0);
     h.f0.assign((size_t)h.coff[E] * 3, 0);
     double gx[kMaxNen * 3];
     for (int s = 0; s < E; s++) {
+      if (h.skind[s] != B200FEM_MAT_LINEAR) continue;
+      const double* prm = params_of(h.perm[s]);
+      linear_tangent(C, prm[0], prm[1]);
       const int t = h.stype[s], nen = elem_nen(t), nip = elem_nip(t);
       double* K0 = &h.K0[(size_t)h.sqoff[s] * 9];
       for (int k = 0; k < nip; k++) {

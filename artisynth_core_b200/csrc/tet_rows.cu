@@ -56,6 +56,7 @@ struct TetRowArgs {
   const double* node_kp;
   const int* conn;
   const int* elem_model;
+  const int* elem_mat;  // per element: its row of mat
   const double* x;
   const double* invJ0;
   const double* mat;
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(32 * kRowsWarps) tet_rows_kernel(TetRowArgs a)
 #pragma unroll
       for (int c = 0; c < 3; c++) g[n][c] = invJ[c] * g0 + invJ[3 + c] * g1 + invJ[6 + c] * g2;
     }
-    const double* mp = a.mat + (size_t)a.elem_model[e] * kMatParams;
+    const double* mp = a.mat + (size_t)a.elem_mat[e] * kMatParams;
     double sig[6];
     T Dt[MAT == B200FEM_MAT_NEOHOOKEAN ? 2 : 36];
     if constexpr (MAT == B200FEM_MAT_NEOHOOKEAN) {
@@ -405,6 +406,7 @@ cudaError_t launch_tet_rows(Engine& eng, bool attr_only) {
   a.node_kp = d.node_kp;
   a.conn = d.conn;
   a.elem_model = d.elem_model;
+  a.elem_mat = d.elem_mat;
   a.x = d.x;
   a.invJ0 = d.invJ0;
   a.mat = d.mat;

@@ -210,8 +210,9 @@ class FemEngine:
 # -------------------------------------------------------------------- model
 class FemModel3d:
     """FemModel3d restricted to the hot path: tet, hex, wedge and pyramid
-    elements, linear or quadratic (one type, or any mix of them), one
-    material, lumped mass, fixed nodes and the BackwardEuler data."""
+    elements, linear or quadratic (one type, or any mix of them), the model's
+    material and optional per-element materials, lumped mass, fixed nodes and
+    the BackwardEuler data."""
 
     def __init__(self):
         self.elem_type = L.ELEM_TET
@@ -219,6 +220,7 @@ class FemModel3d:
         self.conn = None
         self.fixed = None
         self.material = LinearMaterial()
+        self.elem_materials = None  # per element: None (the model's material) or its own
         self.density = 1000.0
         self.mass_damping = 2.0      # FemModel.DEFAULT_MASS_DAMPING (FemModel.java:304)
         self.stiffness_damping = 0.0  # FemModel.DEFAULT_STIFFNESS_DAMPING (:303)
@@ -257,6 +259,7 @@ class FemModel3d:
         self.fixed = (np.zeros(self.rest.shape[0], dtype=np.int32) if fixed is None
                       else np.ascontiguousarray(fixed, dtype=np.int32))
         self._grid = None
+        self.elem_materials = None
         self._invalidate()
 
     def jitterInterior(self, frac, seed):
@@ -281,6 +284,36 @@ class FemModel3d:
     def setMaterial(self, mat):
         self.material = mat
         self._invalidate()
+
+    def setElementMaterial(self, e, mat):
+        """FemElement.setMaterial for element e; None restores the model's
+        material (FemModel3d.getElementMaterial, FemModel3d.java:608-614)."""
+        if self.elem_materials is None:
+            self.elem_materials = [None] * self.numElements()
+        self.elem_materials[int(e)] = mat
+        self._invalidate()
+
+    def setElementMaterials(self, mats):
+        """One entry per element (None: the model's material), or None for
+        the model's material everywhere."""
+        if mats is not None and len(mats) != self.numElements():
+            raise ValueError("one material per element")
+        self.elem_materials = None if mats is None else list(mats)
+        self._invalidate()
+
+    def getElementMaterial(self, e):
+        m = None if self.elem_materials is None else self.elem_materials[int(e)]
+        return self.material if m is None else m
+
+    def _element_material_arrays(self):
+        kinds = np.full(self.numElements(), L.MAT_MODEL, dtype=np.int32)
+        prm = np.zeros((self.numElements(), 8))
+        for e, m in enumerate(self.elem_materials):
+            if m is not None:
+                kinds[e] = m.kind
+                p = m.params()
+                prm[e, : len(p)] = p
+        return kinds, prm
 
     def setDensity(self, d):
         self.density = float(d)
@@ -340,6 +373,10 @@ class FemModel3d:
             p = self.material.params()
             prm[: len(p)] = p
             eng.call("b200fem_set_material", self.material.kind, L.dptr(prm), self.density, self.soft_incomp)
+            if self.elem_materials is not None:
+                kinds, eprm = self._element_material_arrays()
+                eng.call("b200fem_set_element_materials", 0, self.numElements(), kinds.ctypes.data,
+                         eprm.ctypes.data)
             for k, v in getattr(self, "options", {}).items():
                 eng.call("b200fem_set_option", int(k), int(v))
             att = getattr(self, "attachments", None)
@@ -580,6 +617,10 @@ class FemPack:
                 eng.call("b200fem_add_model", m.elem_type, m.numNodes(), L.dptr(rest), m.numElements(),
                          L.iptr(conn), L.iptr(m.fixed), m.material.kind, L.dptr(prm), m.density, m.soft_incomp,
                          ctypes.byref(idx))
+                if m.elem_materials is not None:
+                    kinds, eprm = m._element_material_arrays()
+                    eng.call("b200fem_set_element_materials", idx.value, m.numElements(), kinds.ctypes.data,
+                             eprm.ctypes.data)
             for k, v in self.options.items():
                 eng.call("b200fem_set_option", int(k), int(v))
             eng.call("b200fem_build")

@@ -158,6 +158,20 @@ JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doSetMaterial(JNIEnv* 
   return b200fem_set_material(H(h), kind, prm, density, incomp);
 }
 
+// kinds[e]: B200FEM_MAT_* of element e, or B200FEM_MAT_MODEL (-1) where
+// FemElement.getMaterial() is null; params: 8 per element (kinds == null
+// restores the model's material everywhere)
+JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doSetElementMaterials(JNIEnv* env, jclass, jlong h,
+                                                                                jint model, jintArray kinds,
+                                                                                jdoubleArray params) {
+  if (!kinds) return b200fem_set_element_materials(H(h), model, 0, nullptr, nullptr);
+  if (!params) return B200FEM_ERR_INVALID_ARG;
+  Ints k(env, kinds, false);
+  Doubles p(env, params, false);
+  if ((long long)p.size() != 8LL * k.size()) return B200FEM_ERR_INVALID_ARG;
+  return b200fem_set_element_materials(H(h), model, k.size(), k.p, p.p);
+}
+
 JNIEXPORT jint JNICALL Java_maspack_solvers_B200FemSolver_doAddModel(JNIEnv* env, jclass, jlong h, jint type,
                                                                      jdoubleArray rest, jintArray conn,
                                                                      jintArray fixed, jint kind,

@@ -59,10 +59,10 @@ extern "C" {
                                   soft incompressibility resolves to ELEMENT */
 #define B200FEM_ELEM_QUADHEX 5 /* QuadhexElement, 20 nodes (corners 0-7, then the midpoints of
                                   edges 01 12 23 30, 45 56 67 74, 04 15 26 37), 14 points;
-                                  compressible materials (its soft incompressibility has four
-                                  pressure values per element: B200FEM_ERR_UNSUPPORTED) */
+                                  soft incompressibility resolves to ELEMENT with four pressure
+                                  values per element */
 #define B200FEM_ELEM_QUADWEDGE 6   /* QuadwedgeElement, 15 nodes (edges 01 12 20, 34 45 53, 03 14
-                                      25), 9 points; compressible (two pressure values) */
+                                      25), 9 points; ELEMENT with two pressure values */
 #define B200FEM_ELEM_QUADPYRAMID 7 /* QuadpyramidElement, 13 nodes (edges 01 12 23 30, 04 14 24
                                       34), 5 points; soft incompressibility resolves to ELEMENT */
 
@@ -73,6 +73,7 @@ extern "C" {
                                        form, StVenantKirchoffMaterial.java:136-164) */
 #define B200FEM_MAT_MOONEYRIVLIN 2 /* {c10, c01, c11, c20, c02, kappa, jlimit,
                                       bulk_potential(0 quadratic, 1 log)} */
+#define B200FEM_MAT_MODEL (-1)     /* b200fem_set_element_materials: the model's material */
 
 /* soft incompressibility (FemModel3d.IncompMethod) */
 #define B200FEM_INCOMP_OFF 0
@@ -170,6 +171,22 @@ int b200fem_set_mesh_mixed(b200fem_handle h, int n_nodes, const double* rest_xyz
                            const int* elem_types, const int* conn, const int* fixed);
 int b200fem_set_material(b200fem_handle h, int mat_kind, const double* params, double density,
                          int incomp_method);
+/* Per-element materials (FemElement.setMaterial; FemModel3d.getElementMaterial,
+   FemModel3d.java:608-614, returns the element's own material when it has
+   one, else the model's): mat_kinds[e] is element e's B200FEM_MAT_* kind, or
+   B200FEM_MAT_MODEL for the model's material, and params holds 8 values per
+   element in b200fem_set_material's layout (read only where mat_kinds[e] is
+   a kind).  Elements of a compressible kind run without soft
+   incompressibility (FemModel3d.java:3346-3348); ELEMENT uses each element's
+   own kappa; NODAL (which needs the model's material to be MooneyRivlin)
+   uses the model's kappa and is refused with B200FEM_ERR_UNSUPPORTED at the
+   build when any element's material is compressible (the reference divides
+   by a zero nodal rest volume at a node only such elements touch).  model is
+   the pack index (0 for a single model); n_elems must equal its element
+   count; mat_kinds == NULL gives every element the model's material again.
+   b200fem_set_mesh / _set_mesh_mixed clear them. */
+int b200fem_set_element_materials(b200fem_handle h, int model, int n_elems, const int* mat_kinds,
+                                  const double* params);
 /* builds rest data, the block pattern, the element-to-block scatter map and
    uploads everything (the reference's structure build + analyze) */
 int b200fem_build(b200fem_handle h);

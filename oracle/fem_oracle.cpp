@@ -802,8 +802,15 @@ struct Model {
   std::vector<int> sidx;  // solve index (block row) per node, -1 when fixed
   int nact = 0;
   Material mat;
+  // per-element materials, one per element when any element has its own
+  // (FemModel3d.getElementMaterial, FemModel3d.java:608-614)
+  std::vector<Material> emats;
+  const Material& mat_of(int e) const { return emats.empty() ? mat : emats[e]; }
   double density = 1000;
+  int incomp_request = INCOMP_AUTO;
   int incomp = INCOMP_OFF;  // resolved method
+  // an element of a compressible material runs with OFF (FemModel3d.java:3346-3348)
+  int incomp_of(int e) const { return mat_of(e).incompressible() ? incomp : INCOMP_OFF; }
   // rest data
   std::vector<double> invJ0, detJ0;  // per element per IP
   std::vector<double> winvJ0;        // warping-point invJ0 per element
@@ -885,8 +892,10 @@ static void build_linear_cache(Model& m) {
   m.K0.assign((size_t)m.k0off[m.E] * 9, 0);
   m.f0.assign((size_t)m.eoff[m.E] * 3, 0);
   double C[36];
-  linear_C(C, m.mat.E, m.mat.nu);
   for (int e = 0; e < m.E; e++) {
+    const Material& mat = m.mat_of(e);
+    if (!mat.linear()) continue;
+    linear_C(C, mat.E, mat.nu);
     const ShapeTable& s = m.shp(e);
     const int nen = s.nen;
     const int* nodes = m.nodes_of(e);
@@ -990,8 +999,9 @@ static void multi_pressures(const Model& m, int e, const double* x, std::vector<
   const ShapeTable& s = m.shp(e);
   const int nen = s.nen, npv = s.npv;
   const int* nodes = m.nodes_of(e);
-  const double V0 = m.restVol[e], K = m.mat.kappa;
-  const bool quad = m.mat.bulk_potential == 0;
+  const Material& mat = m.mat_of(e);
+  const double V0 = m.restVol[e], K = mat.kappa;
+  const bool quad = mat.bulk_potential == 0;
   std::vector<double> pbuf(npv, 0.0), R((size_t)npv * npv, 0.0);
   for (int k = 0; k < s.nip; k++) {
     double J[9];
@@ -1030,20 +1040,23 @@ static void multi_pressures(const Model& m, int e, const double* x, std::vector<
 
 
 static void element_update(const Model& m, int e, const double* x, ElemOut& out) {
+  // the element's own material, else the model's (FemModel3d.java:2950-2951)
+  const Material& mat = m.mat_of(e);
+  const int incomp = m.incomp_of(e);
   const ShapeTable& s = m.shp(e);
   int nen = s.nen;
   const int* nodes = m.nodes_of(e);
   out.f.assign(nen * 3, 0);
   out.K.assign(nen * nen * 9, 0);
-  out.div.assign(m.incomp == INCOMP_NODAL ? nen * nen * 3 : 0, 0);
+  out.div.assign(incomp == INCOMP_NODAL ? nen * nen * 3 : 0, 0);
   out.inverted = 0;
   out.minDetJ = 1e300;
-  if (m.mat.linear()) {
+  if (mat.linear()) {
     // linear cached path (FemModel3d.java:3359-3390)
     const double* K0 = &m.K0[(size_t)m.k0off[e] * 9];
     const double* f0 = &m.f0[(size_t)m.eoff[e] * 3];
     double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-    if (m.mat.corotated) {
+    if (mat.corotated) {
       // StiffnessWarper3d.computeWarpingRotation (StiffnessWarper3d.java:154-159)
       double J[9], F[9];
       compute_jacobian(J, s.wGNs.data(), nen, x, nodes);
@@ -1058,7 +1071,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         if (bj >= bi) {
           const double* Kij = &K0[(i * nen + j) * 9];
           double* Ko = &out.K[(i * nen + j) * 9];
-          if (m.mat.corotated) {
+          if (mat.corotated) {
             // StiffnessWarper3d.rotateStiffness: R K R^T (:219-222)
             double T[9];
             for (int a = 0; a < 3; a++)
@@ -1077,7 +1090,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       for (int j = 0; j < nen; j++) {
         const double* p = &x[3 * nodes[j]];
         double pos[3];
-        if (m.mat.corotated) {
+        if (mat.corotated) {
           for (int r = 0; r < 3; r++) pos[r] = R[r] * p[0] + R[3 + r] * p[1] + R[6 + r] * p[2];
         } else {
           pos[0] = p[0]; pos[1] = p[1]; pos[2] = p[2];
@@ -1086,7 +1099,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         for (int r = 0; r < 3; r++) tmp[r] += Kij[3 * r] * pos[0] + Kij[3 * r + 1] * pos[1] + Kij[3 * r + 2] * pos[2];
       }
       for (int r = 0; r < 3; r++) tmp[r] -= f0[3 * i + r];
-      if (m.mat.corotated) {
+      if (mat.corotated) {
         double t2[3];
         for (int r = 0; r < 3; r++) t2[r] = R[3 * r] * tmp[0] + R[3 * r + 1] * tmp[1] + R[3 * r + 2] * tmp[2];
         for (int r = 0; r < 3; r++) out.f[3 * i + r] += t2[r];
@@ -1104,16 +1117,16 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
   // (IncompressibleMaterialBase.java:116-152); the constraint vectors
   // c_i = sum_k GNx_i dv (FemUtilities.addToIncompressConstraints) and the
   // dilational stiffness Rinv c_i c_j^T (:3650-3663)
-  const bool elem_inc = m.incomp == INCOMP_ELEMENT;
+  const bool elem_inc = incomp == INCOMP_ELEMENT;
   const int npv = s.npv;
   double elem_p = 0, elem_rinv = 0;
   std::vector<double> cst, pvals, Rinv;
   if (elem_inc && npv == 1) {
     const double V0 = m.restVol[e];
     const double Jp = current_volume(m, e, x) / V0;
-    const double K = m.mat.kappa;
-    elem_p = (m.mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
-    const double keff = (m.mat.bulk_potential == 0) ? K : K * (1 - std::log(Jp)) / (Jp * Jp);
+    const double K = mat.kappa;
+    elem_p = (mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
+    const double keff = (mat.bulk_potential == 0) ? K : K * (1 - std::log(Jp)) / (Jp * Jp);
     elem_rinv = keff / V0;
     cst.assign(nen * 3, 0);
   } else if (elem_inc) {
@@ -1136,7 +1149,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         GNx[3 * n + c] = invJ[c] * g[0] + invJ[3 + c] * g[1] + invJ[6 + c] * g[2];
     }
     double pressure = 0;
-    if (m.incomp == INCOMP_NODAL) {
+    if (incomp == INCOMP_NODAL) {
       if (m.etype[e] == ELEM_TET) {
         for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
         pressure /= nen;
@@ -1159,7 +1172,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         }
     }
     double sig[6], D[36];
-    material_stress_tangent(sig, D, m.mat, F, detF, pressure);
+    material_stress_tangent(sig, D, mat, F, detF, pressure);
     for (int i = 0; i < nen; i++) {
       add_stress_force(&out.f[3 * i], &GNx[3 * i], sig, dv);
       int bi = m.sidx[nodes[i]];
@@ -1176,7 +1189,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
         }
       }
     }
-    if (m.incomp == INCOMP_NODAL && m.etype[e] != ELEM_TET) {
+    if (incomp == INCOMP_NODAL && m.etype[e] != ELEM_TET) {
       // integration points map to nodes (FemModel3d.java:3604-3614):
       // divBlk(node_k, node_j) += dv * GNx_j
       for (int j = 0; j < nen; j++)
@@ -1212,7 +1225,7 @@ static void element_update(const Model& m, int e, const double* x, ElemOut& out)
       }
     }
   }
-  if (m.incomp == INCOMP_NODAL && m.etype[e] == ELEM_TET) {
+  if (incomp == INCOMP_NODAL && m.etype[e] == ELEM_TET) {
     // TetElement.getAreaWeightedNormals (TetElement.java:333-362) * (-1/12)
     const double *p0 = &x[3 * nodes[0]], *p1 = &x[3 * nodes[1]], *p2 = &x[3 * nodes[2]],
                  *p3 = &x[3 * nodes[3]];
@@ -1315,7 +1328,7 @@ static int update_stress_stiffness(Model& m, const double* x) {
         }
       }
     }
-    if (nodal) {
+    if (nodal && !o.div.empty()) {
       for (int i = 0; i < nen; i++) {
         int n = nodes[i];
         for (int j = 0; j < nen; j++) {
@@ -1654,6 +1667,69 @@ void orc_jitter(int nx, int ny, int nz, double wx, double wy, double wz, double 
 
 // mat_params: LINEAR {E, nu, corotated}; NEOHOOKEAN {E, nu};
 // MOONEYRIVLIN {c10, c01, c11, c20, c02, kappa, jlimit, bulk_potential}
+static Material make_material(int kind, const double* p) {
+  Material mat;
+  mat.kind = kind;
+  if (kind == MAT_LINEAR) {
+    mat.E = p[0]; mat.nu = p[1]; mat.corotated = (int)p[2];
+  } else if (kind == MAT_NEOHOOKEAN || kind == MAT_STVK) {
+    mat.E = p[0]; mat.nu = p[1];
+  } else {
+    mat.c10 = p[0]; mat.c01 = p[1]; mat.c11 = p[2];
+    mat.c20 = p[3]; mat.c02 = p[4]; mat.kappa = p[5];
+    mat.jlimit = p[6]; mat.bulk_potential = (int)p[7];
+  }
+  return mat;
+}
+
+// Soft incompressibility and the data that depend on the materials.  NODAL
+// needs the model's material to be incompressible and every element to be a
+// tet or to have its points at its nodes (softNodalIncompressAllowed,
+// FemModel3d.java:400-405); otherwise NODAL and AUTO resolve to ELEMENT
+// (getAllowedSoftIncompMethod, :462-481), and AUTO -> NODAL when #elements >
+// #active nodes, else ELEMENT.  An element of a compressible material runs
+// with OFF (computeStressAndStiffness, :3346-3348), so a model without an
+// incompressible element resolves to OFF.
+static int finalize_model(Model& m) {
+  bool nodal_ok = true, any_incomp = false, all_incomp = true;
+  for (int e = 0; e < m.E; e++) {
+    const int t = m.etype[e];
+    nodal_ok &= (t == ELEM_TET || t == ELEM_HEX || t == ELEM_WEDGE || t == ELEM_PYRAMID);
+    any_incomp |= m.mat_of(e).incompressible();
+    all_incomp &= m.mat_of(e).incompressible();
+  }
+  int method = m.incomp_request;
+  if (!any_incomp) method = INCOMP_OFF;
+  else if ((!m.mat.incompressible() || !nodal_ok) && (method == INCOMP_NODAL || method == INCOMP_AUTO))
+    method = INCOMP_ELEMENT;
+  else if (method == INCOMP_AUTO) method = (m.E > m.nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
+  m.incomp = method;
+  bool any_linear = false;
+  for (int e = 0; e < m.E; e++) any_linear |= m.mat_of(e).linear();
+  m.K0.clear();
+  m.f0.clear();
+  if (any_linear) build_linear_cache(m);
+  build_pattern(m);
+  m.nodeRestVol.clear();
+  m.nodePressure.clear();
+  if (m.incomp == INCOMP_NODAL) {
+    // updateNodalRestVolumes (FemModel3d.java:2594-2628)
+    m.nodeRestVol.assign(m.N, 0);
+    for (int e = 0; e < m.E; e++) {
+      const int* nodes = m.nodes_of(e);
+      const ShapeTable& st = m.shp(e);
+      if (m.etype[e] == ELEM_TET) {
+        for (int i = 0; i < 4; i++) m.nodeRestVol[nodes[i]] += m.restVol[e] / 4;
+      } else {
+        // integration points map to nodes (FemModel3d.java:2608-2614)
+        for (int i = 0; i < st.nen; i++)
+          m.nodeRestVol[nodes[i]] += st.w[i] * m.detJ0[(size_t)m.ipoff[e] + i];
+      }
+    }
+    if (!all_incomp) return -2;
+  }
+  return 0;
+}
 // A mesh of one element type per element (FemModel3d holds any mix of
 // FemElement3d types, FemModel3d.java:3333): types[e], and conn the
 // concatenation of every element's nodes in its type's local order.
@@ -1693,52 +1769,30 @@ void* orc_create_mixed(int nnodes, const double* rest, int nelems, const int* ty
   m->nact = 0;
   for (int n = 0; n < nnodes; n++)
     if (!fixed[n]) m->sidx[n] = m->nact++;
-  m->mat.kind = mat_kind;
-  if (mat_kind == MAT_LINEAR) {
-    m->mat.E = mat_params[0]; m->mat.nu = mat_params[1]; m->mat.corotated = (int)mat_params[2];
-  } else if (mat_kind == MAT_NEOHOOKEAN || mat_kind == MAT_STVK) {
-    m->mat.E = mat_params[0]; m->mat.nu = mat_params[1];
-  } else {
-    m->mat.c10 = mat_params[0]; m->mat.c01 = mat_params[1]; m->mat.c11 = mat_params[2];
-    m->mat.c20 = mat_params[3]; m->mat.c02 = mat_params[4]; m->mat.kappa = mat_params[5];
-    m->mat.jlimit = mat_params[6]; m->mat.bulk_potential = (int)mat_params[7];
-  }
+  m->mat = make_material(mat_kind, mat_params);
   m->density = density;
-  // FemModel3d.computeStressAndStiffness forces OFF for compressible
-  // materials (:3346-3348).  NODAL needs every element to be a tet or to
-  // have its points at its nodes (softNodalIncompressAllowed, :400-405); the
-  // quadratic types are not, so NODAL and AUTO resolve to ELEMENT
-  // (getAllowedSoftIncompMethod, :462-481); otherwise AUTO -> NODAL when
-  // #elements > #active nodes, else ELEMENT.
-  bool nodal_ok = true;
-  for (int e = 0; e < nelems; e++) {
-    const int t = types[e];
-    nodal_ok &= (t == ELEM_TET || t == ELEM_HEX || t == ELEM_WEDGE || t == ELEM_PYRAMID);
-  }
-  int method = incomp_method;
-  if (!m->mat.incompressible()) method = INCOMP_OFF;
-  else if (!nodal_ok && (method == INCOMP_NODAL || method == INCOMP_AUTO))
-    method = INCOMP_ELEMENT;
-  else if (method == INCOMP_AUTO) method = (nelems > m->nact) ? INCOMP_NODAL : INCOMP_ELEMENT;
-  m->incomp = method;
+  m->incomp_request = incomp_method;
   build_rest_data(*m);
-  if (m->mat.linear()) build_linear_cache(*m);
-  build_pattern(*m);
-  if (m->incomp == INCOMP_NODAL) {
-    m->nodeRestVol.assign(m->N, 0);
-    for (int e = 0; e < m->E; e++) {
-      const int* nodes = m->nodes_of(e);
-      const ShapeTable& st = m->shp(e);
-      if (m->etype[e] == ELEM_TET) {
-        for (int i = 0; i < 4; i++) m->nodeRestVol[nodes[i]] += m->restVol[e] / 4;
-      } else {
-        // integration points map to nodes (FemModel3d.java:2608-2614)
-        for (int i = 0; i < st.nen; i++)
-          m->nodeRestVol[nodes[i]] += st.w[i] * m->detJ0[(size_t)m->ipoff[e] + i];
-      }
-    }
-  }
+  finalize_model(*m);
   return m;
+}
+
+// Per-element materials (FemElement.setMaterial): kinds[e] < 0 keeps the
+// model's material, else element e gets kinds[e] with params[8e .. 8e+7].
+// kinds == NULL gives every element the model's material again.  Returns 0,
+// or -2 when soft incompressibility resolves to NODAL while some element's
+// material is compressible (updateNodalPressures, FemModel3d.java:2471-2503,
+// sums nodal volumes over incompressible elements only; a node that only
+// compressible elements touch has a zero rest volume).
+int orc_set_element_materials(void* h, const int* kinds, const double* params) {
+  Model& m = *(Model*)h;
+  m.emats.clear();
+  if (kinds) {
+    m.emats.assign(m.E, m.mat);
+    for (int e = 0; e < m.E; e++)
+      if (kinds[e] >= 0) m.emats[e] = make_material(kinds[e], params + 8 * (size_t)e);
+  }
+  return finalize_model(m);
 }
 
 void* orc_create(int type, int nnodes, const double* rest, int nelems, const int* conn,
@@ -2123,7 +2177,9 @@ int orc_elem_num_ip(void* h, int e) { return ((Model*)h)->shp(e).nip; }
 // stiffness) and out-of-range e or k.
 int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv, double* sig, double* D) {
   const Model& m = *(const Model*)h;
-  if (m.mat.linear() || e < 0 || e >= m.E) return -1;
+  if (e < 0 || e >= m.E || m.mat_of(e).linear()) return -1;
+  const Material& mat = m.mat_of(e);
+  const int incomp = m.incomp_of(e);
   const ShapeTable& s = m.shp(e);
   if (k < 0 || k >= s.nip) return -1;
   const int nen = s.nen;
@@ -2140,23 +2196,23 @@ int orc_ip_data(void* h, const double* x, int e, int k, double* GNx, double* dv,
     for (int c = 0; c < 3; c++) GNx[3 * n + c] = invJ[c] * g[0] + invJ[3 + c] * g[1] + invJ[6 + c] * g[2];
   }
   double pressure = 0;
-  if (m.incomp == INCOMP_NODAL && !m.nodePressure.empty()) {
+  if (incomp == INCOMP_NODAL && !m.nodePressure.empty()) {
     if (m.etype[e] == ELEM_TET) {
       for (int i = 0; i < nen; i++) pressure += m.nodePressure[nodes[i]];
       pressure /= nen;
     } else {
       pressure = m.nodePressure[nodes[k]];
     }
-  } else if (m.incomp == INCOMP_ELEMENT && s.npv == 1) {
+  } else if (incomp == INCOMP_ELEMENT && s.npv == 1) {
     const double Jp = current_volume(m, e, x) / m.restVol[e];
-    const double K = m.mat.kappa;
-    pressure = (m.mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
-  } else if (m.incomp == INCOMP_ELEMENT) {
+    const double K = mat.kappa;
+    pressure = (mat.bulk_potential == 0) ? K * (Jp - 1) : K * std::log(Jp) / Jp;
+  } else if (incomp == INCOMP_ELEMENT) {
     std::vector<double> pvals, Rinv;
     multi_pressures(m, e, x, pvals, Rinv);
     for (int l = 0; l < s.npv; l++) pressure += s.H[(size_t)k * s.npv + l] * pvals[l];
   }
-  material_stress_tangent(sig, D, m.mat, F, detF, pressure);
+  material_stress_tangent(sig, D, mat, F, detF, pressure);
   return nen;
 }
 

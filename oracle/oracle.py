@@ -88,6 +88,8 @@ def lib():
         L.orc_create_mixed.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, ctypes.c_int, _dp,
                                        ctypes.c_double, ctypes.c_int]
         L.orc_create_mixed.restype = vp
+        L.orc_set_element_materials.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_set_element_materials.restype = ctypes.c_int
         L.orc_elem_num_ip.argtypes = [vp, ctypes.c_int]
         L.orc_elem_num_ip.restype = ctypes.c_int
         L.orc_destroy.argtypes = [vp]
@@ -190,6 +192,28 @@ class OracleModel:
         self.nact = self.L.orc_num_active(self.h)
         self.nnzb = self.L.orc_nnzb(self.h)
         self.incomp = self.L.orc_incomp_method(self.h)
+
+    def set_element_materials(self, materials):
+        """materials: one entry per element, None for the model's material or
+        (kind, params) for the element's own (FemElement.setMaterial); None
+        instead of the list restores the model's material everywhere.  Raises
+        ValueError for NODAL soft incompressibility with an element of a
+        compressible material."""
+        if materials is None:
+            st = self.L.orc_set_element_materials(self.h, None, None)
+        else:
+            assert len(materials) == self.E
+            kinds = np.full(self.E, -1, dtype=np.int32)
+            prm = np.zeros((self.E, 8))
+            for e, m in enumerate(materials):
+                if m is not None:
+                    kinds[e] = m[0]
+                    prm[e, : len(m[1])] = m[1]
+            st = self.L.orc_set_element_materials(self.h, kinds.ctypes.data, prm.ctypes.data)
+        self.nnzb = self.L.orc_nnzb(self.h)
+        self.incomp = self.L.orc_incomp_method(self.h)
+        if st != 0:
+            raise ValueError("NODAL soft incompressibility with elements of compressible materials")
 
     def __del__(self):
         try:
