@@ -40,6 +40,7 @@ OPT_REFINE = 8
 OPT_BARRIER_TIMEOUT_MS, OPT_TEST_SKIP_ARRIVAL = 9, 10
 OPT_TET_ASSEMBLY = 11
 OPT_PCG_RESIDENT = 12
+OPT_NODAL_FACTORED = 13
 INTEGRATOR_BACKWARD_EULER, INTEGRATOR_CONSTRAINED_BACKWARD_EULER = 0, 1
 SPLIT_AUTO, SPLIT_CONTIGUOUS, SPLIT_STRIDED, SPLIT_CLUSTER = 0, 1, 2, 3
 

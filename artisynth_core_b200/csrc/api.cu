@@ -555,6 +555,58 @@ int build_pack(Engine& eng) {
     }
   }
 
+  // ---- NODAL solve matrix in factored form: S1 holds the blocks of direct
+  // neighbours (those with element contributions), the dilational term is
+  // applied in the SpMV as sum_n c kp_n d_n (d_n . v) over the active nodes
+  // n of NODAL models (the gather's dilational triples regrouped by node)
+  eng.factored = any_nodal && eng.opt_nodal_factored != 1 && !eng.tet_rows && !eng.fused && eng.opt_split != 3 &&
+                 !eng.att.active();
+  std::vector<int> s1_rowptr, s1_col, s1_diag, s1_of, dil_rptr, dil_node, dil_slot, nbr_row, dil_nodes;
+  if (eng.factored) {
+    s1_of.assign(NB, -1);
+    s1_rowptr.assign(R + 1, 0);
+    s1_diag.assign(R, 0);
+    int cnt = 0;
+    for (int r = 0; r < R; r++) {
+      for (int p = rowptr[r]; p < rowptr[r + 1]; p++)
+        if (cptr[p + 1] > cptr[p]) {
+          s1_of[p] = cnt++;
+          s1_col.push_back(col[p]);
+        }
+      s1_rowptr[r + 1] = cnt;
+      // (a row without blocks -- an active node in no element -- points at
+      // block 0, as its diagonal does in the full pattern)
+      s1_diag[r] = s1_of[blk_diag[r]] >= 0 ? s1_of[blk_diag[r]] : 0;
+    }
+    nbr_row.resize(nbr_ptr[N]);
+    for (int a = 0; a < nbr_ptr[N]; a++) nbr_row[a] = sidx[nbr_idx[a]];
+    dil_rptr.assign(R + 1, 0);
+    for (int r = 0; r < R; r++) {
+      const int i = act_node[r];
+      if (eng.hosts[row_model[r]].incomp == B200FEM_INCOMP_NODAL) {
+        // nbr(i) ascending: the nodes n whose divBlk row holds a slot for i
+        for (int a = nbr_ptr[i]; a < nbr_ptr[i + 1]; a++) {
+          const int n = nbr_idx[a];
+          if (sidx[n] < 0) continue;  // volumeIsControllable: active nodes only
+          auto b = nbr_idx.begin() + nbr_ptr[n], e = nbr_idx.begin() + nbr_ptr[n + 1];
+          dil_node.push_back(n);
+          dil_slot.push_back((int)(std::lower_bound(b, e, i) - nbr_idx.begin()));
+        }
+      }
+      dil_rptr[r + 1] = (int)dil_node.size();
+    }
+    for (int m = 0; m < M; m++)
+      if (eng.hosts[m].incomp == B200FEM_INCOMP_NODAL)
+        for (int n = eng.node_off[m]; n < eng.node_off[m + 1]; n++)
+          if (sidx[n] >= 0) dil_nodes.push_back(n);
+  }
+  // PCG work per row: its blocks, plus (factored) half a block per
+  // dilational entry (32 against 76 bytes)
+  const std::vector<int>& prow = eng.factored ? s1_rowptr : rowptr;
+  std::vector<long long> wrow(R + 1, 0);
+  for (int r = 0; r <= R; r++) wrow[r] = prow[r] + (eng.factored ? dil_rptr[r] / 2 : 0);
+  const long long WB = wrow[R];
+
   // ---- PCG work split.  Contiguous: CTAs own contiguous row ranges
   // balanced by blocks, cut into pieces at model boundaries.
   // One 1024-thread CTA per SM at most, >= 32 rows (one per warp) each.
@@ -571,8 +623,8 @@ int build_pack(Engine& eng) {
     cut[0] = 0;
     int r = 0;
     for (int c = 1; c < G; c++) {
-      long long target = NB * c / G;
-      while (r < R && rowptr[r] < target) r++;
+      long long target = WB * c / G;
+      while (r < R && wrow[r] < target) r++;
       cut[c] = std::max(r, cut[c - 1]);
     }
     int maxp = 0;
@@ -606,7 +658,7 @@ int build_pack(Engine& eng) {
   for (int c = 0; c < G; c++) {
     int ra = piece_row[cta_piece[c]], rb = piece_row[cta_piece[c + 1]];
     eng.pcg_nloc_max = std::max(eng.pcg_nloc_max, rb - ra);
-    eng.pcg_nb_max = std::max(eng.pcg_nb_max, rowptr[rb] - rowptr[ra]);
+    eng.pcg_nb_max = std::max(eng.pcg_nb_max, prow[rb] - prow[ra]);
   }
   pcg_plan_smem(eng.device, eng.pcg_nloc_max, eng.pcg_nb_max, &eng.pcg_resident, &eng.pcg_cached,
                 eng.precision == B200FEM_PREC_MIXED);
@@ -615,9 +667,14 @@ int build_pack(Engine& eng) {
   // global vectors); a matrix streamed from HBM needs the non-resident
   // form's 1024-thread CTAs, twice the warps for its loads (the 60x30x30
   // MooneyRivlin block, 142 MB FP32: 60 us per iteration against 78
-  // resident).  Auto: resident up to 64 MB of S.
-  const double s_bytes = 9.0 * (eng.precision == B200FEM_PREC_MIXED ? 4 : 8) * (double)NB;
-  if (eng.opt_resident == 1 || (eng.opt_resident == 0 && s_bytes > 64e6)) eng.pcg_resident = eng.pcg_cached = 0;
+  // resident).  Auto: resident up to 64 MB of S; the factored NODAL matrix
+  // (S1, divBlk rows and their indices; gathered, latency-bound) up to 32 MB
+  // (the same block factored: 35.3 us per iteration mixed with global
+  // vectors against 36.9 resident, 48 MB; FP64 41.8 against 41.6, 79 MB)
+  double s_bytes = 9.0 * (eng.precision == B200FEM_PREC_MIXED ? 4 : 8) * (double)prow[R];
+  if (eng.factored) s_bytes += 24.0 * nbr_ptr[N] + 8.0 * dil_rptr[R];
+  const double res_max = eng.factored ? 32e6 : 64e6;
+  if (eng.opt_resident == 1 || (eng.opt_resident == 0 && s_bytes > res_max)) eng.pcg_resident = eng.pcg_cached = 0;
   eng.pcg_strided = 0;
   if (!contiguous_ok) {
     if (eng.opt_split == 1) return fail(&eng, B200FEM_ERR_UNSUPPORTED, "too many models for a contiguous PCG split");
@@ -666,7 +723,7 @@ int build_pack(Engine& eng) {
         auto& top = heap.back();
         const int ra = piece_row[k], rb = piece_row[k + 1];
         owner[k] = top.second;
-        top.first += row_cost * (rb - ra) + blk_cost * (rowptr[rb] - rowptr[ra]);
+        top.first += row_cost * (rb - ra) + blk_cost * (double)(wrow[rb] - wrow[ra]);
         maxp = std::max(maxp, ++count[top.second]);
         std::push_heap(heap.begin(), heap.end(), later);
       }
@@ -704,12 +761,14 @@ int build_pack(Engine& eng) {
   if (eng.opt_row_lanes > 0) {
     eng.pcg_row_lanes = eng.opt_row_lanes;
   } else {
-    const double bpr = R > 0 ? (double)NB / R : 1.0;
+    // (factored NODAL: the direct blocks and as many dilational entries)
+    const double bpr = R > 0 ? (double)(eng.factored ? prow[R] + dil_rptr[R] : NB) / R : 1.0;
     // many rows in flight per warp do best up to hexes' ~27 blocks per row
     // (measured: 40x10x10 hex beam 6.8 us per iteration at 4 lanes, 7.1
     // at 16); NODAL 2-ring rows (~69 blocks) -> 16 (the 60x30x30
     // MooneyRivlin block: 60.4 us per iteration mixed at 16 lanes, 62.9 at
-    // 32, 62.3 at 8)
+    // 32, 62.3 at 8); the same block factored (~24 entries per row) -> 4
+    // (FP64 41.8 us at 4 lanes, 43.6 at 8, 47.3 at 16)
     eng.pcg_row_lanes = bpr <= 40 ? 4 : 16;
   }
 
@@ -759,6 +818,20 @@ int build_pack(Engine& eng) {
       if (!(mirror[p] >= 0 && mirror[p] < p)) up.push_back((int)p);
     d.n_up = (long long)up.size();
     CK(upload(eng, &d.up_blocks, up));
+    if (eng.factored) {
+      // the step's gather: the upper direct blocks, written to S1
+      std::vector<int> u1, u1d, u1m;
+      for (int p : up)
+        if (s1_of[p] >= 0) {
+          u1.push_back(p);
+          u1d.push_back(s1_of[p]);
+          u1m.push_back(s1_of[mirror[p]]);
+        }
+      d.n_up1 = (long long)u1.size();
+      CK(upload(eng, &d.up1, u1));
+      CK(upload(eng, &d.up1_dst, u1d));
+      CK(upload(eng, &d.up1_mdst, u1m));
+    }
   }
   CK(upload(eng, &d.inc_ptr, iptr));
   CK(upload(eng, &d.inc_idx, iidx));
@@ -781,10 +854,26 @@ int build_pack(Engine& eng) {
     std::vector<float> invJ0_f(invJ0.begin(), invJ0.end());
     CK(upload(eng, &d.invJ0_f, invJ0_f));
     CK(dalloc(eng, &d.elemK_f, (size_t)proff[E] * 9));
-    CK(dalloc(eng, &d.S_f, (size_t)NB * 9));
+    if (eng.factored) CK(dalloc(eng, &d.S1_f, std::max<size_t>(s1_col.size(), 1) * 9));
+    else CK(dalloc(eng, &d.S_f, (size_t)NB * 9));
   } else {
     CK(dalloc(eng, &d.elemK, (size_t)proff[E] * 9));
-    CK(dalloc(eng, &d.S, (size_t)NB * 9));
+    if (eng.factored) CK(dalloc(eng, &d.S1, std::max<size_t>(s1_col.size(), 1) * 9));
+    else CK(dalloc(eng, &d.S, (size_t)NB * 9));
+  }
+  if (eng.factored) {
+    d.s1_nnzb = (long long)s1_col.size();
+    CK(upload(eng, &d.s1_rowptr, s1_rowptr));
+    CK(upload(eng, &d.s1_col, s1_col));
+    CK(upload(eng, &d.s1_diag, s1_diag));
+    CK(upload(eng, &d.dil_rptr, dil_rptr));
+    CK(upload(eng, &d.dil_node, dil_node));
+    CK(upload(eng, &d.dil_slot, dil_slot));
+    CK(upload(eng, &d.nbr_row, nbr_row));
+    CK(upload(eng, &d.dil_nodes, dil_nodes));
+    d.n_dil_nodes = (int)dil_nodes.size();
+    CK(dalloc(eng, &d.dil_t, (size_t)N));
+    CK(cudaMemset(d.dil_t, 0, sizeof(double) * (size_t)N));
   }
   CK(dalloc(eng, &d.elemF, (size_t)coff[E] * 3));
   CK(dalloc(eng, &d.Dinv, (size_t)R * 9));
@@ -1330,6 +1419,11 @@ int b200fem_set_option(b200fem_handle h, int key, int value) {
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "PCG_RESIDENT is set before b200fem_build");
       eng.opt_resident = value;
       return B200FEM_OK;
+    case B200FEM_OPT_NODAL_FACTORED:
+      if (value < 0 || value > 2) return fail(&eng, B200FEM_ERR_INVALID_ARG, "NODAL_FACTORED must be 0, 1 or 2");
+      if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "NODAL_FACTORED is set before b200fem_build");
+      eng.opt_nodal_factored = value;
+      return B200FEM_OK;
     case B200FEM_OPT_TET_ASSEMBLY:
       if (value < 0 || value > 1) return fail(&eng, B200FEM_ERR_INVALID_ARG, "TET_ASSEMBLY must be 0 or 1");
       if (eng.built) return fail(&eng, B200FEM_ERR_STATE, "TET_ASSEMBLY is set before b200fem_build");
@@ -1371,6 +1465,9 @@ int b200fem_get_option(b200fem_handle h, int key, int* value) {
     case B200FEM_OPT_BARRIER_TIMEOUT_MS: *value = eng.barrier_timeout_ms; break;
     case B200FEM_OPT_TET_ASSEMBLY: *value = eng.built ? (eng.tet_rows ? 0 : 1) : eng.opt_tet_assembly; break;
     case B200FEM_OPT_PCG_RESIDENT: *value = eng.built ? (eng.pcg_resident ? 2 : 1) : eng.opt_resident; break;
+    case B200FEM_OPT_NODAL_FACTORED:
+      *value = eng.built ? (eng.factored ? 2 : 1) : eng.opt_nodal_factored;
+      break;
     case B200FEM_OPT_TEST_SKIP_ARRIVAL: *value = eng.test_skip_arrival; break;
     default: return fail(&eng, B200FEM_ERR_INVALID_ARG, "unknown option");
   }
@@ -1544,6 +1641,9 @@ int b200fem_update_stress_stiffness(b200fem_handle h, const double* x, double* f
   CK(launch_reset_status(eng));
   CK(cudaEventRecord(eng.ev[0], eng.stream));
   CK(launch_assemble(eng, 1.0, 0.0, true));
+  // the factored solve matrix of the last step reads divBlk and kp, which
+  // this assembly has just replaced
+  if (eng.factored) eng.have_matrix = false;
   CK(launch_forces_only(eng));
   if (eng.att.active()) CK(launch_attach_reduce(eng));
   CK(cudaEventRecord(eng.ev[1], eng.stream));

@@ -180,6 +180,26 @@ struct DevPack {
   int* dil_ptr = nullptr;      // nnzb+1 dilational contributions per block
   int* dil_idx = nullptr;      // (divblk row i, divblk row j, node n) triples
   int has_nodal = 0;
+  // NODAL solve matrix in factored form (B200FEM_OPT_NODAL_FACTORED): the
+  // direct-neighbour blocks S1 (the element terms) assembled, the dilational
+  // term c_m sum_n kp_n d_n d_n^T applied from divBlk inside every SpMV
+  int* s1_rowptr = nullptr;    // n_rows+1
+  int* s1_col = nullptr;       // s1_nnzb
+  int* s1_diag = nullptr;      // n_rows
+  long long s1_nnzb = 0;
+  double* S1 = nullptr;        // s1_nnzb*9 (FP64 form)
+  float* S1_f = nullptr;       // s1_nnzb*9 (mixed form)
+  int* up1_dst = nullptr;      // n_up1: S1 position of each upper direct block (up1 lists them)
+  int* up1_mdst = nullptr;     // n_up1: S1 position of its transpose
+  int* up1 = nullptr;          // n_up1: block index in the full pattern
+  long long n_up1 = 0;
+  int* dil_rptr = nullptr;     // n_rows+1: per row its (node n, divBlk slot of the row's node in nbr(n))
+  int* dil_node = nullptr;
+  int* dil_slot = nullptr;
+  int* nbr_row = nullptr;      // nbr_ptr[N]: block row of each neighbour slot (-1 fixed)
+  int* dil_nodes = nullptr;    // the active nodes of NODAL models (the dilational terms' nodes)
+  int n_dil_nodes = 0;
+  double* dil_t = nullptr;     // N: c_m kp_n (d_n . v) of the SpMV in progress
   // ELEMENT soft incompressibility: per element rest volume, pressure and
   // Rinv (effective modulus / rest volume)
   double* elem_rest_vol = nullptr;
@@ -353,6 +373,8 @@ struct Engine {
   // B200FEM_OPT_TET_ASSEMBLY 0 (default) where supported, 1 element kernel + gather
   int opt_tet_assembly = 1;  // element path (B200FEM_OPT_TET_ASSEMBLY)
   int opt_resident = 0;      // B200FEM_OPT_PCG_RESIDENT
+  int opt_nodal_factored = 0;  // B200FEM_OPT_NODAL_FACTORED: 0 auto, 1 assembled, 2 factored
+  bool factored = false;       // the step's NODAL solve matrix in factored form
   bool tet_rows = false;
   int rows_cap = 32;                   // incidences per task (32 or 64)
   std::vector<int> rows_task_off;      // per element group: its task range

@@ -726,13 +726,17 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
     const int* __restrict__ row_model, const int* __restrict__ act_node, const double* __restrict__ mass,
     const double* __restrict__ step, int mode, TO* __restrict__ out, const int* __restrict__ dptr,
     const int* __restrict__ didx, const double* __restrict__ divblk, const double* __restrict__ node_kp,
-    const int* __restrict__ active, const int* __restrict__ mirror) {
+    const int* __restrict__ active, const int* __restrict__ mirror, const int* __restrict__ dst,
+    const int* __restrict__ mdst) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_up) return;
   const int p = up[q];
   const int row = blk_row[p];
   if (active && !active[row_model[row]]) return;  // blocks of models left out stay
-  const int mp = mirror[p];
+  // output positions: the block's own and its transpose's, or (the factored
+  // NODAL solve matrix) their places in S1
+  const int op = dst ? dst[q] : p;
+  const int mp = dst ? mdst[q] : mirror[p];
   double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   const int c1 = cptr[p + 1];
   for (int c = cptr[p]; c < c1; c++) {
@@ -786,10 +790,10 @@ __global__ void __launch_bounds__(256) gather_block_kernel(
       v[k] = (TO)val;
     }
   }
-  TO* o = out + (size_t)p * 9;
+  TO* o = out + (size_t)op * 9;
 #pragma unroll
   for (int k = 0; k < 9; k++) o[k] = v[k];
-  if (mp != p) {
+  if (mp != op) {
     // off-diagonal: no mass term; the mirror is the transpose
     TO* t = out + (size_t)mp * 9;
 #pragma unroll
@@ -1009,6 +1013,38 @@ __global__ void spmv_kernel(int n_rows, const int* rowptr, const int* col, const
     y[3 * (size_t)warp + 1] = out[1];
     y[3 * (size_t)warp + 2] = out[2];
   }
+}
+
+// factored NODAL solve matrix, outside the PCG: t_n of every dilational
+// node, then each row adds sum t_n d_n(row) over its entries (node order)
+__global__ void dil_t_kernel(int nd, const int* __restrict__ nodes, const int* __restrict__ nbr_ptr,
+                             const int* __restrict__ nbr_row, const double* __restrict__ divblk,
+                             const double* __restrict__ node_kp, const int* __restrict__ node_model,
+                             const double* __restrict__ step, const double* __restrict__ v, double* __restrict__ t) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nd) return;
+  const int n = nodes[k];
+  const double* sp = step + (size_t)node_model[n] * 8;
+  const double c = sp[0] * sp[0] + sp[0] * sp[2];
+  t[n] = c * node_kp[n] * dil_node_t(nbr_ptr[n], nbr_ptr[n + 1], nbr_row, divblk, v);
+}
+
+__global__ void dil_add_kernel(int n_rows, const int* __restrict__ dil_rptr, const int* __restrict__ dil_node,
+                               const int* __restrict__ dil_slot, const double* __restrict__ divblk,
+                               const double* __restrict__ t, double* __restrict__ y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_rows) return;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int e = dil_rptr[r]; e < dil_rptr[r + 1]; e++) {
+    const double tn = t[dil_node[e]];
+    const double* g = divblk + 3 * (size_t)dil_slot[e];
+    a0 += tn * g[0];
+    a1 += tn * g[1];
+    a2 += tn * g[2];
+  }
+  y[3 * (size_t)r] += a0;
+  y[3 * (size_t)r + 1] += a1;
+  y[3 * (size_t)r + 2] += a2;
 }
 
 // full-partition scalar CRS export: value of block p entry (r, c) goes to
@@ -2372,6 +2408,21 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
   }
   const int* act = eng.any_inactive ? d.model_active : nullptr;
   if (d.n_up == 0) return cudaSuccess;
+  if (!want_K && eng.factored) {
+    // the step's factored solve matrix: the direct blocks into S1, without
+    // the dilational triples (the PCG applies that term from divBlk)
+    if (d.n_up1 == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((d.n_up1 + 255) / 256);
+    if (fp32)
+      gather_block_kernel<float, float><<<blocks, 256, 0, eng.stream>>>(
+          d.n_up1, d.up1, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model, d.act_node,
+          d.mass, d.step, 1, d.S1_f, nullptr, nullptr, nullptr, nullptr, act, d.blk_mirror, d.up1_dst, d.up1_mdst);
+    else
+      gather_block_kernel<double, double><<<blocks, 256, 0, eng.stream>>>(
+          d.n_up1, d.up1, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model, d.act_node,
+          d.mass, d.step, 1, d.S1, nullptr, nullptr, nullptr, nullptr, act, d.blk_mirror, d.up1_dst, d.up1_mdst);
+    return cudaGetLastError();
+  }
   // Matrices that stay in L2 (up to 64 MB of blocks): one thread per block
   // with warp-staged contiguous stores (the 40x10x10 hex beam: 13.1 us per
   // gather against 17.3 for the list form); larger ones stream from HBM and
@@ -2402,16 +2453,16 @@ cudaError_t launch_assemble(Engine& eng, double cK, double cM, bool want_K) {
     if (want_K)
       gather_block_kernel<float, double><<<blocks, 256, 0, eng.stream>>>(
           d.n_up, d.up_blocks, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model,
-          d.act_node, d.mass, d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror);
+          d.act_node, d.mass, d.step, 0, d.K, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror, nullptr, nullptr);
     else
       gather_block_kernel<float, float><<<blocks, 256, 0, eng.stream>>>(
           d.n_up, d.up_blocks, d.contrib_ptr, d.contrib_idx, d.elemK_f, d.blk_row, d.blk_diag, d.row_model,
-          d.act_node, d.mass, d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror);
+          d.act_node, d.mass, d.step, 1, d.S_f, d.dil_ptr, d.dil_idx, d.divblk, d.node_kp, act, d.blk_mirror, nullptr, nullptr);
   } else {
     gather_block_kernel<double, double><<<blocks, 256, 0, eng.stream>>>(
         d.n_up, d.up_blocks, d.contrib_ptr, d.contrib_idx, d.elemK, d.blk_row, d.blk_diag, d.row_model,
         d.act_node, d.mass, d.step, want_K ? 0 : 1, want_K ? d.K : d.S, d.dil_ptr, d.dil_idx, d.divblk,
-        d.node_kp, act, d.blk_mirror);
+        d.node_kp, act, d.blk_mirror, nullptr, nullptr);
   }
   return cudaGetLastError();
 }
@@ -2472,6 +2523,19 @@ cudaError_t launch_spmv(Engine& eng, const double* x, double* y) {
   DevPack& d = eng.d;
   int threads = 256;
   long long blocks = ((long long)d.n_rows * 32 + threads - 1) / threads;
+  if (eng.factored) {
+    if (eng.precision == B200FEM_PREC_MIXED)
+      spmv_kernel<float><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.s1_rowptr, d.s1_col, d.S1_f, x, y);
+    else
+      spmv_kernel<double><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.s1_rowptr, d.s1_col, d.S1, x, y);
+    if (d.n_dil_nodes > 0) {
+      dil_t_kernel<<<(d.n_dil_nodes + 127) / 128, 128, 0, eng.stream>>>(
+          d.n_dil_nodes, d.dil_nodes, d.nbr_ptr, d.nbr_row, d.divblk, d.node_kp, d.node_model, d.step, x, d.dil_t);
+      dil_add_kernel<<<(d.n_rows + 127) / 128, 128, 0, eng.stream>>>(d.n_rows, d.dil_rptr, d.dil_node, d.dil_slot,
+                                                                     d.divblk, d.dil_t, y);
+    }
+    return cudaGetLastError();
+  }
   if (eng.precision == B200FEM_PREC_MIXED)
     spmv_kernel<float><<<(unsigned)blocks, threads, 0, eng.stream>>>(d.n_rows, d.blk_rowptr, d.blk_col, d.S_f, x, y);
   else

@@ -156,6 +156,20 @@ struct PcgArgs {
   // normal (zero for rows without a constraint) and the plane's offset
   const double* row_nrm;
   const double* row_off;
+  // the factored NODAL solve matrix (null dil_rptr: S is the whole matrix):
+  // per row its (node, divBlk slot) entries, the dilational nodes with their
+  // neighbour slots' rows, and t_n of the SpMV in progress
+  const int* dil_rptr;
+  const int* dil_node;
+  const int* dil_slot;
+  const int* dil_nodes;
+  int n_dil_nodes;
+  const int* nbr_ptr;
+  const int* nbr_row;
+  const double* divblk;
+  const double* node_kp;
+  const int* node_model;
+  double* dil_t;
 };
 
 // Plane constraints: the constrained velocities of a row lie on its plane,
@@ -370,7 +384,27 @@ struct MatView {
   const int* col_s;
   const MT* S_s;
   int cached;
+  // factored NODAL term (dil_rptr null: none): y_row += sum t_n d_n(row)
+  const int* dil_rptr;
+  const int* dil_node;
+  const int* dil_slot;
+  const double* divblk;
+  const double* dil_t;
 };
+
+// The dilational entries e0, e0 + stride, ... < e1 of one row, added to a
+// lane's partial sums before the row's shuffle reduction.
+template <typename MT>
+__device__ __forceinline__ void dil_row_walk(const MatView<MT>& mv, int e0, int e1, int stride, double& a0,
+                                             double& a1, double& a2) {
+  for (int e = e0; e < e1; e += stride) {
+    const double tn = mv.dil_t[mv.dil_node[e]];
+    const double* g = mv.divblk + 3 * (size_t)mv.dil_slot[e];
+    a0 += tn * g[0];
+    a1 += tn * g[1];
+    a2 += tn * g[2];
+  }
+}
 
 // the FP64-value walk of block_row_walk (below)
 __device__ __forceinline__ void block_row_walk_f64(const int* col, const double* S, const double* x, int p, int p1,
@@ -483,6 +517,7 @@ __device__ __forceinline__ void view_row_spmv(const MatView<MT>& mv, int i, int 
   }
   double a0 = 0, a1 = 0, a2 = 0;
   block_row_walk<MT>(col, S, x, p0 + lane, p1, 32, a0, a1, a2);
+  if (mv.dil_rptr) dil_row_walk(mv, mv.dil_rptr[row] + lane, mv.dil_rptr[row + 1], 32, a0, a1, a2);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -522,6 +557,7 @@ __device__ __forceinline__ void view_rows_spmv_group(const MatView<MT>& mv, int 
   const int gl = lane & (L - 1);
   double a0 = 0, a1 = 0, a2 = 0;
   block_row_walk<MT>(col, S, x, p0 + gl, p1, L, a0, a1, a2);
+  if (mv.dil_rptr && valid) dil_row_walk(mv, mv.dil_rptr[row] + gl, mv.dil_rptr[row + 1], L, a0, a1, a2);
 #pragma unroll
   for (int off = L / 2; off > 0; off >>= 1) {
     a0 += __shfl_xor_sync(0xffffffffu, a0, off);
@@ -686,7 +722,47 @@ __host__ __device__ inline void pcg_smem_layout(int nloc_max, int nb_max, int re
 // RES: compiled for shared-memory resident row state (the contiguous split
 // of packs that fit); otherwise residency is the runtime flag (zero in the
 // strided split), which keeps the register pressure of each form low.
-template <typename MT, bool RES>
+// Factored NODAL solve matrix: t_n = (h^2 + h beta) kp_n (d_n . v) of every
+// dilational node.  A group of kDilLanes lanes takes one node, its lanes
+// the node's neighbour slots with that stride (so a node costs one round of
+// independent loads instead of a chain over its ~15 slots), then a
+// shuffle reduction; the nodes are dealt over all warps of the launch.  v
+// is a published vector; a grid barrier follows before any row reads t.
+constexpr int kDilLanes = 8;
+__device__ __forceinline__ void dil_phase(const PcgArgs& a, const double* v) {
+  constexpr int G = kDilLanes, per_warp = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+  const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  // warp-uniform loop: every lane of the warp takes part in the shuffles
+  for (int base = gwarp * per_warp; base < a.n_dil_nodes; base += nwarps * per_warp) {
+    const int k = base + lane / G;
+    const bool valid = k < a.n_dil_nodes;
+    int n = 0;
+    double s = 0;
+    if (valid) {
+      n = a.dil_nodes[k];
+      const int q1 = a.nbr_ptr[n + 1];
+      for (int q = a.nbr_ptr[n] + gl; q < q1; q += G) {
+        const int r = a.nbr_row[q];
+        if (r < 0) continue;
+        const double* g = a.divblk + 3 * (size_t)q;
+        const double* x = v + 3 * (size_t)r;
+        s += g[0] * x[0] + g[1] * x[1] + g[2] * x[2];
+      }
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (valid && gl == 0) {
+      const double* sp = a.step + (size_t)a.node_model[n] * 8;
+      a.dil_t[n] = (sp[0] * sp[0] + sp[0] * sp[2]) * a.node_kp[n] * s;
+    }
+  }
+}
+
+// DIL: the factored NODAL solve matrix (a separate instantiation, so the
+// 64-register form of the plain matrix keeps its registers)
+template <typename MT, bool RES, bool DIL = false>
 __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   __shared__ double rowbuf[kRowChunk][3];
   __shared__ double sn[kRowChunk][3];
@@ -773,6 +849,14 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
   mv.ro_s = (const int*)(dyn + off_ro);
   mv.col_s = (const int*)(dyn + off_col);
   mv.S_s = (const MT*)(dyn + off_S);
+  mv.dil_rptr = DIL ? a.dil_rptr : nullptr;
+  mv.dil_node = DIL ? a.dil_node : nullptr;
+  mv.dil_slot = DIL ? a.dil_slot : nullptr;
+  mv.divblk = DIL ? a.divblk : nullptr;
+  mv.dil_t = DIL ? a.dil_t : nullptr;
+  // every CTA takes the factored term's extra phase and grid barrier before
+  // each SpMV alike (the same instantiation for the whole launch)
+  constexpr bool dil = DIL;
   // residency and caching are planned only for the contiguous split, where
   // local row i is global row r0 + i
   const int r0 = npc > 0 ? s_grow[0] : 0;
@@ -825,6 +909,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     }
   }
   rescan(s_done);
+  if (dil) {
+    dil_phase(a, a.x);
+    if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+  }
 
   // ---- P0: block-Jacobi inverse, r = b - S x0, u = Dinv r (published to
   // m1 for the next SpMV), ||b||^2
@@ -838,6 +926,19 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       double d[9], inv[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) d[k] = (double)Db[k];
+      if (dil) {
+        // the dilational term's diagonal block: sum_n c kp_n d_n(row) d_n(row)^T
+        const double* sp = a.step + (size_t)a.row_model[row] * 8;
+        const double cm = sp[0] * sp[0] + sp[0] * sp[2];
+        for (int e = a.dil_rptr[row]; e < a.dil_rptr[row + 1]; e++) {
+          const double* g = a.divblk + 3 * (size_t)a.dil_slot[e];
+          const double ck = cm * a.node_kp[a.dil_node[e]];
+#pragma unroll
+          for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) d[3 * r + c] += ck * g[r] * g[c];
+        }
+      }
       if (invert3(inv, d) == 0.0) {
         atomicExch(a.flags, B200FEM_ERR_INVALID_ARG);
 #pragma unroll
@@ -928,6 +1029,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
           total_it += it;
           break;
         }
+        if (dil) {
+          dil_phase(a, a.m1);
+          if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+        }
         cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
                               [&](int i, int row, int j, int ln, bool valid, double* vals) {
           const bool act = valid && !s_conv[j];
@@ -997,6 +1102,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
     // ---- P1: w = S u, m = Dinv w (published to m0); dots r.u, w.u, r.r
     for (int j = threadIdx.x; j < npc; j += blockDim.x) s_first[j] = 1;
     rescan(s_conv);
+    if (dil) {
+      dil_phase(a, a.m1);
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+    }
     cta_row_pass<3, true>(a, active_view(), ph & 1, rowbuf, pacc,
                           [&](int i, int row, int j, int ln, bool valid, double* vals) {
       const bool act = valid && !s_conv[j];
@@ -1028,6 +1137,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       if (blockIdx.x == 0 && threadIdx.x == 0 && idx + 2 <= a.max_iter) a.unconv[idx + 2] = 0;
       const double* mc = mbuf ? a.m1 : a.m0;
       double* mn = mbuf ? a.m0 : a.m1;
+      if (dil) {
+        dil_phase(a, mc);
+        if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+      }
       // The SpMV n = S m does not depend on this iteration's scalars, so it
       // runs on the first warps while the last warps reduce the scalars.
       // Both work on the rows of the models unconverged when the iteration
@@ -1256,6 +1369,10 @@ __global__ void __launch_bounds__(pcg_block(RES)) pcg_kernel(PcgArgs a) {
       for (int i = threadIdx.x; i < nloc; i += blockDim.x) store3(a.x, r0 + i, st.at(VX, i, r0 + i));
     rescan(s_done);
     if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+    if (dil) {
+      dil_phase(a, a.x);
+      if (!grid_barrier(a.barrier, a.flags, &s_bar_round, a.barrier_timeout_ns, a.skip_arrival_cta)) return;
+    }
     cta_row_pass<1, true>(a, active_view(), ph & 1, rowbuf, pacc,
                           [&](int i, int row, int, int ln, bool valid, double* vals) {
       double Ax[3];
@@ -1412,6 +1529,24 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
                   ? d.row_nrm
                   : nullptr;
   a.row_off = a.row_nrm ? d.row_off : nullptr;
+  a.dil_rptr = nullptr;
+  if (eng.factored) {
+    a.rowptr = d.s1_rowptr;
+    a.col = d.s1_col;
+    a.blk_diag = d.s1_diag;
+    a.S = d.S1;
+    if (d.n_dil_nodes > 0) a.dil_rptr = d.dil_rptr;
+    a.dil_node = d.dil_node;
+    a.dil_slot = d.dil_slot;
+    a.dil_nodes = d.dil_nodes;
+    a.n_dil_nodes = d.n_dil_nodes;
+    a.nbr_ptr = d.nbr_ptr;
+    a.nbr_row = d.nbr_row;
+    a.divblk = d.divblk;
+    a.node_kp = d.node_kp;
+    a.node_model = d.node_model;
+    a.dil_t = d.dil_t;
+  }
   a.resident = eng.pcg_resident;
   a.cached = eng.pcg_cached;
   a.nloc_max = eng.pcg_nloc_max;
@@ -1433,10 +1568,16 @@ cudaError_t launch_pcg_on(Engine& eng, int max_iter, bool update_state, const do
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (eng.precision == B200FEM_PREC_MIXED) {
-    a.S = d.S_f;
+    a.S = eng.factored ? (const void*)d.S1_f : (const void*)d.S_f;
+    if (a.dil_rptr)
+      return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<float, true, true>, a)
+                        : cudaLaunchKernelEx(&cfg, pcg_kernel<float, false, true>, a);
     return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<float, true>, a)
                       : cudaLaunchKernelEx(&cfg, pcg_kernel<float, false>, a);
   }
+  if (a.dil_rptr)
+    return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true, true>, a)
+                      : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false, true>, a);
   return a.resident ? cudaLaunchKernelEx(&cfg, pcg_kernel<double, true>, a)
                     : cudaLaunchKernelEx(&cfg, pcg_kernel<double, false>, a);
 }
@@ -1469,6 +1610,12 @@ static cudaError_t ensure_pcg_smem(int device, size_t bytes, bool fp32 = false) 
   if (e == cudaSuccess)
     e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, true>, at, (int)bytes)
              : cudaFuncSetAttribute(pcg_kernel<double, true>, at, (int)bytes);
+  if (e == cudaSuccess)
+    e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, false, true>, at, (int)bytes)
+             : cudaFuncSetAttribute(pcg_kernel<double, false, true>, at, (int)bytes);
+  if (e == cudaSuccess)
+    e = fp32 ? cudaFuncSetAttribute(pcg_kernel<float, true, true>, at, (int)bytes)
+             : cudaFuncSetAttribute(pcg_kernel<double, true, true>, at, (int)bytes);
   if (e == cudaSuccess) cur = (int)bytes;
   return e;
 }
@@ -1741,6 +1888,7 @@ int pcg_solve_noalloc(int n_rows, const int* rowptr, const int* col, const doubl
   a.single_model = 0;
   a.row_nrm = nullptr;
   a.row_off = nullptr;
+  a.dil_rptr = nullptr;
   a.tol_override = 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);

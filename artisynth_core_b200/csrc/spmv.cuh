@@ -38,4 +38,26 @@ __device__ __forceinline__ void warp_row_spmv(int row, const int* __restrict__ r
   y[2] = a2;
 }
 
+// The NODAL dilational term of the factored solve matrix,
+//   S v = S1 v + sum_n t_n d_n,  t_n = c_m kp_n (d_n . v),
+// with d_n the divBlk row of node n (one 3-vector per neighbour slot) and
+// c_m = h^2 + h beta of its model (computeNodalIncompressibility,
+// FemModel3d.java:2632-2669, with the addPosJacobian / addVelJacobian
+// scales).  dil_node_t forms t_n of one node (slots a0 .. a1 of nbr_row and
+// divblk; fixed neighbours have row -1); the rows then add t_n d_n(i) over
+// their own entries.  Plain loads: v is rewritten between the PCG's grid
+// barriers.
+__device__ __forceinline__ double dil_node_t(int a0, int a1, const int* nbr_row, const double* divblk,
+                                             const double* v) {
+  double s = 0;
+  for (int a = a0; a < a1; a++) {
+    const int r = nbr_row[a];
+    if (r < 0) continue;
+    const double* g = divblk + 3 * (size_t)a;
+    const double* x = v + 3 * (size_t)r;
+    s += g[0] * x[0] + g[1] * x[1] + g[2] * x[2];
+  }
+  return s;
+}
+
 }  // namespace b200fem

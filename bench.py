@@ -463,24 +463,54 @@ def run_batched(dev, steps=20, tol=1e-10, sample_every=4, tune=True, layout=None
     }
 
 
-def block_bytes(N, E, nnzb, n_active, s_bytes=72, rest_bytes=72):
+def block_bytes(N, E, nnzb, n_active, s_bytes=72, rest_bytes=72, factored=None):
     """Algorithmic bytes of the MooneyRivlin block (4-node tets, one point):
     assembly 24 N (x) + 16 E (connectivity) + rest_bytes E (invJ0) + 64 E
     (scatter map) + s_bytes nnzb (S written, the NODAL 2-ring included) +
     24 N (f / b); PCG iteration (s_bytes + 4) nnzb (S and block columns) +
-    4 (Na + 1) + 48 Na + 72 Na + 9 * 24 Na."""
+    4 (Na + 1) + 48 Na + 72 Na + 9 * 24 Na.  Factored NODAL solve matrix
+    (factored = (direct blocks nnzb1, divBlk slots of the active nodes)):
+    S1 (nnzb1 blocks) and divBlk (24 per slot) written instead of the 2-ring
+    S; per iteration S1 and its columns, divBlk once, the rows' (node, slot)
+    entries (8 each, one per direct block), the slots' rows (4) and t (8 per
+    active node) in place of the 2-ring S."""
+    vec = 4 * (n_active + 1) + 48 * n_active + 72 * n_active + 9 * 24 * n_active
+    if factored is not None:
+        nnzb1, slots = factored
+        asm = 24 * N + 16 * E + rest_bytes * E + 64 * E + s_bytes * nnzb1 + 24 * slots + 24 * N
+        it = (s_bytes + 4) * nnzb1 + 24 * slots + 8 * nnzb1 + 4 * slots + 8 * n_active + vec
+        return asm, it
     asm = 24 * N + 16 * E + rest_bytes * E + 64 * E + s_bytes * nnzb + 24 * N
-    it = (s_bytes + 4) * nnzb + 4 * (n_active + 1) + 48 * n_active + 72 * n_active + 9 * 24 * n_active
+    it = (s_bytes + 4) * nnzb + vec
     return asm, it
 
 
-def run_block(dev, steps=50, tol=1e-10, cpu=True):
+def direct_counts(conn, fixed):
+    """Blocks between active nodes that share an element (self included),
+    and the neighbour slots (nodes sharing an element, self included) of the
+    active nodes."""
+    c = np.asarray(conn, dtype=np.int64)
+    N = int(c.max()) + 1
+    k = c.shape[1]
+    a = np.repeat(c, k, axis=1).reshape(-1)
+    b = np.tile(c, (1, k)).reshape(-1)
+    key = np.unique(a * N + b)
+    ia, ib = key // N, key % N
+    act = np.asarray(fixed).reshape(-1) == 0
+    return int(np.count_nonzero(act[ia] & act[ib])), int(np.count_nonzero(act[ia]))
+
+
+def run_block(dev, steps=50, tol=1e-10, cpu=True, factored=0, row_lanes=0, resident=0):
     """The MooneyRivlin tet block (60x30x30 cells of a 0.3x0.15x0.15 m block,
     270,000 tets, 58,621 nodes; AUTO soft incompressibility resolves to NODAL:
     3,935,980 blocks), `steps` BackwardEuler steps from rest in the plain
     FP64 form and in the mixed form, on device-resident state (S alone is
     283 MB, above the 126 MB L2, so nothing is flushed); the mixed form's
-    position error against the FP64 run after the same steps."""
+    position error against the FP64 run after the same steps.  factored:
+    B200FEM_OPT_NODAL_FACTORED (0 auto: the factored solve matrix, S1 51 MB
+    f64 with divBlk 21 MB, near the L2 size, so L2 is flushed between steps;
+    1 the assembled 2-ring S, 283 MB f64)."""
+    import ctypes
     import torch
     from artisynth_core_b200 import _lib as L
     from artisynth_core_b200 import workloads as W
@@ -489,10 +519,13 @@ def run_block(dev, steps=50, tol=1e-10, cpu=True):
     peak, kind = peaks()
     out = {"workload": "mooneyrivlin_tet_block_60x30x30 (270,000 tets, NODAL incompressibility, gravity, "
                        f"z-min fixed), {steps} steps h=0.01 from rest, PCG {tol:g}",
-           "steps": steps, "tol": tol, "l2": "working set above L2 (S alone 283 MB f64)"}
+           "steps": steps, "tol": tol, "l2": "flushed between steps (256 MB write)"}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    counts = direct_counts(wl.conn, wl.fixed)
     xs = {}
     for prec, name in ((L.PREC_FP64, "fp64"), (L.PREC_MIXED, "mixed")):
         m = wl.model(precision=prec, device=dev)
+        m.options = {L.OPT_NODAL_FACTORED: factored, L.OPT_ROW_LANES: row_lanes, L.OPT_PCG_RESIDENT: resident}
         ms = MechSystemSolver(m, tol=tol, max_iter=20000)
         t0 = time.perf_counter()
         m.engine()
@@ -503,23 +536,30 @@ def run_block(dev, steps=50, tol=1e-10, cpu=True):
         torch.cuda.synchronize()
         asm = pcg = 0.0
         its = []
-        t0 = time.perf_counter()
+        fv = ctypes.c_int()
+        m.engine().call("b200fem_get_option", L.OPT_NODAL_FACTORED, ctypes.byref(fv))
+        wall = 0.0
         for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
             ms.backwardEuler(wl.h, 1)
             a, p = ms.lastTiming()
+            wall += time.perf_counter() - t0
             asm += a
             pcg += p
             its.append(ms.stats.iterations)
-        wall = time.perf_counter() - t0
         xs[name], _ = m.getState()
         m._invalidate()
         sb = 72 if name == "fp64" else 36
         asm_b, it_b = block_bytes(wl.rest.shape[0], wl.conn.shape[0], sz["nnzb"], sz["n_active"], s_bytes=sb,
-                                  rest_bytes=72 if name == "fp64" else 36)
+                                  rest_bytes=72 if name == "fp64" else 36,
+                                  factored=counts if fv.value == 2 else None)
         mean_it = float(np.mean(its))
         asm_gbs = asm_b / (asm / steps * 1e-3) / 1e9
         pcg_gbs = it_b * (mean_it + 2) / (pcg / steps * 1e-3) / 1e9
         out[name] = {"steps_per_s": steps / wall, "device_ms_per_step": (asm + pcg) / steps,
+                     "solve_matrix": "factored (S1 + divBlk)" if fv.value == 2 else "assembled (2-ring S)",
                      "assembly_ms_per_step": asm / steps, "pcg_ms_per_step": pcg / steps,
                      "pcg_iterations_mean": mean_it, "build_s": build_s,
                      "element_updates_per_s": wl.conn.shape[0] * steps / wall,
@@ -840,7 +880,8 @@ def run_b200(args):
         block = None
         if world == 1 and not args.no_block:
             with ClockSampler(dev) as c:
-                block = run_block(dev, steps=args.block_steps, cpu=not args.no_cpu)
+                block = run_block(dev, steps=args.block_steps, cpu=not args.no_cpu, factored=args.nodal_factored,
+                                  row_lanes=args.block_row_lanes, resident=args.block_resident)
             block["clocks"] = c.summary()
         cpu = None
         if not args.no_cpu and world == 1:
@@ -896,6 +937,12 @@ def main():
                     help="batched leg: B200FEM_OPT_PCG_SPLIT (0 auto, 2 strided, 3 cluster)")
     ap.add_argument("--tet-assembly", type=int, default=1, choices=[0, 1],
                     help="batched leg: B200FEM_OPT_TET_ASSEMBLY (0 node rows, 1 element kernel + gather)")
+    ap.add_argument("--nodal-factored", type=int, default=0, choices=[0, 1, 2],
+                    help="block leg: B200FEM_OPT_NODAL_FACTORED (0 auto, 1 assembled 2-ring S, 2 factored)")
+    ap.add_argument("--block-row-lanes", type=int, default=0, choices=[0, 4, 8, 16, 32],
+                    help="block leg: B200FEM_OPT_ROW_LANES (0 auto)")
+    ap.add_argument("--block-resident", type=int, default=0, choices=[0, 1, 2],
+                    help="block leg: B200FEM_OPT_PCG_RESIDENT (0 auto)")
     ap.add_argument("--served-seconds", type=float, default=60.0, help="length of the served stream (0: skip)")
     ap.add_argument("--batch-tol", type=float, default=1e-10, help="PCG tolerance of the batched leg")
     ap.add_argument("--served-tol", type=float, default=1e-6,
@@ -917,7 +964,8 @@ def main():
     elif args.only == "block":
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_block(0, steps=args.block_steps, cpu=not args.no_cpu)), flush=True)
+        print(json.dumps(run_block(0, steps=args.block_steps, cpu=not args.no_cpu, factored=args.nodal_factored,
+                                   row_lanes=args.block_row_lanes, resident=args.block_resident)), flush=True)
     else:
         run_b200(args)
 

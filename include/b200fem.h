@@ -381,6 +381,22 @@ int b200fem_memory_usage(b200fem_handle h, unsigned long long* bytes);
                                        for the SpMV's loads); 0 (auto) as 2 while the solve
                                        matrix is at most 64 MB (it stays in L2), else as 1.  Set
                                        before b200fem_build; after it, 2 or 1 as in force */
+#define B200FEM_OPT_NODAL_FACTORED 13 /* BackwardEuler solve matrix of NODAL models: 2 factored
+                                         -- the element blocks of direct neighbours assembled
+                                         (S1), the dilational term (h^2 + h beta) sum_n kp_n
+                                         d_n d_n^T (computeNodalIncompressibility,
+                                         FemModel3d.java:2632-2669) applied from the divBlk
+                                         rows d_n inside every SpMV, so the PCG streams the
+                                         1-ring blocks instead of the 2-ring pattern; 1
+                                         assembled (the 2-ring blocks, as the reference
+                                         builds them); 0 (auto) as 2 wherever it applies
+                                         (element-path assembly, grid-wide PCG, no frame
+                                         attachments).  The step results agree to the PCG
+                                         tolerance.  After a b200fem_update_stress_stiffness
+                                         call the factored solve matrix is stale:
+                                         b200fem_spmv and b200fem_pcg_solve then need another
+                                         step.  Set before b200fem_build; after it, 2 or 1 as
+                                         in force */
 int b200fem_set_option(b200fem_handle h, int key, int value);
 /* the value in force (after b200fem_build: the resolved one, e.g. the split chosen by auto) */
 int b200fem_get_option(b200fem_handle h, int key, int* value);
