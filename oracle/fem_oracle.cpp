@@ -824,6 +824,10 @@ struct Model {
   std::vector<int> rowptr, col;
   // NODAL data
   std::vector<double> nodeRestVol, nodeVol, nodePressure;
+  // of the last update: per node kp = effective modulus / rest volume (0 for
+  // fixed nodes) and its divBlk row, one 3-vector per direct neighbour
+  std::vector<double> nodeKp;
+  std::vector<std::vector<double>> divBlk;
   // results of the last update
   std::vector<double> K;     // nnzb * 9
   std::vector<double> fint;  // 3N
@@ -1341,6 +1345,7 @@ static int update_stress_stiffness(Model& m, const double* x) {
   }
   if (nodal) {
     // computeNodalIncompressibility (FemModel3d.java:2632-2669)
+    m.nodeKp.assign(m.N, 0.0);
     for (int n = 0; n < m.N; n++) {
       if (m.sidx[n] < 0) continue;
       double restVol = m.nodeRestVol[n];
@@ -1348,6 +1353,7 @@ static int update_stress_stiffness(Model& m, const double* x) {
       double K = m.mat.kappa;
       double keff = (m.mat.bulk_potential == 0) ? K : K * (1 - std::log(Jn)) / (Jn * Jn);
       double kp = keff / restVol;
+      m.nodeKp[n] = kp;
       if (kp == 0) continue;
       const auto& nb = m.nbr[n];
       for (size_t a = 0; a < nb.size(); a++) {
@@ -1366,6 +1372,7 @@ static int update_stress_stiffness(Model& m, const double* x) {
       }
     }
   }
+  if (nodal) m.divBlk = std::move(div);
   // symmetrise: lower block := transpose of upper (FemModel3d.java:3003-3026)
   for (int bi = 0; bi < m.nact; bi++) {
     for (int p = m.rowptr[bi]; p < m.rowptr[bi + 1]; p++) {
@@ -1804,6 +1811,28 @@ void* orc_create(int type, int nnodes, const double* rest, int nelems, const int
 }
 
 void orc_destroy(void* h) { delete (Model*)h; }
+
+// The NODAL terms of the last orc_update_stress_stiffness: per node its
+// direct neighbours (sorted: ptr[N+1], idx), kp (0 for fixed nodes) and its
+// divBlk row (3 values per neighbour, in idx order).  Any output may be
+// NULL; returns the neighbour count, or -1 when the model is not NODAL or
+// has not been updated.
+int orc_nodal_factors(void* h, int* ptr, int* idx, double* kp, double* div) {
+  const Model& m = *(const Model*)h;
+  if (m.incomp != INCOMP_NODAL || (int)m.divBlk.size() != m.N || (int)m.nodeKp.size() != m.N) return -1;
+  int q = 0;
+  for (int n = 0; n < m.N; n++) {
+    if (ptr) ptr[n] = q;
+    for (size_t a = 0; a < m.nbr[n].size(); a++, q++) {
+      if (idx) idx[q] = m.nbr[n][a];
+      if (div)
+        for (int c = 0; c < 3; c++) div[3 * (size_t)q + c] = m.divBlk[n][3 * a + c];
+    }
+    if (kp) kp[n] = m.nodeKp[n];
+  }
+  if (ptr) ptr[m.N] = q;
+  return q;
+}
 int orc_incomp_method(void* h) { return ((Model*)h)->incomp; }
 int orc_num_active(void* h) { return ((Model*)h)->nact; }
 int orc_nnzb(void* h) { return (int)((Model*)h)->col.size(); }

@@ -88,6 +88,8 @@ def lib():
         L.orc_create_mixed.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _ip, _ip, _ip, ctypes.c_int, _dp,
                                        ctypes.c_double, ctypes.c_int]
         L.orc_create_mixed.restype = vp
+        L.orc_nodal_factors.argtypes = [vp] + [ctypes.c_void_p] * 4
+        L.orc_nodal_factors.restype = ctypes.c_int
         L.orc_set_element_materials.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_element_materials.restype = ctypes.c_int
         L.orc_elem_num_ip.argtypes = [vp, ctypes.c_int]
@@ -192,6 +194,19 @@ class OracleModel:
         self.nact = self.L.orc_num_active(self.h)
         self.nnzb = self.L.orc_nnzb(self.h)
         self.incomp = self.L.orc_incomp_method(self.h)
+
+    def nodal_factors(self):
+        """The NODAL terms of the last update_stress_stiffness: (ptr, idx, kp,
+        div) -- each node's sorted direct neighbours, kp and divBlk row."""
+        q = self.L.orc_nodal_factors(self.h, None, None, None, None)
+        if q < 0:
+            raise ValueError("no NODAL terms (model not NODAL or not updated)")
+        ptr = np.zeros(self.N + 1, dtype=np.int32)
+        idx = np.zeros(q, dtype=np.int32)
+        kp = np.zeros(self.N)
+        div = np.zeros((q, 3))
+        self.L.orc_nodal_factors(self.h, ptr.ctypes.data, idx.ctypes.data, kp.ctypes.data, div.ctypes.data)
+        return ptr, idx, kp, div
 
     def set_element_materials(self, materials):
         """materials: one entry per element, None for the model's material or
