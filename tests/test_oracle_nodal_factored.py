@@ -110,3 +110,20 @@ def test_two_phase_product_equals_the_blocks(oracle):
             assert idx[slot] == i
             y[r] += t[n] * div[slot]
     assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_bench_factored_byte_counts(oracle):
+    """bench.py's counts for the factored roofline: direct blocks between
+    active nodes (the 1-ring pattern, as the oracle builds it without NODAL)
+    and the neighbour slots of the active nodes (the divBlk rows)."""
+    import bench
+    m, xyz, conn = _model(oracle, 0, [1000.0, 500.0, 0, 0, 0, 1e5, 0, 0])
+    fixed = (xyz[:, 0] <= -0.5 + 1e-9).astype(np.int32)
+    nnzb1, slots = bench.direct_counts(np.asarray(conn).reshape(len(conn), -1), fixed)
+    off = oracle.OracleModel(0, xyz, conn, fixed, 2, [1000.0, 500.0, 0, 0, 0, 1e5, 0, 0], 1000.0,
+                             oracle.INCOMP_OFF)
+    assert nnzb1 == off.nnzb
+    m.update_stress_stiffness(xyz)
+    ptr, _, _, _ = m.nodal_factors()
+    act = np.nonzero(fixed == 0)[0]
+    assert slots == int(np.sum(ptr[act + 1] - ptr[act]))
